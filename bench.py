@@ -1,0 +1,362 @@
+"""Benchmark: tetrahedral-cage deform + render frames on B200.
+
+Workload (the reference's tet-cage configuration): 1,100,000 Gaussians drawn
+from the seeded synthetic distribution with means scaled into [-1, 1]^3, a
+5x5x5-cube / 750-tet / 216-vertex cage driven by the spring solver (bottom
+layer pinned, stiffness 40, damping 4/s, dt 1/60), 1920x1080, a camera
+orbiting at radius 4. One step = one frame: a host spring step, then Stage 1
+(deform), Stage 2 (project), Stage 3 (bin + sort) and Stage 4 (composite).
+
+Arms:
+  python bench.py [--gpus N --steps K --warmup W]     this library (CUDA, sm_100a)
+  python bench.py --impl reference ...                the reference's CPU path
+                                                      (its Rayon backend restated
+                                                      in oracle/, all host threads)
+Multi-GPU (torchrun, one process per GPU): replicas; each rank renders its own
+views (frames rank, rank+N, ...), no data exchange; value = all frames / max
+rank time (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "ms/frame per stage & views/s; learned vs exact MVC deform time at ≤1e-3 err"
+UNIT = "views/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--gaussians", type=int, default=1_100_000)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(args):
+    from cindergs_b200 import workloads
+    return workloads.tet_cage_orbit(n=args.gaussians, width=args.width, height=args.height)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        mx.append(float(parts[2]))
+                    except ValueError:
+                        continue
+                    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                             "sw_power_cap"]
+                    for name, v in zip(names, parts[5:9]):
+                        if v.lower().startswith("active"):
+                            reasons.add(name)
+        except Exception:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_frames(wl, bind_tet, bind_w, frames, start_frame=0):
+    """Renders `frames` frames with the restated reference CPU backend; returns
+    (seconds per frame list, threads)."""
+    import oracle
+    m = wl.cage.mesh
+    times = []
+    for f in range(frames):
+        cam = wl.camera(start_frame + f)
+        comp = wl.compositor(cam)
+        t0 = time.perf_counter()
+        oracle.ref_frame(wl.scene.as_dict(), cam.to_array(), wl.width, wl.height,
+                         np.asarray(comp.background_color, np.float32),
+                         np.asarray(comp.camera_position, np.float32), wl.sh_degree,
+                         cage=dict(verts=wl.cage.vertices(), elems=m.elements, inv_dm=m.inv_dm,
+                                   bind_tet=bind_tet, bind_w=bind_w),
+                         split_thr=wl.strain_split_threshold, mip=wl.mip_filter_3d_var)
+        times.append(time.perf_counter() - t0)
+        wl.step()
+    return times, oracle.threads()
+
+
+def config_dict(args, wl, world):
+    return {"workload": "tet-cage deform + render, orbit camera",
+            "gaussians": args.gaussians, "width": args.width, "height": args.height,
+            "cage": "5x5x5 cubes x 6 tets (750 tets, 216 vertices), springs k=40 c=4 dt=1/60",
+            "sh_degree": 3, "keys": "32-bit tile|depth", "radix_bits": 8,
+            "l2": "inputs larger than L2 (resident scene 255 MB + 26M tile entries)",
+            "parallelism": f"replicas x{world} (views sharded, no exchange)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (restated) on host cores."""
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    import oracle
+    from cindergs_b200 import workloads  # noqa: F401
+    wl = workload(args)
+    m = wl.cage.mesh
+    bt, bw = oracle.bind_points(wl.scene.positions, m.rest_vertices, m.elements, m.inv_dm,
+                                m.bounds())
+    for _ in range(args.warmup):
+        wl.step()
+    times, threads = cpu_reference_frames(wl, bt, bw, args.steps)
+    total = sum(times)
+    value = args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(args, wl, 1),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full frames of the workload"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from cindergs_b200 import GpuPipelineState
+
+    wl = workload(args)
+    stream = torch.cuda.Stream(device=local)
+    st = GpuPipelineState(local, stream=stream.cuda_stream)
+    st.upload_scene(wl.scene)
+    cages = wl.bind(st)
+    frame = rank
+
+    def render(profile=False, timings=True):
+        nonlocal frame
+        wl.step()
+        cam = wl.camera(frame)
+        frame += world
+        return st.execute_frame_gpu(wl.scene, cages, cam, wl.compositor(cam),
+                                    wl.strain_split_threshold, wl.mip_filter_3d_var,
+                                    1.0 / 255.0, 0.5, profile_stages=profile,
+                                    stage_timings=timings)
+
+    for _ in range(max(args.warmup, 3)):
+        render()
+    # Per-stage device times of a few representative frames (not timed).
+    stage_rows = [render(profile=True, timings=True) for _ in range(3)]
+    st.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(local)
+
+    # ---- timed region: inputs resident in HBM, CUDA events on the library stream
+    st.kernel_profile_reset()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    clock = ClockSampler(local)
+    barrier()
+    with clock:
+        start.record(stream)
+        for _ in range(args.steps):
+            render(profile=True, timings=False)
+        end.record(stream)
+        barrier()
+    ms = start.elapsed_time(end)
+    kp = st.kernel_profile()
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1000.0)
+
+    # ---- e2e: public API with host buffers, copies inside the timed region
+    pinned_out = torch.empty((args.height, args.width, 4), dtype=torch.uint8).pin_memory()
+    out_np = pinned_out.numpy()
+    vert_pinned = torch.empty(wl.cage.mesh.rest_vertices.shape, dtype=torch.float32).pin_memory()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_start = torch.cuda.Event(enable_timing=True)
+    e2e_end = torch.cuda.Event(enable_timing=True)
+    e2e_start.record(stream)
+    import ctypes
+    for _ in range(args.steps):
+        wl.step()
+        vert_pinned.numpy()[:] = wl.cage.vertices()
+        cam = wl.camera(frame)
+        frame += world
+        # host vertices -> device (pinned source), then the frame, then the pixels back
+        st._check(st._lib.cgs_cage_vertices_update(
+            st.handle, ctypes.c_void_p(vert_pinned.data_ptr()), vert_pinned.shape[0]),
+            "cgs_cage_vertices_update")
+        cam_c = wl.compositor(cam)
+        st.execute_frame_gpu(wl.scene, cages, cam, cam_c, wl.strain_split_threshold,
+                             wl.mip_filter_3d_var, 1.0 / 255.0, 0.5)
+        st._check(st._lib.cgs_readback_rgba8(st.handle, ctypes.c_void_p(out_np.ctypes.data),
+                                             args.width, args.height), "cgs_readback_rgba8")
+    e2e_end.record(stream)
+    barrier()
+    e2e_ms = max(e2e_start.elapsed_time(e2e_end), (time.perf_counter() - t0) * 1000.0)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * args.steps / (e2e_ms / 1000.0)
+
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        kernels = {}
+        for name, d in kp.items():
+            if name == "clear" or d["launches"] == 0:
+                continue
+            avg_ms = d["ms"] / max(args.steps, 1)
+            gbs = d["alg_bytes"] / (d["ms"] / 1000.0) / 1e9 if d["ms"] > 0 else 0.0
+            kernels[name] = {"ms_per_frame": avg_ms, "launches": d["launches"],
+                             "alg_bytes_per_frame": d["alg_bytes"] // max(args.steps, 1),
+                             "achieved_gbs": gbs, "hbm_frac": gbs / hbm}
+        dom = max(kernels, key=lambda k: kernels[k]["ms_per_frame"])
+        dk = kernels[dom]
+        per_launch_bytes = kp[dom]["alg_bytes"] / kp[dom]["launches"]
+        per_launch_ms = kp[dom]["ms"] / kp[dom]["launches"]
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
+        if os.path.exists(tp):
+            try:
+                traffic = json.load(open(tp)).get(dom)
+            except Exception:
+                traffic = None
+        gpu_launches = sum(d["launches"] for n_, d in kp.items() if n_ != "clear")
+        stages = {k: statistics.median(getattr(r, k) for r in stage_rows)
+                  for k in ("stage1_deform_ms", "stage2_project_ms", "stage3_bin_sort_ms",
+                            "stage4_composite_ms")}
+        last = stage_rows[-1]
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(args, wl, world),
+            "stages_ms": stages,
+            "frame_counts": {"active_gaussians": last.active_gaussians,
+                             "surviving_gaussians": last.surviving_gaussians,
+                             "tile_entries": last.total_tile_entries},
+            "kernels": kernels,
+            "roofline": {"kernel": dom, "bound": "hbm",
+                         "achieved": per_launch_bytes / (per_launch_ms / 1000.0) / 1e9,
+                         "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": (per_launch_bytes / (per_launch_ms / 1000.0) / 1e9) / hbm,
+                         "traffic": traffic, "alg_bytes_per_launch": per_launch_bytes},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step":
+                    int(wl.cage.mesh.rest_vertices.nbytes),
+                    "d2h_bytes_per_step": int(args.width * args.height * 4 + 36)},
+            "gpu_launches": gpu_launches,
+            "clocks": clock.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                bt = cages.bind_tet
+                bw = cages.bind_w
+                times, threads = cpu_reference_frames(wl, bt, bw, 1, start_frame=frame)
+                line["cpu_baseline"] = {"value": 1.0 / times[0], "unit": UNIT, "cores": threads,
+                                        "kind": "port",
+                                        "sample": "1 full frame of the workload (reference "
+                                                  "CPU path restated in oracle/)"}
+            except Exception as exc:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
+                                        "kind": "port", "sample": f"failed: {exc}"}
+        print(json.dumps(line), flush=True)
+    st.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,155 @@
+// Host-side launchers for the sm_100a kernels (one per .cu translation unit).
+// All launchers enqueue on `stream` and return the launch error code.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace cgs {
+
+// ---- Stage 1 (stage1_deform.cu) --------------------------------------------
+struct DeformArgs {
+  uint32_t n;                 // rest Gaussians
+  uint32_t num_tets;
+  const float* verts;         // [V*3] current cage vertices
+  const uint4* elems;         // [T]
+  const float* inv_dm;        // [T*9]
+  float* tet_J;               // [T*9] out (column-major)
+  float* tet_R;               // [T*9] out (column-major)
+  float* tet_stretch;         // [T] out
+  const uint32_t* bind_tet;   // [n]
+  const float4* bind_w;       // [n]
+  const float4* rest_pos;     // [n] xyz + opacity
+  const float4* rest_cova;    // [n] xx, xy, xz, yy
+  const float2* rest_covb;    // [n] yz, zz
+  float4* def_pos;            // [2n]
+  float4* def_cova;           // [2n]
+  float2* def_covb;           // [2n]
+  uint2* split_meta;          // [n] (parent, tet)
+  uint32_t* split_count;      // persistent device word
+  unsigned long long* status; // [ceil(n/256)] chained-scan status, zeroed
+  FrameCounters* fc;
+  float split_threshold;
+  float mip;
+};
+cudaError_t launch_tet_transforms(const DeformArgs& a, cudaStream_t s);
+cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s);
+
+struct BindArgs {
+  uint32_t n;
+  uint32_t num_tets;
+  const float4* points;   // [n] xyz (+ unused w)
+  const float* tet_x0;    // [T*3] rest position of each tet's first vertex
+  const float* inv_dm;    // [T*9]
+  int use_bounds;
+  float bmin[3], bmax[3];
+  uint32_t* bind_tet;     // [n] out
+  float4* bind_w;         // [n] out
+};
+cudaError_t launch_bind(const BindArgs& a, cudaStream_t s);
+
+// ---- Stage 2 (stage2_project.cu) -------------------------------------------
+struct ProjectArgs {
+  const float4* pos;          // [max_n] xyz + opacity
+  const float4* cova;         // [max_n]
+  const float2* covb;         // [max_n]
+  const void* sh;             // SH planes: f32 -> float4 [12][sh_stride]; f16 -> uint4 [6][sh_stride]
+  int sh_f16;
+  uint32_t sh_stride;         // plane stride (rest Gaussian count)
+  const uint32_t* bind_tet;   // [n_rest] or null
+  const float* tet_R;         // [T*9] or null
+  uint32_t num_tets;
+  const uint2* split_meta;    // [n_rest] or null
+  const uint32_t* split_count;  // device word or null (no splitting)
+  uint32_t n_rest;
+  uint32_t max_n;             // grid covers max_n splats
+  float cam[24];
+  float cam_pos[3];
+  float mip, min_opacity, min_radius;
+  uint32_t sh_degree;
+  SplatRec* out;              // [max_n]
+  FrameCounters* fc;
+};
+cudaError_t launch_project(const ProjectArgs& a, cudaStream_t s);
+
+// Rest-scene layout conversion from the reference's interleaved SoA.
+cudaError_t launch_scene_layout(uint32_t n, const float* pos, const float* cov, const float* opa,
+                                const void* sh, int sh_f16, float4* out_pos, float4* out_cova,
+                                float2* out_covb, void* out_sh, cudaStream_t s);
+
+// ---- Stage 3 (stage3_bin.cu) -------------------------------------------------
+struct BinArgs {
+  const SplatRec* recs;
+  const uint32_t* split_count;  // null when no splitting
+  uint32_t n_rest;
+  uint32_t max_n;
+  uint32_t width, height, tiles_x, tiles_y;
+  uint32_t* offsets;            // [max_n]
+  unsigned long long* status;   // [ceil(max_n/256)] zeroed
+  FrameCounters* fc;
+  // emission
+  int key64;
+  uint32_t depth_base_bits;     // near-plane exponent bits (32-bit keys)
+  uint32_t depth_bits;          // depth bits in a 32-bit key
+  uint32_t* keys;               // 32-bit: packed keys; 64-bit: tile ids
+  uint32_t* depths;             // 64-bit: raw depth bits
+  uint32_t* ids;
+  uint32_t* hist;               // [passes][1 << radix_bits] digit histograms, zeroed
+  uint32_t radix_bits;
+  uint32_t sort_bits;           // 32-bit key bits (tile + depth)
+  uint32_t tile_bits;           // 64-bit: tile id bits
+  uint32_t entry_cap;           // capacity of keys/depths/ids
+};
+cudaError_t launch_count_scan(const BinArgs& a, cudaStream_t s);
+cudaError_t launch_emit(const BinArgs& a, cudaStream_t s);
+// Per-tile [start, end) from sorted words: tile = word >> shift. ranges zeroed.
+cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
+                               uint32_t total_tiles, uint32_t* ranges, cudaStream_t s);
+// Generic exclusive scan of n u32 (chained scan); total -> *d_total.
+cudaError_t launch_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* d_total,
+                            unsigned long long* status, uint32_t* tile_ctr, uint32_t* status_word,
+                            cudaStream_t s);
+uint32_t scan_tiles(uint32_t n);
+
+// ---- radix sort (radix_sort.cu) ----------------------------------------------
+struct SortArgs {
+  uint32_t* keys[2];     // ping-pong key buffers
+  uint32_t* vals[2];     // ping-pong payload word 0
+  uint32_t* vals2[2];    // ping-pong payload word 1 (null for one-word payloads)
+  const uint32_t* n_ptr; // device element count (may exceed capacity -> capacity flag)
+  uint32_t capacity;     // elements the buffers hold; grid is sized for it
+  uint32_t first_bit;    // lowest key bit to sort on
+  uint32_t num_bits;     // bits to sort on (from first_bit)
+  uint32_t radix_bits;   // 4 or 8
+  uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
+  uint32_t* status;      // [passes][tiles][radix] zeroed
+  uint32_t* tile_ctr;    // [passes] zeroed
+  uint32_t* status_word;
+  int src;               // index of the buffer holding the input
+};
+// Runs the passes; returns in *out_src the index of the buffer with the result.
+cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s);
+cudaError_t launch_histogram(const uint32_t* keys, const uint32_t* n_ptr, uint32_t capacity,
+                             uint32_t first_bit, uint32_t num_bits, uint32_t radix_bits,
+                             uint32_t* hist, cudaStream_t s);
+uint32_t sort_tiles(uint32_t capacity);
+uint32_t sort_passes(uint32_t num_bits, uint32_t radix_bits);
+
+// ---- Stage 4 (stage4_composite.cu) -------------------------------------------
+struct CompositeArgs {
+  const SplatRec* recs;
+  const uint32_t* sorted_ids;
+  const uint32_t* ranges;
+  uint32_t width, height, tiles_x, tiles_y;
+  uint32_t pitch_px;        // RGBA8 row pitch in pixels
+  float bg[4];
+  uint32_t* out_rgba8;
+  float4* out_f32;          // null when not requested
+  FrameCounters* fc;
+  uint32_t num_recs;        // splat records (ids at or above are rejected)
+  uint32_t num_entries;     // sorted ids (ranges beyond are clamped)
+};
+cudaError_t launch_composite(const CompositeArgs& a, cudaStream_t s);
+
+}  // namespace cgs

@@ -1,0 +1,1149 @@
+// Context, device residency, frame orchestration and the C ABI (include/cgs.h).
+//
+// Mirrors GpuPipelineState { GpuSceneState, GpuFrameArena }
+// (render/gpu_state.rs:95-1343): the rest scene and cage topology stay
+// resident and are re-uploaded only when the caller uploads them again; cage
+// vertices are compared with the last upload so a stationary cage skips
+// Stage 1; Stage 3's sorted lists are reused while the Stage 3 cache key
+// (deform generation, camera, viewport, filter parameters) is unchanged;
+// intermediate buffers grow by 1.5x and never shrink (gpu_pool.rs:43-49).
+//
+// One host synchronisation per frame that runs Stage 3: the 16-byte counter
+// block is read back after the fused count+scan kernel to size the key
+// buffers (the reference reads back three counters at the same point,
+// gpu_state.rs:1020-1035). Status bits set by bounded device waits are
+// checked at every synchronisation point and reported as CGS_E_TIMEOUT.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cgs.h"
+#include "kernels.h"
+
+using namespace cgs;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;  // bytes
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+// calculate_exponential_growth (render/gpu_pool.rs:43-49), in bytes.
+size_t grow(size_t current, size_t needed) {
+  if (needed <= current) return current;
+  size_t scaled = (size_t)std::ceil((double)current * 1.5);
+  size_t v = scaled > needed ? scaled : needed;
+  return v < 256 ? 256 : v;
+}
+
+struct Stage3Key {
+  uint64_t deform_generation = ~0ull;
+  uint32_t view[16] = {};
+  uint32_t fx = 0, fy = 0, cx = 0, cy = 0, near_bits = 0;
+  uint32_t width = 0, height = 0;
+  uint32_t mip = 0, min_opa = 0, min_rad = 0;
+  uint32_t radix_bits = 0;
+  bool operator==(const Stage3Key& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
+uint32_t fbits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+}  // namespace
+
+struct cgs_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  // rest scene
+  uint32_t n = 0;
+  bool scene_ready = false;
+  int sh_f16 = 0;
+  DevBuf rest_pos, rest_cova, rest_covb, rest_sh;
+  // cages
+  uint32_t num_tets = 0, num_verts = 0;
+  bool has_cages = false;
+  DevBuf tet_elems, tet_inv_dm, cage_verts, bind_tet, bind_w;
+  std::vector<float> last_verts;
+  bool verts_uploaded = false;
+  bool deformed_valid = false;
+  uint64_t deform_generation = 1;
+  uint32_t last_split_bits = 0xFFFFFFFFu, last_mip_bits = 0xFFFFFFFFu;
+  // arena
+  DevBuf tet_J, tet_R, tet_S, def_pos, def_cova, def_covb, split_meta, persist;
+  DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_status;
+  DevBuf fb_rgba8, fb_f32;
+  DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
+  FrameCounters* h_counters = nullptr;  // pinned: [0] mid-frame, [1] end of frame
+  uint32_t* h_split = nullptr;          // pinned
+  // Stage 3 cache and last-frame state
+  bool s3_valid = false;
+  Stage3Key s3_key;
+  uint32_t s3_entries = 0, s3_surviving = 0, s3_active = 0;
+  int s3_key64 = 0, s3_src = 0;
+  uint32_t s3_depth_bits = 0;
+  uint32_t last_w = 0, last_h = 0, last_pitch = 0, last_active = 0, last_tiles = 0;
+  uint32_t last_sort_passes = 0;
+  bool last_f32 = false, frame_done = false, end_copy_pending = false;
+  // Kernel-level profile (params.profile_stages): an event pair per launch,
+  // double-buffered by frame parity. A frame's events are folded into the
+  // accumulators once they are known to be complete (at the next frame's
+  // mid-frame synchronisation or when the profile is read), so profiling adds
+  // no host synchronisation of its own.
+  static constexpr int kMaxMarks = 32;
+  cudaEvent_t kev[2][2 * kMaxMarks] = {};
+  int kid[2][kMaxMarks] = {};
+  int kcount[2] = {0, 0};
+  bool kpending[2] = {false, false};
+  int kpar = 0;
+  bool kprof = false;
+  cgs_kernel_profile kp_acc{};
+  void kbegin(int id) {
+    const int c = kcount[kpar];
+    if (!kprof || c >= kMaxMarks) return;
+    kid[kpar][c] = id;
+    cudaEventRecord(kev[kpar][2 * c], stream);
+  }
+  void kend() {
+    const int c = kcount[kpar];
+    if (!kprof || c >= kMaxMarks) return;
+    cudaEventRecord(kev[kpar][2 * c + 1], stream);
+    kcount[kpar] = c + 1;
+  }
+  void kfold(int par, cgs_kernel_profile* frame) {
+    if (!kpending[par]) return;
+    for (int c = 0; c < kcount[par]; ++c) {
+      float ms = 0.0f;
+      cudaEventSynchronize(kev[par][2 * c + 1]);
+      cudaEventElapsedTime(&ms, kev[par][2 * c], kev[par][2 * c + 1]);
+      kp_acc.ms[kid[par][c]] += ms;
+      if (frame) frame->ms[kid[par][c]] += ms;
+    }
+    kpending[par] = false;
+    kcount[par] = 0;
+  }
+  void kcount_launch(int id, uint32_t launches, uint64_t bytes) {
+    if (!kprof) return;
+    kp_acc.launches[id] += launches;
+    kp_acc.alg_bytes[id] += bytes;
+  }
+
+  int fail(int code, const std::string& msg) {
+    err = msg;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* what) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return CGS_E_CUDA;
+  }
+  int ensure(DevBuf& b, size_t bytes, const char* what) {
+    if (bytes <= b.cap && b.p) return CGS_OK;
+    size_t nb = grow(b.cap, bytes);
+    if (b.p) {
+      cudaStreamSynchronize(stream);
+      cudaFree(b.p);
+      b.p = nullptr;
+      b.cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, nb);
+    if (e != cudaSuccess) {
+      b.p = nullptr;
+      return fail(CGS_E_OOM, std::string("device allocation failed for ") + what + " (" +
+                                 std::to_string(nb) + " bytes): " + cudaGetErrorString(e));
+    }
+    b.cap = nb;
+    return CGS_OK;
+  }
+  // Checks the status bits of the last completed frame (after a sync).
+  int check_end_status() {
+    if (!end_copy_pending) return CGS_OK;
+    end_copy_pending = false;
+    const uint32_t st = h_counters[1].status;
+    if (st & (kStatusLookbackTimeout | kStatusBarrierTimeout))
+      return fail(CGS_E_TIMEOUT, "a bounded device-side wait gave up during the last frame");
+    if (st & kStatusCapacity) return fail(CGS_E_CAPACITY, "tile entries exceeded capacity");
+    return CGS_OK;
+  }
+};
+
+#define CGS_CUDA(call, what)                 \
+  do {                                       \
+    cudaError_t e_ = (call);                 \
+    if (e_ != cudaSuccess) return ctx->cuda_fail(e_, what); \
+  } while (0)
+#define CGS_TRY(call)          \
+  do {                         \
+    int r_ = (call);           \
+    if (r_ != CGS_OK) return r_; \
+  } while (0)
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+const char* cgs_version(void) { return "cindergs_b200 0.1.0 (sm_100a)"; }
+
+int cgs_ctx_create(int device, void* stream, cgs_ctx** out_ctx) {
+  if (!out_ctx) return CGS_E_ARG;
+  *out_ctx = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CGS_E_CUDA;
+  if (device < 0 || device >= ndev) return CGS_E_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return CGS_E_CUDA;
+  cgs_ctx* ctx = new cgs_ctx();
+  ctx->device = device;
+  if (stream) {
+    ctx->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return CGS_E_CUDA;
+    }
+    ctx->own_stream = true;
+  }
+  if (cudaMallocHost(&ctx->h_counters, 2 * sizeof(FrameCounters)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_split, 16) != cudaSuccess) {
+    delete ctx;
+    return CGS_E_OOM;
+  }
+  std::memset(ctx->h_counters, 0, 2 * sizeof(FrameCounters));
+  for (auto& set : ctx->kev)
+    for (auto& e : set)
+      if (cudaEventCreate(&e) != cudaSuccess) {
+        delete ctx;
+        return CGS_E_CUDA;
+      }
+  // persistent words: [0] split count
+  if (ctx->ensure(ctx->persist, 256, "persistent words") != CGS_OK ||
+      cudaMemset(ctx->persist.p, 0, 256) != cudaSuccess) {
+    delete ctx;
+    return CGS_E_OOM;
+  }
+  *out_ctx = ctx;
+  return CGS_OK;
+}
+
+int cgs_ctx_destroy(cgs_ctx* ctx) {
+  if (!ctx) return CGS_E_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& set : ctx->kev)
+    for (auto& e : set)
+      if (e) cudaEventDestroy(e);
+  if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+  if (ctx->h_split) cudaFreeHost(ctx->h_split);
+  cudaStream_t s = ctx->stream;
+  bool own = ctx->own_stream;
+  delete ctx;
+  if (own) cudaStreamDestroy(s);
+  return CGS_OK;
+}
+
+const char* cgs_last_error(const cgs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int cgs_ctx_synchronize(cgs_ctx* ctx) {
+  if (!ctx) return CGS_E_ARG;
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  return ctx->check_end_status();
+}
+
+int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out) {
+  if (!ctx || !out) return CGS_E_ARG;
+  const DevBuf* bufs[] = {&ctx->rest_pos, &ctx->rest_cova, &ctx->rest_covb, &ctx->rest_sh,
+                          &ctx->tet_elems, &ctx->tet_inv_dm, &ctx->cage_verts, &ctx->bind_tet,
+                          &ctx->bind_w, &ctx->tet_J, &ctx->tet_R, &ctx->tet_S, &ctx->def_pos,
+                          &ctx->def_cova, &ctx->def_covb, &ctx->split_meta, &ctx->persist,
+                          &ctx->recs, &ctx->offsets, &ctx->scratch, &ctx->ranges, &ctx->keys[0],
+                          &ctx->keys[1], &ctx->ids[0], &ctx->ids[1], &ctx->depths[0],
+                          &ctx->depths[1], &ctx->radix_status, &ctx->fb_rgba8, &ctx->fb_f32,
+                          &ctx->prim[0], &ctx->prim[1], &ctx->prim[2], &ctx->prim[3]};
+  uint64_t t = 0;
+  for (auto* b : bufs) t += b->cap;
+  *out = t;
+  return CGS_OK;
+}
+
+int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* cov,
+                     const float* opa, const void* sh, int32_t sh_format) {
+  if (!ctx) return CGS_E_ARG;
+  if (sh_format != CGS_SH_F32 && sh_format != CGS_SH_F16)
+    return ctx->fail(CGS_E_ARG, "sh_format must be CGS_SH_F32 or CGS_SH_F16");
+  if (n >= (1ull << 30)) return ctx->fail(CGS_E_CAPACITY, "scene exceeds 2^30 Gaussians");
+  if (n > 0 && (!pos || !cov || !opa || !sh)) return ctx->fail(CGS_E_ARG, "null scene array");
+  cudaSetDevice(ctx->device);
+  const size_t shb = (size_t)n * 48 * (sh_format == CGS_SH_F16 ? 2 : 4);
+  const size_t nn = n ? n : 1;
+  CGS_TRY(ctx->ensure(ctx->rest_pos, nn * 16, "rest positions"));
+  CGS_TRY(ctx->ensure(ctx->rest_cova, nn * 16, "rest covariances"));
+  CGS_TRY(ctx->ensure(ctx->rest_covb, nn * 8, "rest covariances"));
+  CGS_TRY(ctx->ensure(ctx->rest_sh, shb ? shb : 16, "rest SH"));
+  if (n > 0) {
+    // Stage the interleaved arrays, then convert to the resident layout.
+    void* stage = nullptr;
+    const size_t pb = (size_t)n * 12, cb = (size_t)n * 24, ob = (size_t)n * 4;
+    const size_t ofs_c = (pb + 255) & ~(size_t)255, ofs_o = ofs_c + ((cb + 255) & ~(size_t)255),
+                 ofs_s = ofs_o + ((ob + 255) & ~(size_t)255);
+    CGS_CUDA(cudaMalloc(&stage, ofs_s + shb), "cudaMalloc scene staging");
+    char* st = (char*)stage;
+    cudaError_t e = cudaMemcpyAsync(st, pos, pb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st + ofs_c, cov, cb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st + ofs_o, opa, ob, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st + ofs_s, sh, shb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = launch_scene_layout((uint32_t)n, (const float*)st, (const float*)(st + ofs_c),
+                              (const float*)(st + ofs_o), st + ofs_s, sh_format == CGS_SH_F16,
+                              ctx->rest_pos.as<float4>(), ctx->rest_cova.as<float4>(),
+                              ctx->rest_covb.as<float2>(), ctx->rest_sh.p, ctx->stream);
+    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    cudaFree(stage);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "scene upload");
+    if (e2 != cudaSuccess) return ctx->cuda_fail(e2, "scene upload");
+  }
+  ctx->n = (uint32_t)n;
+  ctx->sh_f16 = sh_format == CGS_SH_F16;
+  ctx->scene_ready = true;
+  ctx->deformed_valid = false;
+  ctx->deform_generation++;
+  ctx->s3_valid = false;
+  ctx->has_cages = false;  // cage bindings refer to the previous scene
+  ctx->num_tets = 0;
+  return CGS_OK;
+}
+
+int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
+                         const float* inv_dm, uint32_t num_verts, const uint32_t* bind_tet,
+                         const float* bind_w) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "upload the scene before the cages");
+  cudaSetDevice(ctx->device);
+  if (num_tets == 0) {
+    if (ctx->has_cages) ctx->deform_generation++;
+    ctx->has_cages = false;
+    ctx->num_tets = 0;
+    ctx->s3_valid = false;
+    return CGS_OK;
+  }
+  if (!elems || !inv_dm || !bind_tet || !bind_w || num_verts == 0)
+    return ctx->fail(CGS_E_ARG, "null cage array or zero vertices");
+  for (uint64_t i = 0; i < (uint64_t)num_tets * 4; ++i)
+    if (elems[i] >= num_verts) return ctx->fail(CGS_E_ARG, "tet element index out of range");
+  const uint32_t n = ctx->n;
+  CGS_TRY(ctx->ensure(ctx->tet_elems, (size_t)num_tets * 16, "tet elements"));
+  CGS_TRY(ctx->ensure(ctx->tet_inv_dm, (size_t)num_tets * 36, "tet inv_dm"));
+  CGS_TRY(ctx->ensure(ctx->cage_verts, (size_t)num_verts * 12, "cage vertices"));
+  CGS_TRY(ctx->ensure(ctx->bind_tet, (size_t)(n ? n : 1) * 4, "bindings"));
+  CGS_TRY(ctx->ensure(ctx->bind_w, (size_t)(n ? n : 1) * 16, "binding weights"));
+  CGS_CUDA(cudaMemcpyAsync(ctx->tet_elems.p, elems, (size_t)num_tets * 16, cudaMemcpyHostToDevice, ctx->stream), "upload elems");
+  CGS_CUDA(cudaMemcpyAsync(ctx->tet_inv_dm.p, inv_dm, (size_t)num_tets * 36, cudaMemcpyHostToDevice, ctx->stream), "upload inv_dm");
+  if (n) {
+    CGS_CUDA(cudaMemcpyAsync(ctx->bind_tet.p, bind_tet, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream), "upload bindings");
+    CGS_CUDA(cudaMemcpyAsync(ctx->bind_w.p, bind_w, (size_t)n * 16, cudaMemcpyHostToDevice, ctx->stream), "upload weights");
+  }
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "cage upload");
+  ctx->num_tets = num_tets;
+  ctx->num_verts = num_verts;
+  ctx->has_cages = true;
+  ctx->verts_uploaded = false;
+  ctx->last_verts.clear();
+  ctx->deformed_valid = false;
+  return CGS_OK;
+}
+
+int cgs_cage_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_verts) {
+  if (!ctx || !verts) return CGS_E_ARG;
+  if (!ctx->has_cages) return ctx->fail(CGS_E_STATE, "no cages uploaded");
+  if (num_verts != ctx->num_verts) return ctx->fail(CGS_E_ARG, "vertex count differs from the cage topology");
+  const size_t cnt = (size_t)num_verts * 3;
+  if (ctx->verts_uploaded && ctx->last_verts.size() == cnt &&
+      std::memcmp(ctx->last_verts.data(), verts, cnt * 4) == 0)
+    return CGS_OK;
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(cudaMemcpyAsync(ctx->cage_verts.p, verts, cnt * 4, cudaMemcpyHostToDevice, ctx->stream), "upload vertices");
+  // pageable source: the copy has completed when cudaMemcpyAsync returns
+  ctx->last_verts.assign(verts, verts + cnt);
+  ctx->verts_uploaded = true;
+  ctx->deformed_valid = false;
+  return CGS_OK;
+}
+
+int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const float* inv_dm,
+                  uint32_t num_verts, const float* rest_verts, int32_t use_bounds,
+                  const float* bmin, const float* bmax, uint32_t* bind_tet, float* bind_w) {
+  if (!ctx || !elems || !inv_dm || !rest_verts || !bind_tet || !bind_w) return CGS_E_ARG;
+  if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "upload the scene before binding");
+  if (use_bounds && (!bmin || !bmax)) return ctx->fail(CGS_E_ARG, "bounds requested but null");
+  cudaSetDevice(ctx->device);
+  const uint32_t n = ctx->n;
+  if (n == 0) return CGS_OK;
+  std::vector<float> x0((size_t)num_tets * 3);
+  for (uint32_t t = 0; t < num_tets; ++t) {
+    const uint32_t v = elems[4 * (size_t)t];
+    if (v >= num_verts) return ctx->fail(CGS_E_ARG, "tet element index out of range");
+    std::memcpy(&x0[3 * (size_t)t], rest_verts + 3 * (size_t)v, 12);
+  }
+  void* d = nullptr;
+  const size_t bx = (size_t)num_tets * 12, bm = (size_t)num_tets * 36;
+  const size_t o_m = (bx + 255) & ~(size_t)255, o_t = o_m + ((bm + 255) & ~(size_t)255),
+               o_w = o_t + (((size_t)n * 4 + 255) & ~(size_t)255);
+  CGS_CUDA(cudaMalloc(&d, o_w + (size_t)n * 16 + 16), "cudaMalloc binding scratch");
+  char* b = (char*)d;
+  cudaError_t e = cudaSuccess;
+  if (num_tets) {
+    e = cudaMemcpyAsync(b, x0.data(), bx, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_m, inv_dm, bm, cudaMemcpyHostToDevice, ctx->stream);
+  }
+  BindArgs a{};
+  a.n = n;
+  a.num_tets = num_tets;
+  a.points = ctx->rest_pos.as<float4>();
+  a.tet_x0 = (const float*)b;
+  a.inv_dm = (const float*)(b + o_m);
+  a.use_bounds = use_bounds;
+  for (int k = 0; k < 3; ++k) {
+    a.bmin[k] = use_bounds ? bmin[k] : 0.0f;
+    a.bmax[k] = use_bounds ? bmax[k] : 0.0f;
+  }
+  a.bind_tet = (uint32_t*)(b + o_t);
+  a.bind_w = (float4*)(b + o_w);
+  if (e == cudaSuccess) e = launch_bind(a, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bind_tet, b + o_t, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bind_w, b + o_w, (size_t)n * 16, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "binding");
+  if (e2 != cudaSuccess) return ctx->cuda_fail(e2, "binding");
+  return CGS_OK;
+}
+
+int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
+                      const cgs_frame_params* params, cgs_stage_timings* timings) {
+  if (!ctx || !camera || !comp || !params) return CGS_E_ARG;
+  if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
+  if (ctx->has_cages && !ctx->verts_uploaded)
+    return ctx->fail(CGS_E_STATE, "cage vertices not uploaded");
+  if (params->radix_bits != 0 && params->radix_bits != 4 && params->radix_bits != 8)
+    return ctx->fail(CGS_E_ARG, "radix_bits must be 0, 4 or 8");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  cgs_stage_timings tm{};
+  const uint32_t W = comp->screen_width ? comp->screen_width : 1u;
+  const uint32_t H = comp->screen_height ? comp->screen_height : 1u;
+  const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+  const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
+  if (total_tiles64 > 0xFFFFFFFFull / 2) return ctx->fail(CGS_E_CAPACITY, "viewport too large");
+  const uint32_t total_tiles = (uint32_t)total_tiles64;
+  const uint32_t pitch = (W + 63) / 64 * 64;
+  if (W != ctx->last_w || H != ctx->last_h) ctx->s3_valid = false;
+  const uint32_t radix_bits = params->radix_bits ? (uint32_t)params->radix_bits : 8u;
+  const bool prof = params->profile_stages != 0;
+
+  CGS_TRY(ctx->ensure(ctx->fb_rgba8, (size_t)pitch * H * 4, "framebuffer"));
+  if (params->write_f32) CGS_TRY(ctx->ensure(ctx->fb_f32, (size_t)W * H * 16, "f32 framebuffer"));
+
+  const uint32_t n = ctx->n;
+  const bool has_cages = ctx->has_cages;
+  const uint32_t split_bits = fbits(params->strain_split_threshold), mip_bits = fbits(params->mip_filter_3d_var);
+  const bool params_changed = split_bits != ctx->last_split_bits || mip_bits != ctx->last_mip_bits;
+  const bool need_deform = has_cages && (!ctx->deformed_valid || params_changed);
+  const bool split_possible = has_cages && params->strain_split_threshold > 0.0f;
+  const uint32_t max_n = split_possible ? 2 * n : n;
+  const uint32_t mn = max_n ? max_n : 1u;
+
+  // scratch: counters | deform status | count-scan status | histograms
+  const size_t def_tiles = (n + 255) / 256, cs_tiles = (mn + 255) / 256;
+  const size_t o_def = 256, o_cs = o_def + def_tiles * 8 + 256, o_hist = o_cs + cs_tiles * 8 + 256;
+  const size_t scratch_bytes = o_hist + 8 * 256 * 4;
+  CGS_TRY(ctx->ensure(ctx->scratch, scratch_bytes, "frame scratch"));
+  CGS_TRY(ctx->ensure(ctx->recs, (size_t)mn * sizeof(SplatRec), "splat records"));
+  CGS_TRY(ctx->ensure(ctx->offsets, (size_t)mn * 4, "tile offsets"));
+  CGS_TRY(ctx->ensure(ctx->ranges, (size_t)total_tiles * 8, "tile ranges"));
+  char* sc = ctx->scratch.as<char>();
+  FrameCounters* fc = (FrameCounters*)sc;
+  uint32_t* d_split = ctx->persist.as<uint32_t>();
+
+  ctx->kpar ^= 1;
+  ctx->kfold(ctx->kpar, nullptr);  // frame f-2 used this event set
+  ctx->kcount[ctx->kpar] = 0;
+  ctx->kprof = prof;
+  ctx->kbegin(CGS_K_CLEAR);
+  CGS_CUDA(cudaMemsetAsync(sc, 0, scratch_bytes, s), "clear frame scratch");
+  ctx->kend();
+
+  // ---------------- Stage 1
+  if (has_cages) {
+    CGS_TRY(ctx->ensure(ctx->tet_J, (size_t)ctx->num_tets * 36, "tet J"));
+    CGS_TRY(ctx->ensure(ctx->tet_R, (size_t)ctx->num_tets * 36, "tet R"));
+    CGS_TRY(ctx->ensure(ctx->tet_S, (size_t)ctx->num_tets * 4, "tet stretch"));
+    CGS_TRY(ctx->ensure(ctx->def_pos, (size_t)mn * 16, "deformed positions"));
+    CGS_TRY(ctx->ensure(ctx->def_cova, (size_t)mn * 16, "deformed covariances"));
+    CGS_TRY(ctx->ensure(ctx->def_covb, (size_t)mn * 8, "deformed covariances"));
+    CGS_TRY(ctx->ensure(ctx->split_meta, (size_t)(n ? n : 1) * 8, "split meta"));
+  }
+  if (need_deform) {
+    DeformArgs d{};
+    d.n = n;
+    d.num_tets = ctx->num_tets;
+    d.verts = ctx->cage_verts.as<float>();
+    d.elems = ctx->tet_elems.as<uint4>();
+    d.inv_dm = ctx->tet_inv_dm.as<float>();
+    d.tet_J = ctx->tet_J.as<float>();
+    d.tet_R = ctx->tet_R.as<float>();
+    d.tet_stretch = ctx->tet_S.as<float>();
+    d.bind_tet = ctx->bind_tet.as<uint32_t>();
+    d.bind_w = ctx->bind_w.as<float4>();
+    d.rest_pos = ctx->rest_pos.as<float4>();
+    d.rest_cova = ctx->rest_cova.as<float4>();
+    d.rest_covb = ctx->rest_covb.as<float2>();
+    d.def_pos = ctx->def_pos.as<float4>();
+    d.def_cova = ctx->def_cova.as<float4>();
+    d.def_covb = ctx->def_covb.as<float2>();
+    d.split_meta = ctx->split_meta.as<uint2>();
+    d.split_count = d_split;
+    d.status = (unsigned long long*)(sc + o_def);
+    d.fc = fc;
+    d.split_threshold = params->strain_split_threshold;
+    d.mip = params->mip_filter_3d_var;
+    ctx->kbegin(CGS_K_TET_TRANSFORMS);
+    CGS_CUDA(launch_tet_transforms(d, s), "tet transforms launch");
+    ctx->kend();
+    ctx->kbegin(CGS_K_DEFORM);
+    CGS_CUDA(launch_deform(d, s), "deform launch");
+    ctx->kend();
+    ctx->deformed_valid = true;
+    ctx->deform_generation++;
+    ctx->last_split_bits = split_bits;
+    ctx->last_mip_bits = mip_bits;
+  }
+  tm.stage1_skipped = need_deform ? 0 : 1;
+
+  // ---------------- Stage 2
+  ProjectArgs p{};
+  if (has_cages) {
+    p.pos = ctx->def_pos.as<float4>();
+    p.cova = ctx->def_cova.as<float4>();
+    p.covb = ctx->def_covb.as<float2>();
+    p.bind_tet = ctx->bind_tet.as<uint32_t>();
+    p.tet_R = ctx->tet_R.as<float>();
+    p.num_tets = ctx->num_tets;
+    p.split_meta = ctx->split_meta.as<uint2>();
+    p.split_count = split_possible ? d_split : nullptr;
+  } else {
+    p.pos = ctx->rest_pos.as<float4>();
+    p.cova = ctx->rest_cova.as<float4>();
+    p.covb = ctx->rest_covb.as<float2>();
+  }
+  p.sh = ctx->rest_sh.p;
+  p.sh_f16 = ctx->sh_f16;
+  p.sh_stride = n;
+  p.n_rest = n;
+  p.max_n = max_n;
+  std::memcpy(p.cam, camera, 24 * sizeof(float));
+  std::memcpy(p.cam_pos, comp->camera_position, 3 * sizeof(float));
+  p.mip = has_cages ? 0.0f : params->mip_filter_3d_var;
+  p.min_opacity = params->min_opacity;
+  p.min_radius = params->min_radius_px;
+  p.sh_degree = comp->sh_degree > 3 ? 3 : comp->sh_degree;
+  p.out = ctx->recs.as<SplatRec>();
+  p.fc = fc;
+  ctx->kbegin(CGS_K_PROJECT);
+  CGS_CUDA(launch_project(p, s), "project launch");
+  ctx->kend();
+
+  // ---------------- Stage 3
+  Stage3Key key;
+  key.deform_generation = has_cages ? ctx->deform_generation : 0;
+  for (int k = 0; k < 16; ++k) key.view[k] = fbits(camera->view[k]);
+  key.fx = fbits(camera->focal_x);
+  key.fy = fbits(camera->focal_y);
+  key.cx = fbits(camera->principal_x);
+  key.cy = fbits(camera->principal_y);
+  key.near_bits = fbits(camera->near_plane);
+  key.width = W;
+  key.height = H;
+  key.mip = mip_bits;
+  key.min_opa = fbits(params->min_opacity);
+  key.min_rad = fbits(params->min_radius_px);
+  key.radix_bits = radix_bits;
+  const bool cached = !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
+  const bool key64 = total_tiles > 65535u;
+  uint32_t entries = 0;
+  int result_src = 0;
+  if (cached) {
+    tm.stage3_cached = 1;
+    entries = ctx->s3_entries;
+    result_src = ctx->s3_src;
+  } else {
+    ctx->s3_valid = false;
+    BinArgs b{};
+    b.recs = ctx->recs.as<SplatRec>();
+    b.split_count = split_possible ? d_split : nullptr;
+    b.n_rest = n;
+    b.max_n = max_n;
+    b.width = W;
+    b.height = H;
+    b.tiles_x = tiles_x;
+    b.tiles_y = tiles_y;
+    b.offsets = ctx->offsets.as<uint32_t>();
+    b.status = (unsigned long long*)(sc + o_cs);
+    b.fc = fc;
+    b.entry_cap = 0xFFFFFFFFu;
+    ctx->kbegin(CGS_K_COUNT_SCAN);
+    CGS_CUDA(launch_count_scan(b, s), "count/scan launch");
+    ctx->kend();
+    CGS_CUDA(cudaMemcpyAsync(&ctx->h_counters[0], fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s), "read counters");
+    CGS_CUDA(cudaMemcpyAsync(ctx->h_split, d_split, 4, cudaMemcpyDeviceToHost, s), "read split count");
+    CGS_CUDA(cudaStreamSynchronize(s), "stage 3 count");
+    ctx->kfold(ctx->kpar ^ 1, nullptr);
+    CGS_TRY(ctx->check_end_status());
+    if (ctx->h_counters[0].status & kStatusLookbackTimeout)
+      return ctx->fail(CGS_E_TIMEOUT, "look-back wait gave up in Stage 1-3");
+    entries = ctx->h_counters[0].entries;
+    if (entries >= (1u << 30))
+      return ctx->fail(CGS_E_CAPACITY, "more than 2^30 tile entries in one frame");
+    const size_t ecap = entries ? entries : 1;
+    for (int k = 0; k < 2; ++k) {
+      CGS_TRY(ctx->ensure(ctx->keys[k], ecap * 4, "sort keys"));
+      CGS_TRY(ctx->ensure(ctx->ids[k], ecap * 4, "sort values"));
+      if (key64) CGS_TRY(ctx->ensure(ctx->depths[k], ecap * 4, "sort depths"));
+    }
+    uint32_t tile_bits = total_tiles <= 1 ? 1u : 32u - (uint32_t)__builtin_clz(total_tiles - 1);
+    uint32_t depth_bits = tile_bits >= 32 ? 0u : (32u - tile_bits < 28u ? 32u - tile_bits : 28u);
+    const uint32_t sort_bits = tile_bits + depth_bits > 32 ? 32 : tile_bits + depth_bits;
+    const uint32_t passes_lo = key64 ? sort_passes(32, radix_bits) : sort_passes(sort_bits, radix_bits);
+    const uint32_t passes_hi = key64 ? sort_passes(tile_bits, radix_bits) : 0u;
+    const uint32_t stiles = sort_tiles(entries);
+    ctx->last_sort_passes = passes_lo + passes_hi;
+    const size_t rstat = (size_t)(passes_lo + passes_hi) * stiles * (1u << radix_bits) * 4 + 256;
+    CGS_TRY(ctx->ensure(ctx->radix_status, rstat, "radix look-back"));
+    ctx->kbegin(CGS_K_CLEAR);
+    CGS_CUDA(cudaMemsetAsync(ctx->radix_status.p, 0, rstat, s), "clear radix status");
+    CGS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0, (size_t)total_tiles * 8, s), "clear ranges");
+    ctx->kend();
+    uint32_t* d_hist = (uint32_t*)(sc + o_hist);
+    b.key64 = key64;
+    const float near_c = camera->near_plane > 1e-6f ? camera->near_plane : 1e-6f;
+    b.depth_base_bits = fbits(near_c) & 0x7F800000u;
+    b.depth_bits = depth_bits;
+    b.keys = ctx->keys[0].as<uint32_t>();
+    b.depths = key64 ? ctx->depths[0].as<uint32_t>() : nullptr;
+    b.ids = ctx->ids[0].as<uint32_t>();
+    b.hist = d_hist;
+    b.radix_bits = radix_bits;
+    b.sort_bits = sort_bits;
+    b.tile_bits = tile_bits;
+    b.entry_cap = (uint32_t)ecap;
+    if (entries > 0) {
+      ctx->kbegin(CGS_K_EMIT);
+      CGS_CUDA(launch_emit(b, s), "emit launch");
+      ctx->kend();
+      uint32_t* rs_status = ctx->radix_status.as<uint32_t>();
+      uint32_t* tile_ctrs = (uint32_t*)((char*)rs_status + rstat - 256);
+      const uint32_t* n_ptr = &fc->entries;
+      if (!key64) {
+        SortArgs sa{};
+        sa.keys[0] = ctx->keys[0].as<uint32_t>();
+        sa.keys[1] = ctx->keys[1].as<uint32_t>();
+        sa.vals[0] = ctx->ids[0].as<uint32_t>();
+        sa.vals[1] = ctx->ids[1].as<uint32_t>();
+        sa.n_ptr = n_ptr;
+        sa.capacity = entries;
+        sa.first_bit = 0;
+        sa.num_bits = sort_bits;
+        sa.radix_bits = radix_bits;
+        sa.hist = d_hist;
+        sa.status = rs_status;
+        sa.tile_ctr = tile_ctrs;
+        sa.status_word = &fc->status;
+        sa.src = 0;
+        ctx->kbegin(CGS_K_RADIX_SORT);
+        CGS_CUDA(run_radix_sort(sa, &result_src, s), "radix sort");
+        ctx->kend();
+        ctx->kbegin(CGS_K_TILE_RANGES);
+        CGS_CUDA(launch_tile_ranges(ctx->keys[result_src].as<uint32_t>(), depth_bits, n_ptr,
+                                    total_tiles, ctx->ranges.as<uint32_t>(), s),
+                 "ranges launch");
+        ctx->kend();
+      } else {
+        // (tile, depth) order: stable sort by depth, then stable sort by tile.
+        SortArgs sa{};
+        sa.keys[0] = ctx->depths[0].as<uint32_t>();
+        sa.keys[1] = ctx->depths[1].as<uint32_t>();
+        sa.vals[0] = ctx->ids[0].as<uint32_t>();
+        sa.vals[1] = ctx->ids[1].as<uint32_t>();
+        sa.vals2[0] = ctx->keys[0].as<uint32_t>();
+        sa.vals2[1] = ctx->keys[1].as<uint32_t>();
+        sa.n_ptr = n_ptr;
+        sa.capacity = entries;
+        sa.first_bit = 0;
+        sa.num_bits = 32;
+        sa.radix_bits = radix_bits;
+        sa.hist = d_hist;
+        sa.status = rs_status;
+        sa.tile_ctr = tile_ctrs;
+        sa.status_word = &fc->status;
+        sa.src = 0;
+        int src1 = 0;
+        ctx->kbegin(CGS_K_RADIX_SORT);
+        CGS_CUDA(run_radix_sort(sa, &src1, s), "radix sort (depth)");
+        SortArgs sb = sa;
+        sb.keys[0] = ctx->keys[0].as<uint32_t>();
+        sb.keys[1] = ctx->keys[1].as<uint32_t>();
+        sb.vals2[0] = ctx->depths[0].as<uint32_t>();
+        sb.vals2[1] = ctx->depths[1].as<uint32_t>();
+        sb.num_bits = tile_bits;
+        sb.hist = d_hist + (size_t)passes_lo * (1u << radix_bits);
+        sb.status = rs_status + (size_t)passes_lo * stiles * (1u << radix_bits);
+        sb.tile_ctr = tile_ctrs + passes_lo;
+        sb.src = src1;
+        CGS_CUDA(run_radix_sort(sb, &result_src, s), "radix sort (tile)");
+        ctx->kend();
+        ctx->kbegin(CGS_K_TILE_RANGES);
+        CGS_CUDA(launch_tile_ranges(ctx->keys[result_src].as<uint32_t>(), 0, n_ptr, total_tiles,
+                                    ctx->ranges.as<uint32_t>(), s),
+                 "ranges launch");
+        ctx->kend();
+      }
+    }
+    ctx->s3_valid = true;
+    ctx->s3_key = key;
+    ctx->s3_entries = entries;
+    ctx->s3_src = result_src;
+    ctx->s3_key64 = key64;
+    ctx->s3_depth_bits = depth_bits;
+    ctx->s3_surviving = ctx->h_counters[0].surviving;
+    ctx->s3_active = n + (split_possible ? *ctx->h_split : 0u);
+  }
+
+  // ---------------- Stage 4
+  CompositeArgs c{};
+  c.recs = ctx->recs.as<SplatRec>();
+  c.sorted_ids = ctx->ids[result_src].p ? ctx->ids[result_src].as<uint32_t>() : nullptr;
+  c.ranges = ctx->ranges.as<uint32_t>();
+  c.width = W;
+  c.height = H;
+  c.tiles_x = tiles_x;
+  c.tiles_y = tiles_y;
+  c.pitch_px = pitch;
+  std::memcpy(c.bg, comp->background, 16);
+  c.out_rgba8 = ctx->fb_rgba8.as<uint32_t>();
+  c.out_f32 = params->write_f32 ? ctx->fb_f32.as<float4>() : nullptr;
+  c.fc = fc;
+  c.num_recs = mn;
+  c.num_entries = entries;
+  ctx->kbegin(CGS_K_COMPOSITE);
+  CGS_CUDA(launch_composite(c, s), "composite launch");
+  ctx->kend();
+  CGS_CUDA(cudaMemcpyAsync(&ctx->h_counters[1], fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s), "read counters");
+  ctx->end_copy_pending = true;
+
+  ctx->last_w = W;
+  ctx->last_h = H;
+  ctx->last_pitch = pitch;
+  ctx->last_f32 = params->write_f32 != 0;
+  ctx->last_tiles = total_tiles;
+  ctx->frame_done = true;
+
+  const uint64_t A = cached ? ctx->s3_active : n + (split_possible ? *ctx->h_split : 0u);
+  const uint64_t S = cached ? ctx->s3_surviving : ctx->h_counters[0].surviving;
+  if (prof) {
+    // Algorithmic HBM bytes per kernel: the data each launch must move once.
+    const uint64_t E = entries, T = ctx->num_tets;
+    const uint64_t shb = ctx->sh_f16 ? 96 : 192;
+    ctx->kcount_launch(CGS_K_CLEAR, cached ? 1 : 2, 0);
+    if (need_deform) {
+      ctx->kcount_launch(CGS_K_TET_TRANSFORMS, 1, T * (16 + 36 + 48 + 76));
+      ctx->kcount_launch(CGS_K_DEFORM, 1, (uint64_t)n * 60 + A * 40 + (A - n) * 8);
+    }
+    ctx->kcount_launch(CGS_K_PROJECT, 1, A * 40 + S * (shb + 48) + (A - S) * 16);
+    if (!cached) {
+      const uint64_t kw = key64 ? 12 : 8;
+      ctx->kcount_launch(CGS_K_COUNT_SCAN, 1, A * 36);
+      if (E) {
+        ctx->kcount_launch(CGS_K_EMIT, 1, A * 36 + E * kw);
+        ctx->kcount_launch(CGS_K_RADIX_SORT, ctx->last_sort_passes,
+                           (uint64_t)ctx->last_sort_passes * E * (key64 ? 24 : 16));
+        ctx->kcount_launch(CGS_K_TILE_RANGES, 1, E * 4 + (uint64_t)total_tiles * 8);
+      }
+    }
+    ctx->kcount_launch(CGS_K_COMPOSITE, 1,
+                       E * 52 + (uint64_t)total_tiles * 8 +
+                           (uint64_t)W * H * (params->write_f32 ? 20 : 4));
+    ctx->kpending[ctx->kpar] = ctx->kcount[ctx->kpar] > 0;
+  }
+  if (prof && timings) {
+    CGS_CUDA(cudaStreamSynchronize(s), "frame");
+    CGS_TRY(ctx->check_end_status());
+    cgs_kernel_profile fr{};
+    ctx->kfold(ctx->kpar, &fr);
+    tm.stage1_deform_ms = fr.ms[CGS_K_TET_TRANSFORMS] + fr.ms[CGS_K_DEFORM];
+    tm.stage2_project_ms = fr.ms[CGS_K_PROJECT];
+    tm.stage3_bin_sort_ms = fr.ms[CGS_K_COUNT_SCAN] + fr.ms[CGS_K_EMIT] +
+                            fr.ms[CGS_K_RADIX_SORT] + fr.ms[CGS_K_TILE_RANGES];
+    tm.stage4_composite_ms = fr.ms[CGS_K_COMPOSITE];
+    tm.used_hardware_timestamps = 1;
+  }
+  tm.surviving_gaussians = S;
+  tm.used_64bit_keys = key64 ? 1 : 0;
+  tm.total_tile_entries = entries;
+  tm.active_gaussians = A;
+  ctx->last_active = (uint32_t)tm.active_gaussians;
+  if (timings) *timings = tm;
+  return CGS_OK;
+}
+
+int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height) {
+  if (!ctx || !dst) return CGS_E_ARG;
+  if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
+  if (width != ctx->last_w || height != ctx->last_h)
+    return ctx->fail(CGS_E_ARG, "size differs from the last frame");
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(cudaMemcpy2DAsync(dst, (size_t)width * 4, ctx->fb_rgba8.p, (size_t)ctx->last_pitch * 4,
+                             (size_t)width * 4, height, cudaMemcpyDeviceToHost, ctx->stream),
+           "framebuffer readback");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "framebuffer readback");
+  return ctx->check_end_status();
+}
+
+int cgs_readback_rgba_f32(cgs_ctx* ctx, float* dst, uint32_t width, uint32_t height) {
+  if (!ctx || !dst) return CGS_E_ARG;
+  if (!ctx->frame_done || !ctx->last_f32) return ctx->fail(CGS_E_STATE, "no f32 frame rendered");
+  if (width != ctx->last_w || height != ctx->last_h)
+    return ctx->fail(CGS_E_ARG, "size differs from the last frame");
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(cudaMemcpyAsync(dst, ctx->fb_f32.p, (size_t)width * height * 16, cudaMemcpyDeviceToHost, ctx->stream), "f32 readback");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "f32 readback");
+  return ctx->check_end_status();
+}
+
+int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px) {
+  if (!ctx || !d_rgba8 || !row_pitch_px) return CGS_E_ARG;
+  if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
+  *d_rgba8 = ctx->fb_rgba8.p;
+  *row_pitch_px = ctx->last_pitch;
+  return CGS_OK;
+}
+
+int cgs_invalidate_stage3(cgs_ctx* ctx) {
+  if (!ctx) return CGS_E_ARG;
+  ctx->s3_valid = false;
+  return CGS_OK;
+}
+
+int cgs_invalidate(cgs_ctx* ctx) {
+  if (!ctx) return CGS_E_ARG;
+  ctx->s3_valid = false;
+  ctx->scene_ready = false;
+  ctx->has_cages = false;
+  ctx->num_tets = 0;
+  ctx->deformed_valid = false;
+  ctx->verts_uploaded = false;
+  ctx->last_verts.clear();
+  ctx->deform_generation++;
+  return CGS_OK;
+}
+
+int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_bytes,
+                          uint64_t* out_bytes) {
+  if (!ctx || !out_bytes) return CGS_E_ARG;
+  if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "read frame buffer");
+  CGS_TRY(ctx->check_end_status());
+  const size_t active = ctx->last_active;
+  const size_t splits = active > ctx->n ? active - ctx->n : 0;
+  const size_t entries = ctx->s3_entries;
+  std::vector<char> tmp;
+  auto fetch = [&](const DevBuf& b, size_t bytes) -> int {
+    tmp.resize(bytes);
+    if (bytes == 0) return CGS_OK;
+    if (!b.p || b.cap < bytes) return ctx->fail(CGS_E_STATE, "buffer not populated by the last frame");
+    cudaError_t e = cudaMemcpy(tmp.data(), b.p, bytes, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? CGS_OK : ctx->cuda_fail(e, "buffer readback");
+  };
+  std::vector<char> out;
+  switch (which) {
+    case CGS_BUF_DEFORMED_POS:
+    case CGS_BUF_DEFORMED_OPA: {
+      if (!ctx->has_cages) return ctx->fail(CGS_E_STATE, "no cages: no deformed scene");
+      CGS_TRY(fetch(ctx->def_pos, active * 16));
+      const float* f = (const float*)tmp.data();
+      if (which == CGS_BUF_DEFORMED_POS) {
+        out.resize(active * 12);
+        float* o = (float*)out.data();
+        for (size_t i = 0; i < active; ++i) {
+          o[3 * i] = f[4 * i]; o[3 * i + 1] = f[4 * i + 1]; o[3 * i + 2] = f[4 * i + 2];
+        }
+      } else {
+        out.resize(active * 4);
+        float* o = (float*)out.data();
+        for (size_t i = 0; i < active; ++i) o[i] = f[4 * i + 3];
+      }
+      break;
+    }
+    case CGS_BUF_DEFORMED_COV: {
+      if (!ctx->has_cages) return ctx->fail(CGS_E_STATE, "no cages: no deformed scene");
+      CGS_TRY(fetch(ctx->def_cova, active * 16));
+      std::vector<char> a = tmp;
+      CGS_TRY(fetch(ctx->def_covb, active * 8));
+      const float* fa = (const float*)a.data();
+      const float* fb = (const float*)tmp.data();
+      out.resize(active * 24);
+      float* o = (float*)out.data();
+      for (size_t i = 0; i < active; ++i) {
+        for (int k = 0; k < 4; ++k) o[6 * i + k] = fa[4 * i + k];
+        o[6 * i + 4] = fb[2 * i];
+        o[6 * i + 5] = fb[2 * i + 1];
+      }
+      break;
+    }
+    case CGS_BUF_SPLIT_META:
+      CGS_TRY(fetch(ctx->split_meta, splits * 8));
+      out = tmp;
+      break;
+    case CGS_BUF_SPLAT_ATTRS:
+    case CGS_BUF_EXTENTS: {
+      CGS_TRY(fetch(ctx->recs, active * sizeof(SplatRec)));
+      const SplatRec* r = (const SplatRec*)tmp.data();
+      if (which == CGS_BUF_EXTENTS) {
+        out.resize(active * 4);
+        uint32_t* o = (uint32_t*)out.data();
+        for (size_t i = 0; i < active; ++i) o[i] = fbits(r[i].cc.w);
+      } else {
+        out.assign(active * 40, 0);
+        float* o = (float*)out.data();
+        for (size_t i = 0; i < active; ++i) {
+          if (fbits(r[i].cc.w) == 0) continue;
+          const float v[10] = {r[i].geo.x, r[i].geo.y, r[i].geo.z, r[i].geo.w, r[i].cc.x,
+                               r[i].cc.y,  r[i].rgb.x, r[i].rgb.y, r[i].rgb.z, r[i].cc.z};
+          std::memcpy(o + 10 * i, v, 40);
+        }
+      }
+      break;
+    }
+    case CGS_BUF_TILE_OFFSETS:
+      CGS_TRY(fetch(ctx->offsets, active * 4));
+      out = tmp;
+      break;
+    case CGS_BUF_SORTED_KEYS:
+      if (!ctx->s3_key64) {
+        CGS_TRY(fetch(ctx->keys[ctx->s3_src], entries * 4));
+        out = tmp;
+      } else {
+        CGS_TRY(fetch(ctx->keys[ctx->s3_src], entries * 4));
+        std::vector<char> t = tmp;
+        CGS_TRY(fetch(ctx->depths[ctx->s3_src], entries * 4));
+        out.resize(entries * 8);
+        uint64_t* o = (uint64_t*)out.data();
+        for (size_t i = 0; i < entries; ++i)
+          o[i] = ((uint64_t)((uint32_t*)t.data())[i] << 32) | ((uint32_t*)tmp.data())[i];
+      }
+      break;
+    case CGS_BUF_SORTED_IDS:
+      CGS_TRY(fetch(ctx->ids[ctx->s3_src], entries * 4));
+      out = tmp;
+      break;
+    case CGS_BUF_TILE_RANGES:
+      CGS_TRY(fetch(ctx->ranges, (size_t)ctx->last_tiles * 8));
+      out = tmp;
+      break;
+    case CGS_BUF_TET_JACOBIANS:
+      CGS_TRY(fetch(ctx->tet_J, (size_t)ctx->num_tets * 36));
+      out = tmp;
+      break;
+    case CGS_BUF_TET_ROTATIONS:
+      CGS_TRY(fetch(ctx->tet_R, (size_t)ctx->num_tets * 36));
+      out = tmp;
+      break;
+    case CGS_BUF_TET_STRETCH:
+      CGS_TRY(fetch(ctx->tet_S, (size_t)ctx->num_tets * 4));
+      out = tmp;
+      break;
+    default:
+      return ctx->fail(CGS_E_ARG, "unknown buffer id");
+  }
+  *out_bytes = out.size();
+  if (dst) {
+    if (dst_bytes < out.size()) return ctx->fail(CGS_E_ARG, "destination too small");
+    std::memcpy(dst, out.data(), out.size());
+  }
+  return CGS_OK;
+}
+
+const char* cgs_kernel_name(int32_t id) {
+  static const char* names[CGS_KERNEL_COUNT] = {
+      "clear",  "tet_transforms", "deform",      "project",  "count_scan",
+      "emit",   "radix_sort",     "tile_ranges", "composite"};
+  return (id >= 0 && id < CGS_KERNEL_COUNT) ? names[id] : "unknown";
+}
+
+int cgs_kernel_profile_read(cgs_ctx* ctx, cgs_kernel_profile* out) {
+  if (!ctx || !out) return CGS_E_ARG;
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "profile read");
+  ctx->kfold(0, nullptr);
+  ctx->kfold(1, nullptr);
+  *out = ctx->kp_acc;
+  return CGS_OK;
+}
+
+int cgs_kernel_profile_reset(cgs_ctx* ctx) {
+  if (!ctx) return CGS_E_ARG;
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "profile reset");
+  ctx->kfold(0, nullptr);
+  ctx->kfold(1, nullptr);
+  ctx->kp_acc = cgs_kernel_profile{};
+  return CGS_OK;
+}
+
+int cgs_scan_u32(cgs_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint64_t n,
+                 uint64_t* total) {
+  if (!ctx) return CGS_E_ARG;
+  if (n > 0 && (!d_in || !d_out)) return ctx->fail(CGS_E_ARG, "null device pointer");
+  if (n >= 0xFFFFFFFFull) return ctx->fail(CGS_E_CAPACITY, "scan length must be < 2^32");
+  cudaSetDevice(ctx->device);
+  if (n == 0) {
+    if (total) *total = 0;
+    return CGS_OK;
+  }
+  const size_t tiles = scan_tiles((uint32_t)n);
+  const size_t bytes = 256 + tiles * 8;
+  CGS_TRY(ctx->ensure(ctx->prim[0], bytes, "scan scratch"));
+  char* b = ctx->prim[0].as<char>();
+  CGS_CUDA(cudaMemsetAsync(b, 0, bytes, ctx->stream), "clear scan scratch");
+  uint32_t* words = (uint32_t*)b;  // [0] total, [1] tile counter, [2] status
+  CGS_CUDA(launch_scan_u32(d_in, d_out, (uint32_t)n, words, (unsigned long long*)(b + 256),
+                           words + 1, words + 2, ctx->stream),
+           "scan launch");
+  uint32_t h[3] = {0, 0, 0};
+  CGS_CUDA(cudaMemcpyAsync(ctx->h_split + 1, words, 12, cudaMemcpyDeviceToHost, ctx->stream), "scan total");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "scan");
+  std::memcpy(h, ctx->h_split + 1, 12);
+  if (h[2] & kStatusLookbackTimeout) return ctx->fail(CGS_E_TIMEOUT, "scan look-back wait gave up");
+  if (total) *total = h[0];
+  return CGS_OK;
+}
+
+static int sort_common(cgs_ctx* ctx, uint32_t* d_keys, uint32_t* d_vals, uint32_t* d_vals2,
+                       uint64_t n, uint32_t key_bits, int32_t digit_bits, int* out_in_scratch,
+                       uint32_t** alt) {
+  const uint32_t rb = digit_bits == 0 ? 8u : (uint32_t)digit_bits;
+  const uint32_t passes = sort_passes(key_bits, rb);
+  const uint32_t stiles = sort_tiles((uint32_t)n);
+  const size_t R = (size_t)1 << rb;
+  const size_t hdr = 256 + 8 * 256 * 4;
+  const size_t bytes = hdr + (size_t)passes * stiles * R * 4;
+  CGS_TRY(ctx->ensure(ctx->prim[0], bytes, "sort scratch"));
+  CGS_TRY(ctx->ensure(ctx->prim[1], (size_t)n * 4, "sort alt keys"));
+  CGS_TRY(ctx->ensure(ctx->prim[2], (size_t)n * 4, "sort alt values"));
+  if (d_vals2) CGS_TRY(ctx->ensure(ctx->prim[3], (size_t)n * 4, "sort alt values"));
+  char* b = ctx->prim[0].as<char>();
+  CGS_CUDA(cudaMemsetAsync(b, 0, bytes, ctx->stream), "clear sort scratch");
+  uint32_t* words = (uint32_t*)b;  // [0] n, [1] status, [2..] tile counters
+  const uint32_t n32 = (uint32_t)n;
+  CGS_CUDA(cudaMemcpyAsync(words, &n32, 4, cudaMemcpyHostToDevice, ctx->stream), "sort n");
+  uint32_t* hist = (uint32_t*)(b + 256);
+  CGS_CUDA(launch_histogram(d_keys, words, n32, 0, key_bits, rb, hist, ctx->stream), "histogram");
+  SortArgs sa{};
+  sa.keys[0] = d_keys;
+  sa.keys[1] = ctx->prim[1].as<uint32_t>();
+  sa.vals[0] = d_vals;
+  sa.vals[1] = ctx->prim[2].as<uint32_t>();
+  if (d_vals2) {
+    sa.vals2[0] = d_vals2;
+    sa.vals2[1] = ctx->prim[3].as<uint32_t>();
+  }
+  sa.n_ptr = words;
+  sa.capacity = n32;
+  sa.first_bit = 0;
+  sa.num_bits = key_bits;
+  sa.radix_bits = rb;
+  sa.hist = hist;
+  sa.status = (uint32_t*)(b + hdr);
+  sa.tile_ctr = words + 2;
+  sa.status_word = words + 1;
+  sa.src = 0;
+  int src = 0;
+  CGS_CUDA(run_radix_sort(sa, &src, ctx->stream), "radix sort");
+  *out_in_scratch = src;
+  alt[0] = sa.keys[1];
+  alt[1] = sa.vals[1];
+  alt[2] = sa.vals2[1];
+  return CGS_OK;
+}
+
+static int sort_status(cgs_ctx* ctx) {
+  uint32_t* words = ctx->prim[0].as<uint32_t>();
+  CGS_CUDA(cudaMemcpyAsync(ctx->h_split + 1, words, 8, cudaMemcpyDeviceToHost, ctx->stream), "sort status");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "sort");
+  if (ctx->h_split[2] & kStatusLookbackTimeout) return ctx->fail(CGS_E_TIMEOUT, "sort look-back wait gave up");
+  return CGS_OK;
+}
+
+int cgs_sort_pairs_u32(cgs_ctx* ctx, uint32_t* d_keys, uint32_t* d_vals, uint64_t n,
+                       uint32_t key_bits, int32_t digit_bits) {
+  if (!ctx) return CGS_E_ARG;
+  if (digit_bits != 0 && digit_bits != 4 && digit_bits != 8)
+    return ctx->fail(CGS_E_ARG, "digit_bits must be 0, 4 or 8");
+  if (key_bits == 0 || key_bits > 32) return ctx->fail(CGS_E_ARG, "key_bits must be in 1..32");
+  if (n >= (1ull << 30)) return ctx->fail(CGS_E_CAPACITY, "sort length must be < 2^30");
+  if (n > 0 && (!d_keys || !d_vals)) return ctx->fail(CGS_E_ARG, "null device pointer");
+  if (n <= 1) return CGS_OK;
+  cudaSetDevice(ctx->device);
+  int src = 0;
+  uint32_t* alt[3];
+  CGS_TRY(sort_common(ctx, d_keys, d_vals, nullptr, n, key_bits, digit_bits, &src, alt));
+  if (src == 1) {
+    CGS_CUDA(cudaMemcpyAsync(d_keys, alt[0], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy keys");
+    CGS_CUDA(cudaMemcpyAsync(d_vals, alt[1], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy values");
+  }
+  return sort_status(ctx);
+}
+
+int cgs_sort_pairs_u64(cgs_ctx* ctx, uint32_t* d_tiles, uint32_t* d_depths, uint32_t* d_ids,
+                       uint64_t n, uint32_t tile_bits, int32_t digit_bits) {
+  if (!ctx) return CGS_E_ARG;
+  if (digit_bits != 0 && digit_bits != 4 && digit_bits != 8)
+    return ctx->fail(CGS_E_ARG, "digit_bits must be 0, 4 or 8");
+  if (tile_bits == 0 || tile_bits > 32) return ctx->fail(CGS_E_ARG, "tile_bits must be in 1..32");
+  if (n >= (1ull << 30)) return ctx->fail(CGS_E_CAPACITY, "sort length must be < 2^30");
+  if (n > 0 && (!d_tiles || !d_depths || !d_ids)) return ctx->fail(CGS_E_ARG, "null device pointer");
+  if (n <= 1) return CGS_OK;
+  cudaSetDevice(ctx->device);
+  // Pass group 1: by depth, carrying (id, tile).
+  int src = 0;
+  uint32_t* alt[3];
+  CGS_TRY(sort_common(ctx, d_depths, d_ids, d_tiles, n, 32, digit_bits, &src, alt));
+  if (src == 1) {
+    CGS_CUDA(cudaMemcpyAsync(d_depths, alt[0], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    CGS_CUDA(cudaMemcpyAsync(d_ids, alt[1], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    CGS_CUDA(cudaMemcpyAsync(d_tiles, alt[2], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+  }
+  CGS_TRY(sort_status(ctx));
+  // Pass group 2: by tile, carrying (id, depth).
+  CGS_TRY(sort_common(ctx, d_tiles, d_ids, d_depths, n, tile_bits, digit_bits, &src, alt));
+  if (src == 1) {
+    CGS_CUDA(cudaMemcpyAsync(d_tiles, alt[0], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    CGS_CUDA(cudaMemcpyAsync(d_ids, alt[1], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    CGS_CUDA(cudaMemcpyAsync(d_depths, alt[2], n * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+  }
+  return sort_status(ctx);
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,278 @@
+// Stable LSD radix sort of 32-bit keys with one or two 32-bit payload words,
+// "onesweep" style (one kernel per digit pass, no separate scan pass), on
+// sm_100a. Replaces gpu_radix_sort_u32_pairs / gpu_radix_sort_u64_pairs
+// (render/kernels/radix_sort.rs:292-477), whose 4-bit passes each ran a
+// histogram kernel, a 1-3 level scan and a scatter kernel.
+//
+// Per pass and per 4096-key tile (256 threads x 16 keys, warp-striped so a
+// warp's item j is 32 consecutive keys):
+//   1. keys and payloads are loaded coalesced into registers;
+//   2. each warp ranks its 512 keys by digit with __match_any_sync, keeping a
+//      per-warp digit counter in shared memory (stable: ranks follow key order);
+//   3. per-digit counts are published to a chained look-back array, one thread
+//      per digit, and the exclusive prefix over earlier tiles is collected
+//      (tiles are taken in order from an atomic counter, so every tile waited
+//      on belongs to a resident block; waits are bounded by kSpinLimit polls);
+//   4. keys are reordered by digit in shared memory and written out so that
+//      each digit's run is a contiguous, mostly coalesced store.
+// The global digit offsets come from digit histograms of all passes, which the
+// Stage 3 emitter accumulates while it writes the keys (launch_histogram does
+// the same for standalone sorts). HBM traffic per pass: one read and one write
+// of keys and payloads (16 B per pair), plus 1 KiB of look-back words per tile.
+#include "kernels.h"
+
+namespace cgs {
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPre = 2u << 30;
+constexpr uint32_t kValueMask = (1u << 30) - 1u;
+
+struct PassArgs {
+  const uint32_t* keys_in;
+  const uint32_t* v0_in;
+  const uint32_t* v1_in;
+  uint32_t* keys_out;
+  uint32_t* v0_out;
+  uint32_t* v1_out;
+  const uint32_t* n_ptr;
+  uint32_t capacity;
+  uint32_t shift;
+  uint32_t dmask;          // digit mask of this pass (narrower on a final partial pass)
+  const uint32_t* hist;    // this pass's digit counts
+  uint32_t* status;        // this pass's [tiles][radix] look-back words
+  uint32_t* tile_ctr;
+  uint32_t* status_word;
+};
+
+template <int RB, bool PAY2>
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
+  constexpr uint32_t R = 1u << RB;
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_keys = smem;                       // [kSortTile]
+  uint32_t* s_v0 = s_keys + kSortTile;           // [kSortTile]
+  uint32_t* s_v1 = s_v0 + kSortTile;             // [kSortTile] (PAY2)
+  uint32_t* s_whist = s_v0 + (PAY2 ? 2 : 1) * kSortTile;  // [8][R]
+  uint32_t* s_tstart = s_whist + 8 * R;          // [R]
+  uint32_t* s_goff = s_tstart + R;               // [R]
+  uint32_t* s_dbase = s_goff + R;                // [R]
+  uint32_t* s_misc = s_dbase + R;                // [40]: tile, warp sums
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t n = *a.n_ptr;
+  if (n > a.capacity) n = a.capacity;
+  const uint32_t num_tiles = (n + kSortTile - 1) / kSortTile;
+  if (tid == 0) s_misc[0] = atomicAdd(a.tile_ctr, 1u);
+  for (uint32_t k = tid; k < 8 * R; k += kSortThreads) s_whist[k] = 0u;
+  __syncthreads();
+  const uint32_t tile = s_misc[0];
+  if (tile >= num_tiles) return;
+
+  // Global digit bases: exclusive scan of this pass's digit histogram.
+  {
+    uint32_t tot;
+    const uint32_t h = (uint32_t)tid < R ? a.hist[tid] : 0u;
+    const uint32_t ex = block_exclusive_sum(h, s_misc + 8, &tot);
+    if ((uint32_t)tid < R) s_dbase[tid] = ex;
+  }
+
+  const size_t tile_base = (size_t)tile * kSortTile;
+  uint32_t k[kSortItems], v0[kSortItems], v1[kSortItems], rk[kSortItems];
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const size_t e = tile_base + (size_t)warp * (32 * kSortItems) + (size_t)j * 32 + lane;
+    const bool valid = e < n;
+    k[j] = valid ? a.keys_in[e] : 0xFFFFFFFFu;
+    v0[j] = valid ? a.v0_in[e] : 0u;
+    if (PAY2) v1[j] = valid ? a.v1_in[e] : 0u;
+  }
+  // Warp-level stable ranking by digit.
+  uint32_t* wh = s_whist + warp * R;
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t d = (k[j] >> a.shift) & a.dmask;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t before = __popc(peers & lanemask_lt());
+    uint32_t old = 0;
+    if (lane == leader) {
+      old = wh[d];
+      wh[d] = old + __popc(peers);
+    }
+    old = __shfl_sync(0xffffffffu, old, leader);
+    rk[j] = old + before;
+    __syncwarp();
+  }
+  __syncthreads();
+  // Per digit: exclusive prefix over warps, tile count (valid keys only).
+  const uint32_t tile_valid = (uint32_t)min((size_t)kSortTile, (size_t)n - tile_base);
+  uint32_t my_count = 0;
+  if ((uint32_t)tid < R) {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const uint32_t c = s_whist[w * R + tid];
+      s_whist[w * R + tid] = run;
+      run += c;
+    }
+    my_count = run;
+  }
+  uint32_t tot2;
+  const uint32_t tstart = block_exclusive_sum(my_count, s_misc + 8, &tot2);
+  if ((uint32_t)tid < R) {
+    s_tstart[tid] = tstart;
+    // Padding keys (past n) carry the largest digit and sit at the end of it.
+    uint32_t agg = my_count;
+    if ((uint32_t)tid == a.dmask) agg -= (kSortTile - tile_valid);
+    uint32_t* st = a.status + (size_t)tile * R + tid;
+    uint32_t excl = 0;
+    if (tile == 0) {
+      st_release_u32(st, kFlagPre | agg);
+    } else {
+      st_release_u32(st, kFlagAgg | agg);
+      long long pred = (long long)tile - 1;
+      uint32_t spins = 0;
+      while (pred >= 0) {
+        const uint32_t w = ld_acquire_u32(a.status + (size_t)pred * R + tid);
+        if ((w & ~kValueMask) == 0u) {
+          if (++spins > kSpinLimit) {
+            atomicOr(a.status_word, kStatusLookbackTimeout);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        excl += w & kValueMask;
+        if ((w & ~kValueMask) == kFlagPre) break;
+        --pred;
+      }
+      st_release_u32(st, kFlagPre | ((excl + agg) & kValueMask));
+    }
+    s_goff[tid] = s_dbase[tid] + excl - tstart;
+  }
+  __syncthreads();
+  // Reorder by digit through shared memory.
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t d = (k[j] >> a.shift) & a.dmask;
+    const uint32_t pos = s_tstart[d] + wh[d] + rk[j];
+    s_keys[pos] = k[j];
+    s_v0[pos] = v0[j];
+    if (PAY2) s_v1[pos] = v1[j];
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < tile_valid; i += kSortThreads) {
+    const uint32_t key = s_keys[i];
+    const uint32_t d = (key >> a.shift) & a.dmask;
+    const uint32_t g = s_goff[d] + i;
+    if (g >= n) {  // inconsistent histogram: report instead of writing out of bounds
+      atomicOr(a.status_word, kStatusCapacity);
+      continue;
+    }
+    a.keys_out[g] = key;
+    a.v0_out[g] = s_v0[i];
+    if (PAY2) a.v1_out[g] = s_v1[i];
+  }
+}
+
+template <int RB, bool PAY2>
+size_t onesweep_smem() {
+  constexpr uint32_t R = 1u << RB;
+  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTile + 8 * R + 3 * R + 48);
+}
+
+template <int RB, bool PAY2>
+cudaError_t launch_pass(const PassArgs& p, uint32_t grid, cudaStream_t s) {
+  const size_t smem = onesweep_smem<RB, PAY2>();
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep<RB, PAY2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k_onesweep<RB, PAY2><<<grid, kSortThreads, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+// Digit histograms of every pass in one read of the keys.
+__global__ void k_histogram(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ n_ptr,
+                            uint32_t capacity, uint32_t first_bit, uint32_t num_bits,
+                            uint32_t radix_bits, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[8 * 256];
+  const uint32_t R = 1u << radix_bits;
+  const uint32_t passes = (num_bits + radix_bits - 1) / radix_bits;
+  for (uint32_t k = threadIdx.x; k < passes * R; k += blockDim.x) s_hist[k] = 0u;
+  __syncthreads();
+  uint32_t n = *n_ptr;
+  if (n > capacity) n = capacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t key = keys[i];
+    for (uint32_t p = 0; p < passes; ++p) {
+      const uint32_t rem = num_bits - p * radix_bits;
+      const uint32_t bits = rem < radix_bits ? rem : radix_bits;
+      const uint32_t d = (key >> (first_bit + p * radix_bits)) & ((1u << bits) - 1u);
+      atomicAdd(&s_hist[p * R + d], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < passes * R; k += blockDim.x)
+    if (s_hist[k]) atomicAdd(&hist[k], s_hist[k]);
+}
+
+}  // namespace
+
+uint32_t sort_tiles(uint32_t capacity) { return (capacity + kSortTile - 1) / kSortTile; }
+
+uint32_t sort_passes(uint32_t num_bits, uint32_t radix_bits) {
+  return (num_bits + radix_bits - 1) / radix_bits;
+}
+
+cudaError_t launch_histogram(const uint32_t* keys, const uint32_t* n_ptr, uint32_t capacity,
+                             uint32_t first_bit, uint32_t num_bits, uint32_t radix_bits,
+                             uint32_t* hist, cudaStream_t s) {
+  k_histogram<<<148 * 2, 512, 0, s>>>(keys, n_ptr, capacity, first_bit, num_bits, radix_bits,
+                                      hist);
+  return cudaGetLastError();
+}
+
+cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
+  const uint32_t rb = a.radix_bits == 4 ? 4u : 8u;
+  const uint32_t R = 1u << rb;
+  const uint32_t passes = sort_passes(a.num_bits, rb);
+  const uint32_t tiles = sort_tiles(a.capacity);
+  int src = a.src;
+  const bool pay2 = a.vals2[0] != nullptr;
+  for (uint32_t p = 0; p < passes; ++p) {
+    PassArgs pa;
+    pa.keys_in = a.keys[src];
+    pa.v0_in = a.vals[src];
+    pa.v1_in = pay2 ? a.vals2[src] : nullptr;
+    pa.keys_out = a.keys[1 - src];
+    pa.v0_out = a.vals[1 - src];
+    pa.v1_out = pay2 ? a.vals2[1 - src] : nullptr;
+    pa.n_ptr = a.n_ptr;
+    pa.capacity = a.capacity;
+    pa.shift = a.first_bit + p * rb;
+    const uint32_t rem = a.num_bits - p * rb;
+    pa.dmask = (1u << (rem < rb ? rem : rb)) - 1u;
+    pa.hist = a.hist + (size_t)p * R;
+    pa.status = a.status + (size_t)p * tiles * R;
+    pa.tile_ctr = a.tile_ctr + p;
+    pa.status_word = a.status_word;
+    cudaError_t e;
+    if (rb == 8)
+      e = pay2 ? launch_pass<8, true>(pa, tiles, s) : launch_pass<8, false>(pa, tiles, s);
+    else
+      e = pay2 ? launch_pass<4, true>(pa, tiles, s) : launch_pass<4, false>(pa, tiles, s);
+    if (e != cudaSuccess) return e;
+    src = 1 - src;
+  }
+  *out_src = src;
+  return cudaSuccess;
+}
+
+}  // namespace cgs

@@ -1,0 +1,441 @@
+// Stage 1: tetrahedral cage deformation on sm_100a.
+//
+//  k_tet_transforms  per tet: J = D_s D_m^-1, largest singular value by
+//                    Cardano on J^T J, rotation by 5 Newton-Schulz polar
+//                    steps with chirality fix
+//                    (render/kernels/deformation.rs:684-865).
+//  k_deform<SPLIT>   per Gaussian: x' = sum w_k x_k, M = J S J^T (diag >= 1e-4,
+//                    symmetrised), det-J opacity, 3D Mip filter, strain split
+//                    along the major eigenvector
+//                    (render/kernels/deformation.rs:874-1211).
+//                    Split children are compacted deterministically: child
+//                    slot = n + (number of splitting Gaussians with a lower
+//                    index), from a block scan chained across blocks, instead
+//                    of the reference's atomic counter whose order varies
+//                    from run to run (deformation.rs:1191).
+//  k_bind            GPU barycentric binding (TetMesh::bind_point,
+//                    deformation/mod.rs:267-310).
+//
+// This file is compiled with -fmad=false: every product and sum is rounded
+// separately, in the reference's operand order, so the host-side restatement
+// reproduces it bit for bit. Memory layout: Gaussians as float4 (xyz,
+// opacity) + float4 (xx, xy, xz, yy) + float2 (yz, zz) arrays, read and
+// written coalesced with 128-bit accesses (40 B read + 20 B binding per
+// Gaussian, 40 B written).
+#include "kernels.h"
+
+namespace cgs {
+namespace {
+
+constexpr int kDeformThreads = 256;
+
+__global__ void __launch_bounds__(128) k_tet_transforms(uint32_t T, const float* __restrict__ verts,
+                                                        const uint4* __restrict__ elems,
+                                                        const float* __restrict__ inv_dm,
+                                                        float* __restrict__ J_out,
+                                                        float* __restrict__ R_out,
+                                                        float* __restrict__ S_out) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const uint4 e = elems[t];
+  const float* x0 = verts + 3 * (size_t)e.x;
+  const float* x1 = verts + 3 * (size_t)e.y;
+  const float* x2 = verts + 3 * (size_t)e.z;
+  const float* x3 = verts + 3 * (size_t)e.w;
+  const float x0x = x0[0], x0y = x0[1], x0z = x0[2];
+  const float ds_00 = x1[0] - x0x, ds_10 = x1[1] - x0y, ds_20 = x1[2] - x0z;
+  const float ds_01 = x2[0] - x0x, ds_11 = x2[1] - x0y, ds_21 = x2[2] - x0z;
+  const float ds_02 = x3[0] - x0x, ds_12 = x3[1] - x0y, ds_22 = x3[2] - x0z;
+  const float* a = inv_dm + 9 * (size_t)t;
+  const float a_00 = a[0], a_10 = a[1], a_20 = a[2], a_01 = a[3], a_11 = a[4], a_21 = a[5];
+  const float a_02 = a[6], a_12 = a[7], a_22 = a[8];
+  const float j_00 = ds_00 * a_00 + ds_01 * a_10 + ds_02 * a_20;
+  const float j_10 = ds_10 * a_00 + ds_11 * a_10 + ds_12 * a_20;
+  const float j_20 = ds_20 * a_00 + ds_21 * a_10 + ds_22 * a_20;
+  const float j_01 = ds_00 * a_01 + ds_01 * a_11 + ds_02 * a_21;
+  const float j_11 = ds_10 * a_01 + ds_11 * a_11 + ds_12 * a_21;
+  const float j_21 = ds_20 * a_01 + ds_21 * a_11 + ds_22 * a_21;
+  const float j_02 = ds_00 * a_02 + ds_01 * a_12 + ds_02 * a_22;
+  const float j_12 = ds_10 * a_02 + ds_11 * a_12 + ds_12 * a_22;
+  const float j_22 = ds_20 * a_02 + ds_21 * a_12 + ds_22 * a_22;
+  float* J = J_out + 9 * (size_t)t;
+  J[0] = j_00; J[1] = j_10; J[2] = j_20; J[3] = j_01; J[4] = j_11; J[5] = j_21;
+  J[6] = j_02; J[7] = j_12; J[8] = j_22;
+
+  // Largest singular value: sqrt of the largest eigenvalue of C = J^T J.
+  const float c00 = j_00 * j_00 + j_10 * j_10 + j_20 * j_20;
+  const float c01 = j_00 * j_01 + j_10 * j_11 + j_20 * j_21;
+  const float c02 = j_00 * j_02 + j_10 * j_12 + j_20 * j_22;
+  const float c11 = j_01 * j_01 + j_11 * j_11 + j_21 * j_21;
+  const float c12 = j_01 * j_02 + j_11 * j_12 + j_21 * j_22;
+  const float c22 = j_02 * j_02 + j_12 * j_12 + j_22 * j_22;
+  const float p1 = c01 * c01 + c02 * c02 + c12 * c12;
+  if (p1 <= 1e-10f) {
+    S_out[t] = sqrtf(fmaxf(fmaxf(c00, fmaxf(c11, c22)), 0.0f));
+  } else {
+    const float q = (c00 + c11 + c22) / 3.0f;
+    const float d0 = c00 - q, d1 = c11 - q, d2 = c22 - q;
+    const float p2 = d0 * d0 + d1 * d1 + d2 * d2 + 2.0f * p1;
+    const float p = sqrtf(fmaxf(p2 / 6.0f, 1e-12f));
+    const float inv_p = 1.0f / p;
+    const float b00 = d0 * inv_p, b11 = d1 * inv_p, b22 = d2 * inv_p;
+    const float b01 = c01 * inv_p, b02 = c02 * inv_p, b12 = c12 * inv_p;
+    const float det_b = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) +
+                        b02 * (b01 * b12 - b11 * b02);
+    const float r = clampf(0.5f * det_b, -1.0f, 1.0f);
+    const float phi = cgs_acosf(r) / 3.0f;
+    const float eig = q + 2.0f * p * cgs_cosf(phi);
+    S_out[t] = sqrtf(fmaxf(eig, 0.0f));
+  }
+
+  // Polar rotation by Newton-Schulz steps R <- (R + R^-T) / 2.
+  float* R = R_out + 9 * (size_t)t;
+  const float det_j = j_00 * (j_11 * j_22 - j_12 * j_21) - j_01 * (j_10 * j_22 - j_12 * j_20) +
+                      j_02 * (j_10 * j_21 - j_11 * j_20);
+  const float abs_det = fabsf(det_j);
+  if (abs_det < 1e-8f) {
+    R[0] = 1.0f; R[1] = 0.0f; R[2] = 0.0f; R[3] = 0.0f; R[4] = 1.0f;
+    R[5] = 0.0f; R[6] = 0.0f; R[7] = 0.0f; R[8] = 1.0f;
+    return;
+  }
+  const float gamma = cgs_expf(-cgs_logf(abs_det) / 3.0f);
+  float r00 = j_00 * gamma, r10 = j_10 * gamma, r20 = j_20 * gamma;
+  float r01 = j_01 * gamma, r11 = j_11 * gamma, r21 = j_21 * gamma;
+  float r02 = j_02 * gamma, r12 = j_12 * gamma, r22 = j_22 * gamma;
+#pragma unroll
+  for (int it = 0; it < 5; ++it) {
+    const float cof00 = r11 * r22 - r21 * r12;
+    const float cof10 = r21 * r02 - r01 * r22;
+    const float cof20 = r01 * r12 - r11 * r02;
+    const float cof01 = r12 * r20 - r22 * r10;
+    const float cof11 = r22 * r00 - r02 * r20;
+    const float cof21 = r02 * r10 - r12 * r00;
+    const float cof02 = r10 * r21 - r20 * r11;
+    const float cof12 = r20 * r01 - r00 * r21;
+    const float cof22 = r00 * r11 - r10 * r01;
+    const float det_r = r00 * cof00 + r10 * cof10 + r20 * cof20;
+    if (fabsf(det_r) > 1e-12f) {
+      const float inv_det = 1.0f / det_r;
+      r00 = 0.5f * (r00 + cof00 * inv_det);
+      r10 = 0.5f * (r10 + cof10 * inv_det);
+      r20 = 0.5f * (r20 + cof20 * inv_det);
+      r01 = 0.5f * (r01 + cof01 * inv_det);
+      r11 = 0.5f * (r11 + cof11 * inv_det);
+      r21 = 0.5f * (r21 + cof21 * inv_det);
+      r02 = 0.5f * (r02 + cof02 * inv_det);
+      r12 = 0.5f * (r12 + cof12 * inv_det);
+      r22 = 0.5f * (r22 + cof22 * inv_det);
+    }
+  }
+  const float det_final = r00 * (r11 * r22 - r21 * r12) + r10 * (r21 * r02 - r01 * r22) +
+                          r20 * (r01 * r12 - r11 * r02);
+  if (det_final < 0.0f) {
+    r02 = -r02;
+    r12 = -r12;
+    r22 = -r22;
+  }
+  R[0] = r00; R[1] = r10; R[2] = r20; R[3] = r01; R[4] = r11; R[5] = r21;
+  R[6] = r02; R[7] = r12; R[8] = r22;
+}
+
+// 3D Mip filter Sigma + s I with opacity * sqrt(det / det_reg), in the operand
+// order of deformation.rs:914-935 (shared by all three call sites).
+__device__ __forceinline__ void mip3d(float& xx, float xy, float xz, float& yy, float yz,
+                                      float& zz, float& alpha, float mip) {
+  const float det_orig = fmaxf(
+      xx * (yy * zz - yz * yz) - xy * (xy * zz - xz * yz) + xz * (xy * yz - xz * yy), 1e-24f);
+  const float rxx = xx + mip, ryy = yy + mip, rzz = zz + mip;
+  const float det_reg = fmaxf(
+      rxx * (ryy * rzz - yz * yz) - xy * (xy * rzz - xz * yz) + xz * (xy * yz - xz * ryy),
+      det_orig);
+  const float comp = sqrtf(clampf(det_orig / det_reg, 0.0f, 1.0f));
+  xx = rxx;
+  yy = ryy;
+  zz = rzz;
+  alpha = clampf(alpha * comp, 0.0f, 1.0f);
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp_sums[32];
+  __shared__ uint32_t s_base;
+  uint32_t tile;
+  if (SPLIT) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&a.fc->tile_ctr[0], 1u);
+    __syncthreads();
+    tile = s_tile;
+  } else {
+    tile = blockIdx.x;
+    if (tile == 0 && threadIdx.x == 0) *a.split_count = 0u;
+  }
+  const uint32_t i = tile * kDeformThreads + threadIdx.x;
+  bool split = false;
+  uint32_t tet_raw = kInvalid;
+  float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+  float4 out_pos = make_float4(0, 0, 0, 0), out_cova = make_float4(0, 0, 0, 0);
+  float2 out_covb = make_float2(0, 0);
+  if (i < a.n) {
+    tet_raw = a.bind_tet[i];
+    const float4 rp = a.rest_pos[i];
+    const float4 rca = a.rest_cova[i];
+    const float2 rcb = a.rest_covb[i];
+    if (tet_raw >= a.num_tets) {
+      // Unbound: rest pose plus the Mip filter (deformation.rs:899-947).
+      float xx = rca.x, xy = rca.y, xz = rca.z, yy = rca.w, yz = rcb.x, zz = rcb.y;
+      float alpha = rp.w;
+      if (a.mip > 0.0f) mip3d(xx, xy, xz, yy, yz, zz, alpha, a.mip);
+      out_pos = make_float4(rp.x, rp.y, rp.z, alpha);
+      out_cova = make_float4(xx, xy, xz, yy);
+      out_covb = make_float2(yz, zz);
+    } else {
+      const float4 w = a.bind_w[i];
+      const uint4 e = __ldg(&a.elems[tet_raw]);
+      const float* v0 = a.verts + 3 * (size_t)e.x;
+      const float* v1 = a.verts + 3 * (size_t)e.y;
+      const float* v2 = a.verts + 3 * (size_t)e.z;
+      const float* v3 = a.verts + 3 * (size_t)e.w;
+      const float px = w.x * __ldg(v0) + w.y * __ldg(v1) + w.z * __ldg(v2) + w.w * __ldg(v3);
+      const float py =
+          w.x * __ldg(v0 + 1) + w.y * __ldg(v1 + 1) + w.z * __ldg(v2 + 1) + w.w * __ldg(v3 + 1);
+      const float pz =
+          w.x * __ldg(v0 + 2) + w.y * __ldg(v1 + 2) + w.z * __ldg(v2 + 2) + w.w * __ldg(v3 + 2);
+      const float* J = a.tet_J + 9 * (size_t)tet_raw;
+      const float j_00 = __ldg(J + 0), j_10 = __ldg(J + 1), j_20 = __ldg(J + 2);
+      const float j_01 = __ldg(J + 3), j_11 = __ldg(J + 4), j_21 = __ldg(J + 5);
+      const float j_02 = __ldg(J + 6), j_12 = __ldg(J + 7), j_22 = __ldg(J + 8);
+      const float s_xx = rca.x, s_xy = rca.y, s_xz = rca.z, s_yy = rca.w, s_yz = rcb.x,
+                  s_zz = rcb.y;
+      const float k_00 = j_00 * s_xx + j_01 * s_xy + j_02 * s_xz;
+      const float k_01 = j_00 * s_xy + j_01 * s_yy + j_02 * s_yz;
+      const float k_02 = j_00 * s_xz + j_01 * s_yz + j_02 * s_zz;
+      const float k_10 = j_10 * s_xx + j_11 * s_xy + j_12 * s_xz;
+      const float k_11 = j_10 * s_xy + j_11 * s_yy + j_12 * s_yz;
+      const float k_12 = j_10 * s_xz + j_11 * s_yz + j_12 * s_zz;
+      const float k_20 = j_20 * s_xx + j_21 * s_xy + j_22 * s_xz;
+      const float k_21 = j_20 * s_xy + j_21 * s_yy + j_22 * s_yz;
+      const float k_22 = j_20 * s_xz + j_21 * s_yz + j_22 * s_zz;
+      const float m00 = fmaxf(1e-4f, k_00 * j_00 + k_01 * j_01 + k_02 * j_02);
+      const float m01 = 0.5f * ((k_00 * j_10 + k_01 * j_11 + k_02 * j_12) +
+                                (k_10 * j_00 + k_11 * j_01 + k_12 * j_02));
+      const float m02 = 0.5f * ((k_00 * j_20 + k_01 * j_21 + k_02 * j_22) +
+                                (k_20 * j_00 + k_21 * j_01 + k_22 * j_02));
+      const float m11 = fmaxf(1e-4f, k_10 * j_10 + k_11 * j_11 + k_12 * j_12);
+      const float m12 = 0.5f * ((k_10 * j_20 + k_11 * j_21 + k_12 * j_22) +
+                                (k_20 * j_10 + k_21 * j_11 + k_22 * j_12));
+      const float m22 = fmaxf(1e-4f, k_20 * j_20 + k_21 * j_21 + k_22 * j_22);
+      const float det_j = j_00 * (j_11 * j_22 - j_12 * j_21) -
+                          j_01 * (j_10 * j_22 - j_12 * j_20) + j_02 * (j_10 * j_21 - j_11 * j_20);
+      const float s_det = clampf(det_j, 0.6f, 1.8f);
+      const float safe_base = clampf(1.0f - rp.w, 1e-4f, 0.999f);
+      const float alpha_prime = clampf(1.0f - cgs_powf(safe_base, 1.0f / s_det), 0.05f, 0.99f);
+      split = SPLIT && a.split_threshold > 0.0f && __ldg(&a.tet_stretch[tet_raw]) > a.split_threshold;
+      if (!split) {
+        float xx = m00, yy = m11, zz = m22, alpha = alpha_prime;
+        if (a.mip > 0.0f) mip3d(xx, m01, m02, yy, m12, zz, alpha, a.mip);
+        out_pos = make_float4(px, py, pz, alpha);
+        out_cova = make_float4(xx, m01, m02, yy);
+        out_covb = make_float2(m12, zz);
+      } else {
+        // Major eigenpair of M by Cardano + cross products (deformation.rs:1066-1143).
+        const float p1 = m01 * m01 + m02 * m02 + m12 * m12;
+        float lambda0 = fmaxf(m00, fmaxf(m11, m22));
+        float ux = 1.0f, uy = 0.0f, uz = 0.0f;
+        if (p1 <= 1e-10f) {
+          if (m11 >= m00 && m11 >= m22) {
+            ux = 0.0f; uy = 1.0f; uz = 0.0f;
+          } else if (m22 >= m00 && m22 >= m11) {
+            ux = 0.0f; uy = 0.0f; uz = 1.0f;
+          }
+        } else {
+          const float q = (m00 + m11 + m22) / 3.0f;
+          const float d0 = m00 - q, d1 = m11 - q, d2 = m22 - q;
+          const float p2 = d0 * d0 + d1 * d1 + d2 * d2 + 2.0f * p1;
+          const float p = sqrtf(fmaxf(p2 / 6.0f, 1e-12f));
+          const float inv_p = 1.0f / p;
+          const float b00 = d0 * inv_p, b11 = d1 * inv_p, b22 = d2 * inv_p;
+          const float b01 = m01 * inv_p, b02 = m02 * inv_p, b12 = m12 * inv_p;
+          const float det_b = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) +
+                              b02 * (b01 * b12 - b11 * b02);
+          const float r = clampf(0.5f * det_b, -1.0f, 1.0f);
+          const float phi = cgs_acosf(r) / 3.0f;
+          lambda0 = q + 2.0f * p * cgs_cosf(phi);
+          const float r0x = m00 - lambda0, r0y = m01, r0z = m02;
+          const float r1x = m01, r1y = m11 - lambda0, r1z = m12;
+          const float r2x = m02, r2y = m12, r2z = m22 - lambda0;
+          const float c01x = r0y * r1z - r0z * r1y, c01y = r0z * r1x - r0x * r1z,
+                      c01z = r0x * r1y - r0y * r1x;
+          const float n01 = c01x * c01x + c01y * c01y + c01z * c01z;
+          const float c12x = r1y * r2z - r1z * r2y, c12y = r1z * r2x - r1x * r2z,
+                      c12z = r1x * r2y - r1y * r2x;
+          const float n12 = c12x * c12x + c12y * c12y + c12z * c12z;
+          const float c02x = r0y * r2z - r0z * r2y, c02y = r0z * r2x - r0x * r2z,
+                      c02z = r0x * r2y - r0y * r2x;
+          const float n02 = c02x * c02x + c02y * c02y + c02z * c02z;
+          if (n01 >= n12 && n01 >= n02 && n01 > 1e-12f) {
+            const float inv = 1.0f / sqrtf(n01);
+            ux = c01x * inv; uy = c01y * inv; uz = c01z * inv;
+          } else if (n12 >= n02 && n12 > 1e-12f) {
+            const float inv = 1.0f / sqrtf(n12);
+            ux = c12x * inv; uy = c12y * inv; uz = c12z * inv;
+          } else if (n02 > 1e-12f) {
+            const float inv = 1.0f / sqrtf(n02);
+            ux = c02x * inv; uy = c02y * inv; uz = c02z * inv;
+          }
+        }
+        const float safe_l0 = fmaxf(lambda0, 1e-8f);
+        const float offset_mag = 0.5f * sqrtf(safe_l0);
+        const float dx = ux * offset_mag, dy = uy * offset_mag, dz = uz * offset_mag;
+        const float shrink = 0.75f * safe_l0;
+        float c00 = fmaxf(1e-8f, m00 - shrink * ux * ux);
+        const float c01 = m01 - shrink * ux * uy;
+        const float c02 = m02 - shrink * ux * uz;
+        float c11 = fmaxf(1e-8f, m11 - shrink * uy * uy);
+        const float c12 = m12 - shrink * uy * uz;
+        float c22 = fmaxf(1e-8f, m22 - shrink * uz * uz);
+        float child_alpha = alpha_prime;
+        if (a.mip > 0.0f) mip3d(c00, c01, c02, c11, c12, c22, child_alpha, a.mip);
+        out_pos = make_float4(px - dx, py - dy, pz - dz, child_alpha);
+        out_cova = make_float4(c00, c01, c02, c11);
+        out_covb = make_float2(c12, c22);
+        cx = px + dx;
+        cy = py + dy;
+        cz = pz + dz;
+      }
+    }
+    a.def_pos[i] = out_pos;
+    a.def_cova[i] = out_cova;
+    a.def_covb[i] = out_covb;
+  }
+  if (SPLIT) {
+    uint32_t agg;
+    const uint32_t excl = block_exclusive_sum(split ? 1u : 0u, s_warp_sums, &agg);
+    if (threadIdx.x < 32) {
+      const uint32_t base = chained_scan_warp(a.status, tile, agg, &a.fc->status);
+      if (threadIdx.x == 0) s_base = base;
+    }
+    __syncthreads();
+    const uint32_t base = s_base;
+    if (split) {
+      const size_t c = (size_t)a.n + base + excl;
+      a.def_pos[c] = make_float4(cx, cy, cz, out_pos.w);
+      a.def_cova[c] = out_cova;
+      a.def_covb[c] = out_covb;
+      a.split_meta[base + excl] = make_uint2(i, tet_raw);
+    }
+    const uint32_t num_tiles = (a.n + kDeformThreads - 1) / kDeformThreads;
+    if (tile == num_tiles - 1 && threadIdx.x == 0) *a.split_count = base + agg;
+  }
+}
+
+// Barycentric binding, first tet with violation <= 1e-4 in index order,
+// else the least-violating tet (strict <), as TetMesh::bind_point. Tet data
+// (first rest vertex + D_m^-1, 12 floats) is staged through shared memory in
+// chunks; the block keeps loading chunks while any of its points still searches.
+constexpr int kBindThreads = 256;
+constexpr int kBindChunk = 1024;
+
+__global__ void __launch_bounds__(kBindThreads) k_bind(BindArgs a) {
+  __shared__ float s_tet[kBindChunk * 12];
+  const uint32_t i = blockIdx.x * kBindThreads + threadIdx.x;
+  float px = 0, py = 0, pz = 0;
+  bool searching = i < a.n;
+  bool outside = false;
+  if (searching) {
+    const float4 p = a.points[i];
+    px = p.x; py = p.y; pz = p.z;
+    if (a.use_bounds) {
+      outside = px < a.bmin[0] || px > a.bmax[0] || py < a.bmin[1] || py > a.bmax[1] ||
+                pz < a.bmin[2] || pz > a.bmax[2];
+      if (outside) searching = false;
+    }
+  }
+  uint32_t found = kInvalid;
+  float4 found_w = make_float4(0, 0, 0, 0);
+  uint32_t best_tet = 0;
+  float best_pen = __uint_as_float(0x7f800000u);
+  float4 best_w = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+  for (uint32_t c0 = 0; c0 < a.num_tets; c0 += kBindChunk) {
+    if (!__syncthreads_or(searching)) break;
+    const uint32_t cn = min((uint32_t)kBindChunk, a.num_tets - c0);
+    for (uint32_t k = threadIdx.x; k < cn; k += kBindThreads) {
+      const float* x0 = a.tet_x0 + 3 * (size_t)(c0 + k);
+      const float* m = a.inv_dm + 9 * (size_t)(c0 + k);
+      float* d = s_tet + 12 * k;
+      d[0] = x0[0]; d[1] = x0[1]; d[2] = x0[2];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) d[3 + q] = m[q];
+    }
+    __syncthreads();
+    if (searching) {
+      for (uint32_t k = 0; k < cn; ++k) {
+        const float* d = s_tet + 12 * k;
+        const float dx = px - d[0], dy = py - d[1], dz = pz - d[2];
+        // glam Mat3 * Vec3: (c0 * x + c1 * y) + c2 * z
+        const float w1 = (d[3] * dx + d[6] * dy) + d[9] * dz;
+        const float w2 = (d[4] * dx + d[7] * dy) + d[10] * dz;
+        const float w3 = (d[5] * dx + d[8] * dy) + d[11] * dz;
+        const float w0 = 1.0f - ((w1 + w2) + w3);
+        const float pen = ((fmaxf(-w0, 0.0f) + fmaxf(-w1, 0.0f)) + fmaxf(-w2, 0.0f)) +
+                          fmaxf(-w3, 0.0f);
+        if (pen <= 1e-4f) {
+          found = c0 + k;
+          found_w = make_float4(w0, w1, w2, w3);
+          searching = false;
+          break;
+        }
+        if (pen < best_pen) {
+          best_pen = pen;
+          best_tet = c0 + k;
+          best_w = make_float4(w0, w1, w2, w3);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (i >= a.n) return;
+  if (outside) {
+    a.bind_tet[i] = kInvalid;
+    a.bind_w[i] = make_float4(0, 0, 0, 0);
+  } else if (found != kInvalid) {
+    a.bind_tet[i] = found;
+    a.bind_w[i] = found_w;
+  } else if (a.use_bounds && best_pen > 0.15f) {
+    a.bind_tet[i] = kInvalid;
+    a.bind_w[i] = make_float4(0, 0, 0, 0);
+  } else if (a.num_tets == 0) {
+    a.bind_tet[i] = kInvalid;
+    a.bind_w[i] = make_float4(0, 0, 0, 0);
+  } else {
+    a.bind_tet[i] = best_tet;
+    a.bind_w[i] = best_w;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_tet_transforms(const DeformArgs& a, cudaStream_t s) {
+  if (a.num_tets == 0) return cudaSuccess;
+  k_tet_transforms<<<(a.num_tets + 127) / 128, 128, 0, s>>>(a.num_tets, a.verts, a.elems,
+                                                            a.inv_dm, a.tet_J, a.tet_R,
+                                                            a.tet_stretch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s) {
+  if (a.n == 0) return cudaSuccess;
+  const uint32_t blocks = (a.n + kDeformThreads - 1) / kDeformThreads;
+  if (a.split_threshold > 0.0f)
+    k_deform<true><<<blocks, kDeformThreads, 0, s>>>(a);
+  else
+    k_deform<false><<<blocks, kDeformThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bind(const BindArgs& a, cudaStream_t s) {
+  if (a.n == 0) return cudaSuccess;
+  k_bind<<<(a.n + kBindThreads - 1) / kBindThreads, kBindThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace cgs

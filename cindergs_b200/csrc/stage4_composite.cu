@@ -1,0 +1,196 @@
+// Stage 4: 16x16 tile compositor on sm_100a (tile_compositor_v2_kernel,
+// render/kernels/compositor.rs:727-883).
+//
+// One block of 256 threads per screen tile, one pixel per thread. The tile's
+// depth-sorted splat list is consumed in batches of 256: each batch's 48-byte
+// splat records are gathered from the Stage 2 record array into shared memory
+// by the Tensor Memory Accelerator's bulk-copy engine (one cp.async.bulk per
+// record, all completing on one mbarrier with an expected byte count), double
+// buffered so the next batch is in flight while the current one is blended.
+// Blending follows the reference: skip opacity <= 1/255; q = -(a dx^2 +
+// 2 b dx dy + c dy^2)/2 clamped to <= 0; skip q < -4; alpha = min(0.99,
+// op e^q); skip alpha < 1/255; front-to-back accumulate; a pixel stops at
+// T < 1e-3 (T := 0). The q cut and the alpha cut are evaluated exactly as the
+// host restatement does (IEEE-rounded q, the deterministic exp near the cut),
+// so the only differences are last-bit colour sums and the rare pixel whose
+// transmittance lands within an ulp of 1e-3 (bounded by that 1e-3). The block stops when no pixel is still accumulating
+// (__syncthreads_or, the reference's double-buffered tile_alive vote). Output
+// is RGBA8 packed in u32 rows padded to 64 pixels, optionally also RGBA f32.
+// Every wait on an mbarrier is bounded; a block never exits with a bulk copy
+// still in flight into its shared memory.
+#include "kernels.h"
+
+namespace cgs {
+namespace {
+
+constexpr int kCompThreads = 256;
+constexpr int kBatch = 256;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for a phase; returns false (and the caller flags it) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs a) {
+  __shared__ __align__(128) SplatRec s_rec[2][kBatch];
+  __shared__ __align__(8) uint64_t s_bar[2];
+
+  const uint32_t tid = threadIdx.x;
+  const uint32_t px = blockIdx.x * 16u + (tid & 15u);
+  const uint32_t py = blockIdx.y * 16u + (tid >> 4);
+  const bool inside = px < a.width && py < a.height;
+  const uint32_t tile_id = blockIdx.y * a.tiles_x + blockIdx.x;
+  const uint32_t rs = min(a.ranges[2 * (size_t)tile_id], a.num_entries);
+  const uint32_t re = min(a.ranges[2 * (size_t)tile_id + 1], a.num_entries);
+  const bool empty = rs >= re;
+  const uint32_t n = empty ? 0u : re - rs;
+  const uint32_t nb = (n + kBatch - 1) / kBatch;
+
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  auto issue = [&](uint32_t b) {
+    const uint32_t stage = b & 1u;
+    const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
+    if (tid == 0) mbar_arrive_expect_tx(&s_bar[stage], cnt * (uint32_t)sizeof(SplatRec));
+    if (tid < cnt) {
+      uint32_t id = a.sorted_ids[rs + b * kBatch + tid];
+      if (id >= a.num_recs) {  // never let a bad id become an out-of-bounds copy
+        if (a.fc) atomicOr(&a.fc->status, kStatusCapacity);
+        id = 0;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      bulk_copy_g2s(&s_rec[stage][tid], a.recs + id, (uint32_t)sizeof(SplatRec), &s_bar[stage]);
+    }
+  };
+
+  float cr = 0.0f, cg = 0.0f, cb = 0.0f, t = 1.0f;
+  bool saturated = false;
+  const float pcx = (float)px + 0.5f, pcy = (float)py + 0.5f;
+  bool ok = true;
+  uint32_t consumed = 0;
+  uint32_t issued = 0;
+  if (nb > 0) {
+    issue(0);
+    issued = 1;
+  }
+  for (uint32_t b = 0; b < nb; ++b) {
+    const uint32_t stage = b & 1u;
+    if (b + 1 < nb) {
+      issue(b + 1);
+      issued = b + 2;
+    }
+    if (!mbar_wait(&s_bar[stage], (b >> 1) & 1u)) ok = false;
+    consumed = b + 1;
+    const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
+    if (inside && !saturated) {
+      const SplatRec* recs = s_rec[stage];
+      for (uint32_t k = 0; k < cnt; ++k) {
+        const float4 cc4 = recs[k].cc;
+        const float op = cc4.y;
+        if (op > 0.003921569f) {
+          const float4 geo = recs[k].geo;
+          const float dx = pcx - geo.x, dy = pcy - geo.y;
+          // q rounded term by term in the reference's order: the q >= -4 cut
+          // then agrees exactly with the host restatement.
+          const float qa = __fmul_rn(__fmul_rn(geo.z, dx), dx);
+          const float qb = __fmul_rn(__fmul_rn(__fmul_rn(2.0f, geo.w), dx), dy);
+          const float qc = __fmul_rn(__fmul_rn(cc4.x, dy), dy);
+          float q = __fmul_rn(-0.5f, __fadd_rn(__fadd_rn(qa, qb), qc));
+          q = fminf(q, 0.0f);
+          if (q >= -4.0f) {
+            float raw = op * __expf(q);
+            // Near the 1/255 visibility cut, re-evaluate with the deterministic
+            // exp so the keep/skip decision matches the host restatement.
+            if (fabsf(raw - 0.003921569f) < 4e-7f) raw = __fmul_rn(op, cgs_expf(q));
+            const float alpha = fminf(0.99f, raw);
+            if (alpha >= 0.003921569f) {
+              const float4 rgb = recs[k].rgb;
+              const float w = alpha * t;
+              cr += w * rgb.x;
+              cg += w * rgb.y;
+              cb += w * rgb.z;
+              t *= 1.0f - alpha;
+              if (t < 0.001f) {
+                saturated = true;
+                t = 0.0f;
+                break;
+              }
+            }
+          }
+        }
+      }
+    }
+    if (!__syncthreads_or(inside && !saturated)) break;
+  }
+  // Never leave with a bulk copy still writing into this block's shared memory.
+  for (uint32_t b = consumed; b < issued; ++b)
+    if (!mbar_wait(&s_bar[b & 1u], (b >> 1) & 1u)) ok = false;
+  if (!ok && a.fc) atomicOr(&a.fc->status, kStatusBarrierTimeout);
+
+  if (inside) {
+    const float fr = clampf(cr + t * a.bg[0], 0.0f, 1.0f);
+    const float fg = clampf(cg + t * a.bg[1], 0.0f, 1.0f);
+    const float fb = clampf(cb + t * a.bg[2], 0.0f, 1.0f);
+    const float fa = empty ? a.bg[3] : clampf(1.0f - t, 0.0f, 1.0f);
+    const uint32_t r8 = (uint32_t)clampf(rintf(fr * 255.0f), 0.0f, 255.0f);
+    const uint32_t g8 = (uint32_t)clampf(rintf(fg * 255.0f), 0.0f, 255.0f);
+    const uint32_t b8 = (uint32_t)clampf(rintf(fb * 255.0f), 0.0f, 255.0f);
+    const uint32_t a8 = (uint32_t)clampf(rintf(fa * 255.0f), 0.0f, 255.0f);
+    a.out_rgba8[(size_t)py * a.pitch_px + px] = r8 | (g8 << 8) | (b8 << 16) | (a8 << 24);
+    if (a.out_f32) a.out_f32[(size_t)py * a.width + px] = make_float4(fr, fg, fb, fa);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_composite(const CompositeArgs& a, cudaStream_t s) {
+  if (a.tiles_x == 0 || a.tiles_y == 0) return cudaSuccess;
+  dim3 grid(a.tiles_x, a.tiles_y);
+  k_composite<<<grid, kCompThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace cgs

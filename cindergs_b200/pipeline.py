@@ -1,0 +1,303 @@
+"""GpuPipelineState: the reference's persistent four-stage GPU frame API
+(render/gpu_state.rs:538-1343) on top of the sm_100a C library.
+
+    state = GpuPipelineState()
+    timings = state.execute_frame_gpu(scene, cages, camera, compositor,
+                                      strain_split_threshold, mip_filter_3d_var,
+                                      min_opacity, min_radius_px,
+                                      profile_stages, force_stage3)
+    rgba8 = state.readback_framebuffer_rgba8(width, height)
+
+Residency rules follow GpuSceneState::sync_scene_and_cages
+(gpu_state.rs:182-343): the rest scene is re-uploaded when its fingerprint
+(array identities, size and a 64-sample value hash) changes, the cage
+topology when the cage list or bindings change, and cage vertices every call
+(the library skips Stage 1 when they are unchanged).
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from .camera import CameraUniforms, CompositorUniforms
+from .cage import CageScene, TetMesh, UNBOUND
+from .scene import GaussianSceneSoa
+
+f32 = np.float32
+
+
+@dataclass
+class GpuStageTimings:
+    """GpuStageTimings (gpu_state.rs:513-534)."""
+    stage1_deform_ms: float = 0.0
+    stage2_project_ms: float = 0.0
+    stage3_bin_sort_ms: float = 0.0
+    stage4_composite_ms: float = 0.0
+    stage1_skipped: bool = False
+    stage3_cached: bool = False
+    used_hardware_timestamps: bool = False
+    used_64bit_keys: bool = False
+    active_gaussians: int = 0
+    surviving_gaussians: int = 0
+    total_tile_entries: int = 0
+
+    @property
+    def total_ms(self) -> float:
+        return (self.stage1_deform_ms + self.stage2_project_ms + self.stage3_bin_sort_ms +
+                self.stage4_composite_ms)
+
+
+def scene_fingerprint(scene: GaussianSceneSoa) -> bytes:
+    """Change detector of GpuSceneState (scene_fingerprint, gpu_state.rs:65-79):
+    count, array identities and 64 evenly spaced samples (plus the last value)
+    of each array, hashed with BLAKE2b."""
+    h = hashlib.blake2b(digest_size=16)
+    h.update(int(scene.count).to_bytes(8, "little"))
+    for arr in (scene.positions, scene.covariances_3d, scene.opacities, scene.sh_coeffs):
+        h.update(int(arr.ctypes.data).to_bytes(8, "little"))
+        flat = arr.reshape(-1)
+        h.update(int(flat.size).to_bytes(8, "little"))
+        step = max(flat.size // 64, 1)
+        h.update(flat[::step].tobytes())
+        if flat.size:
+            h.update(flat[-1:].tobytes())
+    return h.digest()
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class GpuPipelineState:
+    """Persistent GPU state: scene residency + frame arena, on one device."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._lib = _abi.load()
+        self._ctx = ctypes.c_void_p()
+        rc = self._lib.cgs_ctx_create(int(device), ctypes.c_void_p(stream or 0),
+                                      ctypes.byref(self._ctx))
+        if rc != _abi.CGS_OK:
+            raise _abi.CgsError(rc, "cgs_ctx_create", "could not create a CUDA context")
+        self._scene_hash = None
+        self._scene_count = -1
+        self._cage_key = None
+        self._last = None
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.cgs_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, fn: str) -> None:
+        _abi.check(rc, fn, self._ctx)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._ctx
+
+    # -- residency ------------------------------------------------------------
+    def upload_scene(self, scene: GaussianSceneSoa) -> None:
+        pos = np.ascontiguousarray(scene.positions, f32)
+        cov = np.ascontiguousarray(scene.covariances_3d, f32)
+        opa = np.ascontiguousarray(scene.opacities, f32)
+        if scene.sh_coeffs.dtype == np.float16:
+            sh, fmt = np.ascontiguousarray(scene.sh_coeffs), _abi.CGS_SH_F16
+        else:
+            sh, fmt = np.ascontiguousarray(scene.sh_coeffs, f32), _abi.CGS_SH_F32
+        self._check(self._lib.cgs_scene_upload(self._ctx, scene.count, _p(pos), _p(cov), _p(opa),
+                                               _p(sh), fmt), "cgs_scene_upload")
+        self._scene_hash = scene_fingerprint(scene)
+        self._scene_count = scene.count
+        self._cage_key = None
+
+    def upload_cages(self, cages: CageScene | None) -> None:
+        if cages is None or not cages.cages:
+            self._check(self._lib.cgs_tet_cages_upload(self._ctx, 0, None, None, 0, None, None),
+                        "cgs_tet_cages_upload")
+            self._cage_key = ("none",)
+            return
+        elems, inv, nverts, bt, bw = cages.flatten()
+        self._check(self._lib.cgs_tet_cages_upload(self._ctx, elems.shape[0], _p(elems), _p(inv),
+                                                   nverts, _p(bt), _p(bw)),
+                    "cgs_tet_cages_upload")
+        self._cage_key = (id(cages), cages.bind_tet.ctypes.data, len(cages.cages),
+                          tuple((id(c.mesh), c.mesh.num_tets, c.mesh.num_vertices)
+                                for c in cages.cages))
+
+    def sync_scene_and_cages(self, scene: GaussianSceneSoa, cages: CageScene | None) -> None:
+        h = scene_fingerprint(scene)
+        if h != self._scene_hash or scene.count != self._scene_count:
+            self.upload_scene(scene)
+        if cages is None or not cages.cages:
+            if self._cage_key != ("none",):
+                self.upload_cages(None)
+            return
+        key = (id(cages), cages.bind_tet.ctypes.data, len(cages.cages),
+               tuple((id(c.mesh), c.mesh.num_tets, c.mesh.num_vertices) for c in cages.cages))
+        if key != self._cage_key:
+            self.upload_cages(cages)
+        v = np.ascontiguousarray(cages.flat_vertices(), f32)
+        self._check(self._lib.cgs_cage_vertices_update(self._ctx, _p(v), v.shape[0]),
+                    "cgs_cage_vertices_update")
+
+    def bind_tets(self, mesh: TetMesh, bounds=None):
+        """GPU barycentric binding of the resident scene to `mesh`
+        (TetMesh::bind_point). Returns (tet [N] u32, weights [N,4] f32)."""
+        n = max(self._scene_count, 0)
+        tets = np.zeros(n, np.uint32)
+        w = np.zeros((n, 4), f32)
+        elems = np.ascontiguousarray(mesh.elements, np.uint32)
+        inv = np.ascontiguousarray(mesh.inv_dm, f32)
+        rv = np.ascontiguousarray(mesh.rest_vertices, f32)
+        if bounds is not None:
+            bmin = np.ascontiguousarray(bounds[0], f32)
+            bmax = np.ascontiguousarray(bounds[1], f32)
+            ub, pmin, pmax = 1, _p(bmin), _p(bmax)
+        else:
+            ub, pmin, pmax = 0, None, None
+        self._check(self._lib.cgs_bind_tets(self._ctx, mesh.num_tets, _p(elems), _p(inv),
+                                            mesh.num_vertices, _p(rv), ub, pmin, pmax, _p(tets),
+                                            _p(w)), "cgs_bind_tets")
+        return tets, w
+
+    # -- frame ------------------------------------------------------------------
+    def execute_frame_gpu(self, scene: GaussianSceneSoa, cages: CageScene | None,
+                          camera: CameraUniforms, compositor: CompositorUniforms,
+                          strain_split_threshold: float = 0.0, mip_filter_3d_var: float = 0.0,
+                          min_opacity: float = 1.0 / 255.0, min_radius_px: float = 0.5,
+                          profile_stages: bool = False, force_stage3: bool = False,
+                          write_f32: bool = False, radix_bits: int = 0,
+                          stage_timings: bool = True) -> GpuStageTimings:
+        """execute_frame_gpu (gpu_state.rs:613-1243). With profile_stages and
+        stage_timings both set, the call waits for the frame to report its
+        per-stage device ms; with stage_timings=False a profiled frame only
+        accumulates kernel times (read them with kernel_profile())."""
+        self.sync_scene_and_cages(scene, cages)
+        cam = _abi.CgsCamera()
+        arr = camera.to_array()
+        for k in range(16):
+            cam.view[k] = float(arr[k])
+        (cam.focal_x, cam.focal_y, cam.principal_x, cam.principal_y, cam.viewport_width,
+         cam.viewport_height, cam.near_plane) = (float(x) for x in arr[16:23])
+        comp = self._compositor(compositor)
+        params = _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
+                                     float(min_opacity), float(min_radius_px),
+                                     int(bool(profile_stages)), int(bool(force_stage3)),
+                                     int(bool(write_f32)), int(radix_bits))
+        t = _abi.CgsStageTimings()
+        tp = ctypes.byref(t) if (stage_timings or not profile_stages) else None
+        self._check(self._lib.cgs_execute_frame(self._ctx, ctypes.byref(cam), ctypes.byref(comp),
+                                                ctypes.byref(params), tp),
+                    "cgs_execute_frame")
+        self._last = (compositor.screen_width, compositor.screen_height)
+        return GpuStageTimings(t.stage1_deform_ms, t.stage2_project_ms, t.stage3_bin_sort_ms,
+                               t.stage4_composite_ms, bool(t.stage1_skipped),
+                               bool(t.stage3_cached), bool(t.used_hardware_timestamps),
+                               bool(t.used_64bit_keys), int(t.active_gaussians),
+                               int(t.surviving_gaussians), int(t.total_tile_entries))
+
+    @staticmethod
+    def _compositor(c: CompositorUniforms) -> _abi.CgsCompositor:
+        comp = _abi.CgsCompositor()
+        comp.screen_width = int(c.screen_width)
+        comp.screen_height = int(c.screen_height)
+        comp.tiles_x = c.tiles_x
+        comp.tiles_y = c.tiles_y
+        for k in range(4):
+            comp.background[k] = float(c.background_color[k])
+        for k in range(3):
+            comp.camera_position[k] = float(c.camera_position[k])
+        comp.sh_degree = min(int(c.sh_degree), 3)
+        return comp
+
+    def readback_framebuffer_rgba8(self, width: int, height: int) -> np.ndarray:
+        """Tight [H, W, 4] uint8 copy of the last frame (gpu_state.rs:1296-1328)."""
+        out = np.empty((height, width, 4), np.uint8)
+        self._check(self._lib.cgs_readback_rgba8(self._ctx, _p(out), width, height),
+                    "cgs_readback_rgba8")
+        return out
+
+    def readback_framebuffer_f32(self, width: int, height: int) -> np.ndarray:
+        out = np.empty((height, width, 4), f32)
+        self._check(self._lib.cgs_readback_rgba_f32(self._ctx, _p(out), width, height),
+                    "cgs_readback_rgba_f32")
+        return out
+
+    def invalidate(self) -> None:
+        self._check(self._lib.cgs_invalidate(self._ctx), "cgs_invalidate")
+        self._scene_hash = None
+        self._cage_key = None
+
+    def invalidate_stage3(self) -> None:
+        self._check(self._lib.cgs_invalidate_stage3(self._ctx), "cgs_invalidate_stage3")
+
+    def synchronize(self) -> None:
+        self._check(self._lib.cgs_ctx_synchronize(self._ctx), "cgs_ctx_synchronize")
+
+    def device_bytes(self) -> int:
+        v = ctypes.c_uint64()
+        self._check(self._lib.cgs_ctx_device_bytes(self._ctx, ctypes.byref(v)),
+                    "cgs_ctx_device_bytes")
+        return int(v.value)
+
+    def kernel_profile(self) -> dict:
+        """Per-kernel device ms, launches and algorithmic HBM bytes accumulated
+        over the frames run with profile_stages=True since the last reset."""
+        kp = _abi.CgsKernelProfile()
+        self._check(self._lib.cgs_kernel_profile_read(self._ctx, ctypes.byref(kp)),
+                    "cgs_kernel_profile_read")
+        return {name: dict(ms=kp.ms[i], launches=int(kp.launches[i]),
+                           alg_bytes=int(kp.alg_bytes[i]))
+                for i, name in enumerate(_abi.KERNEL_NAMES)}
+
+    def kernel_profile_reset(self) -> None:
+        self._check(self._lib.cgs_kernel_profile_reset(self._ctx), "cgs_kernel_profile_reset")
+
+    def read_buffer(self, which: int, dtype) -> np.ndarray:
+        """Intermediate buffer of the last frame (CGS_BUF_*), as a flat array."""
+        nbytes = ctypes.c_uint64()
+        self._check(self._lib.cgs_read_frame_buffer(self._ctx, which, None, 0,
+                                                    ctypes.byref(nbytes)), "cgs_read_frame_buffer")
+        out = np.empty(int(nbytes.value) // np.dtype(dtype).itemsize, dtype)
+        self._check(self._lib.cgs_read_frame_buffer(self._ctx, which, _p(out), out.nbytes,
+                                                    ctypes.byref(nbytes)), "cgs_read_frame_buffer")
+        return out
+
+
+# -- device-array primitives (render/kernels/scan.rs, radix_sort.rs) ---------------
+
+def exclusive_scan_u32(state: GpuPipelineState, d_in: int, d_out: int, n: int) -> int:
+    """gpu_exclusive_scan_total on raw device pointers; returns the total."""
+    total = ctypes.c_uint64()
+    _abi.check(state._lib.cgs_scan_u32(state.handle, ctypes.c_void_p(d_in),
+                                       ctypes.c_void_p(d_out), n, ctypes.byref(total)),
+               "cgs_scan_u32", state.handle)
+    return int(total.value)
+
+
+def radix_sort_u32_pairs(state: GpuPipelineState, d_keys: int, d_vals: int, n: int,
+                         key_bits: int = 32, digit_bits: int = 0) -> None:
+    """gpu_radix_sort_u32_pairs on raw device pointers (sorted in place)."""
+    _abi.check(state._lib.cgs_sort_pairs_u32(state.handle, ctypes.c_void_p(d_keys),
+                                             ctypes.c_void_p(d_vals), n, key_bits, digit_bits),
+               "cgs_sort_pairs_u32", state.handle)
+
+
+def radix_sort_u64_pairs(state: GpuPipelineState, d_tiles: int, d_depths: int, d_ids: int,
+                         n: int, tile_bits: int, digit_bits: int = 0) -> None:
+    """gpu_radix_sort_u64_pairs on raw device pointers (sorted in place)."""
+    _abi.check(state._lib.cgs_sort_pairs_u64(state.handle, ctypes.c_void_p(d_tiles),
+                                             ctypes.c_void_p(d_depths), ctypes.c_void_p(d_ids),
+                                             n, tile_bits, digit_bits),
+               "cgs_sort_pairs_u64", state.handle)

@@ -1,0 +1,233 @@
+/*
+ * cgs.h - C ABI of the B200 (sm_100a) four-stage Gaussian-splat pipeline.
+ *
+ * This is the drop-in boundary that replaces CinderGS's CubeCL/WGPU backend
+ * (crate `cinder_gs`, v2.0.0). Every entry point below names the reference
+ * interface it stands in for (path:line inside the reference crate). A Rust
+ * `-sys` crate, a ctypes module or a C++ host binds these symbols directly:
+ * plain pointers and sizes, no CUDA or torch types in any signature.
+ *
+ * Conventions
+ *  - Every call returns an int status: CGS_OK (0) or a negative CGS_E_* code.
+ *    cgs_last_error(ctx) returns a message for the last failure on ctx.
+ *  - A context owns one CUDA device, one stream and all device memory
+ *    (scene residency + frame arena). One context per host thread; calls on a
+ *    context are not re-entrant (the reference's `&mut self` API, same rule).
+ *  - Host arrays are borrowed for the duration of the call only.
+ *  - "d_" parameters are device pointers on the context's device; they are
+ *    used on the context's stream.
+ *  - There is no CPU fallback: when the device path cannot run, the call
+ *    returns an error (the reference's orchestrator fell back to the CPU,
+ *    render/pipeline.rs:721-737; this library does not).
+ */
+#ifndef CGS_H
+#define CGS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGS_OK 0
+#define CGS_E_ARG -1       /* invalid argument (null pointer, bad size, bad enum) */
+#define CGS_E_OOM -2       /* device or pinned-host allocation failed */
+#define CGS_E_CUDA -3      /* a CUDA runtime call failed */
+#define CGS_E_TIMEOUT -4   /* a bounded device-side wait gave up (status word set) */
+#define CGS_E_CAPACITY -5  /* a size exceeds a documented hard limit */
+#define CGS_E_STATE -6     /* call order violated (e.g. frame before scene upload) */
+
+#define CGS_SH_F32 0  /* 48 f32 SH coefficients per Gaussian (soa.rs:30-52) */
+#define CGS_SH_F16 1  /* 48 IEEE binary16 SH coefficients per Gaussian (soa.rs:429-608) */
+
+/* Camera uniform block, 96 bytes: render/camera.rs:9-36 (CameraUniforms).
+ * view is the column-major world-to-camera matrix (glam Mat4::to_cols_array). */
+typedef struct cgs_camera {
+  float view[16];
+  float focal_x, focal_y;
+  float principal_x, principal_y;
+  float viewport_width, viewport_height;
+  float near_plane;
+  float pad;
+} cgs_camera;
+
+/* Compositor uniform block, 48 bytes: render/rasterizer/mod.rs:16-37
+ * (CompositorUniforms). tiles_x/tiles_y are recomputed from the screen size. */
+typedef struct cgs_compositor {
+  uint32_t screen_width, screen_height;
+  uint32_t tiles_x, tiles_y;
+  float background[4];
+  float camera_position[3];
+  uint32_t sh_degree;
+} cgs_compositor;
+
+/* The scalar arguments of GpuPipelineState::execute_frame_gpu
+ * (render/gpu_state.rs:613-626), plus this library's output options. */
+typedef struct cgs_frame_params {
+  float strain_split_threshold; /* <= 0 disables strain splitting */
+  float mip_filter_3d_var;      /* <= 0 disables the 3D Mip filter */
+  float min_opacity;            /* reference default 1/255 (math/projection.rs:348) */
+  float min_radius_px;          /* reference default 0.5 (math/projection.rs:351) */
+  int32_t profile_stages;       /* 1: time each stage with CUDA events */
+  int32_t force_stage3;         /* 1: never reuse the cached Stage 3 lists */
+  int32_t write_f32;            /* 1: also write an unquantised RGBA f32 frame */
+  int32_t radix_bits;           /* 0 = autotuned/default (8), else 4 or 8 */
+} cgs_frame_params;
+
+/* GpuStageTimings (render/gpu_state.rs:513-534). */
+typedef struct cgs_stage_timings {
+  double stage1_deform_ms;
+  double stage2_project_ms;
+  double stage3_bin_sort_ms;
+  double stage4_composite_ms;
+  int32_t stage1_skipped;
+  int32_t stage3_cached;
+  int32_t used_hardware_timestamps;
+  int32_t used_64bit_keys;
+  uint64_t active_gaussians;
+  uint64_t surviving_gaussians;
+  uint64_t total_tile_entries;
+} cgs_stage_timings;
+
+typedef struct cgs_ctx cgs_ctx;
+
+/* ---- context (replaces GpuCompute::acquire, render/gpu.rs:70-113) ---- */
+
+/* Creates a context on `device`. `stream` is a cudaStream_t to run on, or
+ * NULL for a context-owned non-blocking stream. */
+int cgs_ctx_create(int device, void* stream, cgs_ctx** out_ctx);
+int cgs_ctx_destroy(cgs_ctx* ctx);
+const char* cgs_last_error(const cgs_ctx* ctx);
+/* Blocks until all work queued on the context's stream has finished. */
+int cgs_ctx_synchronize(cgs_ctx* ctx);
+/* Bytes of device memory the context currently holds. */
+int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out_bytes);
+/* Library version string. */
+const char* cgs_version(void);
+
+/* ---- scene residency (GpuSceneState, render/gpu_state.rs:95-343) ---- */
+
+/* Uploads the rest scene: pos [n*3], cov [n*6] (xx,xy,xz,yy,yz,zz),
+ * opa [n] (activated), sh [n*48] as f32 or f16 (uint16 bits) per sh_format,
+ * channel-major (DC rgb, R rest 15, G rest 15, B rest 15; sh.rs:56-61).
+ * Re-uploading invalidates the deformed scene and the Stage 3 cache. */
+int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* cov,
+                     const float* opa, const void* sh, int32_t sh_format);
+
+/* Uploads flattened tet-cage topology for all cages (gpu_state.rs:248-298):
+ * elems [num_tets*4] global vertex indices, inv_dm [num_tets*9] column-major
+ * D_m^-1, bind_tet [n] global tet index or 0xFFFFFFFF when unbound,
+ * bind_w [n*4] barycentric weights. num_tets == 0 removes all cages. */
+int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
+                         const float* inv_dm, uint32_t num_verts, const uint32_t* bind_tet,
+                         const float* bind_w);
+
+/* Updates the current cage vertex positions [num_verts*3] (gpu_state.rs:316-335).
+ * A change marks the deformed scene dirty; an identical upload does not. */
+int cgs_cage_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_verts);
+
+/* Binds the resident rest scene to a tet cage on the GPU with the reference's
+ * rule (first tet with barycentric violation <= 1e-4, else the least-violating
+ * tet; TetMesh::bind_point, deformation/mod.rs:267-310). When use_bounds is
+ * nonzero, points outside [bmin,bmax] or with best violation > 0.15 are
+ * unbound (0xFFFFFFFF). Writes bind_tet [n] / bind_w [n*4] to host arrays. */
+int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const float* inv_dm,
+                  uint32_t num_verts, const float* rest_verts, int32_t use_bounds,
+                  const float* bmin, const float* bmax, uint32_t* bind_tet, float* bind_w);
+
+/* ---- frame (GpuPipelineState, render/gpu_state.rs:538-1243) ---- */
+
+/* Runs Stages 1-4 on the resident scene (execute_frame_gpu,
+ * gpu_state.rs:613-626). Stage 1 is skipped when cages and deform params are
+ * unchanged; Stage 3 is reused when its cache key (gpu_state.rs:454-500) is
+ * unchanged and force_stage3 is 0. `timings` may be NULL. */
+int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
+                      const cgs_frame_params* params, cgs_stage_timings* timings);
+
+/* Copies the last frame's RGBA8 pixels into a tight [h][w][4] host buffer
+ * (readback_framebuffer_rgba8, gpu_state.rs:1296-1328). */
+int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height);
+/* Copies the last frame's unquantised RGBA f32 pixels [h][w][4] (written when
+ * params.write_f32 was set; render/kernels/compositor.rs f32 output mode). */
+int cgs_readback_rgba_f32(cgs_ctx* ctx, float* dst, uint32_t width, uint32_t height);
+/* Device pointer and row pitch (in u32 pixels) of the padded RGBA8 frame
+ * (rows padded to 64 pixels, padded_rgba8_row_u32 gpu_state.rs:25). */
+int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px);
+
+/* Per-kernel device time, launches and algorithmic traffic accumulated over
+ * the frames run with params.profile_stages set since the last reset (CUDA
+ * events around every launch; profiling adds no host synchronisation to a
+ * frame unless the caller also asks for that frame's cgs_stage_timings).
+ * alg_bytes is the HBM traffic each kernel must move at minimum (inputs read
+ * once, outputs written once), the numerator of its roofline fraction. No
+ * reference counterpart: it refines GpuStageTimings (gpu_state.rs:513-534)
+ * to kernel granularity. */
+#define CGS_K_CLEAR 0
+#define CGS_K_TET_TRANSFORMS 1
+#define CGS_K_DEFORM 2
+#define CGS_K_PROJECT 3
+#define CGS_K_COUNT_SCAN 4
+#define CGS_K_EMIT 5
+#define CGS_K_RADIX_SORT 6
+#define CGS_K_TILE_RANGES 7
+#define CGS_K_COMPOSITE 8
+#define CGS_KERNEL_COUNT 9
+typedef struct cgs_kernel_profile {
+  double ms[CGS_KERNEL_COUNT];
+  uint64_t alg_bytes[CGS_KERNEL_COUNT];
+  uint32_t launches[CGS_KERNEL_COUNT];
+} cgs_kernel_profile;
+int cgs_kernel_profile_read(cgs_ctx* ctx, cgs_kernel_profile* out);
+int cgs_kernel_profile_reset(cgs_ctx* ctx);
+const char* cgs_kernel_name(int32_t id);
+
+/* Drops cached Stage 3 lists (invalidate_stage3, gpu_state.rs:570-573). */
+int cgs_invalidate_stage3(cgs_ctx* ctx);
+/* Drops scene, cages and caches (invalidate, gpu_state.rs:565-568). */
+int cgs_invalidate(cgs_ctx* ctx);
+
+/* Intermediate buffers of the last frame, for stage-isolated parity checks
+ * (the reference's tests read the same buffers, tests/gpu_parity_tests.rs:665-900). */
+#define CGS_BUF_DEFORMED_POS 1   /* f32 [active*3] */
+#define CGS_BUF_DEFORMED_COV 2   /* f32 [active*6] */
+#define CGS_BUF_DEFORMED_OPA 3   /* f32 [active] */
+#define CGS_BUF_SPLIT_META 4     /* u32 [splits*2] (parent, tet) */
+#define CGS_BUF_SPLAT_ATTRS 5    /* f32 [active*10] mu_x,mu_y,a,b,c,alpha,r,g,b,tz */
+#define CGS_BUF_EXTENTS 6        /* u32 [active] ext_x | ext_y << 16, 0 = culled */
+#define CGS_BUF_TILE_OFFSETS 7   /* u32 [active] exclusive scan of tiles touched */
+#define CGS_BUF_SORTED_KEYS 8    /* u32 [entries] (32-bit keys) or u64 [entries] */
+#define CGS_BUF_SORTED_IDS 9     /* u32 [entries] */
+#define CGS_BUF_TILE_RANGES 10   /* u32 [tiles*2] */
+#define CGS_BUF_TET_JACOBIANS 11 /* f32 [tets*9] column-major */
+#define CGS_BUF_TET_ROTATIONS 12 /* f32 [tets*9] column-major */
+#define CGS_BUF_TET_STRETCH 13   /* f32 [tets] */
+/* Reads buffer `which` of the last frame into `dst` (capacity dst_bytes);
+ * *out_bytes receives the byte size of the valid contents. */
+int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_bytes,
+                          uint64_t* out_bytes);
+
+/* ---- stage primitives on device memory (render/kernels/scan.rs, radix_sort.rs) ---- */
+
+/* Exclusive scan of d_in [n] into d_out [n]; *total receives the sum
+ * (gpu_exclusive_scan_total, render/kernels/scan.rs:312-333). The reference
+ * caps n at 512^3 (scan.rs:264-268); this single-pass scan takes n < 2^32. */
+int cgs_scan_u32(cgs_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint64_t n,
+                 uint64_t* total);
+
+/* Stable LSD radix sort of (key, value) pairs on the low key_bits bits
+ * (gpu_radix_sort_u32_pairs, render/kernels/radix_sort.rs:292-368).
+ * d_keys/d_vals [n] are sorted in place; digit_bits is 4 or 8 (0 = 8). */
+int cgs_sort_pairs_u32(cgs_ctx* ctx, uint32_t* d_keys, uint32_t* d_vals, uint64_t n,
+                       uint32_t key_bits, int32_t digit_bits);
+
+/* Stable sort of (tile, depth, id) triples by (tile, depth) for the 64-bit
+ * key path (gpu_radix_sort_u64_pairs, radix_sort.rs:377-477): d_tiles, d_depths
+ * and d_ids [n] are permuted in place; tile_bits bounds the tile ids. */
+int cgs_sort_pairs_u64(cgs_ctx* ctx, uint32_t* d_tiles, uint32_t* d_depths, uint32_t* d_ids,
+                       uint64_t n, uint32_t tile_bits, int32_t digit_bits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGS_H */

@@ -1,0 +1,360 @@
+"""CPU oracle for the splat pipeline -- test infrastructure only.
+
+ctypes bindings over ``oracle/_build/libcgs_oracle.so`` (built from
+``cgs_oracle.cpp`` by ``oracle/Makefile``). Only the tests, the smoke check and
+the CPU-baseline leg of ``bench.py`` use this module; the ``cindergs_b200``
+package never imports it.
+
+Two modes are exposed (see cgs_oracle.cpp): ``v2_*`` restates the reference's
+GPU kernel semantics (the parity gates) and ``ref_*`` restates its Rayon CPU
+backend (pinned by the reference's golden image hash).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libcgs_oracle.so")
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_c_u32 = ctypes.c_uint32
+_c_u64 = ctypes.c_uint64
+_c_f = ctypes.c_float
+_vp = ctypes.c_void_p
+
+
+def build() -> str:
+    """Compiles the oracle library (make -C oracle) and returns its path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_get_threads.restype = ctypes.c_int
+        L.orc_tet_transforms.argtypes = [_c_u32, _f32p, _u32p, _f32p, _f32p, _f32p, _f32p]
+        L.orc_deform_split.restype = _c_u32
+        L.orc_deform_split.argtypes = [_c_u32, _c_u32, _f32p, _u32p, _f32p, _f32p, _u32p, _f32p,
+                                       _f32p, _f32p, _f32p, _c_f, _c_f, _f32p, _f32p, _f32p, _u32p]
+        L.orc_project_v2.restype = _c_u64
+        L.orc_project_v2.argtypes = [_c_u32, _c_u32, _f32p, _f32p, _f32p, _f32p, _vp, _vp, _c_u32,
+                                     _vp, _f32p, _f32p, _c_f, _c_f, _c_f, _c_u32, _c_u32, _f32p,
+                                     _u32p]
+        L.orc_count_tiles.restype = _c_u64
+        L.orc_count_tiles.argtypes = [_c_u32, _f32p, _u32p, _c_u32, _c_u32, _u32p]
+        L.orc_scan.restype = _c_u64
+        L.orc_scan.argtypes = [_c_u64, _u32p, _u32p]
+        L.orc_packed_key_bits.argtypes = [_c_u32, ctypes.POINTER(_c_u32), ctypes.POINTER(_c_u32)]
+        L.orc_emit_keys32.argtypes = [_c_u32, _f32p, _u32p, _u32p, _c_u32, _c_u32, _c_f, _c_u32,
+                                      _u32p, _u32p]
+        L.orc_emit_keys64.argtypes = [_c_u32, _f32p, _u32p, _u32p, _c_u32, _c_u32, _u32p, _u32p,
+                                      _u32p]
+        L.orc_sort_pairs32.argtypes = [_c_u64, _u32p, _u32p, _c_u32]
+        L.orc_sort_triples64.argtypes = [_c_u64, _u32p, _u32p, _u32p]
+        L.orc_tile_ranges.argtypes = [_c_u64, _u32p, _c_u32, _c_u32, _u32p]
+        L.orc_composite_v2.argtypes = [_c_u32, _c_u32, _f32p, _u32p, _u32p, _f32p, _vp, _vp]
+        L.orc_detmath.restype = _c_f
+        L.orc_detmath.argtypes = [ctypes.c_int, _c_f, _c_f]
+        L.orc_bind_points.argtypes = [_c_u32, _f32p, _c_u32, _f32p, _f32p, ctypes.c_int, _vp, _vp,
+                                      _u32p, _f32p]
+        L.orc_fibonacci_cluster.argtypes = [_c_u32, _c_f, _f32p, _f32p, _f32p, _f32p, _f32p]
+        L.orc_ref_project_scene.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _f32p, _i32p,
+                                            _f32p]
+        L.orc_ref_bin_and_sort.restype = _c_u64
+        L.orc_ref_bin_and_sort.argtypes = [_c_u32, _f32p, _f32p, _i32p, _c_u32, _c_u32, _vp, _vp,
+                                           _vp, _vp]
+        L.orc_ref_rasterize.argtypes = [_c_u32, _c_u32, _f32p, _f32p, _f32p, _f32p, _f32p, _u32p,
+                                        _u32p, _f32p, _f32p, _c_u32, _vp, _vp]
+        L.orc_pixel_hash.restype = _c_u64
+        L.orc_pixel_hash.argtypes = [_c_u64, _u8p]
+        L.orc_ref_render_scene.restype = _c_u64
+        L.orc_ref_render_scene.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _f32p, _c_u32,
+                                           _c_u32, _f32p, _f32p, _c_u32, _vp, _vp]
+        L.orc_ref_tet_transforms.argtypes = [_c_u32, _f32p, _u32p, _f32p, _f32p, _f32p, _f32p]
+        L.orc_ref_sh_rotate.argtypes = [_c_u32, _f32p, _f32p, _c_u32]
+        L.orc_ref_frame.restype = _c_u64
+        L.orc_ref_frame.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _c_u32, _vp, _vp, _vp, _vp,
+                                    _vp, _f32p, _c_u32, _c_u32, _f32p, _f32p, _c_u32, _c_f, _c_f,
+                                    _u8p, ctypes.POINTER(_c_u32)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def threads() -> int:
+    return int(lib().orc_get_threads())
+
+
+def detmath(which: str, x: float, y: float = 0.0) -> float:
+    code = {"log": 0, "exp": 1, "acos": 2, "cos": 3, "pow": 4}[which]
+    return float(lib().orc_detmath(code, x, y))
+
+
+# ------------------------------------------------------------------ v2 mode
+
+def v2_tet_transforms(verts, elems, inv_dm):
+    verts, elems, inv_dm = _f32(verts).ravel(), _u32(elems).ravel(), _f32(inv_dm).ravel()
+    T = elems.size // 4
+    J = np.zeros(T * 9, np.float32)
+    R = np.zeros(T * 9, np.float32)
+    S = np.zeros(T, np.float32)
+    lib().orc_tet_transforms(T, verts, elems, inv_dm, J, R, S)
+    return J, R, S
+
+
+def v2_deform_split(verts, elems, J, stretch, bind_tet, bind_w, pos, cov, opa, split_thr, mip):
+    n = int(np.asarray(opa).size)
+    T = int(np.asarray(elems).size // 4)
+    out_pos = np.zeros(2 * n * 3, np.float32)
+    out_cov = np.zeros(2 * n * 6, np.float32)
+    out_opa = np.zeros(2 * n, np.float32)
+    meta = np.zeros(2 * n, np.uint32)
+    k = lib().orc_deform_split(n, T, _f32(verts).ravel(), _u32(elems).ravel(), _f32(J).ravel(),
+                               _f32(stretch).ravel(), _u32(bind_tet).ravel(),
+                               _f32(bind_w).ravel(), _f32(pos).ravel(), _f32(cov).ravel(),
+                               _f32(opa).ravel(), split_thr, mip, out_pos, out_cov, out_opa, meta)
+    m = n + int(k)
+    return out_pos[: 3 * m], out_cov[: 6 * m], out_opa[:m], meta[: 2 * int(k)], int(k)
+
+
+def v2_project(pos, cov, opa, sh, cam24, cam_pos, mip, min_opa, min_rad, sh_degree, n_rest=None,
+               bind_tet=None, tet_R=None, num_tets=0, split_meta=None):
+    pos, cov, opa, sh = _f32(pos).ravel(), _f32(cov).ravel(), _f32(opa).ravel(), _f32(sh).ravel()
+    active = opa.size
+    n_rest = active if n_rest is None else int(n_rest)
+    has_def = 1 if (bind_tet is not None and tet_R is not None) else 0
+    bt = None if bind_tet is None else _u32(bind_tet).ravel()
+    tr = None if tet_R is None else _f32(tet_R).ravel()
+    sm = None if split_meta is None else _u32(split_meta).ravel()
+    attrs = np.zeros(active * 10, np.float32)
+    ext = np.zeros(active, np.uint32)
+    surv = lib().orc_project_v2(active, n_rest, pos, cov, opa, sh, _ptr(bt), _ptr(tr),
+                                int(num_tets), _ptr(sm), _f32(cam24).ravel(),
+                                _f32(cam_pos).ravel(), mip, min_opa, min_rad, int(sh_degree),
+                                has_def, attrs, ext)
+    return attrs, ext, int(surv)
+
+
+def v2_count_tiles(attrs, ext, W, H):
+    ext = _u32(ext).ravel()
+    counts = np.zeros(ext.size, np.uint32)
+    total = lib().orc_count_tiles(ext.size, _f32(attrs).ravel(), ext, W, H, counts)
+    return counts, int(total)
+
+
+def scan(x):
+    x = _u32(x).ravel()
+    out = np.zeros_like(x)
+    total = lib().orc_scan(x.size, x, out)
+    return out, int(total)
+
+
+def packed_key_bits(total_tiles):
+    tb, db = _c_u32(), _c_u32()
+    lib().orc_packed_key_bits(int(total_tiles), ctypes.byref(tb), ctypes.byref(db))
+    return int(tb.value), int(db.value)
+
+
+def v2_emit_keys32(attrs, ext, offsets, total, W, H, near_plane, depth_bits):
+    keys = np.zeros(total, np.uint32)
+    ids = np.zeros(total, np.uint32)
+    ext = _u32(ext).ravel()
+    lib().orc_emit_keys32(ext.size, _f32(attrs).ravel(), ext, _u32(offsets).ravel(), W, H,
+                          near_plane, depth_bits, keys, ids)
+    return keys, ids
+
+
+def v2_emit_keys64(attrs, ext, offsets, total, W, H):
+    t = np.zeros(total, np.uint32)
+    d = np.zeros(total, np.uint32)
+    ids = np.zeros(total, np.uint32)
+    ext = _u32(ext).ravel()
+    lib().orc_emit_keys64(ext.size, _f32(attrs).ravel(), ext, _u32(offsets).ravel(), W, H, t, d,
+                          ids)
+    return t, d, ids
+
+
+def sort_pairs32(keys, vals, key_bits=32):
+    k, v = _u32(keys).copy(), _u32(vals).copy()
+    lib().orc_sort_pairs32(k.size, k, v, int(key_bits))
+    return k, v
+
+
+def sort_triples64(tiles, depths, ids):
+    t, d, i = _u32(tiles).copy(), _u32(depths).copy(), _u32(ids).copy()
+    lib().orc_sort_triples64(t.size, t, d, i)
+    return t, d, i
+
+
+def tile_ranges(sorted_words, shift, total_tiles):
+    s = _u32(sorted_words).ravel()
+    ranges = np.zeros(2 * total_tiles, np.uint32)
+    lib().orc_tile_ranges(s.size, s, int(shift), int(total_tiles), ranges)
+    return ranges
+
+
+def v2_composite(W, H, attrs, sorted_ids, ranges, bg):
+    rgba8 = np.zeros(W * H * 4, np.uint8)
+    f = np.zeros(W * H * 4, np.float32)
+    lib().orc_composite_v2(W, H, _f32(attrs).ravel(), _u32(sorted_ids).ravel(),
+                           _u32(ranges).ravel(), _f32(bg).ravel(), _ptr(rgba8), _ptr(f))
+    return rgba8.reshape(H, W, 4), f.reshape(H, W, 4)
+
+
+def v2_frame(scene, cam24, comp, *, mip=0.0, min_opa=1.0 / 255.0, min_rad=0.5, split_thr=0.0,
+             cage=None):
+    """Whole v2 frame on the CPU. ``scene`` = dict(pos, cov, opa, sh);
+    ``comp`` = dict(width, height, bg, cam_pos, sh_degree); ``cage`` =
+    dict(verts, elems, inv_dm, bind_tet, bind_w) or None. Returns a dict with
+    every intermediate (the same buffers the GPU frame exposes)."""
+    W, H = int(comp["width"]), int(comp["height"])
+    out = {}
+    n = int(np.asarray(scene["opa"]).size)
+    if cage is not None:
+        J, R, S = v2_tet_transforms(cage["verts"], cage["elems"], cage["inv_dm"])
+        pos, cov, opa, meta, k = v2_deform_split(cage["verts"], cage["elems"], J, S,
+                                                 cage["bind_tet"], cage["bind_w"], scene["pos"],
+                                                 scene["cov"], scene["opa"], split_thr, mip)
+        out.update(J=J, R=R, stretch=S, def_pos=pos, def_cov=cov, def_opa=opa, meta=meta,
+                   splits=k)
+        attrs, ext, surv = v2_project(pos, cov, opa, scene["sh"], cam24, comp["cam_pos"], 0.0,
+                                      min_opa, min_rad, comp["sh_degree"], n_rest=n,
+                                      bind_tet=cage["bind_tet"], tet_R=R,
+                                      num_tets=np.asarray(cage["elems"]).size // 4,
+                                      split_meta=meta)
+    else:
+        attrs, ext, surv = v2_project(scene["pos"], scene["cov"], scene["opa"], scene["sh"],
+                                      cam24, comp["cam_pos"], mip, min_opa, min_rad,
+                                      comp["sh_degree"])
+    counts, total = v2_count_tiles(attrs, ext, W, H)
+    offsets, total2 = scan(counts)
+    assert total == total2
+    tiles = ((W + 15) // 16) * ((H + 15) // 16)
+    out.update(attrs=attrs, ext=ext, surviving=surv, counts=counts, offsets=offsets,
+               entries=total, total_tiles=tiles)
+    if tiles <= 65535:
+        tb, db = packed_key_bits(tiles)
+        keys, ids = v2_emit_keys32(attrs, ext, offsets, total, W, H, float(cam24[22]), db)
+        sk, si = sort_pairs32(keys, ids, min(tb + db, 32))
+        ranges = tile_ranges(sk, db, tiles)
+        out.update(keys=keys, sorted_keys=sk, sorted_ids=si, tile_bits=tb, depth_bits=db)
+    else:
+        t, d, ids = v2_emit_keys64(attrs, ext, offsets, total, W, H)
+        st, sd, si = sort_triples64(t, d, ids)
+        ranges = tile_ranges(st, 0, tiles)
+        out.update(sorted_tiles=st, sorted_depths=sd, sorted_ids=si)
+    rgba8, f = v2_composite(W, H, attrs, out["sorted_ids"], ranges, comp["bg"])
+    out.update(ranges=ranges, rgba8=rgba8, rgba_f32=f)
+    return out
+
+
+def bind_points(points, rest_verts, elems, inv_dm, bounds=None):
+    """TetMesh::bind_point for every point; returns (tet [N], weights [N,4])."""
+    pts = _f32(points).reshape(-1, 3)
+    elems = _u32(elems).reshape(-1, 4)
+    rv = _f32(rest_verts).reshape(-1, 3)
+    x0 = np.ascontiguousarray(rv[elems[:, 0].astype(np.int64)], np.float32)
+    n = pts.shape[0]
+    tet = np.zeros(n, np.uint32)
+    w = np.zeros((n, 4), np.float32)
+    if bounds is not None:
+        bmin, bmax = _f32(bounds[0]), _f32(bounds[1])
+        lib().orc_bind_points(n, pts.ravel(), elems.shape[0], x0.ravel(), _f32(inv_dm).ravel(), 1,
+                              _ptr(bmin), _ptr(bmax), tet, w)
+    else:
+        lib().orc_bind_points(n, pts.ravel(), elems.shape[0], x0.ravel(), _f32(inv_dm).ravel(), 0,
+                              None, None, tet, w)
+    return tet, w
+
+
+# ------------------------------------------------------------------ ref mode
+
+def fibonacci_cluster(count, radius, center):
+    pos = np.zeros(count * 3, np.float32)
+    cov = np.zeros(count * 6, np.float32)
+    opa = np.zeros(count, np.float32)
+    sh = np.zeros(count * 48, np.float32)
+    lib().orc_fibonacci_cluster(count, radius, _f32(center), pos, cov, opa, sh)
+    return dict(pos=pos, cov=cov, opa=opa, sh=sh)
+
+
+def ref_render_scene(scene, cam24, W, H, bg, cam_pos, sh_degree):
+    n = int(np.asarray(scene["opa"]).size)
+    rgba8 = np.zeros(W * H * 4, np.uint8)
+    f = np.zeros(W * H * 4, np.float32)
+    entries = lib().orc_ref_render_scene(n, _f32(scene["pos"]).ravel(), _f32(scene["cov"]).ravel(),
+                                         _f32(scene["opa"]).ravel(), _f32(scene["sh"]).ravel(),
+                                         _f32(cam24).ravel(), W, H, _f32(bg), _f32(cam_pos),
+                                         int(sh_degree), _ptr(rgba8), _ptr(f))
+    return rgba8.reshape(H, W, 4), f.reshape(H, W, 4), int(entries)
+
+
+def pixel_hash(rgba8) -> int:
+    b = np.ascontiguousarray(rgba8, dtype=np.uint8).ravel()
+    return int(lib().orc_pixel_hash(b.size, b))
+
+
+def ref_tet_transforms(verts, elems, inv_dm):
+    """Reference CPU tet transforms (glam polar, f64 Jacobi stretch)."""
+    elems = _u32(elems).ravel()
+    T = elems.size // 4
+    J = np.zeros(T * 9, np.float32)
+    R = np.zeros(T * 9, np.float32)
+    S = np.zeros(T, np.float32)
+    lib().orc_ref_tet_transforms(T, _f32(verts).ravel(), elems, _f32(inv_dm).ravel(), J, R, S)
+    return J, R, S
+
+
+def ref_sh_rotate(sh, R9, degree):
+    out = _f32(sh).copy().ravel()
+    lib().orc_ref_sh_rotate(out.size // 48, out, _f32(R9).ravel(), int(degree))
+    return out
+
+
+def ref_frame(scene, cam24, W, H, bg, cam_pos, sh_degree, cage=None, split_thr=0.0, mip=0.0):
+    """execute_cpu_reference_with_options restated (ref CPU mode). Returns
+    (rgba8 [H,W,4], tile entries, split children)."""
+    n = int(np.asarray(scene["opa"]).size)
+    rgba8 = np.zeros(W * H * 4, np.uint8)
+    splits = _c_u32()
+    if cage is not None:
+        verts, elems = _f32(cage["verts"]).ravel(), _u32(cage["elems"]).ravel()
+        inv, bt, bw = _f32(cage["inv_dm"]).ravel(), _u32(cage["bind_tet"]).ravel(), \
+            _f32(cage["bind_w"]).ravel()
+        T = elems.size // 4
+        args = (T, _ptr(verts), _ptr(elems), _ptr(inv), _ptr(bt), _ptr(bw))
+    else:
+        args = (0, None, None, None, None, None)
+    e = lib().orc_ref_frame(n, _f32(scene["pos"]).ravel(), _f32(scene["cov"]).ravel(),
+                            _f32(scene["opa"]).ravel(), _f32(scene["sh"]).ravel(), *args,
+                            _f32(cam24).ravel(), W, H, _f32(bg), _f32(cam_pos), int(sh_degree),
+                            split_thr, mip, rgba8, ctypes.byref(splits))
+    return rgba8.reshape(H, W, 4), int(e), int(splits.value)

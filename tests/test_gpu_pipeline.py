@@ -1,0 +1,130 @@
+"""GPU parity of the four-stage frame against the oracle (v2 semantics).
+
+Stage 2 attributes and every Stage 3 integer (extents, scan offsets, sorted
+keys and ids, tile ranges) must be bit-exact; Stage 4 RGB within 2e-3 absolute
+in f32 and within one RGBA8 step (the reference's GPU tests allow a mean RGB
+difference of 5e-3, tests/gpu_parity_tests.rs:231-290).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cindergs_b200 import (CameraUniforms, CompositorUniforms, GaussianSceneSoa, random_scene)
+from helpers import (assert_stage23_exact, compositor, config0_camera, gpu_buffers, oracle_frame,
+                     parity_camera, varied_scene)
+
+pytestmark = pytest.mark.gpu
+RGB_TOL = 2e-3
+
+
+def run_both(st, scene, cam, comp, **kw):
+    t = st.execute_frame_gpu(scene, None, cam, comp, kw.get("split", 0.0), kw.get("mip", 0.0),
+                             kw.get("min_opa", 1.0 / 255.0), kw.get("min_rad", 0.5),
+                             profile_stages=True, force_stage3=True, write_f32=True,
+                             radix_bits=kw.get("radix_bits", 0))
+    g = gpu_buffers(st, key64=t.used_64bit_keys)
+    g["rgba8"] = st.readback_framebuffer_rgba8(comp.screen_width, comp.screen_height)
+    g["f32"] = st.readback_framebuffer_f32(comp.screen_width, comp.screen_height)
+    o = oracle_frame(scene, cam, comp, mip=kw.get("mip", 0.0), min_opa=kw.get("min_opa", 1 / 255.0),
+                     min_rad=kw.get("min_rad", 0.5))
+    return t, g, o
+
+
+def check_image(g, o):
+    d = np.abs(g["f32"] - o["rgba_f32"])
+    assert d.max() <= RGB_TOL, f"max |rgba| diff {d.max()}"
+    d8 = np.abs(g["rgba8"].astype(np.int32) - o["rgba8"].astype(np.int32))
+    assert d8.max() <= 1, f"max rgba8 diff {d8.max()}"
+
+
+def test_varied_scene_96px(gpu_state):
+    scene = varied_scene()
+    cam = parity_camera(96, 96)
+    comp = compositor(96, 96, cam, deg=3)
+    t, g, o = run_both(gpu_state, scene, cam, comp)
+    assert t.total_tile_entries == o["entries"] > 0
+    assert t.surviving_gaussians == o["surviving"]
+    assert_stage23_exact(g, o)
+    check_image(g, o)
+
+
+@pytest.mark.parametrize("radix_bits", [8, 4])
+def test_config0_scene_100k_720p(gpu_state, radix_bits):
+    scene = random_scene(100_000, seed=0)
+    cam = config0_camera(1280, 720)
+    comp = compositor(1280, 720, cam, deg=3, bg=(0.0, 0.0, 0.0, 1.0))
+    t, g, o = run_both(gpu_state, scene, cam, comp, radix_bits=radix_bits)
+    assert t.total_tile_entries == o["entries"] > 100_000
+    assert_stage23_exact(g, o)
+    check_image(g, o)
+
+
+def test_mip_and_culling_thresholds(gpu_state):
+    scene = varied_scene()
+    cam = parity_camera(96, 96)
+    comp = compositor(96, 96, cam, deg=2)
+    t, g, o = run_both(gpu_state, scene, cam, comp, mip=0.001, min_opa=0.01)
+    assert t.surviving_gaussians == o["surviving"]
+    assert_stage23_exact(g, o)
+    check_image(g, o)
+
+
+@pytest.mark.parametrize("wh", [(19, 19), (1, 1), (17, 300)])
+def test_ragged_viewports(gpu_state, wh):
+    w, h = wh
+    scene = random_scene(20_000, seed=3)
+    cam = config0_camera(w, h)
+    comp = compositor(w, h, cam, deg=1)
+    t, g, o = run_both(gpu_state, scene, cam, comp)
+    assert_stage23_exact(g, o)
+    check_image(g, o)
+
+
+def test_empty_scene(gpu_state):
+    scene = GaussianSceneSoa(np.zeros((0, 3), np.float32), np.zeros((0, 6), np.float32),
+                             np.zeros(0, np.float32), np.zeros((0, 48), np.float32))
+    cam = config0_camera(64, 48)
+    comp = compositor(64, 48, cam, bg=(0.1, 0.2, 0.3, 1.0))
+    t = gpu_state.execute_frame_gpu(scene, None, cam, comp, force_stage3=True, write_f32=True)
+    assert t.total_tile_entries == 0
+    img = gpu_state.readback_framebuffer_f32(64, 48)
+    np.testing.assert_allclose(img.reshape(-1, 4), np.tile([0.1, 0.2, 0.3, 1.0], (64 * 48, 1)),
+                               atol=1e-7)
+
+
+def test_all_culled_behind_camera(gpu_state):
+    scene = random_scene(1000, seed=1)
+    scene.positions[:, 2] = 10.0  # behind the camera at z=4 looking down -z
+    cam = config0_camera(128, 64)
+    comp = compositor(128, 64, cam)
+    t, g, o = run_both(gpu_state, scene, cam, comp)
+    assert t.total_tile_entries == 0 and t.surviving_gaussians == 0
+    check_image(g, o)
+
+
+def test_64bit_key_path_8k(gpu_state):
+    """More than 65,535 tiles selects (tile, raw depth) keys (gpu_state.rs:1064)."""
+    scene = random_scene(50_000, seed=5)
+    cam = config0_camera(7680, 4320)
+    comp = compositor(7680, 4320, cam, deg=3)
+    t, g, o = run_both(gpu_state, scene, cam, comp)
+    assert t.used_64bit_keys
+    assert_stage23_exact(g, o, key64=True)
+    check_image(g, o)
+
+
+def test_stage3_cache_and_repeatability(gpu_state):
+    scene = random_scene(30_000, seed=7)
+    cam = config0_camera(320, 240)
+    comp = compositor(320, 240, cam)
+    st = gpu_state
+    t1 = st.execute_frame_gpu(scene, None, cam, comp, force_stage3=True)
+    a = st.readback_framebuffer_rgba8(320, 240)
+    t2 = st.execute_frame_gpu(scene, None, cam, comp)
+    b = st.readback_framebuffer_rgba8(320, 240)
+    assert not t1.stage3_cached and t2.stage3_cached
+    np.testing.assert_array_equal(a, b)
+    cam2 = CameraUniforms.from_look_at((0.4, 0.2, 4.0), (0, 0, 0), (0, 1, 0), np.deg2rad(60), 320,
+                                       240, 0.2)
+    t3 = st.execute_frame_gpu(scene, None, cam2, comp)
+    assert not t3.stage3_cached
