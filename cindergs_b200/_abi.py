@@ -120,6 +120,7 @@ SIGNATURES = {
     "cgs_scan_u32": (_int, [_vp, _vp, _vp, _u64, ctypes.POINTER(_u64)]),
     "cgs_sort_pairs_u32": (_int, [_vp, _vp, _vp, _u64, _u32, _i32]),
     "cgs_sort_pairs_u64": (_int, [_vp, _vp, _vp, _vp, _u64, _u32, _i32]),
+    "cgs_sort_pairs_u32_noalloc": (_int, [_vp, _vp, _u64, _u32, _i32, _vp]),
 }
 
 

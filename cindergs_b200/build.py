@@ -30,6 +30,7 @@ UNITS = [
     ("radix_sort.cu", []),
     ("stage4_composite.cu", []),
     ("pipeline.cu", []),
+    ("noalloc.cu", []),
 ]
 HEADERS = ["common.cuh", "detmath.h", "kernels.h"]
 

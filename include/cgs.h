@@ -227,6 +227,26 @@ int cgs_sort_pairs_u32(cgs_ctx* ctx, uint32_t* d_keys, uint32_t* d_vals, uint64_
 int cgs_sort_pairs_u64(cgs_ctx* ctx, uint32_t* d_tiles, uint32_t* d_depths, uint32_t* d_ids,
                        uint64_t n, uint32_t tile_bits, int32_t digit_bits);
 
+/* ---- allocation-free variant ----------------------------------------------- */
+
+/* No counterpart in the reference. The same stable LSD radix sort as
+ * cgs_sort_pairs_u32, for callers that cannot let a library call cudaMalloc:
+ * a host engine that owns all device memory through its own allocator or
+ * budget, or a real-time loop where an allocation could synchronise the device
+ * mid-frame. It needs no context and allocates nothing: its scratch is one
+ * fixed array of 9 MiB + 8.25 KiB inside the library image, which every GPU
+ * that loads the library holds until the process exits.
+ * Sorts d_keys/d_vals [n] (device memory of the current device) in place on
+ * `stream` (a cudaStream_t, NULL for the legacy default stream) and returns
+ * once the sort has finished. n above CGS_NOALLOC_SORT_MAX_PAIRS returns
+ * CGS_E_CAPACITY. All calls share the one scratch array: calls that overlap on
+ * the GPU race and must be serialised by the caller. The first call on a
+ * device looks up the array's device address; make that first call before
+ * any stream capture. */
+#define CGS_NOALLOC_SORT_MAX_PAIRS 1048576
+int cgs_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint64_t n,
+                               uint32_t key_bits, int32_t digit_bits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
