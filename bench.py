@@ -200,6 +200,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     from cindergs_b200 import GpuPipelineState
+    from cindergs_b200.replicas import max_over_ranks
 
     wl = workload(args)
     stream = torch.cuda.Stream(device=local)
@@ -242,12 +243,8 @@ def run_ours(args):
             render(profile=True, timings=False)
         end.record(stream)
         barrier()
-    ms = start.elapsed_time(end)
+    ms = max_over_ranks(start.elapsed_time(end), device=f"cuda:{local}")
     kp = st.kernel_profile()
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
     value = world * args.steps / (ms / 1000.0)
 
     # ---- e2e: public API with host buffers, copies inside the timed region
@@ -276,11 +273,8 @@ def run_ours(args):
                                              args.width, args.height), "cgs_readback_rgba8")
     e2e_end.record(stream)
     barrier()
-    e2e_ms = max(e2e_start.elapsed_time(e2e_end), (time.perf_counter() - t0) * 1000.0)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(max(e2e_start.elapsed_time(e2e_end),
+                                (time.perf_counter() - t0) * 1000.0), device=f"cuda:{local}")
     e2e_value = world * args.steps / (e2e_ms / 1000.0)
 
     if rank == 0:

@@ -83,6 +83,10 @@ def lib():
         L.orc_ref_render_scene.restype = _c_u64
         L.orc_ref_render_scene.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _f32p, _c_u32,
                                            _c_u32, _f32p, _f32p, _c_u32, _vp, _vp]
+        L.orc_ellipse_tile.restype = ctypes.c_int
+        L.orc_ellipse_tile.argtypes = [_c_f] * 6 + [_c_u32] * 4
+        L.orc_conic_extents.restype = ctypes.c_int
+        L.orc_conic_extents.argtypes = [_c_f] * 4 + [_f32p, _i32p]
         L.orc_ref_tet_transforms.argtypes = [_c_u32, _f32p, _u32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_ref_sh_rotate.argtypes = [_c_u32, _f32p, _f32p, _c_u32]
         L.orc_ref_frame.restype = _c_u64
@@ -358,3 +362,55 @@ def ref_frame(scene, cam24, W, H, bg, cam_pos, sh_degree, cage=None, split_thr=0
                             _f32(cam24).ravel(), W, H, _f32(bg), _f32(cam_pos), int(sh_degree),
                             split_thr, mip, rgba8, ctypes.byref(splits))
     return rgba8.reshape(H, W, 4), int(e), int(splits.value)
+
+
+def ellipse_tile(mu_x, mu_y, conic, alpha, tx, ty, W, H) -> bool:
+    return bool(lib().orc_ellipse_tile(mu_x, mu_y, conic[0], conic[1], conic[2], alpha, tx, ty,
+                                       W, H))
+
+
+def conic_extents(sxx, sxy, syy, alpha):
+    """compute_conic_and_extents; None when culled, else (conic[3], ext[2])."""
+    c = np.zeros(3, np.float32)
+    e = np.zeros(2, np.int32)
+    ok = lib().orc_conic_extents(sxx, sxy, syy, alpha, c, e)
+    return (c, e) if ok else None
+
+
+def ref_project(pos, cov, cam24):
+    """project_scene_cpu: (xy [N,2], depth [N], radius [N], conic [N,3])."""
+    pos, cov = _f32(pos).reshape(-1, 3), _f32(cov).reshape(-1, 6)
+    n = pos.shape[0]
+    xy = np.zeros(2 * n, np.float32)
+    d = np.zeros(n, np.float32)
+    r = np.zeros(n, np.int32)
+    c = np.zeros(3 * n, np.float32)
+    lib().orc_ref_project_scene(n, pos.ravel(), cov.ravel(), _f32(cam24), xy, d, r, c)
+    return xy.reshape(n, 2), d, r, c.reshape(n, 3)
+
+
+def ref_bin_and_sort(xy, depths, radii, W, H):
+    """bin_and_sort_gaussians_cpu: (tiles, depth_bits, ids, ranges [T,2])."""
+    xy = _f32(xy).ravel()
+    depths = _f32(depths).ravel()
+    radii = np.ascontiguousarray(radii, np.int32).ravel()
+    n = radii.size
+    total = lib().orc_ref_bin_and_sort(n, xy, depths, radii, W, H, None, None, None, None)
+    tiles = ((W + 15) // 16) * ((H + 15) // 16)
+    t = np.zeros(total, np.uint32)
+    d = np.zeros(total, np.uint32)
+    i = np.zeros(total, np.uint32)
+    rg = np.zeros(2 * tiles, np.uint32)
+    lib().orc_ref_bin_and_sort(n, xy, depths, radii, W, H, _ptr(t), _ptr(d), _ptr(i), _ptr(rg))
+    return t, d, i, rg.reshape(tiles, 2)
+
+
+def ref_rasterize(W, H, xy, conics, opa, sh, pos, sorted_ids, ranges, bg, cam_pos, sh_degree):
+    """rasterize_scene_cpu: (rgba8 [H,W,4], rgba_f32 [H,W,4])."""
+    rgba8 = np.zeros(W * H * 4, np.uint8)
+    f = np.zeros(W * H * 4, np.float32)
+    lib().orc_ref_rasterize(W, H, _f32(xy).ravel(), _f32(conics).ravel(), _f32(opa).ravel(),
+                            _f32(sh).ravel(), _f32(pos).ravel(), _u32(sorted_ids).ravel(),
+                            _u32(ranges).ravel(), _f32(bg), _f32(cam_pos), int(sh_degree),
+                            _ptr(rgba8), _ptr(f))
+    return rgba8.reshape(H, W, 4), f.reshape(H, W, 4)

@@ -1178,6 +1178,32 @@ void orc_composite_v2(uint32_t W, uint32_t H, const float* attrs, const uint32_t
   });
 }
 
+
+// Ellipse-vs-tile test (render/tiles/mod.rs:139-184; same formula as
+// binning.rs:37-83) for unit tests.
+int orc_ellipse_tile(float mu_x, float mu_y, float a, float b, float c, float alpha, uint32_t tx,
+                     uint32_t ty, uint32_t W, uint32_t H) {
+  return ellipse_tile(mu_x, mu_y, a, b, c, alpha, tx, ty, W, H) ? 1 : 0;
+}
+
+// compute_conic_and_extents (math/projection.rs:187-222); returns 0 when culled.
+int orc_conic_extents(float sxx_in, float sxy_in, float syy_in, float alpha, float* conic,
+                      int32_t* ext) {
+  const float s_xx = sxx_in + 0.3f, s_xy = sxy_in, s_yy = syy_in + 0.3f;
+  const float det = s_xx * s_yy - s_xy * s_xy;
+  if (det <= 1e-6f) return 0;
+  float sigma = 0.0f;
+  if (!(alpha <= 1.0f / 255.0f)) sigma = std::sqrt(clampf(2.0f * logf(255.0f * alpha), 0.0f, 8.0f));
+  if (sigma <= 0.0f) return 0;
+  const float inv_det = 1.0f / det;
+  conic[0] = s_yy * inv_det;
+  conic[1] = -s_xy * inv_det;
+  conic[2] = s_xx * inv_det;
+  ext[0] = (int32_t)clampf(std::ceil(sigma * std::sqrt(std::fmax(s_xx, 0.0f))), 1.0f, 1024.0f);
+  ext[1] = (int32_t)clampf(std::ceil(sigma * std::sqrt(std::fmax(s_yy, 0.0f))), 1.0f, 1024.0f);
+  return 1;
+}
+
 // Deterministic transcendental functions exposed for their unit tests.
 float orc_detmath(int which, float x, float y) {
   switch (which) {
