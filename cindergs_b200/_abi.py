@@ -81,8 +81,8 @@ class CgsStageTimings(ctypes.Structure):
                 ("total_tile_entries", _u64)]
 
 
-KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "count_scan", "emit",
-                "radix_sort", "tile_ranges", "composite"]
+KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "radix_sort",
+                "tile_ranges", "composite"]
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 

@@ -26,7 +26,7 @@ struct FrameCounters {
   uint32_t surviving;    // Stage 2 survivors
   uint32_t entries;      // Stage 3 tile entries (count_scan total)
   uint32_t status;       // kStatus* bits
-  uint32_t pad;
+  uint32_t fetched;      // splat records the compositor gathered
   uint32_t tile_ctr[16]; // dynamic tile counters for chained-scan kernels
 };
 
@@ -49,20 +49,23 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+// Look-back status words carry their flag and value in one naturally aligned
+// word, so a single-copy-atomic relaxed access at GPU scope is enough: no data
+// other than the word itself is published through it, and no fence is needed.
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
   uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
@@ -110,17 +113,17 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
                                                       uint32_t aggregate, uint32_t* status_word) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
-    if (lane == 0) st_release_u64(&status[0], (2ull << 32) | aggregate);
+    if (lane == 0) st_relaxed_u64(&status[0], (2ull << 32) | aggregate);
     return 0u;
   }
-  if (lane == 0) st_release_u64(&status[tile], (1ull << 32) | aggregate);
+  if (lane == 0) st_relaxed_u64(&status[tile], (1ull << 32) | aggregate);
   uint32_t exclusive = 0;
   long long pred = (long long)tile - 1;
   uint32_t spins = 0;
   bool timed_out = false;
   while (true) {
     long long mine = pred - lane;
-    unsigned long long st = mine >= 0 ? ld_acquire_u64(&status[mine]) : (2ull << 32);
+    unsigned long long st = mine >= 0 ? ld_relaxed_u64(&status[mine]) : (2ull << 32);
     while (__any_sync(0xffffffffu, (st >> 32) == 0ull)) {
       if (++spins > kSpinLimit) {
         timed_out = true;
@@ -128,7 +131,7 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
       }
       if ((st >> 32) == 0ull) {
         __nanosleep(64);
-        st = ld_acquire_u64(&status[mine]);
+        st = ld_relaxed_u64(&status[mine]);
       }
     }
     if (timed_out) break;
@@ -145,7 +148,7 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
     if (lane == 0) atomicOr(status_word, kStatusLookbackTimeout);
     exclusive = 0;
   }
-  if (lane == 0) st_release_u64(&status[tile], (2ull << 32) | (uint32_t)(exclusive + aggregate));
+  if (lane == 0) st_relaxed_u64(&status[tile], (2ull << 32) | (uint32_t)(exclusive + aggregate));
   return exclusive;
 }
 

@@ -101,11 +101,13 @@ struct BinArgs {
   uint32_t tile_bits;           // 64-bit: tile id bits
   uint32_t entry_cap;           // capacity of keys/depths/ids
 };
-cudaError_t launch_count_scan(const BinArgs& a, cudaStream_t s);
-cudaError_t launch_emit(const BinArgs& a, cudaStream_t s);
-// Per-tile [start, end) from sorted words: tile = word >> shift. ranges zeroed.
+// Counts, scans and emits in one launch (k_bin).
+cudaError_t launch_bin(const BinArgs& a, cudaStream_t s);
+// Per-tile [start, end) from sorted words: tile = word >> shift, over
+// min(*n_ptr, capacity) words. ranges zeroed.
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
-                               uint32_t total_tiles, uint32_t* ranges, cudaStream_t s);
+                               uint32_t capacity, uint32_t total_tiles, uint32_t* ranges,
+                               cudaStream_t s);
 // Generic exclusive scan of n u32 (chained scan); total -> *d_total.
 cudaError_t launch_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* d_total,
                             unsigned long long* status, uint32_t* tile_ctr, uint32_t* status_word,
@@ -123,7 +125,11 @@ struct SortArgs {
   uint32_t num_bits;     // bits to sort on (from first_bit)
   uint32_t radix_bits;   // 4 or 8
   uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
-  uint32_t* status;      // [passes][tiles][radix] zeroed
+  uint32_t* status;      // [passes][tiles][radix] zeroed (when status2 is null)
+  uint32_t* status2[2];  // optional: two [tiles][radix] look-back buffers used
+                         // alternately; each pass clears the one it does not
+                         // use for the next pass, so no per-frame memset is needed
+  int* parity;           // in/out: buffer index the next pass uses (with status2)
   uint32_t* tile_ctr;    // [passes] zeroed
   uint32_t* status_word;
   int src;               // index of the buffer holding the input

@@ -8,11 +8,16 @@
 // (deform generation, camera, viewport, filter parameters) is unchanged;
 // intermediate buffers grow by 1.5x and never shrink (gpu_pool.rs:43-49).
 //
-// One host synchronisation per frame that runs Stage 3: the 16-byte counter
-// block is read back after the fused count+scan kernel to size the key
-// buffers (the reference reads back three counters at the same point,
-// gpu_state.rs:1020-1035). Status bits set by bounded device waits are
-// checked at every synchronisation point and reported as CGS_E_TIMEOUT.
+// A frame is enqueued with no host synchronisation inside it (the reference
+// reads three counters back in the middle of every frame,
+// gpu_state.rs:1020-1035). The tile-entry count is only known on the device,
+// so the key buffers are sized from the counts of earlier frames with 30%
+// headroom; every frame copies its counters to pinned host memory and is
+// checked once its completion event has fired. A frame whose entries
+// overflowed the buffers is binned and composited again with grown buffers if
+// it is still the latest frame (so a readback never sees a truncated frame),
+// otherwise it is reported by the next synchronising call. Status bits set by
+// bounded device waits are reported as CGS_E_TIMEOUT.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -64,6 +69,39 @@ uint32_t fbits(float f) {
   return u;
 }
 
+// Everything Stages 3 and 4 of one frame need, kept so that a frame whose
+// tile entries overflowed the key buffers can be binned and composited again.
+struct FrameDesc {
+  uint32_t W = 0, H = 0, tiles_x = 0, tiles_y = 0, total_tiles = 0, pitch = 0;
+  uint32_t n = 0, max_n = 0;
+  bool split_possible = false, key64 = false, write_f32 = false;
+  uint32_t tile_bits = 0, depth_bits = 0, sort_bits = 0, radix_bits = 8, depth_base_bits = 0;
+  float bg[4] = {0, 0, 0, 1};
+};
+
+// Per-frame counters copied to pinned host memory at the end of the frame.
+struct HostCounters {
+  FrameCounters fc;
+  uint32_t split;
+  uint32_t pad[3];
+};
+
+constexpr int kRing = 4;          // frames that may be in flight unchecked
+constexpr int kMaxMarks = 24;     // profiled launches per frame
+
+// Scratch layout of a frame (one memset): counters | deform look-back |
+// binning look-back | radix histograms | radix tile counters.
+struct ScratchLayout {
+  size_t def, bin, hist, rtiles, bytes;
+  ScratchLayout(uint32_t n, uint32_t mn) {
+    def = 256;
+    bin = def + ((size_t)(n + 255) / 256) * 8 + 256;
+    hist = bin + ((size_t)(mn + 255) / 256) * 8 + 256;
+    rtiles = hist + 8 * 256 * 4;
+    bytes = rtiles + 256;
+  }
+};
+
 }  // namespace
 
 struct cgs_ctx {
@@ -87,61 +125,57 @@ struct cgs_ctx {
   uint32_t last_split_bits = 0xFFFFFFFFu, last_mip_bits = 0xFFFFFFFFu;
   // arena
   DevBuf tet_J, tet_R, tet_S, def_pos, def_cova, def_covb, split_meta, persist;
-  DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_status;
+  DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
-  FrameCounters* h_counters = nullptr;  // pinned: [0] mid-frame, [1] end of frame
-  uint32_t* h_split = nullptr;          // pinned
-  // Stage 3 cache and last-frame state
+  uint32_t entry_cap = 0;       // capacity of the key/id buffers (entries)
+  uint32_t radix_lb_tiles = 0;  // tiles the radix look-back buffers cover
+  uint32_t radix_lb_bits = 0;
+  int radix_parity = 0;
+  HostCounters* h_ring = nullptr;  // pinned [kRing]
+  uint32_t* h_misc = nullptr;      // pinned scratch for the primitives
+  // Stage 3 cache
   bool s3_valid = false;
   Stage3Key s3_key;
   uint32_t s3_entries = 0, s3_surviving = 0, s3_active = 0;
   int s3_key64 = 0, s3_src = 0;
   uint32_t s3_depth_bits = 0;
+  // last frame
+  FrameDesc last_desc;
   uint32_t last_w = 0, last_h = 0, last_pitch = 0, last_active = 0, last_tiles = 0;
-  uint32_t last_sort_passes = 0;
-  bool last_f32 = false, frame_done = false, end_copy_pending = false;
-  // Kernel-level profile (params.profile_stages): an event pair per launch,
-  // double-buffered by frame parity. A frame's events are folded into the
-  // accumulators once they are known to be complete (at the next frame's
-  // mid-frame synchronisation or when the profile is read), so profiling adds
-  // no host synchronisation of its own.
-  static constexpr int kMaxMarks = 32;
-  cudaEvent_t kev[2][2 * kMaxMarks] = {};
-  int kid[2][kMaxMarks] = {};
-  int kcount[2] = {0, 0};
-  bool kpending[2] = {false, false};
-  int kpar = 0;
+  bool last_f32 = false, frame_done = false;
+  int latest_slot = -1;
+  // in-flight frames
+  struct Pending {
+    bool used = false, stage3_ran = false, profiled = false, need_deform = false;
+    bool split_possible = false, key64 = false;
+    uint32_t n = 0, cap = 0, sort_passes = 0, total_tiles = 0, W = 0, H = 0;
+    bool write_f32 = false;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t kev[2 * kMaxMarks] = {};
+    int kid[kMaxMarks] = {};
+    int kcount = 0;
+  } ring[kRing];
+  int next_slot = 0;
+  int cur = -1;              // slot of the frame being enqueued
   bool kprof = false;
   cgs_kernel_profile kp_acc{};
+  int sticky = CGS_OK;       // error found while checking an older frame
+  std::string sticky_msg;
+
   void kbegin(int id) {
-    const int c = kcount[kpar];
-    if (!kprof || c >= kMaxMarks) return;
-    kid[kpar][c] = id;
-    cudaEventRecord(kev[kpar][2 * c], stream);
+    if (!kprof || cur < 0) return;
+    Pending& p = ring[cur];
+    if (p.kcount >= kMaxMarks) return;
+    p.kid[p.kcount] = id;
+    cudaEventRecord(p.kev[2 * p.kcount], stream);
   }
   void kend() {
-    const int c = kcount[kpar];
-    if (!kprof || c >= kMaxMarks) return;
-    cudaEventRecord(kev[kpar][2 * c + 1], stream);
-    kcount[kpar] = c + 1;
-  }
-  void kfold(int par, cgs_kernel_profile* frame) {
-    if (!kpending[par]) return;
-    for (int c = 0; c < kcount[par]; ++c) {
-      float ms = 0.0f;
-      cudaEventSynchronize(kev[par][2 * c + 1]);
-      cudaEventElapsedTime(&ms, kev[par][2 * c], kev[par][2 * c + 1]);
-      kp_acc.ms[kid[par][c]] += ms;
-      if (frame) frame->ms[kid[par][c]] += ms;
-    }
-    kpending[par] = false;
-    kcount[par] = 0;
-  }
-  void kcount_launch(int id, uint32_t launches, uint64_t bytes) {
-    if (!kprof) return;
-    kp_acc.launches[id] += launches;
-    kp_acc.alg_bytes[id] += bytes;
+    if (!kprof || cur < 0) return;
+    Pending& p = ring[cur];
+    if (p.kcount >= kMaxMarks) return;
+    cudaEventRecord(p.kev[2 * p.kcount + 1], stream);
+    ++p.kcount;
   }
 
   int fail(int code, const std::string& msg) {
@@ -170,15 +204,11 @@ struct cgs_ctx {
     b.cap = nb;
     return CGS_OK;
   }
-  // Checks the status bits of the last completed frame (after a sync).
-  int check_end_status() {
-    if (!end_copy_pending) return CGS_OK;
-    end_copy_pending = false;
-    const uint32_t st = h_counters[1].status;
-    if (st & (kStatusLookbackTimeout | kStatusBarrierTimeout))
-      return fail(CGS_E_TIMEOUT, "a bounded device-side wait gave up during the last frame");
-    if (st & kStatusCapacity) return fail(CGS_E_CAPACITY, "tile entries exceeded capacity");
-    return CGS_OK;
+  int take_sticky() {
+    if (sticky == CGS_OK) return CGS_OK;
+    const int s = sticky;
+    sticky = CGS_OK;
+    return fail(s, sticky_msg);
   }
 };
 
@@ -192,6 +222,261 @@ struct cgs_ctx {
     int r_ = (call);           \
     if (r_ != CGS_OK) return r_; \
   } while (0)
+
+namespace {
+
+// Key buffers and radix look-back buffers for `cap` entries.
+int ensure_entry_buffers(cgs_ctx* ctx, uint32_t cap, bool key64, uint32_t radix_bits) {
+  const size_t ecap = cap ? cap : 1;
+  for (int k = 0; k < 2; ++k) {
+    CGS_TRY(ctx->ensure(ctx->keys[k], ecap * 4, "sort keys"));
+    CGS_TRY(ctx->ensure(ctx->ids[k], ecap * 4, "sort values"));
+    if (key64) CGS_TRY(ctx->ensure(ctx->depths[k], ecap * 4, "sort depths"));
+  }
+  const uint32_t tiles = sort_tiles((uint32_t)ecap);
+  if (tiles != ctx->radix_lb_tiles || radix_bits != ctx->radix_lb_bits || !ctx->radix_lb[0].p) {
+    const size_t bytes = (size_t)tiles * (1u << radix_bits) * 4;
+    for (int k = 0; k < 2; ++k) {
+      CGS_TRY(ctx->ensure(ctx->radix_lb[k], bytes, "radix look-back"));
+      CGS_CUDA(cudaMemsetAsync(ctx->radix_lb[k].p, 0, bytes, ctx->stream), "clear look-back");
+    }
+    ctx->radix_lb_tiles = tiles;
+    ctx->radix_lb_bits = radix_bits;
+    ctx->radix_parity = 0;
+  }
+  return CGS_OK;
+}
+
+// Enqueues Stage 3 (binning, radix sort, tile ranges) for `d` with the
+// current key-buffer capacity. *result_src receives the buffer holding the
+// sorted lists; *passes the number of radix passes.
+int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int* result_src,
+                   uint32_t* passes) {
+  cudaStream_t s = ctx->stream;
+  char* sc = ctx->scratch.as<char>();
+  FrameCounters* fc = (FrameCounters*)sc;
+  uint32_t* d_split = ctx->persist.as<uint32_t>();
+  uint32_t* d_hist = (uint32_t*)(sc + L.hist);
+  uint32_t* rtiles = (uint32_t*)(sc + L.rtiles);
+  ctx->kbegin(CGS_K_CLEAR);
+  CGS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0, (size_t)d.total_tiles * 8, s), "clear ranges");
+  ctx->kend();
+  BinArgs b{};
+  b.recs = ctx->recs.as<SplatRec>();
+  b.split_count = d.split_possible ? d_split : nullptr;
+  b.n_rest = d.n;
+  b.max_n = d.max_n;
+  b.width = d.W;
+  b.height = d.H;
+  b.tiles_x = d.tiles_x;
+  b.tiles_y = d.tiles_y;
+  b.offsets = ctx->offsets.as<uint32_t>();
+  b.status = (unsigned long long*)(sc + L.bin);
+  b.fc = fc;
+  b.key64 = d.key64;
+  b.depth_base_bits = d.depth_base_bits;
+  b.depth_bits = d.depth_bits;
+  b.keys = ctx->keys[0].as<uint32_t>();
+  b.depths = d.key64 ? ctx->depths[0].as<uint32_t>() : nullptr;
+  b.ids = ctx->ids[0].as<uint32_t>();
+  b.hist = d_hist;
+  b.radix_bits = d.radix_bits;
+  b.sort_bits = d.sort_bits;
+  b.tile_bits = d.tile_bits;
+  b.entry_cap = ctx->entry_cap;
+  ctx->kbegin(CGS_K_BIN);
+  CGS_CUDA(launch_bin(b, s), "bin launch");
+  ctx->kend();
+  const uint32_t* n_ptr = &fc->entries;
+  const uint32_t passes_lo = d.key64 ? sort_passes(32, d.radix_bits) : sort_passes(d.sort_bits, d.radix_bits);
+  const uint32_t passes_hi = d.key64 ? sort_passes(d.tile_bits, d.radix_bits) : 0u;
+  *passes = passes_lo + passes_hi;
+  SortArgs sa{};
+  sa.n_ptr = n_ptr;
+  sa.capacity = ctx->entry_cap;
+  sa.first_bit = 0;
+  sa.radix_bits = d.radix_bits;
+  sa.status2[0] = ctx->radix_lb[0].as<uint32_t>();
+  sa.status2[1] = ctx->radix_lb[1].as<uint32_t>();
+  sa.parity = &ctx->radix_parity;
+  sa.tile_ctr = rtiles;
+  sa.status_word = &fc->status;
+  sa.hist = d_hist;
+  sa.src = 0;
+  ctx->kbegin(CGS_K_RADIX_SORT);
+  if (!d.key64) {
+    sa.keys[0] = ctx->keys[0].as<uint32_t>();
+    sa.keys[1] = ctx->keys[1].as<uint32_t>();
+    sa.vals[0] = ctx->ids[0].as<uint32_t>();
+    sa.vals[1] = ctx->ids[1].as<uint32_t>();
+    sa.num_bits = d.sort_bits;
+    CGS_CUDA(run_radix_sort(sa, result_src, s), "radix sort");
+  } else {
+    // (tile, depth) order: stable sort by depth, then stable sort by tile.
+    sa.keys[0] = ctx->depths[0].as<uint32_t>();
+    sa.keys[1] = ctx->depths[1].as<uint32_t>();
+    sa.vals[0] = ctx->ids[0].as<uint32_t>();
+    sa.vals[1] = ctx->ids[1].as<uint32_t>();
+    sa.vals2[0] = ctx->keys[0].as<uint32_t>();
+    sa.vals2[1] = ctx->keys[1].as<uint32_t>();
+    sa.num_bits = 32;
+    int src1 = 0;
+    CGS_CUDA(run_radix_sort(sa, &src1, s), "radix sort (depth)");
+    SortArgs sb = sa;
+    sb.keys[0] = ctx->keys[0].as<uint32_t>();
+    sb.keys[1] = ctx->keys[1].as<uint32_t>();
+    sb.vals2[0] = ctx->depths[0].as<uint32_t>();
+    sb.vals2[1] = ctx->depths[1].as<uint32_t>();
+    sb.num_bits = d.tile_bits;
+    sb.hist = d_hist + (size_t)passes_lo * (1u << d.radix_bits);
+    sb.tile_ctr = rtiles + passes_lo;
+    sb.src = src1;
+    CGS_CUDA(run_radix_sort(sb, result_src, s), "radix sort (tile)");
+  }
+  ctx->kend();
+  ctx->kbegin(CGS_K_TILE_RANGES);
+  CGS_CUDA(launch_tile_ranges(ctx->keys[*result_src].as<uint32_t>(), d.key64 ? 0u : d.depth_bits,
+                              n_ptr, ctx->entry_cap, d.total_tiles, ctx->ranges.as<uint32_t>(), s),
+           "ranges launch");
+  ctx->kend();
+  return CGS_OK;
+}
+
+int enqueue_stage4(cgs_ctx* ctx, const FrameDesc& d, int result_src) {
+  char* sc = ctx->scratch.as<char>();
+  CompositeArgs c{};
+  c.recs = ctx->recs.as<SplatRec>();
+  c.sorted_ids = ctx->ids[result_src].as<uint32_t>();
+  c.ranges = ctx->ranges.as<uint32_t>();
+  c.width = d.W;
+  c.height = d.H;
+  c.tiles_x = d.tiles_x;
+  c.tiles_y = d.tiles_y;
+  c.pitch_px = d.pitch;
+  std::memcpy(c.bg, d.bg, 16);
+  c.out_rgba8 = ctx->fb_rgba8.as<uint32_t>();
+  c.out_f32 = d.write_f32 ? ctx->fb_f32.as<float4>() : nullptr;
+  c.fc = (FrameCounters*)sc;
+  c.num_recs = d.max_n ? d.max_n : 1u;
+  c.num_entries = ctx->entry_cap;
+  ctx->kbegin(CGS_K_COMPOSITE);
+  CGS_CUDA(launch_composite(c, ctx->stream), "composite launch");
+  ctx->kend();
+  return CGS_OK;
+}
+
+// Re-runs Stages 3 and 4 of the latest frame after its entries overflowed the
+// key buffers (capacity already grown), synchronously.
+int rerun_stage34(cgs_ctx* ctx, uint32_t entries) {
+  const FrameDesc& d = ctx->last_desc;
+  ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)entries + entries / 4 + 4096, 0x3FFFFFFFull);
+  CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, d.key64, d.radix_bits));
+  const ScratchLayout L(d.n, d.max_n ? d.max_n : 1u);
+  char* sc = ctx->scratch.as<char>();
+  // keep fc->surviving (Stage 2's count); clear the Stage 3 words
+  CGS_CUDA(cudaMemsetAsync(sc + 4, 0, sizeof(FrameCounters) - 4, ctx->stream), "clear counters");
+  CGS_CUDA(cudaMemsetAsync(sc + L.bin, 0, L.bytes - L.bin, ctx->stream), "clear scratch");
+  const bool kp = ctx->kprof;
+  const int cur = ctx->cur;
+  ctx->kprof = false;
+  ctx->cur = -1;
+  int src = 0;
+  uint32_t passes = 0;
+  int rc = enqueue_stage3(ctx, d, L, &src, &passes);
+  if (rc == CGS_OK) rc = enqueue_stage4(ctx, d, src);
+  ctx->kprof = kp;
+  ctx->cur = cur;
+  CGS_TRY(rc);
+  CGS_CUDA(cudaMemcpyAsync(&ctx->h_ring[ctx->latest_slot].fc, sc, sizeof(FrameCounters),
+                           cudaMemcpyDeviceToHost, ctx->stream), "read counters");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "stage 3 re-run");
+  ctx->s3_src = src;
+  const FrameCounters& f = ctx->h_ring[ctx->latest_slot].fc;
+  if (f.status & kStatusCapacity) return ctx->fail(CGS_E_CAPACITY, "tile entries still exceed the grown buffers");
+  return CGS_OK;
+}
+
+// Checks frame slot `k` once it has finished: status bits, capacity, Stage 3
+// cache bookkeeping and the kernel profile. `block` waits for it.
+int check_slot(cgs_ctx* ctx, int k, bool block) {
+  cgs_ctx::Pending& p = ctx->ring[k];
+  if (!p.used) return CGS_OK;
+  if (block) {
+    CGS_CUDA(cudaEventSynchronize(p.done), "frame completion");
+  } else {
+    const cudaError_t q = cudaEventQuery(p.done);
+    if (q == cudaErrorNotReady) return CGS_OK;
+    if (q != cudaSuccess) return ctx->cuda_fail(q, "frame completion");
+  }
+  p.used = false;
+  const HostCounters& h = ctx->h_ring[k];
+  uint32_t entries = h.fc.entries;
+  uint32_t status = h.fc.status;
+  if (status & (kStatusLookbackTimeout | kStatusBarrierTimeout)) {
+    ctx->sticky = CGS_E_TIMEOUT;
+    ctx->sticky_msg = "a bounded device-side wait gave up during a frame";
+  }
+  if (p.stage3_ran && (status & kStatusCapacity || entries > p.cap)) {
+    if (k == ctx->latest_slot) {
+      CGS_TRY(rerun_stage34(ctx, entries));
+      entries = ctx->h_ring[k].fc.entries;
+    } else {
+      ctx->sticky = CGS_E_CAPACITY;
+      ctx->sticky_msg = "an earlier frame's tile entries exceeded the key buffers";
+      ctx->entry_cap = std::max(ctx->entry_cap,
+                                (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, 0x3FFFFFFFull));
+    }
+  } else if (p.stage3_ran && entries > ctx->entry_cap / 10 * 8) {
+    // keep 25% headroom for the next frames
+    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, 0x3FFFFFFFull);
+  }
+  if (k == ctx->latest_slot) {
+    if (p.stage3_ran) {
+      ctx->s3_entries = entries;
+      ctx->s3_surviving = h.fc.surviving;
+      ctx->s3_active = p.n + (p.split_possible ? h.split : 0u);
+    }
+    ctx->last_active = p.n + (p.split_possible ? h.split : 0u);
+  }
+  if (p.profiled) {
+    cgs_kernel_profile& kp = ctx->kp_acc;
+    for (int c = 0; c < p.kcount; ++c) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, p.kev[2 * c], p.kev[2 * c + 1]);
+      kp.ms[p.kid[c]] += ms;
+      kp.launches[p.kid[c]] += (p.kid[c] == CGS_K_RADIX_SORT) ? p.sort_passes : 1u;
+    }
+    const uint64_t A = p.n + (p.split_possible ? h.split : 0u);
+    const uint64_t S = h.fc.surviving, E = p.stage3_ran ? entries : 0, T = ctx->num_tets;
+    const uint64_t shb = ctx->sh_f16 ? 96 : 192;
+    if (p.need_deform) {
+      kp.alg_bytes[CGS_K_TET_TRANSFORMS] += T * (16 + 36 + 48 + 76);
+      kp.alg_bytes[CGS_K_DEFORM] += (uint64_t)p.n * 60 + A * 40 + (A - p.n) * 8;
+    }
+    kp.alg_bytes[CGS_K_PROJECT] += A * 40 + S * (shb + 48) + (A - S) * 16;
+    if (p.stage3_ran) {
+      kp.alg_bytes[CGS_K_BIN] += A * 36 + E * (p.key64 ? 12 : 8);
+      kp.alg_bytes[CGS_K_RADIX_SORT] += (uint64_t)p.sort_passes * E * (p.key64 ? 24 : 16);
+      kp.alg_bytes[CGS_K_TILE_RANGES] += E * 4 + (uint64_t)p.total_tiles * 8;
+    }
+    // The compositor stops a tile once every pixel has saturated, so its
+    // algorithmic traffic is the records it actually gathered (48 B + the
+    // 4-byte id each), the ranges and the framebuffer.
+    kp.alg_bytes[CGS_K_COMPOSITE] += (uint64_t)h.fc.fetched * 52 + (uint64_t)p.total_tiles * 8 +
+                                     (uint64_t)p.W * p.H * (p.write_f32 ? 20 : 4);
+  }
+  return CGS_OK;
+}
+
+int drain(cgs_ctx* ctx, bool block) {
+  for (int i = 1; i <= kRing; ++i) {
+    const int k = (ctx->next_slot + i - 1) % kRing;  // oldest first
+    CGS_TRY(check_slot(ctx, k, block));
+  }
+  return CGS_OK;
+}
+
+}  // namespace
 
 #pragma GCC visibility push(default)
 extern "C" {
@@ -216,18 +501,23 @@ int cgs_ctx_create(int device, void* stream, cgs_ctx** out_ctx) {
     }
     ctx->own_stream = true;
   }
-  if (cudaMallocHost(&ctx->h_counters, 2 * sizeof(FrameCounters)) != cudaSuccess ||
-      cudaMallocHost(&ctx->h_split, 16) != cudaSuccess) {
+  if (cudaMallocHost(&ctx->h_ring, kRing * sizeof(HostCounters)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_misc, 64) != cudaSuccess) {
     delete ctx;
     return CGS_E_OOM;
   }
-  std::memset(ctx->h_counters, 0, 2 * sizeof(FrameCounters));
-  for (auto& set : ctx->kev)
-    for (auto& e : set)
+  std::memset(ctx->h_ring, 0, kRing * sizeof(HostCounters));
+  for (auto& p : ctx->ring) {
+    if (cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming) != cudaSuccess) {
+      delete ctx;
+      return CGS_E_CUDA;
+    }
+    for (auto& e : p.kev)
       if (cudaEventCreate(&e) != cudaSuccess) {
         delete ctx;
         return CGS_E_CUDA;
       }
+  }
   // persistent words: [0] split count
   if (ctx->ensure(ctx->persist, 256, "persistent words") != CGS_OK ||
       cudaMemset(ctx->persist.p, 0, 256) != cudaSuccess) {
@@ -242,11 +532,13 @@ int cgs_ctx_destroy(cgs_ctx* ctx) {
   if (!ctx) return CGS_E_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (auto& set : ctx->kev)
-    for (auto& e : set)
+  for (auto& p : ctx->ring) {
+    if (p.done) cudaEventDestroy(p.done);
+    for (auto& e : p.kev)
       if (e) cudaEventDestroy(e);
-  if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
-  if (ctx->h_split) cudaFreeHost(ctx->h_split);
+  }
+  if (ctx->h_ring) cudaFreeHost(ctx->h_ring);
+  if (ctx->h_misc) cudaFreeHost(ctx->h_misc);
   cudaStream_t s = ctx->stream;
   bool own = ctx->own_stream;
   delete ctx;
@@ -258,8 +550,10 @@ const char* cgs_last_error(const cgs_ctx* ctx) { return ctx ? ctx->err.c_str() :
 
 int cgs_ctx_synchronize(cgs_ctx* ctx) {
   if (!ctx) return CGS_E_ARG;
+  cudaSetDevice(ctx->device);
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
-  return ctx->check_end_status();
+  CGS_TRY(drain(ctx, true));
+  return ctx->take_sticky();
 }
 
 int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out) {
@@ -270,8 +564,9 @@ int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out) {
                           &ctx->def_cova, &ctx->def_covb, &ctx->split_meta, &ctx->persist,
                           &ctx->recs, &ctx->offsets, &ctx->scratch, &ctx->ranges, &ctx->keys[0],
                           &ctx->keys[1], &ctx->ids[0], &ctx->ids[1], &ctx->depths[0],
-                          &ctx->depths[1], &ctx->radix_status, &ctx->fb_rgba8, &ctx->fb_f32,
-                          &ctx->prim[0], &ctx->prim[1], &ctx->prim[2], &ctx->prim[3]};
+                          &ctx->depths[1], &ctx->radix_lb[0], &ctx->radix_lb[1], &ctx->fb_rgba8,
+                          &ctx->fb_f32, &ctx->prim[0], &ctx->prim[1], &ctx->prim[2],
+                          &ctx->prim[3]};
   uint64_t t = 0;
   for (auto* b : bufs) t += b->cap;
   *out = t;
@@ -446,45 +741,53 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
   const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
   if (total_tiles64 > 0xFFFFFFFFull / 2) return ctx->fail(CGS_E_CAPACITY, "viewport too large");
-  const uint32_t total_tiles = (uint32_t)total_tiles64;
-  const uint32_t pitch = (W + 63) / 64 * 64;
+
+  // Take a ring slot; the frame that used it last is checked first.
+  const int slot = ctx->next_slot;
+  CGS_TRY(check_slot(ctx, slot, true));
+  CGS_TRY(drain(ctx, false));
+  ctx->next_slot = (slot + 1) % kRing;
+
+  FrameDesc d;
+  d.W = W;
+  d.H = H;
+  d.tiles_x = tiles_x;
+  d.tiles_y = tiles_y;
+  d.total_tiles = (uint32_t)total_tiles64;
+  d.pitch = (W + 63) / 64 * 64;
+  d.radix_bits = params->radix_bits ? (uint32_t)params->radix_bits : 8u;
+  d.write_f32 = params->write_f32 != 0;
+  std::memcpy(d.bg, comp->background, 16);
   if (W != ctx->last_w || H != ctx->last_h) ctx->s3_valid = false;
-  const uint32_t radix_bits = params->radix_bits ? (uint32_t)params->radix_bits : 8u;
   const bool prof = params->profile_stages != 0;
 
-  CGS_TRY(ctx->ensure(ctx->fb_rgba8, (size_t)pitch * H * 4, "framebuffer"));
-  if (params->write_f32) CGS_TRY(ctx->ensure(ctx->fb_f32, (size_t)W * H * 16, "f32 framebuffer"));
+  CGS_TRY(ctx->ensure(ctx->fb_rgba8, (size_t)d.pitch * H * 4, "framebuffer"));
+  if (d.write_f32) CGS_TRY(ctx->ensure(ctx->fb_f32, (size_t)W * H * 16, "f32 framebuffer"));
 
   const uint32_t n = ctx->n;
   const bool has_cages = ctx->has_cages;
   const uint32_t split_bits = fbits(params->strain_split_threshold), mip_bits = fbits(params->mip_filter_3d_var);
   const bool params_changed = split_bits != ctx->last_split_bits || mip_bits != ctx->last_mip_bits;
   const bool need_deform = has_cages && (!ctx->deformed_valid || params_changed);
-  const bool split_possible = has_cages && params->strain_split_threshold > 0.0f;
-  const uint32_t max_n = split_possible ? 2 * n : n;
-  const uint32_t mn = max_n ? max_n : 1u;
+  d.n = n;
+  d.split_possible = has_cages && params->strain_split_threshold > 0.0f;
+  d.max_n = d.split_possible ? 2 * n : n;
+  const uint32_t mn = d.max_n ? d.max_n : 1u;
+  d.key64 = d.total_tiles > 65535u;
+  d.tile_bits = d.total_tiles <= 1 ? 1u : 32u - (uint32_t)__builtin_clz(d.total_tiles - 1);
+  d.depth_bits = d.tile_bits >= 32 ? 0u : (32u - d.tile_bits < 28u ? 32u - d.tile_bits : 28u);
+  d.sort_bits = d.tile_bits + d.depth_bits > 32 ? 32 : d.tile_bits + d.depth_bits;
+  const float near_c = camera->near_plane > 1e-6f ? camera->near_plane : 1e-6f;
+  d.depth_base_bits = fbits(near_c) & 0x7F800000u;
 
-  // scratch: counters | deform status | count-scan status | histograms
-  const size_t def_tiles = (n + 255) / 256, cs_tiles = (mn + 255) / 256;
-  const size_t o_def = 256, o_cs = o_def + def_tiles * 8 + 256, o_hist = o_cs + cs_tiles * 8 + 256;
-  const size_t scratch_bytes = o_hist + 8 * 256 * 4;
-  CGS_TRY(ctx->ensure(ctx->scratch, scratch_bytes, "frame scratch"));
+  const ScratchLayout L(n, mn);
+  CGS_TRY(ctx->ensure(ctx->scratch, L.bytes, "frame scratch"));
   CGS_TRY(ctx->ensure(ctx->recs, (size_t)mn * sizeof(SplatRec), "splat records"));
   CGS_TRY(ctx->ensure(ctx->offsets, (size_t)mn * 4, "tile offsets"));
-  CGS_TRY(ctx->ensure(ctx->ranges, (size_t)total_tiles * 8, "tile ranges"));
+  CGS_TRY(ctx->ensure(ctx->ranges, (size_t)d.total_tiles * 8, "tile ranges"));
   char* sc = ctx->scratch.as<char>();
   FrameCounters* fc = (FrameCounters*)sc;
   uint32_t* d_split = ctx->persist.as<uint32_t>();
-
-  ctx->kpar ^= 1;
-  ctx->kfold(ctx->kpar, nullptr);  // frame f-2 used this event set
-  ctx->kcount[ctx->kpar] = 0;
-  ctx->kprof = prof;
-  ctx->kbegin(CGS_K_CLEAR);
-  CGS_CUDA(cudaMemsetAsync(sc, 0, scratch_bytes, s), "clear frame scratch");
-  ctx->kend();
-
-  // ---------------- Stage 1
   if (has_cages) {
     CGS_TRY(ctx->ensure(ctx->tet_J, (size_t)ctx->num_tets * 36, "tet J"));
     CGS_TRY(ctx->ensure(ctx->tet_R, (size_t)ctx->num_tets * 36, "tet R"));
@@ -494,42 +797,78 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     CGS_TRY(ctx->ensure(ctx->def_covb, (size_t)mn * 8, "deformed covariances"));
     CGS_TRY(ctx->ensure(ctx->split_meta, (size_t)(n ? n : 1) * 8, "split meta"));
   }
+
+  // Stage 3 cache key (gpu_state.rs:454-500). A hit needs the frame that
+  // built the cache to have been checked.
+  Stage3Key key;
+  key.deform_generation = has_cages ? (need_deform ? ctx->deform_generation + 1 : ctx->deform_generation) : 0;
+  for (int k = 0; k < 16; ++k) key.view[k] = fbits(camera->view[k]);
+  key.fx = fbits(camera->focal_x);
+  key.fy = fbits(camera->focal_y);
+  key.cx = fbits(camera->principal_x);
+  key.cy = fbits(camera->principal_y);
+  key.near_bits = fbits(camera->near_plane);
+  key.width = W;
+  key.height = H;
+  key.mip = mip_bits;
+  key.min_opa = fbits(params->min_opacity);
+  key.min_rad = fbits(params->min_radius_px);
+  key.radix_bits = d.radix_bits;
+  bool cached = !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
+  if (cached) {
+    CGS_TRY(drain(ctx, true));
+    cached = ctx->s3_valid && ctx->s3_key == key;
+  }
+  if (!cached) {
+    if (ctx->entry_cap == 0)
+      ctx->entry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(32ull * mn, 1u << 20), 0x3FFFFFFFull);
+    CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, d.key64, d.radix_bits));
+  }
+
+  cgs_ctx::Pending& P = ctx->ring[slot];
+  P.kcount = 0;
+  ctx->kprof = prof;
+  ctx->cur = slot;
+  ctx->kbegin(CGS_K_CLEAR);
+  CGS_CUDA(cudaMemsetAsync(sc, 0, L.bytes, s), "clear frame scratch");
+  ctx->kend();
+
+  // ---------------- Stage 1
   if (need_deform) {
-    DeformArgs d{};
-    d.n = n;
-    d.num_tets = ctx->num_tets;
-    d.verts = ctx->cage_verts.as<float>();
-    d.elems = ctx->tet_elems.as<uint4>();
-    d.inv_dm = ctx->tet_inv_dm.as<float>();
-    d.tet_J = ctx->tet_J.as<float>();
-    d.tet_R = ctx->tet_R.as<float>();
-    d.tet_stretch = ctx->tet_S.as<float>();
-    d.bind_tet = ctx->bind_tet.as<uint32_t>();
-    d.bind_w = ctx->bind_w.as<float4>();
-    d.rest_pos = ctx->rest_pos.as<float4>();
-    d.rest_cova = ctx->rest_cova.as<float4>();
-    d.rest_covb = ctx->rest_covb.as<float2>();
-    d.def_pos = ctx->def_pos.as<float4>();
-    d.def_cova = ctx->def_cova.as<float4>();
-    d.def_covb = ctx->def_covb.as<float2>();
-    d.split_meta = ctx->split_meta.as<uint2>();
-    d.split_count = d_split;
-    d.status = (unsigned long long*)(sc + o_def);
-    d.fc = fc;
-    d.split_threshold = params->strain_split_threshold;
-    d.mip = params->mip_filter_3d_var;
+    DeformArgs da{};
+    da.n = n;
+    da.num_tets = ctx->num_tets;
+    da.verts = ctx->cage_verts.as<float>();
+    da.elems = ctx->tet_elems.as<uint4>();
+    da.inv_dm = ctx->tet_inv_dm.as<float>();
+    da.tet_J = ctx->tet_J.as<float>();
+    da.tet_R = ctx->tet_R.as<float>();
+    da.tet_stretch = ctx->tet_S.as<float>();
+    da.bind_tet = ctx->bind_tet.as<uint32_t>();
+    da.bind_w = ctx->bind_w.as<float4>();
+    da.rest_pos = ctx->rest_pos.as<float4>();
+    da.rest_cova = ctx->rest_cova.as<float4>();
+    da.rest_covb = ctx->rest_covb.as<float2>();
+    da.def_pos = ctx->def_pos.as<float4>();
+    da.def_cova = ctx->def_cova.as<float4>();
+    da.def_covb = ctx->def_covb.as<float2>();
+    da.split_meta = ctx->split_meta.as<uint2>();
+    da.split_count = d_split;
+    da.status = (unsigned long long*)(sc + L.def);
+    da.fc = fc;
+    da.split_threshold = params->strain_split_threshold;
+    da.mip = params->mip_filter_3d_var;
     ctx->kbegin(CGS_K_TET_TRANSFORMS);
-    CGS_CUDA(launch_tet_transforms(d, s), "tet transforms launch");
+    CGS_CUDA(launch_tet_transforms(da, s), "tet transforms launch");
     ctx->kend();
     ctx->kbegin(CGS_K_DEFORM);
-    CGS_CUDA(launch_deform(d, s), "deform launch");
+    CGS_CUDA(launch_deform(da, s), "deform launch");
     ctx->kend();
     ctx->deformed_valid = true;
     ctx->deform_generation++;
     ctx->last_split_bits = split_bits;
     ctx->last_mip_bits = mip_bits;
   }
-  tm.stage1_skipped = need_deform ? 0 : 1;
 
   // ---------------- Stage 2
   ProjectArgs p{};
@@ -541,7 +880,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     p.tet_R = ctx->tet_R.as<float>();
     p.num_tets = ctx->num_tets;
     p.split_meta = ctx->split_meta.as<uint2>();
-    p.split_count = split_possible ? d_split : nullptr;
+    p.split_count = d.split_possible ? d_split : nullptr;
   } else {
     p.pos = ctx->rest_pos.as<float4>();
     p.cova = ctx->rest_cova.as<float4>();
@@ -551,7 +890,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   p.sh_f16 = ctx->sh_f16;
   p.sh_stride = n;
   p.n_rest = n;
-  p.max_n = max_n;
+  p.max_n = d.max_n;
   std::memcpy(p.cam, camera, 24 * sizeof(float));
   std::memcpy(p.cam_pos, comp->camera_position, 3 * sizeof(float));
   p.mip = has_cages ? 0.0f : params->mip_filter_3d_var;
@@ -564,245 +903,72 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   CGS_CUDA(launch_project(p, s), "project launch");
   ctx->kend();
 
-  // ---------------- Stage 3
-  Stage3Key key;
-  key.deform_generation = has_cages ? ctx->deform_generation : 0;
-  for (int k = 0; k < 16; ++k) key.view[k] = fbits(camera->view[k]);
-  key.fx = fbits(camera->focal_x);
-  key.fy = fbits(camera->focal_y);
-  key.cx = fbits(camera->principal_x);
-  key.cy = fbits(camera->principal_y);
-  key.near_bits = fbits(camera->near_plane);
-  key.width = W;
-  key.height = H;
-  key.mip = mip_bits;
-  key.min_opa = fbits(params->min_opacity);
-  key.min_rad = fbits(params->min_radius_px);
-  key.radix_bits = radix_bits;
-  const bool cached = !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
-  const bool key64 = total_tiles > 65535u;
-  uint32_t entries = 0;
-  int result_src = 0;
-  if (cached) {
-    tm.stage3_cached = 1;
-    entries = ctx->s3_entries;
-    result_src = ctx->s3_src;
-  } else {
-    ctx->s3_valid = false;
-    BinArgs b{};
-    b.recs = ctx->recs.as<SplatRec>();
-    b.split_count = split_possible ? d_split : nullptr;
-    b.n_rest = n;
-    b.max_n = max_n;
-    b.width = W;
-    b.height = H;
-    b.tiles_x = tiles_x;
-    b.tiles_y = tiles_y;
-    b.offsets = ctx->offsets.as<uint32_t>();
-    b.status = (unsigned long long*)(sc + o_cs);
-    b.fc = fc;
-    b.entry_cap = 0xFFFFFFFFu;
-    ctx->kbegin(CGS_K_COUNT_SCAN);
-    CGS_CUDA(launch_count_scan(b, s), "count/scan launch");
-    ctx->kend();
-    CGS_CUDA(cudaMemcpyAsync(&ctx->h_counters[0], fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s), "read counters");
-    CGS_CUDA(cudaMemcpyAsync(ctx->h_split, d_split, 4, cudaMemcpyDeviceToHost, s), "read split count");
-    CGS_CUDA(cudaStreamSynchronize(s), "stage 3 count");
-    ctx->kfold(ctx->kpar ^ 1, nullptr);
-    CGS_TRY(ctx->check_end_status());
-    if (ctx->h_counters[0].status & kStatusLookbackTimeout)
-      return ctx->fail(CGS_E_TIMEOUT, "look-back wait gave up in Stage 1-3");
-    entries = ctx->h_counters[0].entries;
-    if (entries >= (1u << 30))
-      return ctx->fail(CGS_E_CAPACITY, "more than 2^30 tile entries in one frame");
-    const size_t ecap = entries ? entries : 1;
-    for (int k = 0; k < 2; ++k) {
-      CGS_TRY(ctx->ensure(ctx->keys[k], ecap * 4, "sort keys"));
-      CGS_TRY(ctx->ensure(ctx->ids[k], ecap * 4, "sort values"));
-      if (key64) CGS_TRY(ctx->ensure(ctx->depths[k], ecap * 4, "sort depths"));
-    }
-    uint32_t tile_bits = total_tiles <= 1 ? 1u : 32u - (uint32_t)__builtin_clz(total_tiles - 1);
-    uint32_t depth_bits = tile_bits >= 32 ? 0u : (32u - tile_bits < 28u ? 32u - tile_bits : 28u);
-    const uint32_t sort_bits = tile_bits + depth_bits > 32 ? 32 : tile_bits + depth_bits;
-    const uint32_t passes_lo = key64 ? sort_passes(32, radix_bits) : sort_passes(sort_bits, radix_bits);
-    const uint32_t passes_hi = key64 ? sort_passes(tile_bits, radix_bits) : 0u;
-    const uint32_t stiles = sort_tiles(entries);
-    ctx->last_sort_passes = passes_lo + passes_hi;
-    const size_t rstat = (size_t)(passes_lo + passes_hi) * stiles * (1u << radix_bits) * 4 + 256;
-    CGS_TRY(ctx->ensure(ctx->radix_status, rstat, "radix look-back"));
-    ctx->kbegin(CGS_K_CLEAR);
-    CGS_CUDA(cudaMemsetAsync(ctx->radix_status.p, 0, rstat, s), "clear radix status");
-    CGS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0, (size_t)total_tiles * 8, s), "clear ranges");
-    ctx->kend();
-    uint32_t* d_hist = (uint32_t*)(sc + o_hist);
-    b.key64 = key64;
-    const float near_c = camera->near_plane > 1e-6f ? camera->near_plane : 1e-6f;
-    b.depth_base_bits = fbits(near_c) & 0x7F800000u;
-    b.depth_bits = depth_bits;
-    b.keys = ctx->keys[0].as<uint32_t>();
-    b.depths = key64 ? ctx->depths[0].as<uint32_t>() : nullptr;
-    b.ids = ctx->ids[0].as<uint32_t>();
-    b.hist = d_hist;
-    b.radix_bits = radix_bits;
-    b.sort_bits = sort_bits;
-    b.tile_bits = tile_bits;
-    b.entry_cap = (uint32_t)ecap;
-    if (entries > 0) {
-      ctx->kbegin(CGS_K_EMIT);
-      CGS_CUDA(launch_emit(b, s), "emit launch");
-      ctx->kend();
-      uint32_t* rs_status = ctx->radix_status.as<uint32_t>();
-      uint32_t* tile_ctrs = (uint32_t*)((char*)rs_status + rstat - 256);
-      const uint32_t* n_ptr = &fc->entries;
-      if (!key64) {
-        SortArgs sa{};
-        sa.keys[0] = ctx->keys[0].as<uint32_t>();
-        sa.keys[1] = ctx->keys[1].as<uint32_t>();
-        sa.vals[0] = ctx->ids[0].as<uint32_t>();
-        sa.vals[1] = ctx->ids[1].as<uint32_t>();
-        sa.n_ptr = n_ptr;
-        sa.capacity = entries;
-        sa.first_bit = 0;
-        sa.num_bits = sort_bits;
-        sa.radix_bits = radix_bits;
-        sa.hist = d_hist;
-        sa.status = rs_status;
-        sa.tile_ctr = tile_ctrs;
-        sa.status_word = &fc->status;
-        sa.src = 0;
-        ctx->kbegin(CGS_K_RADIX_SORT);
-        CGS_CUDA(run_radix_sort(sa, &result_src, s), "radix sort");
-        ctx->kend();
-        ctx->kbegin(CGS_K_TILE_RANGES);
-        CGS_CUDA(launch_tile_ranges(ctx->keys[result_src].as<uint32_t>(), depth_bits, n_ptr,
-                                    total_tiles, ctx->ranges.as<uint32_t>(), s),
-                 "ranges launch");
-        ctx->kend();
-      } else {
-        // (tile, depth) order: stable sort by depth, then stable sort by tile.
-        SortArgs sa{};
-        sa.keys[0] = ctx->depths[0].as<uint32_t>();
-        sa.keys[1] = ctx->depths[1].as<uint32_t>();
-        sa.vals[0] = ctx->ids[0].as<uint32_t>();
-        sa.vals[1] = ctx->ids[1].as<uint32_t>();
-        sa.vals2[0] = ctx->keys[0].as<uint32_t>();
-        sa.vals2[1] = ctx->keys[1].as<uint32_t>();
-        sa.n_ptr = n_ptr;
-        sa.capacity = entries;
-        sa.first_bit = 0;
-        sa.num_bits = 32;
-        sa.radix_bits = radix_bits;
-        sa.hist = d_hist;
-        sa.status = rs_status;
-        sa.tile_ctr = tile_ctrs;
-        sa.status_word = &fc->status;
-        sa.src = 0;
-        int src1 = 0;
-        ctx->kbegin(CGS_K_RADIX_SORT);
-        CGS_CUDA(run_radix_sort(sa, &src1, s), "radix sort (depth)");
-        SortArgs sb = sa;
-        sb.keys[0] = ctx->keys[0].as<uint32_t>();
-        sb.keys[1] = ctx->keys[1].as<uint32_t>();
-        sb.vals2[0] = ctx->depths[0].as<uint32_t>();
-        sb.vals2[1] = ctx->depths[1].as<uint32_t>();
-        sb.num_bits = tile_bits;
-        sb.hist = d_hist + (size_t)passes_lo * (1u << radix_bits);
-        sb.status = rs_status + (size_t)passes_lo * stiles * (1u << radix_bits);
-        sb.tile_ctr = tile_ctrs + passes_lo;
-        sb.src = src1;
-        CGS_CUDA(run_radix_sort(sb, &result_src, s), "radix sort (tile)");
-        ctx->kend();
-        ctx->kbegin(CGS_K_TILE_RANGES);
-        CGS_CUDA(launch_tile_ranges(ctx->keys[result_src].as<uint32_t>(), 0, n_ptr, total_tiles,
-                                    ctx->ranges.as<uint32_t>(), s),
-                 "ranges launch");
-        ctx->kend();
-      }
-    }
+  // ---------------- Stages 3 and 4
+  int src = ctx->s3_src;
+  uint32_t passes = 0;
+  if (!cached) {
+    CGS_TRY(enqueue_stage3(ctx, d, L, &src, &passes));
     ctx->s3_valid = true;
     ctx->s3_key = key;
-    ctx->s3_entries = entries;
-    ctx->s3_src = result_src;
-    ctx->s3_key64 = key64;
-    ctx->s3_depth_bits = depth_bits;
-    ctx->s3_surviving = ctx->h_counters[0].surviving;
-    ctx->s3_active = n + (split_possible ? *ctx->h_split : 0u);
+    ctx->s3_src = src;
+    ctx->s3_key64 = d.key64;
+    ctx->s3_depth_bits = d.depth_bits;
   }
-
-  // ---------------- Stage 4
-  CompositeArgs c{};
-  c.recs = ctx->recs.as<SplatRec>();
-  c.sorted_ids = ctx->ids[result_src].p ? ctx->ids[result_src].as<uint32_t>() : nullptr;
-  c.ranges = ctx->ranges.as<uint32_t>();
-  c.width = W;
-  c.height = H;
-  c.tiles_x = tiles_x;
-  c.tiles_y = tiles_y;
-  c.pitch_px = pitch;
-  std::memcpy(c.bg, comp->background, 16);
-  c.out_rgba8 = ctx->fb_rgba8.as<uint32_t>();
-  c.out_f32 = params->write_f32 ? ctx->fb_f32.as<float4>() : nullptr;
-  c.fc = fc;
-  c.num_recs = mn;
-  c.num_entries = entries;
-  ctx->kbegin(CGS_K_COMPOSITE);
-  CGS_CUDA(launch_composite(c, s), "composite launch");
-  ctx->kend();
-  CGS_CUDA(cudaMemcpyAsync(&ctx->h_counters[1], fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s), "read counters");
-  ctx->end_copy_pending = true;
-
+  CGS_TRY(enqueue_stage4(ctx, d, src));
+  CGS_CUDA(cudaMemcpyAsync(&ctx->h_ring[slot].fc, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s),
+           "read counters");
+  CGS_CUDA(cudaMemcpyAsync(&ctx->h_ring[slot].split, d_split, 4, cudaMemcpyDeviceToHost, s),
+           "read split count");
+  CGS_CUDA(cudaEventRecord(P.done, s), "frame event");
+  P.used = true;
+  P.stage3_ran = !cached;
+  P.profiled = prof;
+  P.need_deform = need_deform;
+  P.split_possible = d.split_possible;
+  P.key64 = d.key64;
+  P.n = n;
+  P.cap = ctx->entry_cap;
+  P.sort_passes = passes;
+  P.total_tiles = d.total_tiles;
+  P.W = W;
+  P.H = H;
+  P.write_f32 = d.write_f32;
+  ctx->cur = -1;
+  ctx->latest_slot = slot;
+  if (!cached) ctx->last_desc = d;
   ctx->last_w = W;
   ctx->last_h = H;
-  ctx->last_pitch = pitch;
-  ctx->last_f32 = params->write_f32 != 0;
-  ctx->last_tiles = total_tiles;
+  ctx->last_pitch = d.pitch;
+  ctx->last_f32 = d.write_f32;
+  ctx->last_tiles = d.total_tiles;
   ctx->frame_done = true;
 
-  const uint64_t A = cached ? ctx->s3_active : n + (split_possible ? *ctx->h_split : 0u);
-  const uint64_t S = cached ? ctx->s3_surviving : ctx->h_counters[0].surviving;
-  if (prof) {
-    // Algorithmic HBM bytes per kernel: the data each launch must move once.
-    const uint64_t E = entries, T = ctx->num_tets;
-    const uint64_t shb = ctx->sh_f16 ? 96 : 192;
-    ctx->kcount_launch(CGS_K_CLEAR, cached ? 1 : 2, 0);
-    if (need_deform) {
-      ctx->kcount_launch(CGS_K_TET_TRANSFORMS, 1, T * (16 + 36 + 48 + 76));
-      ctx->kcount_launch(CGS_K_DEFORM, 1, (uint64_t)n * 60 + A * 40 + (A - n) * 8);
-    }
-    ctx->kcount_launch(CGS_K_PROJECT, 1, A * 40 + S * (shb + 48) + (A - S) * 16);
-    if (!cached) {
-      const uint64_t kw = key64 ? 12 : 8;
-      ctx->kcount_launch(CGS_K_COUNT_SCAN, 1, A * 36);
-      if (E) {
-        ctx->kcount_launch(CGS_K_EMIT, 1, A * 36 + E * kw);
-        ctx->kcount_launch(CGS_K_RADIX_SORT, ctx->last_sort_passes,
-                           (uint64_t)ctx->last_sort_passes * E * (key64 ? 24 : 16));
-        ctx->kcount_launch(CGS_K_TILE_RANGES, 1, E * 4 + (uint64_t)total_tiles * 8);
+  tm.stage1_skipped = need_deform ? 0 : 1;
+  tm.stage3_cached = cached ? 1 : 0;
+  tm.used_64bit_keys = d.key64 ? 1 : 0;
+  if (timings) {
+    // Counts (and per-stage device times) need the frame to have finished.
+    CGS_TRY(drain(ctx, true));
+    CGS_TRY(ctx->take_sticky());
+    const HostCounters& h = ctx->h_ring[slot];
+    tm.total_tile_entries = ctx->s3_entries;
+    tm.surviving_gaussians = h.fc.surviving;
+    tm.active_gaussians = ctx->last_active;
+    if (prof) {
+      double ms[CGS_KERNEL_COUNT] = {};
+      for (int c = 0; c < P.kcount; ++c) {
+        float v = 0.0f;
+        cudaEventElapsedTime(&v, P.kev[2 * c], P.kev[2 * c + 1]);
+        ms[P.kid[c]] += v;
       }
+      tm.stage1_deform_ms = ms[CGS_K_TET_TRANSFORMS] + ms[CGS_K_DEFORM];
+      tm.stage2_project_ms = ms[CGS_K_PROJECT];
+      tm.stage3_bin_sort_ms = ms[CGS_K_BIN] + ms[CGS_K_RADIX_SORT] + ms[CGS_K_TILE_RANGES];
+      tm.stage4_composite_ms = ms[CGS_K_COMPOSITE];
+      tm.used_hardware_timestamps = 1;
     }
-    ctx->kcount_launch(CGS_K_COMPOSITE, 1,
-                       E * 52 + (uint64_t)total_tiles * 8 +
-                           (uint64_t)W * H * (params->write_f32 ? 20 : 4));
-    ctx->kpending[ctx->kpar] = ctx->kcount[ctx->kpar] > 0;
+    *timings = tm;
   }
-  if (prof && timings) {
-    CGS_CUDA(cudaStreamSynchronize(s), "frame");
-    CGS_TRY(ctx->check_end_status());
-    cgs_kernel_profile fr{};
-    ctx->kfold(ctx->kpar, &fr);
-    tm.stage1_deform_ms = fr.ms[CGS_K_TET_TRANSFORMS] + fr.ms[CGS_K_DEFORM];
-    tm.stage2_project_ms = fr.ms[CGS_K_PROJECT];
-    tm.stage3_bin_sort_ms = fr.ms[CGS_K_COUNT_SCAN] + fr.ms[CGS_K_EMIT] +
-                            fr.ms[CGS_K_RADIX_SORT] + fr.ms[CGS_K_TILE_RANGES];
-    tm.stage4_composite_ms = fr.ms[CGS_K_COMPOSITE];
-    tm.used_hardware_timestamps = 1;
-  }
-  tm.surviving_gaussians = S;
-  tm.used_64bit_keys = key64 ? 1 : 0;
-  tm.total_tile_entries = entries;
-  tm.active_gaussians = A;
-  ctx->last_active = (uint32_t)tm.active_gaussians;
-  if (timings) *timings = tm;
   return CGS_OK;
 }
 
@@ -812,11 +978,12 @@ int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t heig
   if (width != ctx->last_w || height != ctx->last_h)
     return ctx->fail(CGS_E_ARG, "size differs from the last frame");
   cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
   CGS_CUDA(cudaMemcpy2DAsync(dst, (size_t)width * 4, ctx->fb_rgba8.p, (size_t)ctx->last_pitch * 4,
                              (size_t)width * 4, height, cudaMemcpyDeviceToHost, ctx->stream),
            "framebuffer readback");
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "framebuffer readback");
-  return ctx->check_end_status();
+  return ctx->take_sticky();
 }
 
 int cgs_readback_rgba_f32(cgs_ctx* ctx, float* dst, uint32_t width, uint32_t height) {
@@ -825,14 +992,16 @@ int cgs_readback_rgba_f32(cgs_ctx* ctx, float* dst, uint32_t width, uint32_t hei
   if (width != ctx->last_w || height != ctx->last_h)
     return ctx->fail(CGS_E_ARG, "size differs from the last frame");
   cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
   CGS_CUDA(cudaMemcpyAsync(dst, ctx->fb_f32.p, (size_t)width * height * 16, cudaMemcpyDeviceToHost, ctx->stream), "f32 readback");
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "f32 readback");
-  return ctx->check_end_status();
+  return ctx->take_sticky();
 }
 
 int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px) {
   if (!ctx || !d_rgba8 || !row_pitch_px) return CGS_E_ARG;
   if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
+  CGS_TRY(drain(ctx, true));
   *d_rgba8 = ctx->fb_rgba8.p;
   *row_pitch_px = ctx->last_pitch;
   return CGS_OK;
@@ -862,8 +1031,8 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
   if (!ctx || !out_bytes) return CGS_E_ARG;
   if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
   cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "read frame buffer");
-  CGS_TRY(ctx->check_end_status());
   const size_t active = ctx->last_active;
   const size_t splits = active > ctx->n ? active - ctx->n : 0;
   const size_t entries = ctx->s3_entries;
@@ -985,9 +1154,8 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
 }
 
 const char* cgs_kernel_name(int32_t id) {
-  static const char* names[CGS_KERNEL_COUNT] = {
-      "clear",  "tet_transforms", "deform",      "project",  "count_scan",
-      "emit",   "radix_sort",     "tile_ranges", "composite"};
+  static const char* names[CGS_KERNEL_COUNT] = {"clear", "tet_transforms", "deform", "project",
+                                                "bin", "radix_sort", "tile_ranges", "composite"};
   return (id >= 0 && id < CGS_KERNEL_COUNT) ? names[id] : "unknown";
 }
 
@@ -995,20 +1163,18 @@ int cgs_kernel_profile_read(cgs_ctx* ctx, cgs_kernel_profile* out) {
   if (!ctx || !out) return CGS_E_ARG;
   cudaSetDevice(ctx->device);
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "profile read");
-  ctx->kfold(0, nullptr);
-  ctx->kfold(1, nullptr);
+  CGS_TRY(drain(ctx, true));
   *out = ctx->kp_acc;
-  return CGS_OK;
+  return ctx->take_sticky();
 }
 
 int cgs_kernel_profile_reset(cgs_ctx* ctx) {
   if (!ctx) return CGS_E_ARG;
   cudaSetDevice(ctx->device);
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "profile reset");
-  ctx->kfold(0, nullptr);
-  ctx->kfold(1, nullptr);
+  CGS_TRY(drain(ctx, true));
   ctx->kp_acc = cgs_kernel_profile{};
-  return CGS_OK;
+  return ctx->take_sticky();
 }
 
 int cgs_scan_u32(cgs_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint64_t n,
@@ -1031,9 +1197,9 @@ int cgs_scan_u32(cgs_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint64_t n
                            words + 1, words + 2, ctx->stream),
            "scan launch");
   uint32_t h[3] = {0, 0, 0};
-  CGS_CUDA(cudaMemcpyAsync(ctx->h_split + 1, words, 12, cudaMemcpyDeviceToHost, ctx->stream), "scan total");
+  CGS_CUDA(cudaMemcpyAsync(ctx->h_misc + 1, words, 12, cudaMemcpyDeviceToHost, ctx->stream), "scan total");
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "scan");
-  std::memcpy(h, ctx->h_split + 1, 12);
+  std::memcpy(h, ctx->h_misc + 1, 12);
   if (h[2] & kStatusLookbackTimeout) return ctx->fail(CGS_E_TIMEOUT, "scan look-back wait gave up");
   if (total) *total = h[0];
   return CGS_OK;
@@ -1089,9 +1255,9 @@ static int sort_common(cgs_ctx* ctx, uint32_t* d_keys, uint32_t* d_vals, uint32_
 
 static int sort_status(cgs_ctx* ctx) {
   uint32_t* words = ctx->prim[0].as<uint32_t>();
-  CGS_CUDA(cudaMemcpyAsync(ctx->h_split + 1, words, 8, cudaMemcpyDeviceToHost, ctx->stream), "sort status");
+  CGS_CUDA(cudaMemcpyAsync(ctx->h_misc + 1, words, 8, cudaMemcpyDeviceToHost, ctx->stream), "sort status");
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "sort");
-  if (ctx->h_split[2] & kStatusLookbackTimeout) return ctx->fail(CGS_E_TIMEOUT, "sort look-back wait gave up");
+  if (ctx->h_misc[2] & kStatusLookbackTimeout) return ctx->fail(CGS_E_TIMEOUT, "sort look-back wait gave up");
   return CGS_OK;
 }
 

@@ -44,12 +44,14 @@ struct PassArgs {
   uint32_t dmask;          // digit mask of this pass (narrower on a final partial pass)
   const uint32_t* hist;    // this pass's digit counts
   uint32_t* status;        // this pass's [tiles][radix] look-back words
+  uint32_t* clear_next;    // [tiles][radix] words to zero for the next pass, or null
+  uint32_t grid_tiles;     // tiles covered by the grid (all of clear_next)
   uint32_t* tile_ctr;
   uint32_t* status_word;
 };
 
 template <int RB, bool PAY2>
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
+__global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const PassArgs a) {
   constexpr uint32_t R = 1u << RB;
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* s_keys = smem;                       // [kSortTile]
@@ -69,7 +71,24 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
   for (uint32_t k = tid; k < 8 * R; k += kSortThreads) s_whist[k] = 0u;
   __syncthreads();
   const uint32_t tile = s_misc[0];
+  // Clear this tile's words of the other look-back buffer for the next pass
+  // (the pass that used it has completed: passes are stream-ordered launches).
+  if (a.clear_next && tile < a.grid_tiles)
+    for (uint32_t k = tid; k < R; k += kSortThreads) a.clear_next[(size_t)tile * R + k] = 0u;
   if (tile >= num_tiles) return;
+
+  // Issue the tile's loads first so their latency overlaps the digit-base scan.
+  const size_t tile_base = (size_t)tile * kSortTile;
+  uint32_t k[kSortItems], v0[kSortItems], v1[kSortItems];
+  uint32_t rk[kSortItems / 2];  // two 16-bit in-warp ranks per word (ranks < 512)
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const size_t e = tile_base + (size_t)warp * (32 * kSortItems) + (size_t)j * 32 + lane;
+    const bool valid = e < n;
+    k[j] = valid ? __ldcs(a.keys_in + e) : 0xFFFFFFFFu;
+    v0[j] = valid ? __ldcs(a.v0_in + e) : 0u;
+    if (PAY2) v1[j] = valid ? __ldcs(a.v1_in + e) : 0u;
+  }
 
   // Global digit bases: exclusive scan of this pass's digit histogram.
   {
@@ -77,17 +96,6 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
     const uint32_t h = (uint32_t)tid < R ? a.hist[tid] : 0u;
     const uint32_t ex = block_exclusive_sum(h, s_misc + 8, &tot);
     if ((uint32_t)tid < R) s_dbase[tid] = ex;
-  }
-
-  const size_t tile_base = (size_t)tile * kSortTile;
-  uint32_t k[kSortItems], v0[kSortItems], v1[kSortItems], rk[kSortItems];
-#pragma unroll
-  for (int j = 0; j < kSortItems; ++j) {
-    const size_t e = tile_base + (size_t)warp * (32 * kSortItems) + (size_t)j * 32 + lane;
-    const bool valid = e < n;
-    k[j] = valid ? a.keys_in[e] : 0xFFFFFFFFu;
-    v0[j] = valid ? a.v0_in[e] : 0u;
-    if (PAY2) v1[j] = valid ? a.v1_in[e] : 0u;
   }
   // Warp-level stable ranking by digit.
   uint32_t* wh = s_whist + warp * R;
@@ -103,7 +111,11 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
       wh[d] = old + __popc(peers);
     }
     old = __shfl_sync(0xffffffffu, old, leader);
-    rk[j] = old + before;
+    const uint32_t r = old + before;
+    if (j & 1)
+      rk[j >> 1] |= r << 16;
+    else
+      rk[j >> 1] = r;
     __syncwarp();
   }
   __syncthreads();
@@ -130,13 +142,13 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
     uint32_t* st = a.status + (size_t)tile * R + tid;
     uint32_t excl = 0;
     if (tile == 0) {
-      st_release_u32(st, kFlagPre | agg);
+      st_relaxed_u32(st, kFlagPre | agg);
     } else {
-      st_release_u32(st, kFlagAgg | agg);
+      st_relaxed_u32(st, kFlagAgg | agg);
       long long pred = (long long)tile - 1;
       uint32_t spins = 0;
       while (pred >= 0) {
-        const uint32_t w = ld_acquire_u32(a.status + (size_t)pred * R + tid);
+        const uint32_t w = ld_relaxed_u32(a.status + (size_t)pred * R + tid);
         if ((w & ~kValueMask) == 0u) {
           if (++spins > kSpinLimit) {
             atomicOr(a.status_word, kStatusLookbackTimeout);
@@ -149,7 +161,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
         if ((w & ~kValueMask) == kFlagPre) break;
         --pred;
       }
-      st_release_u32(st, kFlagPre | ((excl + agg) & kValueMask));
+      st_relaxed_u32(st, kFlagPre | ((excl + agg) & kValueMask));
     }
     s_goff[tid] = s_dbase[tid] + excl - tstart;
   }
@@ -158,7 +170,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const PassArgs a) {
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t d = (k[j] >> a.shift) & a.dmask;
-    const uint32_t pos = s_tstart[d] + wh[d] + rk[j];
+    const uint32_t pos = s_tstart[d] + wh[d] + ((rk[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
     s_keys[pos] = k[j];
     s_v0[pos] = v0[j];
     if (PAY2) s_v1[pos] = v1[j];
@@ -260,7 +272,16 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     const uint32_t rem = a.num_bits - p * rb;
     pa.dmask = (1u << (rem < rb ? rem : rb)) - 1u;
     pa.hist = a.hist + (size_t)p * R;
-    pa.status = a.status + (size_t)p * tiles * R;
+    if (a.status2[0]) {
+      const int par = *a.parity;
+      pa.status = a.status2[par];
+      pa.clear_next = a.status2[par ^ 1];
+      *a.parity = par ^ 1;
+    } else {
+      pa.status = a.status + (size_t)p * tiles * R;
+      pa.clear_next = nullptr;
+    }
+    pa.grid_tiles = tiles;
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
     cudaError_t e;

@@ -1,6 +1,6 @@
-// Stage 3 (binning) on sm_100a: tile counting fused with a single-pass
-// chained scan, key emission fused with the radix digit histograms, and tile
-// range identification.
+// Stage 3 (binning) on sm_100a: one kernel that counts tile intersections,
+// scans the counts in a single chained pass and emits the sort keys together
+// with the radix digit histograms; and tile range identification.
 //
 // Reference semantics: count_tiles_kernel / ellipse_intersects_tile_gpu
 // (render/kernels/binning.rs:37-164), gpu_exclusive_scan (scan.rs:198-333),
@@ -29,6 +29,8 @@ constexpr int kBinWarps = kBinThreads / 32;
 struct WarpSplats {
   uint32_t base[kBinWarps][32];   // exclusive prefix of candidate counts
   uint32_t width[kBinWarps][32];  // tile-box width
+  uint32_t magic[kBinWarps][32];  // ceil(2^32 / width): c / width == umulhi(c, magic)
+  uint32_t owner_at[kBinWarps][32];  // lane whose candidates start at a chunk position
   uint32_t x0[kBinWarps][32];
   uint32_t y0[kBinWarps][32];
   float mu_x[kBinWarps][32];
@@ -122,7 +124,9 @@ __device__ __forceinline__ void stage_warp(WarpSplats& ws, int warp, int lane, c
   base = incl - ncand;
   total = __shfl_sync(0xffffffffu, incl, 31);
   ws.base[warp][lane] = base;
-  ws.width[warp][lane] = b.valid ? (b.x1 - b.x0 + 1u) : 1u;
+  const uint32_t w = b.valid ? (b.x1 - b.x0 + 1u) : 1u;
+  ws.width[warp][lane] = w;
+  ws.magic[warp][lane] = w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w);
   ws.x0[warp][lane] = b.x0;
   ws.y0[warp][lane] = b.y0;
   ws.mu_x[warp][lane] = b.mu_x;
@@ -134,57 +138,103 @@ __device__ __forceinline__ void stage_warp(WarpSplats& ws, int warp, int lane, c
   __syncwarp();
 }
 
-// Owner lane of candidate `item`: the largest lane whose base <= item.
-__device__ __forceinline__ int find_owner(const WarpSplats& ws, int warp, uint32_t item) {
-  int o = 0;
-#pragma unroll
-  for (int step = 16; step > 0; step >>= 1)
-    if (ws.base[warp][o + step] <= item) o += step;
+// Owner lane of each lane's candidate in the chunk [chunk, chunk + 32): the
+// starts of the candidate runs that begin inside the chunk are OR-reduced into
+// a position mask; a lane's owner is the run starting at the highest set
+// position not above it, or the run carried over from the previous chunk.
+// `carry` holds that run's lane between chunks (the first run starts at 0).
+__device__ __forceinline__ int chunk_owner(WarpSplats& ws, int warp, int lane, uint32_t chunk,
+                                           uint32_t base, uint32_t ncand, int& carry) {
+  const bool starts = ncand > 0u && base >= chunk && base - chunk < 32u;
+  if (starts) ws.owner_at[warp][base - chunk] = (uint32_t)lane;
+  const uint32_t smask = __reduce_or_sync(0xffffffffu, starts ? (1u << (base - chunk)) : 0u);
+  __syncwarp();
+  const uint32_t upto = smask & ((2u << lane) - 1u);
+  const int o = upto ? (int)ws.owner_at[warp][31 - __clz(upto)] : carry;
+  if (smask) carry = (int)ws.owner_at[warp][31 - __clz(smask)];
+  __syncwarp();
   return o;
+}
+
+// Tile of candidate `item` of owner lane o (row-major over its tile box).
+__device__ __forceinline__ void candidate_tile(const WarpSplats& ws, int warp, int o, uint32_t item,
+                                               uint32_t& tx, uint32_t& ty) {
+  const uint32_t c = item - ws.base[warp][o];
+  const uint32_t w = ws.width[warp][o];
+  const uint32_t r = w <= 1u ? c : __umulhi(c, ws.magic[warp][o]);
+  tx = ws.x0[warp][o] + (c - r * w);
+  ty = ws.y0[warp][o] + r;
 }
 
 __device__ __forceinline__ bool test_candidate(const WarpSplats& ws, int warp, int o,
                                                uint32_t item, const BinArgs& a, uint32_t& tile) {
-  const uint32_t c = item - ws.base[warp][o];
-  const uint32_t w = ws.width[warp][o];
-  const uint32_t r = c / w;
-  const uint32_t tx = ws.x0[warp][o] + (c - r * w);
-  const uint32_t ty = ws.y0[warp][o] + r;
+  uint32_t tx, ty;
+  candidate_tile(ws, warp, o, item, tx, ty);
   tile = ty * a.tiles_x + tx;
   return ellipse_hit(ws.mu_x[warp][o], ws.mu_y[warp][o], ws.ca[warp][o], ws.cb[warp][o],
                      ws.cc[warp][o], ws.qcut[warp][o], tx, ty, a.width, a.height);
 }
 
-// Tile counts per splat, block exclusive scan, chained scan across blocks ->
-// offsets[s]; the last block writes the entry total to fc->entries.
-__global__ void __launch_bounds__(kBinThreads) k_count_scan(const BinArgs a) {
+// One pass of binning for a block of 256 splats:
+//   1. counting: every candidate tile of the warp's 32 splats is tested once
+//      (ballot per 32 candidates); the ballot masks are kept in shared memory;
+//   2. block exclusive scan of the per-splat counts, chained across blocks
+//      (decoupled look-back) -> each splat's first entry (written to `offsets`);
+//   3. emission: the masks are walked again, each hit is written at
+//      offset + (its rank inside the splat), row-major as in the reference,
+//      with its 32-bit key (tile << depth_bits | depth_q) or, for more than
+//      65,535 tiles, its (tile, raw depth bits) pair; the digit histograms of
+//      every radix pass are accumulated at the same time.
+// Entries at or beyond the key-buffer capacity are not written and set the
+// capacity status bit (the host grows the buffers and runs Stage 3 again).
+// The last block writes the frame's entry total.
+constexpr int kMaskCap = 48;  // stored ballot masks per warp (1,536 candidates)
+
+template <bool KEY64>
+__global__ void __launch_bounds__(kBinThreads) k_bin(const BinArgs a) {
   __shared__ WarpSplats ws;
-  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_off[kBinWarps][32];
+  __shared__ uint32_t s_dq[kBinWarps][32];
+  __shared__ uint32_t s_carry[kBinWarps][32];
+  __shared__ uint32_t s_masks[kBinWarps][kMaskCap];
+  __shared__ uint32_t s_hist[8 * 256];
+  __shared__ uint32_t s_tile, s_base;
   __shared__ uint32_t s_warp_sums[32];
-  __shared__ uint32_t s_base;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
+  const uint32_t passes_lo = KEY64 ? (32u + a.radix_bits - 1u) / a.radix_bits
+                                   : (a.sort_bits + a.radix_bits - 1u) / a.radix_bits;
+  const uint32_t passes_hi = KEY64 ? (a.tile_bits + a.radix_bits - 1u) / a.radix_bits : 0u;
+  const uint32_t nbins = (passes_lo + passes_hi) * radix;
   if (threadIdx.x == 0) s_tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
+  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
   const uint32_t tile = s_tile;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
   const uint32_t s = tile * kBinThreads + threadIdx.x;
   const SplatBox b = load_box(a, s, active);
   uint32_t ncand, base, total;
   stage_warp(ws, warp, lane, b, ncand, base, total);
+
+  // 1. count
   uint32_t count = 0;
-  for (uint32_t chunk = 0; chunk < total; chunk += 32) {
+  int carry = 0;
+  for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
     const uint32_t item = chunk + lane;
+    const int o = chunk_owner(ws, warp, lane, chunk, base, ncand, carry);
     bool hit = false;
     if (item < total) {
-      const int o = find_owner(ws, warp, item);
       uint32_t t;
       hit = test_candidate(ws, warp, o, item, a, t);
     }
     const uint32_t hits = __ballot_sync(0xffffffffu, hit);
+    if (c < (uint32_t)kMaskCap && lane == 0) s_masks[warp][c] = hits;
     const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
     const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
     count += __popc(hits & seg_mask(lo, hi));
   }
+
+  // 2. scan
   uint32_t agg;
   const uint32_t excl = block_exclusive_sum(count, s_warp_sums, &agg);
   if (threadIdx.x < 32) {
@@ -192,39 +242,16 @@ __global__ void __launch_bounds__(kBinThreads) k_count_scan(const BinArgs a) {
     if (threadIdx.x == 0) s_base = pre;
   }
   __syncthreads();
-  if (s < a.max_n) a.offsets[s] = s_base + excl;
+  const uint32_t first = s_base + excl;
+  if (s < a.max_n) a.offsets[s] = first;
   const uint32_t num_tiles = (a.max_n + kBinThreads - 1) / kBinThreads;
   if (tile == num_tiles - 1 && threadIdx.x == 0) {
     const uint32_t e = s_base + agg;
     a.fc->entries = e;
     if (e > a.entry_cap) atomicOr(&a.fc->status, kStatusCapacity);
   }
-}
 
-// Key emission: 32-bit keys (tile << depth_bits | depth_q) or, for more than
-// 65,535 tiles, (tile, raw depth bits) word pairs; plus the digit histograms
-// of every radix pass, accumulated in shared memory and added to `hist`.
-template <bool KEY64>
-__global__ void __launch_bounds__(kBinThreads) k_emit(const BinArgs a) {
-  __shared__ WarpSplats ws;
-  __shared__ uint32_t s_off[kBinWarps][32];
-  __shared__ uint32_t s_dq[kBinWarps][32];
-  __shared__ uint32_t s_carry[kBinWarps][32];
-  __shared__ uint32_t s_hist[8 * 256];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
-  const uint32_t passes_lo = KEY64 ? (32u + a.radix_bits - 1u) / a.radix_bits
-                                   : (a.sort_bits + a.radix_bits - 1u) / a.radix_bits;
-  const uint32_t passes_hi = KEY64 ? (a.tile_bits + a.radix_bits - 1u) / a.radix_bits : 0u;
-  const uint32_t nbins = (passes_lo + passes_hi) * radix;
-  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
-  __syncthreads();
-  const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
-  const uint32_t cap = a.entry_cap;
-  const uint32_t s = blockIdx.x * kBinThreads + threadIdx.x;
-  const SplatBox b = load_box(a, s, active);
-  uint32_t ncand, base, total;
-  stage_warp(ws, warp, lane, b, ncand, base, total);
+  // 3. emit
   uint32_t dq = 0;
   if (b.valid) {
     if (KEY64) {
@@ -235,43 +262,57 @@ __global__ void __launch_bounds__(kBinThreads) k_emit(const BinArgs a) {
       dq = rel >> (28u - a.depth_bits);
     }
   }
-  s_off[warp][lane] = (b.valid && s < a.max_n) ? a.offsets[s] : 0u;
+  s_off[warp][lane] = first;
   s_dq[warp][lane] = dq;
   s_carry[warp][lane] = 0u;
   __syncwarp();
-  for (uint32_t chunk = 0; chunk < total; chunk += 32) {
+  const uint32_t cap = a.entry_cap;
+  bool overflow = false;
+  carry = 0;
+  for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
     const uint32_t item = chunk + lane;
-    bool hit = false;
-    int o = 0;
-    uint32_t tile = 0;
-    if (item < total) {
-      o = find_owner(ws, warp, item);
-      hit = test_candidate(ws, warp, o, item, a, tile);
+    const int o = chunk_owner(ws, warp, lane, chunk, base, ncand, carry);
+    uint32_t hits;
+    uint32_t tile_id = 0;
+    if (c < (uint32_t)kMaskCap) {
+      hits = s_masks[warp][c];
+      if ((hits >> lane) & 1u) {
+        uint32_t tx, ty;
+        candidate_tile(ws, warp, o, item, tx, ty);
+        tile_id = ty * a.tiles_x + tx;
+      }
+    } else {
+      bool hit = false;
+      if (item < total) hit = test_candidate(ws, warp, o, item, a, tile_id);
+      hits = __ballot_sync(0xffffffffu, hit);
     }
-    const uint32_t hits = __ballot_sync(0xffffffffu, hit);
-    if (hit) {
+    if ((hits >> lane) & 1u) {
       const uint32_t ob = ws.base[warp][o];
       const int sstart = ob > chunk ? (int)(ob - chunk) : 0;
       const uint32_t below = hits & lanemask_lt() & ~seg_mask(0, sstart);
       const uint32_t pos = s_off[warp][o] + s_carry[warp][o] + __popc(below);
-      const uint32_t sid = blockIdx.x * kBinThreads + warp * 32 + o;
+      const uint32_t sid = tile * kBinThreads + warp * 32 + o;
       if (pos < cap) {
         if (KEY64) {
-          a.keys[pos] = tile;
+          a.keys[pos] = tile_id;
           a.depths[pos] = s_dq[warp][o];
           a.ids[pos] = sid;
           const uint32_t d = s_dq[warp][o];
           for (uint32_t p = 0; p < passes_lo; ++p)
             atomicAdd(&s_hist[p * radix + ((d >> (p * a.radix_bits)) & rmask)], 1u);
           for (uint32_t p = 0; p < passes_hi; ++p)
-            atomicAdd(&s_hist[(passes_lo + p) * radix + ((tile >> (p * a.radix_bits)) & rmask)], 1u);
+            atomicAdd(&s_hist[(passes_lo + p) * radix + ((tile_id >> (p * a.radix_bits)) & rmask)],
+                      1u);
         } else {
-          const uint32_t key = a.depth_bits >= 32u ? s_dq[warp][o] : ((tile << a.depth_bits) | s_dq[warp][o]);
+          const uint32_t key =
+              a.depth_bits >= 32u ? s_dq[warp][o] : ((tile_id << a.depth_bits) | s_dq[warp][o]);
           a.keys[pos] = key;
           a.ids[pos] = sid;
           for (uint32_t p = 0; p < passes_lo; ++p)
             atomicAdd(&s_hist[p * radix + ((key >> (p * a.radix_bits)) & rmask)], 1u);
         }
+      } else {
+        overflow = true;
       }
     }
     __syncwarp();
@@ -280,6 +321,7 @@ __global__ void __launch_bounds__(kBinThreads) k_emit(const BinArgs a) {
     s_carry[warp][lane] += __popc(hits & seg_mask(lo, hi));
     __syncwarp();
   }
+  if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
     const uint32_t v = s_hist[k];
@@ -288,24 +330,43 @@ __global__ void __launch_bounds__(kBinThreads) k_emit(const BinArgs a) {
 }
 
 // identify_tile_ranges_kernel (binning.rs:356-391): boundaries of equal tile
-// ids in the sorted words. Grid-stride over the device-side entry count.
+// ids in the sorted words. Each thread checks four consecutive words (one
+// 128-bit load plus the word before them), grid-stride over the device-side
+// entry count; boundaries are rare, so the writes are few.
+__device__ __forceinline__ void range_edge(uint32_t i, uint32_t t, uint32_t prev, uint32_t n,
+                                           uint32_t total_tiles, uint32_t* ranges) {
+  if (t >= total_tiles) return;
+  if (i == 0) {
+    ranges[2 * (size_t)t] = 0u;
+  } else if (t != prev) {
+    if (prev < total_tiles) ranges[2 * (size_t)prev + 1] = i;
+    ranges[2 * (size_t)t] = i;
+  }
+  if (i + 1 == n) ranges[2 * (size_t)t + 1] = n;
+}
+
 __global__ void k_tile_ranges(const uint32_t* __restrict__ sorted, uint32_t shift,
-                              const uint32_t* __restrict__ n_ptr, uint32_t total_tiles,
-                              uint32_t* __restrict__ ranges) {
-  const uint32_t n = *n_ptr;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t t = shift >= 32u ? 0u : (sorted[i] >> shift);
-    if (t >= total_tiles) continue;
-    if (i == 0) {
-      ranges[2 * (size_t)t] = 0u;
+                              const uint32_t* __restrict__ n_ptr, uint32_t capacity,
+                              uint32_t total_tiles, uint32_t* __restrict__ ranges) {
+  const uint32_t n = min(*n_ptr, capacity);
+  const uint32_t quads = (n + 3) / 4;
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x) {
+    const uint32_t i0 = 4 * q;
+    uint32_t w[4];
+    if (i0 + 3 < n) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4*>(sorted) + q);
+      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
     } else {
-      const uint32_t prev = shift >= 32u ? 0u : (sorted[i - 1] >> shift);
-      if (t != prev) {
-        if (prev < total_tiles) ranges[2 * (size_t)prev + 1] = i;
-        ranges[2 * (size_t)t] = i;
-      }
+      for (int k = 0; k < 4; ++k) w[k] = i0 + k < n ? sorted[i0 + k] : 0u;
     }
-    if (i + 1 == n) ranges[2 * (size_t)t + 1] = n;
+    uint32_t prev = i0 > 0 ? (shift >= 32u ? 0u : (sorted[i0 - 1] >> shift)) : 0xFFFFFFFFu;
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t i = i0 + k;
+      if (i >= n) break;
+      const uint32_t t = shift >= 32u ? 0u : (w[k] >> shift);
+      range_edge(i, t, prev, n, total_tiles, ranges);
+      prev = t;
+    }
   }
 }
 
@@ -353,25 +414,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_u32(const uint32_t* __res
 
 }  // namespace
 
-cudaError_t launch_count_scan(const BinArgs& a, cudaStream_t s) {
-  if (a.max_n == 0) return cudaSuccess;
-  k_count_scan<<<(a.max_n + kBinThreads - 1) / kBinThreads, kBinThreads, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_emit(const BinArgs& a, cudaStream_t s) {
+cudaError_t launch_bin(const BinArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
   const uint32_t blocks = (a.max_n + kBinThreads - 1) / kBinThreads;
   if (a.key64)
-    k_emit<true><<<blocks, kBinThreads, 0, s>>>(a);
+    k_bin<true><<<blocks, kBinThreads, 0, s>>>(a);
   else
-    k_emit<false><<<blocks, kBinThreads, 0, s>>>(a);
+    k_bin<false><<<blocks, kBinThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
-                               uint32_t total_tiles, uint32_t* ranges, cudaStream_t s) {
-  k_tile_ranges<<<148 * 8, 256, 0, s>>>(sorted, shift, n_ptr, total_tiles, ranges);
+                               uint32_t capacity, uint32_t total_tiles, uint32_t* ranges,
+                               cudaStream_t s) {
+  k_tile_ranges<<<148 * 8, 256, 0, s>>>(sorted, shift, n_ptr, capacity, total_tiles, ranges);
   return cudaGetLastError();
 }
 

@@ -14,8 +14,11 @@
 // host restatement does (IEEE-rounded q, the deterministic exp near the cut),
 // so the only differences are last-bit colour sums and the rare pixel whose
 // transmittance lands within an ulp of 1e-3 (bounded by that 1e-3). The block stops when no pixel is still accumulating
-// (__syncthreads_or, the reference's double-buffered tile_alive vote). Output
-// is RGBA8 packed in u32 rows padded to 64 pixels, optionally also RGBA f32.
+// (the reference's double-buffered tile_alive vote). Between batches the
+// pixels that are still accumulating are re-packed into the lowest threads of
+// the block, so a warp whose 32 pixels have all saturated stops issuing work
+// instead of running the batch with dead lanes. Output is RGBA8 packed in u32
+// rows padded to 64 pixels, optionally also RGBA f32.
 // Every wait on an mbarrier is bounded; a block never exits with a bulk copy
 // still in flight into its shared memory.
 #include "kernels.h"
@@ -106,9 +109,32 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
     }
   };
 
+  // Per-thread pixel state. Pixels still accumulating are re-packed into the
+  // lowest threads at every batch boundary (when that frees whole warps), so
+  // warps whose pixels have all saturated stop issuing instructions.
+  __shared__ uint32_t s_pix[kCompThreads];
+  __shared__ float4 s_acc[kCompThreads];
+  __shared__ uint32_t s_warp_alive[kCompThreads / 32];
+  int pix = inside ? (int)tid : -1;
+  bool alive = inside;
   float cr = 0.0f, cg = 0.0f, cb = 0.0f, t = 1.0f;
-  bool saturated = false;
-  const float pcx = (float)px + 0.5f, pcy = (float)py + 0.5f;
+  float pcx = (float)px + 0.5f, pcy = (float)py + 0.5f;
+
+  auto finalize = [&](int p, float r_, float g_, float b_, float t_) {
+    const uint32_t x = blockIdx.x * 16u + ((uint32_t)p & 15u);
+    const uint32_t y = blockIdx.y * 16u + ((uint32_t)p >> 4);
+    const float fr = clampf(r_ + t_ * a.bg[0], 0.0f, 1.0f);
+    const float fg = clampf(g_ + t_ * a.bg[1], 0.0f, 1.0f);
+    const float fb = clampf(b_ + t_ * a.bg[2], 0.0f, 1.0f);
+    const float fa = empty ? a.bg[3] : clampf(1.0f - t_, 0.0f, 1.0f);
+    const uint32_t r8 = (uint32_t)clampf(rintf(fr * 255.0f), 0.0f, 255.0f);
+    const uint32_t g8 = (uint32_t)clampf(rintf(fg * 255.0f), 0.0f, 255.0f);
+    const uint32_t b8 = (uint32_t)clampf(rintf(fb * 255.0f), 0.0f, 255.0f);
+    const uint32_t a8 = (uint32_t)clampf(rintf(fa * 255.0f), 0.0f, 255.0f);
+    a.out_rgba8[(size_t)y * a.pitch_px + x] = r8 | (g8 << 8) | (b8 << 16) | (a8 << 24);
+    if (a.out_f32) a.out_f32[(size_t)y * a.width + x] = make_float4(fr, fg, fb, fa);
+  };
+
   bool ok = true;
   uint32_t consumed = 0;
   uint32_t issued = 0;
@@ -125,7 +151,7 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
     if (!mbar_wait(&s_bar[stage], (b >> 1) & 1u)) ok = false;
     consumed = b + 1;
     const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
-    if (inside && !saturated) {
+    if (alive) {
       const SplatRec* recs = s_rec[stage];
       for (uint32_t k = 0; k < cnt; ++k) {
         const float4 cc4 = recs[k].cc;
@@ -154,7 +180,7 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
               cb += w * rgb.z;
               t *= 1.0f - alpha;
               if (t < 0.001f) {
-                saturated = true;
+                alive = false;
                 t = 0.0f;
                 break;
               }
@@ -163,25 +189,49 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
         }
       }
     }
-    if (!__syncthreads_or(inside && !saturated)) break;
+    // Batch boundary: write finished pixels, stop when none is left, and
+    // re-pack the survivors when they are spread over more warps than needed.
+    if (pix >= 0 && !alive) {
+      finalize(pix, cr, cg, cb, t);
+      pix = -1;
+    }
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    const uint32_t wmask = __ballot_sync(0xffffffffu, alive);
+    const int n_alive = __syncthreads_count(alive);
+    if (n_alive == 0) break;
+    const int warps_busy = __syncthreads_count(lane == 0 && wmask != 0u);
+    if (b + 1 < nb && warps_busy > (n_alive + 31) / 32) {
+      if (lane == 0) s_warp_alive[warp] = __popc(wmask);
+      __syncthreads();
+      uint32_t base = 0;
+      for (uint32_t w = 0; w < warp; ++w) base += s_warp_alive[w];
+      if (alive) {
+        const uint32_t slot = base + __popc(wmask & lanemask_lt());
+        s_pix[slot] = (uint32_t)pix;
+        s_acc[slot] = make_float4(cr, cg, cb, t);
+      }
+      __syncthreads();
+      alive = (int)tid < n_alive;
+      if (alive) {
+        pix = (int)s_pix[tid];
+        const float4 acc = s_acc[tid];
+        cr = acc.x;
+        cg = acc.y;
+        cb = acc.z;
+        t = acc.w;
+        pcx = (float)(blockIdx.x * 16u + ((uint32_t)pix & 15u)) + 0.5f;
+        pcy = (float)(blockIdx.y * 16u + ((uint32_t)pix >> 4)) + 0.5f;
+      } else {
+        pix = -1;
+      }
+    }
   }
   // Never leave with a bulk copy still writing into this block's shared memory.
   for (uint32_t b = consumed; b < issued; ++b)
     if (!mbar_wait(&s_bar[b & 1u], (b >> 1) & 1u)) ok = false;
   if (!ok && a.fc) atomicOr(&a.fc->status, kStatusBarrierTimeout);
-
-  if (inside) {
-    const float fr = clampf(cr + t * a.bg[0], 0.0f, 1.0f);
-    const float fg = clampf(cg + t * a.bg[1], 0.0f, 1.0f);
-    const float fb = clampf(cb + t * a.bg[2], 0.0f, 1.0f);
-    const float fa = empty ? a.bg[3] : clampf(1.0f - t, 0.0f, 1.0f);
-    const uint32_t r8 = (uint32_t)clampf(rintf(fr * 255.0f), 0.0f, 255.0f);
-    const uint32_t g8 = (uint32_t)clampf(rintf(fg * 255.0f), 0.0f, 255.0f);
-    const uint32_t b8 = (uint32_t)clampf(rintf(fb * 255.0f), 0.0f, 255.0f);
-    const uint32_t a8 = (uint32_t)clampf(rintf(fa * 255.0f), 0.0f, 255.0f);
-    a.out_rgba8[(size_t)py * a.pitch_px + px] = r8 | (g8 << 8) | (b8 << 16) | (a8 << 24);
-    if (a.out_f32) a.out_f32[(size_t)py * a.width + px] = make_float4(fr, fg, fb, fa);
-  }
+  if (tid == 0 && a.fc && issued > 0) atomicAdd(&a.fc->fetched, min(n, issued * (uint32_t)kBatch));
+  if (pix >= 0) finalize(pix, cr, cg, cb, t);
 }
 
 }  // namespace

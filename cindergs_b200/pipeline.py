@@ -179,10 +179,13 @@ class GpuPipelineState:
                           profile_stages: bool = False, force_stage3: bool = False,
                           write_f32: bool = False, radix_bits: int = 0,
                           stage_timings: bool = True) -> GpuStageTimings:
-        """execute_frame_gpu (gpu_state.rs:613-1243). With profile_stages and
-        stage_timings both set, the call waits for the frame to report its
-        per-stage device ms; with stage_timings=False a profiled frame only
-        accumulates kernel times (read them with kernel_profile())."""
+        """execute_frame_gpu (gpu_state.rs:613-1243). With stage_timings (the
+        default) the call waits for the frame and returns its counts (and, with
+        profile_stages, per-stage device ms); with stage_timings=False the frame
+        is only enqueued (no host synchronisation), its kernel times still
+        accumulate when profile_stages is set (read them with kernel_profile()),
+        and the returned timings carry only the stage1_skipped, stage3_cached
+        and used_64bit_keys flags."""
         self.sync_scene_and_cages(scene, cages)
         cam = _abi.CgsCamera()
         arr = camera.to_array()
@@ -196,7 +199,7 @@ class GpuPipelineState:
                                      int(bool(profile_stages)), int(bool(force_stage3)),
                                      int(bool(write_f32)), int(radix_bits))
         t = _abi.CgsStageTimings()
-        tp = ctypes.byref(t) if (stage_timings or not profile_stages) else None
+        tp = ctypes.byref(t) if stage_timings else None
         self._check(self._lib.cgs_execute_frame(self._ctx, ctypes.byref(cam), ctypes.byref(comp),
                                                 ctypes.byref(params), tp),
                     "cgs_execute_frame")

@@ -141,7 +141,11 @@ int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const 
 /* Runs Stages 1-4 on the resident scene (execute_frame_gpu,
  * gpu_state.rs:613-626). Stage 1 is skipped when cages and deform params are
  * unchanged; Stage 3 is reused when its cache key (gpu_state.rs:454-500) is
- * unchanged and force_stage3 is 0. `timings` may be NULL. */
+ * unchanged and force_stage3 is 0. The frame is enqueued without any host
+ * synchronisation when `timings` is NULL; with `timings` the call waits for
+ * the frame and reports its counts (and, with profile_stages, its per-stage
+ * device times). A frame whose tile entries exceeded the key buffers is
+ * binned and composited again with grown buffers before any readback. */
 int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
                       const cgs_frame_params* params, cgs_stage_timings* timings);
 
@@ -163,16 +167,15 @@ int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px)
  * once, outputs written once), the numerator of its roofline fraction. No
  * reference counterpart: it refines GpuStageTimings (gpu_state.rs:513-534)
  * to kernel granularity. */
-#define CGS_K_CLEAR 0
+#define CGS_K_CLEAR 0          /* memsets of per-frame scratch */
 #define CGS_K_TET_TRANSFORMS 1
 #define CGS_K_DEFORM 2
 #define CGS_K_PROJECT 3
-#define CGS_K_COUNT_SCAN 4
-#define CGS_K_EMIT 5
-#define CGS_K_RADIX_SORT 6
-#define CGS_K_TILE_RANGES 7
-#define CGS_K_COMPOSITE 8
-#define CGS_KERNEL_COUNT 9
+#define CGS_K_BIN 4            /* count + chained scan + key emission, one launch */
+#define CGS_K_RADIX_SORT 5     /* all radix passes of the frame */
+#define CGS_K_TILE_RANGES 6
+#define CGS_K_COMPOSITE 7
+#define CGS_KERNEL_COUNT 8
 typedef struct cgs_kernel_profile {
   double ms[CGS_KERNEL_COUNT];
   uint64_t alg_bytes[CGS_KERNEL_COUNT];

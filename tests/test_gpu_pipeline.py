@@ -128,3 +128,26 @@ def test_stage3_cache_and_repeatability(gpu_state):
                                        240, 0.2)
     t3 = st.execute_frame_gpu(scene, None, cam2, comp)
     assert not t3.stage3_cached
+
+
+def test_key_buffer_overflow_is_rebinned(gpu_state):
+    """A fresh context sizes its key buffers before it knows the entry count;
+    a frame whose entries overflow them is binned again, so the readback and
+    every Stage 3 buffer still match the oracle."""
+    from cindergs_b200 import GpuPipelineState
+    st = GpuPipelineState(0)
+    try:
+        scene = random_scene(4000, seed=13)
+        scene.covariances_3d[:] = np.array([0.09, 0.0, 0.0, 0.09, 0.0, 0.09], np.float32)
+        scene.positions *= np.float32(0.4)
+        cam = config0_camera(1920, 1080)
+        comp = compositor(1920, 1080, cam, deg=1)
+        t, g, o = run_both(st, scene, cam, comp)
+        assert t.total_tile_entries == o["entries"] > (1 << 20)  # initial buffers: 2^20
+        assert_stage23_exact(g, o)
+        check_image(g, o)
+        # the next frame runs with grown buffers
+        t2 = st.execute_frame_gpu(scene, None, cam, comp, force_stage3=True)
+        assert t2.total_tile_entries == o["entries"]
+    finally:
+        st.close()
