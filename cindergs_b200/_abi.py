@@ -82,7 +82,7 @@ class CgsStageTimings(ctypes.Structure):
 
 
 KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "radix_sort",
-                "tile_ranges", "composite"]
+                "tile_ranges", "composite", "splat_sort"]
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 

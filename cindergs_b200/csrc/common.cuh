@@ -24,7 +24,8 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 // Per-frame counters, cleared at the start of every frame.
 struct FrameCounters {
   uint32_t surviving;    // Stage 2 survivors
-  uint32_t entries;      // Stage 3 tile entries (count_scan total)
+  uint32_t active;       // splat slots of the frame (rest + split children), from Stage 2
+  uint32_t entries;      // Stage 3 tile entries (binning total)
   uint32_t status;       // kStatus* bits
   uint32_t fetched;      // splat records the compositor gathered
   uint32_t tile_ctr[16]; // dynamic tile counters for chained-scan kernels

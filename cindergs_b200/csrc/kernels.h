@@ -70,6 +70,15 @@ struct ProjectArgs {
   uint32_t sh_degree;
   SplatRec* out;              // [max_n]
   FrameCounters* fc;
+  // Stage 3's per-splat depth keys and slot ids (null when the frame reuses
+  // an earlier frame's Stage 3): 32-bit keys get the quantised depth of the
+  // packed (tile, depth) key, 64-bit keys the raw depth bits; culled splats
+  // get 0xFFFFFFFF, which sorts after every visible depth.
+  uint32_t* depth_keys;       // [max_n]
+  uint32_t* depth_ids;        // [max_n]
+  int key64;
+  uint32_t depth_base_bits;   // near-plane exponent bits (32-bit keys)
+  uint32_t depth_bits;        // depth bits in a 32-bit key
 };
 cudaError_t launch_project(const ProjectArgs& a, cudaStream_t s);
 
@@ -81,11 +90,16 @@ cudaError_t launch_scene_layout(uint32_t n, const float* pos, const float* cov, 
 // ---- Stage 3 (stage3_bin.cu) -------------------------------------------------
 struct BinArgs {
   const SplatRec* recs;
+  // Splats in depth-key order (the stable radix sort of Stage 2's depth keys):
+  // slot s of the binning grid is splat order_ids[s] with depth key
+  // order_keys[s]; its entries are emitted in this order.
+  const uint32_t* order_keys;
+  const uint32_t* order_ids;
   const uint32_t* split_count;  // null when no splitting
   uint32_t n_rest;
   uint32_t max_n;
   uint32_t width, height, tiles_x, tiles_y;
-  uint32_t* offsets;            // [max_n]
+  uint32_t* offsets;            // [max_n] first entry of each slot (depth order)
   unsigned long long* status;   // [ceil(max_n/256)] zeroed
   FrameCounters* fc;
   // emission
@@ -95,10 +109,9 @@ struct BinArgs {
   uint32_t* keys;               // 32-bit: packed keys; 64-bit: tile ids
   uint32_t* depths;             // 64-bit: raw depth bits
   uint32_t* ids;
-  uint32_t* hist;               // [passes][1 << radix_bits] digit histograms, zeroed
+  uint32_t* hist;               // [passes][1 << radix_bits] tile-digit histograms, zeroed
   uint32_t radix_bits;
-  uint32_t sort_bits;           // 32-bit key bits (tile + depth)
-  uint32_t tile_bits;           // 64-bit: tile id bits
+  uint32_t tile_bits;           // tile id bits (the entry sort's key bits)
   uint32_t entry_cap;           // capacity of keys/depths/ids
 };
 // Counts, scans and emits in one launch (k_bin).

@@ -92,15 +92,17 @@ constexpr int kMaxMarks = 24;     // profiled launches per frame
 // Scratch layout of a frame (one memset): counters | deform look-back |
 // binning look-back | radix histograms | radix tile counters.
 struct ScratchLayout {
-  size_t def, bin, hist, rtiles, bytes;
+  size_t def, bin, hist, rtiles, shist, bytes;
   ScratchLayout(uint32_t n, uint32_t mn) {
     def = 256;
     bin = def + ((size_t)(n + 255) / 256) * 8 + 256;
     hist = bin + ((size_t)(mn + 255) / 256) * 8 + 256;
-    rtiles = hist + 8 * 256 * 4;
-    bytes = rtiles + 256;
+    rtiles = hist + 8 * 256 * 4;  // [0, 32): entry passes; [32, 40): splat passes
+    shist = rtiles + 256;         // splat depth-key histograms, 4 passes x 256
+    bytes = shist + 4 * 256 * 4;
   }
 };
+constexpr uint32_t kSplatSortTileCtr = 32;
 
 }  // namespace
 
@@ -128,6 +130,11 @@ struct cgs_ctx {
   DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
+  // splat depth sort (Stage 3): keys/ids ping-pong and look-back pair
+  DevBuf skeys[2], sids[2], splat_lb[2];
+  uint32_t splat_cap = 0;  // slots those buffers hold; fixed between reallocations
+  int splat_parity = 0;
+  int s3_order_src = 0;    // buffer holding the latest Stage 3's splat order
   uint32_t entry_cap = 0;       // capacity of the key/id buffers (entries)
   uint32_t radix_lb_tiles = 0;  // tiles the radix look-back buffers cover
   uint32_t radix_lb_bits = 0;
@@ -149,7 +156,7 @@ struct cgs_ctx {
   struct Pending {
     bool used = false, stage3_ran = false, profiled = false, need_deform = false;
     bool split_possible = false, key64 = false;
-    uint32_t n = 0, cap = 0, sort_passes = 0, total_tiles = 0, W = 0, H = 0;
+    uint32_t n = 0, cap = 0, sort_passes = 0, splat_passes = 0, total_tiles = 0, W = 0, H = 0;
     bool write_f32 = false;
     cudaEvent_t done = nullptr;
     cudaEvent_t kev[2 * kMaxMarks] = {};
@@ -247,11 +254,38 @@ int ensure_entry_buffers(cgs_ctx* ctx, uint32_t cap, bool key64, uint32_t radix_
   return CGS_OK;
 }
 
-// Enqueues Stage 3 (binning, radix sort, tile ranges) for `d` with the
-// current key-buffer capacity. *result_src receives the buffer holding the
-// sorted lists; *passes the number of radix passes.
+// Depth-key buffers and look-back pair of the splat sort for `mn` slots. The
+// capacity (and so the sort's grid) only changes on reallocation, when both
+// look-back buffers are cleared: the passes clear the buffer they do not use
+// over the whole grid, which keeps them clean only while the grid is fixed.
+int ensure_splat_buffers(cgs_ctx* ctx, uint32_t mn) {
+  if (mn <= ctx->splat_cap && ctx->splat_lb[0].p) return CGS_OK;
+  const uint64_t want = std::max<uint64_t>((uint64_t)mn + mn / 4, 4096);
+  const uint32_t cap = (uint32_t)std::min<uint64_t>((want + 4095) / 4096 * 4096, 0xFFFFF000ull);
+  for (int k = 0; k < 2; ++k) {
+    CGS_TRY(ctx->ensure(ctx->skeys[k], (size_t)cap * 4, "splat depth keys"));
+    CGS_TRY(ctx->ensure(ctx->sids[k], (size_t)cap * 4, "splat order"));
+  }
+  const size_t bytes = (size_t)sort_tiles(cap) * 256 * 4;
+  for (int k = 0; k < 2; ++k) {
+    CGS_TRY(ctx->ensure(ctx->splat_lb[k], bytes, "splat sort look-back"));
+    CGS_CUDA(cudaMemsetAsync(ctx->splat_lb[k].p, 0, bytes, ctx->stream), "clear look-back");
+  }
+  ctx->splat_cap = cap;
+  ctx->splat_parity = 0;
+  return CGS_OK;
+}
+
+// Enqueues Stage 3 for `d` with the current key-buffer capacity:
+//   1. stable radix sort of Stage 2's per-splat depth keys (skipped with
+//      `sort_splats` false: a re-run of the same frame reuses its order);
+//   2. binning in that order (k_bin): entries leave ordered by depth;
+//   3. stable radix sort of the entries on their tile bits only;
+//   4. tile ranges.
+// *result_src receives the buffer holding the sorted lists; *passes and
+// *splat_passes the number of radix passes over entries and splats.
 int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int* result_src,
-                   uint32_t* passes) {
+                   uint32_t* passes, uint32_t* splat_passes, bool sort_splats) {
   cudaStream_t s = ctx->stream;
   char* sc = ctx->scratch.as<char>();
   FrameCounters* fc = (FrameCounters*)sc;
@@ -261,8 +295,39 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   ctx->kbegin(CGS_K_CLEAR);
   CGS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0, (size_t)d.total_tiles * 8, s), "clear ranges");
   ctx->kend();
+  const uint32_t dbits = d.key64 ? 32u : d.depth_bits;
+  *splat_passes = 0;
+  if (sort_splats) {
+    uint32_t* shist = (uint32_t*)(sc + L.shist);
+    ctx->kbegin(CGS_K_SPLAT_SORT);
+    CGS_CUDA(launch_histogram(ctx->skeys[0].as<uint32_t>(), &fc->active, ctx->splat_cap, 0, dbits,
+                              8, shist, s),
+             "splat histogram");
+    SortArgs so{};
+    so.keys[0] = ctx->skeys[0].as<uint32_t>();
+    so.keys[1] = ctx->skeys[1].as<uint32_t>();
+    so.vals[0] = ctx->sids[0].as<uint32_t>();
+    so.vals[1] = ctx->sids[1].as<uint32_t>();
+    so.n_ptr = &fc->active;
+    so.capacity = ctx->splat_cap;
+    so.first_bit = 0;
+    so.num_bits = dbits;
+    so.radix_bits = 8;
+    so.hist = shist;
+    so.status2[0] = ctx->splat_lb[0].as<uint32_t>();
+    so.status2[1] = ctx->splat_lb[1].as<uint32_t>();
+    so.parity = &ctx->splat_parity;
+    so.tile_ctr = rtiles + kSplatSortTileCtr;
+    so.status_word = &fc->status;
+    so.src = 0;
+    CGS_CUDA(run_radix_sort(so, &ctx->s3_order_src, s), "splat sort");
+    ctx->kend();
+    *splat_passes = sort_passes(dbits, 8);
+  }
   BinArgs b{};
   b.recs = ctx->recs.as<SplatRec>();
+  b.order_keys = ctx->skeys[ctx->s3_order_src].as<uint32_t>();
+  b.order_ids = ctx->sids[ctx->s3_order_src].as<uint32_t>();
   b.split_count = d.split_possible ? d_split : nullptr;
   b.n_rest = d.n;
   b.max_n = d.max_n;
@@ -281,20 +346,30 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.ids = ctx->ids[0].as<uint32_t>();
   b.hist = d_hist;
   b.radix_bits = d.radix_bits;
-  b.sort_bits = d.sort_bits;
   b.tile_bits = d.tile_bits;
   b.entry_cap = ctx->entry_cap;
   ctx->kbegin(CGS_K_BIN);
   CGS_CUDA(launch_bin(b, s), "bin launch");
   ctx->kend();
   const uint32_t* n_ptr = &fc->entries;
-  const uint32_t passes_lo = d.key64 ? sort_passes(32, d.radix_bits) : sort_passes(d.sort_bits, d.radix_bits);
-  const uint32_t passes_hi = d.key64 ? sort_passes(d.tile_bits, d.radix_bits) : 0u;
-  *passes = passes_lo + passes_hi;
+  *passes = sort_passes(d.tile_bits, d.radix_bits);
+  // Entries arrive in (depth, splat) order; a stable sort on the tile bits
+  // (above the depth bits of a 32-bit key, or the whole tile word of the
+  // 64-bit layout, whose depth word travels as a second payload) completes
+  // the (tile, depth, splat) order.
   SortArgs sa{};
+  sa.keys[0] = ctx->keys[0].as<uint32_t>();
+  sa.keys[1] = ctx->keys[1].as<uint32_t>();
+  sa.vals[0] = ctx->ids[0].as<uint32_t>();
+  sa.vals[1] = ctx->ids[1].as<uint32_t>();
+  if (d.key64) {
+    sa.vals2[0] = ctx->depths[0].as<uint32_t>();
+    sa.vals2[1] = ctx->depths[1].as<uint32_t>();
+  }
   sa.n_ptr = n_ptr;
   sa.capacity = ctx->entry_cap;
-  sa.first_bit = 0;
+  sa.first_bit = d.key64 ? 0u : d.depth_bits;
+  sa.num_bits = d.tile_bits;
   sa.radix_bits = d.radix_bits;
   sa.status2[0] = ctx->radix_lb[0].as<uint32_t>();
   sa.status2[1] = ctx->radix_lb[1].as<uint32_t>();
@@ -304,35 +379,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.hist = d_hist;
   sa.src = 0;
   ctx->kbegin(CGS_K_RADIX_SORT);
-  if (!d.key64) {
-    sa.keys[0] = ctx->keys[0].as<uint32_t>();
-    sa.keys[1] = ctx->keys[1].as<uint32_t>();
-    sa.vals[0] = ctx->ids[0].as<uint32_t>();
-    sa.vals[1] = ctx->ids[1].as<uint32_t>();
-    sa.num_bits = d.sort_bits;
-    CGS_CUDA(run_radix_sort(sa, result_src, s), "radix sort");
-  } else {
-    // (tile, depth) order: stable sort by depth, then stable sort by tile.
-    sa.keys[0] = ctx->depths[0].as<uint32_t>();
-    sa.keys[1] = ctx->depths[1].as<uint32_t>();
-    sa.vals[0] = ctx->ids[0].as<uint32_t>();
-    sa.vals[1] = ctx->ids[1].as<uint32_t>();
-    sa.vals2[0] = ctx->keys[0].as<uint32_t>();
-    sa.vals2[1] = ctx->keys[1].as<uint32_t>();
-    sa.num_bits = 32;
-    int src1 = 0;
-    CGS_CUDA(run_radix_sort(sa, &src1, s), "radix sort (depth)");
-    SortArgs sb = sa;
-    sb.keys[0] = ctx->keys[0].as<uint32_t>();
-    sb.keys[1] = ctx->keys[1].as<uint32_t>();
-    sb.vals2[0] = ctx->depths[0].as<uint32_t>();
-    sb.vals2[1] = ctx->depths[1].as<uint32_t>();
-    sb.num_bits = d.tile_bits;
-    sb.hist = d_hist + (size_t)passes_lo * (1u << d.radix_bits);
-    sb.tile_ctr = rtiles + passes_lo;
-    sb.src = src1;
-    CGS_CUDA(run_radix_sort(sb, result_src, s), "radix sort (tile)");
-  }
+  CGS_CUDA(run_radix_sort(sa, result_src, s), "radix sort");
   ctx->kend();
   ctx->kbegin(CGS_K_TILE_RANGES);
   CGS_CUDA(launch_tile_ranges(ctx->keys[*result_src].as<uint32_t>(), d.key64 ? 0u : d.depth_bits,
@@ -373,16 +420,16 @@ int rerun_stage34(cgs_ctx* ctx, uint32_t entries) {
   CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, d.key64, d.radix_bits));
   const ScratchLayout L(d.n, d.max_n ? d.max_n : 1u);
   char* sc = ctx->scratch.as<char>();
-  // keep fc->surviving (Stage 2's count); clear the Stage 3 words
-  CGS_CUDA(cudaMemsetAsync(sc + 4, 0, sizeof(FrameCounters) - 4, ctx->stream), "clear counters");
+  // keep fc->surviving and fc->active (Stage 2's words); clear the Stage 3 words
+  CGS_CUDA(cudaMemsetAsync(sc + 8, 0, sizeof(FrameCounters) - 8, ctx->stream), "clear counters");
   CGS_CUDA(cudaMemsetAsync(sc + L.bin, 0, L.bytes - L.bin, ctx->stream), "clear scratch");
   const bool kp = ctx->kprof;
   const int cur = ctx->cur;
   ctx->kprof = false;
   ctx->cur = -1;
   int src = 0;
-  uint32_t passes = 0;
-  int rc = enqueue_stage3(ctx, d, L, &src, &passes);
+  uint32_t passes = 0, splat_passes = 0;
+  int rc = enqueue_stage3(ctx, d, L, &src, &passes, &splat_passes, false);
   if (rc == CGS_OK) rc = enqueue_stage4(ctx, d, src);
   ctx->kprof = kp;
   ctx->cur = cur;
@@ -444,7 +491,9 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, p.kev[2 * c], p.kev[2 * c + 1]);
       kp.ms[p.kid[c]] += ms;
-      kp.launches[p.kid[c]] += (p.kid[c] == CGS_K_RADIX_SORT) ? p.sort_passes : 1u;
+      kp.launches[p.kid[c]] += p.kid[c] == CGS_K_RADIX_SORT   ? p.sort_passes
+                               : p.kid[c] == CGS_K_SPLAT_SORT ? 1u + p.splat_passes
+                                                              : 1u;
     }
     const uint64_t A = p.n + (p.split_possible ? h.split : 0u);
     const uint64_t S = h.fc.surviving, E = p.stage3_ran ? entries : 0, T = ctx->num_tets;
@@ -453,9 +502,10 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       kp.alg_bytes[CGS_K_TET_TRANSFORMS] += T * (16 + 36 + 48 + 76);
       kp.alg_bytes[CGS_K_DEFORM] += (uint64_t)p.n * 60 + A * 40 + (A - p.n) * 8;
     }
-    kp.alg_bytes[CGS_K_PROJECT] += A * 40 + S * (shb + 48) + (A - S) * 16;
+    kp.alg_bytes[CGS_K_PROJECT] += A * 40 + S * (shb + 48) + (A - S) * 16 + (p.stage3_ran ? A * 8 : 0);
     if (p.stage3_ran) {
-      kp.alg_bytes[CGS_K_BIN] += A * 36 + E * (p.key64 ? 12 : 8);
+      kp.alg_bytes[CGS_K_SPLAT_SORT] += A * 4 + (uint64_t)p.splat_passes * A * 16;
+      kp.alg_bytes[CGS_K_BIN] += A * 44 + E * (p.key64 ? 12 : 8);
       kp.alg_bytes[CGS_K_RADIX_SORT] += (uint64_t)p.sort_passes * E * (p.key64 ? 24 : 16);
       kp.alg_bytes[CGS_K_TILE_RANGES] += E * 4 + (uint64_t)p.total_tiles * 8;
     }
@@ -823,6 +873,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     if (ctx->entry_cap == 0)
       ctx->entry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(32ull * mn, 1u << 20), 0x3FFFFFFFull);
     CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, d.key64, d.radix_bits));
+    CGS_TRY(ensure_splat_buffers(ctx, mn));
   }
 
   cgs_ctx::Pending& P = ctx->ring[slot];
@@ -899,15 +950,22 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   p.sh_degree = comp->sh_degree > 3 ? 3 : comp->sh_degree;
   p.out = ctx->recs.as<SplatRec>();
   p.fc = fc;
+  if (!cached) {
+    p.depth_keys = ctx->skeys[0].as<uint32_t>();
+    p.depth_ids = ctx->sids[0].as<uint32_t>();
+  }
+  p.key64 = d.key64;
+  p.depth_base_bits = d.depth_base_bits;
+  p.depth_bits = d.depth_bits;
   ctx->kbegin(CGS_K_PROJECT);
   CGS_CUDA(launch_project(p, s), "project launch");
   ctx->kend();
 
   // ---------------- Stages 3 and 4
   int src = ctx->s3_src;
-  uint32_t passes = 0;
+  uint32_t passes = 0, splat_passes = 0;
   if (!cached) {
-    CGS_TRY(enqueue_stage3(ctx, d, L, &src, &passes));
+    CGS_TRY(enqueue_stage3(ctx, d, L, &src, &passes, &splat_passes, true));
     ctx->s3_valid = true;
     ctx->s3_key = key;
     ctx->s3_src = src;
@@ -929,6 +987,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   P.n = n;
   P.cap = ctx->entry_cap;
   P.sort_passes = passes;
+  P.splat_passes = splat_passes;
   P.total_tiles = d.total_tiles;
   P.W = W;
   P.H = H;
@@ -1104,10 +1163,31 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
       }
       break;
     }
-    case CGS_BUF_TILE_OFFSETS:
-      CGS_TRY(fetch(ctx->offsets, active * 4));
-      out = tmp;
+    case CGS_BUF_TILE_OFFSETS: {
+      // The binning kernel scans the counts in depth order; the reference's
+      // buffer is the scan in splat order, rebuilt here from the per-slot
+      // offsets, the splat order and the entry total.
+      const size_t sa = ctx->s3_active;
+      CGS_TRY(fetch(ctx->offsets, sa * 4));
+      const std::vector<char> off_b = tmp;
+      CGS_TRY(fetch(ctx->sids[ctx->s3_order_src], sa * 4));
+      const uint32_t* off = (const uint32_t*)off_b.data();
+      const uint32_t* ord = (const uint32_t*)tmp.data();
+      std::vector<uint32_t> cnt(sa, 0);
+      for (size_t j = 0; j < sa; ++j) {
+        const uint32_t next = j + 1 < sa ? off[j + 1] : (uint32_t)entries;
+        if (ord[j] >= sa) return ctx->fail(CGS_E_STATE, "splat order out of range");
+        cnt[ord[j]] = next - off[j];
+      }
+      out.resize(sa * 4);
+      uint32_t* o = (uint32_t*)out.data();
+      uint32_t run = 0;
+      for (size_t i = 0; i < sa; ++i) {
+        o[i] = run;
+        run += cnt[i];
+      }
       break;
+    }
     case CGS_BUF_SORTED_KEYS:
       if (!ctx->s3_key64) {
         CGS_TRY(fetch(ctx->keys[ctx->s3_src], entries * 4));
@@ -1155,7 +1235,8 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
 
 const char* cgs_kernel_name(int32_t id) {
   static const char* names[CGS_KERNEL_COUNT] = {"clear", "tet_transforms", "deform", "project",
-                                                "bin", "radix_sort", "tile_ranges", "composite"};
+                                                "bin", "radix_sort", "tile_ranges", "composite",
+                                                "splat_sort"};
   return (id >= 0 && id < CGS_KERNEL_COUNT) ? names[id] : "unknown";
 }
 

@@ -239,7 +239,26 @@ __global__ void __launch_bounds__(kProjectThreads) k_project(const ProjectArgs a
     } else {
       rec->cc = make_float4(0.0f, 0.0f, tz, 0.0f);
     }
+    if (a.depth_keys) {
+      // The depth part of the splat's tile keys (emit_tile_keys_kernel,
+      // binning.rs:170-328): Stage 3 sorts the splats by it once, then emits
+      // their entries in that order and sorts the entries by tile alone.
+      uint32_t dk = 0xFFFFFFFFu;
+      if (visible) {
+        if (a.key64) {
+          dk = __float_as_uint(fmaxf(tz, 0.0f));
+        } else {
+          const uint32_t raw = __float_as_uint(fmaxf(tz, 1e-6f));
+          const uint32_t rel =
+              raw > a.depth_base_bits ? min(raw - a.depth_base_bits, 0x0FFFFFFFu) : 0u;
+          dk = rel >> (28u - a.depth_bits);
+        }
+      }
+      a.depth_keys[idx] = dk;
+      a.depth_ids[idx] = idx;
+    }
   }
+  if (idx == 0) a.fc->active = active < a.max_n ? active : a.max_n;
   const uint32_t vote = __ballot_sync(0xffffffffu, visible);
   if ((threadIdx.x & 31) == 0 && vote) atomicAdd(&a.fc->surviving, (uint32_t)__popc(vote));
 }

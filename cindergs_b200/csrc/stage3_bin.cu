@@ -175,16 +175,22 @@ __device__ __forceinline__ bool test_candidate(const WarpSplats& ws, int warp, i
                      ws.cc[warp][o], ws.qcut[warp][o], tx, ty, a.width, a.height);
 }
 
-// One pass of binning for a block of 256 splats:
+// One pass of binning for a block of 256 splats, taken in depth-key order
+// (slot s is splat order_ids[s]; Stage 2's depth keys were radix-sorted
+// stably, so slots run by (depth key, splat index)):
 //   1. counting: every candidate tile of the warp's 32 splats is tested once
 //      (ballot per 32 candidates); the ballot masks are kept in shared memory;
-//   2. block exclusive scan of the per-splat counts, chained across blocks
-//      (decoupled look-back) -> each splat's first entry (written to `offsets`);
+//   2. block exclusive scan of the per-slot counts, chained across blocks
+//      (decoupled look-back) -> each slot's first entry (written to `offsets`);
 //   3. emission: the masks are walked again, each hit is written at
 //      offset + (its rank inside the splat), row-major as in the reference,
 //      with its 32-bit key (tile << depth_bits | depth_q) or, for more than
 //      65,535 tiles, its (tile, raw depth bits) pair; the digit histograms of
-//      every radix pass are accumulated at the same time.
+//      the tile bits are accumulated at the same time.
+// The entries therefore leave this kernel ordered by (depth, splat index), and
+// a stable sort on the tile bits alone yields the reference's (tile, depth,
+// splat index) order: sorting the splats once (N keys) replaces the depth
+// passes over all entries.
 // Entries at or beyond the key-buffer capacity are not written and set the
 // capacity status bit (the host grows the buffers and runs Stage 3 again).
 // The last block writes the frame's entry total.
@@ -195,6 +201,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(const BinArgs a) {
   __shared__ WarpSplats ws;
   __shared__ uint32_t s_off[kBinWarps][32];
   __shared__ uint32_t s_dq[kBinWarps][32];
+  __shared__ uint32_t s_sid[kBinWarps][32];
   __shared__ uint32_t s_carry[kBinWarps][32];
   __shared__ uint32_t s_masks[kBinWarps][kMaskCap];
   __shared__ uint32_t s_hist[8 * 256];
@@ -202,17 +209,21 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(const BinArgs a) {
   __shared__ uint32_t s_warp_sums[32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
-  const uint32_t passes_lo = KEY64 ? (32u + a.radix_bits - 1u) / a.radix_bits
-                                   : (a.sort_bits + a.radix_bits - 1u) / a.radix_bits;
-  const uint32_t passes_hi = KEY64 ? (a.tile_bits + a.radix_bits - 1u) / a.radix_bits : 0u;
-  const uint32_t nbins = (passes_lo + passes_hi) * radix;
+  const uint32_t passes = (a.tile_bits + a.radix_bits - 1u) / a.radix_bits;
+  const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
+  const uint32_t nbins = passes * radix;
   if (threadIdx.x == 0) s_tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
-  const uint32_t s = tile * kBinThreads + threadIdx.x;
-  const SplatBox b = load_box(a, s, active);
+  const uint32_t s = tile * kBinThreads + threadIdx.x;  // slot in depth order
+  uint32_t sid = kInvalid, dq = 0;
+  if (s < active && s < a.max_n) {
+    sid = a.order_ids[s];
+    dq = a.order_keys[s];
+  }
+  const SplatBox b = load_box(a, sid, active);
   uint32_t ncand, base, total;
   stage_warp(ws, warp, lane, b, ncand, base, total);
 
@@ -252,18 +263,9 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(const BinArgs a) {
   }
 
   // 3. emit
-  uint32_t dq = 0;
-  if (b.valid) {
-    if (KEY64) {
-      dq = __float_as_uint(fmaxf(b.tz, 0.0f));
-    } else {
-      const uint32_t raw = __float_as_uint(fmaxf(b.tz, 1e-6f));
-      const uint32_t rel = raw > a.depth_base_bits ? min(raw - a.depth_base_bits, 0x0FFFFFFFu) : 0u;
-      dq = rel >> (28u - a.depth_bits);
-    }
-  }
   s_off[warp][lane] = first;
   s_dq[warp][lane] = dq;
+  s_sid[warp][lane] = sid;
   s_carry[warp][lane] = 0u;
   __syncwarp();
   const uint32_t cap = a.entry_cap;
@@ -291,26 +293,19 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(const BinArgs a) {
       const int sstart = ob > chunk ? (int)(ob - chunk) : 0;
       const uint32_t below = hits & lanemask_lt() & ~seg_mask(0, sstart);
       const uint32_t pos = s_off[warp][o] + s_carry[warp][o] + __popc(below);
-      const uint32_t sid = tile * kBinThreads + warp * 32 + o;
+      const uint32_t osid = s_sid[warp][o];
       if (pos < cap) {
+        uint32_t word;
         if (KEY64) {
-          a.keys[pos] = tile_id;
+          word = tile_id;
           a.depths[pos] = s_dq[warp][o];
-          a.ids[pos] = sid;
-          const uint32_t d = s_dq[warp][o];
-          for (uint32_t p = 0; p < passes_lo; ++p)
-            atomicAdd(&s_hist[p * radix + ((d >> (p * a.radix_bits)) & rmask)], 1u);
-          for (uint32_t p = 0; p < passes_hi; ++p)
-            atomicAdd(&s_hist[(passes_lo + p) * radix + ((tile_id >> (p * a.radix_bits)) & rmask)],
-                      1u);
         } else {
-          const uint32_t key =
-              a.depth_bits >= 32u ? s_dq[warp][o] : ((tile_id << a.depth_bits) | s_dq[warp][o]);
-          a.keys[pos] = key;
-          a.ids[pos] = sid;
-          for (uint32_t p = 0; p < passes_lo; ++p)
-            atomicAdd(&s_hist[p * radix + ((key >> (p * a.radix_bits)) & rmask)], 1u);
+          word = a.depth_bits >= 32u ? s_dq[warp][o] : ((tile_id << a.depth_bits) | s_dq[warp][o]);
         }
+        a.keys[pos] = word;
+        a.ids[pos] = osid;
+        for (uint32_t p = 0; p < passes; ++p)
+          atomicAdd(&s_hist[p * radix + ((word >> (tshift + p * a.radix_bits)) & rmask)], 1u);
       } else {
         overflow = true;
       }

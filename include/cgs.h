@@ -172,10 +172,11 @@ int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px)
 #define CGS_K_DEFORM 2
 #define CGS_K_PROJECT 3
 #define CGS_K_BIN 4            /* count + chained scan + key emission, one launch */
-#define CGS_K_RADIX_SORT 5     /* all radix passes of the frame */
+#define CGS_K_RADIX_SORT 5     /* radix passes over the tile entries */
 #define CGS_K_TILE_RANGES 6
 #define CGS_K_COMPOSITE 7
-#define CGS_KERNEL_COUNT 8
+#define CGS_K_SPLAT_SORT 8     /* depth-key histogram + radix passes over the splats */
+#define CGS_KERNEL_COUNT 9
 typedef struct cgs_kernel_profile {
   double ms[CGS_KERNEL_COUNT];
   uint64_t alg_bytes[CGS_KERNEL_COUNT];
