@@ -99,23 +99,31 @@ struct BinArgs {
   uint32_t n_rest;
   uint32_t max_n;
   uint32_t width, height, tiles_x, tiles_y;
-  uint32_t* offsets;            // [max_n] first entry of each slot (depth order)
-  unsigned long long* status;   // [ceil(max_n/256)] zeroed
+  // per slot (depth order): the counting kernel writes the tile count, the
+  // scan turns it into the first entry in place
+  uint32_t* offsets;            // [max_n]
+  uint32_t* tile_stage;         // [ceil(max_n/32)] staging start of each 32-slot tile
+  uint32_t* tile_count;         // [ceil(max_n/32)] entries of each 32-slot tile
   FrameCounters* fc;
-  // emission
   int key64;
-  uint32_t depth_base_bits;     // near-plane exponent bits (32-bit keys)
   uint32_t depth_bits;          // depth bits in a 32-bit key
-  uint32_t* keys;               // 32-bit: packed keys; 64-bit: tile ids
-  uint32_t* depths;             // 64-bit: raw depth bits
+  // staged entries (counting kernel) and their final places (placement kernel)
+  uint32_t* stage_keys;         // 32-bit: packed keys; 64-bit: tile ids
+  uint32_t* stage_depths;       // 64-bit: raw depth bits
+  uint32_t* stage_ids;
+  uint32_t* keys;
+  uint32_t* depths;
   uint32_t* ids;
   uint32_t* hist;               // [passes][1 << radix_bits] tile-digit histograms, zeroed
   uint32_t radix_bits;
   uint32_t tile_bits;           // tile id bits (the entry sort's key bits)
-  uint32_t entry_cap;           // capacity of keys/depths/ids
+  uint32_t entry_cap;           // capacity of every entry buffer
 };
-// Counts, scans and emits in one launch (k_bin).
-cudaError_t launch_bin(const BinArgs& a, cudaStream_t s);
+// Counts each slot's tiles, stages its entries and accumulates the histograms
+// (k_bin_count); the caller then scans `offsets` in place (launch_scan_u32,
+// total -> fc->entries) and places the staged entries (launch_bin_place).
+cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s);
+cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s);
 // Per-tile [start, end) from sorted words: tile = word >> shift, over
 // min(*n_ptr, capacity) words. ranges zeroed.
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,

@@ -21,7 +21,7 @@
 // the same time) race on it and must be serialised by the caller.
 #include <mutex>
 
-#include "../../include/cgs.h"
+#include "cgs.h"
 #include "kernels.h"
 
 namespace cgs {

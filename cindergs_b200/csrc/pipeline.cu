@@ -26,7 +26,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cgs.h"
+#include "cgs.h"
 #include "kernels.h"
 
 using namespace cgs;
@@ -92,11 +92,12 @@ constexpr int kMaxMarks = 24;     // profiled launches per frame
 // Scratch layout of a frame (one memset): counters | deform look-back |
 // binning look-back | radix histograms | radix tile counters.
 struct ScratchLayout {
-  size_t def, bin, hist, rtiles, shist, bytes;
+  size_t def, bin, btile, hist, rtiles, shist, bytes;
   ScratchLayout(uint32_t n, uint32_t mn) {
     def = 256;
-    bin = def + ((size_t)(n + 255) / 256) * 8 + 256;
-    hist = bin + ((size_t)(mn + 255) / 256) * 8 + 256;
+    bin = def + ((size_t)(n + 255) / 256) * 8 + 256;      // offsets scan look-back
+    btile = bin + ((size_t)(mn + 4095) / 4096) * 8 + 256;  // staging start / count per 32 slots
+    hist = btile + ((size_t)(mn + 31) / 32) * 8 + 256;
     rtiles = hist + 8 * 256 * 4;  // [0, 32): entry passes; [32, 40): splat passes
     shist = rtiles + 256;         // splat depth-key histograms, 4 passes x 256
     bytes = shist + 4 * 256 * 4;
@@ -336,11 +337,14 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.tiles_x = d.tiles_x;
   b.tiles_y = d.tiles_y;
   b.offsets = ctx->offsets.as<uint32_t>();
-  b.status = (unsigned long long*)(sc + L.bin);
+  b.tile_stage = (uint32_t*)(sc + L.btile);
+  b.tile_count = b.tile_stage + (d.max_n + 31) / 32;
   b.fc = fc;
   b.key64 = d.key64;
-  b.depth_base_bits = d.depth_base_bits;
   b.depth_bits = d.depth_bits;
+  b.stage_keys = ctx->keys[1].as<uint32_t>();
+  b.stage_depths = d.key64 ? ctx->depths[1].as<uint32_t>() : nullptr;
+  b.stage_ids = ctx->ids[1].as<uint32_t>();
   b.keys = ctx->keys[0].as<uint32_t>();
   b.depths = d.key64 ? ctx->depths[0].as<uint32_t>() : nullptr;
   b.ids = ctx->ids[0].as<uint32_t>();
@@ -348,8 +352,14 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.radix_bits = d.radix_bits;
   b.tile_bits = d.tile_bits;
   b.entry_cap = ctx->entry_cap;
+  // count + stage, scan of the per-slot counts (-> first entries, entry
+  // total), placement of the staged ranges
   ctx->kbegin(CGS_K_BIN);
-  CGS_CUDA(launch_bin(b, s), "bin launch");
+  CGS_CUDA(launch_bin_count(b, s), "bin count launch");
+  CGS_CUDA(launch_scan_u32(b.offsets, b.offsets, d.max_n, &fc->entries,
+                           (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
+           "offsets scan launch");
+  CGS_CUDA(launch_bin_place(b, s), "bin place launch");
   ctx->kend();
   const uint32_t* n_ptr = &fc->entries;
   *passes = sort_passes(d.tile_bits, d.radix_bits);
@@ -493,6 +503,7 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       kp.ms[p.kid[c]] += ms;
       kp.launches[p.kid[c]] += p.kid[c] == CGS_K_RADIX_SORT   ? p.sort_passes
                                : p.kid[c] == CGS_K_SPLAT_SORT ? 1u + p.splat_passes
+                               : p.kid[c] == CGS_K_BIN        ? 3u
                                                               : 1u;
     }
     const uint64_t A = p.n + (p.split_possible ? h.split : 0u);
@@ -791,6 +802,8 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
   const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
   if (total_tiles64 > 0xFFFFFFFFull / 2) return ctx->fail(CGS_E_CAPACITY, "viewport too large");
+  if (W >= (1u << 22) || H >= (1u << 22))
+    return ctx->fail(CGS_E_CAPACITY, "viewport wider or taller than 4,194,303 pixels");
 
   // Take a ring slot; the frame that used it last is checked first.
   const int slot = ctx->next_slot;

@@ -18,6 +18,8 @@
 //
 // Compiled with -fmad=false: the ellipse test's quadratic is rounded term by
 // term as in the reference, so counts, offsets and keys are bit-exact.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace cgs {
@@ -25,26 +27,28 @@ namespace {
 
 constexpr int kBinThreads = 256;
 constexpr int kBinWarps = kBinThreads / 32;
+constexpr int kMaskCap = 128;  // stored ballot masks per warp (4,096 candidates)
+constexpr int kHitCap = 736;   // stored hit records per warp (4 blocks fit an SM)
 
-struct WarpSplats {
-  uint32_t base[kBinWarps][32];   // exclusive prefix of candidate counts
-  uint32_t width[kBinWarps][32];  // tile-box width
-  uint32_t magic[kBinWarps][32];  // ceil(2^32 / width): c / width == umulhi(c, magic)
-  uint32_t owner_at[kBinWarps][32];  // lane whose candidates start at a chunk position
-  uint32_t x0[kBinWarps][32];
-  uint32_t y0[kBinWarps][32];
-  float mu_x[kBinWarps][32];
-  float mu_y[kBinWarps][32];
-  float ca[kBinWarps][32];
-  float cb[kBinWarps][32];
-  float cc[kBinWarps][32];
-  float qcut[kBinWarps][32];
+// Per-splat constants of a warp's 32 splats, read by the lane that tests one
+// of the splat's candidate tiles (three 128-bit loads and two 32-bit loads).
+struct BinSplats {
+  double2 rcp[kBinWarps][32]; // RN64(1 / max(c, 1e-12)), RN64(1 / max(a, 1e-12))
+  uint4 box[kBinWarps][32];   // x0, y0, width (tiles), ceil(2^32 / width)
+  float4 geo[kBinWarps][32];  // mu_x, mu_y, -b, 2b
+  float4 con[kBinWarps][32];  // a, c, max(a, 1e-12), max(c, 1e-12)
+  float qlim[kBinWarps][32];  // q_max + 1e-4
+  uint32_t base[kBinWarps][32];  // exclusive prefix of the candidate counts
+  uint32_t dq[kBinWarps][32];    // depth part of the key
+  uint32_t sid[kBinWarps][32];   // splat index
 };
+constexpr size_t kBinSmem = sizeof(BinSplats) + sizeof(uint32_t) * kBinWarps * (2 * kMaskCap + kHitCap) +
+                            sizeof(uint32_t) * 1024;  // + tile-digit histograms (<= 4 x 256)
 
 struct SplatBox {
   bool valid;
   uint32_t x0, x1, y0, y1;
-  float mu_x, mu_y, ca, cb, cc, alpha, tz;
+  float mu_x, mu_y, ca, cb, cc, alpha;
 };
 
 __device__ __forceinline__ uint32_t tile_coord(float v, int32_t hi) {
@@ -58,6 +62,8 @@ __device__ __forceinline__ uint32_t tile_coord(float v, int32_t hi) {
 __device__ __forceinline__ SplatBox load_box(const BinArgs& a, uint32_t s, uint32_t active) {
   SplatBox b;
   b.valid = false;
+  b.x0 = b.x1 = b.y0 = b.y1 = 0;
+  b.mu_x = b.mu_y = b.ca = b.cb = b.cc = b.alpha = 0.0f;
   if (s >= active || a.tiles_x == 0 || a.tiles_y == 0) return b;
   const float4 cc4 = a.recs[s].cc;
   const uint32_t p = __float_as_uint(cc4.w);
@@ -70,7 +76,6 @@ __device__ __forceinline__ SplatBox load_box(const BinArgs& a, uint32_t s, uint3
   b.cb = geo.w;
   b.cc = cc4.x;
   b.alpha = cc4.y;
-  b.tz = cc4.z;
   const int32_t mx = (int32_t)a.tiles_x - 1, my = (int32_t)a.tiles_y - 1;
   b.x0 = tile_coord(b.mu_x - ext_x, mx);
   b.x1 = tile_coord(b.mu_x + ext_x, mx);
@@ -81,24 +86,58 @@ __device__ __forceinline__ SplatBox load_box(const BinArgs& a, uint32_t s, uint3
   return b;
 }
 
-__device__ __forceinline__ bool ellipse_hit(float mu_x, float mu_y, float ca, float cb, float cc,
-                                            float qcut, uint32_t tx, uint32_t ty, uint32_t W,
-                                            uint32_t H) {
-  const uint32_t x_start = tx * 16u, y_start = ty * 16u;
-  if (x_start >= W || y_start >= H) return false;
-  const uint32_t x_end = min(x_start + 15u, W - 1u);
-  const uint32_t y_end = min(y_start + 15u, H - 1u);
-  const float dx0 = ((float)x_start + 0.5f) - mu_x;
-  const float dx1 = ((float)x_end + 0.5f) - mu_x;
-  const float dy0 = ((float)y_start + 0.5f) - mu_y;
-  const float dy1 = ((float)y_end + 0.5f) - mu_y;
+// (float)v + 0.5f for v < 2^22, exactly: 2^23 + v is exact in binary32 and
+// the subtraction of 2^23 - 0.5 is exact (Sterbenz), so the result equals the
+// reference's integer-to-float conversion plus one half without a conversion.
+__device__ __forceinline__ float pixel_center(uint32_t v) {
+  return __int_as_float(0x4B000000u | v) - 8388607.5f;
+}
+
+// n / d correctly rounded to binary32, for d > 0, from y = RN64(1 / d) (one
+// binary64 reciprocal per splat instead of a binary32 division per tile).
+// The binary64 product n * y is within 2^-52 (relative) of n / d. A quotient
+// of two binary32 numbers is never closer than 2^-49 (relative) to a midpoint
+// of two binary32 neighbours in the normal range: if n / d = m (1 + e) with m
+// a midpoint, m = M 2^k with M odd and M >= 2^24, then n - d m is a nonzero
+// multiple of 2^k ulp(d) -- an odd factor of M >= 2^24 cannot divide a 24-bit
+// significand -- so |e| >= 2^-49. Hence n * y and n / d round to the same
+// binary32 value. Results below 2^-125 in magnitude, where the binary32 grid
+// is finer relative to the value than that argument assumes, use the binary32
+// division itself; zero stays a signed zero.
+__device__ __noinline__ float div_ieee(float n, float d) { return n / d; }
+
+__device__ __forceinline__ float div_rcp64(float n, float d, double y) {
+  const double q = (double)n * y;
+  float r = __double2float_rn(q);
+  // a call, so that the compiler cannot turn the rare case into a division
+  // on every lane
+  if (q != 0.0 && fabs(q) < 0x1p-125) r = div_ieee(n, d);
+  return r;
+}
+
+// ellipse_intersects_tile_gpu (binning.rs:37-96) for tile (tx, ty) of the
+// splat's tile box, in the reference's operand order (compiled without FMA
+// contraction): the quadratic form is evaluated at the tile point nearest the
+// centre along x (y minimised, clamped) and along y (x minimised, clamped).
+// The reference's "tile starts outside the viewport" exit never fires for a
+// tile of the clamped box. geo = (mu_x, mu_y, -b, 2b), con = (a, c, max(a,
+// 1e-12), max(c, 1e-12)), rcp = their binary64 reciprocals (c term, a term),
+// qlim = q_max + 1e-4.
+__device__ __forceinline__ bool tile_hit(uint32_t tx, uint32_t ty, uint32_t wm1, uint32_t hm1,
+                                         const float4 geo, const float4 con, const double2 rcp,
+                                         float qlim) {
+  const uint32_t xs = tx << 4, ys = ty << 4;
+  const float dx0 = pixel_center(xs) - geo.x;
+  const float dx1 = pixel_center(min(xs + 15u, wm1)) - geo.x;
+  const float dy0 = pixel_center(ys) - geo.y;
+  const float dy1 = pixel_center(min(ys + 15u, hm1)) - geo.y;
   const float x_near = clampf(0.0f, dx0, dx1);
-  const float y1 = clampf(-cb * x_near / fmaxf(cc, 1e-12f), dy0, dy1);
-  const float q1 = ca * x_near * x_near + 2.0f * cb * x_near * y1 + cc * y1 * y1;
+  const float y1 = clampf(div_rcp64(geo.z * x_near, con.w, rcp.x), dy0, dy1);
+  const float q1 = con.x * x_near * x_near + geo.w * x_near * y1 + con.y * y1 * y1;
   const float y_near = clampf(0.0f, dy0, dy1);
-  const float x2 = clampf(-cb * y_near / fmaxf(ca, 1e-12f), dx0, dx1);
-  const float q2 = ca * x2 * x2 + 2.0f * cb * x2 * y_near + cc * y_near * y_near;
-  return fminf(q1, q2) <= qcut + 1e-4f;
+  const float x2 = clampf(div_rcp64(geo.z * y_near, con.z, rcp.y), dx0, dx1);
+  const float q2 = con.x * x2 * x2 + geo.w * x2 * y_near + con.y * y_near * y_near;
+  return fminf(q1, q2) <= qlim;
 }
 
 __device__ __forceinline__ uint32_t seg_mask(int lo, int hi) {
@@ -109,218 +148,282 @@ __device__ __forceinline__ uint32_t seg_mask(int lo, int hi) {
   return upper & ~lower;
 }
 
-// Stages one warp's splats in shared memory; returns this lane's candidate
-// count and exclusive base, and the warp's total candidate count.
-__device__ __forceinline__ void stage_warp(WarpSplats& ws, int warp, int lane, const SplatBox& b,
-                                           uint32_t& ncand, uint32_t& base, uint32_t& total) {
-  ncand = 0;
-  if (b.valid) ncand = (b.x1 - b.x0 + 1u) * (b.y1 - b.y0 + 1u);
-  uint32_t incl = ncand;
+// Lane of the warp's splat that owns candidate `item`: the last lane whose
+// exclusive candidate prefix is <= item (lanes with no candidates share the
+// next lane's prefix and are skipped by "last").
+__device__ __forceinline__ int find_owner(const uint32_t* base, uint32_t item) {
+  int o = 0;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  base = incl - ncand;
-  total = __shfl_sync(0xffffffffu, incl, 31);
-  ws.base[warp][lane] = base;
-  const uint32_t w = b.valid ? (b.x1 - b.x0 + 1u) : 1u;
-  ws.width[warp][lane] = w;
-  ws.magic[warp][lane] = w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w);
-  ws.x0[warp][lane] = b.x0;
-  ws.y0[warp][lane] = b.y0;
-  ws.mu_x[warp][lane] = b.mu_x;
-  ws.mu_y[warp][lane] = b.mu_y;
-  ws.ca[warp][lane] = b.ca;
-  ws.cb[warp][lane] = b.cb;
-  ws.cc[warp][lane] = b.cc;
-  ws.qcut[warp][lane] = b.valid ? clampf(2.0f * cgs_logf(255.0f * b.alpha), 0.0f, 8.0f) : 0.0f;
-  __syncwarp();
-}
-
-// Owner lane of each lane's candidate in the chunk [chunk, chunk + 32): the
-// starts of the candidate runs that begin inside the chunk are OR-reduced into
-// a position mask; a lane's owner is the run starting at the highest set
-// position not above it, or the run carried over from the previous chunk.
-// `carry` holds that run's lane between chunks (the first run starts at 0).
-__device__ __forceinline__ int chunk_owner(WarpSplats& ws, int warp, int lane, uint32_t chunk,
-                                           uint32_t base, uint32_t ncand, int& carry) {
-  const bool starts = ncand > 0u && base >= chunk && base - chunk < 32u;
-  if (starts) ws.owner_at[warp][base - chunk] = (uint32_t)lane;
-  const uint32_t smask = __reduce_or_sync(0xffffffffu, starts ? (1u << (base - chunk)) : 0u);
-  __syncwarp();
-  const uint32_t upto = smask & ((2u << lane) - 1u);
-  const int o = upto ? (int)ws.owner_at[warp][31 - __clz(upto)] : carry;
-  if (smask) carry = (int)ws.owner_at[warp][31 - __clz(smask)];
-  __syncwarp();
+  for (int step = 16; step >= 1; step >>= 1)
+    if (base[o + step] <= item) o += step;
   return o;
 }
 
-// Tile of candidate `item` of owner lane o (row-major over its tile box).
-__device__ __forceinline__ void candidate_tile(const WarpSplats& ws, int warp, int o, uint32_t item,
-                                               uint32_t& tx, uint32_t& ty) {
-  const uint32_t c = item - ws.base[warp][o];
-  const uint32_t w = ws.width[warp][o];
-  const uint32_t r = w <= 1u ? c : __umulhi(c, ws.magic[warp][o]);
-  tx = ws.x0[warp][o] + (c - r * w);
-  ty = ws.y0[warp][o] + r;
+// Candidate `c` of a splat's tile box (row-major) -> tile coordinates.
+__device__ __forceinline__ void box_tile(const uint4 box, uint32_t c, uint32_t& tx, uint32_t& ty) {
+  const uint32_t r = box.z <= 1u ? c : __umulhi(c, box.w);
+  tx = box.x + (c - r * box.z);
+  ty = box.y + r;
 }
 
-__device__ __forceinline__ bool test_candidate(const WarpSplats& ws, int warp, int o,
-                                               uint32_t item, const BinArgs& a, uint32_t& tile) {
-  uint32_t tx, ty;
-  candidate_tile(ws, warp, o, item, tx, ty);
-  tile = ty * a.tiles_x + tx;
-  return ellipse_hit(ws.mu_x[warp][o], ws.mu_y[warp][o], ws.ca[warp][o], ws.cb[warp][o],
-                     ws.cc[warp][o], ws.qcut[warp][o], tx, ty, a.width, a.height);
-}
-
-// One pass of binning for a block of 256 splats, taken in depth-key order
-// (slot s is splat order_ids[s]; Stage 2's depth keys were radix-sorted
-// stably, so slots run by (depth key, splat index)):
-//   1. counting: every candidate tile of the warp's 32 splats is tested once
-//      (ballot per 32 candidates); the ballot masks are kept in shared memory;
-//   2. block exclusive scan of the per-slot counts, chained across blocks
-//      (decoupled look-back) -> each slot's first entry (written to `offsets`);
-//   3. emission: the masks are walked again, each hit is written at
-//      offset + (its rank inside the splat), row-major as in the reference,
-//      with its 32-bit key (tile << depth_bits | depth_q) or, for more than
-//      65,535 tiles, its (tile, raw depth bits) pair; the digit histograms of
-//      the tile bits are accumulated at the same time.
-// The entries therefore leave this kernel ordered by (depth, splat index), and
-// a stable sort on the tile bits alone yields the reference's (tile, depth,
-// splat index) order: sorting the splats once (N keys) replaces the depth
-// passes over all entries.
-// Entries at or beyond the key-buffer capacity are not written and set the
-// capacity status bit (the host grows the buffers and runs Stage 3 again).
-// The last block writes the frame's entry total.
-constexpr int kMaskCap = 48;  // stored ballot masks per warp (1,536 candidates)
-
+// Binning in depth-key order, part 1 (slot s is splat order_ids[s]; Stage 2's
+// depth keys were radix-sorted stably, so slots run by (depth key, splat
+// index)). Persistent warps: each warp takes 32 consecutive slots at a time
+// from a counter and handles them alone, without waiting for any other warp.
+// The 32 splats' candidate tiles (each splat's tile box, row-major) are
+// concatenated and tested 32 at a time, one per lane, so large and small
+// splats share the lanes evenly.
+//   1. counting: ballot per 32 candidates; the masks, the hits before each
+//      mask, and one record per hit (tile id or candidate index, owner lane)
+//      are kept in shared memory. A slot's count is the number of hits inside
+//      its candidate range, read from the masks, and is written to `offsets`
+//      (scanned in place afterwards).
+//   2. staging: the tile's hits, in candidate order (= the reference's
+//      emission order: splat by splat, row-major), get a contiguous range of
+//      the staging buffers from an atomic counter and are written there with
+//      their 32-bit keys (tile << depth_bits | depth_q) or, beyond 65,535
+//      tiles, (tile, raw depth bits) pairs; the block's digit histograms of
+//      the tile bits are accumulated. Warps with more hits or candidates than
+//      the shared-memory stores hold walk their candidates again for the rest.
+// The staging order of the tiles is whatever the counter gave; k_bin_place
+// moves each tile's range to its scanned offset, which restores the
+// (depth, splat index) order, and a stable sort on the tile bits alone then
+// yields the reference's (tile, depth, splat index) order. Entries at or
+// beyond the buffer capacity are not written and set the capacity status bit
+// (the host grows the buffers and runs Stage 3 again).
 template <bool KEY64>
-__global__ void __launch_bounds__(kBinThreads) k_bin(const BinArgs a) {
-  __shared__ WarpSplats ws;
-  __shared__ uint32_t s_off[kBinWarps][32];
-  __shared__ uint32_t s_dq[kBinWarps][32];
-  __shared__ uint32_t s_sid[kBinWarps][32];
-  __shared__ uint32_t s_carry[kBinWarps][32];
-  __shared__ uint32_t s_masks[kBinWarps][kMaskCap];
-  __shared__ uint32_t s_hist[8 * 256];
-  __shared__ uint32_t s_tile, s_base;
-  __shared__ uint32_t s_warp_sums[32];
+__global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
+  extern __shared__ __align__(16) unsigned char bin_smem[];
+  BinSplats& sp = *reinterpret_cast<BinSplats*>(bin_smem);
+  uint32_t* s_mask = reinterpret_cast<uint32_t*>(bin_smem + sizeof(BinSplats));  // [w][kMaskCap]
+  uint32_t* s_mrun = s_mask + kBinWarps * kMaskCap;  // [w][kMaskCap] hits before mask c
+  uint32_t* s_hits = s_mrun + kBinWarps * kMaskCap;  // [w][kHitCap]
+  uint32_t* s_hist = s_hits + kBinWarps * kHitCap;   // [passes][radix]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
   const uint32_t passes = (a.tile_bits + a.radix_bits - 1u) / a.radix_bits;
   const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
   const uint32_t nbins = passes * radix;
-  if (threadIdx.x == 0) s_tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
+  const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
-  const uint32_t tile = s_tile;
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
-  const uint32_t s = tile * kBinThreads + threadIdx.x;  // slot in depth order
-  uint32_t sid = kInvalid, dq = 0;
-  if (s < active && s < a.max_n) {
-    sid = a.order_ids[s];
-    dq = a.order_keys[s];
-  }
-  const SplatBox b = load_box(a, sid, active);
-  uint32_t ncand, base, total;
-  stage_warp(ws, warp, lane, b, ncand, base, total);
-
-  // 1. count
-  uint32_t count = 0;
-  int carry = 0;
-  for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
-    const uint32_t item = chunk + lane;
-    const int o = chunk_owner(ws, warp, lane, chunk, base, ncand, carry);
-    bool hit = false;
-    if (item < total) {
-      uint32_t t;
-      hit = test_candidate(ws, warp, o, item, a, t);
-    }
-    const uint32_t hits = __ballot_sync(0xffffffffu, hit);
-    if (c < (uint32_t)kMaskCap && lane == 0) s_masks[warp][c] = hits;
-    const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
-    const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
-    count += __popc(hits & seg_mask(lo, hi));
-  }
-
-  // 2. scan
-  uint32_t agg;
-  const uint32_t excl = block_exclusive_sum(count, s_warp_sums, &agg);
-  if (threadIdx.x < 32) {
-    const uint32_t pre = chained_scan_warp(a.status, tile, agg, &a.fc->status);
-    if (threadIdx.x == 0) s_base = pre;
-  }
-  __syncthreads();
-  const uint32_t first = s_base + excl;
-  if (s < a.max_n) a.offsets[s] = first;
-  const uint32_t num_tiles = (a.max_n + kBinThreads - 1) / kBinThreads;
-  if (tile == num_tiles - 1 && threadIdx.x == 0) {
-    const uint32_t e = s_base + agg;
-    a.fc->entries = e;
-    if (e > a.entry_cap) atomicOr(&a.fc->status, kStatusCapacity);
-  }
-
-  // 3. emit
-  s_off[warp][lane] = first;
-  s_dq[warp][lane] = dq;
-  s_sid[warp][lane] = sid;
-  s_carry[warp][lane] = 0u;
-  __syncwarp();
+  const uint32_t num_tiles = (a.max_n + 31u) / 32u;
+  const uint32_t* wbase = sp.base[warp];
+  uint32_t* wmask = s_mask + warp * kMaskCap;
+  uint32_t* wmrun = s_mrun + warp * kMaskCap;
+  uint32_t* whits = s_hits + warp * kHitCap;
   const uint32_t cap = a.entry_cap;
   bool overflow = false;
-  carry = 0;
-  for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
-    const uint32_t item = chunk + lane;
-    const int o = chunk_owner(ws, warp, lane, chunk, base, ncand, carry);
-    uint32_t hits;
-    uint32_t tile_id = 0;
-    if (c < (uint32_t)kMaskCap) {
-      hits = s_masks[warp][c];
-      if ((hits >> lane) & 1u) {
+
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= num_tiles) break;
+    const uint32_t s = tile * 32u + lane;  // slot in depth order
+    uint32_t sid = kInvalid, dq = 0;
+    if (s < active && s < a.max_n) {
+      sid = a.order_ids[s];
+      dq = a.order_keys[s];
+    }
+    const SplatBox b = load_box(a, sid, active);
+
+    // Stage the warp's splats.
+    const uint32_t ncand = b.valid ? (b.x1 - b.x0 + 1u) * (b.y1 - b.y0 + 1u) : 0u;
+    uint32_t incl = ncand;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t base = incl - ncand;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();  // the previous tile's readers are done with the warp's shared memory
+    {
+      const uint32_t w = b.valid ? (b.x1 - b.x0 + 1u) : 1u;
+      const float ca_ = fmaxf(b.ca, 1e-12f), cc_ = fmaxf(b.cc, 1e-12f);
+      sp.box[warp][lane] =
+          make_uint4(b.x0, b.y0, w, w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w));
+      sp.geo[warp][lane] = make_float4(b.mu_x, b.mu_y, -b.cb, 2.0f * b.cb);
+      sp.con[warp][lane] = make_float4(b.ca, b.cc, ca_, cc_);
+      sp.rcp[warp][lane] = make_double2(1.0 / (double)cc_, 1.0 / (double)ca_);
+      sp.qlim[warp][lane] =
+          (b.valid ? clampf(2.0f * cgs_logf(255.0f * b.alpha), 0.0f, 8.0f) : 0.0f) + 1e-4f;
+      sp.base[warp][lane] = base;
+      sp.dq[warp][lane] = dq;
+      sp.sid[warp][lane] = sid;
+    }
+    __syncwarp();
+    const bool big = total > (uint32_t)kMaskCap * 32u;  // warp-uniform
+
+    // 1. count
+    uint32_t run = 0;  // hits before the current chunk (warp-uniform)
+    uint32_t own = 0;  // this lane's hits, accumulated only when `big`
+    for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
+      const uint32_t item = chunk + lane;
+      bool hit = false;
+      uint32_t rec = 0;
+      if (item < total) {
+        const int o = find_owner(wbase, item);
+        const uint32_t ci = item - wbase[o];
         uint32_t tx, ty;
-        candidate_tile(ws, warp, o, item, tx, ty);
+        box_tile(sp.box[warp][o], ci, tx, ty);
+        hit = tile_hit(tx, ty, wm1, hm1, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
+                       sp.qlim[warp][o]);
+        rec = ((KEY64 ? ci : ty * a.tiles_x + tx) << 5) | (uint32_t)o;
+      }
+      const uint32_t hits = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0 && c < (uint32_t)kMaskCap) {
+        wmask[c] = hits;
+        wmrun[c] = run;
+      }
+      if (hit) {
+        const uint32_t k = run + __popc(hits & lanemask_lt());
+        if (k < (uint32_t)kHitCap) whits[k] = rec;
+      }
+      if (big) {
+        const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
+        const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
+        own += __popc(hits & seg_mask(lo, hi));
+      }
+      run += __popc(hits);
+    }
+    __syncwarp();
+    uint32_t count = own;
+    if (!big) {
+      // hits before this lane's first candidate, from the stored masks
+      uint32_t before = run;
+      if (base < total) {
+        const uint32_t c = base >> 5;
+        before = wmrun[c] + __popc(wmask[c] & ((1u << (base & 31u)) - 1u));
+      }
+      const uint32_t next = __shfl_down_sync(0xffffffffu, before, 1);
+      count = (lane == 31 ? run : next) - before;
+    }
+    if (s < a.max_n) a.offsets[s] = count;
+
+    // 2. stage
+    uint32_t sbase = 0;
+    if (lane == 0) {
+      sbase = run ? atomicAdd(&a.fc->tile_ctr[2], run) : 0u;
+      a.tile_stage[tile] = sbase;
+      a.tile_count[tile] = run;
+    }
+    sbase = __shfl_sync(0xffffffffu, sbase, 0);
+    auto put = [&](uint32_t k, uint32_t tile_id, int o) {
+      const uint32_t pos = sbase + k;
+      if (pos >= cap) {
+        overflow = true;
+        return;
+      }
+      const uint32_t d = sp.dq[warp][o];
+      uint32_t word;
+      if (KEY64) {
+        word = tile_id;
+        a.stage_depths[pos] = d;
+      } else {
+        word = a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d);
+      }
+      a.stage_keys[pos] = word;
+      a.stage_ids[pos] = sp.sid[warp][o];
+      for (uint32_t p = 0; p < passes; ++p)
+        atomicAdd(&s_hist[p * radix + ((word >> (tshift + p * a.radix_bits)) & rmask)], 1u);
+    };
+    const uint32_t stored = min(run, (uint32_t)kHitCap);
+    for (uint32_t k = lane; k < stored; k += 32) {
+      const uint32_t v = whits[k];
+      const int o = (int)(v & 31u);
+      uint32_t tile_id = v >> 5;
+      if (KEY64) {
+        uint32_t tx, ty;
+        box_tile(sp.box[warp][o], tile_id, tx, ty);
         tile_id = ty * a.tiles_x + tx;
       }
-    } else {
-      bool hit = false;
-      if (item < total) hit = test_candidate(ws, warp, o, item, a, tile_id);
-      hits = __ballot_sync(0xffffffffu, hit);
+      put(k, tile_id, o);
     }
-    if ((hits >> lane) & 1u) {
-      const uint32_t ob = ws.base[warp][o];
-      const int sstart = ob > chunk ? (int)(ob - chunk) : 0;
-      const uint32_t below = hits & lanemask_lt() & ~seg_mask(0, sstart);
-      const uint32_t pos = s_off[warp][o] + s_carry[warp][o] + __popc(below);
-      const uint32_t osid = s_sid[warp][o];
-      if (pos < cap) {
-        uint32_t word;
-        if (KEY64) {
-          word = tile_id;
-          a.depths[pos] = s_dq[warp][o];
+    if (run > (uint32_t)kHitCap) {
+      // Hits beyond the stored records: walk the candidates again, using the
+      // stored masks where there are any.
+      uint32_t hrun = 0;
+      for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
+        uint32_t hits;
+        const uint32_t item = chunk + lane;
+        if (c < (uint32_t)kMaskCap) {
+          hits = wmask[c];
+          hrun = wmrun[c];
+          if (hrun + __popc(hits) <= (uint32_t)kHitCap) {
+            hrun += __popc(hits);
+            continue;
+          }
         } else {
-          word = a.depth_bits >= 32u ? s_dq[warp][o] : ((tile_id << a.depth_bits) | s_dq[warp][o]);
+          bool hit = false;
+          if (item < total) {
+            const int o = find_owner(wbase, item);
+            uint32_t tx, ty;
+            box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
+            hit = tile_hit(tx, ty, wm1, hm1, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
+                           sp.qlim[warp][o]);
+          }
+          hits = __ballot_sync(0xffffffffu, hit);
         }
-        a.keys[pos] = word;
-        a.ids[pos] = osid;
-        for (uint32_t p = 0; p < passes; ++p)
-          atomicAdd(&s_hist[p * radix + ((word >> (tshift + p * a.radix_bits)) & rmask)], 1u);
-      } else {
-        overflow = true;
+        const uint32_t k = hrun + __popc(hits & lanemask_lt());
+        if (((hits >> lane) & 1u) && k >= (uint32_t)kHitCap) {
+          const int o = find_owner(wbase, item);
+          uint32_t tx, ty;
+          box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
+          put(k, ty * a.tiles_x + tx, o);
+        }
+        hrun += __popc(hits);
       }
     }
-    __syncwarp();
-    const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
-    const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
-    s_carry[warp][lane] += __popc(hits & seg_mask(lo, hi));
-    __syncwarp();
   }
   if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
     const uint32_t v = s_hist[k];
     if (v) atomicAdd(&a.hist[k], v);
+  }
+}
+
+// Binning, part 3: each 32-slot tile's staged range moves to the tile's first
+// entry (the scanned offset of its first slot), one warp per tile, coalesced
+// on both sides. Ranges that reach past the buffers were not staged (the
+// capacity bit is set) and are clamped here.
+template <bool KEY64>
+__global__ void __launch_bounds__(256) k_bin_place(const BinArgs a) {
+  const uint32_t num_tiles = (a.max_n + 31u) / 32u;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  const uint32_t cap = a.entry_cap;
+  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < num_tiles; t += warps) {
+    const uint32_t n = a.tile_count[t];
+    if (n == 0) continue;
+    const uint32_t src = a.tile_stage[t];
+    const uint32_t dst = a.offsets[32u * t];
+    if (src >= cap || dst >= cap) continue;
+    const uint32_t m = min(n, min(cap - src, cap - dst));
+    for (uint32_t k0 = 0; k0 < m; k0 += 128) {  // four loads in flight per lane and array
+      uint32_t kk[4], ii[4], dd[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t k = k0 + 32u * u + lane;
+        if (k < m) {
+          kk[u] = __ldcs(a.stage_keys + src + k);
+          ii[u] = __ldcs(a.stage_ids + src + k);
+          if (KEY64) dd[u] = __ldcs(a.stage_depths + src + k);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t k = k0 + 32u * u + lane;
+        if (k < m) {
+          a.keys[dst + k] = kk[u];
+          a.ids[dst + k] = ii[u];
+          if (KEY64) a.depths[dst + k] = dd[u];
+        }
+      }
+    }
   }
 }
 
@@ -409,13 +512,43 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_u32(const uint32_t* __res
 
 }  // namespace
 
-cudaError_t launch_bin(const BinArgs& a, cudaStream_t s) {
+// Persistent grid: as many blocks as fit on the device at once (at most one
+// warp per 32-slot tile).
+template <bool KEY64>
+cudaError_t launch_bin_count_t(const BinArgs& a, cudaStream_t s) {
+  static int resident = 0;  // blocks of k_bin_count<KEY64> the device runs at once
+  if (resident == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_bin_count<KEY64>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBinSmem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_count<KEY64>, kBinThreads,
+                                                           kBinSmem)) != cudaSuccess)
+      return e;
+    resident = std::max(1, sms * std::max(per_sm, 1));
+  }
+  const uint32_t tiles = (a.max_n + 31u) / 32u;
+  const uint32_t blocks = std::min<uint32_t>((uint32_t)resident, (tiles + kBinWarps - 1) / kBinWarps);
+  k_bin_count<KEY64><<<blocks, kBinThreads, kBinSmem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
-  const uint32_t blocks = (a.max_n + kBinThreads - 1) / kBinThreads;
+  if (a.width >= (1u << 22) || a.height >= (1u << 22)) return cudaErrorInvalidValue;
+  return a.key64 ? launch_bin_count_t<true>(a, s) : launch_bin_count_t<false>(a, s);
+}
+
+cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s) {
+  if (a.max_n == 0) return cudaSuccess;
+  const uint32_t tiles = (a.max_n + 31u) / 32u;
+  const uint32_t blocks = std::min<uint32_t>(148u * 8u, (tiles + 7u) / 8u);
   if (a.key64)
-    k_bin<true><<<blocks, kBinThreads, 0, s>>>(a);
+    k_bin_place<true><<<blocks, 256, 0, s>>>(a);
   else
-    k_bin<false><<<blocks, kBinThreads, 0, s>>>(a);
+    k_bin_place<false><<<blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

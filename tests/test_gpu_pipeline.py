@@ -113,6 +113,25 @@ def test_64bit_key_path_8k(gpu_state):
     check_image(g, o)
 
 
+@pytest.mark.parametrize("wh", [(1920, 1080), (7680, 4320)])
+def test_huge_splats(gpu_state, wh):
+    """Every 37th splat scaled 20x: tile boxes of up to 8,160 (1080p) and
+    16,641 (8K, 64-bit keys) tiles, so binning warps exceed their stored
+    ballot masks (4,096 candidates) and hit records (1,024) and re-walk their
+    candidates for the rest."""
+    w, h = wh
+    scene = random_scene(3000, seed=21)
+    scene.covariances_3d[::37] *= 400.0
+    cam = config0_camera(w, h)
+    comp = compositor(w, h, cam, deg=1)
+    t, g, o = run_both(gpu_state, scene, cam, comp)
+    counts = np.diff(np.append(o["offsets"], o["entries"]))
+    assert counts.max() > 4096
+    assert t.total_tile_entries == o["entries"]
+    assert_stage23_exact(g, o, key64=t.used_64bit_keys)
+    check_image(g, o)
+
+
 def test_stage3_cache_and_repeatability(gpu_state):
     scene = random_scene(30_000, seed=7)
     cam = config0_camera(320, 240)
