@@ -38,6 +38,21 @@ UNIT = "views/s"
 FALLBACK_HBM_GBS = 6650.0
 
 
+def radix_digits(args) -> str:
+    """Digit widths of the entry sort's passes over the tile bits, e.g. "7+6"."""
+    tiles = ((args.width + 15) // 16) * ((args.height + 15) // 16)
+    tile_bits = max(1, (tiles - 1).bit_length())
+    rb = args.radix_bits
+    if rb == 0:
+        passes = (tile_bits + 7) // 8
+        rb = max(4, -(-tile_bits // passes))
+    widths, left = [], tile_bits
+    while left > 0:
+        widths.append(min(rb, left))
+        left -= rb
+    return "+".join(str(w) for w in widths)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -48,6 +63,10 @@ def parse():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--entry-sort", type=int, default=0,
+                    help="tile-entry sort: 0 auto, 1 radix passes, 2 one-pass tile transpose")
+    ap.add_argument("--radix-bits", type=int, default=0,
+                    help="entry-sort digit width (0 = balanced digits of at most 8 bits)")
     return ap.parse_args()
 
 
@@ -156,7 +175,8 @@ def config_dict(args, wl, world):
     return {"workload": "tet-cage deform + render, orbit camera",
             "gaussians": args.gaussians, "width": args.width, "height": args.height,
             "cage": "5x5x5 cubes x 6 tets (750 tets, 216 vertices), springs k=40 c=4 dt=1/60",
-            "sh_degree": 3, "keys": "32-bit tile|depth", "radix_bits": 8,
+            "sh_degree": 3, "keys": "32-bit tile|depth", "radix_digits": radix_digits(args),
+            "entry_sort": ["auto (radix)", "radix", "tile transpose"][args.entry_sort],
             "l2": "inputs larger than L2 (resident scene 255 MB + 26M tile entries)",
             "parallelism": f"replicas x{world} (views sharded, no exchange)"}
 
@@ -217,7 +237,8 @@ def run_ours(args):
         return st.execute_frame_gpu(wl.scene, cages, cam, wl.compositor(cam),
                                     wl.strain_split_threshold, wl.mip_filter_3d_var,
                                     1.0 / 255.0, 0.5, profile_stages=profile,
-                                    stage_timings=timings)
+                                    stage_timings=timings, radix_bits=args.radix_bits,
+                                    entry_sort=args.entry_sort)
 
     for _ in range(max(args.warmup, 3)):
         render()
@@ -268,7 +289,8 @@ def run_ours(args):
             "cgs_cage_vertices_update")
         cam_c = wl.compositor(cam)
         st.execute_frame_gpu(wl.scene, cages, cam, cam_c, wl.strain_split_threshold,
-                             wl.mip_filter_3d_var, 1.0 / 255.0, 0.5)
+                             wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, radix_bits=args.radix_bits,
+                             entry_sort=args.entry_sort)
         st._check(st._lib.cgs_readback_rgba8(st.handle, ctypes.c_void_p(out_np.ctypes.data),
                                              args.width, args.height), "cgs_readback_rgba8")
     e2e_end.record(stream)

@@ -69,7 +69,7 @@ class CgsFrameParams(ctypes.Structure):
     _fields_ = [("strain_split_threshold", ctypes.c_float), ("mip_filter_3d_var", ctypes.c_float),
                 ("min_opacity", ctypes.c_float), ("min_radius_px", ctypes.c_float),
                 ("profile_stages", _i32), ("force_stage3", _i32), ("write_f32", _i32),
-                ("radix_bits", _i32)]
+                ("radix_bits", _i32), ("entry_sort", _i32)]
 
 
 class CgsStageTimings(ctypes.Structure):
@@ -81,7 +81,9 @@ class CgsStageTimings(ctypes.Structure):
                 ("total_tile_entries", _u64)]
 
 
-KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "radix_sort",
+SORT_AUTO, SORT_RADIX, SORT_TRANSPOSE = 0, 1, 2
+
+KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "entry_sort",
                 "tile_ranges", "composite", "splat_sort"]
 KERNEL_COUNT = len(KERNEL_NAMES)
 

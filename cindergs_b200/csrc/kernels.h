@@ -118,12 +118,47 @@ struct BinArgs {
   uint32_t radix_bits;
   uint32_t tile_bits;           // tile id bits (the entry sort's key bits)
   uint32_t entry_cap;           // capacity of every entry buffer
+  // Record mode (the tile transpose): stage one word per hit, tile << 5 |
+  // slot lane, instead of keys and ids; no histograms. Each 32-slot tile
+  // stages one run per group of 2^group_shift screen tiles, so tile_stage /
+  // tile_count are [ceil(max_n/32)][groups].
+  int records;
+  uint32_t groups;              // <= 8
+  uint32_t group_shift;
 };
 // Counts each slot's tiles, stages its entries and accumulates the histograms
 // (k_bin_count); the caller then scans `offsets` in place (launch_scan_u32,
 // total -> fc->entries) and places the staged entries (launch_bin_place).
 cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s);
 cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s);
+// Tile transpose (the entry sort when the tiles fit shared memory): a
+// one-pass stable counting sort of the staged records by tile. Chunk k is the
+// 32-slot tiles [k * chunk_wtiles, (k + 1) * chunk_wtiles); warp w of a chunk
+// block owns the w-th eighth of them.
+struct TransposeArgs {
+  const uint32_t* records;      // staged tile << 5 | slot lane
+  const uint32_t* tile_stage;   // [num_wtiles][groups] staging start of each run
+  const uint32_t* tile_count;   // [num_wtiles][groups] records of each run
+  const uint32_t* order_ids;    // slot -> splat index
+  uint32_t num_wtiles;
+  uint32_t chunk_wtiles;        // multiple of 8, at most 2040
+  uint32_t num_chunks;
+  uint32_t num_tiles;           // screen tiles
+  uint32_t groups;              // tile groups (runs per 32-slot tile)
+  uint32_t group_tiles;         // screen tiles per group (a power of two)
+  uint32_t* cmat;               // [num_tiles][num_chunks] counts -> first entries (in place)
+  uint32_t* totals;             // [num_tiles] entries per tile, zeroed
+  const uint32_t* tile_base;    // [num_tiles] exclusive scan of totals
+  uint32_t* ranges;             // [num_tiles] (start, end), (0, 0) when empty
+  uint32_t* ids_out;            // [capacity] sorted splat indices
+  uint32_t capacity;
+  uint32_t* status_word;
+};
+constexpr uint32_t kTransposeGroupTiles = 2048;  // screen tiles per group (2^11)
+cudaError_t launch_chunk_counts(const TransposeArgs& a, cudaStream_t s);
+cudaError_t launch_column_scan(const TransposeArgs& a, cudaStream_t s);
+cudaError_t launch_chunk_place(const TransposeArgs& a, cudaStream_t s);
+
 // Per-tile [start, end) from sorted words: tile = word >> shift, over
 // min(*n_ptr, capacity) words. ranges zeroed.
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
@@ -144,8 +179,9 @@ struct SortArgs {
   uint32_t capacity;     // elements the buffers hold; grid is sized for it
   uint32_t first_bit;    // lowest key bit to sort on
   uint32_t num_bits;     // bits to sort on (from first_bit)
-  uint32_t radix_bits;   // 4 or 8
+  uint32_t radix_bits;   // digit width, 4..8
   uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
+                         // (turned into exclusive bases in place by the sort)
   uint32_t* status;      // [passes][tiles][radix] zeroed (when status2 is null)
   uint32_t* status2[2];  // optional: two [tiles][radix] look-back buffers used
                          // alternately; each pass clears the one it does not

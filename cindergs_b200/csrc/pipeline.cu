@@ -20,6 +20,7 @@
 // bounded device waits are reported as CGS_E_TIMEOUT.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -76,6 +77,7 @@ struct FrameDesc {
   uint32_t n = 0, max_n = 0;
   bool split_possible = false, key64 = false, write_f32 = false;
   uint32_t tile_bits = 0, depth_bits = 0, sort_bits = 0, radix_bits = 8, depth_base_bits = 0;
+  int entry_sort = CGS_SORT_AUTO;
   float bg[4] = {0, 0, 0, 1};
 };
 
@@ -91,16 +93,24 @@ constexpr int kMaxMarks = 24;     // profiled launches per frame
 
 // Scratch layout of a frame (one memset): counters | deform look-back |
 // binning look-back | radix histograms | radix tile counters.
+// Screen tiles up to which the entries are sorted by the one-pass tile
+// transpose (its per-chunk tile counts fit shared memory); beyond, by radix
+// passes.
+constexpr uint32_t kTransposeMaxTiles = 8 * kTransposeGroupTiles;
+
 struct ScratchLayout {
-  size_t def, bin, btile, hist, rtiles, shist, bytes;
+  size_t def, bin, btile, hist, rtiles, shist, ttot, tbase, tscan, bytes;
   ScratchLayout(uint32_t n, uint32_t mn) {
     def = 256;
     bin = def + ((size_t)(n + 255) / 256) * 8 + 256;      // offsets scan look-back
     btile = bin + ((size_t)(mn + 4095) / 4096) * 8 + 256;  // staging start / count per 32 slots
-    hist = btile + ((size_t)(mn + 31) / 32) * 8 + 256;
+    hist = btile + ((size_t)(mn + 31) / 32) * 8 * 8 + 256;  // (x 8 tile groups)
     rtiles = hist + 8 * 256 * 4;  // [0, 32): entry passes; [32, 40): splat passes
     shist = rtiles + 256;         // splat depth-key histograms, 4 passes x 256
-    bytes = shist + 4 * 256 * 4;
+    ttot = shist + 4 * 256 * 4;   // tile transpose: entries per screen tile
+    tbase = ttot + (size_t)kTransposeMaxTiles * 4;   // first entry per screen tile
+    tscan = tbase + (size_t)kTransposeMaxTiles * 4;  // look-back of that scan
+    bytes = tscan + ((kTransposeMaxTiles + 4095) / 4096) * 8 + 256;
   }
 };
 constexpr uint32_t kSplatSortTileCtr = 32;
@@ -136,6 +146,8 @@ struct cgs_ctx {
   uint32_t splat_cap = 0;  // slots those buffers hold; fixed between reallocations
   int splat_parity = 0;
   int s3_order_src = 0;    // buffer holding the latest Stage 3's splat order
+  bool s3_transpose = false;  // the latest Stage 3 sorted by the tile transpose
+  DevBuf cmat;             // tile transpose: [tiles][chunks] counts / first entries
   uint32_t entry_cap = 0;       // capacity of the key/id buffers (entries)
   uint32_t radix_lb_tiles = 0;  // tiles the radix look-back buffers cover
   uint32_t radix_lb_bits = 0;
@@ -158,6 +170,7 @@ struct cgs_ctx {
     bool used = false, stage3_ran = false, profiled = false, need_deform = false;
     bool split_possible = false, key64 = false;
     uint32_t n = 0, cap = 0, sort_passes = 0, splat_passes = 0, total_tiles = 0, W = 0, H = 0;
+    uint32_t bin_launches = 0, sort_launches = 0;
     bool write_f32 = false;
     cudaEvent_t done = nullptr;
     cudaEvent_t kev[2 * kMaxMarks] = {};
@@ -286,16 +299,22 @@ int ensure_splat_buffers(cgs_ctx* ctx, uint32_t mn) {
 // *result_src receives the buffer holding the sorted lists; *passes and
 // *splat_passes the number of radix passes over entries and splats.
 int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int* result_src,
-                   uint32_t* passes, uint32_t* splat_passes, bool sort_splats) {
+                   uint32_t* passes, uint32_t* splat_passes, bool sort_splats,
+                   uint32_t* bin_launches = nullptr, uint32_t* sort_launches = nullptr) {
   cudaStream_t s = ctx->stream;
   char* sc = ctx->scratch.as<char>();
   FrameCounters* fc = (FrameCounters*)sc;
   uint32_t* d_split = ctx->persist.as<uint32_t>();
   uint32_t* d_hist = (uint32_t*)(sc + L.hist);
   uint32_t* rtiles = (uint32_t*)(sc + L.rtiles);
-  ctx->kbegin(CGS_K_CLEAR);
-  CGS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0, (size_t)d.total_tiles * 8, s), "clear ranges");
-  ctx->kend();
+  const bool transpose =
+      d.entry_sort == CGS_SORT_TRANSPOSE && !d.key64 && d.total_tiles <= kTransposeMaxTiles;
+  ctx->s3_transpose = transpose;
+  if (!transpose) {
+    ctx->kbegin(CGS_K_CLEAR);
+    CGS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0, (size_t)d.total_tiles * 8, s), "clear ranges");
+    ctx->kend();
+  }
   const uint32_t dbits = d.key64 ? 32u : d.depth_bits;
   *splat_passes = 0;
   if (sort_splats) {
@@ -338,7 +357,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.tiles_y = d.tiles_y;
   b.offsets = ctx->offsets.as<uint32_t>();
   b.tile_stage = (uint32_t*)(sc + L.btile);
-  b.tile_count = b.tile_stage + (d.max_n + 31) / 32;
+  b.tile_count = b.tile_stage + (size_t)8 * ((d.max_n + 31) / 32);
   b.fc = fc;
   b.key64 = d.key64;
   b.depth_bits = d.depth_bits;
@@ -352,15 +371,57 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.radix_bits = d.radix_bits;
   b.tile_bits = d.tile_bits;
   b.entry_cap = ctx->entry_cap;
+  b.records = transpose ? 1 : 0;
+  b.group_shift = 11;  // kTransposeGroupTiles = 2^11
+  b.groups = transpose ? (d.total_tiles + kTransposeGroupTiles - 1) / kTransposeGroupTiles : 1u;
   // count + stage, scan of the per-slot counts (-> first entries, entry
-  // total), placement of the staged ranges
+  // total), and for the radix path the placement of the staged ranges
   ctx->kbegin(CGS_K_BIN);
   CGS_CUDA(launch_bin_count(b, s), "bin count launch");
   CGS_CUDA(launch_scan_u32(b.offsets, b.offsets, d.max_n, &fc->entries,
                            (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
            "offsets scan launch");
-  CGS_CUDA(launch_bin_place(b, s), "bin place launch");
+  if (!transpose) CGS_CUDA(launch_bin_place(b, s), "bin place launch");
   ctx->kend();
+  if (bin_launches) *bin_launches = transpose ? 2u : 3u;
+  if (transpose) {
+    // one-pass stable counting sort of the staged records by tile
+    const uint32_t nwt = (d.max_n + 31) / 32;
+    const uint32_t target = 296;  // chunks: two per SM
+    uint32_t m = 8 * ((nwt + 8 * target - 1) / (8 * target));
+    m = std::min<uint32_t>(std::max<uint32_t>(m, 8u), 2040u);
+    TransposeArgs ta{};
+    ta.records = ctx->keys[1].as<uint32_t>();
+    ta.tile_stage = b.tile_stage;
+    ta.tile_count = b.tile_count;
+    ta.order_ids = b.order_ids;
+    ta.num_wtiles = nwt;
+    ta.chunk_wtiles = m;
+    ta.num_chunks = (nwt + m - 1) / m;
+    ta.num_tiles = d.total_tiles;
+    ta.groups = b.groups;
+    ta.group_tiles = kTransposeGroupTiles;
+    CGS_TRY(ctx->ensure(ctx->cmat, (size_t)d.total_tiles * ta.num_chunks * 4, "tile transpose counts"));
+    ta.cmat = ctx->cmat.as<uint32_t>();
+    ta.totals = (uint32_t*)(sc + L.ttot);
+    ta.tile_base = (uint32_t*)(sc + L.tbase);
+    ta.ranges = ctx->ranges.as<uint32_t>();
+    ta.ids_out = ctx->ids[0].as<uint32_t>();
+    ta.capacity = ctx->entry_cap;
+    ta.status_word = &fc->status;
+    *passes = 0;
+    ctx->kbegin(CGS_K_ENTRY_SORT);
+    CGS_CUDA(launch_chunk_counts(ta, s), "chunk counts launch");
+    CGS_CUDA(launch_scan_u32(ta.totals, (uint32_t*)(sc + L.tbase), d.total_tiles, &fc->tile_ctr[5],
+                             (unsigned long long*)(sc + L.tscan), &fc->tile_ctr[4], &fc->status, s),
+             "tile totals scan launch");
+    CGS_CUDA(launch_column_scan(ta, s), "column scan launch");
+    CGS_CUDA(launch_chunk_place(ta, s), "chunk place launch");
+    ctx->kend();
+    if (sort_launches) *sort_launches = 4;
+    *result_src = 0;
+    return CGS_OK;
+  }
   const uint32_t* n_ptr = &fc->entries;
   *passes = sort_passes(d.tile_bits, d.radix_bits);
   // Entries arrive in (depth, splat) order; a stable sort on the tile bits
@@ -388,8 +449,9 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.status_word = &fc->status;
   sa.hist = d_hist;
   sa.src = 0;
-  ctx->kbegin(CGS_K_RADIX_SORT);
+  ctx->kbegin(CGS_K_ENTRY_SORT);
   CGS_CUDA(run_radix_sort(sa, result_src, s), "radix sort");
+  if (sort_launches) *sort_launches = 1 + *passes;
   ctx->kend();
   ctx->kbegin(CGS_K_TILE_RANGES);
   CGS_CUDA(launch_tile_ranges(ctx->keys[*result_src].as<uint32_t>(), d.key64 ? 0u : d.depth_bits,
@@ -501,9 +563,9 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, p.kev[2 * c], p.kev[2 * c + 1]);
       kp.ms[p.kid[c]] += ms;
-      kp.launches[p.kid[c]] += p.kid[c] == CGS_K_RADIX_SORT   ? p.sort_passes
+      kp.launches[p.kid[c]] += p.kid[c] == CGS_K_ENTRY_SORT   ? p.sort_launches
                                : p.kid[c] == CGS_K_SPLAT_SORT ? 1u + p.splat_passes
-                               : p.kid[c] == CGS_K_BIN        ? 3u
+                               : p.kid[c] == CGS_K_BIN        ? p.bin_launches
                                                               : 1u;
     }
     const uint64_t A = p.n + (p.split_possible ? h.split : 0u);
@@ -517,8 +579,14 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
     if (p.stage3_ran) {
       kp.alg_bytes[CGS_K_SPLAT_SORT] += A * 4 + (uint64_t)p.splat_passes * A * 16;
       kp.alg_bytes[CGS_K_BIN] += A * 44 + E * (p.key64 ? 12 : 8);
-      kp.alg_bytes[CGS_K_RADIX_SORT] += (uint64_t)p.sort_passes * E * (p.key64 ? 24 : 16);
-      kp.alg_bytes[CGS_K_TILE_RANGES] += E * 4 + (uint64_t)p.total_tiles * 8;
+      if (p.sort_passes) {
+        kp.alg_bytes[CGS_K_ENTRY_SORT] += (uint64_t)p.sort_passes * E * (p.key64 ? 24 : 16);
+        kp.alg_bytes[CGS_K_TILE_RANGES] += E * 4 + (uint64_t)p.total_tiles * 8;
+      } else {
+        // tile transpose: records read twice (counts, placement), splat
+        // index gathered and written once
+        kp.alg_bytes[CGS_K_ENTRY_SORT] += E * 16 + (uint64_t)p.total_tiles * 8;
+      }
     }
     // The compositor stops a tile once every pixel has saturated, so its
     // algorithmic traffic is the records it actually gathered (48 B + the
@@ -792,8 +860,10 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
   if (ctx->has_cages && !ctx->verts_uploaded)
     return ctx->fail(CGS_E_STATE, "cage vertices not uploaded");
-  if (params->radix_bits != 0 && params->radix_bits != 4 && params->radix_bits != 8)
-    return ctx->fail(CGS_E_ARG, "radix_bits must be 0, 4 or 8");
+  if (params->radix_bits != 0 && (params->radix_bits < 4 || params->radix_bits > 8))
+    return ctx->fail(CGS_E_ARG, "radix_bits must be 0 or 4..8");
+  if (params->entry_sort < CGS_SORT_AUTO || params->entry_sort > CGS_SORT_TRANSPOSE)
+    return ctx->fail(CGS_E_ARG, "entry_sort must be one of CGS_SORT_*");
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   cgs_stage_timings tm{};
@@ -818,7 +888,8 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   d.tiles_y = tiles_y;
   d.total_tiles = (uint32_t)total_tiles64;
   d.pitch = (W + 63) / 64 * 64;
-  d.radix_bits = params->radix_bits ? (uint32_t)params->radix_bits : 8u;
+  d.radix_bits = (uint32_t)params->radix_bits;
+  d.entry_sort = params->entry_sort;
   d.write_f32 = params->write_f32 != 0;
   std::memcpy(d.bg, comp->background, 16);
   if (W != ctx->last_w || H != ctx->last_h) ctx->s3_valid = false;
@@ -840,6 +911,12 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   d.tile_bits = d.total_tiles <= 1 ? 1u : 32u - (uint32_t)__builtin_clz(d.total_tiles - 1);
   d.depth_bits = d.tile_bits >= 32 ? 0u : (32u - d.tile_bits < 28u ? 32u - d.tile_bits : 28u);
   d.sort_bits = d.tile_bits + d.depth_bits > 32 ? 32 : d.tile_bits + d.depth_bits;
+  if (d.radix_bits == 0) {
+    // balanced digits: the fewest passes of at most 8 bits over the tile bits,
+    // split as evenly as possible (13 bits -> 7 + 6), at least 4 bits
+    const uint32_t passes = (d.tile_bits + 7) / 8;
+    d.radix_bits = std::max(4u, (d.tile_bits + passes - 1) / passes);
+  }
   const float near_c = camera->near_plane > 1e-6f ? camera->near_plane : 1e-6f;
   d.depth_base_bits = fbits(near_c) & 0x7F800000u;
 
@@ -876,7 +953,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   key.mip = mip_bits;
   key.min_opa = fbits(params->min_opacity);
   key.min_rad = fbits(params->min_radius_px);
-  key.radix_bits = d.radix_bits;
+  key.radix_bits = d.radix_bits | ((uint32_t)d.entry_sort << 8);
   bool cached = !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
   if (cached) {
     CGS_TRY(drain(ctx, true));
@@ -976,9 +1053,10 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
 
   // ---------------- Stages 3 and 4
   int src = ctx->s3_src;
-  uint32_t passes = 0, splat_passes = 0;
+  uint32_t passes = 0, splat_passes = 0, bin_launches = 0, sort_launches = 0;
   if (!cached) {
-    CGS_TRY(enqueue_stage3(ctx, d, L, &src, &passes, &splat_passes, true));
+    CGS_TRY(enqueue_stage3(ctx, d, L, &src, &passes, &splat_passes, true, &bin_launches,
+                           &sort_launches));
     ctx->s3_valid = true;
     ctx->s3_key = key;
     ctx->s3_src = src;
@@ -1001,6 +1079,8 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   P.cap = ctx->entry_cap;
   P.sort_passes = passes;
   P.splat_passes = splat_passes;
+  P.bin_launches = bin_launches;
+  P.sort_launches = sort_launches;
   P.total_tiles = d.total_tiles;
   P.W = W;
   P.H = H;
@@ -1035,7 +1115,8 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
       }
       tm.stage1_deform_ms = ms[CGS_K_TET_TRANSFORMS] + ms[CGS_K_DEFORM];
       tm.stage2_project_ms = ms[CGS_K_PROJECT];
-      tm.stage3_bin_sort_ms = ms[CGS_K_BIN] + ms[CGS_K_RADIX_SORT] + ms[CGS_K_TILE_RANGES];
+      tm.stage3_bin_sort_ms =
+          ms[CGS_K_SPLAT_SORT] + ms[CGS_K_BIN] + ms[CGS_K_ENTRY_SORT] + ms[CGS_K_TILE_RANGES];
       tm.stage4_composite_ms = ms[CGS_K_COMPOSITE];
       tm.used_hardware_timestamps = 1;
     }
@@ -1202,7 +1283,31 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
       break;
     }
     case CGS_BUF_SORTED_KEYS:
-      if (!ctx->s3_key64) {
+      if (ctx->s3_transpose) {
+        // The tile transpose sorts splat indices only; the 32-bit keys are
+        // tile << depth_bits | depth key, from the ranges and the splat order.
+        const size_t sa = ctx->s3_active;
+        CGS_TRY(fetch(ctx->ranges, (size_t)ctx->last_tiles * 8));
+        const std::vector<char> rg = tmp;
+        CGS_TRY(fetch(ctx->sids[ctx->s3_order_src], sa * 4));
+        const std::vector<char> ord = tmp;
+        CGS_TRY(fetch(ctx->skeys[ctx->s3_order_src], sa * 4));
+        const std::vector<char> dk = tmp;
+        CGS_TRY(fetch(ctx->ids[ctx->s3_src], entries * 4));
+        const uint32_t* r = (const uint32_t*)rg.data();
+        const uint32_t* os = (const uint32_t*)ord.data();
+        const uint32_t* ds = (const uint32_t*)dk.data();
+        const uint32_t* ids = (const uint32_t*)tmp.data();
+        std::vector<uint32_t> dq_of(sa, 0);
+        for (size_t j = 0; j < sa; ++j)
+          if (os[j] < sa) dq_of[os[j]] = ds[j];
+        out.assign(entries * 4, 0);
+        uint32_t* o = (uint32_t*)out.data();
+        const uint32_t db = ctx->s3_depth_bits;
+        for (uint32_t t = 0; t < ctx->last_tiles; ++t)
+          for (uint32_t i = r[2 * t]; i < r[2 * t + 1] && i < entries; ++i)
+            o[i] = (db >= 32 ? 0u : (t << db)) | (ids[i] < sa ? dq_of[ids[i]] : 0u);
+      } else if (!ctx->s3_key64) {
         CGS_TRY(fetch(ctx->keys[ctx->s3_src], entries * 4));
         out = tmp;
       } else {
@@ -1248,7 +1353,7 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
 
 const char* cgs_kernel_name(int32_t id) {
   static const char* names[CGS_KERNEL_COUNT] = {"clear", "tet_transforms", "deform", "project",
-                                                "bin", "radix_sort", "tile_ranges", "composite",
+                                                "bin", "entry_sort", "tile_ranges", "composite",
                                                 "splat_sort"};
   return (id >= 0 && id < CGS_KERNEL_COUNT) ? names[id] : "unknown";
 }

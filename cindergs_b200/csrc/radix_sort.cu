@@ -16,8 +16,9 @@
 //   4. keys are reordered by digit in shared memory and written out so that
 //      each digit's run is a contiguous, mostly coalesced store.
 // The global digit offsets come from digit histograms of all passes, which the
-// Stage 3 emitter accumulates while it writes the keys (launch_histogram does
-// the same for standalone sorts). HBM traffic per pass: one read and one write
+// Stage 3 binning kernel accumulates while it writes the keys (launch_histogram
+// does the same for standalone sorts); k_digit_bases turns them into
+// exclusive bases once per sort. HBM traffic per pass: one read and one write
 // of keys and payloads (16 B per pair), plus 1 KiB of look-back words per tile.
 #include "kernels.h"
 
@@ -42,7 +43,7 @@ struct PassArgs {
   uint32_t capacity;
   uint32_t shift;
   uint32_t dmask;          // digit mask of this pass (narrower on a final partial pass)
-  const uint32_t* hist;    // this pass's digit counts
+  const uint32_t* dbase;   // this pass's exclusive digit bases (k_digit_bases)
   uint32_t* status;        // this pass's [tiles][radix] look-back words
   uint32_t* clear_next;    // [tiles][radix] words to zero for the next pass, or null
   uint32_t grid_tiles;     // tiles covered by the grid (all of clear_next)
@@ -60,8 +61,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   uint32_t* s_whist = s_v0 + (PAY2 ? 2 : 1) * kSortTile;  // [8][R]
   uint32_t* s_tstart = s_whist + 8 * R;          // [R]
   uint32_t* s_goff = s_tstart + R;               // [R]
-  uint32_t* s_dbase = s_goff + R;                // [R]
-  uint32_t* s_misc = s_dbase + R;                // [40]: tile, warp sums
+  uint32_t* s_misc = s_goff + R;                 // [40]: tile, warp sums
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   uint32_t n = *a.n_ptr;
@@ -77,50 +77,52 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     for (uint32_t k = tid; k < R; k += kSortThreads) a.clear_next[(size_t)tile * R + k] = 0u;
   if (tile >= num_tiles) return;
 
-  // Issue the tile's loads first so their latency overlaps the digit-base scan.
+  // Load (warp-striped: a warp's item j is 32 consecutive keys). Full tiles,
+  // all but the last, need no bounds checks.
   const size_t tile_base = (size_t)tile * kSortTile;
+  const bool full = tile_base + kSortTile <= (size_t)n;
+  const size_t first = tile_base + (size_t)warp * (32 * kSortItems) + lane;
   uint32_t k[kSortItems], v0[kSortItems], v1[kSortItems];
   uint32_t rk[kSortItems / 2];  // two 16-bit in-warp ranks per word (ranks < 512)
+  if (full) {
 #pragma unroll
-  for (int j = 0; j < kSortItems; ++j) {
-    const size_t e = tile_base + (size_t)warp * (32 * kSortItems) + (size_t)j * 32 + lane;
-    const bool valid = e < n;
-    k[j] = valid ? __ldcs(a.keys_in + e) : 0xFFFFFFFFu;
-    v0[j] = valid ? __ldcs(a.v0_in + e) : 0u;
-    if (PAY2) v1[j] = valid ? __ldcs(a.v1_in + e) : 0u;
+    for (int j = 0; j < kSortItems; ++j) {
+      k[j] = __ldcs(a.keys_in + first + 32 * j);
+      v0[j] = __ldcs(a.v0_in + first + 32 * j);
+      if (PAY2) v1[j] = __ldcs(a.v1_in + first + 32 * j);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+      const bool valid = first + 32 * j < n;
+      k[j] = valid ? __ldcs(a.keys_in + first + 32 * j) : 0xFFFFFFFFu;
+      v0[j] = valid ? __ldcs(a.v0_in + first + 32 * j) : 0u;
+      if (PAY2) v1[j] = valid ? __ldcs(a.v1_in + first + 32 * j) : 0u;
+    }
   }
 
-  // Global digit bases: exclusive scan of this pass's digit histogram.
-  {
-    uint32_t tot;
-    const uint32_t h = (uint32_t)tid < R ? a.hist[tid] : 0u;
-    const uint32_t ex = block_exclusive_sum(h, s_misc + 8, &tot);
-    if ((uint32_t)tid < R) s_dbase[tid] = ex;
-  }
-  // Warp-level stable ranking by digit.
+  // Warp-level stable ranking by digit: the lanes holding the same digit
+  // (match) take consecutive ranks after the warp's running count, which the
+  // highest of them advances.
   uint32_t* wh = s_whist + warp * R;
+  const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t d = (k[j] >> a.shift) & a.dmask;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const int leader = __ffs(peers) - 1;
-    const uint32_t before = __popc(peers & lanemask_lt());
+    const int leader = 31 - __clz(peers);
     uint32_t old = 0;
-    if (lane == leader) {
-      old = wh[d];
-      wh[d] = old + __popc(peers);
-    }
+    if (lane == leader) old = atomicAdd(&wh[d], (uint32_t)__popc(peers));
     old = __shfl_sync(0xffffffffu, old, leader);
-    const uint32_t r = old + before;
+    const uint32_t r = old + __popc(peers & lt);
     if (j & 1)
       rk[j >> 1] |= r << 16;
     else
       rk[j >> 1] = r;
-    __syncwarp();
   }
   __syncthreads();
   // Per digit: exclusive prefix over warps, tile count (valid keys only).
-  const uint32_t tile_valid = (uint32_t)min((size_t)kSortTile, (size_t)n - tile_base);
+  const uint32_t tile_valid = full ? kSortTile : (uint32_t)((size_t)n - tile_base);
   uint32_t my_count = 0;
   if ((uint32_t)tid < R) {
     uint32_t run = 0;
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
       }
       st_relaxed_u32(st, kFlagPre | ((excl + agg) & kValueMask));
     }
-    s_goff[tid] = s_dbase[tid] + excl - tstart;
+    s_goff[tid] = a.dbase[tid] + excl - tstart;
   }
   __syncthreads();
   // Reorder by digit through shared memory.
@@ -176,18 +178,34 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     if (PAY2) s_v1[pos] = v1[j];
   }
   __syncthreads();
-  for (uint32_t i = tid; i < tile_valid; i += kSortThreads) {
+  // Scatter: each digit's run is contiguous in the output.
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = tid + kSortThreads * j;
+    if (!full && i >= tile_valid) break;
     const uint32_t key = s_keys[i];
-    const uint32_t d = (key >> a.shift) & a.dmask;
-    const uint32_t g = s_goff[d] + i;
+    const uint32_t g = s_goff[(key >> a.shift) & a.dmask] + i;
     if (g >= n) {  // inconsistent histogram: report instead of writing out of bounds
-      atomicOr(a.status_word, kStatusCapacity);
+      bad = true;
       continue;
     }
     a.keys_out[g] = key;
     a.v0_out[g] = s_v0[i];
     if (PAY2) a.v1_out[g] = s_v1[i];
   }
+  if (bad) atomicOr(a.status_word, kStatusCapacity);
+}
+
+// Exclusive digit bases of every pass from the digit counts, in place: block
+// p scans pass p's R counts.
+__global__ void k_digit_bases(uint32_t* hist, uint32_t radix) {
+  __shared__ uint32_t s_sums[32];
+  uint32_t* h = hist + (size_t)blockIdx.x * radix;
+  const uint32_t v = threadIdx.x < radix ? h[threadIdx.x] : 0u;
+  uint32_t tot;
+  const uint32_t ex = block_exclusive_sum(v, s_sums, &tot);
+  if (threadIdx.x < radix) h[threadIdx.x] = ex;
 }
 
 template <int RB, bool PAY2>
@@ -252,12 +270,16 @@ cudaError_t launch_histogram(const uint32_t* keys, const uint32_t* n_ptr, uint32
 }
 
 cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
-  const uint32_t rb = a.radix_bits == 4 ? 4u : 8u;
+  const uint32_t rb = a.radix_bits < 4 ? 4u : (a.radix_bits > 8 ? 8u : a.radix_bits);
   const uint32_t R = 1u << rb;
   const uint32_t passes = sort_passes(a.num_bits, rb);
   const uint32_t tiles = sort_tiles(a.capacity);
   int src = a.src;
   const bool pay2 = a.vals2[0] != nullptr;
+  // counts -> exclusive bases (in place)
+  k_digit_bases<<<passes, 256, 0, s>>>(a.hist, R);
+  cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) return le;
   for (uint32_t p = 0; p < passes; ++p) {
     PassArgs pa;
     pa.keys_in = a.keys[src];
@@ -271,7 +293,7 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.shift = a.first_bit + p * rb;
     const uint32_t rem = a.num_bits - p * rb;
     pa.dmask = (1u << (rem < rb ? rem : rb)) - 1u;
-    pa.hist = a.hist + (size_t)p * R;
+    pa.dbase = a.hist + (size_t)p * R;
     if (a.status2[0]) {
       const int par = *a.parity;
       pa.status = a.status2[par];
@@ -285,10 +307,13 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
     cudaError_t e;
-    if (rb == 8)
-      e = pay2 ? launch_pass<8, true>(pa, tiles, s) : launch_pass<8, false>(pa, tiles, s);
-    else
-      e = pay2 ? launch_pass<4, true>(pa, tiles, s) : launch_pass<4, false>(pa, tiles, s);
+    switch (rb) {
+      case 4: e = pay2 ? launch_pass<4, true>(pa, tiles, s) : launch_pass<4, false>(pa, tiles, s); break;
+      case 5: e = pay2 ? launch_pass<5, true>(pa, tiles, s) : launch_pass<5, false>(pa, tiles, s); break;
+      case 6: e = pay2 ? launch_pass<6, true>(pa, tiles, s) : launch_pass<6, false>(pa, tiles, s); break;
+      case 7: e = pay2 ? launch_pass<7, true>(pa, tiles, s) : launch_pass<7, false>(pa, tiles, s); break;
+      default: e = pay2 ? launch_pass<8, true>(pa, tiles, s) : launch_pass<8, false>(pa, tiles, s); break;
+    }
     if (e != cudaSuccess) return e;
     src = 1 - src;
   }

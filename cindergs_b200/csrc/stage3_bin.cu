@@ -29,6 +29,7 @@ constexpr int kBinThreads = 256;
 constexpr int kBinWarps = kBinThreads / 32;
 constexpr int kMaskCap = 128;  // stored ballot masks per warp (4,096 candidates)
 constexpr int kHitCap = 736;   // stored hit records per warp (4 blocks fit an SM)
+constexpr uint32_t kMaxGroups = 8;  // tile groups of the record mode
 
 // Per-splat constants of a warp's 32 splats, read by the lane that tests one
 // of the splat's candidate tiles (three 128-bit loads and two 32-bit loads).
@@ -207,6 +208,14 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
   const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
+  // Record mode: per warp, per tile group, the hits counted, the staging
+  // start and the records written (in the histogram area, unused here).
+  const bool rec_mode = !KEY64 && a.records;
+  const uint32_t G = a.groups, gshift = a.group_shift;
+  uint32_t* s_gcnt = s_hist + warp * 3 * kMaxGroups;
+  uint32_t* s_gbase = s_gcnt + kMaxGroups;
+  uint32_t* s_grun = s_gbase + kMaxGroups;
+  const uint32_t lt = lanemask_lt();
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
   const uint32_t num_tiles = (a.max_n + 31u) / 32u;
   const uint32_t* wbase = sp.base[warp];
@@ -254,6 +263,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
       sp.dq[warp][lane] = dq;
       sp.sid[warp][lane] = sid;
     }
+    if (rec_mode && lane < (int)kMaxGroups) s_gcnt[lane] = 0u;
     __syncwarp();
     const bool big = total > (uint32_t)kMaskCap * 32u;  // warp-uniform
 
@@ -287,6 +297,12 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
         const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
         own += __popc(hits & seg_mask(lo, hi));
       }
+      if (rec_mode) {  // hits per tile group (one counter update per group present)
+        const uint32_t g = hit ? (rec >> 5) >> gshift : 0xFFFFFFFFu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, g);
+        if (hit && lane == 31 - __clz(peers)) s_gcnt[g] += __popc(peers);
+        __syncwarp();
+      }
       run += __popc(hits);
     }
     __syncwarp();
@@ -304,6 +320,76 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
     if (s < a.max_n) a.offsets[s] = count;
 
     // 2. stage
+    if (rec_mode) {
+      // One run per tile group, each in the hits' order: record = tile << 5 |
+      // slot lane.
+      if (lane < (int)G) {
+        const uint32_t gc = s_gcnt[lane];
+        const uint32_t gb = gc ? atomicAdd(&a.fc->tile_ctr[2], gc) : 0u;
+        a.tile_stage[(size_t)tile * G + lane] = gb;
+        a.tile_count[(size_t)tile * G + lane] = gc;
+        s_gbase[lane] = gb;
+        s_grun[lane] = 0u;
+      }
+      __syncwarp();
+      // called by the whole warp with the lanes' hits in order
+      auto put_rec = [&](bool h, uint32_t rec) {
+        const uint32_t g = h ? (rec >> 5) >> gshift : 0xFFFFFFFFu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, g);
+        if (h) {
+          const uint32_t pos = s_gbase[g] + s_grun[g] + __popc(peers & lt);
+          if (pos < cap)
+            a.stage_keys[pos] = rec;
+          else
+            overflow = true;
+        }
+        __syncwarp();
+        if (h && lane == 31 - __clz(peers)) s_grun[g] += __popc(peers);
+        __syncwarp();
+      };
+      const uint32_t stored = min(run, (uint32_t)kHitCap);
+      for (uint32_t k0 = 0; k0 < stored; k0 += 32) {
+        const uint32_t k = k0 + lane;
+        put_rec(k < stored, k < stored ? whits[k] : 0u);
+      }
+      if (run > (uint32_t)kHitCap) {
+        uint32_t hrun = 0;
+        for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
+          uint32_t hits;
+          const uint32_t item = chunk + lane;
+          if (c < (uint32_t)kMaskCap) {
+            hits = wmask[c];
+            hrun = wmrun[c];
+            if (hrun + __popc(hits) <= (uint32_t)kHitCap) {
+              hrun += __popc(hits);
+              continue;
+            }
+          } else {
+            bool hit = false;
+            if (item < total) {
+              const int o = find_owner(wbase, item);
+              uint32_t tx, ty;
+              box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
+              hit = tile_hit(tx, ty, wm1, hm1, sp.geo[warp][o], sp.con[warp][o],
+                             sp.rcp[warp][o], sp.qlim[warp][o]);
+            }
+            hits = __ballot_sync(0xffffffffu, hit);
+          }
+          const uint32_t k = hrun + __popc(hits & lt);
+          const bool sel = ((hits >> lane) & 1u) && k >= (uint32_t)kHitCap;
+          uint32_t rec = 0;
+          if (sel) {
+            const int o = find_owner(wbase, item);
+            uint32_t tx, ty;
+            box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
+            rec = ((ty * a.tiles_x + tx) << 5) | (uint32_t)o;
+          }
+          put_rec(sel, rec);
+          hrun += __popc(hits);
+        }
+      }
+      continue;
+    }
     uint32_t sbase = 0;
     if (lane == 0) {
       sbase = run ? atomicAdd(&a.fc->tile_ctr[2], run) : 0u;
@@ -379,6 +465,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
     }
   }
   if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
+  if (rec_mode) return;  // no histograms (the area held the group counters)
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
     const uint32_t v = s_hist[k];
@@ -425,6 +512,210 @@ __global__ void __launch_bounds__(256) k_bin_place(const BinArgs a) {
       }
     }
   }
+}
+
+// ---- Tile transpose ---------------------------------------------------------
+// The binning kernel stages each 32-slot tile's hits in the reference's
+// emission order. Sorting them stably by tile is a transpose of the
+// (slot, tile) incidence from slot-major to tile-major; with few enough
+// screen tiles it is done in one counting pass instead of radix passes:
+//   k_chunk_counts: entries of every (tile, chunk) pair;
+//   scan of the per-tile totals (launch_scan_u32) -> each tile's first entry;
+//   k_column_scan:  per tile, exclusive scan over the chunks -> each
+//                   (tile, chunk) pair's first entry; tile ranges;
+//   k_chunk_place:  per (chunk, group of tiles): each warp counts its eighth
+//                   of the chunk per tile, the counts are turned into per-warp
+//                   bases, and each warp walks its records again in order,
+//                   ranking equal tiles with match_any and per-warp counters,
+//                   and writes every splat index to its final entry.
+// The order inside a tile is chunk, then warp, then record order: the slots'
+// (depth, splat index) order, as the reference's stable key sort gives.
+
+// A warp's walk over the records of group g in the 32-slot tiles [w0, w1):
+// the run descriptors (length, staging start) of 32 tiles at a time sit one
+// per lane; their records are concatenated and taken 32 at a time, one per
+// lane, in order. Each lane finds its record's run by a 5-step search over
+// the runs' exclusive prefix (held in lanes).
+struct RunWalk {
+  uint32_t n, st, pre, total;  // this lane's run: length, start, exclusive prefix; sum
+  __device__ __forceinline__ void load(const TransposeArgs& a, uint32_t wb, uint32_t w1,
+                                       uint32_t g, int lane) {
+    n = 0;
+    st = 0;
+    if (wb + lane < w1) {
+      n = a.tile_count[(size_t)(wb + lane) * a.groups + g];
+      st = a.tile_stage[(size_t)(wb + lane) * a.groups + g];
+    }
+    uint32_t incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    pre = incl - n;
+    total = __shfl_sync(0xffffffffu, incl, 31);
+  }
+  // run (lane) holding record i (< total) of the concatenation, and its address
+  __device__ __forceinline__ int find(uint32_t i, uint32_t& addr) const {
+    int q = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1)
+      if (__shfl_sync(0xffffffffu, pre, q + step) <= i) q += step;
+    addr = __shfl_sync(0xffffffffu, st, q) + (i - __shfl_sync(0xffffffffu, pre, q));
+    return q;
+  }
+};
+
+// Entries of every (tile, chunk) pair of one tile group, and per-tile totals.
+// Block (chunk k, group g); warp w walks the w-th eighth of the chunk.
+__global__ void __launch_bounds__(256) k_chunk_counts(const TransposeArgs a) {
+  __shared__ uint32_t s_cnt[kTransposeGroupTiles];
+  const uint32_t k = blockIdx.x, g = blockIdx.y;
+  const uint32_t t0 = g * a.group_tiles;
+  const uint32_t tn = min(a.group_tiles, a.num_tiles - t0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t t = threadIdx.x; t < tn; t += blockDim.x) s_cnt[t] = 0u;
+  __syncthreads();
+  const uint32_t sub = a.chunk_wtiles / 8;
+  const uint32_t w0 = min(k * a.chunk_wtiles + warp * sub, a.num_wtiles);
+  const uint32_t w1 = min(w0 + sub, a.num_wtiles);
+  for (uint32_t wb = w0; wb < w1; wb += 32) {
+    RunWalk rw;
+    rw.load(a, wb, w1, g, lane);
+    for (uint32_t i0 = 0; i0 < rw.total; i0 += 32) {
+      uint32_t addr;
+      rw.find(i0 + lane, addr);
+      if (i0 + lane < rw.total && addr < a.capacity) {
+        const uint32_t t = (__ldg(a.records + addr) >> 5) - t0;
+        if (t < tn) atomicAdd(&s_cnt[t], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t t = threadIdx.x; t < tn; t += blockDim.x) {
+    const uint32_t c = s_cnt[t];
+    a.cmat[(size_t)(t0 + t) * a.num_chunks + k] = c;
+    if (c) atomicAdd(&a.totals[t0 + t], c);
+  }
+}
+
+// One warp per tile: first entry of each (tile, chunk) pair, and the range.
+__global__ void __launch_bounds__(256) k_column_scan(const TransposeArgs a) {
+  const uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= a.num_tiles) return;
+  uint32_t run = a.tile_base[t];
+  uint32_t* row = a.cmat + (size_t)t * a.num_chunks;
+  for (uint32_t k0 = 0; k0 < a.num_chunks; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const uint32_t v = k < a.num_chunks ? row[k] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (k < a.num_chunks) row[k] = run + incl - v;
+    run += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0) {
+    const uint32_t total = a.totals[t], base = a.tile_base[t];
+    a.ranges[2 * (size_t)t] = total ? base : 0u;
+    a.ranges[2 * (size_t)t + 1] = total ? base + total : 0u;
+  }
+}
+
+// Block (chunk k, tile group g): places the chunk's entries of the group.
+// Shared memory: per-warp counters (two 16-bit counters per word: a warp's
+// eighth of a chunk holds fewer than 2^16 slots, and so does a chunk) and the
+// chunk's first entry per tile.
+constexpr int kPlaceWarps = 8;
+
+__global__ void __launch_bounds__(kPlaceWarps * 32) k_chunk_place(const TransposeArgs a) {
+  constexpr uint32_t GW = kTransposeGroupTiles / 2;
+  __shared__ uint32_t whist[kPlaceWarps * GW];
+  __shared__ uint32_t obase[kTransposeGroupTiles];
+  const uint32_t k = blockIdx.x, g = blockIdx.y, G = a.groups;
+  const uint32_t t0 = g * a.group_tiles;
+  const uint32_t tn = min(a.group_tiles, a.num_tiles - t0);  // tiles of this group
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t i = threadIdx.x; i < kPlaceWarps * GW; i += blockDim.x) whist[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < tn; i += blockDim.x)
+    obase[i] = a.cmat[(size_t)(t0 + i) * a.num_chunks + k];
+  // this warp's eighth of the chunk (at most 32 32-slot tiles per descriptor load)
+  const uint32_t sub = a.chunk_wtiles / kPlaceWarps;
+  const uint32_t w0 = min(k * a.chunk_wtiles + warp * sub, a.num_wtiles);
+  const uint32_t w1 = min(w0 + sub, a.num_wtiles);
+  __syncthreads();
+  uint32_t* wh = whist + warp * GW;
+  // 1. per-warp counts
+  for (uint32_t wb = w0; wb < w1; wb += 32) {
+    RunWalk rw;
+    rw.load(a, wb, w1, g, lane);
+    for (uint32_t i0 = 0; i0 < rw.total; i0 += 32) {
+      uint32_t addr;
+      rw.find(i0 + lane, addr);
+      if (i0 + lane < rw.total && addr < a.capacity) {
+        const uint32_t t = (__ldg(a.records + addr) >> 5) - t0;
+        if (t < tn) atomicAdd(&wh[t >> 1], 1u << ((t & 1u) * 16u));
+      }
+    }
+  }
+  __syncthreads();
+  // 2. counts -> per-warp exclusive bases (both halves of a word at once)
+  for (uint32_t j = threadIdx.x; j < GW; j += blockDim.x) {
+    uint32_t lo = 0, hi = 0;
+#pragma unroll
+    for (int w = 0; w < kPlaceWarps; ++w) {
+      const uint32_t c = whist[w * GW + j];
+      whist[w * GW + j] = lo | (hi << 16);
+      lo += c & 0xFFFFu;
+      hi += c >> 16;
+    }
+  }
+  __syncthreads();
+  // 3. stable placement: records in order, equal tiles ranked by lane; the
+  // next batch's record and this batch's splat index are loaded ahead.
+  const uint32_t lt = lanemask_lt();
+  bool bad = false;
+  for (uint32_t wb = w0; wb < w1; wb += 32) {
+    RunWalk rw;
+    rw.load(a, wb, w1, g, lane);
+    auto fetch = [&](uint32_t i0, uint32_t& rec, uint32_t& wt) {
+      uint32_t addr;
+      const int q = rw.find(i0 + lane, addr);
+      wt = wb + (uint32_t)q;
+      rec = 0xFFFFFFFFu;
+      if (i0 + lane < rw.total && addr < a.capacity) rec = __ldg(a.records + addr);
+    };
+    uint32_t rec, wt;
+    if (rw.total) fetch(0, rec, wt);
+    for (uint32_t i0 = 0; i0 < rw.total; i0 += 32) {
+      const uint32_t sidx = rec == 0xFFFFFFFFu ? 0u : __ldg(a.order_ids + 32u * wt + (rec & 31u));
+      uint32_t t = rec == 0xFFFFFFFFu ? 0xFFFFFFFFu : (rec >> 5) - t0;
+      if (t >= tn) t = 0xFFFFFFFFu;
+      uint32_t nrec = 0xFFFFFFFFu, nwt = wt;
+      if (i0 + 32 < rw.total) fetch(i0 + 32, nrec, nwt);
+      const uint32_t peers = __match_any_sync(0xffffffffu, t);
+      const int leader = 31 - __clz(peers);
+      uint32_t old = 0;
+      if (lane == leader && t != 0xFFFFFFFFu) {
+        const uint32_t sh = (t & 1u) * 16u;
+        old = (atomicAdd(&wh[t >> 1], (uint32_t)__popc(peers) << sh) >> sh) & 0xFFFFu;
+      }
+      old = __shfl_sync(0xffffffffu, old, leader);
+      if (t != 0xFFFFFFFFu) {
+        const uint32_t pos = obase[t] + old + __popc(peers & lt);
+        if (pos < a.capacity)
+          a.ids_out[pos] = sidx;
+        else
+          bad = true;
+      }
+      rec = nrec;
+      wt = nwt;
+    }
+  }
+  if (bad) atomicOr(a.status_word, kStatusCapacity);
 }
 
 // identify_tile_ranges_kernel (binning.rs:356-391): boundaries of equal tile
@@ -549,6 +840,29 @@ cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s) {
     k_bin_place<true><<<blocks, 256, 0, s>>>(a);
   else
     k_bin_place<false><<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chunk_counts(const TransposeArgs& a, cudaStream_t s) {
+  if (a.num_chunks == 0 || a.num_tiles == 0) return cudaSuccess;
+  if (a.group_tiles > kTransposeGroupTiles || a.groups * a.group_tiles < a.num_tiles)
+    return cudaErrorInvalidValue;
+  k_chunk_counts<<<dim3(a.num_chunks, a.groups), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_column_scan(const TransposeArgs& a, cudaStream_t s) {
+  if (a.num_tiles == 0) return cudaSuccess;
+  k_column_scan<<<(a.num_tiles + 7) / 8, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chunk_place(const TransposeArgs& a, cudaStream_t s) {
+  if (a.num_chunks == 0 || a.num_tiles == 0) return cudaSuccess;
+  if (a.group_tiles > kTransposeGroupTiles || a.groups * a.group_tiles < a.num_tiles ||
+      a.chunk_wtiles % kPlaceWarps != 0 || a.chunk_wtiles > 2040u)
+    return cudaErrorInvalidValue;
+  k_chunk_place<<<dim3(a.num_chunks, a.groups), kPlaceWarps * 32, 0, s>>>(a);
   return cudaGetLastError();
 }
 

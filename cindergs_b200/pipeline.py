@@ -178,14 +178,15 @@ class GpuPipelineState:
                           min_opacity: float = 1.0 / 255.0, min_radius_px: float = 0.5,
                           profile_stages: bool = False, force_stage3: bool = False,
                           write_f32: bool = False, radix_bits: int = 0,
-                          stage_timings: bool = True) -> GpuStageTimings:
+                          stage_timings: bool = True, entry_sort: int = 0) -> GpuStageTimings:
         """execute_frame_gpu (gpu_state.rs:613-1243). With stage_timings (the
         default) the call waits for the frame and returns its counts (and, with
         profile_stages, per-stage device ms); with stage_timings=False the frame
         is only enqueued (no host synchronisation), its kernel times still
         accumulate when profile_stages is set (read them with kernel_profile()),
-        and the returned timings carry only the stage1_skipped, stage3_cached
-        and used_64bit_keys flags."""
+        and the returned timings are all zero. radix_bits and entry_sort choose
+        how the tile entries are sorted (include/cgs.h: CGS_SORT_*); every
+        choice gives the same lists."""
         self.sync_scene_and_cages(scene, cages)
         cam = _abi.CgsCamera()
         arr = camera.to_array()
@@ -197,7 +198,7 @@ class GpuPipelineState:
         params = _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
                                      float(min_opacity), float(min_radius_px),
                                      int(bool(profile_stages)), int(bool(force_stage3)),
-                                     int(bool(write_f32)), int(radix_bits))
+                                     int(bool(write_f32)), int(radix_bits), int(entry_sort))
         t = _abi.CgsStageTimings()
         tp = ctypes.byref(t) if stage_timings else None
         self._check(self._lib.cgs_execute_frame(self._ctx, ctypes.byref(cam), ctypes.byref(comp),

@@ -72,8 +72,16 @@ typedef struct cgs_frame_params {
   int32_t profile_stages;       /* 1: time each stage with CUDA events */
   int32_t force_stage3;         /* 1: never reuse the cached Stage 3 lists */
   int32_t write_f32;            /* 1: also write an unquantised RGBA f32 frame */
-  int32_t radix_bits;           /* 0 = autotuned/default (8), else 4 or 8 */
+  int32_t radix_bits;           /* entry-sort digit width: 0 = balanced digits of at most
+                                   8 bits over the tile bits (13 bits -> 7 + 6), else 4..8 */
+  int32_t entry_sort;           /* CGS_SORT_*: how the tile entries are sorted by tile */
 } cgs_frame_params;
+
+/* Entry sort methods (the result is the same, bit for bit). */
+#define CGS_SORT_AUTO 0       /* radix passes */
+#define CGS_SORT_RADIX 1      /* LSD radix passes over the tile bits */
+#define CGS_SORT_TRANSPOSE 2  /* one-pass tile transpose (32-bit keys and at most 16,384
+                                 tiles; otherwise radix passes) */
 
 /* GpuStageTimings (render/gpu_state.rs:513-534). */
 typedef struct cgs_stage_timings {
@@ -172,8 +180,9 @@ int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px)
 #define CGS_K_DEFORM 2
 #define CGS_K_PROJECT 3
 #define CGS_K_BIN 4            /* count + chained scan + key emission, one launch */
-#define CGS_K_RADIX_SORT 5     /* radix passes over the tile entries */
-#define CGS_K_TILE_RANGES 6
+#define CGS_K_ENTRY_SORT 5     /* stable sort of the tile entries by tile: the one-pass
+                                  tile transpose, or radix passes for many tiles */
+#define CGS_K_TILE_RANGES 6    /* (the tile transpose writes the ranges itself) */
 #define CGS_K_COMPOSITE 7
 #define CGS_K_SPLAT_SORT 8     /* depth-key histogram + radix passes over the splats */
 #define CGS_KERNEL_COUNT 9

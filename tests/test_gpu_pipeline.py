@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
+from cindergs_b200 import _abi
 from cindergs_b200 import (CameraUniforms, CompositorUniforms, GaussianSceneSoa, random_scene)
 from helpers import (assert_stage23_exact, compositor, config0_camera, gpu_buffers, oracle_frame,
                      parity_camera, varied_scene)
@@ -21,7 +22,8 @@ def run_both(st, scene, cam, comp, **kw):
     t = st.execute_frame_gpu(scene, None, cam, comp, kw.get("split", 0.0), kw.get("mip", 0.0),
                              kw.get("min_opa", 1.0 / 255.0), kw.get("min_rad", 0.5),
                              profile_stages=True, force_stage3=True, write_f32=True,
-                             radix_bits=kw.get("radix_bits", 0))
+                             radix_bits=kw.get("radix_bits", 0),
+                             entry_sort=kw.get("entry_sort", 0))
     g = gpu_buffers(st, key64=t.used_64bit_keys)
     g["rgba8"] = st.readback_framebuffer_rgba8(comp.screen_width, comp.screen_height)
     g["f32"] = st.readback_framebuffer_f32(comp.screen_width, comp.screen_height)
@@ -37,23 +39,29 @@ def check_image(g, o):
     assert d8.max() <= 1, f"max rgba8 diff {d8.max()}"
 
 
-def test_varied_scene_96px(gpu_state):
+SORTS = [_abi.SORT_RADIX, _abi.SORT_TRANSPOSE]
+
+
+@pytest.mark.parametrize("entry_sort", SORTS)
+def test_varied_scene_96px(gpu_state, entry_sort):
     scene = varied_scene()
     cam = parity_camera(96, 96)
     comp = compositor(96, 96, cam, deg=3)
-    t, g, o = run_both(gpu_state, scene, cam, comp)
+    t, g, o = run_both(gpu_state, scene, cam, comp, entry_sort=entry_sort)
     assert t.total_tile_entries == o["entries"] > 0
     assert t.surviving_gaussians == o["surviving"]
     assert_stage23_exact(g, o)
     check_image(g, o)
 
 
-@pytest.mark.parametrize("radix_bits", [8, 4])
-def test_config0_scene_100k_720p(gpu_state, radix_bits):
+@pytest.mark.parametrize("radix_bits,entry_sort", [(0, _abi.SORT_TRANSPOSE), (0, _abi.SORT_RADIX),
+                                                   (8, _abi.SORT_RADIX), (5, _abi.SORT_RADIX),
+                                                   (4, _abi.SORT_RADIX)])
+def test_config0_scene_100k_720p(gpu_state, radix_bits, entry_sort):
     scene = random_scene(100_000, seed=0)
     cam = config0_camera(1280, 720)
     comp = compositor(1280, 720, cam, deg=3, bg=(0.0, 0.0, 0.0, 1.0))
-    t, g, o = run_both(gpu_state, scene, cam, comp, radix_bits=radix_bits)
+    t, g, o = run_both(gpu_state, scene, cam, comp, radix_bits=radix_bits, entry_sort=entry_sort)
     assert t.total_tile_entries == o["entries"] > 100_000
     assert_stage23_exact(g, o)
     check_image(g, o)
@@ -69,13 +77,14 @@ def test_mip_and_culling_thresholds(gpu_state):
     check_image(g, o)
 
 
+@pytest.mark.parametrize("entry_sort", SORTS)
 @pytest.mark.parametrize("wh", [(19, 19), (1, 1), (17, 300)])
-def test_ragged_viewports(gpu_state, wh):
+def test_ragged_viewports(gpu_state, wh, entry_sort):
     w, h = wh
     scene = random_scene(20_000, seed=3)
     cam = config0_camera(w, h)
     comp = compositor(w, h, cam, deg=1)
-    t, g, o = run_both(gpu_state, scene, cam, comp)
+    t, g, o = run_both(gpu_state, scene, cam, comp, entry_sort=entry_sort)
     assert_stage23_exact(g, o)
     check_image(g, o)
 
@@ -113,8 +122,10 @@ def test_64bit_key_path_8k(gpu_state):
     check_image(g, o)
 
 
-@pytest.mark.parametrize("wh", [(1920, 1080), (7680, 4320)])
-def test_huge_splats(gpu_state, wh):
+@pytest.mark.parametrize("wh,entry_sort", [((1920, 1080), _abi.SORT_RADIX),
+                                           ((1920, 1080), _abi.SORT_TRANSPOSE),
+                                           ((7680, 4320), _abi.SORT_TRANSPOSE)])
+def test_huge_splats(gpu_state, wh, entry_sort):
     """Every 37th splat scaled 20x: tile boxes of up to 8,160 (1080p) and
     16,641 (8K, 64-bit keys) tiles, so binning warps exceed their stored
     ballot masks (4,096 candidates) and hit records (1,024) and re-walk their
@@ -124,7 +135,7 @@ def test_huge_splats(gpu_state, wh):
     scene.covariances_3d[::37] *= 400.0
     cam = config0_camera(w, h)
     comp = compositor(w, h, cam, deg=1)
-    t, g, o = run_both(gpu_state, scene, cam, comp)
+    t, g, o = run_both(gpu_state, scene, cam, comp, entry_sort=entry_sort)
     counts = np.diff(np.append(o["offsets"], o["entries"]))
     assert counts.max() > 4096
     assert t.total_tile_entries == o["entries"]
