@@ -278,21 +278,26 @@ def run_ours(args):
     e2e_end = torch.cuda.Event(enable_timing=True)
     e2e_start.record(stream)
     import ctypes
+    wl.step()
+    vert_pinned.numpy()[:] = wl.cage.vertices()
     for _ in range(args.steps):
-        wl.step()
-        vert_pinned.numpy()[:] = wl.cage.vertices()
         cam = wl.camera(frame)
         frame += world
-        # host vertices -> device (pinned source), then the frame, then the pixels back
+        # host vertices -> device (pinned source), then the frame (enqueued),
+        # the next step's spring update on the host while it renders, then the
+        # pixels back
         st._check(st._lib.cgs_cage_vertices_update(
             st.handle, ctypes.c_void_p(vert_pinned.data_ptr()), vert_pinned.shape[0]),
             "cgs_cage_vertices_update")
         cam_c = wl.compositor(cam)
         st.execute_frame_gpu(wl.scene, cages, cam, cam_c, wl.strain_split_threshold,
                              wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, radix_bits=args.radix_bits,
-                             entry_sort=args.entry_sort)
+                             entry_sort=args.entry_sort, stage_timings=False)
+        wl.step()
+        next_verts = wl.cage.vertices()
         st._check(st._lib.cgs_readback_rgba8(st.handle, ctypes.c_void_p(out_np.ctypes.data),
                                              args.width, args.height), "cgs_readback_rgba8")
+        vert_pinned.numpy()[:] = next_verts
     e2e_end.record(stream)
     barrier()
     e2e_ms = max_over_ranks(max(e2e_start.elapsed_time(e2e_end),
