@@ -40,6 +40,7 @@ BUF_TILE_RANGES = 10
 BUF_TET_JACOBIANS = 11
 BUF_TET_ROTATIONS = 12
 BUF_TET_STRETCH = 13
+BUF_MVC_ROTATIONS = 14
 
 # Every function include/cgs.h declares, with (restype, argtypes).
 _vp = ctypes.c_void_p
@@ -84,7 +85,7 @@ class CgsStageTimings(ctypes.Structure):
 SORT_AUTO, SORT_RADIX, SORT_TRANSPOSE = 0, 1, 2
 
 KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "entry_sort",
-                "tile_ranges", "composite", "splat_sort"]
+                "tile_ranges", "composite", "splat_sort", "mvc"]
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 
@@ -119,6 +120,11 @@ SIGNATURES = {
     "cgs_kernel_profile_read": (_int, [_vp, ctypes.POINTER(CgsKernelProfile)]),
     "cgs_kernel_profile_reset": (_int, [_vp]),
     "cgs_kernel_name": (ctypes.c_char_p, [_i32]),
+    "cgs_mvc_cage_upload": (_i32, [_vp, _u32, _vp, _u32, _vp]),
+    "cgs_mvc_vertices_update": (_i32, [_vp, _vp, _u32]),
+    "cgs_mvc_bind": (_i32, [_vp, ctypes.POINTER(_u32)]),
+    "cgs_mvc_weights": (_i32, [_vp, _u64, _vp, _vp]),
+    "cgs_mvc_read_bindings": (_i32, [_vp, _u64, _vp, _vp, ctypes.POINTER(_u64)]),
     "cgs_scan_u32": (_int, [_vp, _vp, _vp, _u64, ctypes.POINTER(_u64)]),
     "cgs_sort_pairs_u32": (_int, [_vp, _vp, _vp, _u64, _u32, _i32]),
     "cgs_sort_pairs_u64": (_int, [_vp, _vp, _vp, _vp, _u64, _u32, _i32]),

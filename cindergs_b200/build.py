@@ -25,6 +25,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hi
 # (source, extra flags)
 UNITS = [
     ("stage1_deform.cu", ["-fmad=false"]),
+    ("stage1_mvc.cu", ["-fmad=false"]),
     ("stage2_project.cu", ["-fmad=false"]),
     ("stage3_bin.cu", ["-fmad=false"]),
     ("radix_sort.cu", []),

@@ -32,8 +32,36 @@ struct DeformArgs {
   FrameCounters* fc;
   float split_threshold;
   float mip;
+  // MVC-bound Gaussians (bind_tet == kMvcBound): per slot the deformed
+  // position and gradient (3 float4, k_mvc_jacobian) in, the polar rotation
+  // (9 floats, column-major) out for Stage 2's SH directions
+  const float4* mvc_xf;
+  float* mvc_R;
 };
 cudaError_t launch_tet_transforms(const DeformArgs& a, cudaStream_t s);
+
+// ---- MVC (stage1_mvc.cu) -----------------------------------------------------
+// bind_tet value of a Gaussian bound to the polygon (MVC) cage; its bind_w.x
+// holds the bits of its MVC slot.
+constexpr uint32_t kMvcBound = 0xFFFFFFFEu;
+struct MvcCage {
+  uint32_t V, F;
+  const float4* verts;      // [V] rest (binding) or current vertices
+  const uint4* tris;        // [F] outward triangles
+  const uint32_t* vf_off;   // [V + 1] incident faces per vertex (CSR)
+  const uint32_t* vf_list;  // face << 2 | corner, ascending faces per vertex
+};
+bool mvc_cage_fits(uint32_t V, uint32_t F);
+cudaError_t launch_mvc_weights(const MvcCage& c, uint32_t n, const float* pts, float* w,
+                               cudaStream_t s);
+cudaError_t launch_mvc_inside(const MvcCage& c, uint32_t n, const float4* rest_pos,
+                              const uint32_t* bind_tet, uint32_t* flag, cudaStream_t s);
+cudaError_t launch_mvc_compact(uint32_t n, const uint32_t* flag, const uint32_t* slot_of,
+                               uint32_t* bind_tet, float4* bind_w, uint32_t* list, cudaStream_t s);
+cudaError_t launch_mvc_bind_weights(const MvcCage& c, uint32_t nb, const uint32_t* list,
+                                    const float4* rest_pos, float h, float4* wg, cudaStream_t s);
+cudaError_t launch_mvc_jacobian(uint32_t V, const float4* verts, uint32_t nb, const float4* wg,
+                                float4* xf, cudaStream_t s);
 cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s);
 
 struct BindArgs {
@@ -58,8 +86,10 @@ struct ProjectArgs {
   int sh_f16;
   uint32_t sh_stride;         // plane stride (rest Gaussian count)
   const uint32_t* bind_tet;   // [n_rest] or null
+  const float4* bind_w;       // [n_rest] (MVC slot bits in .x for kMvcBound) or null
   const float* tet_R;         // [T*9] or null
   uint32_t num_tets;
+  const float* mvc_R;         // [MVC slots * 9] or null
   const uint2* split_meta;    // [n_rest] or null
   const uint32_t* split_count;  // device word or null (no splitting)
   uint32_t n_rest;

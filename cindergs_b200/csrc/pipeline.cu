@@ -132,6 +132,23 @@ struct cgs_ctx {
   bool has_cages = false;
   DevBuf tet_elems, tet_inv_dm, cage_verts, bind_tet, bind_w;
   std::vector<float> last_verts;
+  // polygon (MVC) cage: topology, rest and current vertices, exact bindings
+  uint32_t mvc_V = 0, mvc_F = 0, mvc_nb = 0;
+  bool mvc_ready = false;
+  float mvc_h = 0.0f;
+  DevBuf mvc_rest, mvc_verts, mvc_tris, mvc_vf_off, mvc_vf_list, mvc_list, mvc_wg, mvc_xf, mvc_R;
+  std::vector<float> mvc_last_verts;
+  bool deform_on() const { return has_cages || mvc_nb > 0; }
+  MvcCage mvc_cage(bool rest) const {
+    MvcCage c;
+    c.V = mvc_V;
+    c.F = mvc_F;
+    c.verts = rest ? mvc_rest.as<float4>() : mvc_verts.as<float4>();
+    c.tris = mvc_tris.as<uint4>();
+    c.vf_off = mvc_vf_off.as<uint32_t>();
+    c.vf_list = mvc_vf_list.as<uint32_t>();
+    return c;
+  }
   bool verts_uploaded = false;
   bool deformed_valid = false;
   uint64_t deform_generation = 1;
@@ -571,6 +588,10 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
     const uint64_t A = p.n + (p.split_possible ? h.split : 0u);
     const uint64_t S = h.fc.surviving, E = p.stage3_ran ? entries : 0, T = ctx->num_tets;
     const uint64_t shb = ctx->sh_f16 ? 96 : 192;
+    if (p.need_deform && ctx->mvc_nb) {
+      // stored bindings: (w, grad w) per cage vertex in, position + F out
+      kp.alg_bytes[CGS_K_MVC] += (uint64_t)ctx->mvc_nb * ((uint64_t)ctx->mvc_V * 16 + 48);
+    }
     if (p.need_deform) {
       kp.alg_bytes[CGS_K_TET_TRANSFORMS] += T * (16 + 36 + 48 + 76);
       kp.alg_bytes[CGS_K_DEFORM] += (uint64_t)p.n * 60 + A * 40 + (A - p.n) * 8;
@@ -746,6 +767,7 @@ int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* co
   ctx->s3_valid = false;
   ctx->has_cages = false;  // cage bindings refer to the previous scene
   ctx->num_tets = 0;
+  ctx->mvc_nb = 0;
   return CGS_OK;
 }
 
@@ -756,7 +778,12 @@ int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "upload the scene before the cages");
   cudaSetDevice(ctx->device);
   if (num_tets == 0) {
-    if (ctx->has_cages) ctx->deform_generation++;
+    // Tet-bound Gaussians fall back to the rest pose (their tet index is now
+    // out of range); polygon-cage bindings stay valid.
+    if (ctx->has_cages) {
+      ctx->deform_generation++;
+      ctx->deformed_valid = false;
+    }
     ctx->has_cages = false;
     ctx->num_tets = 0;
     ctx->s3_valid = false;
@@ -782,6 +809,7 @@ int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
   ctx->num_tets = num_tets;
   ctx->num_verts = num_verts;
   ctx->has_cages = true;
+  ctx->mvc_nb = 0;  // the bindings were replaced: bind the polygon cage again
   ctx->verts_uploaded = false;
   ctx->last_verts.clear();
   ctx->deformed_valid = false;
@@ -802,6 +830,184 @@ int cgs_cage_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_vert
   ctx->last_verts.assign(verts, verts + cnt);
   ctx->verts_uploaded = true;
   ctx->deformed_valid = false;
+  return CGS_OK;
+}
+
+int cgs_mvc_cage_upload(cgs_ctx* ctx, uint32_t V, const float* rest, uint32_t F,
+                        const uint32_t* tris) {
+  if (!ctx || !rest || !tris) return CGS_E_ARG;
+  if (V < 4 || F < 4) return ctx->fail(CGS_E_ARG, "a polygon cage needs at least 4 vertices and 4 triangles");
+  if (!mvc_cage_fits(V, F)) return ctx->fail(CGS_E_CAPACITY, "polygon cage too large (1,024 vertices, 12,800 vertices + triangles)");
+  for (uint32_t f = 0; f < F; ++f) {
+    const uint32_t* t = tris + 3 * (size_t)f;
+    if (t[0] >= V || t[1] >= V || t[2] >= V) return ctx->fail(CGS_E_ARG, "triangle index out of range");
+    if (t[0] == t[1] || t[1] == t[2] || t[2] == t[0]) return ctx->fail(CGS_E_ARG, "degenerate triangle");
+  }
+  cudaSetDevice(ctx->device);
+  // incident faces per vertex, ascending (the order the reference adds them in)
+  std::vector<uint32_t> off(V + 1, 0), list(3 * (size_t)F);
+  for (uint32_t f = 0; f < F; ++f)
+    for (int k = 0; k < 3; ++k) ++off[tris[3 * (size_t)f + k] + 1];
+  for (uint32_t j = 0; j < V; ++j) off[j + 1] += off[j];
+  std::vector<uint32_t> fill(off.begin(), off.end() - 1);
+  for (uint32_t f = 0; f < F; ++f)
+    for (uint32_t k = 0; k < 3; ++k) list[fill[tris[3 * (size_t)f + k]]++] = (f << 2) | k;
+  std::vector<float4> v4(V);
+  for (uint32_t j = 0; j < V; ++j) v4[j] = make_float4(rest[3 * j], rest[3 * j + 1], rest[3 * j + 2], 0.0f);
+  std::vector<uint4> t4(F);
+  for (uint32_t f = 0; f < F; ++f) t4[f] = make_uint4(tris[3 * f], tris[3 * f + 1], tris[3 * f + 2], 0u);
+  // jacobian_step_size (mvc.rs:484-494): 1e-3 of the bounding-box diagonal,
+  // clamped to [1e-5, 1e-2]
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t j = 0; j < V; ++j)
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = std::fmin(mn[k], rest[3 * j + k]);
+      mx[k] = std::fmax(mx[k], rest[3 * j + k]);
+    }
+  const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+  const float diag = std::fmax(std::sqrt((dx * dx + dy * dy) + dz * dz), 1e-3f);
+  ctx->mvc_h = std::fmin(std::fmax(diag * 1e-3f, 1e-5f), 1e-2f);
+  CGS_TRY(ctx->ensure(ctx->mvc_rest, (size_t)V * 16, "mvc rest vertices"));
+  CGS_TRY(ctx->ensure(ctx->mvc_verts, (size_t)V * 16, "mvc vertices"));
+  CGS_TRY(ctx->ensure(ctx->mvc_tris, (size_t)F * 16, "mvc triangles"));
+  CGS_TRY(ctx->ensure(ctx->mvc_vf_off, (size_t)(V + 1) * 4, "mvc incidence"));
+  CGS_TRY(ctx->ensure(ctx->mvc_vf_list, (size_t)F * 12, "mvc incidence"));
+  cudaStream_t s = ctx->stream;
+  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_rest.p, v4.data(), (size_t)V * 16, cudaMemcpyHostToDevice, s), "mvc upload");
+  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_verts.p, v4.data(), (size_t)V * 16, cudaMemcpyHostToDevice, s), "mvc upload");
+  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_tris.p, t4.data(), (size_t)F * 16, cudaMemcpyHostToDevice, s), "mvc upload");
+  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_vf_off.p, off.data(), (size_t)(V + 1) * 4, cudaMemcpyHostToDevice, s), "mvc upload");
+  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_vf_list.p, list.data(), (size_t)F * 12, cudaMemcpyHostToDevice, s), "mvc upload");
+  CGS_CUDA(cudaStreamSynchronize(s), "mvc upload");
+  ctx->mvc_V = V;
+  ctx->mvc_F = F;
+  ctx->mvc_ready = true;
+  ctx->mvc_last_verts.assign(rest, rest + 3 * (size_t)V);
+  if (ctx->mvc_nb) {
+    ctx->mvc_nb = 0;
+    ctx->deformed_valid = false;
+    ctx->deform_generation++;
+  }
+  return CGS_OK;
+}
+
+int cgs_mvc_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t V) {
+  if (!ctx || !verts) return CGS_E_ARG;
+  if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
+  if (V != ctx->mvc_V) return ctx->fail(CGS_E_ARG, "vertex count differs from the polygon cage");
+  const size_t cnt = (size_t)V * 3;
+  if (ctx->mvc_last_verts.size() == cnt && std::memcmp(ctx->mvc_last_verts.data(), verts, cnt * 4) == 0)
+    return CGS_OK;
+  cudaSetDevice(ctx->device);
+  std::vector<float4> v4(V);
+  for (uint32_t j = 0; j < V; ++j) v4[j] = make_float4(verts[3 * j], verts[3 * j + 1], verts[3 * j + 2], 0.0f);
+  // a pageable staging vector: the copy has completed when the call returns
+  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_verts.p, v4.data(), (size_t)V * 16, cudaMemcpyHostToDevice, ctx->stream),
+           "mvc vertices");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "mvc vertices");
+  ctx->mvc_last_verts.assign(verts, verts + cnt);
+  if (ctx->mvc_nb) ctx->deformed_valid = false;
+  return CGS_OK;
+}
+
+int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
+  if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  cudaStream_t s = ctx->stream;
+  const uint32_t n = ctx->n;
+  if (!ctx->has_cages) {
+    CGS_TRY(ctx->ensure(ctx->bind_tet, (size_t)(n ? n : 1) * 4, "bindings"));
+    CGS_TRY(ctx->ensure(ctx->bind_w, (size_t)(n ? n : 1) * 16, "binding weights"));
+    CGS_CUDA(cudaMemsetAsync(ctx->bind_tet.p, 0xFF, (size_t)(n ? n : 1) * 4, s), "clear bindings");
+    CGS_CUDA(cudaMemsetAsync(ctx->bind_w.p, 0, (size_t)(n ? n : 1) * 16, s), "clear bindings");
+  }
+  uint32_t nb = 0;
+  if (n) {
+    DevBuf flag, slot;
+    const size_t scan_status = ((size_t)scan_tiles(n) + 1) * 8 + 64;
+    CGS_CUDA(cudaMalloc(&flag.p, (size_t)n * 4), "mvc flags");
+    flag.cap = (size_t)n * 4;
+    CGS_CUDA(cudaMalloc(&slot.p, (size_t)n * 4 + scan_status), "mvc slots");
+    slot.cap = (size_t)n * 4 + scan_status;
+    char* sb = slot.as<char>() + (size_t)n * 4;
+    int rc = CGS_OK;
+    cudaError_t e = cudaMemsetAsync(sb, 0, scan_status, s);
+    const MvcCage rest = ctx->mvc_cage(true);
+    if (e == cudaSuccess)
+      e = launch_mvc_inside(rest, n, ctx->rest_pos.as<float4>(), ctx->bind_tet.as<uint32_t>(),
+                            flag.as<uint32_t>(), s);
+    uint32_t* words = (uint32_t*)(sb + scan_status - 64);
+    if (e == cudaSuccess)
+      e = launch_scan_u32(flag.as<uint32_t>(), slot.as<uint32_t>(), n, words,
+                          (unsigned long long*)sb, words + 1, words + 2, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nb, words, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && nb) {
+      const size_t wg_bytes = (size_t)nb * ctx->mvc_V * 16;
+      if ((rc = ctx->ensure(ctx->mvc_list, (size_t)nb * 4, "mvc slots")) == CGS_OK &&
+          (rc = ctx->ensure(ctx->mvc_wg, wg_bytes, "mvc bindings")) == CGS_OK &&
+          (rc = ctx->ensure(ctx->mvc_xf, (size_t)nb * 48, "mvc position/gradient")) == CGS_OK &&
+          (rc = ctx->ensure(ctx->mvc_R, (size_t)nb * 36, "mvc rotations")) == CGS_OK) {
+        e = launch_mvc_compact(n, flag.as<uint32_t>(), slot.as<uint32_t>(),
+                               ctx->bind_tet.as<uint32_t>(), ctx->bind_w.as<float4>(),
+                               ctx->mvc_list.as<uint32_t>(), s);
+        if (e == cudaSuccess)
+          e = launch_mvc_bind_weights(rest, nb, ctx->mvc_list.as<uint32_t>(),
+                                      ctx->rest_pos.as<float4>(), ctx->mvc_h,
+                                      ctx->mvc_wg.as<float4>(), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      }
+    }
+    cudaFree(flag.p);
+    cudaFree(slot.p);
+    flag.p = slot.p = nullptr;
+    if (rc != CGS_OK) return rc;
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "mvc binding");
+  }
+  ctx->mvc_nb = nb;
+  ctx->deformed_valid = false;
+  ctx->deform_generation++;
+  ctx->s3_valid = false;
+  if (out_bound) *out_bound = nb;
+  return CGS_OK;
+}
+
+int cgs_mvc_weights(cgs_ctx* ctx, uint64_t n, const float* d_points, float* d_weights) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
+  if (n == 0) return CGS_OK;
+  if (!d_points || !d_weights) return CGS_E_ARG;
+  if (n > 0xFFFFFFFFull) return ctx->fail(CGS_E_CAPACITY, "at most 2^32 - 1 points");
+  cudaSetDevice(ctx->device);
+  CGS_CUDA(launch_mvc_weights(ctx->mvc_cage(true), (uint32_t)n, d_points, d_weights, ctx->stream),
+           "mvc weights launch");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "mvc weights");
+  return CGS_OK;
+}
+
+int cgs_mvc_read_bindings(cgs_ctx* ctx, uint64_t max_slots, uint32_t* gaussian, float* wg,
+                          uint64_t* out_slots) {
+  if (!ctx || !out_slots) return CGS_E_ARG;
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  const uint64_t k = std::min<uint64_t>(max_slots, ctx->mvc_nb);
+  *out_slots = k;
+  if (k == 0) return CGS_OK;
+  const uint32_t V = ctx->mvc_V, nb = ctx->mvc_nb;
+  if (gaussian)
+    CGS_CUDA(cudaMemcpy(gaussian, ctx->mvc_list.p, k * 4, cudaMemcpyDeviceToHost), "read mvc slots");
+  if (wg) {
+    // vertex-major on the device: row j holds every slot's entry for vertex j
+    std::vector<float4> row(k);
+    for (uint32_t j = 0; j < V; ++j) {
+      CGS_CUDA(cudaMemcpy(row.data(), ctx->mvc_wg.as<float4>() + (size_t)j * nb, k * 16,
+                          cudaMemcpyDeviceToHost), "read mvc bindings");
+      for (uint64_t i = 0; i < k; ++i) std::memcpy(wg + 4 * ((size_t)i * V + j), &row[i], 16);
+    }
+  }
   return CGS_OK;
 }
 
@@ -899,12 +1105,13 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   if (d.write_f32) CGS_TRY(ctx->ensure(ctx->fb_f32, (size_t)W * H * 16, "f32 framebuffer"));
 
   const uint32_t n = ctx->n;
-  const bool has_cages = ctx->has_cages;
+  const bool has_cages = ctx->has_cages;   // tet cages
+  const bool deform_on = ctx->deform_on();  // tet and/or polygon cage bindings
   const uint32_t split_bits = fbits(params->strain_split_threshold), mip_bits = fbits(params->mip_filter_3d_var);
   const bool params_changed = split_bits != ctx->last_split_bits || mip_bits != ctx->last_mip_bits;
-  const bool need_deform = has_cages && (!ctx->deformed_valid || params_changed);
+  const bool need_deform = deform_on && (!ctx->deformed_valid || params_changed);
   d.n = n;
-  d.split_possible = has_cages && params->strain_split_threshold > 0.0f;
+  d.split_possible = deform_on && params->strain_split_threshold > 0.0f;
   d.max_n = d.split_possible ? 2 * n : n;
   const uint32_t mn = d.max_n ? d.max_n : 1u;
   d.key64 = d.total_tiles > 65535u;
@@ -932,6 +1139,8 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     CGS_TRY(ctx->ensure(ctx->tet_J, (size_t)ctx->num_tets * 36, "tet J"));
     CGS_TRY(ctx->ensure(ctx->tet_R, (size_t)ctx->num_tets * 36, "tet R"));
     CGS_TRY(ctx->ensure(ctx->tet_S, (size_t)ctx->num_tets * 4, "tet stretch"));
+  }
+  if (deform_on) {
     CGS_TRY(ctx->ensure(ctx->def_pos, (size_t)mn * 16, "deformed positions"));
     CGS_TRY(ctx->ensure(ctx->def_cova, (size_t)mn * 16, "deformed covariances"));
     CGS_TRY(ctx->ensure(ctx->def_covb, (size_t)mn * 8, "deformed covariances"));
@@ -941,7 +1150,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   // Stage 3 cache key (gpu_state.rs:454-500). A hit needs the frame that
   // built the cache to have been checked.
   Stage3Key key;
-  key.deform_generation = has_cages ? (need_deform ? ctx->deform_generation + 1 : ctx->deform_generation) : 0;
+  key.deform_generation = deform_on ? (need_deform ? ctx->deform_generation + 1 : ctx->deform_generation) : 0;
   for (int k = 0; k < 16; ++k) key.view[k] = fbits(camera->view[k]);
   key.fx = fbits(camera->focal_x);
   key.fy = fbits(camera->focal_y);
@@ -999,9 +1208,21 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     da.fc = fc;
     da.split_threshold = params->strain_split_threshold;
     da.mip = params->mip_filter_3d_var;
-    ctx->kbegin(CGS_K_TET_TRANSFORMS);
-    CGS_CUDA(launch_tet_transforms(da, s), "tet transforms launch");
-    ctx->kend();
+    if (!has_cages) da.num_tets = 0;
+    if (ctx->mvc_nb) {
+      da.mvc_xf = ctx->mvc_xf.as<float4>();
+      da.mvc_R = ctx->mvc_R.as<float>();
+      ctx->kbegin(CGS_K_MVC);
+      CGS_CUDA(launch_mvc_jacobian(ctx->mvc_V, ctx->mvc_verts.as<float4>(), ctx->mvc_nb,
+                                   ctx->mvc_wg.as<float4>(), ctx->mvc_xf.as<float4>(), s),
+               "mvc jacobian launch");
+      ctx->kend();
+    }
+    if (has_cages) {
+      ctx->kbegin(CGS_K_TET_TRANSFORMS);
+      CGS_CUDA(launch_tet_transforms(da, s), "tet transforms launch");
+      ctx->kend();
+    }
     ctx->kbegin(CGS_K_DEFORM);
     CGS_CUDA(launch_deform(da, s), "deform launch");
     ctx->kend();
@@ -1013,13 +1234,15 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
 
   // ---------------- Stage 2
   ProjectArgs p{};
-  if (has_cages) {
+  if (deform_on) {
     p.pos = ctx->def_pos.as<float4>();
     p.cova = ctx->def_cova.as<float4>();
     p.covb = ctx->def_covb.as<float2>();
     p.bind_tet = ctx->bind_tet.as<uint32_t>();
-    p.tet_R = ctx->tet_R.as<float>();
-    p.num_tets = ctx->num_tets;
+    p.bind_w = ctx->bind_w.as<float4>();
+    p.tet_R = has_cages ? ctx->tet_R.as<float>() : nullptr;
+    p.num_tets = has_cages ? ctx->num_tets : 0;
+    p.mvc_R = ctx->mvc_nb ? ctx->mvc_R.as<float>() : nullptr;
     p.split_meta = ctx->split_meta.as<uint2>();
     p.split_count = d.split_possible ? d_split : nullptr;
   } else {
@@ -1034,7 +1257,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   p.max_n = d.max_n;
   std::memcpy(p.cam, camera, 24 * sizeof(float));
   std::memcpy(p.cam_pos, comp->camera_position, 3 * sizeof(float));
-  p.mip = has_cages ? 0.0f : params->mip_filter_3d_var;
+  p.mip = deform_on ? 0.0f : params->mip_filter_3d_var;
   p.min_opacity = params->min_opacity;
   p.min_radius = params->min_radius_px;
   p.sh_degree = comp->sh_degree > 3 ? 3 : comp->sh_degree;
@@ -1172,6 +1395,7 @@ int cgs_invalidate(cgs_ctx* ctx) {
   ctx->scene_ready = false;
   ctx->has_cages = false;
   ctx->num_tets = 0;
+  ctx->mvc_nb = 0;
   ctx->deformed_valid = false;
   ctx->verts_uploaded = false;
   ctx->last_verts.clear();
@@ -1201,7 +1425,7 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
   switch (which) {
     case CGS_BUF_DEFORMED_POS:
     case CGS_BUF_DEFORMED_OPA: {
-      if (!ctx->has_cages) return ctx->fail(CGS_E_STATE, "no cages: no deformed scene");
+      if (!ctx->deform_on()) return ctx->fail(CGS_E_STATE, "no cages: no deformed scene");
       CGS_TRY(fetch(ctx->def_pos, active * 16));
       const float* f = (const float*)tmp.data();
       if (which == CGS_BUF_DEFORMED_POS) {
@@ -1218,7 +1442,7 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
       break;
     }
     case CGS_BUF_DEFORMED_COV: {
-      if (!ctx->has_cages) return ctx->fail(CGS_E_STATE, "no cages: no deformed scene");
+      if (!ctx->deform_on()) return ctx->fail(CGS_E_STATE, "no cages: no deformed scene");
       CGS_TRY(fetch(ctx->def_cova, active * 16));
       std::vector<char> a = tmp;
       CGS_TRY(fetch(ctx->def_covb, active * 8));
@@ -1336,6 +1560,10 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
       CGS_TRY(fetch(ctx->tet_R, (size_t)ctx->num_tets * 36));
       out = tmp;
       break;
+    case CGS_BUF_MVC_ROTATIONS:
+      CGS_TRY(fetch(ctx->mvc_R, (size_t)ctx->mvc_nb * 36));
+      out = tmp;
+      break;
     case CGS_BUF_TET_STRETCH:
       CGS_TRY(fetch(ctx->tet_S, (size_t)ctx->num_tets * 4));
       out = tmp;
@@ -1354,7 +1582,7 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
 const char* cgs_kernel_name(int32_t id) {
   static const char* names[CGS_KERNEL_COUNT] = {"clear", "tet_transforms", "deform", "project",
                                                 "bin", "entry_sort", "tile_ranges", "composite",
-                                                "splat_sort"};
+                                                "splat_sort", "mvc"};
   return (id >= 0 && id < CGS_KERNEL_COUNT) ? names[id] : "unknown";
 }
 

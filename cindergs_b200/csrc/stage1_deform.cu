@@ -155,6 +155,149 @@ __device__ __forceinline__ void mip3d(float& xx, float xy, float xz, float& yy, 
   alpha = clampf(alpha * comp, 0.0f, 1.0f);
 }
 
+// ---- CPU-path semantics for MVC-bound Gaussians ------------------------------
+// The reference deforms polygon-cage (MVC) bindings only on its CPU path
+// (PolyCageMesh::deform_scene_cpu, deformation/mvc.rs:564-749), so these
+// helpers follow glam 0.28's Mat3 operation order and the f64 eigen-solver of
+// math/covariance.rs instead of the GPU tet kernel's.
+struct GM3 {
+  float c[9];  // column-major: c[3 * col + row]
+};
+__device__ __forceinline__ GM3 gm3_mul(const GM3& A, const GM3& B) {
+  GM3 C;
+#pragma unroll
+  for (int col = 0; col < 3; ++col)
+#pragma unroll
+    for (int row = 0; row < 3; ++row)
+      C.c[3 * col + row] = (A.c[row] * B.c[3 * col] + A.c[3 + row] * B.c[3 * col + 1]) +
+                           A.c[6 + row] * B.c[3 * col + 2];
+  return C;
+}
+__device__ __forceinline__ GM3 gm3_t(const GM3& A) {
+  GM3 T;
+#pragma unroll
+  for (int col = 0; col < 3; ++col)
+#pragma unroll
+    for (int row = 0; row < 3; ++row) T.c[3 * col + row] = A.c[3 * row + col];
+  return T;
+}
+__device__ __forceinline__ void gcross(const float* a, const float* b, float* o) {
+  o[0] = a[1] * b[2] - b[1] * a[2];
+  o[1] = a[2] * b[0] - b[2] * a[0];
+  o[2] = a[0] * b[1] - b[0] * a[1];
+}
+__device__ __forceinline__ float gdot(const float* a, const float* b) {
+  return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+}
+__device__ __forceinline__ float gm3_det(const GM3& A) {
+  float x[3];
+  gcross(A.c, A.c + 3, x);
+  return gdot(A.c + 6, x);
+}
+// Mat3::inverse: cofactor columns by cross products, scaled by 1/det, transposed.
+__device__ __forceinline__ GM3 gm3_inverse(const GM3& A) {
+  float t0[3], t1[3], t2[3];
+  gcross(A.c + 3, A.c + 6, t0);
+  gcross(A.c + 6, A.c, t1);
+  gcross(A.c, A.c + 3, t2);
+  const float inv = 1.0f / gdot(A.c + 6, t2);
+  GM3 R;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    R.c[3 * k + 0] = t0[k] * inv;
+    R.c[3 * k + 1] = t1[k] * inv;
+    R.c[3 * k + 2] = t2[k] * inv;
+  }
+  return R;
+}
+// higham_polar_decomposition (deformation/polar.rs:13-42), rotation only.
+__device__ GM3 polar_rotation(const GM3& J) {
+  GM3 r = {{1, 0, 0, 0, 1, 0, 0, 0, 1}};
+  const float det = gm3_det(J);
+  if (fabsf(det) < 1e-8f) return r;
+  const float gamma = cgs_powf(fabsf(det), -1.0f / 3.0f);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r.c[k] = J.c[k] * gamma;
+  for (int it = 0; it < 5; ++it) {
+    const GM3 rit = gm3_t(gm3_inverse(r));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) r.c[k] = 0.5f * (r.c[k] + rit.c[k]);
+  }
+  if (gm3_det(r) < 0.0f)
+    for (int k = 6; k < 9; ++k) r.c[k] = -r.c[k];
+  return r;
+}
+// symmetric_eigen_3x3 (math/covariance.rs:181-265): f64 cyclic Jacobi, 12
+// sweeps; eigenvalues descending, right-handed basis (columns).
+__device__ void sym_eigen3_f64(const float* cov, float* evals, GM3& basis) {
+  double a[3][3] = {{cov[0], cov[1], cov[2]}, {cov[1], cov[3], cov[4]}, {cov[2], cov[4], cov[5]}};
+  double v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int sweep = 0; sweep < 12; ++sweep) {
+    for (int e = 0; e < 3; ++e) {
+      const int p = e == 2 ? 1 : 0, q = e == 0 ? 1 : 2;
+      const double apq = a[p][q];
+      if (fabs(apq) <= 1e-15) continue;
+      const double tau = (a[q][q] - a[p][p]) / (2.0 * apq);
+      const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau))
+                                  : -1.0 / (-tau + sqrt(1.0 + tau * tau));
+      const double c = 1.0 / sqrt(1.0 + t * t);
+      const double s = t * c;
+      const double app = a[p][p], aqq = a[q][q];
+      a[p][p] = app - t * apq;
+      a[q][q] = aqq + t * apq;
+      a[p][q] = 0.0;
+      a[q][p] = 0.0;
+      const int r = 3 - p - q;  // the remaining index
+      const double arp = a[r][p], arq = a[r][q];
+      a[r][p] = c * arp - s * arq;
+      a[p][r] = a[r][p];
+      a[r][q] = s * arp + c * arq;
+      a[q][r] = a[r][q];
+      for (int k = 0; k < 3; ++k) {
+        const double vrp = v[k][p], vrq = v[k][q];
+        v[k][p] = c * vrp - s * vrq;
+        v[k][q] = s * vrp + c * vrq;
+      }
+    }
+  }
+  double ev[3] = {a[0][0], a[1][1], a[2][2]};
+  double vec[3][3];
+  for (int k = 0; k < 3; ++k) {
+    const double x = v[0][k], y = v[1][k], z = v[2][k];
+    const double inv = 1.0 / sqrt((x * x + y * y) + z * z);
+    vec[k][0] = x * inv;
+    vec[k][1] = y * inv;
+    vec[k][2] = z * inv;
+  }
+  int ord[3] = {0, 1, 2};  // stable sort by eigenvalue, descending
+  for (int i = 1; i < 3; ++i)
+    for (int j = i; j > 0 && ev[ord[j - 1]] < ev[ord[j]]; --j) {
+      const int t = ord[j];
+      ord[j] = ord[j - 1];
+      ord[j - 1] = t;
+    }
+  for (int k = 0; k < 3; ++k) {
+    evals[k] = (float)ev[ord[k]];
+    for (int j = 0; j < 3; ++j) basis.c[3 * k + j] = (float)vec[ord[k]][j];
+  }
+  if (gm3_det(basis) < 0.0f)
+    for (int j = 0; j < 3; ++j) basis.c[6 + j] = -basis.c[6 + j];
+}
+// covariance_determinant (math/covariance.rs:113-123) in f64, rounded to f32.
+__device__ __forceinline__ float cov_det_f64(const float* c) {
+  const double xx = c[0], xy = c[1], xz = c[2], yy = c[3], yz = c[4], zz = c[5];
+  return (float)(xx * (yy * zz - yz * yz) - xy * (xy * zz - xz * yz) + xz * (xy * yz - xz * yy));
+}
+// apply_mip_filter_3d (math/covariance.rs:288-305).
+__device__ __forceinline__ void mip3d_cpu(float* cov, float& alpha, float var) {
+  const float d0 = fmaxf(cov_det_f64(cov), 1e-24f);
+  cov[0] = cov[0] + var;
+  cov[3] = cov[3] + var;
+  cov[5] = cov[5] + var;
+  const float dr = fmaxf(cov_det_f64(cov), d0);
+  alpha = clampf(alpha * sqrtf(clampf(d0 / dr, 0.0f, 1.0f)), 0.0f, 1.0f);
+}
+
 template <bool SPLIT>
 __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
   __shared__ uint32_t s_tile;
@@ -180,7 +323,60 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
     const float4 rp = a.rest_pos[i];
     const float4 rca = a.rest_cova[i];
     const float2 rcb = a.rest_covb[i];
-    if (tet_raw >= a.num_tets) {
+    if (tet_raw == kMvcBound && a.mvc_xf) {
+      // Polygon-cage binding (deform_scene_cpu, mvc.rs:616-749): position and
+      // F from k_mvc_jacobian, rotation for SH, F S F^T, opacity unchanged.
+      const uint32_t slot = __float_as_uint(a.bind_w[i].x);
+      const float4 q0 = a.mvc_xf[3 * (size_t)slot], q1 = a.mvc_xf[3 * (size_t)slot + 1],
+                   q2 = a.mvc_xf[3 * (size_t)slot + 2];
+      const GM3 Fm = {{q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
+      const GM3 R = polar_rotation(Fm);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a.mvc_R[9 * (size_t)slot + k] = R.c[k];
+      const GM3 S = {{rca.x, rca.y, rca.z, rca.y, rca.w, rcb.x, rca.z, rcb.x, rcb.y}};
+      const GM3 m = gm3_mul(gm3_mul(Fm, S), gm3_t(Fm));
+      float cv[6] = {m.c[0], m.c[1], m.c[2], m.c[4], m.c[5], m.c[8]};
+      float alpha = rp.w;
+      if (SPLIT && a.split_threshold > 0.0f) {
+        // jacobian_singular_values (polar.rs:89-109): sigma_1 of F
+        const GM3 C = gm3_mul(gm3_t(Fm), Fm);
+        const float packed[6] = {C.c[0], C.c[1], C.c[2], C.c[4], C.c[5], C.c[8]};
+        float ev[3];
+        GM3 basis;
+        sym_eigen3_f64(packed, ev, basis);
+        split = sqrtf(fmaxf(ev[0], 0.0f)) > a.split_threshold;
+      }
+      if (!split) {
+        if (a.mip > 0.0f) mip3d_cpu(cv, alpha, a.mip);
+        out_pos = make_float4(q0.x, q0.y, q0.z, alpha);
+      } else {
+        // split_gaussian_along_major_axis (math/covariance.rs:331-378)
+        float ev[3];
+        GM3 B;
+        sym_eigen3_f64(cv, ev, B);
+        const float min_var = 1e-4f * 1e-4f;
+        const GM3 D = {{fmaxf(ev[0] * 0.25f, min_var), 0, 0, 0, fmaxf(ev[1], min_var), 0, 0, 0,
+                        fmaxf(ev[2], min_var)}};
+        float ax[3] = {B.c[0], B.c[1], B.c[2]};
+        const float len2 = gdot(ax, ax);
+        if (len2 > 0.0f) {
+          const float inv = 1.0f / sqrtf(len2);
+          ax[0] *= inv; ax[1] *= inv; ax[2] *= inv;
+        }
+        const float om = 0.5f * sqrtf(fmaxf(ev[0], min_var));
+        const GM3 cm = gm3_mul(gm3_mul(B, D), gm3_t(B));
+        cv[0] = cm.c[0]; cv[1] = cm.c[1]; cv[2] = cm.c[2];
+        cv[3] = cm.c[4]; cv[4] = cm.c[5]; cv[5] = cm.c[8];
+        if (a.mip > 0.0f) mip3d_cpu(cv, alpha, a.mip);
+        const float ox = ax[0] * om, oy = ax[1] * om, oz = ax[2] * om;
+        out_pos = make_float4(q0.x + (-ox), q0.y + (-oy), q0.z + (-oz), alpha);
+        cx = q0.x + ox;
+        cy = q0.y + oy;
+        cz = q0.z + oz;
+      }
+      out_cova = make_float4(cv[0], cv[1], cv[2], cv[3]);
+      out_covb = make_float2(cv[4], cv[5]);
+    } else if (tet_raw >= a.num_tets) {
       // Unbound: rest pose plus the Mip filter (deformation.rs:899-947).
       float xx = rca.x, xy = rca.y, xz = rca.z, yy = rca.w, yz = rcb.x, zz = rcb.y;
       float alpha = rp.w;

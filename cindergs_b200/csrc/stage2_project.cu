@@ -220,8 +220,12 @@ __global__ void __launch_bounds__(kProjectThreads) k_project(const ProjectArgs a
         sh_idx = m.x;
         tet_raw = m.y;
       }
-      if (a.tet_R && tet_raw < a.num_tets) {
-        const float* R = a.tet_R + 9 * (size_t)tet_raw;
+      const float* R = nullptr;
+      if (a.tet_R && tet_raw < a.num_tets)
+        R = a.tet_R + 9 * (size_t)tet_raw;
+      else if (a.mvc_R && tet_raw == kMvcBound)
+        R = a.mvc_R + 9 * (size_t)__float_as_uint(a.bind_w[sh_idx].x);
+      if (R) {
         const float ldx = __ldg(R + 0) * dx + __ldg(R + 1) * dy + __ldg(R + 2) * dz;
         const float ldy = __ldg(R + 3) * dx + __ldg(R + 4) * dy + __ldg(R + 5) * dz;
         const float ldz = __ldg(R + 6) * dx + __ldg(R + 7) * dy + __ldg(R + 8) * dz;

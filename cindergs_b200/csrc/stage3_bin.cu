@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(kPlaceWarps * 32) k_chunk_place(const Transpos
   constexpr uint32_t GW = kTransposeGroupTiles / 2;
   __shared__ uint32_t whist[kPlaceWarps * GW];
   __shared__ uint32_t obase[kTransposeGroupTiles];
-  const uint32_t k = blockIdx.x, g = blockIdx.y, G = a.groups;
+  const uint32_t k = blockIdx.x, g = blockIdx.y;
   const uint32_t t0 = g * a.group_tiles;
   const uint32_t tn = min(a.group_tiles, a.num_tiles - t0);  // tiles of this group
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -82,10 +82,12 @@ class GpuPipelineState:
                                       ctypes.byref(self._ctx))
         if rc != _abi.CGS_OK:
             raise _abi.CgsError(rc, "cgs_ctx_create", "could not create a CUDA context")
+        self.device = int(device)
         self._scene_hash = None
         self._scene_count = -1
         self._cage_key = None
         self._last = None
+        self._mvc_V = 0
 
     # -- lifetime -------------------------------------------------------------
     def close(self) -> None:
@@ -170,6 +172,60 @@ class GpuPipelineState:
                                             mesh.num_vertices, _p(rv), ub, pmin, pmax, _p(tets),
                                             _p(w)), "cgs_bind_tets")
         return tets, w
+
+    # -- polygon cage (mean value coordinates) -----------------------------------
+    def mvc_cage_upload(self, cage) -> None:
+        """Uploads a PolyCageMesh (cindergs_b200.mvc) and drops earlier MVC bindings."""
+        v = np.ascontiguousarray(cage.rest_vertices, f32)
+        t = np.ascontiguousarray(cage.triangles, np.uint32)
+        self._check(self._lib.cgs_mvc_cage_upload(self._ctx, v.shape[0], _p(v), t.shape[0], _p(t)),
+                    "cgs_mvc_cage_upload")
+        self._mvc_V = int(v.shape[0])
+
+    def mvc_vertices_update(self, verts) -> None:
+        v = np.ascontiguousarray(verts, f32).reshape(-1, 3)
+        self._check(self._lib.cgs_mvc_vertices_update(self._ctx, _p(v), v.shape[0]),
+                    "cgs_mvc_vertices_update")
+
+    def mvc_bind(self) -> int:
+        """PolyCageMesh::bind_gaussians (mvc.rs:498-541) for the resident scene
+        on the GPU; returns how many Gaussians were bound."""
+        nb = ctypes.c_uint32(0)
+        self._check(self._lib.cgs_mvc_bind(self._ctx, ctypes.byref(nb)), "cgs_mvc_bind")
+        return int(nb.value)
+
+    def mvc_weights(self, points):
+        """Exact MVC weights of points against the rest cage: a torch CUDA
+        tensor [n, 3] -> [n, V] (device), or numpy -> numpy."""
+        import torch
+        host = not (isinstance(points, torch.Tensor) and points.is_cuda)
+        pts = torch.as_tensor(np.asarray(points, f32) if host else points, dtype=torch.float32)
+        pts = pts.reshape(-1, 3).contiguous().to(f"cuda:{self.device}")
+        out = torch.empty((pts.shape[0], self._mvc_V), dtype=torch.float32, device=pts.device)
+        torch.cuda.synchronize(pts.device)
+        self._check(self._lib.cgs_mvc_weights(self._ctx, pts.shape[0], ctypes.c_void_p(pts.data_ptr()),
+                                              ctypes.c_void_p(out.data_ptr())), "cgs_mvc_weights")
+        return out.cpu().numpy() if host else out
+
+    def mvc_read_bindings(self, max_slots: int | None = None):
+        """(gaussian index [k] u32, wg [k, V, 4] f32) of the first k MVC bindings."""
+        k = int(max_slots if max_slots is not None else 1 << 62)
+        cnt = ctypes.c_uint64(0)
+        self._check(self._lib.cgs_mvc_read_bindings(self._ctx, 0, None, None, ctypes.byref(cnt)),
+                    "cgs_mvc_read_bindings")
+        n = min(k, self._mvc_bound_hint()) if k else 0
+        g = np.zeros(max(n, 1), np.uint32)
+        wg = np.zeros((max(n, 1), self._mvc_V, 4), f32)
+        self._check(self._lib.cgs_mvc_read_bindings(self._ctx, n, _p(g), _p(wg), ctypes.byref(cnt)),
+                    "cgs_mvc_read_bindings")
+        n = int(cnt.value)
+        return g[:n], wg[:n]
+
+    def _mvc_bound_hint(self) -> int:
+        cnt = ctypes.c_uint64(0)
+        self._check(self._lib.cgs_mvc_read_bindings(self._ctx, 1 << 62, None, None,
+                                                    ctypes.byref(cnt)), "cgs_mvc_read_bindings")
+        return int(cnt.value)
 
     # -- frame ------------------------------------------------------------------
     def execute_frame_gpu(self, scene: GaussianSceneSoa, cages: CageScene | None,

@@ -144,6 +144,38 @@ int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const 
                   uint32_t num_verts, const float* rest_verts, int32_t use_bounds,
                   const float* bmin, const float* bmax, uint32_t* bind_tet, float* bind_w);
 
+/* ---- polygon cage, mean value coordinates (deformation/mvc.rs) ---- */
+
+/* Uploads a closed, outward-oriented triangle cage (PolyCageMesh,
+ * mvc.rs:15-21): rest vertices [V*3], triangles [F*3]. At most 1,024
+ * vertices; vertices + triangles at most 12,800. Drops earlier MVC
+ * bindings. The current vertices start at the rest pose. */
+int cgs_mvc_cage_upload(cgs_ctx* ctx, uint32_t num_verts, const float* rest_verts,
+                        uint32_t num_tris, const uint32_t* tris);
+
+/* Current (deformed) cage vertices [V*3]; unchanged values are skipped. */
+int cgs_mvc_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_verts);
+
+/* PolyCageMesh::bind_gaussians (mvc.rs:498-541) on the GPU for the resident
+ * scene: Gaussians not bound to a tet cage whose rest centre has |winding
+ * number| >= 0.5 get exact MVC weights and central-difference gradients
+ * (step jacobian_step_size, mvc.rs:484-494), stored on the device
+ * (16 bytes per Gaussian and cage vertex). Tet bindings win over the
+ * polygon cage. Frames then deform the bound Gaussians as deform_scene_cpu
+ * (mvc.rs:564-749) does. *out_bound receives the number bound. */
+int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound);
+
+/* compute_mvc_weights (mvc.rs:366-471) of n points against the rest cage:
+ * d_points [n*3] and d_weights [n*V] are device pointers (no counterpart in
+ * the reference's GPU API). */
+int cgs_mvc_weights(cgs_ctx* ctx, uint64_t n, const float* d_points, float* d_weights);
+
+/* Host copy of the first max_slots MVC bindings: gaussian [slots] (scene
+ * index of each slot, ascending) and wg [slots*V*4] = (w, dw/dx, dw/dy,
+ * dw/dz) per cage vertex. *out_slots receives the number copied. */
+int cgs_mvc_read_bindings(cgs_ctx* ctx, uint64_t max_slots, uint32_t* gaussian, float* wg,
+                          uint64_t* out_slots);
+
 /* ---- frame (GpuPipelineState, render/gpu_state.rs:538-1243) ---- */
 
 /* Runs Stages 1-4 on the resident scene (execute_frame_gpu,
@@ -185,7 +217,8 @@ int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px)
 #define CGS_K_TILE_RANGES 6    /* (the tile transpose writes the ranges itself) */
 #define CGS_K_COMPOSITE 7
 #define CGS_K_SPLAT_SORT 8     /* depth-key histogram + radix passes over the splats */
-#define CGS_KERNEL_COUNT 9
+#define CGS_K_MVC 9            /* MVC position + gradient of every polygon-cage binding */
+#define CGS_KERNEL_COUNT 10
 typedef struct cgs_kernel_profile {
   double ms[CGS_KERNEL_COUNT];
   uint64_t alg_bytes[CGS_KERNEL_COUNT];
@@ -215,6 +248,7 @@ int cgs_invalidate(cgs_ctx* ctx);
 #define CGS_BUF_TET_JACOBIANS 11 /* f32 [tets*9] column-major */
 #define CGS_BUF_TET_ROTATIONS 12 /* f32 [tets*9] column-major */
 #define CGS_BUF_TET_STRETCH 13   /* f32 [tets] */
+#define CGS_BUF_MVC_ROTATIONS 14 /* f32 [MVC slots*9] polar rotations, column-major */
 /* Reads buffer `which` of the last frame into `dst` (capacity dst_bytes);
  * *out_bytes receives the byte size of the valid contents. */
 int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_bytes,

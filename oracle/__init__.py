@@ -78,6 +78,15 @@ def lib():
                                            _vp, _vp]
         L.orc_ref_rasterize.argtypes = [_c_u32, _c_u32, _f32p, _f32p, _f32p, _f32p, _f32p, _u32p,
                                         _u32p, _f32p, _f32p, _c_u32, _vp, _vp]
+        L.orc_mvc_winding.restype = _c_f
+        L.orc_mvc_winding.argtypes = [_c_u32, _f32p, _u32p, _f32p]
+        L.orc_mvc_weights.argtypes = [_c_u32, _f32p, _c_u32, _f32p, _c_u32, _u32p, _f32p]
+        L.orc_mvc_step.restype = _c_f
+        L.orc_mvc_step.argtypes = [_c_u32, _f32p]
+        L.orc_mvc_bind.argtypes = [_c_u32, _f32p, _c_u32, _f32p, _c_u32, _u32p, _u8p, _f32p]
+        L.orc_mvc_deform.restype = _c_u32
+        L.orc_mvc_deform.argtypes = [_c_u32, _f32p, _f32p, _f32p, _u8p, _f32p, _c_u32, _f32p, _c_f,
+                                     _c_f, _f32p, _f32p, _f32p, _u32p, _f32p]
         L.orc_pixel_hash.restype = _c_u64
         L.orc_pixel_hash.argtypes = [_c_u64, _u8p]
         L.orc_ref_render_scene.restype = _c_u64
@@ -414,3 +423,56 @@ def ref_rasterize(W, H, xy, conics, opa, sh, pos, sorted_ids, ranges, bg, cam_po
                             _u32(ranges).ravel(), _f32(bg), _f32(cam_pos), int(sh_degree),
                             _ptr(rgba8), _ptr(f))
     return rgba8.reshape(H, W, 4), f.reshape(H, W, 4)
+
+
+# ---------------------------------------------------------------- MVC (ref)
+def mvc_winding(verts, tris, point) -> float:
+    """PolyCageMesh::winding_number (deformation/mvc.rs:339-357)."""
+    return float(lib().orc_mvc_winding(int(np.asarray(tris).reshape(-1, 3).shape[0]),
+                                       _f32(verts), _u32(tris), _f32(point)))
+
+
+def mvc_weights(points, verts, tris):
+    """compute_mvc_weights (deformation/mvc.rs:366-471) for each point: [n, V]."""
+    pts = _f32(points).reshape(-1, 3)
+    v = _f32(verts).reshape(-1, 3)
+    t = _u32(tris).reshape(-1, 3)
+    out = np.zeros((pts.shape[0], v.shape[0]), np.float32)
+    lib().orc_mvc_weights(pts.shape[0], pts, v.shape[0], v, t.shape[0], t, out)
+    return out
+
+
+def mvc_step(verts) -> float:
+    """jacobian_step_size (deformation/mvc.rs:484-494)."""
+    v = _f32(verts).reshape(-1, 3)
+    return float(lib().orc_mvc_step(v.shape[0], v))
+
+
+def mvc_bind(points, verts, tris):
+    """bind_gaussians (deformation/mvc.rs:498-541): (inside [n] bool, wg [n, V, 4]) with
+    wg[..., 0] the weights and wg[..., 1:] the central-difference gradients."""
+    pts = _f32(points).reshape(-1, 3)
+    v = _f32(verts).reshape(-1, 3)
+    t = _u32(tris).reshape(-1, 3)
+    inside = np.zeros(pts.shape[0], np.uint8)
+    wg = np.zeros((pts.shape[0], v.shape[0], 4), np.float32)
+    lib().orc_mvc_bind(pts.shape[0], pts, v.shape[0], v, t.shape[0], t, inside, wg)
+    return inside.astype(bool), wg
+
+
+def mvc_deform(pos, cov, opa, inside, wg, deformed_verts, split_thr=0.0, mip=0.0):
+    """deform_scene_cpu (deformation/mvc.rs:564-749) without SH coefficient
+    rotation; returns dict(pos, cov, opa, parent, R) with children appended."""
+    pos = _f32(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    V = np.asarray(deformed_verts).reshape(-1, 3).shape[0]
+    op = np.zeros((2 * n, 3), np.float32)
+    oc = np.zeros((2 * n, 6), np.float32)
+    oa = np.zeros(2 * n, np.float32)
+    par = np.zeros(max(n, 1), np.uint32)
+    R = np.zeros((n, 9), np.float32)
+    total = lib().orc_mvc_deform(n, pos, _f32(cov).reshape(-1, 6), _f32(opa),
+                                 np.ascontiguousarray(inside, np.uint8),
+                                 _f32(wg).reshape(-1), V, _f32(deformed_verts).reshape(-1, 3),
+                                 float(split_thr), float(mip), op, oc, oa, par, R)
+    return dict(pos=op[:total], cov=oc[:total], opa=oa[:total], parent=par[:total - n], R=R)

@@ -892,6 +892,122 @@ void ref_mip3d(float* cov, float* opa, float var) {
   *opa = clampf(*opa * comp, 0.0f, 1.0f);
 }
 
+// ---------------------------------------------------------------- MVC (ref)
+// PolyCageMesh (deformation/mvc.rs) in f32 with glam 0.28's Vec3/Mat3 order:
+// length = sqrt(dot), dot = (x*x + y*y) + z*z, Vec3 / f32 per component.
+struct V3 {
+  float x, y, z;
+};
+inline V3 v3(const float* p) { return {p[0], p[1], p[2]}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 operator/(V3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+inline float vdot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline float vlen(V3 a) { return std::sqrt(vdot(a, a)); }
+inline V3 vcross(V3 a, V3 b) {
+  return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+
+// winding_number (mvc.rs:339-357).
+float mvc_winding(uint32_t F, const float* verts, const uint32_t* tris, V3 p) {
+  float sum = 0.0f;
+  for (uint32_t f = 0; f < F; ++f) {
+    const V3 a = v3(verts + 3 * tris[3 * f]) - p;
+    const V3 b = v3(verts + 3 * tris[3 * f + 1]) - p;
+    const V3 c = v3(verts + 3 * tris[3 * f + 2]) - p;
+    const float la = vlen(a), lb = vlen(b), lc = vlen(c);
+    if (la < 1e-7f || lb < 1e-7f || lc < 1e-7f) return 1.0f;
+    const float det = vdot(a, vcross(b, c));
+    const float denom = ((la * lb * lc + vdot(a, b) * lc) + vdot(b, c) * la) + vdot(c, a) * lb;
+    sum += 2.0f * std::atan2(det, denom);
+  }
+  return sum / (4.0f * (float)M_PI);
+}
+
+// compute_mvc_weights (mvc.rs:366-471), Ju, Schaefer & Warren 2005.
+void mvc_weights(uint32_t V, uint32_t F, const float* verts, const uint32_t* tris, V3 x,
+                 float* w) {
+  std::vector<float> dists(V);
+  std::vector<V3> dirs(V);
+  for (uint32_t i = 0; i < V; ++i) {
+    const V3 diff = v3(verts + 3 * i) - x;
+    const float d = vlen(diff);
+    if (d < 1e-6f) {
+      for (uint32_t j = 0; j < V; ++j) w[j] = 0.0f;
+      w[i] = 1.0f;
+      return;
+    }
+    dists[i] = d;
+    dirs[i] = diff / d;
+  }
+  for (uint32_t j = 0; j < V; ++j) w[j] = 0.0f;
+  float total = 0.0f;
+  const float PI_F = (float)M_PI;
+  for (uint32_t f = 0; f < F; ++f) {
+    const uint32_t i0 = tris[3 * f], i1 = tris[3 * f + 1], i2 = tris[3 * f + 2];
+    const V3 u0 = dirs[i0], u1 = dirs[i1], u2 = dirs[i2];
+    const float l0 = vlen(u1 - u2), l1 = vlen(u2 - u0), l2 = vlen(u0 - u1);
+    const float t0 = 2.0f * std::asin(clampf(l0 * 0.5f, 0.0f, 1.0f));
+    const float t1 = 2.0f * std::asin(clampf(l1 * 0.5f, 0.0f, 1.0f));
+    const float t2 = 2.0f * std::asin(clampf(l2 * 0.5f, 0.0f, 1.0f));
+    const float h = 0.5f * ((t0 + t1) + t2);
+    if (std::fabs(PI_F - h) < 1e-5f) {
+      const float w0 = std::sin(t0) * dists[i1] * dists[i2];
+      const float w1 = std::sin(t1) * dists[i2] * dists[i0];
+      const float w2 = std::sin(t2) * dists[i0] * dists[i1];
+      const float sum = (w0 + w1) + w2;
+      for (uint32_t j = 0; j < V; ++j) w[j] = 0.0f;
+      if (std::fabs(sum) > 1e-12f) {
+        w[i0] = w0 / sum;
+        w[i1] = w1 / sum;
+        w[i2] = w2 / sum;
+      }
+      return;
+    }
+    const float st0 = std::sin(t0), st1 = std::sin(t1), st2 = std::sin(t2);
+    if (std::fabs(st0) < 1e-6f || std::fabs(st1) < 1e-6f || std::fabs(st2) < 1e-6f) continue;
+    const float sh = std::sin(h);
+    const float c0 = clampf((2.0f * sh * std::sin(h - t0)) / (st1 * st2) - 1.0f, -1.0f, 1.0f);
+    const float c1 = clampf((2.0f * sh * std::sin(h - t1)) / (st2 * st0) - 1.0f, -1.0f, 1.0f);
+    const float c2 = clampf((2.0f * sh * std::sin(h - t2)) / (st0 * st1) - 1.0f, -1.0f, 1.0f);
+    const float det = vdot(u2, vcross(u0, u1));  // Mat3::from_cols(u0,u1,u2).determinant()
+    const float sg = det >= 0.0f ? 1.0f : -1.0f;
+    const float s0 = sg * std::sqrt(std::fmax(1.0f - c0 * c0, 0.0f));
+    const float s1 = sg * std::sqrt(std::fmax(1.0f - c1 * c1, 0.0f));
+    const float s2 = sg * std::sqrt(std::fmax(1.0f - c2 * c2, 0.0f));
+    if (std::fabs(s0) <= 1e-6f || std::fabs(s1) <= 1e-6f || std::fabs(s2) <= 1e-6f) continue;
+    const float mu0 = ((t0 - c1 * t2) - c2 * t1) / (2.0f * dists[i0] * st1 * s2);
+    const float mu1 = ((t1 - c2 * t0) - c0 * t2) / (2.0f * dists[i1] * st2 * s0);
+    const float mu2 = ((t2 - c0 * t1) - c1 * t0) / (2.0f * dists[i2] * st0 * s1);
+    w[i0] += mu0;
+    w[i1] += mu1;
+    w[i2] += mu2;
+    total += (mu0 + mu1) + mu2;
+  }
+  if (std::fabs(total) > 1e-12f) {
+    const float inv = 1.0f / total;
+    for (uint32_t j = 0; j < V; ++j) w[j] *= inv;
+  } else {
+    uint32_t best = 0;
+    for (uint32_t i = 1; i < V; ++i)
+      if (dists[i] < dists[best]) best = i;
+    w[best] = 1.0f;
+  }
+}
+
+// jacobian_step_size (mvc.rs:484-494).
+float mvc_step(uint32_t V, const float* verts) {
+  V3 mn = {INFINITY, INFINITY, INFINITY}, mx = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = 0; i < V; ++i) {
+    const V3 p = v3(verts + 3 * i);
+    mn = {std::fmin(mn.x, p.x), std::fmin(mn.y, p.y), std::fmin(mn.z, p.z)};
+    mx = {std::fmax(mx.x, p.x), std::fmax(mx.y, p.y), std::fmax(mx.z, p.z)};
+  }
+  const float diag = std::fmax(vlen(mx - mn), 1e-3f);
+  return clampf(diag * 1e-3f, 1e-5f, 1e-2f);
+}
+
 }  // namespace
 
 
@@ -1677,6 +1793,148 @@ uint64_t orc_ref_frame(uint32_t n, const float* pos, const float* cov, const flo
   orc_ref_rasterize(W, H, xy.data(), conic.data(), copa.data(), dsh.data(), dpos.data(),
                     ids.data(), ranges.data(), bg, cam_pos, sh_degree, rgba8, nullptr);
   return e;
+}
+
+// ------------------------------------------------------------ MVC (ref)
+float orc_mvc_winding(uint32_t F, const float* verts, const uint32_t* tris, const float* p) {
+  return mvc_winding(F, verts, tris, v3(p));
+}
+
+void orc_mvc_weights(uint32_t n, const float* pts, uint32_t V, const float* verts, uint32_t F,
+                     const uint32_t* tris, float* w) {
+  parallel_for(n, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) mvc_weights(V, F, verts, tris, v3(pts + 3 * i), w + V * i);
+  });
+}
+
+float orc_mvc_step(uint32_t V, const float* verts) { return mvc_step(V, verts); }
+
+// bind_gaussians (mvc.rs:498-541): inside flag, weights and central-difference
+// gradients (w, dw/dx, dw/dy, dw/dz) per point and cage vertex.
+void orc_mvc_bind(uint32_t n, const float* pts, uint32_t V, const float* verts, uint32_t F,
+                  const uint32_t* tris, uint8_t* inside, float* wg /* [n][V][4] */) {
+  const float h = mvc_step(V, verts);
+  const float inv_2h = 0.5f / h;
+  parallel_for(n, [&](size_t b, size_t e) {
+    std::vector<float> wp(V), wm(V);
+    for (size_t i = b; i < e; ++i) {
+      const V3 p = v3(pts + 3 * i);
+      float* out = wg + 4 * (size_t)V * i;
+      const bool in = std::fabs(mvc_winding(F, verts, tris, p)) >= 0.5f;
+      inside[i] = in ? 1 : 0;
+      if (!in) {
+        for (uint32_t j = 0; j < 4 * V; ++j) out[j] = 0.0f;
+        continue;
+      }
+      mvc_weights(V, F, verts, tris, p, wp.data());
+      for (uint32_t j = 0; j < V; ++j) out[4 * j] = wp[j];
+      for (int axis = 0; axis < 3; ++axis) {
+        float pp[3] = {p.x, p.y, p.z}, pm[3] = {p.x, p.y, p.z};
+        pp[axis] += h;
+        pm[axis] -= h;
+        mvc_weights(V, F, verts, tris, v3(pp), wp.data());
+        mvc_weights(V, F, verts, tris, v3(pm), wm.data());
+        for (uint32_t j = 0; j < V; ++j) out[4 * j + 1 + axis] = (wp[j] - wm[j]) * inv_2h;
+      }
+    }
+  });
+}
+
+// deform_scene_cpu (mvc.rs:564-749) without the SH coefficient rotation:
+// position sum w v, F = sum v g^T (MvcBindings::local_jacobian), rotation by
+// higham_polar_decomposition, covariance F S F^T, opacity unchanged, strain
+// split and 3D Mip. Returns the output count; out_R gets each input Gaussian's
+// rotation (identity when unbound), split children are appended in parent
+// order.
+uint32_t orc_mvc_deform(uint32_t n, const float* pos, const float* cov, const float* opa,
+                        const uint8_t* inside, const float* wg, uint32_t V, const float* dverts,
+                        float split_thr, float mip, float* out_pos, float* out_cov,
+                        float* out_opa, uint32_t* out_parent, float* out_R) {
+  std::vector<float> P(pos, pos + 3 * (size_t)n), C(cov, cov + 6 * (size_t)n), A(opa, opa + n);
+  std::vector<M3> Fs(n);
+  std::vector<uint8_t> split(n, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    M3 I = {{1, 0, 0, 0, 1, 0, 0, 0, 1}};
+    if (out_R) std::memcpy(out_R + 9 * (size_t)i, I.c, 36);
+    if (!inside[i]) continue;
+    const float* row = wg + 4 * (size_t)V * i;
+    V3 p = {0, 0, 0}, c0 = {0, 0, 0}, c1 = {0, 0, 0}, c2 = {0, 0, 0};
+    for (uint32_t j = 0; j < V; ++j) {
+      const V3 v = v3(dverts + 3 * j);
+      p = p + v * row[4 * j];
+      c0 = c0 + v * row[4 * j + 1];
+      c1 = c1 + v * row[4 * j + 2];
+      c2 = c2 + v * row[4 * j + 3];
+    }
+    M3 Fm = {{c0.x, c0.y, c0.z, c1.x, c1.y, c1.z, c2.x, c2.y, c2.z}};
+    Fs[i] = Fm;
+    const M3 R = higham_polar(Fm);
+    if (out_R) std::memcpy(out_R + 9 * (size_t)i, R.c, 36);
+    const float* c = cov + 6 * (size_t)i;
+    M3 S = {{c[0], c[1], c[2], c[1], c[3], c[4], c[2], c[4], c[5]}};
+    M3 m = m3_mul(m3_mul(Fm, S), m3_t(Fm));
+    P[3 * i] = p.x;
+    P[3 * i + 1] = p.y;
+    P[3 * i + 2] = p.z;
+    float* o = &C[6 * (size_t)i];
+    o[0] = m.at(0, 0); o[1] = m.at(0, 1); o[2] = m.at(0, 2);
+    o[3] = m.at(1, 1); o[4] = m.at(1, 2); o[5] = m.at(2, 2);
+    if (split_thr > 0.0f) {
+      M3 Cg = m3_mul(m3_t(Fm), Fm);
+      const float packed[6] = {Cg.at(0, 0), Cg.at(0, 1), Cg.at(0, 2), Cg.at(1, 1), Cg.at(1, 2),
+                               Cg.at(2, 2)};
+      float ev[3];
+      M3 basis;
+      sym_eigen3(packed, ev, &basis);
+      split[i] = std::sqrt(std::fmax(ev[0], 0.0f)) > split_thr ? 1 : 0;
+    }
+  }
+  std::vector<uint32_t> parent;
+  uint32_t total = n;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!split[i]) {
+      if (mip > 0.0f) ref_mip3d(&C[6 * (size_t)i], &A[i], mip);
+      continue;
+    }
+    float ev[3];
+    M3 B;
+    sym_eigen3(&C[6 * (size_t)i], ev, &B);
+    const float min_var = 1e-4f * 1e-4f;
+    const float l0 = std::fmax(ev[0] * 0.25f, min_var), l1 = std::fmax(ev[1], min_var),
+                l2 = std::fmax(ev[2], min_var);
+    float ax[3] = {B.c[0], B.c[1], B.c[2]};
+    const float len2 = dot3(ax, ax);
+    if (len2 > 0.0f) {
+      const float inv = 1.0f / std::sqrt(len2);
+      for (auto& v : ax) v *= inv;
+    }
+    const float om = 0.5f * std::sqrt(std::fmax(ev[0], min_var));
+    M3 D = {{l0, 0, 0, 0, l1, 0, 0, 0, l2}};
+    M3 cm = m3_mul(m3_mul(B, D), m3_t(B));
+    float cc[6] = {cm.at(0, 0), cm.at(0, 1), cm.at(0, 2), cm.at(1, 1), cm.at(1, 2), cm.at(2, 2)};
+    float ca[6], cb[6];
+    std::memcpy(ca, cc, 24);
+    std::memcpy(cb, cc, 24);
+    float aa = A[i], ab = A[i];
+    if (mip > 0.0f) {
+      ref_mip3d(ca, &aa, mip);
+      ref_mip3d(cb, &ab, mip);
+    }
+    float center[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+    for (int k = 0; k < 3; ++k) P[3 * i + k] = center[k] + (-(ax[k] * om));
+    std::memcpy(&C[6 * (size_t)i], ca, 24);
+    A[i] = aa;
+    for (int k = 0; k < 3; ++k) P.push_back(center[k] + ax[k] * om);
+    C.insert(C.end(), cb, cb + 6);
+    A.push_back(ab);
+    parent.push_back(i);
+    ++total;
+  }
+  if (out_pos) std::memcpy(out_pos, P.data(), 12 * (size_t)total);
+  if (out_cov) std::memcpy(out_cov, C.data(), 24 * (size_t)total);
+  if (out_opa) std::memcpy(out_opa, A.data(), 4 * (size_t)total);
+  if (out_parent && !parent.empty()) std::memcpy(out_parent, parent.data(), 4 * parent.size());
+  return total;
 }
 
 }  // extern "C"
