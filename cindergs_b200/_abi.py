@@ -85,13 +85,13 @@ class CgsStageTimings(ctypes.Structure):
 SORT_AUTO, SORT_RADIX, SORT_TRANSPOSE = 0, 1, 2
 
 KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "entry_sort",
-                "tile_ranges", "composite", "splat_sort", "mvc"]
+                "tile_ranges", "composite", "splat_sort", "mvc", "field"]
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 
 class CgsKernelProfile(ctypes.Structure):
     _fields_ = [("ms", ctypes.c_double * KERNEL_COUNT), ("alg_bytes", _u64 * KERNEL_COUNT),
-                ("launches", _u32 * KERNEL_COUNT)]
+                ("launches", _u32 * KERNEL_COUNT), ("alg_flops", _u64 * KERNEL_COUNT)]
 
 
 assert ctypes.sizeof(CgsCamera) == 96
@@ -125,6 +125,16 @@ SIGNATURES = {
     "cgs_mvc_bind": (_i32, [_vp, ctypes.POINTER(_u32)]),
     "cgs_mvc_weights": (_i32, [_vp, _u64, _vp, _vp]),
     "cgs_mvc_read_bindings": (_i32, [_vp, _u64, _vp, _vp, ctypes.POINTER(_u64)]),
+    "cgs_mvc_field_create": (_i32, [_vp, _u64]),
+    "cgs_mvc_field_layout": (_i32, [_vp, _vp, _vp, _vp]),
+    "cgs_mvc_field_params": (_i32, [_vp, _vp, _vp]),
+    "cgs_mvc_field_train": (_i32, [_vp, _u64, _vp, _vp, _u32, _u32, ctypes.c_float, ctypes.c_float,
+                                   _u64, _vp]),
+    "cgs_mvc_field_grads": (_i32, [_vp, _u64, _vp, _vp, ctypes.c_float, _vp, _vp]),
+    "cgs_mvc_field_eval": (_i32, [_vp, _u64, _vp, _vp]),
+    "cgs_mvc_field_infer": (_i32, [_vp, _u64, _vp, _i32, _vp]),
+    "cgs_mvc_bind_learned": (_i32, [_vp, ctypes.c_float, ctypes.POINTER(_u32),
+                                    ctypes.POINTER(_u32)]),
     "cgs_scan_u32": (_int, [_vp, _vp, _vp, _u64, ctypes.POINTER(_u64)]),
     "cgs_sort_pairs_u32": (_int, [_vp, _vp, _vp, _u64, _u32, _i32]),
     "cgs_sort_pairs_u64": (_int, [_vp, _vp, _vp, _vp, _u64, _u32, _i32]),

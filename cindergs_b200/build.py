@@ -30,10 +30,12 @@ UNITS = [
     ("stage3_bin.cu", ["-fmad=false"]),
     ("radix_sort.cu", []),
     ("stage4_composite.cu", []),
+    ("mvc_field.cu", []),
+    ("field.cu", []),
     ("pipeline.cu", []),
     ("noalloc.cu", []),
 ]
-HEADERS = ["common.cuh", "detmath.h", "kernels.h"]
+HEADERS = ["common.cuh", "detmath.h", "kernels.h", "field.h"]
 
 
 def _nvcc() -> str:

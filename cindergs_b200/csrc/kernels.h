@@ -1,6 +1,7 @@
 // Host-side launchers for the sm_100a kernels (one per .cu translation unit).
 // All launchers enqueue on `stream` and return the launch error code.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,6 +63,92 @@ cudaError_t launch_mvc_bind_weights(const MvcCage& c, uint32_t nb, const uint32_
                                     const float4* rest_pos, float h, float4* wg, cudaStream_t s);
 cudaError_t launch_mvc_jacobian(uint32_t V, const float4* verts, uint32_t nb, const float4* wg,
                                 float4* xf, cudaStream_t s);
+// Linear-precision residual |x' - x| / s at each listed rest position, where
+// x' (xf, 3 float4 per slot) is the learned field's position on the rest
+// cage; flag = residual > threshold.
+cudaError_t launch_mvc_residual(uint32_t nb, const uint32_t* list, const float4* rest_pos,
+                                const float4* xf, float inv_scale, float threshold, float* resid,
+                                uint32_t* flag, cudaStream_t s);
+
+// ---- learned MVC field (mvc_field.cu) ------------------------------------------
+constexpr int kFieldBands = 8;
+constexpr int kFieldIn = 64;    // 3 + 6 * bands, zero-padded
+constexpr int kFieldHid = 128;
+constexpr int kEpiF32 = 0, kEpiBias = 1, kEpiBiasSilu = 2;
+// per-frame projection: Pc (128 x 3), pc (3), A3 (3 x 3)
+constexpr int kFieldProj = 3 * kFieldHid + 3 + 9;
+struct FieldMat {  // M = (Vb Vb^T)^-1, row-major 4 x 4
+  float m[16];
+};
+
+struct FieldNet {  // device pointers into one parameter block
+  const __nv_bfloat16 *W1b, *W2b, *W3b, *W4b, *W5b;
+  const float *b1, *b2, *b3, *b4, *b5;
+};
+struct GemmArgs {  // C = A B^T (+ bias), D = bf16(silu(C))
+  const __nv_bfloat16* A;
+  const __nv_bfloat16* B;
+  uint32_t M, N, K, lda, ldb;
+  float* C;
+  uint32_t ldc;
+  const float* bias;
+  __nv_bfloat16* D;
+  uint32_t ldd;
+};
+struct FieldBatch {
+  const float* points;   // [n*3]
+  const float* target;   // [n*V] exact weights or null
+  uint32_t n, V, B, ldw;
+  uint32_t seed;         // 0: rows r % n in order
+  const float* enc;      // [4] centre xyz, 1/s
+  float* x;              // [B*3]
+  float* wt;             // [B*ldw]
+  __nv_bfloat16* a0;     // [B*64]
+};
+struct FieldLoss {
+  const float* z;        // [B*ldz]
+  const float* wt;       // [B*ldw]
+  const float* x;        // [B*3]
+  const float4* verts;   // [V] rest vertices
+  uint32_t B, V, ldz, ldw;
+  float lambda, s2;
+  float M[16];           // (Vb Vb^T)^-1 of the rest cage
+  float* dz;             // [B*ldz]
+  __nv_bfloat16* dzb;    // [B*ldz]
+  float* loss;           // [2] accumulated (weight term, residual term)
+};
+struct FieldInfer {
+  FieldNet net;
+  const float* enc;      // [4]
+  const float* proj;     // [kFieldProj]
+  const uint32_t* gauss; // item -> point index, or null (identity)
+  const float4* points4; // rest positions (xyz), or null
+  const float* points3;  // packed xyz when points4 is null
+  uint32_t first, count, out_first;
+  float4* xf;            // [(out_first + count) * 3]
+};
+size_t field_infer_smem();
+cudaError_t launch_field_gather(const FieldBatch& b, cudaStream_t s);
+cudaError_t launch_gemm_nt(const GemmArgs& g, int epi, cudaStream_t s);
+cudaError_t launch_transpose_f32(const float* in, uint32_t R, uint32_t C, uint32_t ldi,
+                                 __nv_bfloat16* out, uint32_t ldo, cudaStream_t s);
+cudaError_t launch_transpose_bf16(const __nv_bfloat16* in, uint32_t R, uint32_t C, uint32_t ldi,
+                                  __nv_bfloat16* out, uint32_t ldo, cudaStream_t s);
+cudaError_t launch_field_loss(const FieldLoss& l, cudaStream_t s);
+cudaError_t launch_silu_back(uint32_t n, const float* da, const float* pre, float* dpre,
+                             __nv_bfloat16* dpreb, cudaStream_t s);
+cudaError_t launch_colsum(const float* g, uint32_t B, uint32_t N, uint32_t ld, float* out,
+                          cudaStream_t s);
+cudaError_t launch_adam(uint32_t n, float* p, const float* g, float* m, float* v,
+                        __nv_bfloat16* pb, float lr, float b1, float b2, float eps, float c1,
+                        float c2, cudaStream_t s);
+// verts null: the network's own rest position (no linear-precision
+// projection); otherwise the projected weights on current vertices verts.
+cudaError_t launch_field_project(const FieldNet& net, uint32_t V, const float4* rest,
+                                 const float4* verts, const float* M, float* proj,
+                                 cudaStream_t s);
+cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s);
+
 cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s);
 
 struct BindArgs {

@@ -1,0 +1,847 @@
+// Learned MVC weight field on sm_100a: a Fourier-feature encoding feeding a
+// 4 x 128 SiLU MLP with BF16 weights and activations and FP32 accumulation on
+// the tensor cores, whose V outputs are made a partition of unity by adding
+// (1 - sum z) / V to each. It stands in for the exact mean value coordinates
+// (deformation/mvc.rs:366-471) of the Gaussians it reproduces well enough.
+//
+// The partition-of-unity weights w0 are then projected onto the weights that
+// also reproduce linear functions (sum_j w_j v_j = x on the rest cage), the
+// two properties exact MVC has: w = w0 - Vb^T M (Vb w0 - [1; x]) with
+// Vb = [1; rest vertices] (4 x V) and M = (Vb Vb^T)^-1, so affine cage
+// motions are reproduced exactly and the network only carries the rest. The
+// linear-precision residual r = sum_j w0_j v_j - x of the network's own
+// weights decides which Gaussians fall back to exact MVC.
+//
+// Training (forward, backward, Adam) runs as separate kernels over batches of
+// points with exact weights; inference for the frame is one fused kernel that
+// evaluates the network and its forward-mode Jacobian per Gaussian and emits
+// the deformed position and deformation gradient in the layout of the exact
+// path (k_mvc_jacobian). The weights enter the position linearly, so with
+// A = v'^T Vb^T M (3 x 4, v' the current vertices) and A3 its last three
+// columns, x' = sum_j w_j v'_j = v'^T w0 - A3 r = Pc^T h + pc + A3 x, where
+// Pc (128 x 3), pc and A3 are formed once per frame from the output layer
+// and the current and rest vertices; F = Pc^T dh/dx + A3.
+//
+// Network layout (row-major, out x in): W1 [128 x 64], W2..W4 [128 x 128],
+// W5 [V x 128]; biases b1..b4 [128], b5 [V]. Features of x^ = (x - c) / s
+// (c, s: centre and half of the largest extent of the rest cage): x^ (3), then
+// sin and cos of w_b x^_d for bands b = 0..7 (w_b = 2^b pi / 2) and axes d,
+// zero-padded to 64. Layer inputs (features, activations, tangents) are
+// rounded to bf16 in training and inference alike.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "field.h"
+#include "kernels.h"
+
+namespace cgs {
+namespace {
+
+constexpr int kIn = kFieldIn;    // 64 features
+constexpr int kHid = kFieldHid;  // 128
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ float round_bf16(float x) {
+  return __bfloat162float(__float2bfloat16_rn(x));
+}
+
+// D += A B, m16n8k16, A row-major, B column-major, bf16 in, fp32 accumulate.
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float sigmoid_fast(float x) { return 1.0f / (1.0f + __expf(-x)); }
+__device__ __forceinline__ float silu(float x) { return x * sigmoid_fast(x); }
+__device__ __forceinline__ float silu_grad(float x) {
+  const float s = sigmoid_fast(x);
+  return s * (1.0f + x * (1.0f - s));
+}
+
+// Feature j of x^ (value) and its derivatives with respect to x (chain factor
+// 1/s), for j in [0, 64).
+__device__ __forceinline__ void feature(int j, const float* xh, float inv_s, float& f,
+                                        float (&df)[3]) {
+  f = 0.0f;
+  df[0] = df[1] = df[2] = 0.0f;
+  if (j < 3) {
+    f = xh[j];
+    df[j] = inv_s;
+  } else if (j < 3 + 6 * kFieldBands) {
+    const int q = j - 3, b = q / 6, d = (q % 6) >> 1;
+    const float w = (float)(1 << b) * 1.57079632679489662f;
+    float sn, cs;
+    sincosf(w * xh[d], &sn, &cs);
+    if ((q & 1) == 0) {
+      f = sn;
+      df[d] = w * cs * inv_s;
+    } else {
+      f = cs;
+      df[d] = -w * sn * inv_s;
+    }
+  }
+}
+
+// ---- training kernels --------------------------------------------------------
+
+__device__ __forceinline__ uint32_t mix32(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return (uint32_t)((z ^ (z >> 31)) >> 32);
+}
+
+// Batch gather and features: row r uses point idx = mix(seed, r) % n (or r
+// when seed is 0); writes x [B*3], target weights [B x ldw] and features
+// A0 [B x 64] (bf16).
+__global__ void k_field_gather(FieldBatch fb) {
+  const uint32_t r = blockIdx.x;
+  if (r >= fb.B) return;
+  const uint32_t idx = fb.seed ? mix32(((uint64_t)fb.seed << 32) | r) % fb.n : r % fb.n;
+  __shared__ float xh[3];
+  if (threadIdx.x < 3) {
+    const float x = fb.points[3 * (size_t)idx + threadIdx.x];
+    fb.x[3 * (size_t)r + threadIdx.x] = x;
+    xh[threadIdx.x] = (x - fb.enc[threadIdx.x]) * fb.enc[3];
+  }
+  __syncthreads();
+  if (fb.target)
+    for (uint32_t j = threadIdx.x; j < fb.V; j += blockDim.x)
+      fb.wt[(size_t)r * fb.ldw + j] = fb.target[(size_t)idx * fb.V + j];
+  for (int j = threadIdx.x; j < kIn; j += blockDim.x) {
+    float f, df[3];
+    feature(j, xh, fb.enc[3], f, df);
+    fb.a0[(size_t)r * kIn + j] = __float2bfloat16_rn(f);
+  }
+}
+
+// C = A * B^T: A [M x K] bf16 (lda), B [N x K] bf16 (ldb), fp32 accumulate.
+// 64 x 64 tiles, 4 warps of 32 x 32, K in steps of 32 through shared memory
+// (rows padded by 8 bf16, so the fragment loads hit distinct banks).
+// lda, ldb multiples of 8 and 16-byte-aligned rows; edges zero-filled.
+constexpr int kBM = 64, kBN = 64, kBK = 32, kPad = 8;
+
+template <int EPI>
+__global__ void __launch_bounds__(128) k_gemm_nt(GemmArgs g) {
+  __shared__ __align__(16) __nv_bfloat16 As[kBM][kBK + kPad];
+  __shared__ __align__(16) __nv_bfloat16 Bs[kBN][kBK + kPad];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const uint32_t m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.0f;
+  for (uint32_t k0 = 0; k0 < g.K; k0 += kBK) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = tid * 2 + h;  // 16-byte chunk 0..255
+      const int row = c >> 2, col = (c & 3) * 8;
+      const uint32_t ka = k0 + col;
+      uint4 va = make_uint4(0, 0, 0, 0), vb = make_uint4(0, 0, 0, 0);
+      if (m0 + row < g.M) {
+        const __nv_bfloat16* p = g.A + (size_t)(m0 + row) * g.lda + ka;
+        if (ka + 8 <= g.K) {
+          va = *reinterpret_cast<const uint4*>(p);
+        } else {
+          __align__(16) __nv_bfloat16 t[8];
+          for (int e = 0; e < 8; ++e) t[e] = ka + e < g.K ? p[e] : __float2bfloat16_rn(0.0f);
+          va = *reinterpret_cast<const uint4*>(t);
+        }
+      }
+      if (n0 + row < g.N) {
+        const __nv_bfloat16* p = g.B + (size_t)(n0 + row) * g.ldb + ka;
+        if (ka + 8 <= g.K) {
+          vb = *reinterpret_cast<const uint4*>(p);
+        } else {
+          __align__(16) __nv_bfloat16 t[8];
+          for (int e = 0; e < 8; ++e) t[e] = ka + e < g.K ? p[e] : __float2bfloat16_rn(0.0f);
+          vb = *reinterpret_cast<const uint4*>(t);
+        }
+      }
+      *reinterpret_cast<uint4*>(&As[row][col]) = va;
+      *reinterpret_cast<uint4*>(&Bs[row][col]) = vb;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 16) {
+      uint32_t af[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + i * 16 + gq;
+        af[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * tq]);
+        af[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * tq]);
+        af[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 8 + 2 * tq]);
+        af[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 8 + 2 * tq]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int n = wn + j * 8 + gq;
+        const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 2 * tq]);
+        const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 8 + 2 * tq]);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) mma_bf16(acc[i][j], af[i], b0, b1);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t row = m0 + wm + i * 16 + gq + h * 8;
+        if (row >= g.M) continue;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const uint32_t col = n0 + wn + j * 8 + 2 * tq + e;
+          if (col >= g.N) continue;
+          float v = acc[i][j][2 * h + e];
+          if (EPI != kEpiF32) v += g.bias[col];
+          g.C[(size_t)row * g.ldc + col] = v;
+          if (EPI == kEpiBiasSilu) g.D[(size_t)row * g.ldd + col] = __float2bfloat16_rn(silu(v));
+        }
+      }
+}
+
+// out [C x R] bf16 = transpose of in [R x C] (fp32 or bf16).
+template <typename T>
+__global__ void k_transpose(const T* __restrict__ in, uint32_t R, uint32_t C, uint32_t ldi,
+                            __nv_bfloat16* __restrict__ out, uint32_t ldo) {
+  __shared__ float tile[32][33];
+  const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const uint32_t r = r0 + k, c = c0 + threadIdx.x;
+    tile[k][threadIdx.x] = (r < R && c < C) ? (float)in[(size_t)r * ldi + c] : 0.0f;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const uint32_t c = c0 + k, r = r0 + threadIdx.x;
+    if (c < C && r < R) out[(size_t)c * ldo + r] = __float2bfloat16_rn(tile[threadIdx.x][k]);
+  }
+}
+
+// Sums of K values over the block (blockDim.x a multiple of 32, at most 1024);
+// every thread gets the totals. red holds K x 32 floats.
+template <int K>
+__device__ __forceinline__ void block_sums(float (&v)[K], float* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k * 32 + warp] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    float t = 0.0f;
+    for (int w = 0; w < nw; ++w) t += red[k * 32 + w];
+    v[k] = t;
+  }
+}
+
+// u = M[:, 1:4] r: the correction of the weights is u0 + v_j . (u1, u2, u3).
+__device__ __forceinline__ void lp_correction(const float* M, const float (&r)[3], float (&u)[4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) u[a] = M[4 * a + 1] * r[0] + M[4 * a + 2] * r[1] + M[4 * a + 3] * r[2];
+}
+
+// Loss and dL/dz per batch row. w0 = z + (1 - sum z) / V; r = sum_j w0_j v_j
+// - x; w = w0 - Vb^T M (Vb w0 - [1; x]) (Vb w0 = [1; x + r]). L = (1/B)
+// sum_b sum_j (w - w*)^2 + lambda (1/B) sum_b |r|^2 / (3 s^2). dL/dw0 = Pi g
+// + (2 lambda / (3 B s^2)) (r . v_j) with g = 2 (w - w*) / B and the
+// projector Pi = I - Vb^T M Vb; dz = dL/dw0 - mean (the sum in w0). dz is
+// written in fp32 and bf16; the loss terms (residual without lambda) are
+// added to loss[0..1].
+__global__ void k_field_loss(FieldLoss fl) {
+  const uint32_t row = blockIdx.x;
+  if (row >= fl.B) return;
+  __shared__ float red[6 * 32];
+  const float* z = fl.z + (size_t)row * fl.ldz;
+  const float* wt = fl.wt + (size_t)row * fl.ldw;
+  const float* x = fl.x + 3 * (size_t)row;
+  float s1[1] = {0.0f};
+  for (uint32_t j = threadIdx.x; j < fl.V; j += blockDim.x) s1[0] += z[j];
+  block_sums<1>(s1, red);
+  const float add = (1.0f - s1[0]) / (float)fl.V;
+  float s3[3] = {0.0f, 0.0f, 0.0f};
+  for (uint32_t j = threadIdx.x; j < fl.V; j += blockDim.x) {
+    const float w0 = z[j] + add;
+    const float4 v = fl.verts[j];
+    s3[0] += w0 * v.x;
+    s3[1] += w0 * v.y;
+    s3[2] += w0 * v.z;
+  }
+  block_sums<3>(s3, red);
+  const float r[3] = {s3[0] - x[0], s3[1] - x[1], s3[2] - x[2]};
+  float u[4];
+  lp_correction(fl.M, r, u);
+  const float inv_b = 1.0f / (float)fl.B;
+  // pass: squared error of w and Vb g (g = 2 e / B)
+  float s5[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  for (uint32_t j = threadIdx.x; j < fl.V; j += blockDim.x) {
+    const float4 v = fl.verts[j];
+    const float w = z[j] + add - (u[0] + (v.x * u[1] + v.y * u[2] + v.z * u[3]));
+    const float e = w - wt[j];
+    const float g = 2.0f * e * inv_b;
+    s5[0] += e * e;
+    s5[1] += g;
+    s5[2] += g * v.x;
+    s5[3] += g * v.y;
+    s5[4] += g * v.z;
+  }
+  block_sums<5>(s5, red);
+  float q[4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+    q[a] = fl.M[4 * a] * s5[1] + fl.M[4 * a + 1] * s5[2] + fl.M[4 * a + 2] * s5[3] +
+           fl.M[4 * a + 3] * s5[4];
+  const float cres = fl.lambda * 2.0f / (3.0f * (float)fl.B * fl.s2);
+  auto grad_w0 = [&](uint32_t j) {
+    const float4 v = fl.verts[j];
+    const float w = z[j] + add - (u[0] + (v.x * u[1] + v.y * u[2] + v.z * u[3]));
+    const float g = 2.0f * (w - wt[j]) * inv_b;
+    return g - (q[0] + (v.x * q[1] + v.y * q[2] + v.z * q[3])) +
+           cres * ((r[0] * v.x + r[1] * v.y) + r[2] * v.z);
+  };
+  float sg[1] = {0.0f};
+  for (uint32_t j = threadIdx.x; j < fl.V; j += blockDim.x) sg[0] += grad_w0(j);
+  block_sums<1>(sg, red);
+  const float gmean = sg[0] / (float)fl.V;
+  for (uint32_t j = threadIdx.x; j < fl.V; j += blockDim.x) {
+    const float dz = grad_w0(j) - gmean;
+    fl.dz[(size_t)row * fl.ldz + j] = dz;
+    fl.dzb[(size_t)row * fl.ldz + j] = __float2bfloat16_rn(dz);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&fl.loss[0], s5[0] * inv_b);
+    atomicAdd(&fl.loss[1], ((r[0] * r[0] + r[1] * r[1]) + r[2] * r[2]) /
+                               (3.0f * (float)fl.B * fl.s2));
+  }
+}
+
+// dpre = dA * silu'(pre) (fp32 and bf16 copies), elementwise.
+__global__ void k_silu_back(uint32_t n, const float* __restrict__ da,
+                            const float* __restrict__ pre, float* __restrict__ dpre,
+                            __nv_bfloat16* __restrict__ dpreb) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = da[i] * silu_grad(pre[i]);
+  dpre[i] = v;
+  dpreb[i] = __float2bfloat16_rn(v);
+}
+
+// Column sums of g [B x ld] over rows -> out [N] (bias gradients).
+__global__ void k_colsum(const float* __restrict__ g, uint32_t B, uint32_t N, uint32_t ld,
+                         float* __restrict__ out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  float s = 0.0f;
+  for (uint32_t r = 0; r < B; ++r) s += g[(size_t)r * ld + c];
+  out[c] = s;
+}
+
+// Adam (Kingma & Ba 2015) on fp32 master weights, refreshing the bf16 copy:
+// m = b1 m + (1-b1) g; v = b2 v + (1-b2) g^2; p -= lr mh / (sqrt(vh) + eps)
+// with the bias corrections mh = m c1, vh = v c2.
+__global__ void k_adam(uint32_t n, float* __restrict__ p, const float* __restrict__ g,
+                       float* __restrict__ m, float* __restrict__ v,
+                       __nv_bfloat16* __restrict__ pb, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  p[i] = pi;
+  if (pb) pb[i] = __float2bfloat16_rn(pi);
+}
+
+// ---- frame: per-frame projection and fused inference ---------------------------
+
+// Per-frame projection of the output layer (one block of 128 threads). For
+// vertices u (rest or current), P_u[k] = sum_j W5[j][k] u_j - c_k ubar with
+// c_k = sum_j W5[j][k], and p0_u = sum_j b5_j u_j + (1 - sum_j b5_j) ubar, so
+// that sum_j w0_j u_j = P_u^T h + p0_u. Raw mode (verts == null): P_rest,
+// p0_rest and A3 = 0, i.e. the network's own rest position sum_j w0_j v_j.
+// Otherwise A = v'^T Vb^T M, Pc = P_cur - P_rest A3^T, pc = p0_cur - A3 p0_rest.
+// proj = [Pc (128 x 3) | pc (3) | A3 (3 x 3, row-major)].
+__global__ void __launch_bounds__(128) k_field_project(FieldNet net, uint32_t V,
+                                                       const float4* __restrict__ rest,
+                                                       const float4* __restrict__ verts,
+                                                       const float* __restrict__ M,
+                                                       float* __restrict__ proj) {
+  __shared__ float red[20 * 32];
+  __shared__ float sh[20];
+  const bool raw = verts == nullptr;
+  // sums: rest (3), rest . b5 (3), sum b5 (1), current (3), current . b5 (3),
+  // S = v'^T Vb^T without its first column's duplicate (9: sum_j v'_j v_j^T)
+  float t[20];
+#pragma unroll
+  for (int k = 0; k < 20; ++k) t[k] = 0.0f;
+  for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
+    const float4 v = rest[j];
+    const float b = net.b5[j];
+    t[0] += v.x; t[1] += v.y; t[2] += v.z;
+    t[3] += b * v.x; t[4] += b * v.y; t[5] += b * v.z;
+    t[6] += b;
+    if (!raw) {
+      const float4 c = verts[j];
+      t[7] += c.x; t[8] += c.y; t[9] += c.z;
+      t[10] += b * c.x; t[11] += b * c.y; t[12] += b * c.z;
+      t[13] += c.x * v.x; t[14] += c.x * v.y; t[15] += c.x * v.z;
+      t[16] += c.y * v.x; t[17] += c.y * v.y; t[18] += c.y * v.z;
+      t[19] += c.z * v.x;
+    }
+  }
+  // the last entry of S (c.z * v.y, c.z * v.z) goes through a second pass
+  block_sums<20>(t, red);
+  float t2[2] = {0.0f, 0.0f};
+  if (!raw)
+    for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
+      const float4 v = rest[j], c = verts[j];
+      t2[0] += c.z * v.y;
+      t2[1] += c.z * v.z;
+    }
+  block_sums<2>(t2, red);
+  if (threadIdx.x == 0) {
+    const float inv_v = 1.0f / (float)V;
+    const float rb[3] = {t[0] * inv_v, t[1] * inv_v, t[2] * inv_v};
+    float p0r[3];
+    for (int q = 0; q < 3; ++q) p0r[q] = t[3 + q] + (1.0f - t[6]) * rb[q];
+    for (int q = 0; q < 3; ++q) {
+      sh[q] = rb[q];
+      sh[3 + q] = p0r[q];
+    }
+    if (raw) {
+      for (int q = 0; q < 3; ++q) proj[3 * kHid + q] = p0r[q];
+      for (int k = 0; k < 9; ++k) proj[3 * kHid + 3 + k] = 0.0f;
+    } else {
+      const float cb[3] = {t[7] * inv_v, t[8] * inv_v, t[9] * inv_v};
+      // S (3 x 4): column 0 = sum_j v'_j, columns 1..3 = sum_j v'_j v_j^T
+      const float S[3][4] = {{t[7], t[13], t[14], t[15]},
+                             {t[8], t[16], t[17], t[18]},
+                             {t[9], t[19], t2[0], t2[1]}};
+      float A3[3][3];
+      for (int q = 0; q < 3; ++q)
+        for (int d = 0; d < 3; ++d) {
+          float a = 0.0f;
+          for (int k = 0; k < 4; ++k) a += S[q][k] * M[4 * k + 1 + d];
+          A3[q][d] = a;
+          sh[11 + 3 * q + d] = a;
+        }
+      for (int q = 0; q < 3; ++q) {
+        sh[6 + q] = cb[q];
+        const float p0c = t[10 + q] + (1.0f - t[6]) * cb[q];
+        proj[3 * kHid + q] =
+            p0c - (A3[q][0] * p0r[0] + A3[q][1] * p0r[1] + A3[q][2] * p0r[2]);
+        for (int d = 0; d < 3; ++d) proj[3 * kHid + 3 + 3 * q + d] = A3[q][d];
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t k = threadIdx.x;  // hidden unit (blockDim.x == 128)
+  float ar[3] = {0.0f, 0.0f, 0.0f}, ac[3] = {0.0f, 0.0f, 0.0f}, c = 0.0f;
+  for (uint32_t j = 0; j < V; ++j) {
+    const float w = __bfloat162float(net.W5b[(size_t)j * kHid + k]);
+    const float4 v = rest[j];
+    ar[0] += w * v.x; ar[1] += w * v.y; ar[2] += w * v.z;
+    if (!raw) {
+      const float4 u = verts[j];
+      ac[0] += w * u.x; ac[1] += w * u.y; ac[2] += w * u.z;
+    }
+    c += w;
+  }
+  float pr[3];
+  for (int q = 0; q < 3; ++q) pr[q] = ar[q] - c * sh[q];
+  if (raw) {
+    for (int q = 0; q < 3; ++q) proj[3 * k + q] = pr[q];
+  } else {
+    for (int q = 0; q < 3; ++q) {
+      const float pc = ac[q] - c * sh[6 + q];
+      proj[3 * k + q] = pc - (sh[11 + 3 * q] * pr[0] + sh[12 + 3 * q] * pr[1] +
+                              sh[13 + 3 * q] * pr[2]);
+    }
+  }
+}
+
+// Fused inference: per warp 4 points x 4 streams (value, d/dx, d/dy, d/dz) as
+// one 16-row MMA tile: row r <-> stream (r / 4 for r < 8, 2 + (r - 8) / 4
+// otherwise), point r % 4. Lane groups 0-3 hold the value and d/dy rows,
+// 4-7 the d/dx and d/dz rows of the same points and columns, so the
+// activation slope crosses over with one shuffle. Activations stay in
+// registers between layers (an MMA C tile pair is the next layer's A tile).
+constexpr int kFwdWarps = 8;
+constexpr int kW1ld = kIn + 8, kWld = kHid + 8;  // padded smem rows (bf16)
+
+template <int KT>
+__device__ __forceinline__ void layer_mma(const uint32_t (&a)[KT][4], const __nv_bfloat16* W,
+                                          int ld, int gq, int tq, float (&c)[16][4]) {
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
+    const __nv_bfloat16* wr = W + (size_t)(nt * 8 + gq) * ld;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + kt * 16 + 2 * tq);
+      const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + kt * 16 + 8 + 2 * tq);
+      mma_bf16(c[nt], a[kt], b0, b1);
+    }
+  }
+}
+
+// bias + SiLU on value rows, slope times tangent rows; fp32 result in c.
+__device__ __forceinline__ void layer_act(float (&c)[16][4], const float* bias, bool value_lane,
+                                          int tq) {
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const float b = bias[nt * 8 + 2 * tq + e];
+      float slope = 0.0f;
+      if (value_lane) {
+        const float pre = c[nt][e] + b;
+        slope = silu_grad(pre);
+        c[nt][e] = silu(pre);
+      }
+      const float other = __shfl_xor_sync(0xffffffffu, slope, 16);
+      if (value_lane) {
+        c[nt][2 + e] *= slope;  // d/dy row
+      } else {
+        c[nt][e] *= other;      // d/dx row
+        c[nt][2 + e] *= other;  // d/dz row
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void to_a(const float (&c)[16][4], uint32_t (&a)[8][4]) {
+#pragma unroll
+  for (int kt = 0; kt < 8; ++kt) {
+    a[kt][0] = pack_bf16(c[2 * kt][0], c[2 * kt][1]);
+    a[kt][1] = pack_bf16(c[2 * kt][2], c[2 * kt][3]);
+    a[kt][2] = pack_bf16(c[2 * kt + 1][0], c[2 * kt + 1][1]);
+    a[kt][3] = pack_bf16(c[2 * kt + 1][2], c[2 * kt + 1][3]);
+  }
+}
+
+__global__ void __launch_bounds__(kFwdWarps * 32, 1) k_field_infer(FieldInfer fi) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  __nv_bfloat16* W1 = reinterpret_cast<__nv_bfloat16*>(fsm);
+  __nv_bfloat16* Wh = W1 + kHid * kW1ld;  // 3 x [128][kWld]
+  float* bias = reinterpret_cast<float*>(Wh + 3 * kHid * kWld);  // 4 x 128
+  float* proj = bias + 4 * kHid;                                  // kFieldProj
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kHid * kIn; i += blockDim.x)
+    W1[(i / kIn) * kW1ld + (i % kIn)] = fi.net.W1b[i];
+  for (int l = 0; l < 3; ++l) {
+    const __nv_bfloat16* src = l == 0 ? fi.net.W2b : (l == 1 ? fi.net.W3b : fi.net.W4b);
+    for (int i = tid; i < kHid * kHid; i += blockDim.x)
+      Wh[l * kHid * kWld + (i / kHid) * kWld + (i % kHid)] = src[i];
+  }
+  for (int i = tid; i < kHid; i += blockDim.x) {
+    bias[i] = fi.net.b1[i];
+    bias[kHid + i] = fi.net.b2[i];
+    bias[2 * kHid + i] = fi.net.b3[i];
+    bias[3 * kHid + i] = fi.net.b4[i];
+  }
+  for (int i = tid; i < kFieldProj; i += blockDim.x) proj[i] = fi.proj[i];
+  __syncthreads();
+
+  const int warp = tid >> 5, lane = tid & 31, gq = lane >> 2, tq = lane & 3;
+  const bool value_lane = gq < 4;
+  const int p = gq & 3;  // point of this lane's rows
+  const uint32_t groups = (fi.count + 3) / 4;
+  for (uint32_t grp = blockIdx.x * kFwdWarps + warp; grp < groups;
+       grp += gridDim.x * kFwdWarps) {
+    const uint32_t k = grp * 4 + p;  // item of this lane's point
+    const bool valid = k < fi.count;
+    float xr[3] = {0.0f, 0.0f, 0.0f};
+    if (valid) {
+      const uint32_t gi = fi.gauss ? fi.gauss[fi.first + k] : fi.first + k;
+      if (fi.points4) {
+        const float4 x4 = fi.points4[gi];
+        xr[0] = x4.x;
+        xr[1] = x4.y;
+        xr[2] = x4.z;
+      } else {
+        xr[0] = fi.points3[3 * (size_t)gi];
+        xr[1] = fi.points3[3 * (size_t)gi + 1];
+        xr[2] = fi.points3[3 * (size_t)gi + 2];
+      }
+    }
+    const float xh[3] = {(xr[0] - fi.enc[0]) * fi.enc[3], (xr[1] - fi.enc[1]) * fi.enc[3],
+                         (xr[2] - fi.enc[2]) * fi.enc[3]};
+    // layer-1 A fragments: rows (g, g+8) = (value, d/dy) or (d/dx, d/dz)
+    uint32_t a1[4][4];
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      float v[2][4];  // [row h][column e]
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int col = kt * 16 + (e >> 1) * 8 + 2 * tq + (e & 1);
+        float f, df[3];
+        feature(col, xh, fi.enc[3], f, df);
+        v[0][e] = value_lane ? f : df[0];
+        v[1][e] = value_lane ? df[1] : df[2];
+      }
+      a1[kt][0] = pack_bf16(v[0][0], v[0][1]);
+      a1[kt][1] = pack_bf16(v[1][0], v[1][1]);
+      a1[kt][2] = pack_bf16(v[0][2], v[0][3]);
+      a1[kt][3] = pack_bf16(v[1][2], v[1][3]);
+    }
+    float c[16][4];
+    uint32_t a[8][4];
+    layer_mma<4>(a1, W1, kW1ld, gq, tq, c);
+    layer_act(c, bias, value_lane, tq);
+#pragma unroll 1
+    for (int l = 0; l < 3; ++l) {
+      to_a(c, a);
+      layer_mma<8>(a, Wh + l * kHid * kWld, kWld, gq, tq, c);
+      layer_act(c, bias + (l + 1) * kHid, value_lane, tq);
+    }
+    // x' = P^T h + p0 on value rows, F columns = P^T dh on tangent rows; h
+    // and dh in bf16, as the output layer saw them in training
+    float o[2][3] = {{0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const float* pr = proj + 3 * (nt * 8 + 2 * tq + e);
+        const float h0 = round_bf16(c[nt][e]), h1 = round_bf16(c[nt][2 + e]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          o[0][q] += h0 * pr[q];
+          o[1][q] += h1 * pr[q];
+        }
+      }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        o[h][q] += __shfl_xor_sync(0xffffffffu, o[h][q], 1);
+        o[h][q] += __shfl_xor_sync(0xffffffffu, o[h][q], 2);
+      }
+    // lane 4p (value, d/dy) takes d/dx and d/dz from lane 4p + 16
+    float tx[3], tz[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      tx[q] = __shfl_down_sync(0xffffffffu, o[0][q], 16);
+      tz[q] = __shfl_down_sync(0xffffffffu, o[1][q], 16);
+    }
+    if (value_lane && tq == 0 && valid) {
+      const float* pc = proj + 3 * kHid;
+      const float* A3 = pc + 3;  // row-major
+      float px[3], F[3][3];      // F[q][d] = d x'_q / d x_d
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        px[q] = o[0][q] + pc[q] + (A3[3 * q] * xr[0] + A3[3 * q + 1] * xr[1] + A3[3 * q + 2] * xr[2]);
+        F[q][0] = tx[q] + A3[3 * q];
+        F[q][1] = o[1][q] + A3[3 * q + 1];
+        F[q][2] = tz[q] + A3[3 * q + 2];
+      }
+      float4* out = fi.xf + 3 * (size_t)(fi.out_first + k);
+      // F column-major
+      out[0] = make_float4(px[0], px[1], px[2], F[0][0]);
+      out[1] = make_float4(F[1][0], F[2][0], F[0][1], F[1][1]);
+      out[2] = make_float4(F[2][1], F[0][2], F[1][2], F[2][2]);
+    }
+  }
+}
+
+// Final weights per row: w0 = z + (1 - sum z) / V, then the linear-precision
+// projection w = w0 - (u0 + v_j . u[1..3]), u = M[:, 1:4] (sum_j w0_j v_j - x).
+__global__ void k_field_weights(const float* __restrict__ z, uint32_t B, uint32_t V,
+                                uint32_t ldz, const float* __restrict__ x,
+                                const float4* __restrict__ verts, FieldMat M,
+                                float* __restrict__ w) {
+  const uint32_t row = blockIdx.x;
+  if (row >= B) return;
+  __shared__ float red[3 * 32];
+  const float* zr = z + (size_t)row * ldz;
+  float s1[1] = {0.0f};
+  for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) s1[0] += zr[j];
+  block_sums<1>(s1, red);
+  const float add = (1.0f - s1[0]) / (float)V;
+  float s3[3] = {0.0f, 0.0f, 0.0f};
+  for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
+    const float w0 = zr[j] + add;
+    const float4 v = verts[j];
+    s3[0] += w0 * v.x;
+    s3[1] += w0 * v.y;
+    s3[2] += w0 * v.z;
+  }
+  block_sums<3>(s3, red);
+  const float* xr = x + 3 * (size_t)row;
+  const float r[3] = {s3[0] - xr[0], s3[1] - xr[1], s3[2] - xr[2]};
+  float u[4];
+  lp_correction(M.m, r, u);
+  for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
+    const float4 v = verts[j];
+    w[(size_t)row * V + j] = zr[j] + add - (u[0] + (v.x * u[1] + v.y * u[2] + v.z * u[3]));
+  }
+}
+
+// Linear-precision residual of the learned position on the rest cage.
+__global__ void k_mvc_residual(uint32_t nb, const uint32_t* __restrict__ list,
+                               const float4* __restrict__ rest_pos,
+                               const float4* __restrict__ xf, float inv_scale, float threshold,
+                               float* __restrict__ resid, uint32_t* __restrict__ flag) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nb) return;
+  const float4 x = rest_pos[list[s]];
+  const float4 y = xf[3 * (size_t)s];
+  const float dx = y.x - x.x, dy = y.y - x.y, dz = y.z - x.z;
+  const float r = sqrtf(dx * dx + dy * dy + dz * dz) * inv_scale;
+  if (resid) resid[s] = r;
+  flag[s] = (r > threshold || !(r == r)) ? 1u : 0u;
+}
+
+// Slots renumbered so the exact fallbacks come first (in slot order), then
+// the learned ones: rank = exclusive scan of the fallback flags.
+__global__ void k_mvc_reslot(uint32_t nb, const uint32_t* __restrict__ flag,
+                             const uint32_t* __restrict__ rank, uint32_t nfb,
+                             const uint32_t* __restrict__ list_in, uint32_t* __restrict__ list_out,
+                             float4* __restrict__ bind_w) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nb) return;
+  const uint32_t i = list_in[s];
+  const uint32_t slot = flag[s] ? rank[s] : nfb + (s - rank[s]);
+  list_out[slot] = i;
+  bind_w[i] = make_float4(__uint_as_float(slot), 0.0f, 0.0f, 0.0f);
+}
+
+}  // namespace
+
+size_t field_infer_smem() {
+  return (size_t)kHid * kW1ld * 2 + (size_t)3 * kHid * kWld * 2 + (size_t)4 * kHid * 4 +
+         (size_t)kFieldProj * 4;
+}
+
+cudaError_t launch_field_gather(const FieldBatch& b, cudaStream_t s) {
+  if (b.B == 0) return cudaSuccess;
+  k_field_gather<<<b.B, 128, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_nt(const GemmArgs& g, int epi, cudaStream_t s) {
+  if (g.M == 0 || g.N == 0) return cudaSuccess;
+  if ((g.lda & 7) || (g.ldb & 7)) return cudaErrorInvalidValue;
+  const dim3 grid((g.N + kBN - 1) / kBN, (g.M + kBM - 1) / kBM);
+  if (epi == kEpiF32)
+    k_gemm_nt<kEpiF32><<<grid, 128, 0, s>>>(g);
+  else if (epi == kEpiBias)
+    k_gemm_nt<kEpiBias><<<grid, 128, 0, s>>>(g);
+  else
+    k_gemm_nt<kEpiBiasSilu><<<grid, 128, 0, s>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_f32(const float* in, uint32_t R, uint32_t C, uint32_t ldi,
+                                 __nv_bfloat16* out, uint32_t ldo, cudaStream_t s) {
+  if (R == 0 || C == 0) return cudaSuccess;
+  k_transpose<float><<<dim3((C + 31) / 32, (R + 31) / 32), dim3(32, 8), 0, s>>>(in, R, C, ldi, out,
+                                                                                ldo);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_bf16(const __nv_bfloat16* in, uint32_t R, uint32_t C, uint32_t ldi,
+                                  __nv_bfloat16* out, uint32_t ldo, cudaStream_t s) {
+  if (R == 0 || C == 0) return cudaSuccess;
+  k_transpose<__nv_bfloat16><<<dim3((C + 31) / 32, (R + 31) / 32), dim3(32, 8), 0, s>>>(
+      in, R, C, ldi, out, ldo);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_loss(const FieldLoss& l, cudaStream_t s) {
+  if (l.B == 0) return cudaSuccess;
+  k_field_loss<<<l.B, 128, 0, s>>>(l);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_silu_back(uint32_t n, const float* da, const float* pre, float* dpre,
+                             __nv_bfloat16* dpreb, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_silu_back<<<(n + 255) / 256, 256, 0, s>>>(n, da, pre, dpre, dpreb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_colsum(const float* g, uint32_t B, uint32_t N, uint32_t ld, float* out,
+                          cudaStream_t s) {
+  if (N == 0) return cudaSuccess;
+  k_colsum<<<(N + 127) / 128, 128, 0, s>>>(g, B, N, ld, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(uint32_t n, float* p, const float* g, float* m, float* v,
+                        __nv_bfloat16* pb, float lr, float b1, float b2, float eps, float c1,
+                        float c2, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_adam<<<(n + 255) / 256, 256, 0, s>>>(n, p, g, m, v, pb, lr, b1, b2, eps, c1, c2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_project(const FieldNet& net, uint32_t V, const float4* rest,
+                                 const float4* verts, const float* M, float* proj,
+                                 cudaStream_t s) {
+  k_field_project<<<1, 128, 0, s>>>(net, V, rest, verts, M, proj);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s) {
+  if (fi.count == 0) return cudaSuccess;
+  const size_t smem = field_infer_smem();
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_field_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint32_t groups = (fi.count + 3) / 4;
+  const uint32_t blocks = std::min<uint32_t>(148u, (groups + kFwdWarps - 1) / kFwdWarps);
+  k_field_infer<<<blocks, kFwdWarps * 32, smem, s>>>(fi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_weights(const float* z, uint32_t B, uint32_t V, uint32_t ldz,
+                                 const float* x, const float4* verts, const FieldMat& M, float* w,
+                                 cudaStream_t s) {
+  if (B == 0) return cudaSuccess;
+  k_field_weights<<<B, 128, 0, s>>>(z, B, V, ldz, x, verts, M, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mvc_residual(uint32_t nb, const uint32_t* list, const float4* rest_pos,
+                                const float4* xf, float inv_scale, float threshold, float* resid,
+                                uint32_t* flag, cudaStream_t s) {
+  if (nb == 0) return cudaSuccess;
+  k_mvc_residual<<<(nb + 255) / 256, 256, 0, s>>>(nb, list, rest_pos, xf, inv_scale, threshold,
+                                                  resid, flag);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mvc_reslot(uint32_t nb, const uint32_t* flag, const uint32_t* rank,
+                              uint32_t nfb, const uint32_t* list_in, uint32_t* list_out,
+                              float4* bind_w, cudaStream_t s) {
+  if (nb == 0) return cudaSuccess;
+  k_mvc_reslot<<<(nb + 255) / 256, 256, 0, s>>>(nb, flag, rank, nfb, list_in, list_out, bind_w);
+  return cudaGetLastError();
+}
+
+}  // namespace cgs

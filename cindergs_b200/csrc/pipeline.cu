@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "cgs.h"
+#include "field.h"
 #include "kernels.h"
 
 using namespace cgs;
@@ -138,6 +139,33 @@ struct cgs_ctx {
   float mvc_h = 0.0f;
   DevBuf mvc_rest, mvc_verts, mvc_tris, mvc_vf_off, mvc_vf_list, mvc_list, mvc_wg, mvc_xf, mvc_R;
   std::vector<float> mvc_last_verts;
+  // learned MVC field; with learned bindings the slots [0, mvc_nfb) keep
+  // exact stored weights (the residual fallbacks), [mvc_nfb, mvc_nb) are
+  // evaluated by the network every frame
+  FieldState field;
+  bool field_ready = false, mvc_learned = false;
+  uint32_t mvc_nfb = 0;
+  uint32_t mvc_nwg() const { return mvc_learned ? mvc_nfb : mvc_nb; }  // stored slots
+  void mvc_unbind() {
+    mvc_nb = 0;
+    mvc_nfb = 0;
+    mvc_learned = false;
+  }
+  // Field inference over the learned slots: rest positions in, position and
+  // gradient into mvc_xf at the same slots.
+  FieldInfer field_infer_args(const float* proj) const {
+    FieldInfer fi{};
+    fi.net = field.net();
+    fi.enc = field.enc_d.as<float>();
+    fi.proj = proj;
+    fi.gauss = mvc_list.as<uint32_t>();
+    fi.points4 = rest_pos.as<float4>();
+    fi.first = mvc_nfb;
+    fi.count = mvc_nb - mvc_nfb;
+    fi.out_first = mvc_nfb;
+    fi.xf = mvc_xf.as<float4>();
+    return fi;
+  }
   bool deform_on() const { return has_cages || mvc_nb > 0; }
   MvcCage mvc_cage(bool rest) const {
     MvcCage c;
@@ -588,9 +616,17 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
     const uint64_t A = p.n + (p.split_possible ? h.split : 0u);
     const uint64_t S = h.fc.surviving, E = p.stage3_ran ? entries : 0, T = ctx->num_tets;
     const uint64_t shb = ctx->sh_f16 ? 96 : 192;
-    if (p.need_deform && ctx->mvc_nb) {
+    if (p.need_deform && ctx->mvc_nwg()) {
       // stored bindings: (w, grad w) per cage vertex in, position + F out
-      kp.alg_bytes[CGS_K_MVC] += (uint64_t)ctx->mvc_nb * ((uint64_t)ctx->mvc_V * 16 + 48);
+      kp.alg_bytes[CGS_K_MVC] += (uint64_t)ctx->mvc_nwg() * ((uint64_t)ctx->mvc_V * 16 + 48);
+    }
+    if (p.need_deform && ctx->mvc_learned && ctx->mvc_nb > ctx->mvc_nfb) {
+      // learned slots: slot -> Gaussian, rest position in, position + F out;
+      // four streams (value and three tangents) through the hidden layers
+      const uint64_t L = ctx->mvc_nb - ctx->mvc_nfb;
+      kp.alg_bytes[CGS_K_FIELD] += L * (4 + 16 + 48);
+      kp.alg_flops[CGS_K_FIELD] +=
+          L * 4 * 2 * ((uint64_t)kFieldIn * kFieldHid + 3ull * kFieldHid * kFieldHid);
     }
     if (p.need_deform) {
       kp.alg_bytes[CGS_K_TET_TRANSFORMS] += T * (16 + 36 + 48 + 76);
@@ -767,7 +803,7 @@ int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* co
   ctx->s3_valid = false;
   ctx->has_cages = false;  // cage bindings refer to the previous scene
   ctx->num_tets = 0;
-  ctx->mvc_nb = 0;
+  ctx->mvc_unbind();
   return CGS_OK;
 }
 
@@ -809,7 +845,7 @@ int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
   ctx->num_tets = num_tets;
   ctx->num_verts = num_verts;
   ctx->has_cages = true;
-  ctx->mvc_nb = 0;  // the bindings were replaced: bind the polygon cage again
+  ctx->mvc_unbind();  // the bindings were replaced: bind the polygon cage again
   ctx->verts_uploaded = false;
   ctx->last_verts.clear();
   ctx->deformed_valid = false;
@@ -882,9 +918,10 @@ int cgs_mvc_cage_upload(cgs_ctx* ctx, uint32_t V, const float* rest, uint32_t F,
   ctx->mvc_V = V;
   ctx->mvc_F = F;
   ctx->mvc_ready = true;
+  ctx->field_ready = false;  // the network belongs to the previous cage
   ctx->mvc_last_verts.assign(rest, rest + 3 * (size_t)V);
   if (ctx->mvc_nb) {
-    ctx->mvc_nb = 0;
+    ctx->mvc_unbind();
     ctx->deformed_valid = false;
     ctx->deform_generation++;
   }
@@ -910,10 +947,31 @@ int cgs_mvc_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t V) {
   return CGS_OK;
 }
 
-int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound) {
+namespace {
+
+// Learned bindings were made with the current network: a new or changed
+// network drops them (the Gaussians fall back to their rest pose until bound
+// again).
+void field_changed(cgs_ctx* ctx) {
+  if (!ctx->mvc_learned) return;
+  ctx->mvc_unbind();
+  ctx->deformed_valid = false;
+  ctx->deform_generation++;
+  ctx->s3_valid = false;
+}
+
+// PolyCageMesh::bind_gaussians (mvc.rs:498-541) over the resident scene:
+// inside test, slots in index order, then either exact stored weights for
+// every slot, or (learned) the network for the slots whose residual on the
+// rest cage is at most `threshold` and exact weights for the others, which
+// are renumbered to come first.
+int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, uint32_t* out_bound,
+             uint32_t* out_fallback) {
   if (!ctx) return CGS_E_ARG;
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
   if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
+  if (learned && !ctx->field_ready) return ctx->fail(CGS_E_STATE, "no learned field created");
+  if (learned && !(threshold >= 0.0f)) return ctx->fail(CGS_E_ARG, "threshold must be >= 0");
   cudaSetDevice(ctx->device);
   CGS_TRY(drain(ctx, true));
   cudaStream_t s = ctx->stream;
@@ -924,54 +982,261 @@ int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound) {
     CGS_CUDA(cudaMemsetAsync(ctx->bind_tet.p, 0xFF, (size_t)(n ? n : 1) * 4, s), "clear bindings");
     CGS_CUDA(cudaMemsetAsync(ctx->bind_w.p, 0, (size_t)(n ? n : 1) * 16, s), "clear bindings");
   }
-  uint32_t nb = 0;
+  ctx->mvc_unbind();
+  uint32_t nb = 0, nfb = 0;
   if (n) {
-    DevBuf flag, slot;
+    DevBuf flag, slot, tmp;
     const size_t scan_status = ((size_t)scan_tiles(n) + 1) * 8 + 64;
     CGS_CUDA(cudaMalloc(&flag.p, (size_t)n * 4), "mvc flags");
     flag.cap = (size_t)n * 4;
     CGS_CUDA(cudaMalloc(&slot.p, (size_t)n * 4 + scan_status), "mvc slots");
     slot.cap = (size_t)n * 4 + scan_status;
     char* sb = slot.as<char>() + (size_t)n * 4;
+    uint32_t* words = (uint32_t*)(sb + scan_status - 64);
+    uint32_t hw[4] = {};
     int rc = CGS_OK;
     cudaError_t e = cudaMemsetAsync(sb, 0, scan_status, s);
     const MvcCage rest = ctx->mvc_cage(true);
     if (e == cudaSuccess)
       e = launch_mvc_inside(rest, n, ctx->rest_pos.as<float4>(), ctx->bind_tet.as<uint32_t>(),
                             flag.as<uint32_t>(), s);
-    uint32_t* words = (uint32_t*)(sb + scan_status - 64);
     if (e == cudaSuccess)
       e = launch_scan_u32(flag.as<uint32_t>(), slot.as<uint32_t>(), n, words,
                           (unsigned long long*)sb, words + 1, words + 2, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&nb, words, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hw, words, 12, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess && nb) {
-      const size_t wg_bytes = (size_t)nb * ctx->mvc_V * 16;
+    if (e == cudaSuccess && hw[2]) rc = ctx->fail(CGS_E_TIMEOUT, "mvc slot scan gave up waiting");
+    nb = hw[0];
+    if (e == cudaSuccess && rc == CGS_OK && nb) {
       if ((rc = ctx->ensure(ctx->mvc_list, (size_t)nb * 4, "mvc slots")) == CGS_OK &&
-          (rc = ctx->ensure(ctx->mvc_wg, wg_bytes, "mvc bindings")) == CGS_OK &&
           (rc = ctx->ensure(ctx->mvc_xf, (size_t)nb * 48, "mvc position/gradient")) == CGS_OK &&
           (rc = ctx->ensure(ctx->mvc_R, (size_t)nb * 36, "mvc rotations")) == CGS_OK) {
         e = launch_mvc_compact(n, flag.as<uint32_t>(), slot.as<uint32_t>(),
                                ctx->bind_tet.as<uint32_t>(), ctx->bind_w.as<float4>(),
                                ctx->mvc_list.as<uint32_t>(), s);
-        if (e == cudaSuccess)
-          e = launch_mvc_bind_weights(rest, nb, ctx->mvc_list.as<uint32_t>(),
-                                      ctx->rest_pos.as<float4>(), ctx->mvc_h,
-                                      ctx->mvc_wg.as<float4>(), s);
+        nfb = nb;
+        if (learned && e == cudaSuccess) {
+          // residual of the network on the rest cage; fallbacks get the first slots
+          FieldState& f = ctx->field;
+          ctx->mvc_nfb = 0;
+          ctx->mvc_nb = nb;
+          e = f.project(nullptr, f.proj_rest.as<float>(), s);  // raw: sum_j w0_j v_j
+          if (e == cudaSuccess) {
+            FieldInfer fi = ctx->field_infer_args(f.proj_rest.as<float>());
+            e = launch_field_infer(fi, s);
+          }
+          ctx->mvc_nb = 0;
+          if (e == cudaSuccess)
+            e = launch_mvc_residual(nb, ctx->mvc_list.as<uint32_t>(), ctx->rest_pos.as<float4>(),
+                                    ctx->mvc_xf.as<float4>(), f.enc[3], threshold, nullptr,
+                                    flag.as<uint32_t>(), s);
+          if (e == cudaSuccess) e = cudaMemsetAsync(sb, 0, scan_status, s);
+          if (e == cudaSuccess)
+            e = launch_scan_u32(flag.as<uint32_t>(), slot.as<uint32_t>(), nb, words,
+                                (unsigned long long*)sb, words + 1, words + 2, s);
+          if (e == cudaSuccess) e = cudaMemcpyAsync(hw, words, 12, cudaMemcpyDeviceToHost, s);
+          if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+          if (e == cudaSuccess && hw[2])
+            rc = ctx->fail(CGS_E_TIMEOUT, "mvc fallback scan gave up waiting");
+          nfb = hw[0];
+          if (e == cudaSuccess && rc == CGS_OK) {
+            e = cudaMalloc(&tmp.p, (size_t)nb * 4);
+            if (e == cudaSuccess) {
+              tmp.cap = (size_t)nb * 4;
+              e = launch_mvc_reslot(nb, flag.as<uint32_t>(), slot.as<uint32_t>(), nfb,
+                                    ctx->mvc_list.as<uint32_t>(), tmp.as<uint32_t>(),
+                                    ctx->bind_w.as<float4>(), s);
+            }
+            if (e == cudaSuccess)
+              e = cudaMemcpyAsync(ctx->mvc_list.p, tmp.p, (size_t)nb * 4,
+                                  cudaMemcpyDeviceToDevice, s);
+          }
+        }
+        if (e == cudaSuccess && rc == CGS_OK && nfb) {
+          rc = ctx->ensure(ctx->mvc_wg, (size_t)nfb * ctx->mvc_V * 16, "mvc bindings");
+          if (rc == CGS_OK)
+            e = launch_mvc_bind_weights(rest, nfb, ctx->mvc_list.as<uint32_t>(),
+                                        ctx->rest_pos.as<float4>(), ctx->mvc_h,
+                                        ctx->mvc_wg.as<float4>(), s);
+        }
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       }
     }
-    cudaFree(flag.p);
-    cudaFree(slot.p);
-    flag.p = slot.p = nullptr;
-    if (rc != CGS_OK) return rc;
-    if (e != cudaSuccess) return ctx->cuda_fail(e, "mvc binding");
+    if (rc != CGS_OK || e != cudaSuccess) {
+      cudaStreamSynchronize(s);
+      ctx->mvc_unbind();
+      ctx->deformed_valid = false;
+      ctx->deform_generation++;
+      ctx->s3_valid = false;
+      return rc != CGS_OK ? rc : ctx->cuda_fail(e, "mvc binding");
+    }
   }
   ctx->mvc_nb = nb;
+  ctx->mvc_learned = learned;
+  ctx->mvc_nfb = learned ? nfb : 0;
   ctx->deformed_valid = false;
   ctx->deform_generation++;
   ctx->s3_valid = false;
   if (out_bound) *out_bound = nb;
+  if (out_fallback) *out_fallback = learned ? nfb : nb;
+  return CGS_OK;
+}
+
+int field_check(cgs_ctx* ctx) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
+  if (!ctx->field_ready) return ctx->fail(CGS_E_STATE, "no learned field created");
+  cudaSetDevice(ctx->device);
+  return drain(ctx, true);
+}
+
+}  // namespace
+
+int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound) {
+  return mvc_bind(ctx, false, 0.0f, out_bound, nullptr);
+}
+
+int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t* out_bound,
+                         uint32_t* out_fallback) {
+  return mvc_bind(ctx, true, threshold, out_bound, out_fallback);
+}
+
+int cgs_mvc_field_create(cgs_ctx* ctx, uint64_t seed) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  field_changed(ctx);
+  std::vector<float> r4((size_t)ctx->mvc_V * 4);
+  CGS_CUDA(cudaMemcpy(r4.data(), ctx->mvc_rest.p, r4.size() * 4, cudaMemcpyDeviceToHost),
+           "field rest cage");
+  ctx->field_ready = false;
+  CGS_CUDA(ctx->field.init(ctx->mvc_V, r4.data(), seed, ctx->stream), "field init");
+  ctx->field_ready = true;
+  return CGS_OK;
+}
+
+int cgs_mvc_field_layout(cgs_ctx* ctx, uint32_t* offsets, uint32_t* total, float* enc) {
+  CGS_TRY(field_check(ctx));
+  if (offsets)
+    for (int k = 0; k < kFieldParams; ++k) offsets[k] = ctx->field.off[k];
+  if (total) *total = ctx->field.total();
+  if (enc) std::memcpy(enc, ctx->field.enc, 16);
+  return CGS_OK;
+}
+
+int cgs_mvc_field_params(cgs_ctx* ctx, float* dst, const float* src) {
+  CGS_TRY(field_check(ctx));
+  FieldState& f = ctx->field;
+  const size_t bytes = (size_t)f.total() * 4;
+  if (dst) CGS_CUDA(cudaMemcpy(dst, f.p32.p, bytes, cudaMemcpyDeviceToHost), "field params");
+  if (src) {
+    field_changed(ctx);
+    cudaStream_t s = ctx->stream;
+    CGS_CUDA(cudaMemcpyAsync(f.p32.p, src, bytes, cudaMemcpyHostToDevice, s), "field params");
+    // bf16 copy: a 1 x total transpose is an elementwise conversion
+    CGS_CUDA(launch_transpose_f32(f.p32.as<float>(), 1, f.total(), f.total(),
+                                  f.pb.as<__nv_bfloat16>(), 1, s), "field params");
+    CGS_CUDA(cudaMemsetAsync(f.m1.p, 0, bytes, s), "field params");
+    CGS_CUDA(cudaMemsetAsync(f.m2.p, 0, bytes, s), "field params");
+    CGS_CUDA(cudaStreamSynchronize(s), "field params");
+    f.step = 0;
+  }
+  return CGS_OK;
+}
+
+int cgs_mvc_field_train(cgs_ctx* ctx, uint64_t n, const float* d_points, const float* d_weights,
+                        uint32_t steps, uint32_t batch, float lr, float lambda, uint64_t seed,
+                        float* out_loss) {
+  CGS_TRY(field_check(ctx));
+  if (!d_points || !d_weights || n == 0) return ctx->fail(CGS_E_ARG, "no training points");
+  if (n > 0xFFFFFFFFull) return ctx->fail(CGS_E_CAPACITY, "at most 2^32 - 1 points");
+  if (batch == 0 || batch % 8) return ctx->fail(CGS_E_ARG, "batch must be a positive multiple of 8");
+  if (!(lr > 0.0f) || !(lambda >= 0.0f)) return ctx->fail(CGS_E_ARG, "lr > 0 and lambda >= 0");
+  field_changed(ctx);
+  FieldState& f = ctx->field;
+  cudaStream_t s = ctx->stream;
+  const uint32_t tail = std::max<uint32_t>(1, steps / 10);
+  CGS_CUDA(cudaMemsetAsync(f.loss.p, 0, 8, s), "field train");
+  uint64_t st = seed ^ 0xD1B54A32D192ED03ull;
+  for (uint32_t t = 0; t < steps; ++t) {
+    if (t == steps - tail) CGS_CUDA(cudaMemsetAsync(f.loss.p, 0, 8, s), "field train");
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    const uint32_t bseed = (uint32_t)(z ^ (z >> 31)) | 1u;
+    CGS_CUDA(f.forward(d_points, d_weights, (uint32_t)n, batch, bseed, ctx->mvc_rest.as<float4>(),
+                       lambda, s), "field forward");
+    CGS_CUDA(f.backward(batch, s), "field backward");
+    const double c = 0.5 * (1.0 + std::cos(3.141592653589793 * (double)t / (double)steps));
+    CGS_CUDA(f.adam(lr * (float)(0.05 + 0.95 * c), s), "field adam");
+  }
+  float hl[2] = {0.0f, 0.0f};
+  CGS_CUDA(cudaMemcpyAsync(hl, f.loss.p, 8, cudaMemcpyDeviceToHost, s), "field train");
+  CGS_CUDA(cudaStreamSynchronize(s), "field train");
+  if (out_loss) {
+    out_loss[0] = steps ? hl[0] / (float)tail : 0.0f;
+    out_loss[1] = steps ? hl[1] / (float)tail : 0.0f;
+  }
+  return CGS_OK;
+}
+
+int cgs_mvc_field_grads(cgs_ctx* ctx, uint64_t n, const float* d_points, const float* d_weights,
+                        float lambda, float* grads, float* out_loss) {
+  CGS_TRY(field_check(ctx));
+  if (!d_points || !d_weights || n == 0 || n % 8 || n > 0x7FFFFFFFull)
+    return ctx->fail(CGS_E_ARG, "n must be a positive multiple of 8");
+  FieldState& f = ctx->field;
+  cudaStream_t s = ctx->stream;
+  CGS_CUDA(cudaMemsetAsync(f.loss.p, 0, 8, s), "field grads");
+  CGS_CUDA(f.forward(d_points, d_weights, (uint32_t)n, (uint32_t)n, 0, ctx->mvc_rest.as<float4>(),
+                     lambda, s), "field forward");
+  CGS_CUDA(f.backward((uint32_t)n, s), "field backward");
+  float hl[2];
+  CGS_CUDA(cudaMemcpyAsync(hl, f.loss.p, 8, cudaMemcpyDeviceToHost, s), "field grads");
+  CGS_CUDA(cudaStreamSynchronize(s), "field grads");
+  if (grads)
+    CGS_CUDA(cudaMemcpy(grads, f.g32.p, (size_t)f.total() * 4, cudaMemcpyDeviceToHost),
+             "field grads");
+  if (out_loss) {
+    out_loss[0] = hl[0];
+    out_loss[1] = hl[1];
+  }
+  return CGS_OK;
+}
+
+int cgs_mvc_field_eval(cgs_ctx* ctx, uint64_t n, const float* d_points, float* d_weights) {
+  CGS_TRY(field_check(ctx));
+  if (n == 0) return CGS_OK;
+  if (!d_points || !d_weights) return CGS_E_ARG;
+  if (n > 0xFFFFFFFFull) return ctx->fail(CGS_E_CAPACITY, "at most 2^32 - 1 points");
+  CGS_CUDA(ctx->field.eval((uint32_t)n, d_points, d_weights, ctx->stream), "field eval");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "field eval");
+  return CGS_OK;
+}
+
+int cgs_mvc_field_infer(cgs_ctx* ctx, uint64_t n, const float* d_points, int32_t use_rest,
+                        float* d_out) {
+  CGS_TRY(field_check(ctx));
+  if (n == 0) return CGS_OK;
+  if (!d_points || !d_out) return CGS_E_ARG;
+  if ((uintptr_t)d_out & 15) return ctx->fail(CGS_E_ARG, "d_out must be 16-byte aligned");
+  if (n > 0xFFFFFFFFull) return ctx->fail(CGS_E_CAPACITY, "at most 2^32 - 1 points");
+  FieldState& f = ctx->field;
+  cudaStream_t s = ctx->stream;
+  float* pr = use_rest ? f.proj_rest.as<float>() : f.proj.as<float>();
+  CGS_CUDA(f.project(use_rest ? nullptr : ctx->mvc_verts.as<float4>(), pr, s),
+           "field projection");
+  FieldInfer fi{};
+  fi.net = f.net();
+  fi.enc = f.enc_d.as<float>();
+  fi.proj = pr;
+  fi.points3 = d_points;
+  fi.count = (uint32_t)n;
+  fi.xf = reinterpret_cast<float4*>(d_out);
+  CGS_CUDA(launch_field_infer(fi, s), "field inference");
+  CGS_CUDA(cudaStreamSynchronize(s), "field inference");
   return CGS_OK;
 }
 
@@ -993,10 +1258,10 @@ int cgs_mvc_read_bindings(cgs_ctx* ctx, uint64_t max_slots, uint32_t* gaussian, 
   if (!ctx || !out_slots) return CGS_E_ARG;
   cudaSetDevice(ctx->device);
   CGS_TRY(drain(ctx, true));
-  const uint64_t k = std::min<uint64_t>(max_slots, ctx->mvc_nb);
+  const uint64_t k = std::min<uint64_t>(max_slots, ctx->mvc_nwg());
   *out_slots = k;
   if (k == 0) return CGS_OK;
-  const uint32_t V = ctx->mvc_V, nb = ctx->mvc_nb;
+  const uint32_t V = ctx->mvc_V, nb = ctx->mvc_nwg();
   if (gaussian)
     CGS_CUDA(cudaMemcpy(gaussian, ctx->mvc_list.p, k * 4, cudaMemcpyDeviceToHost), "read mvc slots");
   if (wg) {
@@ -1212,11 +1477,21 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     if (ctx->mvc_nb) {
       da.mvc_xf = ctx->mvc_xf.as<float4>();
       da.mvc_R = ctx->mvc_R.as<float>();
-      ctx->kbegin(CGS_K_MVC);
-      CGS_CUDA(launch_mvc_jacobian(ctx->mvc_V, ctx->mvc_verts.as<float4>(), ctx->mvc_nb,
-                                   ctx->mvc_wg.as<float4>(), ctx->mvc_xf.as<float4>(), s),
-               "mvc jacobian launch");
-      ctx->kend();
+      if (ctx->mvc_nwg()) {
+        ctx->kbegin(CGS_K_MVC);
+        CGS_CUDA(launch_mvc_jacobian(ctx->mvc_V, ctx->mvc_verts.as<float4>(), ctx->mvc_nwg(),
+                                     ctx->mvc_wg.as<float4>(), ctx->mvc_xf.as<float4>(), s),
+                 "mvc jacobian launch");
+        ctx->kend();
+      }
+      if (ctx->mvc_learned && ctx->mvc_nb > ctx->mvc_nfb) {
+        ctx->kbegin(CGS_K_FIELD);
+        CGS_CUDA(ctx->field.project(ctx->mvc_verts.as<float4>(), ctx->field.proj.as<float>(), s),
+                 "field projection launch");
+        CGS_CUDA(launch_field_infer(ctx->field_infer_args(ctx->field.proj.as<float>()), s),
+                 "field inference launch");
+        ctx->kend();
+      }
     }
     if (has_cages) {
       ctx->kbegin(CGS_K_TET_TRANSFORMS);
@@ -1395,7 +1670,7 @@ int cgs_invalidate(cgs_ctx* ctx) {
   ctx->scene_ready = false;
   ctx->has_cages = false;
   ctx->num_tets = 0;
-  ctx->mvc_nb = 0;
+  ctx->mvc_unbind();
   ctx->deformed_valid = false;
   ctx->verts_uploaded = false;
   ctx->last_verts.clear();
@@ -1582,7 +1857,7 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
 const char* cgs_kernel_name(int32_t id) {
   static const char* names[CGS_KERNEL_COUNT] = {"clear", "tet_transforms", "deform", "project",
                                                 "bin", "entry_sort", "tile_ranges", "composite",
-                                                "splat_sort", "mvc"};
+                                                "splat_sort", "mvc", "field"};
   return (id >= 0 && id < CGS_KERNEL_COUNT) ? names[id] : "unknown";
 }
 

@@ -221,6 +221,111 @@ class GpuPipelineState:
         n = int(cnt.value)
         return g[:n], wg[:n]
 
+    # -- learned MVC field -------------------------------------------------------
+    def _dev_f32(self, a, cols: int):
+        import torch
+        host = not (isinstance(a, torch.Tensor) and a.is_cuda)
+        t = torch.as_tensor(np.asarray(a, f32) if host else a, dtype=torch.float32)
+        return t.reshape(-1, cols).contiguous().to(f"cuda:{self.device}"), host
+
+    def mvc_field_create(self, seed: int = 0) -> None:
+        """New seeded network for the uploaded polygon cage (drops learned bindings)."""
+        self._check(self._lib.cgs_mvc_field_create(self._ctx, int(seed)), "cgs_mvc_field_create")
+
+    def mvc_field_layout(self) -> tuple[dict, int, np.ndarray]:
+        """({name: offset} for W1, b1, ... W5, b5, total floats, enc [c, 1/s])."""
+        off = np.zeros(10, np.uint32)
+        tot = ctypes.c_uint32(0)
+        enc = np.zeros(4, f32)
+        self._check(self._lib.cgs_mvc_field_layout(self._ctx, _p(off), ctypes.byref(tot), _p(enc)),
+                    "cgs_mvc_field_layout")
+        names = ["W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4", "W5", "b5"]
+        return dict(zip(names, (int(o) for o in off))), int(tot.value), enc
+
+    def mvc_field_params(self, values=None) -> np.ndarray:
+        """The fp32 parameter block; with `values`, loads it first (resets Adam)."""
+        _, tot, _ = self.mvc_field_layout()
+        src = None
+        if values is not None:
+            src = np.ascontiguousarray(values, f32).reshape(-1)
+            if src.size != tot:
+                raise ValueError(f"expected {tot} parameters, got {src.size}")
+        out = np.zeros(tot, f32)
+        self._check(self._lib.cgs_mvc_field_params(self._ctx, None, None if src is None else _p(src)),
+                    "cgs_mvc_field_params")
+        self._check(self._lib.cgs_mvc_field_params(self._ctx, _p(out), None), "cgs_mvc_field_params")
+        return out
+
+    def mvc_field_train(self, points, weights, steps: int, batch: int = 4096, lr: float = 1e-3,
+                        lam: float = 1.0, seed: int = 1) -> tuple[float, float]:
+        """Adam steps on (points [n, 3], exact weights [n, V]); returns the weight
+        and residual loss terms averaged over the last tenth of the steps."""
+        import torch
+        pts, _ = self._dev_f32(points, 3)
+        w, _ = self._dev_f32(weights, self._mvc_V)
+        torch.cuda.synchronize(pts.device)
+        loss = np.zeros(2, f32)
+        self._check(self._lib.cgs_mvc_field_train(self._ctx, pts.shape[0],
+                                                  ctypes.c_void_p(pts.data_ptr()),
+                                                  ctypes.c_void_p(w.data_ptr()), int(steps),
+                                                  int(batch), float(lr), float(lam), int(seed),
+                                                  _p(loss)), "cgs_mvc_field_train")
+        return float(loss[0]), float(loss[1])
+
+    def mvc_field_grads(self, points, weights, lam: float = 1.0):
+        """(gradient of the loss over all rows [total], (weight term, residual term))."""
+        import torch
+        pts, _ = self._dev_f32(points, 3)
+        w, _ = self._dev_f32(weights, self._mvc_V)
+        torch.cuda.synchronize(pts.device)
+        _, tot, _ = self.mvc_field_layout()
+        g = np.zeros(tot, f32)
+        loss = np.zeros(2, f32)
+        self._check(self._lib.cgs_mvc_field_grads(self._ctx, pts.shape[0],
+                                                  ctypes.c_void_p(pts.data_ptr()),
+                                                  ctypes.c_void_p(w.data_ptr()), float(lam), _p(g),
+                                                  _p(loss)), "cgs_mvc_field_grads")
+        return g, (float(loss[0]), float(loss[1]))
+
+    def mvc_field_eval(self, points):
+        """Network weights [n, V] of points [n, 3] (device tensor in, device out;
+        numpy in, numpy out)."""
+        import torch
+        pts, host = self._dev_f32(points, 3)
+        out = torch.empty((pts.shape[0], self._mvc_V), dtype=torch.float32, device=pts.device)
+        torch.cuda.synchronize(pts.device)
+        self._check(self._lib.cgs_mvc_field_eval(self._ctx, pts.shape[0],
+                                                 ctypes.c_void_p(pts.data_ptr()),
+                                                 ctypes.c_void_p(out.data_ptr())),
+                    "cgs_mvc_field_eval")
+        return out.cpu().numpy() if host else out
+
+    def mvc_field_infer(self, points, rest: bool = False):
+        """Fused inference: (positions [n, 3], gradients F [n, 3, 3]) on the
+        current cage (rest cage with rest=True)."""
+        import torch
+        pts, host = self._dev_f32(points, 3)
+        out = torch.empty((pts.shape[0], 12), dtype=torch.float32, device=pts.device)
+        torch.cuda.synchronize(pts.device)
+        self._check(self._lib.cgs_mvc_field_infer(self._ctx, pts.shape[0],
+                                                  ctypes.c_void_p(pts.data_ptr()), int(rest),
+                                                  ctypes.c_void_p(out.data_ptr())),
+                    "cgs_mvc_field_infer")
+        pos = out[:, :3]
+        F = out[:, 3:].reshape(-1, 3, 3).transpose(1, 2)  # stored column-major
+        if host:
+            return pos.cpu().numpy(), F.cpu().numpy()
+        return pos, F
+
+    def mvc_bind_learned(self, threshold: float = 2e-3) -> tuple[int, int]:
+        """Binds the polygon cage with the network where its residual on the rest
+        cage is at most threshold (relative to the cage half-extent); returns
+        (bound, exact fallbacks)."""
+        nb, nfb = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        self._check(self._lib.cgs_mvc_bind_learned(self._ctx, float(threshold), ctypes.byref(nb),
+                                                   ctypes.byref(nfb)), "cgs_mvc_bind_learned")
+        return int(nb.value), int(nfb.value)
+
     def _mvc_bound_hint(self) -> int:
         cnt = ctypes.c_uint64(0)
         self._check(self._lib.cgs_mvc_read_bindings(self._ctx, 1 << 62, None, None,
@@ -318,7 +423,7 @@ class GpuPipelineState:
         self._check(self._lib.cgs_kernel_profile_read(self._ctx, ctypes.byref(kp)),
                     "cgs_kernel_profile_read")
         return {name: dict(ms=kp.ms[i], launches=int(kp.launches[i]),
-                           alg_bytes=int(kp.alg_bytes[i]))
+                           alg_bytes=int(kp.alg_bytes[i]), alg_flops=int(kp.alg_flops[i]))
                 for i, name in enumerate(_abi.KERNEL_NAMES)}
 
     def kernel_profile_reset(self) -> None:

@@ -170,11 +170,77 @@ int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound);
  * the reference's GPU API). */
 int cgs_mvc_weights(cgs_ctx* ctx, uint64_t n, const float* d_points, float* d_weights);
 
-/* Host copy of the first max_slots MVC bindings: gaussian [slots] (scene
- * index of each slot, ascending) and wg [slots*V*4] = (w, dw/dx, dw/dy,
- * dw/dz) per cage vertex. *out_slots receives the number copied. */
+/* Host copy of the first max_slots stored MVC bindings: gaussian [slots]
+ * (scene index of each slot, ascending) and wg [slots*V*4] = (w, dw/dx,
+ * dw/dy, dw/dz) per cage vertex. *out_slots receives the number copied.
+ * With learned bindings only the exact fallbacks are stored. */
 int cgs_mvc_read_bindings(cgs_ctx* ctx, uint64_t max_slots, uint32_t* gaussian, float* wg,
                           uint64_t* out_slots);
+
+/* ---- learned MVC weight field (no reference counterpart) ----
+ * A network that stands in for compute_mvc_weights (mvc.rs:366-471) of the
+ * uploaded polygon cage: Fourier features of the point (x^ = (x - c) / s,
+ * c and s the centre and half the largest extent of the rest cage's box;
+ * x^ and sin, cos of 2^b (pi/2) x^ for b = 0..7, zero-padded to 64), four
+ * 128-wide SiLU layers, V outputs z made a partition of unity by
+ * w0 = z + (1 - sum z) / V, then projected onto the weights that also
+ * reproduce linear functions on the rest cage:
+ * w = w0 - Vb^T M (Vb w0 - [1; x]), Vb = [1; rest vertices], M =
+ * (Vb Vb^T)^-1 (exact MVC has both properties; affine cage motions are then
+ * reproduced exactly). Weights and layer inputs are bf16, accumulation fp32
+ * on the tensor cores. Frames evaluate it per Gaussian together with its
+ * Jacobian. The linear-precision residual r = sum_j w0_j v_j - x of the
+ * network's own weights on the rest cage selects the Gaussians that keep
+ * exact stored weights. */
+
+/* New network (seeded) for the uploaded polygon cage. Drops learned
+ * bindings. */
+int cgs_mvc_field_create(cgs_ctx* ctx, uint64_t seed);
+
+/* Parameter block layout: offsets[10] (elements) of W1 [128x64], b1, W2,
+ * b2, W3, b3 [128x128 / 128], W4, b4, W5 [Vx128], b5 [V] (row-major
+ * out x in), *total floats, enc[4] = c and 1/s. Any pointer may be NULL. */
+int cgs_mvc_field_layout(cgs_ctx* ctx, uint32_t* offsets, uint32_t* total, float* enc);
+
+/* Copies the fp32 parameters to dst and/or from src (either may be NULL);
+ * loading resets the optimiser state and drops learned bindings. */
+int cgs_mvc_field_params(cgs_ctx* ctx, float* dst, const float* src);
+
+/* Trains with Adam (beta 0.9 / 0.999, eps 1e-8) for `steps` steps on batches
+ * of `batch` rows (a multiple of 8) drawn by a seeded hash from n device
+ * points d_points [n*3] with their exact weights d_weights [n*V]. Loss per
+ * batch of B rows: (1/B) sum_rows sum_j (w_j - w*_j)^2 + lambda (1/B)
+ * sum_rows |r|^2 / (3 s^2). The step size follows a cosine from lr down to
+ * lr/20 over the call's steps. out_loss[2] (may be NULL) receives the weight
+ * term and the residual term (without lambda) averaged over the last tenth
+ * of the steps. Drops learned bindings. */
+int cgs_mvc_field_train(cgs_ctx* ctx, uint64_t n, const float* d_points, const float* d_weights,
+                        uint32_t steps, uint32_t batch, float lr, float lambda, uint64_t seed,
+                        float* out_loss);
+
+/* Gradient of that loss over the first n points (n a multiple of 8, one
+ * batch, no update) into grads [total] on the host; out_loss[2] as above. */
+int cgs_mvc_field_grads(cgs_ctx* ctx, uint64_t n, const float* d_points, const float* d_weights,
+                        float lambda, float* grads, float* out_loss);
+
+/* Final (projected) network weights of n device points [n*3] into
+ * d_weights [n*V]. */
+int cgs_mvc_field_eval(cgs_ctx* ctx, uint64_t n, const float* d_points, float* d_weights);
+
+/* Fused inference as frames run it: for n device points [n*3], 12 floats
+ * each into d_out: position sum_j w_j v_j and its gradient F (column-major)
+ * on the current cage vertices; with use_rest, the network's own rest
+ * position sum_j w0_j v_j (x + r) and its gradient instead. d_out must be
+ * 16-byte aligned. */
+int cgs_mvc_field_infer(cgs_ctx* ctx, uint64_t n, const float* d_points, int32_t use_rest,
+                        float* d_out);
+
+/* As cgs_mvc_bind, with the network for every bound Gaussian whose
+ * linear-precision residual |r| / s is at most `threshold`; the others get
+ * exact stored weights (fallbacks, listed first by cgs_mvc_read_bindings).
+ * *out_bound and *out_fallback (either may be NULL) receive both counts. */
+int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t* out_bound,
+                         uint32_t* out_fallback);
 
 /* ---- frame (GpuPipelineState, render/gpu_state.rs:538-1243) ---- */
 
@@ -217,12 +283,15 @@ int cgs_framebuffer_device(cgs_ctx* ctx, void** d_rgba8, uint32_t* row_pitch_px)
 #define CGS_K_TILE_RANGES 6    /* (the tile transpose writes the ranges itself) */
 #define CGS_K_COMPOSITE 7
 #define CGS_K_SPLAT_SORT 8     /* depth-key histogram + radix passes over the splats */
-#define CGS_K_MVC 9            /* MVC position + gradient of every polygon-cage binding */
-#define CGS_KERNEL_COUNT 10
+#define CGS_K_MVC 9            /* MVC position + gradient of every stored polygon-cage binding */
+#define CGS_K_FIELD 10         /* learned MVC field: output projection + fused inference */
+#define CGS_KERNEL_COUNT 11
 typedef struct cgs_kernel_profile {
   double ms[CGS_KERNEL_COUNT];
   uint64_t alg_bytes[CGS_KERNEL_COUNT];
   uint32_t launches[CGS_KERNEL_COUNT];
+  /* tensor-core work of the kernels that have any (multiply-adds count 2) */
+  uint64_t alg_flops[CGS_KERNEL_COUNT];
 } cgs_kernel_profile;
 int cgs_kernel_profile_read(cgs_ctx* ctx, cgs_kernel_profile* out);
 int cgs_kernel_profile_reset(cgs_ctx* ctx);
