@@ -15,6 +15,14 @@ Arms:
 Multi-GPU (torchrun, one process per GPU): replicas; each rank renders its own
 views (frames rank, rank+N, ...), no data exchange; value = all frames / max
 rank time (weak scaling).
+
+  python bench.py --workload mvc [--steps K --warmup W]
+Polygon-cage workload (3,000,000 Gaussians uniform in the unit ball, level-3
+icosphere cage of radius 1.15 displaced by a smooth random field of amplitude
+0.1, moved every frame by another such field, 1920x1080): Stage 1 with exact
+stored MVC bindings against Stage 1 with the learned weight field trained on
+2,000,000 interior points with exact weights, on the same frames; the learned
+deformation's error is judged by the exact one. One JSON line, 1 GPU.
 """
 from __future__ import annotations
 
@@ -59,7 +67,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--gaussians", type=int, default=1_100_000)
+    ap.add_argument("--workload", choices=["tet", "mvc"], default="tet")
+    ap.add_argument("--gaussians", type=int, default=None,
+                    help="default 1,100,000 (tet) or 3,000,000 (mvc)")
+    ap.add_argument("--train-points", type=int, default=2_000_000)
+    ap.add_argument("--train-steps", type=int, default=6000)
+    ap.add_argument("--fallback-quantile", type=float, default=0.99,
+                    help="residual quantile above which bound Gaussians keep exact weights")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -79,7 +93,8 @@ def dist_setup(args):
 
 def workload(args):
     from cindergs_b200 import workloads
-    return workloads.tet_cage_orbit(n=args.gaussians, width=args.width, height=args.height)
+    return workloads.tet_cage_orbit(n=args.gaussians or 1_100_000, width=args.width,
+                                    height=args.height)
 
 
 def peaks():
@@ -173,7 +188,7 @@ def cpu_reference_frames(wl, bind_tet, bind_w, frames, start_frame=0):
 
 def config_dict(args, wl, world):
     return {"workload": "tet-cage deform + render, orbit camera",
-            "gaussians": args.gaussians, "width": args.width, "height": args.height,
+            "gaussians": wl.scene.count, "width": args.width, "height": args.height,
             "cage": "5x5x5 cubes x 6 tets (750 tets, 216 vertices), springs k=40 c=4 dt=1/60",
             "sh_degree": 3, "keys": "32-bit tile|depth", "radix_digits": radix_digits(args),
             "entry_sort": ["auto (radix)", "radix", "tile transpose"][args.entry_sort],
@@ -372,8 +387,157 @@ def run_ours(args):
     return 0
 
 
+def run_mvc(args):
+    """Exact vs learned MVC Stage 1 on the polygon-cage workload (1 GPU)."""
+    import torch
+    from cindergs_b200 import GpuPipelineState, _abi, workloads
+    torch.cuda.set_device(0)
+    n = args.gaussians or 3_000_000
+    wl = workloads.mvc_cage_sphere(n=n, width=args.width, height=args.height)
+    stream = torch.cuda.Stream(device=0)
+    st = GpuPipelineState(0, stream=stream.cuda_stream)
+    st.upload_scene(wl.scene)
+    st.upload_cages(None)
+    st.mvc_cage_upload(wl.cage)
+    stage1 = ("mvc", "field", "deform")
+
+    def timed(t0_event_fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = t0_event_fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return out, a.elapsed_time(b)
+
+    def frames(first):
+        """warm-up, then `steps` profiled frames from frame `first`; returns
+        (per-kernel ms per frame, frame ms, deformed positions of frame `first`)."""
+        def one(f, profile, timings):
+            st.mvc_vertices_update(wl.vertices(f))
+            cam = wl.camera(f)
+            return st.execute_frame_gpu(wl.scene, None, cam, wl.compositor(cam), 0.0, 0.0,
+                                        profile_stages=profile, stage_timings=timings)
+        one(first, False, True)
+        pos = st.read_buffer(_abi.BUF_DEFORMED_POS, np.float32).reshape(-1, 3).copy()
+        for f in range(max(args.warmup, 3)):
+            one(first + 1 + f, False, False)
+        st.synchronize()
+        st.kernel_profile_reset()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for f in range(args.steps):
+            one(first + 1 + f, True, False)
+        b.record(stream)
+        st.synchronize()
+        torch.cuda.synchronize()
+        kp = st.kernel_profile()
+        per = {k: dict(ms=d["ms"] / args.steps, alg_bytes=d["alg_bytes"] // args.steps,
+                       alg_flops=d["alg_flops"] // args.steps, launches=d["launches"])
+               for k, d in kp.items() if d["launches"]}
+        return per, a.elapsed_time(b) / args.steps, pos
+
+    # ---- exact: inside test + weights + central-difference gradients, stored
+    nb, bind_ms = timed(st.mvc_bind)
+    k_exact, frame_exact, pos_exact = frames(0)
+    s1_exact = sum(k_exact.get(k, {}).get("ms", 0.0) for k in stage1)
+
+    # ---- training data and training (exact weights from the MVC kernel)
+    pts = torch.from_numpy(wl.training_points(args.train_points)).to("cuda:0")
+    w, weights_ms = timed(lambda: st.mvc_weights(pts))
+    st.mvc_field_create(seed=1)
+    loss, train_ms = timed(lambda: st.mvc_field_train(pts, w, steps=args.train_steps, batch=4096,
+                                                      lr=2e-3, lam=0.05, seed=5))
+    del w, pts
+    torch.cuda.empty_cache()
+
+    # ---- learned bindings: fallback threshold at a quantile of the residuals
+    _, _, enc = st.mvc_field_layout()
+    s = 1.0 / float(enc[3])
+    rng = np.random.default_rng(7)
+    sample = wl.scene.positions[rng.choice(n, min(n, 200_000), replace=False)]
+    raw, _ = st.mvc_field_infer(sample, rest=True)
+    res = np.linalg.norm(raw - sample, axis=1) / s
+    thr = float(np.quantile(res, args.fallback_quantile))
+    (nbl, nfb), pf_bind_ms = timed(lambda: st.mvc_bind_learned(thr, per_frame=True))
+    k_pf, frame_pf, pos_pf = frames(0)
+    s1_pf = sum(k_pf.get(k, {}).get("ms", 0.0) for k in stage1)
+    (nbl, nfb), learned_bind_ms = timed(lambda: st.mvc_bind_learned(thr))
+    k_learned, frame_learned, pos_learned = frames(0)
+    s1_learned = sum(k_learned.get(k, {}).get("ms", 0.0) for k in stage1)
+    mode_diff = float((np.linalg.norm(pos_learned[:n].astype(np.float64) - pos_pf[:n], axis=1)
+                       / (1.0 / float(enc[3]))).max())
+
+    err = np.linalg.norm(pos_learned[:n].astype(np.float64) - pos_exact[:n], axis=1) / s
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+        pk = json.load(f)
+    fk = k_pf.get("field", {})
+    ck = k_learned.get("field", {})
+    code_gbs = ck["alg_bytes"] / (ck["ms"] / 1000.0) / 1e9 if ck.get("ms") else None
+    field_tflops = fk["alg_flops"] / (fk["ms"] / 1000.0) / 1e12 if fk.get("ms") else None
+    mk = k_exact.get("mvc", {})
+    mvc_gbs = mk["alg_bytes"] / (mk["ms"] / 1000.0) / 1e9 if mk.get("ms") else None
+    line = {
+        "metric": "MVC Stage 1 ms/frame: learned weight field vs exact stored bindings",
+        "value": s1_learned, "unit": "ms/frame", "higher_is_better": False, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "bf16 MLP (fp32 accumulate)",
+        "data": "synthetic",
+        "config": {"workload": "polygon-cage MVC, exact vs learned", "gaussians": n,
+                   "cage": "icosphere L3 r=1.15, 642 vertices / 1280 triangles, displaced 0.1",
+                   "motion": "moving smooth random field, amplitude 0.1",
+                   "width": args.width, "height": args.height,
+                   "train_points": args.train_points, "train_steps": args.train_steps},
+        "stage1_ms": {"exact": s1_exact, "learned": s1_learned,
+                      "speedup": s1_exact / s1_learned if s1_learned else None,
+                      "learned_per_frame_network": s1_pf,
+                      "speedup_per_frame_network": s1_exact / s1_pf if s1_pf else None},
+        "frame_ms": {"exact": frame_exact, "learned": frame_learned,
+                     "learned_per_frame_network": frame_pf},
+        "kernels_ms": {"exact": {k: v["ms"] for k, v in k_exact.items()},
+                       "learned": {k: v["ms"] for k, v in k_learned.items()},
+                       "learned_per_frame_network": {k: v["ms"] for k, v in k_pf.items()}},
+        "modes": {"learned": "network codes kept per Gaussian (1 KB), output layer per frame",
+                  "learned_per_frame_network": "whole network per Gaussian every frame",
+                  "max_rel_position_difference": mode_diff},
+        "exact_weights": {"bind_ms": bind_ms, "bound": nb,
+                          "stored_bytes": nb * wl.cage.num_vertices * 16,
+                          "train_weights_ms": weights_ms},
+        "learned": {"bind_ms": learned_bind_ms, "bind_ms_per_frame_network": pf_bind_ms,
+                    "bound": nbl, "fallbacks": nfb, "code_bytes": (nbl - nfb) * 1024,
+                    "residual_threshold": thr, "train_ms": train_ms, "loss_terms": loss},
+        "error": {"judge": "exact MVC deformation of the same frame",
+                  "mean_rel_position": float(err.mean()),
+                  "p99_rel_position": float(np.quantile(err, 0.99)),
+                  "max_rel_position": float(err.max()), "relative_to": "cage half-extent s",
+                  "s": s},
+        "roofline": {
+            "field": {"bound": "tensor", "achieved": field_tflops,
+                      "peak": pk.get("bf16_tflops"), "unit": "TFLOP/s",
+                      "frac": field_tflops / pk["bf16_tflops"] if field_tflops else None,
+                      "flops_per_launch": fk.get("alg_flops")},
+            "field_codes": {"bound": "hbm", "achieved": code_gbs, "peak": pk.get("hbm_gbs"),
+                            "unit": "GB/s",
+                            "frac": code_gbs / pk["hbm_gbs"] if code_gbs else None,
+                            "bytes_per_launch": ck.get("alg_bytes")},
+            "mvc_exact": {"bound": "hbm", "achieved": mvc_gbs, "peak": pk.get("hbm_gbs"),
+                          "unit": "GB/s", "frac": mvc_gbs / pk["hbm_gbs"] if mvc_gbs else None,
+                          "bytes_per_launch": mk.get("alg_bytes")}},
+    }
+    print(json.dumps(line), flush=True)
+    st.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "mvc":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference's MVC deformation is its CPU path; "
+                              "exact GPU MVC is this leg's judge"}))
+            return 0
+        return run_mvc(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -83,6 +83,7 @@ class CgsStageTimings(ctypes.Structure):
 
 
 SORT_AUTO, SORT_RADIX, SORT_TRANSPOSE = 0, 1, 2
+FIELD_PER_FRAME = 1
 
 KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "entry_sort",
                 "tile_ranges", "composite", "splat_sort", "mvc", "field"]
@@ -133,7 +134,7 @@ SIGNATURES = {
     "cgs_mvc_field_grads": (_i32, [_vp, _u64, _vp, _vp, ctypes.c_float, _vp, _vp]),
     "cgs_mvc_field_eval": (_i32, [_vp, _u64, _vp, _vp]),
     "cgs_mvc_field_infer": (_i32, [_vp, _u64, _vp, _i32, _vp]),
-    "cgs_mvc_bind_learned": (_i32, [_vp, ctypes.c_float, ctypes.POINTER(_u32),
+    "cgs_mvc_bind_learned": (_i32, [_vp, ctypes.c_float, _u32, ctypes.POINTER(_u32),
                                     ctypes.POINTER(_u32)]),
     "cgs_scan_u32": (_int, [_vp, _vp, _vp, _u64, ctypes.POINTER(_u64)]),
     "cgs_sort_pairs_u32": (_int, [_vp, _vp, _vp, _u64, _u32, _i32]),

@@ -126,6 +126,11 @@ struct FieldInfer {
   const float* points3;  // packed xyz when points4 is null
   uint32_t first, count, out_first;
   float4* xf;            // [(out_first + count) * 3]
+  // cached codes [count][4][128] bf16 and the items' rest positions
+  // [count]: written by launch_field_infer when codes is set (instead of
+  // xf), read by launch_field_apply
+  __nv_bfloat16* codes;
+  float4* code_pos;
 };
 size_t field_infer_smem();
 cudaError_t launch_field_gather(const FieldBatch& b, cudaStream_t s);
@@ -148,6 +153,8 @@ cudaError_t launch_field_project(const FieldNet& net, uint32_t V, const float4* 
                                  const float4* verts, const float* M, float* proj,
                                  cudaStream_t s);
 cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s);
+// Output layer over cached codes (needs codes, points4): position + gradient.
+cudaError_t launch_field_apply(const FieldInfer& fi, cudaStream_t s);
 
 cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s);
 

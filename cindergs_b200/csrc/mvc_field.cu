@@ -378,51 +378,49 @@ __global__ void k_adam(uint32_t n, float* __restrict__ p, const float* __restric
 
 // ---- frame: per-frame projection and fused inference ---------------------------
 
-// Per-frame projection of the output layer (one block of 128 threads). For
+// Per-frame projection of the output layer (one block of 1024 threads). For
 // vertices u (rest or current), P_u[k] = sum_j W5[j][k] u_j - c_k ubar with
 // c_k = sum_j W5[j][k], and p0_u = sum_j b5_j u_j + (1 - sum_j b5_j) ubar, so
 // that sum_j w0_j u_j = P_u^T h + p0_u. Raw mode (verts == null): P_rest,
 // p0_rest and A3 = 0, i.e. the network's own rest position sum_j w0_j v_j.
 // Otherwise A = v'^T Vb^T M, Pc = P_cur - P_rest A3^T, pc = p0_cur - A3 p0_rest.
-// proj = [Pc (128 x 3) | pc (3) | A3 (3 x 3, row-major)].
-__global__ void __launch_bounds__(128) k_field_project(FieldNet net, uint32_t V,
-                                                       const float4* __restrict__ rest,
-                                                       const float4* __restrict__ verts,
-                                                       const float* __restrict__ M,
-                                                       float* __restrict__ proj) {
-  __shared__ float red[20 * 32];
+// proj = [Pc (128 x 3) | pc (3) | A3 (3 x 3, row-major)]. Both vertex sets
+// are staged in shared memory; thread (g, k) sums vertices j = g mod 8 for
+// hidden unit k and the eight partial sums are added in g order.
+constexpr int kProjThreads = 1024, kProjGroups = kProjThreads / kHid;
+__global__ void __launch_bounds__(kProjThreads) k_field_project(FieldNet net, uint32_t V,
+                                                                const float4* __restrict__ rest,
+                                                                const float4* __restrict__ verts,
+                                                                const float* __restrict__ M,
+                                                                float* __restrict__ proj) {
+  extern __shared__ float4 pv[];  // [V] rest, [V] current
+  __shared__ float red[22 * 32];
+  __shared__ float part[kProjGroups][7][kHid];
   __shared__ float sh[20];
   const bool raw = verts == nullptr;
-  // sums: rest (3), rest . b5 (3), sum b5 (1), current (3), current . b5 (3),
-  // S = v'^T Vb^T without its first column's duplicate (9: sum_j v'_j v_j^T)
-  float t[20];
-#pragma unroll
-  for (int k = 0; k < 20; ++k) t[k] = 0.0f;
   for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
-    const float4 v = rest[j];
+    pv[j] = rest[j];
+    pv[V + j] = raw ? make_float4(0.f, 0.f, 0.f, 0.f) : verts[j];
+  }
+  __syncthreads();
+  // sums: rest (3), rest . b5 (3), sum b5 (1), current (3), current . b5 (3),
+  // sum_j v'_j v_j^T (9)
+  float t[22];
+#pragma unroll
+  for (int k = 0; k < 22; ++k) t[k] = 0.0f;
+  for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
+    const float4 v = pv[j], c = pv[V + j];
     const float b = net.b5[j];
     t[0] += v.x; t[1] += v.y; t[2] += v.z;
     t[3] += b * v.x; t[4] += b * v.y; t[5] += b * v.z;
     t[6] += b;
-    if (!raw) {
-      const float4 c = verts[j];
-      t[7] += c.x; t[8] += c.y; t[9] += c.z;
-      t[10] += b * c.x; t[11] += b * c.y; t[12] += b * c.z;
-      t[13] += c.x * v.x; t[14] += c.x * v.y; t[15] += c.x * v.z;
-      t[16] += c.y * v.x; t[17] += c.y * v.y; t[18] += c.y * v.z;
-      t[19] += c.z * v.x;
-    }
+    t[7] += c.x; t[8] += c.y; t[9] += c.z;
+    t[10] += b * c.x; t[11] += b * c.y; t[12] += b * c.z;
+    t[13] += c.x * v.x; t[14] += c.x * v.y; t[15] += c.x * v.z;
+    t[16] += c.y * v.x; t[17] += c.y * v.y; t[18] += c.y * v.z;
+    t[19] += c.z * v.x; t[20] += c.z * v.y; t[21] += c.z * v.z;
   }
-  // the last entry of S (c.z * v.y, c.z * v.z) goes through a second pass
-  block_sums<20>(t, red);
-  float t2[2] = {0.0f, 0.0f};
-  if (!raw)
-    for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) {
-      const float4 v = rest[j], c = verts[j];
-      t2[0] += c.z * v.y;
-      t2[1] += c.z * v.z;
-    }
-  block_sums<2>(t2, red);
+  block_sums<22>(t, red);
   if (threadIdx.x == 0) {
     const float inv_v = 1.0f / (float)V;
     const float rb[3] = {t[0] * inv_v, t[1] * inv_v, t[2] * inv_v};
@@ -440,14 +438,14 @@ __global__ void __launch_bounds__(128) k_field_project(FieldNet net, uint32_t V,
       // S (3 x 4): column 0 = sum_j v'_j, columns 1..3 = sum_j v'_j v_j^T
       const float S[3][4] = {{t[7], t[13], t[14], t[15]},
                              {t[8], t[16], t[17], t[18]},
-                             {t[9], t[19], t2[0], t2[1]}};
+                             {t[9], t[19], t[20], t[21]}};
       float A3[3][3];
       for (int q = 0; q < 3; ++q)
         for (int d = 0; d < 3; ++d) {
-          float a = 0.0f;
-          for (int k = 0; k < 4; ++k) a += S[q][k] * M[4 * k + 1 + d];
-          A3[q][d] = a;
-          sh[11 + 3 * q + d] = a;
+          float acc = 0.0f;
+          for (int k = 0; k < 4; ++k) acc += S[q][k] * M[4 * k + 1 + d];
+          A3[q][d] = acc;
+          sh[11 + 3 * q + d] = acc;
         }
       for (int q = 0; q < 3; ++q) {
         sh[6 + q] = cb[q];
@@ -458,26 +456,32 @@ __global__ void __launch_bounds__(128) k_field_project(FieldNet net, uint32_t V,
       }
     }
   }
-  __syncthreads();
-  const uint32_t k = threadIdx.x;  // hidden unit (blockDim.x == 128)
-  float ar[3] = {0.0f, 0.0f, 0.0f}, ac[3] = {0.0f, 0.0f, 0.0f}, c = 0.0f;
-  for (uint32_t j = 0; j < V; ++j) {
+  const uint32_t k = threadIdx.x % kHid, g = threadIdx.x / kHid;
+  float acc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // rest (3), current (3), c
+  for (uint32_t j = g; j < V; j += kProjGroups) {
     const float w = __bfloat162float(net.W5b[(size_t)j * kHid + k]);
-    const float4 v = rest[j];
-    ar[0] += w * v.x; ar[1] += w * v.y; ar[2] += w * v.z;
-    if (!raw) {
-      const float4 u = verts[j];
-      ac[0] += w * u.x; ac[1] += w * u.y; ac[2] += w * u.z;
-    }
-    c += w;
+    const float4 v = pv[j], u = pv[V + j];
+    acc[0] += w * v.x; acc[1] += w * v.y; acc[2] += w * v.z;
+    acc[3] += w * u.x; acc[4] += w * u.y; acc[5] += w * u.z;
+    acc[6] += w;
+  }
+#pragma unroll
+  for (int q = 0; q < 7; ++q) part[g][q][k] = acc[q];
+  __syncthreads();  // also publishes sh
+  if (g != 0) return;
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    float tot = 0.0f;
+    for (int gg = 0; gg < kProjGroups; ++gg) tot += part[gg][q][k];
+    acc[q] = tot;
   }
   float pr[3];
-  for (int q = 0; q < 3; ++q) pr[q] = ar[q] - c * sh[q];
+  for (int q = 0; q < 3; ++q) pr[q] = acc[q] - acc[6] * sh[q];
   if (raw) {
     for (int q = 0; q < 3; ++q) proj[3 * k + q] = pr[q];
   } else {
     for (int q = 0; q < 3; ++q) {
-      const float pc = ac[q] - c * sh[6 + q];
+      const float pc = acc[3 + q] - acc[6] * sh[6 + q];
       proj[3 * k + q] = pc - (sh[11 + 3 * q] * pr[0] + sh[12 + 3 * q] * pr[1] +
                               sh[13 + 3 * q] * pr[2]);
     }
@@ -544,6 +548,10 @@ __device__ __forceinline__ void to_a(const float (&c)[16][4], uint32_t (&a)[8][4
   }
 }
 
+// CODES: instead of the position and gradient, store the last hidden layer
+// and its three tangents (bf16, as the output layer consumes them) per item:
+// codes[item][stream][128], stream 0 = h, 1..3 = dh/dx, dh/dy, dh/dz.
+template <bool CODES>
 __global__ void __launch_bounds__(kFwdWarps * 32, 1) k_field_infer(FieldInfer fi) {
   extern __shared__ __align__(16) unsigned char fsm[];
   __nv_bfloat16* W1 = reinterpret_cast<__nv_bfloat16*>(fsm);
@@ -618,6 +626,21 @@ __global__ void __launch_bounds__(kFwdWarps * 32, 1) k_field_infer(FieldInfer fi
       to_a(c, a);
       layer_mma<8>(a, Wh + l * kHid * kWld, kWld, gq, tq, c);
       layer_act(c, bias + (l + 1) * kHid, value_lane, tq);
+    }
+    if (CODES) {
+      if (valid && value_lane && tq == 0) fi.code_pos[k] = make_float4(xr[0], xr[1], xr[2], 0.0f);
+      if (valid) {
+        // rows: value lanes (h, dh/dy), tangent lanes (dh/dx, dh/dz)
+        const int s0 = value_lane ? 0 : 1, s1 = value_lane ? 2 : 3;
+        __nv_bfloat16* base = fi.codes + (size_t)k * (4 * kHid);
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) {
+          const int col = nt * 8 + 2 * tq;
+          *reinterpret_cast<uint32_t*>(base + s0 * kHid + col) = pack_bf16(c[nt][0], c[nt][1]);
+          *reinterpret_cast<uint32_t*>(base + s1 * kHid + col) = pack_bf16(c[nt][2], c[nt][3]);
+        }
+      }
+      continue;
     }
     // x' = P^T h + p0 on value rows, F columns = P^T dh on tangent rows; h
     // and dh in bf16, as the output layer saw them in training
@@ -730,6 +753,100 @@ __global__ void k_mvc_reslot(uint32_t nb, const uint32_t* __restrict__ flag,
   bind_w[i] = make_float4(__uint_as_float(slot), 0.0f, 0.0f, 0.0f);
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Per-frame output layer over cached codes (k_field_infer<true>). Each warp
+// owns a contiguous range of items and streams them through a kApStages-deep
+// ring in shared memory with cp.async: lane l copies 16-byte chunks 2l, 2l+1
+// of the item's 1 KB code (the ones it reads back: hidden units 16 (l % 8)
+// .. + 15 of stream l / 8), lane 0 also the item's rest position. Lane l
+// keeps its 48 projection entries in registers; the eight lanes of a stream
+// reduce their partial P^T code, and lanes 0..11 each form one output float
+// (position + pc + A3 x, gradient + A3) and store the item's 48 bytes
+// together (k_mvc_jacobian's layout).
+constexpr int kApStages = 8, kApWarps = 8, kApStage = 4 * kHid * 2 / 16 + 1;  // uint4 per stage
+
+__global__ void __launch_bounds__(kApWarps * 32) k_field_apply(FieldInfer fi) {
+  extern __shared__ uint4 ap_ring[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint4* ring = ap_ring + (size_t)warp * kApStages * kApStage;
+  const int k0 = (lane & 7) * 16;
+  float pr[16][3];
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pr[i][c] = fi.proj[3 * (k0 + i) + c];
+  // output float o = lane (< 12): 0..2 position, 3 + 3 d + c gradient F[c][d]
+  const int o = lane < 12 ? lane : 0;
+  const int oc = o < 3 ? o : (o - 3) % 3;
+  const int os = o < 3 ? 0 : 1 + (o - 3) / 3;  // stream feeding this output
+  const float* pc = fi.proj + 3 * kHid;
+  const float* A3 = pc + 3;
+  const float bias0 = o < 3 ? pc[oc] : A3[3 * oc + (os - 1)];
+  const float a30 = A3[3 * oc], a31 = A3[3 * oc + 1], a32 = A3[3 * oc + 2];
+  const uint32_t gw = blockIdx.x * kApWarps + warp, nw = gridDim.x * kApWarps;
+  const uint32_t per = (fi.count + nw - 1) / nw;
+  const uint32_t i0 = min(fi.count, gw * per), i1 = min(fi.count, i0 + per);
+  auto issue = [&](uint32_t item, int stage) {
+    if (item < i1) {
+      const uint4* src = reinterpret_cast<const uint4*>(fi.codes + (size_t)item * (4 * kHid));
+      uint4* dst = ring + stage * kApStage;
+      cp_async16(dst + 2 * lane, src + 2 * lane);
+      cp_async16(dst + 2 * lane + 1, src + 2 * lane + 1);
+      if (lane == 0) cp_async16(dst + kApStage - 1, fi.code_pos + item);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < kApStages - 1; ++k) issue(i0 + k, k);
+  int stage = 0;
+  for (uint32_t item = i0; item < i1; ++item) {
+    issue(item + kApStages - 1, (stage + kApStages - 1) % kApStages);
+    cp_async_wait<kApStages - 1>();
+    __syncwarp();  // lane 0's copy of the position
+    const uint4* sb = ring + stage * kApStage;
+    const uint4 q[2] = {sb[2 * lane], sb[2 * lane + 1]};
+    const float4 x4 = *reinterpret_cast<const float4*>(sb + kApStage - 1);
+    float a[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t u[4] = {q[h].x, q[h].y, q[h].z, q[h].w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float lo = __uint_as_float(u[e] << 16), hi = __uint_as_float(u[e] & 0xFFFF0000u);
+        const int i = 8 * h + 2 * e;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[c] += lo * pr[i][c] + hi * pr[i + 1][c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      a[c] += __shfl_xor_sync(0xffffffffu, a[c], 4);
+      a[c] += __shfl_xor_sync(0xffffffffu, a[c], 2);
+      a[c] += __shfl_xor_sync(0xffffffffu, a[c], 1);
+    }
+    const float t0 = __shfl_sync(0xffffffffu, a[0], 8 * os);
+    const float t1 = __shfl_sync(0xffffffffu, a[1], 8 * os);
+    const float t2 = __shfl_sync(0xffffffffu, a[2], 8 * os);
+    float v = (oc == 0 ? t0 : (oc == 1 ? t1 : t2)) + bias0;
+    if (o < 3) v += a30 * x4.x + a31 * x4.y + a32 * x4.z;
+    if (lane < 12) reinterpret_cast<float*>(fi.xf)[12 * (size_t)(fi.out_first + item) + lane] = v;
+    __syncwarp();  // every lane has read this stage before it is refilled
+    stage = stage + 1 == kApStages ? 0 : stage + 1;
+  }
+  cp_async_wait<0>();
+}
+
 }  // namespace
 
 size_t field_infer_smem() {
@@ -803,19 +920,44 @@ cudaError_t launch_adam(uint32_t n, float* p, const float* g, float* m, float* v
 cudaError_t launch_field_project(const FieldNet& net, uint32_t V, const float4* rest,
                                  const float4* verts, const float* M, float* proj,
                                  cudaStream_t s) {
-  k_field_project<<<1, 128, 0, s>>>(net, V, rest, verts, M, proj);
+  // static shared memory (~32 KB) plus the two vertex sets
+  const size_t smem = (size_t)V * 32;
+  const cudaError_t e = cudaFuncSetAttribute(
+      k_field_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_field_project<<<1, kProjThreads, smem, s>>>(net, V, rest, verts, M, proj);
   return cudaGetLastError();
 }
 
 cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s) {
   if (fi.count == 0) return cudaSuccess;
   const size_t smem = field_infer_smem();
-  const cudaError_t e =
-      cudaFuncSetAttribute(k_field_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   const uint32_t groups = (fi.count + 3) / 4;
   const uint32_t blocks = std::min<uint32_t>(148u, (groups + kFwdWarps - 1) / kFwdWarps);
-  k_field_infer<<<blocks, kFwdWarps * 32, smem, s>>>(fi);
+  if (fi.codes) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        k_field_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_field_infer<true><<<blocks, kFwdWarps * 32, smem, s>>>(fi);
+  } else {
+    const cudaError_t e = cudaFuncSetAttribute(
+        k_field_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_field_infer<false><<<blocks, kFwdWarps * 32, smem, s>>>(fi);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_apply(const FieldInfer& fi, cudaStream_t s) {
+  if (fi.count == 0) return cudaSuccess;
+  if (!fi.codes || !fi.code_pos) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)kApWarps * kApStages * kApStage * 16;
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_field_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // three blocks per SM (registers and shared memory allow it)
+  const uint32_t blocks = std::min<uint32_t>(148u * 3u, (fi.count + 7) / 8);
+  k_field_apply<<<blocks, kApWarps * 32, smem, s>>>(fi);
   return cudaGetLastError();
 }
 

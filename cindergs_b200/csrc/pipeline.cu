@@ -144,12 +144,15 @@ struct cgs_ctx {
   // evaluated by the network every frame
   FieldState field;
   bool field_ready = false, mvc_learned = false;
+  bool mvc_cached = false;  // learned slots keep the network's codes (1 KB each)
   uint32_t mvc_nfb = 0;
+  DevBuf mvc_codes, mvc_code_pos;
   uint32_t mvc_nwg() const { return mvc_learned ? mvc_nfb : mvc_nb; }  // stored slots
   void mvc_unbind() {
     mvc_nb = 0;
     mvc_nfb = 0;
     mvc_learned = false;
+    mvc_cached = false;
   }
   // Field inference over the learned slots: rest positions in, position and
   // gradient into mvc_xf at the same slots.
@@ -164,6 +167,8 @@ struct cgs_ctx {
     fi.count = mvc_nb - mvc_nfb;
     fi.out_first = mvc_nfb;
     fi.xf = mvc_xf.as<float4>();
+    fi.codes = nullptr;
+    fi.code_pos = nullptr;
     return fi;
   }
   bool deform_on() const { return has_cages || mvc_nb > 0; }
@@ -198,6 +203,17 @@ struct cgs_ctx {
   uint32_t radix_lb_bits = 0;
   int radix_parity = 0;
   HostCounters* h_ring = nullptr;  // pinned [kRing]
+  // Pinned staging of the per-frame uploads (cage vertices): a copy from
+  // pageable memory synchronises the stream before it starts, one from a
+  // pinned slot is enqueued behind the frames in flight. A slot is refilled
+  // once the copy that last read it has completed (its event).
+  struct UploadRing {
+    void* p[kRing] = {};
+    size_t cap[kRing] = {};
+    cudaEvent_t ev[kRing] = {};
+    bool pending[kRing] = {};
+    int next = 0;
+  } up;
   uint32_t* h_misc = nullptr;      // pinned scratch for the primitives
   // Stage 3 cache
   bool s3_valid = false;
@@ -624,9 +640,14 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       // learned slots: slot -> Gaussian, rest position in, position + F out;
       // four streams (value and three tangents) through the hidden layers
       const uint64_t L = ctx->mvc_nb - ctx->mvc_nfb;
-      kp.alg_bytes[CGS_K_FIELD] += L * (4 + 16 + 48);
-      kp.alg_flops[CGS_K_FIELD] +=
-          L * 4 * 2 * ((uint64_t)kFieldIn * kFieldHid + 3ull * kFieldHid * kFieldHid);
+      if (ctx->mvc_cached) {
+        // cached code (value + 3 tangents, 128 bf16 each) in
+        kp.alg_bytes[CGS_K_FIELD] += L * (16 + 48 + 4 * kFieldHid * 2);
+      } else {
+        kp.alg_bytes[CGS_K_FIELD] += L * (4 + 16 + 48);
+        kp.alg_flops[CGS_K_FIELD] +=
+            L * 4 * 2 * ((uint64_t)kFieldIn * kFieldHid + 3ull * kFieldHid * kFieldHid);
+      }
     }
     if (p.need_deform) {
       kp.alg_bytes[CGS_K_TET_TRANSFORMS] += T * (16 + 36 + 48 + 76);
@@ -659,6 +680,32 @@ int drain(cgs_ctx* ctx, bool block) {
     const int k = (ctx->next_slot + i - 1) % kRing;  // oldest first
     CGS_TRY(check_slot(ctx, k, block));
   }
+  return CGS_OK;
+}
+
+// Enqueues a host -> device copy of `bytes` through the next pinned upload
+// slot; fill(slot) writes the bytes into the slot.
+template <typename Fill>
+int staged_upload(cgs_ctx* ctx, void* dst, size_t bytes, Fill fill, const char* what) {
+  auto& r = ctx->up;
+  const int k = r.next;
+  r.next = (k + 1) % kRing;
+  if (r.pending[k]) {
+    CGS_CUDA(cudaEventSynchronize(r.ev[k]), what);
+    r.pending[k] = false;
+  }
+  if (r.cap[k] < bytes) {
+    if (r.p[k]) cudaFreeHost(r.p[k]);
+    r.p[k] = nullptr;
+    r.cap[k] = 0;
+    CGS_CUDA(cudaHostAlloc(&r.p[k], bytes, cudaHostAllocDefault), what);
+    r.cap[k] = bytes;
+  }
+  if (!r.ev[k]) CGS_CUDA(cudaEventCreateWithFlags(&r.ev[k], cudaEventDisableTiming), what);
+  fill(r.p[k]);
+  CGS_CUDA(cudaMemcpyAsync(dst, r.p[k], bytes, cudaMemcpyHostToDevice, ctx->stream), what);
+  CGS_CUDA(cudaEventRecord(r.ev[k], ctx->stream), what);
+  r.pending[k] = true;
   return CGS_OK;
 }
 
@@ -725,6 +772,10 @@ int cgs_ctx_destroy(cgs_ctx* ctx) {
   }
   if (ctx->h_ring) cudaFreeHost(ctx->h_ring);
   if (ctx->h_misc) cudaFreeHost(ctx->h_misc);
+  for (int k = 0; k < kRing; ++k) {
+    if (ctx->up.p[k]) cudaFreeHost(ctx->up.p[k]);
+    if (ctx->up.ev[k]) cudaEventDestroy(ctx->up.ev[k]);
+  }
   cudaStream_t s = ctx->stream;
   bool own = ctx->own_stream;
   delete ctx;
@@ -861,8 +912,8 @@ int cgs_cage_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_vert
       std::memcmp(ctx->last_verts.data(), verts, cnt * 4) == 0)
     return CGS_OK;
   cudaSetDevice(ctx->device);
-  CGS_CUDA(cudaMemcpyAsync(ctx->cage_verts.p, verts, cnt * 4, cudaMemcpyHostToDevice, ctx->stream), "upload vertices");
-  // pageable source: the copy has completed when cudaMemcpyAsync returns
+  CGS_TRY(staged_upload(ctx, ctx->cage_verts.p, cnt * 4,
+                        [&](void* dst) { std::memcpy(dst, verts, cnt * 4); }, "upload vertices"));
   ctx->last_verts.assign(verts, verts + cnt);
   ctx->verts_uploaded = true;
   ctx->deformed_valid = false;
@@ -936,12 +987,11 @@ int cgs_mvc_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t V) {
   if (ctx->mvc_last_verts.size() == cnt && std::memcmp(ctx->mvc_last_verts.data(), verts, cnt * 4) == 0)
     return CGS_OK;
   cudaSetDevice(ctx->device);
-  std::vector<float4> v4(V);
-  for (uint32_t j = 0; j < V; ++j) v4[j] = make_float4(verts[3 * j], verts[3 * j + 1], verts[3 * j + 2], 0.0f);
-  // a pageable staging vector: the copy has completed when the call returns
-  CGS_CUDA(cudaMemcpyAsync(ctx->mvc_verts.p, v4.data(), (size_t)V * 16, cudaMemcpyHostToDevice, ctx->stream),
-           "mvc vertices");
-  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "mvc vertices");
+  CGS_TRY(staged_upload(ctx, ctx->mvc_verts.p, (size_t)V * 16, [&](void* dst) {
+    float4* v4 = static_cast<float4*>(dst);
+    for (uint32_t j = 0; j < V; ++j)
+      v4[j] = make_float4(verts[3 * j], verts[3 * j + 1], verts[3 * j + 2], 0.0f);
+  }, "mvc vertices"));
   ctx->mvc_last_verts.assign(verts, verts + cnt);
   if (ctx->mvc_nb) ctx->deformed_valid = false;
   return CGS_OK;
@@ -965,7 +1015,7 @@ void field_changed(cgs_ctx* ctx) {
 // every slot, or (learned) the network for the slots whose residual on the
 // rest cage is at most `threshold` and exact weights for the others, which
 // are renumbered to come first.
-int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, uint32_t* out_bound,
+int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, bool cache, uint32_t* out_bound,
              uint32_t* out_fallback) {
   if (!ctx) return CGS_E_ARG;
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
@@ -1052,6 +1102,22 @@ int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, uint32_t* out_bound,
                                   cudaMemcpyDeviceToDevice, s);
           }
         }
+        if (learned && cache && e == cudaSuccess && rc == CGS_OK && nb > nfb) {
+          // codes of the learned slots, in their new order
+          rc = ctx->ensure(ctx->mvc_codes, (size_t)(nb - nfb) * 4 * kFieldHid * 2, "field codes");
+          if (rc == CGS_OK)
+            rc = ctx->ensure(ctx->mvc_code_pos, (size_t)(nb - nfb) * 16, "field code positions");
+          if (rc == CGS_OK) {
+            ctx->mvc_nb = nb;
+            ctx->mvc_nfb = nfb;
+            FieldInfer fi = ctx->field_infer_args(ctx->field.proj_rest.as<float>());
+            fi.codes = ctx->mvc_codes.as<__nv_bfloat16>();
+            fi.code_pos = ctx->mvc_code_pos.as<float4>();
+            e = launch_field_infer(fi, s);
+            ctx->mvc_nb = 0;
+            ctx->mvc_nfb = 0;
+          }
+        }
         if (e == cudaSuccess && rc == CGS_OK && nfb) {
           rc = ctx->ensure(ctx->mvc_wg, (size_t)nfb * ctx->mvc_V * 16, "mvc bindings");
           if (rc == CGS_OK)
@@ -1073,6 +1139,7 @@ int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, uint32_t* out_bound,
   }
   ctx->mvc_nb = nb;
   ctx->mvc_learned = learned;
+  ctx->mvc_cached = learned && cache;
   ctx->mvc_nfb = learned ? nfb : 0;
   ctx->deformed_valid = false;
   ctx->deform_generation++;
@@ -1093,12 +1160,14 @@ int field_check(cgs_ctx* ctx) {
 }  // namespace
 
 int cgs_mvc_bind(cgs_ctx* ctx, uint32_t* out_bound) {
-  return mvc_bind(ctx, false, 0.0f, out_bound, nullptr);
+  return mvc_bind(ctx, false, 0.0f, false, out_bound, nullptr);
 }
 
-int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t* out_bound,
+int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t flags, uint32_t* out_bound,
                          uint32_t* out_fallback) {
-  return mvc_bind(ctx, true, threshold, out_bound, out_fallback);
+  if (ctx && (flags & ~(uint32_t)CGS_FIELD_PER_FRAME))
+    return ctx->fail(CGS_E_ARG, "unknown field binding flags");
+  return mvc_bind(ctx, true, threshold, !(flags & CGS_FIELD_PER_FRAME), out_bound, out_fallback);
 }
 
 int cgs_mvc_field_create(cgs_ctx* ctx, uint64_t seed) {
@@ -1488,8 +1557,14 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
         ctx->kbegin(CGS_K_FIELD);
         CGS_CUDA(ctx->field.project(ctx->mvc_verts.as<float4>(), ctx->field.proj.as<float>(), s),
                  "field projection launch");
-        CGS_CUDA(launch_field_infer(ctx->field_infer_args(ctx->field.proj.as<float>()), s),
-                 "field inference launch");
+        FieldInfer fi = ctx->field_infer_args(ctx->field.proj.as<float>());
+        if (ctx->mvc_cached) {
+          fi.codes = ctx->mvc_codes.as<__nv_bfloat16>();
+          fi.code_pos = ctx->mvc_code_pos.as<float4>();
+          CGS_CUDA(launch_field_apply(fi, s), "field output layer launch");
+        } else {
+          CGS_CUDA(launch_field_infer(fi, s), "field inference launch");
+        }
         ctx->kend();
       }
     }

@@ -263,26 +263,74 @@ __global__ void k_mvc_compact(uint32_t n, const uint32_t* __restrict__ flag,
 // F = sum_j v_j grad(w_j)^T of every stored binding (MvcBindings::local_jacobian,
 // evaluate_position), vertex by vertex in order. xf[slot] = 3 float4:
 // (x, y, z, F00), (F10, F20, F01, F11), (F21, F02, F12, F22), F column-major.
-__global__ void __launch_bounds__(256) k_mvc_jacobian(uint32_t V, const float4* __restrict__ verts,
-                                                      uint32_t nb, const float4* __restrict__ wg,
-                                                      float4* __restrict__ xf) {
-  extern __shared__ float4 s_v[];
+//
+// One thread per slot. Each thread streams its own column of wg through a
+// kJacStages-deep ring of kJacChunk vertices in shared memory with cp.async
+// (16 bytes per vertex, the warp's copies of one vertex contiguous), so that
+// up to (kJacStages - 1) * kJacChunk copies per thread are in flight even
+// when there are only a few thousand slots; the sums stay sequential in j.
+// A thread reads only the ring entries it copied itself, and in-order issue
+// puts every read of a stage before the copy that refills it.
+constexpr int kJacThreads = 128, kJacChunk = 8, kJacStages = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(kJacThreads) k_mvc_jacobian(uint32_t V, const float4* __restrict__ verts,
+                                                              uint32_t nb, const float4* __restrict__ wg,
+                                                              float4* __restrict__ xf) {
+  extern __shared__ float4 s_v[];  // [V] vertices, then the ring
+  float4* ring = s_v + V;          // [kJacStages][kJacChunk][kJacThreads]
   for (uint32_t j = threadIdx.x; j < V; j += blockDim.x) s_v[j] = verts[j];
   __syncthreads();
   const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= nb) return;
+  const bool active = slot < nb;
+  const float4* row = wg + slot;
+  const uint32_t chunks = (V + kJacChunk - 1) / kJacChunk;
+  auto issue = [&](uint32_t c) {
+    if (active && c < chunks) {
+      float4* dst = ring + (size_t)(c % kJacStages) * kJacChunk * kJacThreads + threadIdx.x;
+#pragma unroll
+      for (int u = 0; u < kJacChunk; ++u) {
+        const uint32_t j = c * kJacChunk + u;
+        if (j < V) cp_async16(dst + u * kJacThreads, row + (size_t)j * nb);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int c = 0; c < kJacStages - 1; ++c) issue(c);
   float px = 0, py = 0, pz = 0, a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0, c0 = 0, c1 = 0,
         c2 = 0;
-  const float4* row = wg + slot;
-#pragma unroll 4
-  for (uint32_t j = 0; j < V; ++j) {
-    const float4 g = __ldcs(row + (size_t)j * nb);
-    const float4 v = s_v[j];
-    px = px + v.x * g.x; py = py + v.y * g.x; pz = pz + v.z * g.x;
-    a0 = a0 + v.x * g.y; a1 = a1 + v.y * g.y; a2 = a2 + v.z * g.y;
-    b0 = b0 + v.x * g.z; b1 = b1 + v.y * g.z; b2 = b2 + v.z * g.z;
-    c0 = c0 + v.x * g.w; c1 = c1 + v.y * g.w; c2 = c2 + v.z * g.w;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    issue(c + kJacStages - 1);
+    cp_async_wait<kJacStages - 1>();
+    if (!active) continue;
+    const float4* src = ring + (size_t)(c % kJacStages) * kJacChunk * kJacThreads + threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < kJacChunk; ++u) {
+      const uint32_t j = c * kJacChunk + u;
+      if (j < V) {
+        const float4 g = src[u * kJacThreads];
+        const float4 v = s_v[j];
+        px = px + v.x * g.x; py = py + v.y * g.x; pz = pz + v.z * g.x;
+        a0 = a0 + v.x * g.y; a1 = a1 + v.y * g.y; a2 = a2 + v.z * g.y;
+        b0 = b0 + v.x * g.z; b1 = b1 + v.y * g.z; b2 = b2 + v.z * g.z;
+        c0 = c0 + v.x * g.w; c1 = c1 + v.y * g.w; c2 = c2 + v.z * g.w;
+      }
+    }
   }
+  cp_async_wait<0>();
+  if (!active) return;
   xf[3 * (size_t)slot] = make_float4(px, py, pz, a0);
   xf[3 * (size_t)slot + 1] = make_float4(a1, a2, b0, b1);
   xf[3 * (size_t)slot + 2] = make_float4(b2, c0, c1, c2);
@@ -341,10 +389,11 @@ cudaError_t launch_mvc_bind_weights(const MvcCage& c, uint32_t nb, const uint32_
 cudaError_t launch_mvc_jacobian(uint32_t V, const float4* verts, uint32_t nb, const float4* wg,
                                 float4* xf, cudaStream_t s) {
   if (nb == 0) return cudaSuccess;
-  const size_t smem = (size_t)V * 16;
+  const size_t smem = (size_t)V * 16 + (size_t)kJacStages * kJacChunk * kJacThreads * 16;
   cudaError_t e = set_smem(k_mvc_jacobian, smem);
   if (e != cudaSuccess) return e;
-  k_mvc_jacobian<<<(nb + 255) / 256, 256, smem, s>>>(V, verts, nb, wg, xf);
+  k_mvc_jacobian<<<(nb + kJacThreads - 1) / kJacThreads, kJacThreads, smem, s>>>(V, verts, nb, wg,
+                                                                                   xf);
   return cudaGetLastError();
 }
 

@@ -317,13 +317,17 @@ class GpuPipelineState:
             return pos.cpu().numpy(), F.cpu().numpy()
         return pos, F
 
-    def mvc_bind_learned(self, threshold: float = 2e-3) -> tuple[int, int]:
-        """Binds the polygon cage with the network where its residual on the rest
-        cage is at most threshold (relative to the cage half-extent); returns
-        (bound, exact fallbacks)."""
+    def mvc_bind_learned(self, threshold: float, per_frame: bool = False) -> tuple[int, int]:
+        """Binds the polygon cage with the network where its linear-precision
+        residual on the rest cage is at most threshold (relative to the cage
+        half-extent); returns (bound, exact fallbacks). Frames apply the output
+        layer to codes kept per Gaussian, or evaluate the whole network every
+        frame with per_frame=True."""
         nb, nfb = ctypes.c_uint32(0), ctypes.c_uint32(0)
-        self._check(self._lib.cgs_mvc_bind_learned(self._ctx, float(threshold), ctypes.byref(nb),
-                                                   ctypes.byref(nfb)), "cgs_mvc_bind_learned")
+        flags = _abi.FIELD_PER_FRAME if per_frame else 0
+        self._check(self._lib.cgs_mvc_bind_learned(self._ctx, float(threshold), flags,
+                                                   ctypes.byref(nb), ctypes.byref(nfb)),
+                    "cgs_mvc_bind_learned")
         return int(nb.value), int(nfb.value)
 
     def _mvc_bound_hint(self) -> int:

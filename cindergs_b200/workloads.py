@@ -1,5 +1,11 @@
 """The benchmark workloads, built from seeded synthetic inputs.
 
+``mvc_cage_sphere`` is the polygon-cage workload: Gaussians drawn as in
+``random_scene`` with means uniform in the unit ball, a level-3 icosphere cage
+of radius 1.15 (642 vertices, 1280 triangles) displaced by a smooth random
+field of amplitude 0.1, deformed every frame by a moving smooth random field
+of amplitude 0.1, rendered at 1920 x 1080 by the orbiting camera.
+
 ``tet_cage_orbit`` is the tetrahedral-cage deform + render workload: Gaussians
 drawn as in ``random_scene`` with means scaled to fill [-1, 1]^3, a cage of
 5 x 5 x 5 cubes over [-1.1, 1.1]^3 split into 6 tets each (750 tets, 216
@@ -17,6 +23,7 @@ import numpy as np
 
 from .cage import Cage, CageScene, TetMesh
 from .camera import CameraUniforms, CompositorUniforms, orbit_camera
+from .mvc import PolyCageMesh
 from .scene import GaussianSceneSoa, random_scene
 
 f32 = np.float32
@@ -70,3 +77,69 @@ def tet_cage_orbit(n: int = 1_100_000, seed: int = 0, width: int = 1920, height:
     disp[sim.pinned] = 0.0
     sim.current_positions = (mesh.rest_vertices + disp).astype(f32)
     return CageOrbitWorkload(scene, cage, width, height, frames, 4.0)
+
+
+def ball_points(n: int, rng: np.random.Generator, radius: float = 1.0) -> np.ndarray:
+    """n points uniform in the ball of `radius` (direction from a normal
+    sample, radius from the cube root of a uniform)."""
+    d = rng.standard_normal((n, 3))
+    d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-12)
+    r = radius * rng.uniform(0.0, 1.0, n) ** (1.0 / 3.0)
+    return (d * r[:, None]).astype(f32)
+
+
+@dataclass
+class PolyCageWorkload:
+    scene: GaussianSceneSoa
+    cage: PolyCageMesh
+    width: int
+    height: int
+    frames: int
+    radius: float
+    amplitude: float
+    waves: np.ndarray       # [k, 3] wave vectors
+    phases: np.ndarray      # [k]
+    speeds: np.ndarray      # [k] phase change per frame
+    dirs: np.ndarray        # [k, 3] unit displacement directions
+    sh_degree: int = 3
+    background: tuple = (0.0, 0.0, 0.0, 1.0)
+
+    def camera(self, frame: int) -> CameraUniforms:
+        return orbit_camera(frame % self.frames, self.frames, self.radius, self.width,
+                            self.height, 60.0)
+
+    def compositor(self, cam: CameraUniforms) -> CompositorUniforms:
+        return CompositorUniforms(self.width, self.height, self.background,
+                                  tuple(float(x) for x in cam.eye()), self.sh_degree)
+
+    def vertices(self, frame: int) -> np.ndarray:
+        """Cage vertices of a frame: rest + sum_k dir_k sin(k_k . v + phase_k +
+        speed_k frame), scaled so the largest displacement is `amplitude`."""
+        v = self.cage.rest_vertices.astype(np.float64)
+        s = np.sin(v @ self.waves.T + self.phases[None, :] + self.speeds[None, :] * frame)
+        d = s @ self.dirs
+        d *= self.amplitude / max(np.linalg.norm(d, axis=1).max(), 1e-12)
+        return (v + d).astype(f32)
+
+    def training_points(self, n: int, seed: int = 1) -> np.ndarray:
+        """Interior training points: uniform in the unit ball (where the
+        Gaussians are)."""
+        return ball_points(n, np.random.Generator(np.random.PCG64(seed)))
+
+
+def mvc_cage_sphere(n: int = 3_000_000, seed: int = 0, width: int = 1920, height: int = 1080,
+                    frames: int = 120) -> PolyCageWorkload:
+    scene = random_scene(n, seed=seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    scene.positions[:] = ball_points(n, rng)
+    cage = PolyCageMesh.icosphere([0.0, 0.0, 0.0], 1.15, 3).displace_sinusoids(0.1, 8, seed=seed)
+    k = 8
+    dirs = rng.standard_normal((k, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    waves = dirs * rng.uniform(2.0, 4.0, (k, 1))
+    disp = rng.standard_normal((k, 3))
+    disp /= np.linalg.norm(disp, axis=1, keepdims=True)
+    return PolyCageWorkload(scene=scene, cage=cage, width=width, height=height, frames=frames,
+                            radius=4.0, amplitude=0.1, waves=waves,
+                            phases=rng.uniform(0.0, 2.0 * np.pi, k),
+                            speeds=rng.uniform(0.02, 0.06, k), dirs=disp)

@@ -238,8 +238,15 @@ int cgs_mvc_field_infer(cgs_ctx* ctx, uint64_t n, const float* d_points, int32_t
 /* As cgs_mvc_bind, with the network for every bound Gaussian whose
  * linear-precision residual |r| / s is at most `threshold`; the others get
  * exact stored weights (fallbacks, listed first by cgs_mvc_read_bindings).
- * *out_bound and *out_fallback (either may be NULL) receive both counts. */
-int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t* out_bound,
+ * The network's last hidden layer and its three tangents depend only on the
+ * rest position, so by default they are evaluated here and kept (bf16, 1 KB
+ * per Gaussian) and frames apply only the output layer folded with the
+ * current vertices; with CGS_FIELD_PER_FRAME frames evaluate the whole
+ * network instead and nothing is stored per Gaussian. Both give the same
+ * result up to summation order. *out_bound and *out_fallback (either may be
+ * NULL) receive both counts. */
+#define CGS_FIELD_PER_FRAME 1u
+int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t flags, uint32_t* out_bound,
                          uint32_t* out_fallback);
 
 /* ---- frame (GpuPipelineState, render/gpu_state.rs:538-1243) ---- */

@@ -202,9 +202,18 @@ def test_learned_bindings_in_the_frame(fst, trained):
     raw, _ = st.mvc_field_infer(scene.positions[gall], rest=True)
     res = np.linalg.norm(raw - scene.positions[gall], axis=1) / s
     thr = float(np.quantile(res, 0.9))
-    nb, nfb = st.mvc_bind_learned(threshold=thr)
+    nb, nfb = st.mvc_bind_learned(threshold=thr, per_frame=True)
     assert nb == nb_exact and abs(nfb - int((res > thr).sum())) <= 2, (nfb, (res > thr).sum())
+    pos3, cov3 = frame_positions(st, scene)
+    # default: codes kept per Gaussian, output layer per frame -- the same
+    # deformation up to summation order
+    nb, nfb2 = st.mvc_bind_learned(threshold=thr)
+    assert nfb2 == nfb
     pos2, cov2 = frame_positions(st, scene)
+    d = np.linalg.norm(pos2 - pos3, axis=1) / s
+    assert d.max() < 1e-6, d.max()
+    cs = np.abs(cov3).max(axis=1, keepdims=True) + 1e-30
+    assert (np.abs(cov2 - cov3) / cs).max() < 1e-5
     gidx, _ = st.mvc_read_bindings()
     assert len(gidx) == nfb
     np.testing.assert_array_equal(pos2[gidx], pos_e[gidx])
