@@ -90,6 +90,11 @@ KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "entry_so
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 
+class CgsViewsStats(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double), ("total_tile_entries", _u64), ("graph_replayed", _u32),
+                ("graph_captured", _u32), ("views_rerendered", _u32), ("pad", _u32)]
+
+
 class CgsKernelProfile(ctypes.Structure):
     _fields_ = [("ms", ctypes.c_double * KERNEL_COUNT), ("alg_bytes", _u64 * KERNEL_COUNT),
                 ("launches", _u32 * KERNEL_COUNT), ("alg_flops", _u64 * KERNEL_COUNT)]
@@ -126,6 +131,8 @@ SIGNATURES = {
     "cgs_mvc_bind": (_i32, [_vp, ctypes.POINTER(_u32)]),
     "cgs_mvc_weights": (_i32, [_vp, _u64, _vp, _vp]),
     "cgs_mvc_read_bindings": (_i32, [_vp, _u64, _vp, _vp, ctypes.POINTER(_u64)]),
+    "cgs_execute_views": (_i32, [_vp, _u32, _vp, _vp, ctypes.POINTER(CgsFrameParams), _vp, _i32,
+                                 ctypes.POINTER(CgsViewsStats)]),
     "cgs_mvc_field_create": (_i32, [_vp, _u64]),
     "cgs_mvc_field_layout": (_i32, [_vp, _vp, _vp, _vp]),
     "cgs_mvc_field_params": (_i32, [_vp, _vp, _vp]),

@@ -314,6 +314,10 @@ struct SortArgs {
   uint32_t* tile_ctr;    // [passes] zeroed
   uint32_t* status_word;
   int src;               // index of the buffer holding the input
+  // bit p: pass p finds the lanes sharing a digit with one ballot per digit
+  // bit (a fixed cost) instead of __match_any_sync (cheap when a warp's keys
+  // share few digits, expensive when they are all different)
+  uint32_t ballot_mask = ~0u;
 };
 // Runs the passes; returns in *out_src the index of the buffer with the result.
 cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s);

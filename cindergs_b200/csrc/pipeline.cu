@@ -80,6 +80,8 @@ struct FrameDesc {
   uint32_t tile_bits = 0, depth_bits = 0, sort_bits = 0, radix_bits = 8, depth_base_bits = 0;
   int entry_sort = CGS_SORT_AUTO;
   float bg[4] = {0, 0, 0, 1};
+  uint32_t* out_rgba8 = nullptr;  // Stage 4 target when not the context's framebuffer
+  uint32_t out_pitch = 0;         // its row pitch in pixels
 };
 
 // Per-frame counters copied to pinned host memory at the end of the frame.
@@ -203,6 +205,16 @@ struct cgs_ctx {
   uint32_t radix_lb_bits = 0;
   int radix_parity = 0;
   HostCounters* h_ring = nullptr;  // pinned [kRing]
+  // Buffer reallocations and state changes (uploads, bindings), for the
+  // validity of captured graphs, which hold device pointers and launch shapes.
+  uint64_t alloc_epoch = 0, state_epoch = 0;
+  // multi-view steps (cgs_execute_views)
+  HostCounters* h_views = nullptr;  // pinned [views_cap]
+  uint32_t views_cap = 0;
+  cudaGraphExec_t views_exec = nullptr;
+  std::vector<unsigned char> views_key;
+  int views_radix_parity = 0, views_splat_parity = 0;  // host parities after a replay
+  cudaEvent_t views_ev[2] = {};
   // Pinned staging of the per-frame uploads (cage vertices): a copy from
   // pageable memory synchronises the stream before it starts, one from a
   // pinned slot is enqueued behind the frames in flight. A slot is refilled
@@ -277,6 +289,7 @@ struct cgs_ctx {
       b.p = nullptr;
       b.cap = 0;
     }
+    ++alloc_epoch;
     cudaError_t e = cudaMalloc(&b.p, nb);
     if (e != cudaSuccess) {
       b.p = nullptr;
@@ -532,9 +545,9 @@ int enqueue_stage4(cgs_ctx* ctx, const FrameDesc& d, int result_src) {
   c.height = d.H;
   c.tiles_x = d.tiles_x;
   c.tiles_y = d.tiles_y;
-  c.pitch_px = d.pitch;
+  c.pitch_px = d.out_rgba8 ? d.out_pitch : d.pitch;
   std::memcpy(c.bg, d.bg, 16);
-  c.out_rgba8 = ctx->fb_rgba8.as<uint32_t>();
+  c.out_rgba8 = d.out_rgba8 ? d.out_rgba8 : ctx->fb_rgba8.as<uint32_t>();
   c.out_f32 = d.write_f32 ? ctx->fb_f32.as<float4>() : nullptr;
   c.fc = (FrameCounters*)sc;
   c.num_recs = d.max_n ? d.max_n : 1u;
@@ -776,6 +789,10 @@ int cgs_ctx_destroy(cgs_ctx* ctx) {
     if (ctx->up.p[k]) cudaFreeHost(ctx->up.p[k]);
     if (ctx->up.ev[k]) cudaEventDestroy(ctx->up.ev[k]);
   }
+  if (ctx->views_exec) cudaGraphExecDestroy(ctx->views_exec);
+  if (ctx->h_views) cudaFreeHost(ctx->h_views);
+  for (auto& e : ctx->views_ev)
+    if (e) cudaEventDestroy(e);
   cudaStream_t s = ctx->stream;
   bool own = ctx->own_stream;
   delete ctx;
@@ -812,6 +829,7 @@ int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out) {
 
 int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* cov,
                      const float* opa, const void* sh, int32_t sh_format) {
+  if (ctx) ++ctx->state_epoch;
   if (!ctx) return CGS_E_ARG;
   if (sh_format != CGS_SH_F32 && sh_format != CGS_SH_F16)
     return ctx->fail(CGS_E_ARG, "sh_format must be CGS_SH_F32 or CGS_SH_F16");
@@ -861,6 +879,7 @@ int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* co
 int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
                          const float* inv_dm, uint32_t num_verts, const uint32_t* bind_tet,
                          const float* bind_w) {
+  if (ctx) ++ctx->state_epoch;
   if (!ctx) return CGS_E_ARG;
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "upload the scene before the cages");
   cudaSetDevice(ctx->device);
@@ -922,6 +941,7 @@ int cgs_cage_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_vert
 
 int cgs_mvc_cage_upload(cgs_ctx* ctx, uint32_t V, const float* rest, uint32_t F,
                         const uint32_t* tris) {
+  if (ctx) ++ctx->state_epoch;
   if (!ctx || !rest || !tris) return CGS_E_ARG;
   if (V < 4 || F < 4) return ctx->fail(CGS_E_ARG, "a polygon cage needs at least 4 vertices and 4 triangles");
   if (!mvc_cage_fits(V, F)) return ctx->fail(CGS_E_CAPACITY, "polygon cage too large (1,024 vertices, 12,800 vertices + triangles)");
@@ -1003,6 +1023,7 @@ namespace {
 // network drops them (the Gaussians fall back to their rest pose until bound
 // again).
 void field_changed(cgs_ctx* ctx) {
+  ++ctx->state_epoch;
   if (!ctx->mvc_learned) return;
   ctx->mvc_unbind();
   ctx->deformed_valid = false;
@@ -1018,6 +1039,7 @@ void field_changed(cgs_ctx* ctx) {
 int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, bool cache, uint32_t* out_bound,
              uint32_t* out_fallback) {
   if (!ctx) return CGS_E_ARG;
+  ++ctx->state_epoch;
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
   if (!ctx->mvc_ready) return ctx->fail(CGS_E_STATE, "no polygon cage uploaded");
   if (learned && !ctx->field_ready) return ctx->fail(CGS_E_STATE, "no learned field created");
@@ -1348,6 +1370,7 @@ int cgs_mvc_read_bindings(cgs_ctx* ctx, uint64_t max_slots, uint32_t* gaussian, 
 int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const float* inv_dm,
                   uint32_t num_verts, const float* rest_verts, int32_t use_bounds,
                   const float* bmin, const float* bmax, uint32_t* bind_tet, float* bind_w) {
+  if (ctx) ++ctx->state_epoch;
   if (!ctx || !elems || !inv_dm || !rest_verts || !bind_tet || !bind_w) return CGS_E_ARG;
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "upload the scene before binding");
   if (use_bounds && (!bmin || !bmax)) return ctx->fail(CGS_E_ARG, "bounds requested but null");
@@ -1394,8 +1417,25 @@ int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const 
   return CGS_OK;
 }
 
-int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
-                      const cgs_frame_params* params, cgs_stage_timings* timings) {
+namespace {
+
+// How a frame is enqueued (cgs_execute_frame, cgs_execute_views).
+struct FrameCtl {
+  bool allow_cache = true;     // may reuse the cached Stage 3 lists
+  bool force_stage1 = false;   // deform even when the deformed scene is current
+  HostCounters* counters = nullptr;  // pinned destination of the frame's counters
+  cudaEvent_t done = nullptr;        // recorded after the frame, if set
+  uint32_t* out_rgba8 = nullptr;     // Stage 4 target (else the context's framebuffer)
+  uint32_t out_pitch = 0;            // its row pitch in pixels
+};
+struct FrameInfo {
+  FrameDesc d;
+  bool cached = false, need_deform = false;
+  uint32_t passes = 0, splat_passes = 0, bin_launches = 0, sort_launches = 0;
+};
+
+int check_frame_args(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
+                     const cgs_frame_params* params) {
   if (!ctx || !camera || !comp || !params) return CGS_E_ARG;
   if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
   if (ctx->has_cages && !ctx->verts_uploaded)
@@ -1404,9 +1444,6 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     return ctx->fail(CGS_E_ARG, "radix_bits must be 0 or 4..8");
   if (params->entry_sort < CGS_SORT_AUTO || params->entry_sort > CGS_SORT_TRANSPOSE)
     return ctx->fail(CGS_E_ARG, "entry_sort must be one of CGS_SORT_*");
-  cudaSetDevice(ctx->device);
-  cudaStream_t s = ctx->stream;
-  cgs_stage_timings tm{};
   const uint32_t W = comp->screen_width ? comp->screen_width : 1u;
   const uint32_t H = comp->screen_height ? comp->screen_height : 1u;
   const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
@@ -1414,13 +1451,19 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   if (total_tiles64 > 0xFFFFFFFFull / 2) return ctx->fail(CGS_E_CAPACITY, "viewport too large");
   if (W >= (1u << 22) || H >= (1u << 22))
     return ctx->fail(CGS_E_CAPACITY, "viewport wider or taller than 4,194,303 pixels");
+  return CGS_OK;
+}
 
-  // Take a ring slot; the frame that used it last is checked first.
-  const int slot = ctx->next_slot;
-  CGS_TRY(check_slot(ctx, slot, true));
-  CGS_TRY(drain(ctx, false));
-  ctx->next_slot = (slot + 1) % kRing;
-
+// Enqueues one frame (Stages 1-4) on the context's stream without waiting
+// for anything: buffers are grown here, so a frame being captured into a
+// graph must find them large enough already.
+int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
+                  const cgs_frame_params* params, const FrameCtl& ctl, FrameInfo* fi) {
+  cudaStream_t s = ctx->stream;
+  const uint32_t W = comp->screen_width ? comp->screen_width : 1u;
+  const uint32_t H = comp->screen_height ? comp->screen_height : 1u;
+  const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+  const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
   FrameDesc d;
   d.W = W;
   d.H = H;
@@ -1433,9 +1476,13 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   d.write_f32 = params->write_f32 != 0;
   std::memcpy(d.bg, comp->background, 16);
   if (W != ctx->last_w || H != ctx->last_h) ctx->s3_valid = false;
-  const bool prof = params->profile_stages != 0;
 
-  CGS_TRY(ctx->ensure(ctx->fb_rgba8, (size_t)d.pitch * H * 4, "framebuffer"));
+  if (ctl.out_rgba8) {
+    d.out_rgba8 = ctl.out_rgba8;
+    d.out_pitch = ctl.out_pitch;
+  } else {
+    CGS_TRY(ctx->ensure(ctx->fb_rgba8, (size_t)d.pitch * H * 4, "framebuffer"));
+  }
   if (d.write_f32) CGS_TRY(ctx->ensure(ctx->fb_f32, (size_t)W * H * 16, "f32 framebuffer"));
 
   const uint32_t n = ctx->n;
@@ -1443,7 +1490,8 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   const bool deform_on = ctx->deform_on();  // tet and/or polygon cage bindings
   const uint32_t split_bits = fbits(params->strain_split_threshold), mip_bits = fbits(params->mip_filter_3d_var);
   const bool params_changed = split_bits != ctx->last_split_bits || mip_bits != ctx->last_mip_bits;
-  const bool need_deform = deform_on && (!ctx->deformed_valid || params_changed);
+  const bool need_deform =
+      deform_on && (ctl.force_stage1 || !ctx->deformed_valid || params_changed);
   d.n = n;
   d.split_possible = deform_on && params->strain_split_threshold > 0.0f;
   d.max_n = d.split_possible ? 2 * n : n;
@@ -1497,7 +1545,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   key.min_opa = fbits(params->min_opacity);
   key.min_rad = fbits(params->min_radius_px);
   key.radix_bits = d.radix_bits | ((uint32_t)d.entry_sort << 8);
-  bool cached = !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
+  bool cached = ctl.allow_cache && !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
   if (cached) {
     CGS_TRY(drain(ctx, true));
     cached = ctx->s3_valid && ctx->s3_key == key;
@@ -1509,10 +1557,6 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     CGS_TRY(ensure_splat_buffers(ctx, mn));
   }
 
-  cgs_ctx::Pending& P = ctx->ring[slot];
-  P.kcount = 0;
-  ctx->kprof = prof;
-  ctx->cur = slot;
   ctx->kbegin(CGS_K_CLEAR);
   CGS_CUDA(cudaMemsetAsync(sc, 0, L.bytes, s), "clear frame scratch");
   ctx->kend();
@@ -1637,11 +1681,54 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
     ctx->s3_depth_bits = d.depth_bits;
   }
   CGS_TRY(enqueue_stage4(ctx, d, src));
-  CGS_CUDA(cudaMemcpyAsync(&ctx->h_ring[slot].fc, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s),
+  CGS_CUDA(cudaMemcpyAsync(&ctl.counters->fc, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s),
            "read counters");
-  CGS_CUDA(cudaMemcpyAsync(&ctx->h_ring[slot].split, d_split, 4, cudaMemcpyDeviceToHost, s),
+  CGS_CUDA(cudaMemcpyAsync(&ctl.counters->split, d_split, 4, cudaMemcpyDeviceToHost, s),
            "read split count");
-  CGS_CUDA(cudaEventRecord(P.done, s), "frame event");
+  if (ctl.done) CGS_CUDA(cudaEventRecord(ctl.done, s), "frame event");
+  fi->d = d;
+  fi->cached = cached;
+  fi->need_deform = need_deform;
+  fi->passes = passes;
+  fi->splat_passes = splat_passes;
+  fi->bin_launches = bin_launches;
+  fi->sort_launches = sort_launches;
+  return CGS_OK;
+}
+
+}  // namespace
+
+int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
+                      const cgs_frame_params* params, cgs_stage_timings* timings) {
+  CGS_TRY(check_frame_args(ctx, camera, comp, params));
+  cudaSetDevice(ctx->device);
+  cgs_stage_timings tm{};
+  const bool prof = params->profile_stages != 0;
+
+  // Take a ring slot; the frame that used it last is checked first.
+  const int slot = ctx->next_slot;
+  CGS_TRY(check_slot(ctx, slot, true));
+  CGS_TRY(drain(ctx, false));
+  ctx->next_slot = (slot + 1) % kRing;
+
+  cgs_ctx::Pending& P = ctx->ring[slot];
+  P.kcount = 0;
+  ctx->kprof = prof;
+  ctx->cur = slot;
+  FrameCtl ctl;
+  ctl.counters = &ctx->h_ring[slot];
+  ctl.done = P.done;
+  FrameInfo fi;
+  const int rc = enqueue_frame(ctx, camera, comp, params, ctl, &fi);
+  if (rc != CGS_OK) {
+    ctx->cur = -1;
+    return rc;
+  }
+  const FrameDesc& d = fi.d;
+  const bool cached = fi.cached, need_deform = fi.need_deform;
+  const uint32_t n = d.n, W = d.W, H = d.H;
+  const uint32_t passes = fi.passes, splat_passes = fi.splat_passes;
+  const uint32_t bin_launches = fi.bin_launches, sort_launches = fi.sort_launches;
   P.used = true;
   P.stage3_ran = !cached;
   P.profiled = prof;
@@ -1698,6 +1785,225 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   return CGS_OK;
 }
 
+namespace {
+
+// Reads the views' counters after the step has completed: bounded waits that
+// gave up are errors; views whose entries exceeded the key buffers are
+// listed (the capacity is grown for them and kept 30% above the largest
+// count).
+int check_views(cgs_ctx* ctx, uint32_t nv, const uint32_t* cap_used,
+                std::vector<uint32_t>* overflowed, uint64_t* total_entries) {
+  uint32_t most = 0;
+  *total_entries = 0;
+  overflowed->clear();
+  for (uint32_t v = 0; v < nv; ++v) {
+    const FrameCounters& fc = ctx->h_views[v].fc;
+    if (fc.status & (kStatusLookbackTimeout | kStatusBarrierTimeout))
+      return ctx->fail(CGS_E_TIMEOUT, "a bounded device-side wait gave up during a view");
+    if ((fc.status & kStatusCapacity) || fc.entries > cap_used[v]) overflowed->push_back(v);
+    most = std::max(most, fc.entries);
+    *total_entries += fc.entries;
+  }
+  if (most > ctx->entry_cap / 10 * 8)
+    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)most * 13 / 10 + 4096, 0x3FFFFFFFull);
+  return CGS_OK;
+}
+
+int enqueue_view(cgs_ctx* ctx, const cgs_camera* cam, const cgs_compositor* comp,
+                 const cgs_frame_params* params, uint32_t v, uint32_t* out, bool force_stage1,
+                 uint32_t* cap_used) {
+  FrameCtl ctl;
+  ctl.allow_cache = false;
+  ctl.force_stage1 = force_stage1;
+  ctl.counters = &ctx->h_views[v];
+  ctl.out_rgba8 = out;
+  ctl.out_pitch = comp->screen_width ? comp->screen_width : 1u;
+  FrameInfo fi;
+  CGS_TRY(enqueue_frame(ctx, cam, comp, params, ctl, &fi));
+  *cap_used = ctx->entry_cap;
+  return CGS_OK;
+}
+
+// The views one by one (each view's launches issued from the host), then a
+// wait and the counter check; overflowed views are rendered again with grown
+// buffers.
+int views_eager(cgs_ctx* ctx, uint32_t nv, const cgs_camera* cams, const cgs_compositor* comps,
+                const cgs_frame_params* params, uint32_t* const* outs, uint32_t* rerendered,
+                uint64_t* entries) {
+  std::vector<uint32_t> cap(nv), over;
+  for (uint32_t v = 0; v < nv; ++v)
+    CGS_TRY(enqueue_view(ctx, &cams[v], &comps[v], params, v, outs[v], false, &cap[v]));
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "views");
+  CGS_TRY(check_views(ctx, nv, cap.data(), &over, entries));
+  for (int round = 0; !over.empty() && round < 3; ++round) {
+    for (uint32_t v : over) {
+      CGS_TRY(enqueue_view(ctx, &cams[v], &comps[v], params, v, outs[v], false, &cap[v]));
+      ++*rerendered;
+    }
+    CGS_CUDA(cudaStreamSynchronize(ctx->stream), "views");
+    CGS_TRY(check_views(ctx, nv, cap.data(), &over, entries));
+  }
+  if (!over.empty()) return ctx->fail(CGS_E_CAPACITY, "tile entries kept exceeding the key buffers");
+  return CGS_OK;
+}
+
+void drop_views_graph(cgs_ctx* ctx) {
+  if (ctx->views_exec) cudaGraphExecDestroy(ctx->views_exec);
+  ctx->views_exec = nullptr;
+  ctx->views_key.clear();
+}
+
+void put_bytes(std::vector<unsigned char>& k, const void* p, size_t bytes) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  k.insert(k.end(), b, b + bytes);
+}
+
+// Captures the step (Stage 1 of the first view, then every view) into a
+// graph. The look-back buffers of both radix sorts are cleared at its start,
+// so a replay does not depend on the alternation state the previous work
+// left behind.
+int capture_views(cgs_ctx* ctx, uint32_t nv, const cgs_camera* cams, const cgs_compositor* comps,
+                  const cgs_frame_params* params, uint32_t* const* outs) {
+  cudaStream_t s = ctx->stream;
+  drop_views_graph(ctx);
+  std::vector<uint32_t> cap(nv);
+  cudaGraph_t g = nullptr;
+  CGS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "begin capture");
+  int rc = CGS_OK;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+    if (ctx->radix_lb[k].p) e = cudaMemsetAsync(ctx->radix_lb[k].p, 0, ctx->radix_lb[k].cap, s);
+    if (e == cudaSuccess && ctx->splat_lb[k].p)
+      e = cudaMemsetAsync(ctx->splat_lb[k].p, 0, ctx->splat_lb[k].cap, s);
+  }
+  ctx->radix_parity = 0;
+  ctx->splat_parity = 0;
+  const uint64_t epoch = ctx->alloc_epoch;
+  for (uint32_t v = 0; v < nv && rc == CGS_OK && e == cudaSuccess; ++v)
+    rc = enqueue_view(ctx, &cams[v], &comps[v], params, v, outs[v], v == 0 && ctx->deform_on(),
+                      &cap[v]);
+  const cudaError_t ee = cudaStreamEndCapture(s, &g);
+  if (e == cudaSuccess) e = ee;
+  if (rc == CGS_OK && e == cudaSuccess && ctx->alloc_epoch != epoch)
+    rc = ctx->fail(CGS_E_STATE, "buffers grew while capturing the views");
+  if (rc == CGS_OK && e == cudaSuccess) e = cudaGraphInstantiate(&ctx->views_exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  // Both look-back pairs clean again for whatever runs next, eagerly or as
+  // the graph (nothing captured has run yet).
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->radix_lb[k].p) cudaMemsetAsync(ctx->radix_lb[k].p, 0, ctx->radix_lb[k].cap, s);
+    if (ctx->splat_lb[k].p) cudaMemsetAsync(ctx->splat_lb[k].p, 0, ctx->splat_lb[k].cap, s);
+  }
+  ctx->views_radix_parity = ctx->radix_parity;
+  ctx->views_splat_parity = ctx->splat_parity;
+  if (rc != CGS_OK || e != cudaSuccess) {
+    ctx->views_exec = nullptr;
+    return rc != CGS_OK ? rc : ctx->cuda_fail(e, "views capture");
+  }
+  return CGS_OK;
+}
+
+}  // namespace
+
+int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* cameras,
+                      const cgs_compositor* comps, const cgs_frame_params* params,
+                      uint32_t* const* d_rgba8, int32_t use_graph, cgs_views_stats* stats) {
+  if (!ctx || !params || (num_views && (!cameras || !comps || !d_rgba8))) return CGS_E_ARG;
+  for (uint32_t v = 0; v < num_views; ++v) {
+    CGS_TRY(check_frame_args(ctx, &cameras[v], &comps[v], params));
+    if (!d_rgba8[v] || ((uintptr_t)d_rgba8[v] & 3)) return ctx->fail(CGS_E_ARG, "view image pointer");
+  }
+  cgs_views_stats st{};
+  if (num_views == 0) {
+    if (stats) *stats = st;
+    return CGS_OK;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  CGS_TRY(drain(ctx, true));
+  CGS_TRY(ctx->take_sticky());
+  if (num_views > ctx->views_cap) {
+    if (ctx->h_views) cudaFreeHost(ctx->h_views);
+    ctx->h_views = nullptr;
+    ctx->views_cap = 0;
+    CGS_CUDA(cudaHostAlloc((void**)&ctx->h_views, (size_t)num_views * sizeof(HostCounters),
+                           cudaHostAllocDefault), "view counters");
+    ctx->views_cap = num_views;
+    drop_views_graph(ctx);  // it wrote the old counters
+  }
+  for (auto& ev : ctx->views_ev)
+    if (!ev) CGS_CUDA(cudaEventCreate(&ev), "views event");
+  cgs_frame_params prm = *params;
+  prm.profile_stages = 0;
+  prm.write_f32 = 0;
+  prm.force_stage3 = 1;
+  ctx->kprof = false;
+  ctx->cur = -1;
+
+  auto key_of = [&]() {
+    std::vector<unsigned char> k;
+    put_bytes(k, &num_views, sizeof(num_views));
+    put_bytes(k, cameras, num_views * sizeof(cgs_camera));
+    put_bytes(k, comps, num_views * sizeof(cgs_compositor));
+    put_bytes(k, &prm, sizeof(prm));
+    put_bytes(k, d_rgba8, num_views * sizeof(uint32_t*));
+    put_bytes(k, &ctx->alloc_epoch, sizeof(ctx->alloc_epoch));
+    put_bytes(k, &ctx->state_epoch, sizeof(ctx->state_epoch));
+    put_bytes(k, &ctx->entry_cap, sizeof(ctx->entry_cap));
+    return k;
+  };
+  CGS_CUDA(cudaEventRecord(ctx->views_ev[0], s), "views event");
+  if (use_graph && ctx->views_exec && ctx->views_key == key_of()) {
+    CGS_CUDA(cudaGraphLaunch(ctx->views_exec, s), "views graph launch");
+    CGS_CUDA(cudaEventRecord(ctx->views_ev[1], s), "views event");
+    CGS_CUDA(cudaStreamSynchronize(s), "views");
+    ctx->radix_parity = ctx->views_radix_parity;
+    ctx->splat_parity = ctx->views_splat_parity;
+    st.graph_replayed = 1;
+    std::vector<uint32_t> cap(num_views, ctx->entry_cap), over;
+    const uint32_t cap_before = ctx->entry_cap;
+    CGS_TRY(check_views(ctx, num_views, cap.data(), &over, &st.total_tile_entries));
+    if (!over.empty()) {
+      // render the overflowed views again eagerly; the graph is rebuilt on
+      // the next call (its capacity no longer matches)
+      for (uint32_t v : over) {
+        CGS_TRY(enqueue_view(ctx, &cameras[v], &comps[v], &prm, v, d_rgba8[v], false, &cap[v]));
+        ++st.views_rerendered;
+      }
+      CGS_CUDA(cudaStreamSynchronize(s), "views");
+      CGS_TRY(check_views(ctx, num_views, cap.data(), &over, &st.total_tile_entries));
+      if (!over.empty()) return ctx->fail(CGS_E_CAPACITY, "tile entries exceeded the key buffers");
+    }
+    if (ctx->entry_cap != cap_before) drop_views_graph(ctx);
+  } else {
+    CGS_TRY(views_eager(ctx, num_views, cameras, comps, &prm, d_rgba8, &st.views_rerendered,
+                        &st.total_tile_entries));
+    CGS_CUDA(cudaEventRecord(ctx->views_ev[1], s), "views event");
+    if (use_graph) {
+      // grow the key buffers to the capacity the graph will be captured with
+      bool key64 = false;
+      for (uint32_t v = 0; v < num_views; ++v)
+        key64 = key64 || (uint64_t)((comps[v].screen_width + 15) / 16) *
+                                 ((comps[v].screen_height + 15) / 16) > 65535u;
+      CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, key64, ctx->radix_lb_bits ? ctx->radix_lb_bits : 8));
+      CGS_TRY(capture_views(ctx, num_views, cameras, comps, &prm, d_rgba8));
+      ctx->views_key = key_of();
+      st.graph_captured = 1;
+    }
+    CGS_CUDA(cudaStreamSynchronize(s), "views");
+  }
+  float ms = 0.0f;
+  CGS_CUDA(cudaEventElapsedTime(&ms, ctx->views_ev[0], ctx->views_ev[1]), "views time");
+  st.ms = ms;
+  // The deformed scene is current; Stage 3 lists and the framebuffer belong
+  // to no single frame.
+  ctx->deformed_valid = ctx->deform_on();
+  ctx->s3_valid = false;
+  ctx->frame_done = false;
+  if (stats) *stats = st;
+  return CGS_OK;
+}
+
 int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height) {
   if (!ctx || !dst) return CGS_E_ARG;
   if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
@@ -1740,6 +2046,7 @@ int cgs_invalidate_stage3(cgs_ctx* ctx) {
 }
 
 int cgs_invalidate(cgs_ctx* ctx) {
+  if (ctx) ++ctx->state_epoch;
   if (!ctx) return CGS_E_ARG;
   ctx->s3_valid = false;
   ctx->scene_ready = false;

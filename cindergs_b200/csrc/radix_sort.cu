@@ -28,6 +28,11 @@ namespace {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // 4096
+// Reorder buffers hold one padding word per 32 keys: the lanes of a warp
+// whose keys fall in different digits write positions about one digit run
+// (~32 keys) apart, which without padding map to the same bank.
+constexpr uint32_t kSortTileP = kSortTile + kSortTile / 32;
+__device__ __forceinline__ uint32_t padded(uint32_t i) { return i + (i >> 5); }
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
@@ -49,16 +54,17 @@ struct PassArgs {
   uint32_t grid_tiles;     // tiles covered by the grid (all of clear_next)
   uint32_t* tile_ctr;
   uint32_t* status_word;
+  uint32_t ballot;         // 1: peers from per-bit ballots, 0: __match_any_sync
 };
 
 template <int RB, bool PAY2>
 __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const PassArgs a) {
   constexpr uint32_t R = 1u << RB;
   extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t* s_keys = smem;                       // [kSortTile]
-  uint32_t* s_v0 = s_keys + kSortTile;           // [kSortTile]
-  uint32_t* s_v1 = s_v0 + kSortTile;             // [kSortTile] (PAY2)
-  uint32_t* s_whist = s_v0 + (PAY2 ? 2 : 1) * kSortTile;  // [8][R]
+  uint32_t* s_keys = smem;                       // [kSortTileP]
+  uint32_t* s_v0 = s_keys + kSortTileP;          // [kSortTileP]
+  uint32_t* s_v1 = s_v0 + kSortTileP;            // [kSortTileP] (PAY2)
+  uint32_t* s_whist = s_v0 + (PAY2 ? 2 : 1) * kSortTileP;  // [8][R]
   uint32_t* s_tstart = s_whist + 8 * R;          // [R]
   uint32_t* s_goff = s_tstart + R;               // [R]
   uint32_t* s_misc = s_goff + R;                 // [40]: tile, warp sums
@@ -109,7 +115,17 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t d = (k[j] >> a.shift) & a.dmask;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t peers;
+    if (a.ballot) {
+      peers = 0xffffffffu;
+#pragma unroll
+      for (int b = 0; b < RB; ++b) {
+        const uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? m : ~m;
+      }
+    } else {
+      peers = __match_any_sync(0xffffffffu, d);
+    }
     const int leader = 31 - __clz(peers);
     uint32_t old = 0;
     if (lane == leader) old = atomicAdd(&wh[d], (uint32_t)__popc(peers));
@@ -172,7 +188,8 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t d = (k[j] >> a.shift) & a.dmask;
-    const uint32_t pos = s_tstart[d] + wh[d] + ((rk[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
+    const uint32_t pos =
+        padded(s_tstart[d] + wh[d] + ((rk[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu));
     s_keys[pos] = k[j];
     s_v0[pos] = v0[j];
     if (PAY2) s_v1[pos] = v1[j];
@@ -184,15 +201,15 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t i = tid + kSortThreads * j;
     if (!full && i >= tile_valid) break;
-    const uint32_t key = s_keys[i];
+    const uint32_t key = s_keys[padded(i)];
     const uint32_t g = s_goff[(key >> a.shift) & a.dmask] + i;
     if (g >= n) {  // inconsistent histogram: report instead of writing out of bounds
       bad = true;
       continue;
     }
     a.keys_out[g] = key;
-    a.v0_out[g] = s_v0[i];
-    if (PAY2) a.v1_out[g] = s_v1[i];
+    a.v0_out[g] = s_v0[padded(i)];
+    if (PAY2) a.v1_out[g] = s_v1[padded(i)];
   }
   if (bad) atomicOr(a.status_word, kStatusCapacity);
 }
@@ -211,19 +228,16 @@ __global__ void k_digit_bases(uint32_t* hist, uint32_t radix) {
 template <int RB, bool PAY2>
 size_t onesweep_smem() {
   constexpr uint32_t R = 1u << RB;
-  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTile + 8 * R + 3 * R + 48);
+  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTileP + 8 * R + 3 * R + 48);
 }
 
 template <int RB, bool PAY2>
 cudaError_t launch_pass(const PassArgs& p, uint32_t grid, cudaStream_t s) {
   const size_t smem = onesweep_smem<RB, PAY2>();
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_onesweep<RB, PAY2>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  // per device: set on every launch (a host-side attribute write)
+  const cudaError_t e = cudaFuncSetAttribute(k_onesweep<RB, PAY2>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   k_onesweep<RB, PAY2><<<grid, kSortThreads, smem, s>>>(p);
   return cudaGetLastError();
 }
@@ -306,6 +320,7 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.grid_tiles = tiles;
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
+    pa.ballot = (a.ballot_mask >> p) & 1u;
     cudaError_t e;
     switch (rb) {
       case 4: e = pay2 ? launch_pass<4, true>(pa, tiles, s) : launch_pass<4, false>(pa, tiles, s); break;

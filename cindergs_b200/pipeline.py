@@ -353,12 +353,7 @@ class GpuPipelineState:
         how the tile entries are sorted (include/cgs.h: CGS_SORT_*); every
         choice gives the same lists."""
         self.sync_scene_and_cages(scene, cages)
-        cam = _abi.CgsCamera()
-        arr = camera.to_array()
-        for k in range(16):
-            cam.view[k] = float(arr[k])
-        (cam.focal_x, cam.focal_y, cam.principal_x, cam.principal_y, cam.viewport_width,
-         cam.viewport_height, cam.near_plane) = (float(x) for x in arr[16:23])
+        cam = self._camera(camera)
         comp = self._compositor(compositor)
         params = _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
                                      float(min_opacity), float(min_radius_px),
@@ -375,6 +370,48 @@ class GpuPipelineState:
                                bool(t.stage3_cached), bool(t.used_hardware_timestamps),
                                bool(t.used_64bit_keys), int(t.active_gaussians),
                                int(t.surviving_gaussians), int(t.total_tile_entries))
+
+    @staticmethod
+    def _camera(camera: CameraUniforms) -> _abi.CgsCamera:
+        cam = _abi.CgsCamera()
+        arr = camera.to_array()
+        for k in range(16):
+            cam.view[k] = float(arr[k])
+        (cam.focal_x, cam.focal_y, cam.principal_x, cam.principal_y, cam.viewport_width,
+         cam.viewport_height, cam.near_plane) = (float(x) for x in arr[16:23])
+        return cam
+
+    def view_images(self, compositors) -> list:
+        """Device RGBA8 images [H, W] (int32 words) for execute_views; keep and
+        pass the same list every step so a captured graph can be replayed."""
+        import torch
+        return [torch.empty((int(c.screen_height), int(c.screen_width)), dtype=torch.int32,
+                            device=f"cuda:{self.device}") for c in compositors]
+
+    def execute_views(self, scene: GaussianSceneSoa, cages: CageScene | None, cameras,
+                      compositors, images, use_graph: bool = True,
+                      strain_split_threshold: float = 0.0, mip_filter_3d_var: float = 0.0,
+                      min_opacity: float = 1.0 / 255.0, min_radius_px: float = 0.5,
+                      radix_bits: int = 0, entry_sort: int = 0) -> dict:
+        """One step of many views (cgs_execute_views): Stage 1 once, Stages 2-4
+        per view into images[v] (from view_images). With use_graph the step is
+        captured as a CUDA graph on the first call for a set of views and
+        replayed afterwards. Returns the step's stats."""
+        self.sync_scene_and_cages(scene, cages)
+        n = len(cameras)
+        cams = (_abi.CgsCamera * n)(*[self._camera(c) for c in cameras])
+        comps = (_abi.CgsCompositor * n)(*[self._compositor(c) for c in compositors])
+        outs = (ctypes.c_void_p * n)(*[ctypes.c_void_p(t.data_ptr()) for t in images])
+        params = _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
+                                     float(min_opacity), float(min_radius_px), 0, 1, 0,
+                                     int(radix_bits), int(entry_sort))
+        st = _abi.CgsViewsStats()
+        self._check(self._lib.cgs_execute_views(self._ctx, n, cams, comps, ctypes.byref(params),
+                                                outs, int(bool(use_graph)), ctypes.byref(st)),
+                    "cgs_execute_views")
+        return dict(ms=st.ms, total_tile_entries=int(st.total_tile_entries),
+                    graph_replayed=bool(st.graph_replayed), graph_captured=bool(st.graph_captured),
+                    views_rerendered=int(st.views_rerendered))
 
     @staticmethod
     def _compositor(c: CompositorUniforms) -> _abi.CgsCompositor:

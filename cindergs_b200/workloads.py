@@ -63,8 +63,8 @@ class CageOrbitWorkload:
 
 
 def tet_cage_orbit(n: int = 1_100_000, seed: int = 0, width: int = 1920, height: int = 1080,
-                   frames: int = 120, cells: int = 5) -> CageOrbitWorkload:
-    scene = random_scene(n, seed=seed, box=1.0)
+                   frames: int = 120, cells: int = 5, box: float | None = 1.0) -> CageOrbitWorkload:
+    scene = random_scene(n, seed=seed, box=box)
     mesh = TetMesh.create_grid_cage((cells, cells, cells), (-1.1,) * 3, (1.1,) * 3)
     cage = Cage("grid", mesh)
     sim = cage.simulator
@@ -77,6 +77,41 @@ def tet_cage_orbit(n: int = 1_100_000, seed: int = 0, width: int = 1920, height:
     disp[sim.pinned] = 0.0
     sim.current_positions = (mesh.rest_vertices + disp).astype(f32)
     return CageOrbitWorkload(scene, cage, width, height, frames, 4.0)
+
+
+RESOLUTIONS = ((640, 360), (1280, 720), (1920, 1080))
+
+
+def spiral_views(count: int = 64, fov_deg: float = 60.0):
+    """(cameras, compositors) of `count` views on a spiral around the origin:
+    view i at radius 3 + 2 t and elevation -30 + 90 t degrees (t = i / (count
+    - 1)), azimuth advancing by the golden angle, looking at the origin, at
+    resolutions cycling through 640x360, 1280x720 and 1920x1080."""
+    cams, comps = [], []
+    golden = np.pi * (3.0 - np.sqrt(5.0))
+    for i in range(count):
+        t = i / max(count - 1, 1)
+        r = 3.0 + 2.0 * t
+        el = np.deg2rad(-30.0 + 90.0 * t)
+        az = golden * i
+        eye = (r * np.cos(el) * np.sin(az), r * np.sin(el), r * np.cos(el) * np.cos(az))
+        w, h = RESOLUTIONS[i % len(RESOLUTIONS)]
+        cam = CameraUniforms.from_look_at(eye, (0, 0, 0), (0, 1, 0), np.deg2rad(fov_deg), w, h,
+                                          0.2)
+        cams.append(cam)
+        comps.append(CompositorUniforms(w, h, (0.0, 0.0, 0.0, 1.0),
+                                        tuple(float(x) for x in cam.eye()), 3))
+    return cams, comps
+
+
+def multiview_cage(n: int = 2_000_000, views: int = 64, seed: int = 0):
+    """The batched multi-view workload: Gaussians as in ``random_scene``
+    (means N(0, I3), not rescaled), the spring-driven tet cage of
+    ``tet_cage_orbit`` deforming them once per step, and ``spiral_views``.
+    Returns (CageOrbitWorkload, cameras, compositors)."""
+    wl = tet_cage_orbit(n=n, seed=seed, box=None)
+    cams, comps = spiral_views(views)
+    return wl, cams, comps
 
 
 def ball_points(n: int, rng: np.random.Generator, radius: float = 1.0) -> np.ndarray:

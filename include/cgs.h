@@ -262,6 +262,30 @@ int cgs_mvc_bind_learned(cgs_ctx* ctx, float threshold, uint32_t flags, uint32_t
 int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
                       const cgs_frame_params* params, cgs_stage_timings* timings);
 
+/* One step of many views; no reference counterpart (execute_frame_gpu renders
+ * one view per call). Stage 1 runs once (when the cages moved), then Stages
+ * 2-4 run per view with that view's camera and viewport, writing view v's
+ * RGBA8 image to the device buffer d_rgba8[v] (rows of screen_width pixels).
+ * The Stage 3 cache is not used and stage profiling is off. With use_graph,
+ * the first call for a set of views (same cameras, viewports, parameters,
+ * output buffers, scene/cage/binding state and buffer capacities) renders
+ * eagerly and captures the whole step as a CUDA graph; later calls with the
+ * same set replay it (a view whose tile entries exceeded the captured
+ * capacity is rendered again eagerly and the graph is rebuilt next time).
+ * Without use_graph every view's launches are issued from the host. The call
+ * returns when the step has finished. */
+typedef struct cgs_views_stats {
+  double ms;                    /* device time of the step, CUDA events */
+  uint64_t total_tile_entries;  /* over all views */
+  uint32_t graph_replayed;      /* the step ran as a graph replay */
+  uint32_t graph_captured;      /* a graph was captured in this call */
+  uint32_t views_rerendered;    /* views rendered again after an overflow */
+  uint32_t pad;
+} cgs_views_stats;
+int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* cameras,
+                      const cgs_compositor* comps, const cgs_frame_params* params,
+                      uint32_t* const* d_rgba8, int32_t use_graph, cgs_views_stats* stats);
+
 /* Copies the last frame's RGBA8 pixels into a tight [h][w][4] host buffer
  * (readback_framebuffer_rgba8, gpu_state.rs:1296-1328). */
 int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height);
