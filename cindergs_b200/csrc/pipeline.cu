@@ -1832,12 +1832,12 @@ int views_eager(cgs_ctx* ctx, uint32_t nv, const cgs_camera* cams, const cgs_com
                 uint64_t* entries) {
   std::vector<uint32_t> cap(nv), over;
   for (uint32_t v = 0; v < nv; ++v)
-    CGS_TRY(enqueue_view(ctx, &cams[v], &comps[v], params, v, outs[v], false, &cap[v]));
+    CGS_TRY(enqueue_view(ctx, &cams[v], &comps[v], &params[v], v, outs[v], false, &cap[v]));
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "views");
   CGS_TRY(check_views(ctx, nv, cap.data(), &over, entries));
   for (int round = 0; !over.empty() && round < 3; ++round) {
     for (uint32_t v : over) {
-      CGS_TRY(enqueue_view(ctx, &cams[v], &comps[v], params, v, outs[v], false, &cap[v]));
+      CGS_TRY(enqueue_view(ctx, &cams[v], &comps[v], &params[v], v, outs[v], false, &cap[v]));
       ++*rerendered;
     }
     CGS_CUDA(cudaStreamSynchronize(ctx->stream), "views");
@@ -1880,8 +1880,8 @@ int capture_views(cgs_ctx* ctx, uint32_t nv, const cgs_camera* cams, const cgs_c
   ctx->splat_parity = 0;
   const uint64_t epoch = ctx->alloc_epoch;
   for (uint32_t v = 0; v < nv && rc == CGS_OK && e == cudaSuccess; ++v)
-    rc = enqueue_view(ctx, &cams[v], &comps[v], params, v, outs[v], v == 0 && ctx->deform_on(),
-                      &cap[v]);
+    rc = enqueue_view(ctx, &cams[v], &comps[v], &params[v], v, outs[v],
+                      v == 0 && ctx->deform_on(), &cap[v]);
   const cudaError_t ee = cudaStreamEndCapture(s, &g);
   if (e == cudaSuccess) e = ee;
   if (rc == CGS_OK && e == cudaSuccess && ctx->alloc_epoch != epoch)
@@ -1908,10 +1908,13 @@ int capture_views(cgs_ctx* ctx, uint32_t nv, const cgs_camera* cams, const cgs_c
 int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* cameras,
                       const cgs_compositor* comps, const cgs_frame_params* params,
                       uint32_t* const* d_rgba8, int32_t use_graph, cgs_views_stats* stats) {
-  if (!ctx || !params || (num_views && (!cameras || !comps || !d_rgba8))) return CGS_E_ARG;
+  if (!ctx || (num_views && (!cameras || !comps || !d_rgba8 || !params))) return CGS_E_ARG;
   for (uint32_t v = 0; v < num_views; ++v) {
-    CGS_TRY(check_frame_args(ctx, &cameras[v], &comps[v], params));
+    CGS_TRY(check_frame_args(ctx, &cameras[v], &comps[v], &params[v]));
     if (!d_rgba8[v] || ((uintptr_t)d_rgba8[v] & 3)) return ctx->fail(CGS_E_ARG, "view image pointer");
+    if (fbits(params[v].strain_split_threshold) != fbits(params[0].strain_split_threshold) ||
+        fbits(params[v].mip_filter_3d_var) != fbits(params[0].mip_filter_3d_var))
+      return ctx->fail(CGS_E_ARG, "views must share the strain split and Mip settings");
   }
   cgs_views_stats st{};
   if (num_views == 0) {
@@ -1933,10 +1936,12 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
   }
   for (auto& ev : ctx->views_ev)
     if (!ev) CGS_CUDA(cudaEventCreate(&ev), "views event");
-  cgs_frame_params prm = *params;
-  prm.profile_stages = 0;
-  prm.write_f32 = 0;
-  prm.force_stage3 = 1;
+  std::vector<cgs_frame_params> prm(params, params + num_views);
+  for (auto& q : prm) {
+    q.profile_stages = 0;
+    q.write_f32 = 0;
+    q.force_stage3 = 1;
+  }
   ctx->kprof = false;
   ctx->cur = -1;
 
@@ -1945,7 +1950,7 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
     put_bytes(k, &num_views, sizeof(num_views));
     put_bytes(k, cameras, num_views * sizeof(cgs_camera));
     put_bytes(k, comps, num_views * sizeof(cgs_compositor));
-    put_bytes(k, &prm, sizeof(prm));
+    put_bytes(k, prm.data(), num_views * sizeof(cgs_frame_params));
     put_bytes(k, d_rgba8, num_views * sizeof(uint32_t*));
     put_bytes(k, &ctx->alloc_epoch, sizeof(ctx->alloc_epoch));
     put_bytes(k, &ctx->state_epoch, sizeof(ctx->state_epoch));
@@ -1967,7 +1972,7 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
       // render the overflowed views again eagerly; the graph is rebuilt on
       // the next call (its capacity no longer matches)
       for (uint32_t v : over) {
-        CGS_TRY(enqueue_view(ctx, &cameras[v], &comps[v], &prm, v, d_rgba8[v], false, &cap[v]));
+        CGS_TRY(enqueue_view(ctx, &cameras[v], &comps[v], &prm[v], v, d_rgba8[v], false, &cap[v]));
         ++st.views_rerendered;
       }
       CGS_CUDA(cudaStreamSynchronize(s), "views");
@@ -1976,7 +1981,7 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
     }
     if (ctx->entry_cap != cap_before) drop_views_graph(ctx);
   } else {
-    CGS_TRY(views_eager(ctx, num_views, cameras, comps, &prm, d_rgba8, &st.views_rerendered,
+    CGS_TRY(views_eager(ctx, num_views, cameras, comps, prm.data(), d_rgba8, &st.views_rerendered,
                         &st.total_tile_entries));
     CGS_CUDA(cudaEventRecord(ctx->views_ev[1], s), "views event");
     if (use_graph) {
@@ -1986,7 +1991,7 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
         key64 = key64 || (uint64_t)((comps[v].screen_width + 15) / 16) *
                                  ((comps[v].screen_height + 15) / 16) > 65535u;
       CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, key64, ctx->radix_lb_bits ? ctx->radix_lb_bits : 8));
-      CGS_TRY(capture_views(ctx, num_views, cameras, comps, &prm, d_rgba8));
+      CGS_TRY(capture_views(ctx, num_views, cameras, comps, prm.data(), d_rgba8));
       ctx->views_key = key_of();
       st.graph_captured = 1;
     }

@@ -392,21 +392,26 @@ class GpuPipelineState:
                       compositors, images, use_graph: bool = True,
                       strain_split_threshold: float = 0.0, mip_filter_3d_var: float = 0.0,
                       min_opacity: float = 1.0 / 255.0, min_radius_px: float = 0.5,
-                      radix_bits: int = 0, entry_sort: int = 0) -> dict:
+                      radix_bits=0, entry_sort=0) -> dict:
         """One step of many views (cgs_execute_views): Stage 1 once, Stages 2-4
-        per view into images[v] (from view_images). With use_graph the step is
-        captured as a CUDA graph on the first call for a set of views and
-        replayed afterwards. Returns the step's stats."""
+        per view into images[v] (from view_images). radix_bits and entry_sort
+        are one value for every view or a list with one per view (see
+        cindergs_b200.autotune). With use_graph the step is captured as a CUDA
+        graph on the first call for a set of views and replayed afterwards.
+        Returns the step's stats."""
         self.sync_scene_and_cages(scene, cages)
         n = len(cameras)
         cams = (_abi.CgsCamera * n)(*[self._camera(c) for c in cameras])
         comps = (_abi.CgsCompositor * n)(*[self._compositor(c) for c in compositors])
         outs = (ctypes.c_void_p * n)(*[ctypes.c_void_p(t.data_ptr()) for t in images])
-        params = _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
-                                     float(min_opacity), float(min_radius_px), 0, 1, 0,
-                                     int(radix_bits), int(entry_sort))
+        rbs = list(radix_bits) if hasattr(radix_bits, "__len__") else [radix_bits] * n
+        ess = list(entry_sort) if hasattr(entry_sort, "__len__") else [entry_sort] * n
+        params = (_abi.CgsFrameParams * n)(*[
+            _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
+                                float(min_opacity), float(min_radius_px), 0, 1, 0, int(rbs[v]),
+                                int(ess[v])) for v in range(n)])
         st = _abi.CgsViewsStats()
-        self._check(self._lib.cgs_execute_views(self._ctx, n, cams, comps, ctypes.byref(params),
+        self._check(self._lib.cgs_execute_views(self._ctx, n, cams, comps, params,
                                                 outs, int(bool(use_graph)), ctypes.byref(st)),
                     "cgs_execute_views")
         return dict(ms=st.ms, total_tile_entries=int(st.total_tile_entries),

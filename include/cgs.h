@@ -264,8 +264,10 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
 
 /* One step of many views; no reference counterpart (execute_frame_gpu renders
  * one view per call). Stage 1 runs once (when the cages moved), then Stages
- * 2-4 run per view with that view's camera and viewport, writing view v's
- * RGBA8 image to the device buffer d_rgba8[v] (rows of screen_width pixels).
+ * 2-4 run per view with that view's camera, viewport and parameters
+ * (params[v]: every view's strain split and Mip settings must agree, the
+ * digit width and entry sort may differ), writing view v's RGBA8 image to
+ * the device buffer d_rgba8[v] (rows of screen_width pixels).
  * The Stage 3 cache is not used and stage profiling is off. With use_graph,
  * the first call for a set of views (same cameras, viewports, parameters,
  * output buffers, scene/cage/binding state and buffer capacities) renders

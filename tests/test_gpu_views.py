@@ -83,3 +83,20 @@ def test_replay_overflow_renders_again(setup):
     again = st.execute_views(wl.scene, cages, cams, comps, imgs, use_graph=True)
     assert again["graph_captured"], again  # rebuilt with the grown capacity
     sim.current_positions = rest.copy()
+
+
+def test_autotuned_views_render_the_same(setup):
+    """Per-view digit widths and entry-sort methods chosen by the autotuner
+    give the same images as the defaults."""
+    from cindergs_b200 import autotune
+    st, wl, cages, cams, comps = setup
+    wl.step()
+    best = autotune.tune_views(st, wl.scene, cages, cams, comps, repeats=1)
+    assert set(best) == {(c.screen_width, c.screen_height) for c in comps}
+    rbs, ess = autotune.per_view(best, comps)
+    a, b = st.view_images(comps), st.view_images(comps)
+    st.execute_views(wl.scene, cages, cams, comps, a, use_graph=False)
+    st.execute_views(wl.scene, cages, cams, comps, b, use_graph=True, radix_bits=rbs,
+                     entry_sort=ess)
+    for x, y in zip(images_np(a), images_np(b)):
+        np.testing.assert_array_equal(x, y)
