@@ -131,6 +131,7 @@ SIGNATURES = {
     "cgs_mvc_bind": (_i32, [_vp, ctypes.POINTER(_u32)]),
     "cgs_mvc_weights": (_i32, [_vp, _u64, _vp, _vp]),
     "cgs_mvc_read_bindings": (_i32, [_vp, _u64, _vp, _vp, ctypes.POINTER(_u64)]),
+    "cgs_scene_upload_quantized": (_i32, [_vp, _u64, _vp, _vp, _vp, _vp, _u32]),
     "cgs_execute_views": (_i32, [_vp, _u32, _vp, _vp, _vp, _vp, _i32,
                                  ctypes.POINTER(CgsViewsStats)]),
     "cgs_mvc_field_create": (_i32, [_vp, _u64]),

@@ -206,6 +206,12 @@ struct ProjectArgs {
 };
 cudaError_t launch_project(const ProjectArgs& a, cudaStream_t s);
 
+// QuantizedGaussianSceneSoa words (f16 covariance pairs, degree-trimmed f16
+// SH) into the resident layout with f16 SH planes.
+cudaError_t launch_scene_decode_quantized(uint32_t n, const float* pos, const uint32_t* cov_words,
+                                          const float* opa, const uint32_t* sh_words,
+                                          uint32_t sh_degree, float4* out_pos, float4* out_cova,
+                                          float2* out_covb, void* out_sh, cudaStream_t s);
 // Rest-scene layout conversion from the reference's interleaved SoA.
 cudaError_t launch_scene_layout(uint32_t n, const float* pos, const float* cov, const float* opa,
                                 const void* sh, int sh_f16, float4* out_pos, float4* out_cova,

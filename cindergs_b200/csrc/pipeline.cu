@@ -876,6 +876,58 @@ int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* co
   return CGS_OK;
 }
 
+int cgs_scene_upload_quantized(cgs_ctx* ctx, uint64_t n, const float* pos,
+                               const uint32_t* cov_f16x2, const float* opa,
+                               const uint32_t* sh_f16x2, uint32_t sh_degree) {
+  if (ctx) ++ctx->state_epoch;
+  if (!ctx) return CGS_E_ARG;
+  if (sh_degree > 3) return ctx->fail(CGS_E_ARG, "sh_degree must be 0..3");
+  if (n >= (1ull << 30)) return ctx->fail(CGS_E_CAPACITY, "scene exceeds 2^30 Gaussians");
+  if (n > 0 && (!pos || !cov_f16x2 || !opa || !sh_f16x2))
+    return ctx->fail(CGS_E_ARG, "null scene array");
+  cudaSetDevice(ctx->device);
+  const size_t nn = n ? n : 1;
+  const size_t bases = sh_degree == 0 ? 1 : (sh_degree == 1 ? 4 : (sh_degree == 2 ? 9 : 16));
+  const size_t words = (bases * 3 + 1) / 2;
+  CGS_TRY(ctx->ensure(ctx->rest_pos, nn * 16, "rest positions"));
+  CGS_TRY(ctx->ensure(ctx->rest_cova, nn * 16, "rest covariances"));
+  CGS_TRY(ctx->ensure(ctx->rest_covb, nn * 8, "rest covariances"));
+  CGS_TRY(ctx->ensure(ctx->rest_sh, nn * 96, "rest SH"));
+  if (n > 0) {
+    void* stage = nullptr;
+    const size_t pb = (size_t)n * 12, cb = (size_t)n * 12, ob = (size_t)n * 4,
+                 sb = (size_t)n * words * 4;
+    const size_t ofs_c = (pb + 255) & ~(size_t)255, ofs_o = ofs_c + ((cb + 255) & ~(size_t)255),
+                 ofs_s = ofs_o + ((ob + 255) & ~(size_t)255);
+    CGS_CUDA(cudaMalloc(&stage, ofs_s + sb), "cudaMalloc scene staging");
+    char* st = (char*)stage;
+    cudaError_t e = cudaMemcpyAsync(st, pos, pb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st + ofs_c, cov_f16x2, cb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st + ofs_o, opa, ob, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st + ofs_s, sh_f16x2, sb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = launch_scene_decode_quantized((uint32_t)n, (const float*)st, (const uint32_t*)(st + ofs_c),
+                                        (const float*)(st + ofs_o), (const uint32_t*)(st + ofs_s),
+                                        sh_degree, ctx->rest_pos.as<float4>(),
+                                        ctx->rest_cova.as<float4>(), ctx->rest_covb.as<float2>(),
+                                        ctx->rest_sh.p, ctx->stream);
+    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    cudaFree(stage);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "quantized scene upload");
+    if (e2 != cudaSuccess) return ctx->cuda_fail(e2, "quantized scene upload");
+  }
+  ctx->n = (uint32_t)n;
+  ctx->sh_f16 = 1;
+  ctx->scene_ready = true;
+  ctx->deformed_valid = false;
+  ctx->deform_generation++;
+  ctx->s3_valid = false;
+  ctx->has_cages = false;
+  ctx->num_tets = 0;
+  ctx->mvc_unbind();
+  return CGS_OK;
+}
+
 int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
                          const float* inv_dm, uint32_t num_verts, const uint32_t* bind_tet,
                          const float* bind_w) {

@@ -293,7 +293,61 @@ __global__ void k_scene_layout(uint32_t n, const float* __restrict__ pos,
   }
 }
 
+// QuantizedGaussianSceneSoa (scene/soa.rs:429-608) into the resident layout:
+// covariances from three words of f16 pairs ((xx, xy), (xz, yy), (yz, zz),
+// first value in the low half), SH from the degree-trimmed words (DC rgb,
+// then each channel's higher-order coefficients, two f16 per word) into the
+// 48-coefficient channel-major f16 planes with zeros above the degree. f16
+// to f32 is exact, so this equals uploading the dequantized scene.
+__global__ void k_scene_decode_quantized(uint32_t n, const float* __restrict__ pos,
+                                         const uint32_t* __restrict__ cov_words,
+                                         const float* __restrict__ opa,
+                                         const uint32_t* __restrict__ sh_words, uint32_t sh_degree,
+                                         float4* __restrict__ out_pos, float4* __restrict__ out_cova,
+                                         float2* __restrict__ out_covb, uint4* __restrict__ out_sh) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out_pos[i] = make_float4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], opa[i]);
+  const uint32_t* cw = cov_words + 3 * (size_t)i;
+  auto lo = [](uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu))); };
+  auto hi = [](uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); };
+  const uint32_t w0 = cw[0], w1 = cw[1], w2 = cw[2];
+  out_cova[i] = make_float4(lo(w0), hi(w0), lo(w1), hi(w1));
+  out_covb[i] = make_float2(lo(w2), hi(w2));
+  const uint32_t deg = sh_degree > 3 ? 3 : sh_degree;
+  const uint32_t bases = deg == 0 ? 1 : (deg == 1 ? 4 : (deg == 2 ? 9 : 16));
+  const uint32_t rest = bases - 1, words = (bases * 3 + 1) / 2;
+  const uint32_t* sw = sh_words + (size_t)words * i;
+  uint32_t half_bits[48];
+#pragma unroll
+  for (int k = 0; k < 48; ++k) {
+    int l;
+    if (k < 3) l = k;
+    else if (k < 18) l = (uint32_t)(k - 3) < rest ? 3 + (k - 3) : -1;
+    else if (k < 33) l = (uint32_t)(k - 18) < rest ? 3 + (int)rest + (k - 18) : -1;
+    else l = (uint32_t)(k - 33) < rest ? 3 + 2 * (int)rest + (k - 33) : -1;
+    half_bits[k] = l < 0 ? 0u : (sw[l >> 1] >> (16 * (l & 1))) & 0xFFFFu;
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const uint32_t* h = half_bits + 8 * j;
+    out_sh[(size_t)j * n + i] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16),
+                                           h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_scene_decode_quantized(uint32_t n, const float* pos, const uint32_t* cov_words,
+                                          const float* opa, const uint32_t* sh_words,
+                                          uint32_t sh_degree, float4* out_pos, float4* out_cova,
+                                          float2* out_covb, void* out_sh, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_scene_decode_quantized<<<(n + 255) / 256, 256, 0, s>>>(
+      n, pos, cov_words, opa, sh_words, sh_degree, out_pos, out_cova, out_covb,
+      reinterpret_cast<uint4*>(out_sh));
+  return cudaGetLastError();
+}
 
 cudaError_t launch_project(const ProjectArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;

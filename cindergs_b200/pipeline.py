@@ -25,7 +25,7 @@ import numpy as np
 from . import _abi
 from .camera import CameraUniforms, CompositorUniforms
 from .cage import CageScene, TetMesh, UNBOUND
-from .scene import GaussianSceneSoa
+from .scene import GaussianSceneSoa, QuantizedGaussianSceneSoa
 
 f32 = np.float32
 
@@ -57,7 +57,9 @@ def scene_fingerprint(scene: GaussianSceneSoa) -> bytes:
     of each array, hashed with BLAKE2b."""
     h = hashlib.blake2b(digest_size=16)
     h.update(int(scene.count).to_bytes(8, "little"))
-    for arr in (scene.positions, scene.covariances_3d, scene.opacities, scene.sh_coeffs):
+    arrays = (scene.fingerprint_arrays() if hasattr(scene, "fingerprint_arrays") else
+              (scene.positions, scene.covariances_3d, scene.opacities, scene.sh_coeffs))
+    for arr in arrays:
         h.update(int(arr.ctypes.data).to_bytes(8, "little"))
         flat = arr.reshape(-1)
         h.update(int(flat.size).to_bytes(8, "little"))
@@ -109,7 +111,21 @@ class GpuPipelineState:
         return self._ctx
 
     # -- residency ------------------------------------------------------------
-    def upload_scene(self, scene: GaussianSceneSoa) -> None:
+    def upload_scene(self, scene) -> None:
+        """GaussianSceneSoa (f32 or f16 SH) or QuantizedGaussianSceneSoa."""
+        if isinstance(scene, QuantizedGaussianSceneSoa):
+            pos = np.ascontiguousarray(scene.positions, f32)
+            cov = np.ascontiguousarray(scene.covariances_f16_packed, np.uint32)
+            opa = np.ascontiguousarray(scene.opacities, f32)
+            sh = np.ascontiguousarray(scene.sh_coeffs_f16_packed, np.uint32)
+            self._check(self._lib.cgs_scene_upload_quantized(self._ctx, scene.count, _p(pos),
+                                                             _p(cov), _p(opa), _p(sh),
+                                                             int(scene.sh_degree)),
+                        "cgs_scene_upload_quantized")
+            self._scene_hash = scene_fingerprint(scene)
+            self._scene_count = scene.count
+            self._cage_key = None
+            return
         pos = np.ascontiguousarray(scene.positions, f32)
         cov = np.ascontiguousarray(scene.covariances_3d, f32)
         opa = np.ascontiguousarray(scene.opacities, f32)

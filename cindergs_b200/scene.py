@@ -52,6 +52,107 @@ class GaussianSceneSoa:
         return s
 
 
+def sh_bases_for_degree(sh_degree: int) -> int:
+    """SH basis functions up to a degree (soa.rs:331-338)."""
+    return {0: 1, 1: 4, 2: 9}.get(int(sh_degree), 16)
+
+
+def sh_packed_words_for_degree(sh_degree: int) -> int:
+    """u32 words of f16 pairs per splat (soa.rs:342-344)."""
+    return (sh_bases_for_degree(sh_degree) * 3 + 1) // 2
+
+
+def pack_f16_pairs(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """low = f16(a), high = f16(b), round to nearest even (soa.rs:348-352)."""
+    ha = np.asarray(a, np.float32).astype(np.float16).view(np.uint16).astype(np.uint32)
+    hb = np.asarray(b, np.float32).astype(np.float16).view(np.uint16).astype(np.uint32)
+    return ha | (hb << np.uint32(16))
+
+
+def unpack_f16_pairs(w: np.ndarray):
+    """(low, high) of f16 pair words as float32 (soa.rs:356-360)."""
+    w = np.asarray(w, np.uint32)
+    lo = (w & np.uint32(0xFFFF)).astype(np.uint16).view(np.float16).astype(np.float32)
+    hi = (w >> np.uint32(16)).astype(np.uint16).view(np.float16).astype(np.float32)
+    return lo, hi
+
+
+@dataclass
+class QuantizedGaussianSceneSoa:
+    """QuantizedGaussianSceneSoa (scene/soa.rs:429-608): f32 positions and
+    opacities, covariances as three words of f16 pairs per splat, SH up to
+    `sh_degree` as f16 pairs in the order DC rgb, then each channel's higher
+    orders. The reference's octahedral rotation word is used by no stage of
+    the frame and is not kept."""
+    positions: np.ndarray              # [N,3] f32
+    covariances_f16_packed: np.ndarray  # [N,3] u32
+    opacities: np.ndarray              # [N] f32
+    sh_coeffs_f16_packed: np.ndarray   # [N,words] u32
+    sh_degree: int = 3
+
+    @property
+    def count(self) -> int:
+        return int(self.opacities.shape[0])
+
+    def __len__(self) -> int:
+        return self.count
+
+    def fingerprint_arrays(self):
+        return (self.positions, self.covariances_f16_packed, self.opacities,
+                self.sh_coeffs_f16_packed)
+
+    @staticmethod
+    def from_soa(scene: GaussianSceneSoa, sh_degree: int = 3) -> "QuantizedGaussianSceneSoa":
+        """from_soa_with_degree (soa.rs:453-498)."""
+        deg = min(int(sh_degree), 3)
+        bases = sh_bases_for_degree(deg)
+        rest = bases - 1
+        c = np.asarray(scene.covariances_3d, np.float32)
+        cov = np.stack([pack_f16_pairs(c[:, 0], c[:, 1]), pack_f16_pairs(c[:, 2], c[:, 3]),
+                        pack_f16_pairs(c[:, 4], c[:, 5])], axis=1)
+        sh = np.asarray(scene.sh_coeffs, np.float32)
+        words = sh_packed_words_for_degree(deg)
+        lin = np.zeros((scene.count, words * 2), np.float32)
+        lin[:, 0:3] = sh[:, 0:3]
+        if rest:
+            lin[:, 3:3 + rest] = sh[:, 3:3 + rest]
+            lin[:, 3 + rest:3 + 2 * rest] = sh[:, 18:18 + rest]
+            lin[:, 3 + 2 * rest:3 + 3 * rest] = sh[:, 33:33 + rest]
+        packed = pack_f16_pairs(lin[:, 0::2], lin[:, 1::2])
+        return QuantizedGaussianSceneSoa(np.ascontiguousarray(scene.positions, np.float32),
+                                         np.ascontiguousarray(cov, np.uint32),
+                                         np.ascontiguousarray(scene.opacities, np.float32),
+                                         np.ascontiguousarray(packed, np.uint32), deg)
+
+    def unpack_covariance_3d(self) -> np.ndarray:
+        """[N,6] (soa.rs:508-515)."""
+        out = np.empty((self.count, 6), np.float32)
+        for k in range(3):
+            out[:, 2 * k], out[:, 2 * k + 1] = unpack_f16_pairs(self.covariances_f16_packed[:, k])
+        return out
+
+    def unpack_sh_48(self) -> np.ndarray:
+        """[N,48] channel-major, zeros above the degree (soa.rs:518-546)."""
+        bases = sh_bases_for_degree(self.sh_degree)
+        rest = bases - 1
+        lo, hi = unpack_f16_pairs(self.sh_coeffs_f16_packed)
+        lin = np.empty((self.count, lo.shape[1] * 2), np.float32)
+        lin[:, 0::2], lin[:, 1::2] = lo, hi
+        lin[:, bases * 3:] = 0.0
+        out = np.zeros((self.count, 48), np.float32)
+        out[:, 0:3] = lin[:, 0:3]
+        if rest:
+            out[:, 3:3 + rest] = lin[:, 3:3 + rest]
+            out[:, 18:18 + rest] = lin[:, 3 + rest:3 + 2 * rest]
+            out[:, 33:33 + rest] = lin[:, 3 + 2 * rest:3 + 3 * rest]
+        return out
+
+    def to_soa(self) -> GaussianSceneSoa:
+        """Dequantized scene (soa.rs:549-560), SH kept as float32."""
+        return GaussianSceneSoa(self.positions.copy(), self.unpack_covariance_3d(),
+                                self.opacities.copy(), self.unpack_sh_48())
+
+
 def activate_opacity(raw: np.ndarray) -> np.ndarray:
     """1 / (1 + exp(-raw)) (covariance.rs:13-15)."""
     raw = raw.astype(f32)

@@ -114,6 +114,61 @@ def multiview_cage(n: int = 2_000_000, views: int = 64, seed: int = 0):
     return wl, cams, comps
 
 
+@dataclass
+class LargeMultiCageWorkload:
+    """Quantized scene, several spring-driven tet cages and a polygon cage."""
+    scene: object            # QuantizedGaussianSceneSoa
+    cages: list              # tet cages (Cage)
+    poly: "PolyCageWorkload"  # polygon cage and its motion (scene unused)
+    width: int
+    height: int
+    frames: int
+    radius: float
+    dt: float = 1.0 / 60.0
+
+    def camera(self, frame: int) -> CameraUniforms:
+        return orbit_camera(frame % self.frames, self.frames, self.radius, self.width,
+                            self.height, 60.0)
+
+    def compositor(self, cam: CameraUniforms) -> CompositorUniforms:
+        return CompositorUniforms(self.width, self.height, (0.0, 0.0, 0.0, 1.0),
+                                  tuple(float(x) for x in cam.eye()), 3)
+
+
+def spring_cage(lo, hi, cells: int, rng: np.random.Generator) -> Cage:
+    """Grid cage of cells^3 cubes (6 tets each) over [lo, hi] with the spring
+    parameters of the tet-cage workload: bottom layer pinned, the rest
+    displaced by N(0, 0.05)."""
+    mesh = TetMesh.create_grid_cage((cells, cells, cells), lo, hi)
+    cage = Cage("grid", mesh)
+    sim = cage.simulator
+    sim.stiffness = f32(40.0)
+    sim.damping = f32(np.exp(-4.0 / 60.0))
+    sim.pinned = mesh.rest_vertices[:, 1] <= mesh.rest_vertices[:, 1].min()
+    disp = rng.normal(0.0, 0.05, mesh.rest_vertices.shape).astype(f32)
+    disp[sim.pinned] = 0.0
+    sim.current_positions = (mesh.rest_vertices + disp).astype(f32)
+    return cage
+
+
+def large_multicage(n: int = 6_000_000, seed: int = 0, width: int = 7680, height: int = 4320,
+                    frames: int = 30, radius: float = 8.0) -> LargeMultiCageWorkload:
+    """The large-scene workload: Gaussians drawn as in ``random_scene`` and
+    scaled into [-1, 1]^3, stored as a QuantizedGaussianSceneSoa (f16
+    covariances and SH degree 3); four 4x4x4-cube (384-tet) spring cages over
+    the upper half (x and z halves of [-1.1, 1.1], y in [0, 1.1]); the
+    level-3 icosphere polygon cage of ``mvc_cage_sphere`` (its moving field)
+    for the rest; 7680 x 4320 (129,600 tiles, 64-bit keys), a camera orbiting
+    at `radius`."""
+    from .scene import QuantizedGaussianSceneSoa
+    scene = QuantizedGaussianSceneSoa.from_soa(random_scene(n, seed=seed, box=1.0), 3)
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    cages = [spring_cage((x0, 0.0, z0), (x0 + 1.1, 1.1, z0 + 1.1), 4, rng)
+             for x0 in (-1.1, 0.0) for z0 in (-1.1, 0.0)]
+    poly = mvc_cage_sphere(n=1, seed=seed, width=width, height=height, frames=frames)
+    return LargeMultiCageWorkload(scene, cages, poly, width, height, frames, radius)
+
+
 def ball_points(n: int, rng: np.random.Generator, radius: float = 1.0) -> np.ndarray:
     """n points uniform in the ball of `radius` (direction from a normal
     sample, radius from the cube root of a uniform)."""

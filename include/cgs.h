@@ -123,6 +123,19 @@ const char* cgs_version(void);
 int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* cov,
                      const float* opa, const void* sh, int32_t sh_format);
 
+/* Uploads a QuantizedGaussianSceneSoa (scene/soa.rs:429-608): pos [n*3] f32,
+ * cov_f16x2 [n*3] words of f16 pairs ((xx,xy), (xz,yy), (yz,zz), first value
+ * in the low half), opa [n] f32, sh_f16x2 [n*words] with the coefficients up
+ * to sh_degree (0..3) in its order (DC rgb, then each channel's higher
+ * orders), two f16 per word, words = ceil(3 (sh_degree+1)^2 / 2) (24 for
+ * degree 3). The octahedral rotation words are not used by any stage and
+ * are not taken. Decoded on the GPU into the resident layout with f16 SH
+ * planes; f16 to f32 is exact, so frames equal those of the dequantized
+ * scene (to_soa) uploaded with CGS_SH_F16. */
+int cgs_scene_upload_quantized(cgs_ctx* ctx, uint64_t n, const float* pos,
+                               const uint32_t* cov_f16x2, const float* opa,
+                               const uint32_t* sh_f16x2, uint32_t sh_degree);
+
 /* Uploads flattened tet-cage topology for all cages (gpu_state.rs:248-298):
  * elems [num_tets*4] global vertex indices, inv_dm [num_tets*9] column-major
  * D_m^-1, bind_tet [n] global tet index or 0xFFFFFFFF when unbound,
