@@ -31,6 +31,7 @@ UNITS = [
     ("radix_sort.cu", []),
     ("stage4_composite.cu", []),
     ("mvc_field.cu", []),
+    ("mvc_field_tc.cu", []),
     ("field.cu", []),
     ("pipeline.cu", []),
     ("noalloc.cu", []),

@@ -126,6 +126,7 @@ cudaError_t FieldState::init(uint32_t nv, const float* rest_v4, uint64_t seed, c
   FIELD_TRY(proj.ensure((size_t)kFieldProj * 4));
   FIELD_TRY(proj_rest.ensure((size_t)kFieldProj * 4));
   FIELD_TRY(loss.ensure(16));
+  FIELD_TRY(status.ensure(16));
   FIELD_TRY(wT.ensure((size_t)kFieldHid * std::max<uint32_t>(ldV, kFieldHid) * 2));
   FIELD_TRY(cudaMemsetAsync(m1.p, 0, (size_t)o * 4, s));
   FIELD_TRY(cudaMemsetAsync(m2.p, 0, (size_t)o * 4, s));

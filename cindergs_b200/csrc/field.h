@@ -36,7 +36,7 @@ struct FieldState {
   float scale = 1.0f;       // s: half of the largest rest-cage extent
   FieldMat M{};             // (Vb Vb^T)^-1, Vb = [1; rest vertices]
   uint32_t step = 0;        // Adam steps taken
-  FieldBuf p32, g32, m1, m2, pb, enc_d, M_d, rest_d, proj, proj_rest, loss, wT;
+  FieldBuf p32, g32, m1, m2, pb, enc_d, M_d, rest_d, proj, proj_rest, loss, wT, status;
   // training batch (B rows)
   uint32_t Bcap = 0;
   FieldBuf x, wt, a0, pre[4], h[4], z, dz, dzb, dzT, hT, dpre, dpreb, dpreT, dh;

@@ -131,8 +131,8 @@ struct FieldInfer {
   // xf), read by launch_field_apply
   __nv_bfloat16* codes;
   float4* code_pos;
+  uint32_t* status;      // kStatusBarrierTimeout when a bounded wait gave up, or null
 };
-size_t field_infer_smem();
 cudaError_t launch_field_gather(const FieldBatch& b, cudaStream_t s);
 cudaError_t launch_gemm_nt(const GemmArgs& g, int epi, cudaStream_t s);
 cudaError_t launch_transpose_f32(const float* in, uint32_t R, uint32_t C, uint32_t ldi,
@@ -153,6 +153,8 @@ cudaError_t launch_field_project(const FieldNet& net, uint32_t V, const float4* 
                                  const float4* verts, const float* M, float* proj,
                                  cudaStream_t s);
 cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s);
+// The same on the tcgen05 tensor cores (mvc_field_tc.cu).
+cudaError_t launch_field_infer_tc(const FieldInfer& fi, cudaStream_t s);
 // Output layer over cached codes (needs codes, points4): position + gradient.
 cudaError_t launch_field_apply(const FieldInfer& fi, cudaStream_t s);
 

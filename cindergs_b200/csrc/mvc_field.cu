@@ -13,10 +13,12 @@
 // weights decides which Gaussians fall back to exact MVC.
 //
 // Training (forward, backward, Adam) runs as separate kernels over batches of
-// points with exact weights; inference for the frame is one fused kernel that
+// points with exact weights (mma.sync GEMMs: small, latency-bound shapes);
+// inference for the frame is one fused tcgen05 kernel (mvc_field_tc.cu) that
 // evaluates the network and its forward-mode Jacobian per Gaussian and emits
 // the deformed position and deformation gradient in the layout of the exact
-// path (k_mvc_jacobian). The weights enter the position linearly, so with
+// path (k_mvc_jacobian), or keeps the last hidden layer as the Gaussian's
+// code for k_field_apply. The weights enter the position linearly, so with
 // A = v'^T Vb^T M (3 x 4, v' the current vertices) and A3 its last three
 // columns, x' = sum_j w_j v'_j = v'^T w0 - A3 r = Pc^T h + pc + A3 x, where
 // Pc (128 x 3), pc and A3 are formed once per frame from the output layer
@@ -40,14 +42,6 @@ namespace {
 
 constexpr int kIn = kFieldIn;    // 64 features
 constexpr int kHid = kFieldHid;  // 128
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<const uint32_t*>(&v);
-}
-__device__ __forceinline__ float round_bf16(float x) {
-  return __bfloat162float(__float2bfloat16_rn(x));
-}
 
 // D += A B, m16n8k16, A row-major, B column-major, bf16 in, fp32 accumulate.
 __device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
@@ -488,209 +482,6 @@ __global__ void __launch_bounds__(kProjThreads) k_field_project(FieldNet net, ui
   }
 }
 
-// Fused inference: per warp 4 points x 4 streams (value, d/dx, d/dy, d/dz) as
-// one 16-row MMA tile: row r <-> stream (r / 4 for r < 8, 2 + (r - 8) / 4
-// otherwise), point r % 4. Lane groups 0-3 hold the value and d/dy rows,
-// 4-7 the d/dx and d/dz rows of the same points and columns, so the
-// activation slope crosses over with one shuffle. Activations stay in
-// registers between layers (an MMA C tile pair is the next layer's A tile).
-constexpr int kFwdWarps = 8;
-constexpr int kW1ld = kIn + 8, kWld = kHid + 8;  // padded smem rows (bf16)
-
-template <int KT>
-__device__ __forceinline__ void layer_mma(const uint32_t (&a)[KT][4], const __nv_bfloat16* W,
-                                          int ld, int gq, int tq, float (&c)[16][4]) {
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
-    const __nv_bfloat16* wr = W + (size_t)(nt * 8 + gq) * ld;
-#pragma unroll
-    for (int kt = 0; kt < KT; ++kt) {
-      const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + kt * 16 + 2 * tq);
-      const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + kt * 16 + 8 + 2 * tq);
-      mma_bf16(c[nt], a[kt], b0, b1);
-    }
-  }
-}
-
-// bias + SiLU on value rows, slope times tangent rows; fp32 result in c.
-__device__ __forceinline__ void layer_act(float (&c)[16][4], const float* bias, bool value_lane,
-                                          int tq) {
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const float b = bias[nt * 8 + 2 * tq + e];
-      float slope = 0.0f;
-      if (value_lane) {
-        const float pre = c[nt][e] + b;
-        slope = silu_grad(pre);
-        c[nt][e] = silu(pre);
-      }
-      const float other = __shfl_xor_sync(0xffffffffu, slope, 16);
-      if (value_lane) {
-        c[nt][2 + e] *= slope;  // d/dy row
-      } else {
-        c[nt][e] *= other;      // d/dx row
-        c[nt][2 + e] *= other;  // d/dz row
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ void to_a(const float (&c)[16][4], uint32_t (&a)[8][4]) {
-#pragma unroll
-  for (int kt = 0; kt < 8; ++kt) {
-    a[kt][0] = pack_bf16(c[2 * kt][0], c[2 * kt][1]);
-    a[kt][1] = pack_bf16(c[2 * kt][2], c[2 * kt][3]);
-    a[kt][2] = pack_bf16(c[2 * kt + 1][0], c[2 * kt + 1][1]);
-    a[kt][3] = pack_bf16(c[2 * kt + 1][2], c[2 * kt + 1][3]);
-  }
-}
-
-// CODES: instead of the position and gradient, store the last hidden layer
-// and its three tangents (bf16, as the output layer consumes them) per item:
-// codes[item][stream][128], stream 0 = h, 1..3 = dh/dx, dh/dy, dh/dz.
-template <bool CODES>
-__global__ void __launch_bounds__(kFwdWarps * 32, 1) k_field_infer(FieldInfer fi) {
-  extern __shared__ __align__(16) unsigned char fsm[];
-  __nv_bfloat16* W1 = reinterpret_cast<__nv_bfloat16*>(fsm);
-  __nv_bfloat16* Wh = W1 + kHid * kW1ld;  // 3 x [128][kWld]
-  float* bias = reinterpret_cast<float*>(Wh + 3 * kHid * kWld);  // 4 x 128
-  float* proj = bias + 4 * kHid;                                  // kFieldProj
-  const int tid = threadIdx.x;
-  for (int i = tid; i < kHid * kIn; i += blockDim.x)
-    W1[(i / kIn) * kW1ld + (i % kIn)] = fi.net.W1b[i];
-  for (int l = 0; l < 3; ++l) {
-    const __nv_bfloat16* src = l == 0 ? fi.net.W2b : (l == 1 ? fi.net.W3b : fi.net.W4b);
-    for (int i = tid; i < kHid * kHid; i += blockDim.x)
-      Wh[l * kHid * kWld + (i / kHid) * kWld + (i % kHid)] = src[i];
-  }
-  for (int i = tid; i < kHid; i += blockDim.x) {
-    bias[i] = fi.net.b1[i];
-    bias[kHid + i] = fi.net.b2[i];
-    bias[2 * kHid + i] = fi.net.b3[i];
-    bias[3 * kHid + i] = fi.net.b4[i];
-  }
-  for (int i = tid; i < kFieldProj; i += blockDim.x) proj[i] = fi.proj[i];
-  __syncthreads();
-
-  const int warp = tid >> 5, lane = tid & 31, gq = lane >> 2, tq = lane & 3;
-  const bool value_lane = gq < 4;
-  const int p = gq & 3;  // point of this lane's rows
-  const uint32_t groups = (fi.count + 3) / 4;
-  for (uint32_t grp = blockIdx.x * kFwdWarps + warp; grp < groups;
-       grp += gridDim.x * kFwdWarps) {
-    const uint32_t k = grp * 4 + p;  // item of this lane's point
-    const bool valid = k < fi.count;
-    float xr[3] = {0.0f, 0.0f, 0.0f};
-    if (valid) {
-      const uint32_t gi = fi.gauss ? fi.gauss[fi.first + k] : fi.first + k;
-      if (fi.points4) {
-        const float4 x4 = fi.points4[gi];
-        xr[0] = x4.x;
-        xr[1] = x4.y;
-        xr[2] = x4.z;
-      } else {
-        xr[0] = fi.points3[3 * (size_t)gi];
-        xr[1] = fi.points3[3 * (size_t)gi + 1];
-        xr[2] = fi.points3[3 * (size_t)gi + 2];
-      }
-    }
-    const float xh[3] = {(xr[0] - fi.enc[0]) * fi.enc[3], (xr[1] - fi.enc[1]) * fi.enc[3],
-                         (xr[2] - fi.enc[2]) * fi.enc[3]};
-    // layer-1 A fragments: rows (g, g+8) = (value, d/dy) or (d/dx, d/dz)
-    uint32_t a1[4][4];
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      float v[2][4];  // [row h][column e]
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int col = kt * 16 + (e >> 1) * 8 + 2 * tq + (e & 1);
-        float f, df[3];
-        feature(col, xh, fi.enc[3], f, df);
-        v[0][e] = value_lane ? f : df[0];
-        v[1][e] = value_lane ? df[1] : df[2];
-      }
-      a1[kt][0] = pack_bf16(v[0][0], v[0][1]);
-      a1[kt][1] = pack_bf16(v[1][0], v[1][1]);
-      a1[kt][2] = pack_bf16(v[0][2], v[0][3]);
-      a1[kt][3] = pack_bf16(v[1][2], v[1][3]);
-    }
-    float c[16][4];
-    uint32_t a[8][4];
-    layer_mma<4>(a1, W1, kW1ld, gq, tq, c);
-    layer_act(c, bias, value_lane, tq);
-#pragma unroll 1
-    for (int l = 0; l < 3; ++l) {
-      to_a(c, a);
-      layer_mma<8>(a, Wh + l * kHid * kWld, kWld, gq, tq, c);
-      layer_act(c, bias + (l + 1) * kHid, value_lane, tq);
-    }
-    if (CODES) {
-      if (valid && value_lane && tq == 0) fi.code_pos[k] = make_float4(xr[0], xr[1], xr[2], 0.0f);
-      if (valid) {
-        // rows: value lanes (h, dh/dy), tangent lanes (dh/dx, dh/dz)
-        const int s0 = value_lane ? 0 : 1, s1 = value_lane ? 2 : 3;
-        __nv_bfloat16* base = fi.codes + (size_t)k * (4 * kHid);
-#pragma unroll
-        for (int nt = 0; nt < 16; ++nt) {
-          const int col = nt * 8 + 2 * tq;
-          *reinterpret_cast<uint32_t*>(base + s0 * kHid + col) = pack_bf16(c[nt][0], c[nt][1]);
-          *reinterpret_cast<uint32_t*>(base + s1 * kHid + col) = pack_bf16(c[nt][2], c[nt][3]);
-        }
-      }
-      continue;
-    }
-    // x' = P^T h + p0 on value rows, F columns = P^T dh on tangent rows; h
-    // and dh in bf16, as the output layer saw them in training
-    float o[2][3] = {{0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-    for (int nt = 0; nt < 16; ++nt)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const float* pr = proj + 3 * (nt * 8 + 2 * tq + e);
-        const float h0 = round_bf16(c[nt][e]), h1 = round_bf16(c[nt][2 + e]);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          o[0][q] += h0 * pr[q];
-          o[1][q] += h1 * pr[q];
-        }
-      }
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        o[h][q] += __shfl_xor_sync(0xffffffffu, o[h][q], 1);
-        o[h][q] += __shfl_xor_sync(0xffffffffu, o[h][q], 2);
-      }
-    // lane 4p (value, d/dy) takes d/dx and d/dz from lane 4p + 16
-    float tx[3], tz[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      tx[q] = __shfl_down_sync(0xffffffffu, o[0][q], 16);
-      tz[q] = __shfl_down_sync(0xffffffffu, o[1][q], 16);
-    }
-    if (value_lane && tq == 0 && valid) {
-      const float* pc = proj + 3 * kHid;
-      const float* A3 = pc + 3;  // row-major
-      float px[3], F[3][3];      // F[q][d] = d x'_q / d x_d
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        px[q] = o[0][q] + pc[q] + (A3[3 * q] * xr[0] + A3[3 * q + 1] * xr[1] + A3[3 * q + 2] * xr[2]);
-        F[q][0] = tx[q] + A3[3 * q];
-        F[q][1] = o[1][q] + A3[3 * q + 1];
-        F[q][2] = tz[q] + A3[3 * q + 2];
-      }
-      float4* out = fi.xf + 3 * (size_t)(fi.out_first + k);
-      // F column-major
-      out[0] = make_float4(px[0], px[1], px[2], F[0][0]);
-      out[1] = make_float4(F[1][0], F[2][0], F[0][1], F[1][1]);
-      out[2] = make_float4(F[2][1], F[0][2], F[1][2], F[2][2]);
-    }
-  }
-}
-
 // Final weights per row: w0 = z + (1 - sum z) / V, then the linear-precision
 // projection w = w0 - (u0 + v_j . u[1..3]), u = M[:, 1:4] (sum_j w0_j v_j - x).
 __global__ void k_field_weights(const float* __restrict__ z, uint32_t B, uint32_t V,
@@ -849,11 +640,6 @@ __global__ void __launch_bounds__(kApWarps * 32) k_field_apply(FieldInfer fi) {
 
 }  // namespace
 
-size_t field_infer_smem() {
-  return (size_t)kHid * kW1ld * 2 + (size_t)3 * kHid * kWld * 2 + (size_t)4 * kHid * 4 +
-         (size_t)kFieldProj * 4;
-}
-
 cudaError_t launch_field_gather(const FieldBatch& b, cudaStream_t s) {
   if (b.B == 0) return cudaSuccess;
   k_field_gather<<<b.B, 128, 0, s>>>(b);
@@ -930,22 +716,7 @@ cudaError_t launch_field_project(const FieldNet& net, uint32_t V, const float4* 
 }
 
 cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s) {
-  if (fi.count == 0) return cudaSuccess;
-  const size_t smem = field_infer_smem();
-  const uint32_t groups = (fi.count + 3) / 4;
-  const uint32_t blocks = std::min<uint32_t>(148u, (groups + kFwdWarps - 1) / kFwdWarps);
-  if (fi.codes) {
-    const cudaError_t e = cudaFuncSetAttribute(
-        k_field_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_field_infer<true><<<blocks, kFwdWarps * 32, smem, s>>>(fi);
-  } else {
-    const cudaError_t e = cudaFuncSetAttribute(
-        k_field_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_field_infer<false><<<blocks, kFwdWarps * 32, smem, s>>>(fi);
-  }
-  return cudaGetLastError();
+  return launch_field_infer_tc(fi, s);
 }
 
 cudaError_t launch_field_apply(const FieldInfer& fi, cudaStream_t s) {

@@ -171,6 +171,7 @@ struct cgs_ctx {
     fi.xf = mvc_xf.as<float4>();
     fi.codes = nullptr;
     fi.code_pos = nullptr;
+    fi.status = field.status.as<uint32_t>();
     return fi;
   }
   bool deform_on() const { return has_cages || mvc_nb > 0; }
@@ -1144,7 +1145,8 @@ int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, bool cache, uint32_t* 
           FieldState& f = ctx->field;
           ctx->mvc_nfb = 0;
           ctx->mvc_nb = nb;
-          e = f.project(nullptr, f.proj_rest.as<float>(), s);  // raw: sum_j w0_j v_j
+          e = cudaMemsetAsync(f.status.p, 0, 4, s);
+          if (e == cudaSuccess) e = f.project(nullptr, f.proj_rest.as<float>(), s);  // raw: sum_j w0_j v_j
           if (e == cudaSuccess) {
             FieldInfer fi = ctx->field_infer_args(f.proj_rest.as<float>());
             e = launch_field_infer(fi, s);
@@ -1200,6 +1202,12 @@ int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, bool cache, uint32_t* 
                                         ctx->mvc_wg.as<float4>(), s);
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (learned && e == cudaSuccess && rc == CGS_OK) {
+          uint32_t fst = 0;
+          e = cudaMemcpy(&fst, ctx->field.status.p, 4, cudaMemcpyDeviceToHost);
+          if (e == cudaSuccess && fst)
+            rc = ctx->fail(CGS_E_TIMEOUT, "field inference gave up waiting for the tensor cores");
+        }
       }
     }
     if (rc != CGS_OK || e != cudaSuccess) {
@@ -1378,8 +1386,13 @@ int cgs_mvc_field_infer(cgs_ctx* ctx, uint64_t n, const float* d_points, int32_t
   fi.points3 = d_points;
   fi.count = (uint32_t)n;
   fi.xf = reinterpret_cast<float4*>(d_out);
+  fi.status = f.status.as<uint32_t>();
+  CGS_CUDA(cudaMemsetAsync(f.status.p, 0, 4, s), "field inference");
   CGS_CUDA(launch_field_infer(fi, s), "field inference");
+  uint32_t fst = 0;
+  CGS_CUDA(cudaMemcpyAsync(&fst, f.status.p, 4, cudaMemcpyDeviceToHost, s), "field inference");
   CGS_CUDA(cudaStreamSynchronize(s), "field inference");
+  if (fst) return ctx->fail(CGS_E_TIMEOUT, "field inference gave up waiting for the tensor cores");
   return CGS_OK;
 }
 
@@ -1654,6 +1667,7 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
         CGS_CUDA(ctx->field.project(ctx->mvc_verts.as<float4>(), ctx->field.proj.as<float>(), s),
                  "field projection launch");
         FieldInfer fi = ctx->field_infer_args(ctx->field.proj.as<float>());
+        fi.status = &fc->status;
         if (ctx->mvc_cached) {
           fi.codes = ctx->mvc_codes.as<__nv_bfloat16>();
           fi.code_pos = ctx->mvc_code_pos.as<float4>();
