@@ -10,11 +10,13 @@
 //   2. each warp ranks its 512 keys by digit with __match_any_sync, keeping a
 //      per-warp digit counter in shared memory (stable: ranks follow key order);
 //   3. per-digit counts are published to a chained look-back array, one thread
-//      per digit, and the exclusive prefix over earlier tiles is collected
+//      per digit, and the keys are reordered by digit in shared memory (tile-
+//      local offsets only);
+//   4. the digit threads then collect the exclusive prefix over earlier tiles
 //      (tiles are taken in order from an atomic counter, so every tile waited
-//      on belongs to a resident block; waits are bounded by kSpinLimit polls);
-//   4. keys are reordered by digit in shared memory and written out so that
-//      each digit's run is a contiguous, mostly coalesced store.
+//      on belongs to a resident block; waits are bounded by kSpinLimit polls),
+//      and each digit's run is written out as a contiguous, mostly coalesced
+//      store.
 // The global digit offsets come from digit histograms of all passes, which the
 // Stage 3 binning kernel accumulates while it writes the keys (launch_histogram
 // does the same for standalone sorts); k_digit_bases turns them into
@@ -152,17 +154,31 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   }
   uint32_t tot2;
   const uint32_t tstart = block_exclusive_sum(my_count, s_misc + 8, &tot2);
+  // Publish the tile's counts, then reorder by digit through shared memory
+  // (tile-local offsets only) before walking back for the global prefix, so
+  // the walk starts later (its predecessors have had more time to publish
+  // their prefixes) and the reorder does not wait for it.
+  uint32_t agg = 0;
   if ((uint32_t)tid < R) {
     s_tstart[tid] = tstart;
     // Padding keys (past n) carry the largest digit and sit at the end of it.
-    uint32_t agg = my_count;
+    agg = my_count;
     if ((uint32_t)tid == a.dmask) agg -= (kSortTile - tile_valid);
-    uint32_t* st = a.status + (size_t)tile * R + tid;
+    st_relaxed_u32(a.status + (size_t)tile * R + tid, (tile == 0 ? kFlagPre : kFlagAgg) | agg);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t d = (k[j] >> a.shift) & a.dmask;
+    const uint32_t pos =
+        padded(s_tstart[d] + wh[d] + ((rk[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu));
+    s_keys[pos] = k[j];
+    s_v0[pos] = v0[j];
+    if (PAY2) s_v1[pos] = v1[j];
+  }
+  if ((uint32_t)tid < R) {
     uint32_t excl = 0;
-    if (tile == 0) {
-      st_relaxed_u32(st, kFlagPre | agg);
-    } else {
-      st_relaxed_u32(st, kFlagAgg | agg);
+    if (tile != 0) {
       long long pred = (long long)tile - 1;
       uint32_t spins = 0;
       while (pred >= 0) {
@@ -179,20 +195,9 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
         if ((w & ~kValueMask) == kFlagPre) break;
         --pred;
       }
-      st_relaxed_u32(st, kFlagPre | ((excl + agg) & kValueMask));
+      st_relaxed_u32(a.status + (size_t)tile * R + tid, kFlagPre | ((excl + agg) & kValueMask));
     }
     s_goff[tid] = a.dbase[tid] + excl - tstart;
-  }
-  __syncthreads();
-  // Reorder by digit through shared memory.
-#pragma unroll
-  for (int j = 0; j < kSortItems; ++j) {
-    const uint32_t d = (k[j] >> a.shift) & a.dmask;
-    const uint32_t pos =
-        padded(s_tstart[d] + wh[d] + ((rk[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu));
-    s_keys[pos] = k[j];
-    s_v0[pos] = v0[j];
-    if (PAY2) s_v1[pos] = v1[j];
   }
   __syncthreads();
   // Scatter: each digit's run is contiguous in the output.
