@@ -27,8 +27,9 @@ namespace {
 
 constexpr int kBinThreads = 256;
 constexpr int kBinWarps = kBinThreads / 32;
-constexpr int kMaskCap = 128;  // stored ballot masks per warp (4,096 candidates)
-constexpr int kHitCap = 736;   // stored hit records per warp (4 blocks fit an SM)
+constexpr int kMaskCap = 64;   // stored ballot masks per warp (2,048 candidates)
+constexpr int kHitCap = 896;   // stored hit records per warp (4 blocks fit an SM); a warp's
+                               // 32 splats emit ~770 entries at 1080p on average
 constexpr uint32_t kMaxGroups = 8;  // tile groups of the record mode
 
 // Per-splat constants of a warp's 32 splats, read by the lane that tests one
