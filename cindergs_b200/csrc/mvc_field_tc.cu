@@ -47,8 +47,10 @@ constexpr uint32_t kOffW4 = kOffW3 + 128 * 128 * 2;
 constexpr uint32_t kOffP = kOffW4 + 128 * 128 * 2;    // [16 x 128]   4 KB
 constexpr uint32_t kOffA = kOffP + 16 * 128 * 2;      // [128 x 128] per warpgroup
 constexpr uint32_t kOffBias = kOffA + kTcWG * 128 * 128 * 2;  // 4 x 128 f32
+constexpr uint32_t kChunk = 64;                        // columns per epilogue step
+constexpr uint32_t kXStride = kChunk + 4;                // floats per item row (bank spread)
 constexpr uint32_t kOffX = kOffBias + 4 * 128 * 4;    // per warpgroup: exchange area
-constexpr uint32_t kXBytes = 3 * 32 * 32 * 4;            //   pre, act, slope [32 col][32 item]
+constexpr uint32_t kXBytes = 2 * 32 * kXStride * 4;      //   pre (then act), slope [32 item][68]
 constexpr uint32_t kOffMisc = kOffX + kTcWG * kXBytes;   // pc, A3, mbarriers, tmem
 constexpr uint32_t kTcSmem = kOffMisc + 256 + 1024;      // + alignment slack
 
@@ -157,9 +159,8 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   const int wg = warp >> 2, r = tid & 127;  // warpgroup, row within its tile
   const int s_st = warp & 3, p = lane;      // stream (warp in the warpgroup), item (lane)
   float* X = reinterpret_cast<float*>(sm + kOffX + (uint32_t)wg * kXBytes);
-  float* X_pre = X;              // [32 columns][32 items]
-  float* X_act = X + 32 * 32;
-  float* X_slp = X + 2 * 32 * 32;
+  float* X_pre = X + p * kXStride;                 // this item's row: pre-activation, then act
+  float* X_slp = X + (32 + p) * kXStride;          // this item's row: SiLU slope
 
   // ---- weights, biases and the projection into shared memory
   auto put_w = [&](uint32_t off, const __nv_bfloat16* W, uint32_t R, uint32_t K) {
@@ -315,44 +316,68 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
       const float* bias = s_bias + l * kHid;
       const bool last = l == 3;
 #pragma unroll 1
-      for (int q = 0; q < kHid / 32; ++q) {
-        uint32_t v[32];
-        tmem_ld32(t_row + (uint32_t)q * 32, v);
+      for (int q = 0; q < kHid / (int)kChunk; ++q) {
+        uint32_t v[kChunk];
+        {
+          uint32_t (&v0)[32] = *reinterpret_cast<uint32_t(*)[32]>(&v[0]);
+          uint32_t (&v1)[32] = *reinterpret_cast<uint32_t(*)[32]>(&v[32]);
+          tmem_ld32(t_row + (uint32_t)q * kChunk, v0);
+          tmem_ld32(t_row + (uint32_t)q * kChunk + 32, v1);
+        }
+        const float* bq = bias + q * kChunk;
         if (s_st == 0) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) X_pre[j * 32 + p] = __uint_as_float(v[j]) + bias[q * 32 + j];
+          for (int j = 0; j < (int)kChunk; j += 4)
+            *reinterpret_cast<float4*>(X_pre + j) =
+                make_float4(__uint_as_float(v[j]) + bq[j], __uint_as_float(v[j + 1]) + bq[j + 1],
+                            __uint_as_float(v[j + 2]) + bq[j + 2], __uint_as_float(v[j + 3]) + bq[j + 3]);
         }
         wg_sync(wg);
-        // SiLU and its slope for columns 8 w .. 8 w + 7 of every item
+        // SiLU and its slope for columns 16 w .. 16 w + 15 of this item (the
+        // activation replaces the pre-activation)
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int j = 8 * s_st + k;
-          const float pre = X_pre[j * 32 + p];
-          const float sg = __fdividef(1.0f, 1.0f + __expf(-pre));
-          X_act[j * 32 + p] = pre * sg;
-          X_slp[j * 32 + p] = sg * (1.0f + pre * (1.0f - sg));
+        for (int k = 0; k < 16; k += 4) {
+          const int j = 16 * s_st + k;
+          const float4 pre4 = *reinterpret_cast<const float4*>(X_pre + j);
+          const float pr[4] = {pre4.x, pre4.y, pre4.z, pre4.w};
+          float ac[4], sl[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float sg = __fdividef(1.0f, 1.0f + __expf(-pr[e]));
+            ac[e] = pr[e] * sg;
+            sl[e] = sg * (1.0f + pr[e] * (1.0f - sg));
+          }
+          *reinterpret_cast<float4*>(X_pre + j) = make_float4(ac[0], ac[1], ac[2], ac[3]);
+          *reinterpret_cast<float4*>(X_slp + j) = make_float4(sl[0], sl[1], sl[2], sl[3]);
         }
         wg_sync(wg);
-        uint32_t outw[16];
+        uint32_t outw[kChunk / 2];
+        const float* src = s_st == 0 ? X_pre : X_slp;
 #pragma unroll
-        for (int j = 0; j < 32; j += 2) {
-          float o2[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-            o2[h] = s_st == 0 ? X_act[(j + h) * 32 + p] : __uint_as_float(v[j + h]) * X_slp[(j + h) * 32 + p];
-          outw[j >> 1] = pack2(o2[0], o2[1]);
+        for (int j = 0; j < (int)kChunk; j += 4) {
+          const float4 w4 = *reinterpret_cast<const float4*>(src + j);
+          if (s_st == 0) {
+            outw[j >> 1] = pack2(w4.x, w4.y);
+            outw[(j >> 1) + 1] = pack2(w4.z, w4.w);
+          } else {
+            outw[j >> 1] = pack2(__uint_as_float(v[j]) * w4.x, __uint_as_float(v[j + 1]) * w4.y);
+            outw[(j >> 1) + 1] =
+                pack2(__uint_as_float(v[j + 2]) * w4.z, __uint_as_float(v[j + 3]) * w4.w);
+          }
         }
 #pragma unroll
-        for (int c4 = 0; c4 < 4; ++c4)
-          *reinterpret_cast<uint4*>(A + sw_off(128, r, q * 32 + c4 * 8)) =
+        for (int c4 = 0; c4 < (int)kChunk / 8; ++c4)
+          *reinterpret_cast<uint4*>(A + sw_off(128, r, q * kChunk + c4 * 8)) =
               make_uint4(outw[4 * c4], outw[4 * c4 + 1], outw[4 * c4 + 2], outw[4 * c4 + 3]);
         if (CODES && last && valid) {
           uint4* dst = reinterpret_cast<uint4*>(fi.codes + (size_t)k_item * (4 * kHid) +
-                                                s_st * kHid + q * 32);
+                                                s_st * kHid + q * kChunk);
 #pragma unroll
-          for (int c4 = 0; c4 < 4; ++c4)
+          for (int c4 = 0; c4 < (int)kChunk / 8; ++c4)
             dst[c4] = make_uint4(outw[4 * c4], outw[4 * c4 + 1], outw[4 * c4 + 2], outw[4 * c4 + 3]);
         }
+        // (the next chunk's first writes come after every warp passed this
+        // chunk's second barrier, i.e. after all reads of the pre-activations)
       }
     }
     if (!ok) break;
