@@ -485,6 +485,22 @@ def run_mvc(args):
                        / (1.0 / float(enc[3]))).max())
 
     err = np.linalg.norm(pos_learned[:n].astype(np.float64) - pos_exact[:n], axis=1) / s
+    cpu = None
+    if not args.no_cpu_baseline:
+        # the reference's CPU path for this step: deform_scene_cpu with stored
+        # exact bindings (restated in oracle/, one thread), on a sample
+        import oracle
+        m = min(n, 10_000)
+        sidx = np.random.default_rng(11).choice(n, m, replace=False)
+        sp = wl.scene.positions[sidx]
+        inside, wgs = oracle.mvc_bind(sp, wl.cage.rest_vertices, wl.cage.triangles)
+        t0 = time.perf_counter()
+        oracle.mvc_deform(sp, wl.scene.covariances_3d[sidx], wl.scene.opacities[sidx], inside,
+                          wgs, wl.vertices(1))
+        cpu_ms = (time.perf_counter() - t0) * 1000.0 * n / m
+        cpu = {"value": cpu_ms, "unit": "ms/frame (Stage 1)", "cores": 1, "kind": "port",
+               "sample": f"exact MVC deformation with stored bindings (deform_scene_cpu "
+                         f"restated in oracle/) of {m:,} of the Gaussians, scaled to {n:,}"}
     with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
         pk = json.load(f)
     fk = k_pf.get("field", {})
@@ -526,6 +542,7 @@ def run_mvc(args):
                   "p99_rel_position": float(np.quantile(err, 0.99)),
                   "max_rel_position": float(err.max()), "relative_to": "cage half-extent s",
                   "s": s},
+        "cpu_baseline": cpu,
         "roofline": {
             "field": {"bound": "tensor", "achieved": field_tflops,
                       "peak": pk.get("bf16_tflops"), "unit": "TFLOP/s",
@@ -601,6 +618,22 @@ def run_views(args):
         graph_ms, graph_wall, gst = timed(lambda: batched(True))
     replays = sum(1 for x in gst if x["graph_replayed"])
     nv = len(cams)
+    cpu = None
+    if not args.no_cpu_baseline:
+        # one 1280x720 view through the restated reference CPU backend
+        import oracle
+        v = 1
+        m = wl.cage.mesh
+        _, _, _, flat_bt, flat_bw = cages.flatten()  # 0xFFFFFFFF marks unbound Gaussians
+        t0 = time.perf_counter()
+        oracle.ref_frame(wl.scene.as_dict(), cams[v].to_array(), comps[v].screen_width,
+                         comps[v].screen_height, np.asarray(comps[v].background_color, np.float32),
+                         np.asarray(comps[v].camera_position, np.float32), 3,
+                         cage=dict(verts=wl.cage.vertices(), elems=m.elements, inv_dm=m.inv_dm,
+                                   bind_tet=flat_bt, bind_w=flat_bw))
+        cpu = {"value": 1.0 / (time.perf_counter() - t0), "unit": "views/s",
+               "cores": __import__("oracle").threads(), "kind": "port",
+               "sample": "one 1280x720 view of the step (reference CPU path restated in oracle/)"}
     line = {
         "metric": "views/s of a 64-view step: one replayed CUDA graph vs per-view frame launches",
         "value": nv / (graph_ms / 1000.0), "unit": "views/s", "higher_is_better": True,
@@ -620,6 +653,7 @@ def run_views(args):
         "autotuned": {f"{w}x{h}": {"radix_bits": rb, "entry_sort": ["auto", "radix", "transpose"][es],
                                   "stage3_ms": ms} for (w, h), (rb, es, ms) in tuned.items()},
         "tile_entries_per_step": gst[-1]["total_tile_entries"] if gst else None,
+        "cpu_baseline": cpu,
         "clocks": clock.summary(),
     }
     print(json.dumps(line), flush=True)
