@@ -11,11 +11,12 @@ from .cage import Cage, CageScene, CageSpringSimulator, TetMesh, UNBOUND
 from .pipeline import (GpuPipelineState, GpuStageTimings, exclusive_scan_u32,
                        radix_sort_u32_pairs, radix_sort_u64_pairs, scene_fingerprint)
 from .mvc import PolyCageMesh
+from . import ply
 from .scene import GaussianSceneSoa, QuantizedGaussianSceneSoa, fibonacci_cluster, random_scene
 
 __all__ = [
     "CameraUniforms", "CompositorUniforms", "look_at_lh", "orbit_camera", "Cage", "CageScene",
     "CageSpringSimulator", "TetMesh", "UNBOUND", "GpuPipelineState", "GpuStageTimings",
     "exclusive_scan_u32", "radix_sort_u32_pairs", "radix_sort_u64_pairs", "scene_fingerprint",
-    "GaussianSceneSoa", "QuantizedGaussianSceneSoa", "fibonacci_cluster", "random_scene", "PolyCageMesh",
+    "GaussianSceneSoa", "QuantizedGaussianSceneSoa", "fibonacci_cluster", "random_scene", "PolyCageMesh", "ply",
 ]

@@ -100,6 +100,21 @@ class CgsKernelProfile(ctypes.Structure):
                 ("launches", _u32 * KERNEL_COUNT), ("alg_flops", _u64 * KERNEL_COUNT)]
 
 
+class CgsSpringCage(ctypes.Structure):
+    """cgs_spring_cage: one spring-driven cage's vertex range, parameters and planes."""
+    _fields_ = [("stiffness", ctypes.c_float), ("damping", ctypes.c_float),
+                ("mass", ctypes.c_float), ("first_vertex", _u32), ("num_vertices", _u32),
+                ("first_plane", _u32), ("num_planes", _u32), ("pad", _u32)]
+
+
+class CgsCollisionPlane(ctypes.Structure):
+    """cgs_collision_plane (CollisionPlane, dynamics.rs:4-14)."""
+    _fields_ = [("normal", ctypes.c_float * 3), ("offset", ctypes.c_float),
+                ("restitution", ctypes.c_float), ("friction", ctypes.c_float),
+                ("pad", ctypes.c_float * 2)]
+
+
+assert ctypes.sizeof(CgsSpringCage) == 32 and ctypes.sizeof(CgsCollisionPlane) == 32
 assert ctypes.sizeof(CgsCamera) == 96
 assert ctypes.sizeof(CgsCompositor) == 48
 
@@ -144,6 +159,12 @@ SIGNATURES = {
     "cgs_mvc_field_infer": (_i32, [_vp, _u64, _vp, _i32, _vp]),
     "cgs_mvc_bind_learned": (_i32, [_vp, ctypes.c_float, _u32, ctypes.POINTER(_u32),
                                     ctypes.POINTER(_u32)]),
+    "cgs_sh_rotate": (_i32, [_vp, _u64, _vp, _u32, _vp, _vp, _u32]),
+    "cgs_springs_upload": (_i32, [_vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
+    "cgs_springs_step": (_i32, [_vp, ctypes.c_float, _u32]),
+    "cgs_springs_impulse": (_i32, [_vp, ctypes.c_float]),
+    "cgs_springs_read": (_i32, [_vp, _vp, _vp]),
+    "cgs_export_deformed": (_i32, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, ctypes.POINTER(_u64)]),
     "cgs_scan_u32": (_int, [_vp, _vp, _vp, _u64, ctypes.POINTER(_u64)]),
     "cgs_sort_pairs_u32": (_int, [_vp, _vp, _vp, _u64, _u32, _i32]),
     "cgs_sort_pairs_u64": (_int, [_vp, _vp, _vp, _vp, _u64, _u32, _i32]),

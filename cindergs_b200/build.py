@@ -28,6 +28,8 @@ UNITS = [
     ("stage1_mvc.cu", ["-fmad=false"]),
     ("stage2_project.cu", ["-fmad=false"]),
     ("stage3_bin.cu", ["-fmad=false"]),
+    ("sh_rotate.cu", ["-fmad=false"]),
+    ("springs.cu", ["-fmad=false"]),
     ("radix_sort.cu", []),
     ("stage4_composite.cu", []),
     ("mvc_field.cu", []),

@@ -2,8 +2,10 @@
 multi-cage bindings (deformation/mod.rs, deformation/dynamics.rs).
 
 Host-side set-up code. Binding Gaussians to tets runs on the GPU through the
-library (cgs_bind_tets); the per-frame spring step is host code over a few
-hundred vertices, as in the reference.
+library (cgs_bind_tets). The spring step runs here over a few hundred
+vertices, as in the reference, or on the device
+(GpuPipelineState.springs_upload / springs_step, cgs_springs_*) where the
+cage state then stays resident between frames.
 """
 from __future__ import annotations
 
@@ -118,6 +120,45 @@ class TetMesh:
         return TetMesh(verts, np.array(elems, np.uint32))
 
 
+@dataclass
+class CollisionPlane:
+    """Half-space normal . x >= offset with restitution and friction
+    (CollisionPlane, dynamics.rs:4-33); the normal is normalised on creation."""
+    normal: np.ndarray
+    offset: float
+    restitution: float = 0.25
+    friction: float = 0.2
+
+    def __post_init__(self):
+        n = np.asarray(self.normal, f32).reshape(3)
+        l2 = f32((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2])
+        self.normal = (n * (f32(1.0) / np.sqrt(l2))).astype(f32) if l2 > f32(1e-8) else \
+            np.array([0, 1, 0], f32)
+        self.offset = f32(self.offset)
+        self.restitution = f32(min(max(float(self.restitution), 0.0), 1.0))
+        self.friction = f32(min(max(float(self.friction), 0.0), 1.0))
+
+    @staticmethod
+    def ground_y(y: float) -> "CollisionPlane":
+        """CollisionPlane::ground_y (dynamics.rs:35-39)."""
+        return CollisionPlane(np.array([0, 1, 0], f32), y, 0.25, 0.2)
+
+    def resolve(self, pos: np.ndarray, vel: np.ndarray, mask: np.ndarray) -> None:
+        """resolve_contact (dynamics.rs:57-71) on the rows of `mask`, in place."""
+        n = self.normal
+        d = ((n[0] * pos[:, 0] + n[1] * pos[:, 1]) + n[2] * pos[:, 2] - self.offset).astype(f32)
+        hit = mask & (d < 0)
+        if not hit.any():
+            return
+        pos[hit] = (pos[hit] - n[None, :] * d[hit, None]).astype(f32)
+        v = vel[hit]
+        vn = ((v[:, 0] * n[0] + v[:, 1] * n[1]) + v[:, 2] * n[2]).astype(f32)
+        vnorm = (n[None, :] * vn[:, None]).astype(f32)
+        vtan = (v - vnorm).astype(f32)
+        new = (vtan * (f32(1.0) - self.friction) - vnorm * self.restitution).astype(f32)
+        vel[hit] = np.where((vn < 0)[:, None], new, v)
+
+
 class CageSpringSimulator:
     """Semi-implicit Euler springs toward the rest pose with frame-rate
     independent exponential damping and pinned vertices
@@ -133,6 +174,7 @@ class CageSpringSimulator:
         self.damping = f32(0.92)  # velocity retention per 1/60 s
         self.mass = f32(1.0)
         self.pinned = np.zeros(self.rest_positions.shape[0], bool)
+        self.collision_planes: list[CollisionPlane] = []
 
     @staticmethod
     def damping_coefficient(damping) -> np.float32:
@@ -157,6 +199,29 @@ class CageSpringSimulator:
         self.current_positions = np.where(free[:, None],
                                           self.current_positions + self.velocities * dt_sim,
                                           self.current_positions).astype(f32)
+        for plane in self.collision_planes:
+            plane.resolve(self.current_positions, self.velocities, free)
+
+    def trigger_jiggle_impulse(self, magnitude: float) -> None:
+        """Outward radial velocity pulse from the rest centroid on unpinned
+        vertices (trigger_jiggle_impulse, dynamics.rs:280-305)."""
+        n = self.rest_positions.shape[0]
+        if n == 0:
+            return
+        c = np.zeros(3, f32)
+        for p in self.rest_positions:  # sequential float32 sum, vertex order
+            c = (c + p).astype(f32)
+        c = (c / f32(n)).astype(f32)
+        d = (self.rest_positions - c).astype(f32)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rcp = (f32(1.0) / np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])).astype(f32)
+        ok = np.isfinite(rcp) & (rcp > 0)
+        r = np.where(ok[:, None], d * rcp[:, None], f32(0.0)).astype(f32)
+        big = ((r[:, 0] * r[:, 0] + r[:, 1] * r[:, 1]) + r[:, 2] * r[:, 2]) > f32(1e-4)
+        m = f32(magnitude)
+        imp = np.where(big[:, None], r * m, np.array([0, 1, 0], f32) * m).astype(f32)
+        free = ~self.pinned
+        self.velocities[free] = (self.velocities[free] + imp[free]).astype(f32)
 
     def positions_array(self) -> np.ndarray:
         return self.current_positions

@@ -335,6 +335,59 @@ cudaError_t launch_histogram(const uint32_t* keys, const uint32_t* n_ptr, uint32
 uint32_t sort_tiles(uint32_t capacity);
 uint32_t sort_passes(uint32_t num_bits, uint32_t radix_bits);
 
+// ---- Cage springs (springs.cu) -----------------------------------------------
+struct SpringCageDev {
+  float kim;        // stiffness / max(mass, 0.001)
+  float gamma;      // velocity factor exp(-c dt) of one step
+  float dt;         // min(dt, 0.033); a step is skipped unless > 0
+  float pad;
+  float cx, cy, cz; // rest centroid (jiggle impulse)
+  uint32_t planes;  // first plane | count << 16
+};
+struct SpringArgs {
+  uint32_t V, num_cages, steps;
+  const float4* rest;          // [V] xyz + cage index bits (>= num_cages: no cage)
+  float4* vel;                 // [V]
+  const uint8_t* pinned;       // [V]
+  float* verts;                // [V*3] the resident cage vertices, stepped in place
+  const SpringCageDev* cages;  // [num_cages]
+  const float4* planes;        // [2 per plane] (nx, ny, nz, offset), (restitution, friction, -, -)
+};
+cudaError_t launch_springs_step(const SpringArgs& a, cudaStream_t s);
+cudaError_t launch_springs_impulse(const SpringArgs& a, float magnitude, cudaStream_t s);
+
+// ---- SH coefficient rotation and export (sh_rotate.cu) ------------------------
+// Floats per rotation in the band-matrix table: M1 (9), M2 (25), M3 (49), pad.
+constexpr uint32_t kShRotStride = 84;
+struct ExportArgs {
+  uint32_t n_rest;            // rest Gaussians (splats at or above are split children)
+  uint32_t first, count;      // the chunk of splats to write
+  const float4* pos;          // [first + count] xyz + opacity (deformed or rest)
+  const float4* cova;         // xx, xy, xz, yy
+  const float2* covb;         // yz, zz
+  const void* sh;             // resident SH planes (f32 [12][sh_stride] or f16 [6][sh_stride])
+  int sh_f16;
+  uint32_t sh_stride;
+  const uint32_t* bind_tet;   // [n_rest] or null (no rotation)
+  const float4* bind_w;       // [n_rest] (MVC slot bits in .x)
+  const uint2* split_meta;    // [children] (parent, tet)
+  uint32_t num_tets;          // table rows [0, num_tets) are tet rotations
+  int mvc;                    // table rows num_tets + slot are MVC rotations
+  const float* table;         // [rotations * kShRotStride] or null
+  uint32_t degree;
+  float* out_pos;             // [count * 3] or null
+  float* out_cov;             // [count * 6] or null
+  float* out_opa;             // [count] or null
+  float* out_sh;              // [count * 48] or null
+};
+size_t sh_basis_bytes();
+cudaError_t launch_sh_basis(void* basis, cudaStream_t s);
+cudaError_t launch_sh_rotators(uint32_t count, const float* rot, const void* basis, uint32_t degree,
+                               float* table, cudaStream_t s);
+cudaError_t launch_sh_apply(uint64_t n, float* sh, const float* table, uint32_t num_rot,
+                            const uint32_t* index, uint32_t degree, uint32_t* bad, cudaStream_t s);
+cudaError_t launch_export(const ExportArgs& a, cudaStream_t s);
+
 // ---- Stage 4 (stage4_composite.cu) -------------------------------------------
 struct CompositeArgs {
   const SplatRec* recs;

@@ -70,6 +70,11 @@ uint32_t fbits(float f) {
   std::memcpy(&u, &f, 4);
   return u;
 }
+float bitsf(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
 
 // Everything Stages 3 and 4 of one frame need, kept so that a frame whose
 // tile entries overflowed the key buffers can be binned and composited again.
@@ -194,6 +199,17 @@ struct cgs_ctx {
   DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
+  // SH coefficient rotation (cgs_sh_rotate, cgs_export_deformed): the band
+  // bases (built once), the per-rotation band matrices and the export chunk
+  DevBuf sh_basis, sh_table, sh_stage;
+  bool sh_basis_ready = false;
+  // device cage springs (cgs_springs_*): per-vertex rest (+ cage index),
+  // velocity and pin; per-cage parameters and planes
+  DevBuf spr_rest, spr_vel, spr_pin, spr_cages, spr_planes;
+  std::vector<cgs_spring_cage> spr_host;
+  std::vector<float> spr_centroid;  // 3 per cage
+  uint32_t spr_V = 0;
+  bool spr_ready = false;
   // splat depth sort (Stage 3): keys/ids ping-pong and look-back pair
   DevBuf skeys[2], sids[2], splat_lb[2];
   uint32_t splat_cap = 0;  // slots those buffers hold; fixed between reallocations
@@ -872,6 +888,7 @@ int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* co
   ctx->deform_generation++;
   ctx->s3_valid = false;
   ctx->has_cages = false;  // cage bindings refer to the previous scene
+  ctx->spr_ready = false;
   ctx->num_tets = 0;
   ctx->mvc_unbind();
   return CGS_OK;
@@ -924,6 +941,7 @@ int cgs_scene_upload_quantized(cgs_ctx* ctx, uint64_t n, const float* pos,
   ctx->deform_generation++;
   ctx->s3_valid = false;
   ctx->has_cages = false;
+  ctx->spr_ready = false;
   ctx->num_tets = 0;
   ctx->mvc_unbind();
   return CGS_OK;
@@ -944,6 +962,7 @@ int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
       ctx->deformed_valid = false;
     }
     ctx->has_cages = false;
+    ctx->spr_ready = false;
     ctx->num_tets = 0;
     ctx->s3_valid = false;
     return CGS_OK;
@@ -968,6 +987,7 @@ int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
   ctx->num_tets = num_tets;
   ctx->num_verts = num_verts;
   ctx->has_cages = true;
+  ctx->spr_ready = false;
   ctx->mvc_unbind();  // the bindings were replaced: bind the polygon cage again
   ctx->verts_uploaded = false;
   ctx->last_verts.clear();
@@ -1427,6 +1447,174 @@ int cgs_mvc_read_bindings(cgs_ctx* ctx, uint64_t max_slots, uint32_t* gaussian, 
       CGS_CUDA(cudaMemcpy(row.data(), ctx->mvc_wg.as<float4>() + (size_t)j * nb, k * 16,
                           cudaMemcpyDeviceToHost), "read mvc bindings");
       for (uint64_t i = 0; i < k; ++i) std::memcpy(wg + 4 * ((size_t)i * V + j), &row[i], 16);
+    }
+  }
+  return CGS_OK;
+}
+
+namespace {
+
+// f32::min / f32::max: a NaN operand yields the other one.
+float rmin(float a, float b) { return std::isnan(a) ? b : (std::isnan(b) ? a : (a < b ? a : b)); }
+float rmax(float a, float b) { return std::isnan(a) ? b : (std::isnan(b) ? a : (a > b ? a : b)); }
+
+// CageSpringSimulator::frame_damping (deformation/dynamics.rs:137-148), with
+// the C library's logf / expf.
+float spring_frame_damping(float damping, float dt) {
+  float r = damping;
+  if (r < 1.0e-4f) r = 1.0e-4f;
+  if (r > 0.9999f) r = 0.9999f;
+  const float c = -logf(r) * 60.0f;
+  return expf(-c * dt);
+}
+
+SpringArgs spring_args(cgs_ctx* ctx, uint32_t steps) {
+  SpringArgs a{};
+  a.V = ctx->spr_V;
+  a.num_cages = (uint32_t)ctx->spr_host.size();
+  a.steps = steps;
+  a.rest = ctx->spr_rest.as<float4>();
+  a.vel = ctx->spr_vel.as<float4>();
+  a.pinned = ctx->spr_pin.as<uint8_t>();
+  a.verts = ctx->cage_verts.as<float>();
+  a.cages = ctx->spr_cages.as<SpringCageDev>();
+  a.planes = ctx->spr_planes.as<float4>();
+  return a;
+}
+
+// Per-cage step constants for `dt`, uploaded through the pinned ring.
+int spring_params(cgs_ctx* ctx, float dt) {
+  const size_t nc = ctx->spr_host.size();
+  std::vector<SpringCageDev> p(nc);
+  const float dt_sim = rmin(dt, 0.033f);
+  for (size_t c = 0; c < nc; ++c) {
+    const cgs_spring_cage& h = ctx->spr_host[c];
+    p[c].kim = h.stiffness * (1.0f / rmax(h.mass, 0.001f));
+    p[c].gamma = dt_sim > 0.0f ? spring_frame_damping(h.damping, dt_sim) : 1.0f;
+    p[c].dt = dt_sim > 0.0f ? dt_sim : 0.0f;
+    p[c].cx = ctx->spr_centroid[3 * c];
+    p[c].cy = ctx->spr_centroid[3 * c + 1];
+    p[c].cz = ctx->spr_centroid[3 * c + 2];
+    p[c].planes = h.first_plane | (h.num_planes << 16);
+  }
+  return staged_upload(ctx, ctx->spr_cages.p, nc * sizeof(SpringCageDev),
+                       [&](void* dst) { std::memcpy(dst, p.data(), nc * sizeof(SpringCageDev)); },
+                       "spring parameters");
+}
+
+}  // namespace
+
+int cgs_springs_upload(cgs_ctx* ctx, uint32_t num_cages, const cgs_spring_cage* cages,
+                       uint32_t num_planes, const cgs_collision_plane* planes, uint32_t num_verts,
+                       const float* rest, const float* current, const float* velocity,
+                       const uint8_t* pinned) {
+  if (!ctx) return CGS_E_ARG;
+  ctx->spr_ready = false;
+  if (!ctx->has_cages) return ctx->fail(CGS_E_STATE, "no tet cages uploaded");
+  if (num_verts != ctx->num_verts) return ctx->fail(CGS_E_ARG, "vertex count differs from the cage topology");
+  if (num_cages == 0 || !cages || !rest || !current) return CGS_E_ARG;
+  if (num_planes > 0xFFFFu || (num_planes && !planes)) return ctx->fail(CGS_E_ARG, "bad collision planes");
+  std::vector<float4> r(num_verts), v(num_verts);
+  std::vector<uint8_t> pin(num_verts, 0);
+  for (uint32_t i = 0; i < num_verts; ++i) {
+    r[i] = make_float4(rest[3 * i], rest[3 * i + 1], rest[3 * i + 2], bitsf(kInvalid));
+    v[i] = velocity ? make_float4(velocity[3 * i], velocity[3 * i + 1], velocity[3 * i + 2], 0.0f)
+                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (pinned) pin[i] = pinned[i] ? 1 : 0;
+  }
+  std::vector<float> centroid(3 * (size_t)num_cages, 0.0f);
+  for (uint32_t c = 0; c < num_cages; ++c) {
+    const cgs_spring_cage& h = cages[c];
+    if ((uint64_t)h.first_vertex + h.num_vertices > num_verts)
+      return ctx->fail(CGS_E_ARG, "spring cage vertex range outside the cage vertices");
+    if ((uint64_t)h.first_plane + h.num_planes > num_planes)
+      return ctx->fail(CGS_E_ARG, "spring cage plane range outside the planes");
+    float s[3] = {0.0f, 0.0f, 0.0f};  // rest centroid, summed in vertex order
+    for (uint32_t i = h.first_vertex; i < h.first_vertex + h.num_vertices; ++i) {
+      if (fbits(r[i].w) != kInvalid)
+        return ctx->fail(CGS_E_ARG, "spring cage vertex ranges overlap");
+      r[i].w = bitsf(c);
+      s[0] = s[0] + rest[3 * i];
+      s[1] = s[1] + rest[3 * i + 1];
+      s[2] = s[2] + rest[3 * i + 2];
+    }
+    for (int k = 0; k < 3; ++k)
+      centroid[3 * c + k] = h.num_vertices ? s[k] / (float)h.num_vertices : 0.0f;
+  }
+  cudaSetDevice(ctx->device);
+  CGS_TRY(ctx->ensure(ctx->spr_rest, (size_t)num_verts * 16, "spring rest"));
+  CGS_TRY(ctx->ensure(ctx->spr_vel, (size_t)num_verts * 16, "spring velocities"));
+  CGS_TRY(ctx->ensure(ctx->spr_pin, num_verts ? num_verts : 1, "spring pins"));
+  CGS_TRY(ctx->ensure(ctx->spr_cages, (size_t)num_cages * sizeof(SpringCageDev), "spring cages"));
+  CGS_TRY(ctx->ensure(ctx->spr_planes, (size_t)(num_planes ? num_planes : 1) * 32, "spring planes"));
+  CGS_TRY(drain(ctx, true));
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "spring upload");
+  CGS_CUDA(cudaMemcpy(ctx->spr_rest.p, r.data(), (size_t)num_verts * 16, cudaMemcpyHostToDevice), "spring rest");
+  CGS_CUDA(cudaMemcpy(ctx->spr_vel.p, v.data(), (size_t)num_verts * 16, cudaMemcpyHostToDevice), "spring velocities");
+  CGS_CUDA(cudaMemcpy(ctx->spr_pin.p, pin.data(), num_verts, cudaMemcpyHostToDevice), "spring pins");
+  if (num_planes) {
+    std::vector<float4> pl(2 * (size_t)num_planes);
+    for (uint32_t q = 0; q < num_planes; ++q) {
+      const cgs_collision_plane& h = planes[q];
+      pl[2 * q] = make_float4(h.normal[0], h.normal[1], h.normal[2], h.offset);
+      pl[2 * q + 1] = make_float4(h.restitution, h.friction, 0.0f, 0.0f);
+    }
+    CGS_CUDA(cudaMemcpy(ctx->spr_planes.p, pl.data(), pl.size() * 16, cudaMemcpyHostToDevice),
+             "spring planes");
+  }
+  CGS_CUDA(cudaMemcpy(ctx->cage_verts.p, current, (size_t)num_verts * 12, cudaMemcpyHostToDevice),
+           "spring positions");
+  ctx->spr_host.assign(cages, cages + num_cages);
+  ctx->spr_centroid = centroid;
+  ctx->spr_V = num_verts;
+  ctx->spr_ready = true;
+  ctx->last_verts.assign(current, current + (size_t)num_verts * 3);
+  ctx->verts_uploaded = true;
+  ctx->deformed_valid = false;
+  return CGS_OK;
+}
+
+int cgs_springs_step(cgs_ctx* ctx, float dt, uint32_t steps) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->spr_ready) return ctx->fail(CGS_E_STATE, "no device springs uploaded");
+  if (steps == 0) return CGS_OK;
+  cudaSetDevice(ctx->device);
+  CGS_TRY(spring_params(ctx, dt));
+  CGS_CUDA(launch_springs_step(spring_args(ctx, steps), ctx->stream), "springs launch");
+  if (rmin(dt, 0.033f) > 0.0f) {
+    ctx->last_verts.clear();  // the host copy no longer matches
+    ctx->deformed_valid = false;
+  }
+  return CGS_OK;
+}
+
+int cgs_springs_impulse(cgs_ctx* ctx, float magnitude) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->spr_ready) return ctx->fail(CGS_E_STATE, "no device springs uploaded");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(spring_params(ctx, 0.0f));
+  CGS_CUDA(launch_springs_impulse(spring_args(ctx, 0), magnitude, ctx->stream), "impulse launch");
+  return CGS_OK;
+}
+
+int cgs_springs_read(cgs_ctx* ctx, float* current, float* velocity) {
+  if (!ctx) return CGS_E_ARG;
+  if (!ctx->spr_ready) return ctx->fail(CGS_E_STATE, "no device springs uploaded");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "springs read");
+  const uint32_t V = ctx->spr_V;
+  if (current)
+    CGS_CUDA(cudaMemcpy(current, ctx->cage_verts.p, (size_t)V * 12, cudaMemcpyDeviceToHost),
+             "read spring positions");
+  if (velocity) {
+    std::vector<float4> v(V);
+    CGS_CUDA(cudaMemcpy(v.data(), ctx->spr_vel.p, (size_t)V * 16, cudaMemcpyDeviceToHost),
+             "read spring velocities");
+    for (uint32_t i = 0; i < V; ++i) {
+      velocity[3 * i] = v[i].x;
+      velocity[3 * i + 1] = v[i].y;
+      velocity[3 * i + 2] = v[i].z;
     }
   }
   return CGS_OK;
@@ -2124,6 +2312,7 @@ int cgs_invalidate(cgs_ctx* ctx) {
   ctx->has_cages = false;
   ctx->num_tets = 0;
   ctx->mvc_unbind();
+  ctx->spr_ready = false;
   ctx->deformed_valid = false;
   ctx->verts_uploaded = false;
   ctx->last_verts.clear();
@@ -2304,6 +2493,135 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
     if (dst_bytes < out.size()) return ctx->fail(CGS_E_ARG, "destination too small");
     std::memcpy(dst, out.data(), out.size());
   }
+  return CGS_OK;
+}
+
+namespace {
+
+// The band bases B_l and B_l^+ are constants: built on the device once.
+int ensure_sh_basis(cgs_ctx* ctx) {
+  if (ctx->sh_basis_ready) return CGS_OK;
+  CGS_TRY(ctx->ensure(ctx->sh_basis, sh_basis_bytes(), "sh basis"));
+  CGS_CUDA(launch_sh_basis(ctx->sh_basis.p, ctx->stream), "sh basis launch");
+  ctx->sh_basis_ready = true;
+  return CGS_OK;
+}
+
+}  // namespace
+
+int cgs_sh_rotate(cgs_ctx* ctx, uint64_t n, float* d_sh, uint32_t num_rotations,
+                  const float* d_rotations, const uint32_t* d_index, uint32_t degree) {
+  if (!ctx) return CGS_E_ARG;
+  if (n == 0 || degree == 0) return CGS_OK;
+  if (!d_sh || !d_rotations || num_rotations == 0) return CGS_E_ARG;
+  if (((uintptr_t)d_sh & 15u) != 0) return ctx->fail(CGS_E_ARG, "coefficients must be 16-byte aligned");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  const uint32_t deg = degree > 3 ? 3u : degree;
+  CGS_TRY(ensure_sh_basis(ctx));
+  CGS_TRY(ctx->ensure(ctx->sh_table, (size_t)num_rotations * kShRotStride * 4 + 64, "sh rotations"));
+  uint32_t* bad = (uint32_t*)(ctx->sh_table.as<char>() + (size_t)num_rotations * kShRotStride * 4);
+  CGS_CUDA(cudaMemsetAsync(bad, 0, 4, ctx->stream), "sh rotate status");
+  CGS_CUDA(launch_sh_rotators(num_rotations, d_rotations, ctx->sh_basis.p, deg,
+                              ctx->sh_table.as<float>(), ctx->stream), "sh rotators launch");
+  CGS_CUDA(launch_sh_apply(n, d_sh, ctx->sh_table.as<float>(), num_rotations, d_index, deg, bad,
+                           ctx->stream), "sh rotate launch");
+  uint32_t h_bad = 0;
+  CGS_CUDA(cudaMemcpyAsync(&h_bad, bad, 4, cudaMemcpyDeviceToHost, ctx->stream), "sh rotate status");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "sh rotate");
+  if (h_bad) return ctx->fail(CGS_E_ARG, "rotation index out of range (those blocks left unchanged)");
+  return CGS_OK;
+}
+
+int cgs_export_deformed(cgs_ctx* ctx, uint32_t sh_degree, uint64_t capacity, float* pos, float* cov,
+                        float* opa, float* sh, uint64_t* out_count) {
+  if (!ctx || !out_count) return CGS_E_ARG;
+  *out_count = 0;
+  if (!ctx->scene_ready) return ctx->fail(CGS_E_STATE, "no scene uploaded");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  const bool deformed = ctx->deform_on();
+  if (deformed && !ctx->deformed_valid)
+    return ctx->fail(CGS_E_STATE, "the cage state has changed since the last frame; execute a frame first");
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "export");
+  const uint32_t n = ctx->n;
+  uint32_t splits = 0;
+  if (deformed) CGS_CUDA(cudaMemcpy(&splits, ctx->persist.p, 4, cudaMemcpyDeviceToHost), "split count");
+  const uint64_t total = (uint64_t)n + splits;
+  *out_count = total;
+  if (!pos && !cov && !opa && !sh) return CGS_OK;
+  if (capacity < total) return ctx->fail(CGS_E_ARG, "capacity below the exported splat count");
+  if (total == 0) return CGS_OK;
+  const uint32_t deg = sh_degree > 3 ? 3u : sh_degree;
+  cudaStream_t s = ctx->stream;
+
+  ExportArgs a{};
+  a.n_rest = n;
+  if (deformed) {
+    a.pos = ctx->def_pos.as<float4>();
+    a.cova = ctx->def_cova.as<float4>();
+    a.covb = ctx->def_covb.as<float2>();
+  } else {
+    a.pos = ctx->rest_pos.as<float4>();
+    a.cova = ctx->rest_cova.as<float4>();
+    a.covb = ctx->rest_covb.as<float2>();
+  }
+  a.sh = ctx->rest_sh.p;
+  a.sh_f16 = ctx->sh_f16;
+  a.sh_stride = n;
+  a.degree = deg;
+  if (deformed && sh && deg > 0) {
+    // band matrices of every tet's and every MVC slot's rotation of the last
+    // Stage 1, tets first
+    const uint32_t T = ctx->has_cages ? ctx->num_tets : 0u, nb = ctx->mvc_nb;
+    CGS_TRY(ensure_sh_basis(ctx));
+    CGS_TRY(ctx->ensure(ctx->sh_table, ((size_t)T + nb) * kShRotStride * 4 + 64, "sh rotations"));
+    float* table = ctx->sh_table.as<float>();
+    CGS_CUDA(launch_sh_rotators(T, ctx->tet_R.as<float>(), ctx->sh_basis.p, deg, table, s),
+             "sh rotators launch");
+    if (nb)
+      CGS_CUDA(launch_sh_rotators(nb, ctx->mvc_R.as<float>(), ctx->sh_basis.p, deg,
+                                  table + (size_t)T * kShRotStride, s), "sh rotators launch");
+    a.bind_tet = ctx->bind_tet.as<uint32_t>();
+    a.bind_w = ctx->bind_w.as<float4>();
+    a.split_meta = ctx->split_meta.as<uint2>();
+    a.num_tets = T;
+    a.mvc = nb > 0;
+    a.table = table;
+  } else if (deformed) {
+    a.split_meta = ctx->split_meta.as<uint2>();
+  }
+  // Children read their parent's SH even when nothing rotates.
+  if (!a.split_meta && splits) return ctx->fail(CGS_E_STATE, "split children without their meta");
+
+  // Chunks of at most 2^20 splats through one device staging area (58 floats
+  // a splat), copied into the caller's arrays.
+  const uint32_t chunk = (uint32_t)std::min<uint64_t>(total, 1u << 20);
+  CGS_TRY(ctx->ensure(ctx->sh_stage, (size_t)chunk * 58 * 4, "export staging"));
+  float* st = ctx->sh_stage.as<float>();
+  for (uint64_t first = 0; first < total; first += chunk) {
+    const uint32_t cnt = (uint32_t)std::min<uint64_t>(chunk, total - first);
+    a.first = (uint32_t)first;
+    a.count = cnt;
+    a.out_pos = pos ? st : nullptr;
+    a.out_cov = cov ? st + (size_t)chunk * 3 : nullptr;
+    a.out_opa = opa ? st + (size_t)chunk * 9 : nullptr;
+    a.out_sh = sh ? st + (size_t)chunk * 10 : nullptr;
+    CGS_CUDA(launch_export(a, s), "export launch");
+    if (pos)
+      CGS_CUDA(cudaMemcpyAsync(pos + 3 * first, a.out_pos, (size_t)cnt * 12, cudaMemcpyDeviceToHost, s),
+               "export positions");
+    if (cov)
+      CGS_CUDA(cudaMemcpyAsync(cov + 6 * first, a.out_cov, (size_t)cnt * 24, cudaMemcpyDeviceToHost, s),
+               "export covariances");
+    if (opa)
+      CGS_CUDA(cudaMemcpyAsync(opa + first, a.out_opa, (size_t)cnt * 4, cudaMemcpyDeviceToHost, s),
+               "export opacities");
+    if (sh)
+      CGS_CUDA(cudaMemcpyAsync(sh + 48 * first, a.out_sh, (size_t)cnt * 192, cudaMemcpyDeviceToHost, s),
+               "export sh");
+  }
+  CGS_CUDA(cudaStreamSynchronize(s), "export");
   return CGS_OK;
 }
 

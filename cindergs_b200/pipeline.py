@@ -90,6 +90,8 @@ class GpuPipelineState:
         self._cage_key = None
         self._last = None
         self._mvc_V = 0
+        self._device_springs = False
+        self._num_cage_verts = 0
 
     # -- lifetime -------------------------------------------------------------
     def close(self) -> None:
@@ -140,6 +142,8 @@ class GpuPipelineState:
         self._cage_key = None
 
     def upload_cages(self, cages: CageScene | None) -> None:
+        self._device_springs = False
+        self._num_cage_verts = 0 if cages is None else sum(c.mesh.num_vertices for c in cages.cages)
         if cages is None or not cages.cages:
             self._check(self._lib.cgs_tet_cages_upload(self._ctx, 0, None, None, 0, None, None),
                         "cgs_tet_cages_upload")
@@ -165,9 +169,56 @@ class GpuPipelineState:
                tuple((id(c.mesh), c.mesh.num_tets, c.mesh.num_vertices) for c in cages.cages))
         if key != self._cage_key:
             self.upload_cages(cages)
+        if self._device_springs:
+            return  # the cage state lives on the device (springs_upload)
         v = np.ascontiguousarray(cages.flat_vertices(), f32)
         self._check(self._lib.cgs_cage_vertices_update(self._ctx, _p(v), v.shape[0]),
                     "cgs_cage_vertices_update")
+
+    # -- cage springs on the device ------------------------------------------------
+    def springs_upload(self, cages: CageScene) -> None:
+        """Moves every cage's CageSpringSimulator state (rest, current,
+        velocity, pins, stiffness / damping / mass, collision planes) to the
+        device; frames then deform with the device state and the host stops
+        uploading cage vertices (cgs_springs_upload). Upload the cages first."""
+        specs, planes, first = [], [], 0
+        for c in cages.cages:
+            sim = c.simulator
+            spec = _abi.CgsSpringCage(float(sim.stiffness), float(sim.damping), float(sim.mass),
+                                      first, sim.rest_positions.shape[0], len(planes),
+                                      len(sim.collision_planes), 0)
+            for pl in sim.collision_planes:
+                planes.append(_abi.CgsCollisionPlane((ctypes.c_float * 3)(*map(float, pl.normal)),
+                                                     float(pl.offset), float(pl.restitution),
+                                                     float(pl.friction)))
+            specs.append(spec)
+            first += sim.rest_positions.shape[0]
+        rest = np.ascontiguousarray(np.concatenate([c.simulator.rest_positions for c in cages.cages]), f32)
+        cur = np.ascontiguousarray(np.concatenate([c.simulator.current_positions for c in cages.cages]), f32)
+        vel = np.ascontiguousarray(np.concatenate([c.simulator.velocities for c in cages.cages]), f32)
+        pin = np.ascontiguousarray(np.concatenate([c.simulator.pinned for c in cages.cages]), np.uint8)
+        spec_arr = (_abi.CgsSpringCage * len(specs))(*specs)
+        plane_arr = (_abi.CgsCollisionPlane * max(len(planes), 1))(*planes)
+        self._check(self._lib.cgs_springs_upload(self._ctx, len(specs), spec_arr, len(planes),
+                                                 plane_arr if planes else None, rest.shape[0],
+                                                 _p(rest), _p(cur), _p(vel), _p(pin)),
+                    "cgs_springs_upload")
+        self._device_springs = True
+
+    def springs_step(self, dt: float, steps: int = 1) -> None:
+        """Enqueues `steps` spring steps of `dt` on the device (cgs_springs_step)."""
+        self._check(self._lib.cgs_springs_step(self._ctx, float(dt), int(steps)), "cgs_springs_step")
+
+    def springs_impulse(self, magnitude: float) -> None:
+        """trigger_jiggle_impulse on every device cage (cgs_springs_impulse)."""
+        self._check(self._lib.cgs_springs_impulse(self._ctx, float(magnitude)), "cgs_springs_impulse")
+
+    def springs_read(self) -> tuple[np.ndarray, np.ndarray]:
+        """Device cage positions and velocities [V,3] (cgs_springs_read)."""
+        n = self._num_cage_verts
+        cur, vel = np.empty((n, 3), f32), np.empty((n, 3), f32)
+        self._check(self._lib.cgs_springs_read(self._ctx, _p(cur), _p(vel)), "cgs_springs_read")
+        return cur, vel
 
     def bind_tets(self, mesh: TetMesh, bounds=None):
         """GPU barycentric binding of the resident scene to `mesh`
@@ -465,6 +516,7 @@ class GpuPipelineState:
         self._check(self._lib.cgs_invalidate(self._ctx), "cgs_invalidate")
         self._scene_hash = None
         self._cage_key = None
+        self._device_springs = False
 
     def invalidate_stage3(self) -> None:
         self._check(self._lib.cgs_invalidate_stage3(self._ctx), "cgs_invalidate_stage3")
@@ -490,6 +542,61 @@ class GpuPipelineState:
 
     def kernel_profile_reset(self) -> None:
         self._check(self._lib.cgs_kernel_profile_reset(self._ctx), "cgs_kernel_profile_reset")
+
+    # -- SH coefficient rotation and the deformed-scene export -------------------
+    def sh_rotate(self, sh, rotations, index=None, degree: int = 3):
+        """Rotates [n, 48] SH coefficient blocks on the GPU: block i by
+        rotations[index[i]] (or rotations[i % k]), rotations [k, 3, 3]
+        indexed [k, row, col] (ShRotator::apply, sh_rotation.rs:389-471;
+        cgs_sh_rotate). numpy in, numpy out; a CUDA tensor is rotated in
+        place and returned."""
+        import torch
+        dev = f"cuda:{self.device}"
+        on_device = isinstance(sh, torch.Tensor) and sh.is_cuda
+        t = sh if on_device else torch.as_tensor(np.ascontiguousarray(sh, f32)).to(dev)
+        if t.dtype != torch.float32 or not t.is_contiguous() or t.numel() % 48:
+            raise ValueError("sh must be contiguous float32 [n, 48]")
+        rot = torch.as_tensor(np.asarray(rotations, f32).reshape(-1, 3, 3)) if not (
+            isinstance(rotations, torch.Tensor)) else rotations.float().reshape(-1, 3, 3)
+        r9 = rot.transpose(1, 2).contiguous().to(dev)  # column-major per rotation
+        idx = None
+        if index is not None:
+            idx = torch.as_tensor(np.asarray(index, np.uint32).astype(np.int32)).to(dev) if not (
+                isinstance(index, torch.Tensor)) else index.to(dev, torch.int32).contiguous()
+        n = t.numel() // 48
+        self._check(self._lib.cgs_sh_rotate(self._ctx, n, ctypes.c_void_p(t.data_ptr()),
+                                            int(r9.shape[0]), ctypes.c_void_p(r9.data_ptr()),
+                                            ctypes.c_void_p(idx.data_ptr()) if idx is not None else None,
+                                            int(degree)), "cgs_sh_rotate")
+        return t if on_device else t.cpu().numpy().reshape(np.shape(sh))
+
+    def export_deformed(self, sh_degree: int = 3) -> GaussianSceneSoa:
+        """The last frame's deformed scene, SH coefficients rotated by each
+        splat's tet or polygon-cage rotation, split children after the rest
+        Gaussians (Timeline::deform_scene_at, app/timeline.rs:205-229;
+        cgs_export_deformed)."""
+        cnt = ctypes.c_uint64()
+        self._check(self._lib.cgs_export_deformed(self._ctx, int(sh_degree), 0, None, None, None,
+                                                  None, ctypes.byref(cnt)), "cgs_export_deformed")
+        n = int(cnt.value)
+        pos, cov = np.empty((n, 3), f32), np.empty((n, 6), f32)
+        opa, sh = np.empty(n, f32), np.empty((n, 48), f32)
+        self._check(self._lib.cgs_export_deformed(self._ctx, int(sh_degree), n, _p(pos), _p(cov),
+                                                  _p(opa), _p(sh), ctypes.byref(cnt)),
+                    "cgs_export_deformed")
+        return GaussianSceneSoa(pos, cov, opa, sh)
+
+    def export_deformed_ply_bytes(self, sh_degree: int = 3) -> bytes:
+        """Binary PLY of the deformed scene (export_deformed_ply_bytes_at,
+        app/timeline.rs:232-250)."""
+        from .ply import write_binary_ply_bytes
+        return write_binary_ply_bytes(self.export_deformed(sh_degree))
+
+    def export_deformed_ply(self, path, sh_degree: int = 3) -> None:
+        """Writes the deformed scene as binary PLY (export_deformed_ply_at,
+        app/timeline.rs:253-272)."""
+        from .ply import save_file
+        save_file(path, self.export_deformed(sh_degree))
 
     def read_buffer(self, which: int, dtype) -> np.ndarray:
         """Intermediate buffer of the last frame (CGS_BUF_*), as a flat array."""

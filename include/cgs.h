@@ -148,6 +148,47 @@ int cgs_tet_cages_upload(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems,
  * A change marks the deformed scene dirty; an identical upload does not. */
 int cgs_cage_vertices_update(cgs_ctx* ctx, const float* verts, uint32_t num_verts);
 
+/* ---- cage spring dynamics on the device (deformation/dynamics.rs) ---- */
+
+/* One spring-driven cage: the vertex range [first_vertex, first_vertex +
+ * num_vertices) of the flattened tet-cage vertices, its CageSpringSimulator
+ * parameters (stiffness, damping = velocity retention per 1/60 s, mass;
+ * dynamics.rs:75-131) and its collision planes [first_plane, first_plane +
+ * num_planes). */
+typedef struct cgs_spring_cage {
+  float stiffness, damping, mass;
+  uint32_t first_vertex, num_vertices;
+  uint32_t first_plane, num_planes;
+  uint32_t pad;
+} cgs_spring_cage;
+/* CollisionPlane (dynamics.rs:4-33): allowed half-space normal . x >= offset,
+ * normal of unit length, restitution and friction in [0, 1]. */
+typedef struct cgs_collision_plane {
+  float normal[3];
+  float offset, restitution, friction;
+  float pad[2];
+} cgs_collision_plane;
+/* Makes the tet-cage vertices spring-driven on the device: rest, current and
+ * velocity [num_verts*3], pinned [num_verts] (0/1, null = none). current
+ * becomes the resident cage state. num_verts must equal the tet cages'
+ * vertex count; cage ranges must not overlap (vertices outside every range
+ * are never stepped); at most 65,535 planes. Replaces the host-side
+ * CageSpringSimulator state (dynamics.rs:115-131). */
+int cgs_springs_upload(cgs_ctx* ctx, uint32_t num_cages, const cgs_spring_cage* cages,
+                       uint32_t num_planes, const cgs_collision_plane* planes, uint32_t num_verts,
+                       const float* rest, const float* current, const float* velocity,
+                       const uint8_t* pinned);
+/* Enqueues `steps` calls of CageSpringSimulator::step(dt) (dynamics.rs:
+ * 249-277; dt clamped to 0.033 s, no step when it is not positive) on the
+ * resident cage vertices; the next frame deforms with the result. Nothing is
+ * copied to or from the host. */
+int cgs_springs_step(cgs_ctx* ctx, float dt, uint32_t steps);
+/* trigger_jiggle_impulse(magnitude) on every spring cage (dynamics.rs:280-305). */
+int cgs_springs_impulse(cgs_ctx* ctx, float magnitude);
+/* Copies the device spring state back: current and velocity [num_verts*3]
+ * (either may be null). */
+int cgs_springs_read(cgs_ctx* ctx, float* current, float* velocity);
+
 /* Binds the resident rest scene to a tet cage on the GPU with the reference's
  * rule (first tet with barycentric violation <= 1e-4, else the least-violating
  * tet; TetMesh::bind_point, deformation/mod.rs:267-310). When use_bounds is
@@ -368,6 +409,34 @@ int cgs_invalidate(cgs_ctx* ctx);
  * *out_bytes receives the byte size of the valid contents. */
 int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_bytes,
                           uint64_t* out_bytes);
+
+/* ---- SH coefficient rotation and deformed-scene export ---- */
+
+/* Rotates n blocks of 48 SH coefficients (DC rgb, then 15 per channel) in
+ * device memory in place: block i by rotation d_index[i] (or i % num_rotations
+ * when d_index is null) of d_rotations [num_rotations * 9] (column-major),
+ * bands 1..min(degree, 3), each band by the f32 matrix
+ * (B_l T_l(R^T) B_l^+)^T with an f32 running sum. Replaces ShRotator::new +
+ * ShRotator::apply / rotate_sh_buffer (render/rasterizer/sh_rotation.rs:
+ * 403-471), with the per-rotation matrices built on the device. d_sh must be
+ * 16-byte aligned. An index at or above num_rotations leaves its block
+ * unchanged and returns CGS_E_ARG. */
+int cgs_sh_rotate(cgs_ctx* ctx, uint64_t n, float* d_sh, uint32_t num_rotations,
+                  const float* d_rotations, const uint32_t* d_index, uint32_t degree);
+
+/* The deformed scene of the last frame's Stage 1 as host arrays in the
+ * GaussianSceneSoa layout: pos [count*3], cov [count*6] (xx, xy, xz, yy, yz,
+ * zz), opa [count], sh [count*48]: the n rest Gaussians' deformed records
+ * then the split children, each splat's SH coefficients (a child's are its
+ * parent's) rotated by its tet's or polygon-cage slot's rotation up to
+ * sh_degree. Replaces Timeline::deform_scene_at + write_binary_ply_bytes'
+ * input (app/timeline.rs:205-275, the CPU's per-tet ShRotator in
+ * deformation/cpu_reference.rs:172-183) with the GPU frame's own deformation.
+ * Null output pointers are skipped; with all four null only *out_count is
+ * written. Without cages the rest scene is exported; with cages whose state
+ * changed after the last frame, CGS_E_STATE. */
+int cgs_export_deformed(cgs_ctx* ctx, uint32_t sh_degree, uint64_t capacity, float* pos, float* cov,
+                        float* opa, float* sh, uint64_t* out_count);
 
 /* ---- stage primitives on device memory (render/kernels/scan.rs, radix_sort.rs) ---- */
 

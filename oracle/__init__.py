@@ -98,6 +98,12 @@ def lib():
         L.orc_conic_extents.argtypes = [_c_f] * 4 + [_f32p, _i32p]
         L.orc_ref_tet_transforms.argtypes = [_c_u32, _f32p, _u32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_ref_sh_rotate.argtypes = [_c_u32, _f32p, _f32p, _c_u32]
+        L.orc_sh_rotation_matrix.argtypes = [_f32p, _c_u32, _f32p]
+        L.orc_spring_frame_damping.restype = _c_f
+        L.orc_spring_frame_damping.argtypes = [_c_f, _c_f]
+        L.orc_spring_step.argtypes = [_c_u32, _f32p, _f32p, _f32p, _vp, _c_f, _c_f, _c_f, _c_u32,
+                                      _vp, _c_f]
+        L.orc_spring_impulse.argtypes = [_c_u32, _f32p, _f32p, _vp, _c_f]
         L.orc_ref_frame.restype = _c_u64
         L.orc_ref_frame.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _c_u32, _vp, _vp, _vp, _vp,
                                     _vp, _f32p, _c_u32, _c_u32, _f32p, _f32p, _c_u32, _c_f, _c_f,
@@ -347,9 +353,52 @@ def ref_tet_transforms(verts, elems, inv_dm):
 
 
 def ref_sh_rotate(sh, R9, degree):
+    """ShRotator::new(R, degree).apply on every 48-coefficient block of `sh`
+    (render/rasterizer/sh_rotation.rs:389-440); R9 column-major."""
     out = _f32(sh).copy().ravel()
     lib().orc_ref_sh_rotate(out.size // 48, out, _f32(R9).ravel(), int(degree))
     return out
+
+
+def sh_rotation_matrix(R9, band):
+    """sh_rotation_matrix(R, band) (sh_rotation.rs:367-385): row-major
+    (2 band + 1)^2 float32 matrix; R9 column-major."""
+    n = 2 * int(band) + 1
+    out = np.zeros(n * n, np.float32)
+    lib().orc_sh_rotation_matrix(_f32(R9).ravel(), int(band), out)
+    return out.reshape(n, n)
+
+
+def spring_frame_damping(damping, dt) -> float:
+    """CageSpringSimulator::frame_damping (deformation/dynamics.rs:137-148)."""
+    return float(lib().orc_spring_frame_damping(float(damping), float(dt)))
+
+
+def spring_step(rest, cur, vel, pinned, stiffness, damping, mass, planes, dt):
+    """One CageSpringSimulator::step (dynamics.rs:249-277) of one cage; returns
+    new (current, velocity) [V,3]. planes [P,8]: nx ny nz offset restitution
+    friction pad pad."""
+    rest = _f32(rest).reshape(-1, 3)
+    c = _f32(cur).reshape(-1, 3).copy()
+    v = _f32(vel).reshape(-1, 3).copy()
+    pin = np.ascontiguousarray(pinned, np.uint8) if pinned is not None else None
+    pl = np.ascontiguousarray(planes, np.float32).reshape(-1, 8) if planes is not None and len(
+        planes) else None
+    lib().orc_spring_step(rest.shape[0], rest.ravel(), c.ravel(), v.ravel(),
+                          _ptr(pin) if pin is not None else None, float(stiffness), float(damping),
+                          float(mass), 0 if pl is None else pl.shape[0],
+                          _ptr(pl) if pl is not None else None, float(dt))
+    return c, v
+
+
+def spring_impulse(rest, vel, pinned, magnitude):
+    """CageSpringSimulator::trigger_jiggle_impulse (dynamics.rs:280-305)."""
+    rest = _f32(rest).reshape(-1, 3)
+    v = _f32(vel).reshape(-1, 3).copy()
+    pin = np.ascontiguousarray(pinned, np.uint8) if pinned is not None else None
+    lib().orc_spring_impulse(rest.shape[0], rest.ravel(), v.ravel(),
+                             _ptr(pin) if pin is not None else None, float(magnitude))
+    return v
 
 
 def ref_frame(scene, cam24, W, H, bg, cam_pos, sh_degree, cage=None, split_thr=0.0, mip=0.0):

@@ -740,96 +740,180 @@ M3 higham_polar(const M3& J) {
   return r;
 }
 
-// Real SH basis of eval_sh (render/rasterizer/sh.rs:29-137), bands 1-3, in f64.
-void sh_band(int l, const double* d, double* y) {
-  const double x = d[0], yy_ = d[1], z = d[2];
+// ShRotator (render/rasterizer/sh_rotation.rs:1-460). Real SH of band l are
+// homogeneous polynomials of degree l: Y_l(d) = B_l v_l(d) over the monomials
+// v_l, and v_l(R^T d) = T_l v_l(d). The band's rotation matrix is
+// M_l = (B_l T_l B_l^+)^T with B_l^+ = B_l^T (B_l B_l^T)^-1, built in f64 with
+// the reference's operation order (poly_mul_linear, mat_mul, Gauss-Jordan with
+// the last maximal pivot), rounded to f32, and applied to each channel's block
+// with an f32 running sum (apply_block).
+
+// Monomial order of exps_of (sh_rotation.rs:47-56): x exponent descending,
+// then y descending.
+int sh_exps(int d, int (*e)[3]) {
+  int k = 0;
+  for (int x = d; x >= 0; --x)
+    for (int y = d - x; y >= 0; --y) {
+      e[k][0] = x;
+      e[k][1] = y;
+      e[k][2] = d - x - y;
+      ++k;
+    }
+  return k;
+}
+int sh_exp_index(int d, const int* e) {
+  int k = 0;
+  for (int x = d; x > e[0]; --x) k += d - x + 1;
+  return k + (d - e[0] - e[1]);
+}
+
+// basis_rows (sh_rotation.rs:139-226) as integer monomial coefficients times
+// the band constants: B[row * m + mono].
+void sh_basis_rows(int l, double* B) {
+  const double C1 = 0.4886025119029199, C2_0 = 1.0925484305920792, C2_2 = 0.31539156525252005,
+               C2_4 = 0.5462742152960396, C3_0 = -0.5900435899266435, C3_1 = 2.890611442640554,
+               C3_2 = -0.4570457994644658, C3_3 = 0.3731763325901154, C3_5 = 1.445305721320277;
+  struct T { int row, mono; double k, c; };
+  static const T t1[] = {{0, 1, 1, 0}, {1, 2, 1, 0}, {2, 0, 1, 0}};
+  const int m = (l + 1) * (l + 2) / 2, n = 2 * l + 1;
+  for (int i = 0; i < n * m; ++i) B[i] = 0.0;
   if (l == 1) {
-    y[0] = -0.4886025119029199 * yy_; y[1] = 0.4886025119029199 * z; y[2] = -0.4886025119029199 * x;
+    const double c[3] = {-C1, C1, -C1};
+    for (const T& e : t1) B[e.row * m + e.mono] = e.k * c[e.row];
   } else if (l == 2) {
-    const double xx = x * x, yy = yy_ * yy_, zz = z * z;
-    y[0] = 1.0925484305920792 * x * yy_;
-    y[1] = -1.0925484305920792 * yy_ * z;
-    y[2] = 0.31539156525252005 * (2.0 * zz - xx - yy);
-    y[3] = -1.0925484305920792 * x * z;
-    y[4] = 0.5462742152960396 * (xx - yy);
+    // monomials xx xy xz yy yz zz
+    const T t[] = {{0, 1, 1, C2_0}, {1, 4, 1, -C2_0}, {2, 0, -1, C2_2}, {2, 3, -1, C2_2},
+                   {2, 5, 2, C2_2}, {3, 2, 1, -C2_0}, {4, 0, 1, C2_4}, {4, 3, -1, C2_4}};
+    for (const T& e : t) B[e.row * m + e.mono] = e.k * e.c;
   } else {
-    const double xx = x * x, yy = yy_ * yy_, zz = z * z;
-    y[0] = -0.5900435899266435 * yy_ * (3.0 * xx - yy);
-    y[1] = 2.890611442640554 * x * yy_ * z;
-    y[2] = -0.4570457994644658 * yy_ * (4.0 * zz - xx - yy);
-    y[3] = 0.3731763325901154 * z * (2.0 * zz - 3.0 * xx - 3.0 * yy);
-    y[4] = -0.4570457994644658 * x * (4.0 * zz - xx - yy);
-    y[5] = 1.445305721320277 * z * (xx - yy);
-    y[6] = -0.5900435899266435 * x * (xx - 3.0 * yy);
+    // monomials xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+    const T t[] = {{0, 1, 3, C3_0}, {0, 6, -1, C3_0}, {1, 4, 1, C3_1},  {2, 1, -1, C3_2},
+                   {2, 6, -1, C3_2}, {2, 8, 4, C3_2}, {3, 2, -3, C3_3}, {3, 7, -3, C3_3},
+                   {3, 9, 2, C3_3}, {4, 0, -1, C3_2}, {4, 3, -1, C3_2}, {4, 5, 4, C3_2},
+                   {5, 2, 1, C3_5}, {5, 7, -1, C3_5}, {6, 0, 1, C3_0},  {6, 3, -3, C3_0}};
+    for (const T& e : t) B[e.row * m + e.mono] = e.k * e.c;
   }
 }
 
-// Solves X A = B for X (n x n, n <= 7) by Gauss-Jordan with partial pivoting
-// on the transposed system A^T X^T = B^T.
-void solve_right(int n, const double* A, const double* B, double* X) {
-  double M[7][14];
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j) {
-      M[i][j] = A[j * n + i];       // A^T
-      M[i][n + j] = B[j * n + i];   // B^T
+// mat_mul (sh_rotation.rs:228-245): out[i][j] = sum over k of a[i][k] b[k][j],
+// k ascending, terms with a[i][k] == 0 skipped.
+void sh_mat_mul(int r, int inner, int c, const double* a, const double* b, double* out) {
+  for (int i = 0; i < r * c; ++i) out[i] = 0.0;
+  for (int i = 0; i < r; ++i)
+    for (int k = 0; k < inner; ++k) {
+      const double aik = a[i * inner + k];
+      if (aik == 0.0) continue;
+      for (int j = 0; j < c; ++j) out[i * c + j] += aik * b[k * c + j];
     }
+}
+
+// invert (sh_rotation.rs:260-300): Gauss-Jordan, pivot = the last row of
+// largest magnitude (Iterator::max_by), pivot row scaled by 1/pivot.
+bool sh_invert(int n, const double* A, double* out) {
+  double aug[10][20];
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < 2 * n; ++j) aug[i][j] = j < n ? A[i * n + j] : (j - n == i ? 1.0 : 0.0);
   for (int col = 0; col < n; ++col) {
     int piv = col;
     for (int r = col + 1; r < n; ++r)
-      if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
+      if (!(std::fabs(aug[piv][col]) > std::fabs(aug[r][col]))) piv = r;
+    if (std::fabs(aug[piv][col]) < 1e-12) return false;
     if (piv != col)
-      for (int j = 0; j < 2 * n; ++j) std::swap(M[col][j], M[piv][j]);
-    const double d = M[col][col];
-    for (int j = 0; j < 2 * n; ++j) M[col][j] /= d;
+      for (int j = 0; j < 2 * n; ++j) std::swap(aug[col][j], aug[piv][j]);
+    const double inv = 1.0 / aug[col][col];
+    for (int j = 0; j < 2 * n; ++j) aug[col][j] *= inv;
     for (int r = 0; r < n; ++r) {
       if (r == col) continue;
-      const double f = M[r][col];
-      for (int j = 0; j < 2 * n; ++j) M[r][j] -= f * M[col][j];
+      const double f = aug[r][col];
+      if (f == 0.0) continue;
+      for (int j = 0; j < 2 * n; ++j) aug[r][j] -= f * aug[col][j];
     }
   }
   for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j) X[j * n + i] = M[i][n + j];  // X = (X^T)^T
+    for (int j = 0; j < n; ++j) out[i * n + j] = aug[i][n + j];
+  return true;
 }
 
-// Coefficient rotation of ShRotator (render/rasterizer/sh_rotation.rs:372-460):
-// per band l, the matrix D_l with Y_l(R^T d) = D_l Y_l(d) for every d, found
-// from 2l+1 fixed directions (bands are rotation-invariant subspaces, so the
-// map is exact); rotated coefficients are c' = D_l^T c.
+// basis_for (sh_rotation.rs:307-330): B and B^+ = B^T (B B^T)^-1.
+struct ShBasis {
+  double B[70], P[70];
+};
+const ShBasis& sh_basis(int l) {
+  static ShBasis cache[3];
+  static bool ready[3] = {false, false, false};
+  ShBasis& b = cache[l - 1];
+  if (!ready[l - 1]) {
+    const int m = (l + 1) * (l + 2) / 2, n = 2 * l + 1;
+    sh_basis_rows(l, b.B);
+    double Bt[70], G[49], Gi[49];
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < m; ++j) Bt[j * n + i] = b.B[i * m + j];
+    sh_mat_mul(n, m, n, b.B, Bt, G);
+    sh_invert(n, G, Gi);
+    sh_mat_mul(m, n, n, Bt, Gi, b.P);
+    ready[l - 1] = true;
+  }
+  return b;
+}
+
+// poly_mul_linear (sh_rotation.rs:332-352).
+void sh_poly_mul_linear(const double* a, int deg, const double* lf, double* out) {
+  int ea[10][3];
+  const int na = sh_exps(deg, ea), nd = (deg + 2) * (deg + 3) / 2;
+  for (int k = 0; k < nd; ++k) out[k] = 0.0;
+  for (int ia = 0; ia < na; ++ia) {
+    const double coeff = a[ia];
+    if (coeff == 0.0) continue;
+    for (int ax = 0; ax < 3; ++ax) {
+      if (lf[ax] == 0.0) continue;
+      int ne[3] = {ea[ia][0], ea[ia][1], ea[ia][2]};
+      ne[ax] += 1;
+      out[sh_exp_index(deg + 1, ne)] += coeff * lf[ax];
+    }
+  }
+}
+
+// sh_rotation_matrix (sh_rotation.rs:354-387): row-major f32 M_l.
+void sh_rotation_matrix(const M3& R, int l, float* M) {
+  const int m = (l + 1) * (l + 2) / 2, n = 2 * l + 1;
+  // monomial_transform: the linear forms are the columns of R (rows of R^T).
+  double lf[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int k = 0; k < 3; ++k) lf[a][k] = (double)R.at(a, k);
+  int ex[10][3];
+  sh_exps(l, ex);
+  double T[100];
+  for (int row = 0; row < m; ++row) {
+    double poly[10] = {1.0}, next[10];
+    int deg = 0;
+    for (int a = 0; a < 3; ++a)
+      for (int rep = 0; rep < ex[row][a]; ++rep) {
+        sh_poly_mul_linear(poly, deg, lf[a], next);
+        ++deg;
+        for (int k = 0; k < (deg + 1) * (deg + 2) / 2; ++k) poly[k] = next[k];
+      }
+    for (int k = 0; k < m; ++k) T[row * m + k] = poly[k];
+  }
+  const ShBasis& b = sh_basis(l);
+  double C[70], D[49];
+  sh_mat_mul(n, m, m, b.B, T, C);
+  sh_mat_mul(n, m, n, C, b.P, D);
+  for (int row = 0; row < n; ++row)
+    for (int col = 0; col < n; ++col) M[row * n + col] = (float)D[col * n + row];
+}
+
 struct ShRot {
-  double D[3][49];
+  float M[3][49];
   int degree;
 };
 ShRot make_sh_rotator(const M3& R, int degree) {
   ShRot out;
-  out.degree = degree;
-  static const double dirs[7][3] = {{0.267, 0.535, 0.802}, {-0.707, 0.1, 0.7},
-                                    {0.3, -0.9, 0.316}, {0.9, 0.3, -0.316},
-                                    {-0.2, -0.4, -0.894}, {0.577, -0.577, 0.577},
-                                    {0.1, 0.95, -0.296}};
-  for (int l = 1; l <= degree; ++l) {
-    const int n = 2 * l + 1;
-    double Y[49], Z[49];
-    for (int k = 0; k < n; ++k) {
-      double d[3], inv;
-      inv = 1.0 / std::sqrt(dirs[k][0] * dirs[k][0] + dirs[k][1] * dirs[k][1] + dirs[k][2] * dirs[k][2]);
-      for (int j = 0; j < 3; ++j) d[j] = dirs[k][j] * inv;
-      double rd[3];  // R^T d
-      for (int j = 0; j < 3; ++j)
-        rd[j] = (double)R.at(j, 0) * d[0] + (double)R.at(j, 1) * d[1] + (double)R.at(j, 2) * d[2];
-      double yv[7], zv[7];
-      sh_band(l, d, yv);
-      sh_band(l, rd, zv);
-      for (int i = 0; i < n; ++i) {
-        Y[k * n + i] = yv[i];  // column k
-        Z[k * n + i] = zv[i];
-      }
-    }
-    // D Y = Z  ->  D = Z Y^-1
-    solve_right(n, Y, Z, out.D[l - 1]);
-  }
+  out.degree = degree < 0 ? 0 : (degree > 3 ? 3 : degree);
+  for (int l = 1; l <= out.degree; ++l) sh_rotation_matrix(R, l, out.M[l - 1]);
   return out;
 }
 
+// ShRotator::apply / apply_block (sh_rotation.rs:389-440).
 void apply_sh_rotation(const ShRot& r, float* c48) {
   static const int starts[3] = {0, 3, 8};
   for (int ch = 0; ch < 3; ++ch) {
@@ -837,13 +921,13 @@ void apply_sh_rotation(const ShRot& r, float* c48) {
     for (int l = 1; l <= r.degree; ++l) {
       const int n = 2 * l + 1;
       float* c = rest + starts[l - 1];
-      double out[7];
-      for (int j = 0; j < n; ++j) {
-        double acc = 0.0;
-        for (int i = 0; i < n; ++i) acc += r.D[l - 1][j * n + i] * c[i];  // (D^T c)_j
-        out[j] = acc;
+      float out[7];
+      for (int row = 0; row < n; ++row) {
+        float acc = 0.0f;
+        for (int col = 0; col < n; ++col) acc += r.M[l - 1][row * n + col] * c[col];
+        out[row] = acc;
       }
-      for (int j = 0; j < n; ++j) c[j] = (float)out[j];
+      for (int j = 0; j < n; ++j) c[j] = out[j];
     }
   }
 }
@@ -1595,6 +1679,14 @@ void orc_ref_tet_transforms(uint32_t T, const float* verts, const uint32_t* elem
   }
 }
 
+// sh_rotation_matrix (sh_rotation.rs:367-385) for band l in 1..3: the row-major
+// (2l+1)^2 f32 matrix for rotation R (column-major 9).
+void orc_sh_rotation_matrix(const float* R9, uint32_t l, float* out) {
+  M3 R;
+  std::memcpy(R.c, R9, 36);
+  sh_rotation_matrix(R, (int)l, out);
+}
+
 // Rotates SH coefficients [n*48] in place by rotation R (column-major 9) up to
 // `degree` (ShRotator::apply).
 void orc_ref_sh_rotate(uint32_t n, float* sh, const float* R9, uint32_t degree) {
@@ -1935,6 +2027,99 @@ uint32_t orc_mvc_deform(uint32_t n, const float* pos, const float* cov, const fl
   if (out_opa) std::memcpy(out_opa, A.data(), 4 * (size_t)total);
   if (out_parent && !parent.empty()) std::memcpy(out_parent, parent.data(), 4 * parent.size());
   return total;
+}
+
+
+// ------------------------------------------------------------ cage springs
+// CageSpringSimulator (deformation/dynamics.rs:75-313) for one cage: rest,
+// current and velocity [V*3], pinned [V] (0/1), collision planes [P*8]
+// (nx, ny, nz, offset, restitution, friction, pad, pad).
+
+static float spring_min(float a, float b) {  // f32::min: NaN yields the other
+  if (std::isnan(a)) return b;
+  if (std::isnan(b)) return a;
+  return a < b ? a : b;
+}
+static float spring_max(float a, float b) {
+  if (std::isnan(a)) return b;
+  if (std::isnan(b)) return a;
+  return a > b ? a : b;
+}
+// damping_coefficient / frame_damping (dynamics.rs:137-148)
+float orc_spring_frame_damping(float damping, float dt) {
+  float r = damping;
+  if (r < 1.0e-4f) r = 1.0e-4f;
+  if (r > 0.9999f) r = 0.9999f;
+  const float c = -logf(r) * 60.0f;
+  return expf(-c * dt);
+}
+
+// CollisionPlane::resolve_contact (dynamics.rs:57-71).
+static void spring_contact(const float* pl, float* p, float* v) {
+  const float d = ((pl[0] * p[0] + pl[1] * p[1]) + pl[2] * p[2]) - pl[3];
+  if (d >= 0.0f) return;
+  for (int k = 0; k < 3; ++k) p[k] = p[k] - pl[k] * d;
+  const float vn = (v[0] * pl[0] + v[1] * pl[1]) + v[2] * pl[2];
+  if (vn < 0.0f) {
+    float vnorm[3], vtan[3];
+    for (int k = 0; k < 3; ++k) vnorm[k] = pl[k] * vn;
+    for (int k = 0; k < 3; ++k) vtan[k] = v[k] - vnorm[k];
+    const float keep = 1.0f - pl[5];
+    for (int k = 0; k < 3; ++k) v[k] = vtan[k] * keep - vnorm[k] * pl[4];
+  }
+}
+
+// CageSpringSimulator::step (dynamics.rs:249-277).
+void orc_spring_step(uint32_t V, const float* rest, float* cur, float* vel, const uint8_t* pinned,
+                     float stiffness, float damping, float mass, uint32_t num_planes,
+                     const float* planes, float dt) {
+  const float dt_sim = spring_min(dt, 0.033f);
+  if (!(dt_sim > 0.0f)) return;
+  const float inv_mass = 1.0f / spring_max(mass, 0.001f);
+  const float gamma = orc_spring_frame_damping(damping, dt_sim);
+  const float kim = stiffness * inv_mass;
+  for (uint32_t i = 0; i < V; ++i) {
+    float* x = cur + 3 * (size_t)i;
+    float* v = vel + 3 * (size_t)i;
+    if (pinned && pinned[i]) {
+      v[0] = v[1] = v[2] = 0.0f;
+      continue;
+    }
+    for (int k = 0; k < 3; ++k) {
+      const float accel = (rest[3 * (size_t)i + k] - x[k]) * kim;
+      v[k] = (v[k] + accel * dt_sim) * gamma;
+      x[k] = x[k] + v[k] * dt_sim;
+    }
+    for (uint32_t q = 0; q < num_planes; ++q) spring_contact(planes + 8 * (size_t)q, x, v);
+  }
+}
+
+// CageSpringSimulator::trigger_jiggle_impulse (dynamics.rs:280-305).
+void orc_spring_impulse(uint32_t V, const float* rest, float* vel, const uint8_t* pinned,
+                        float magnitude) {
+  if (V == 0) return;
+  float c[3] = {0.0f, 0.0f, 0.0f};
+  for (uint32_t i = 0; i < V; ++i)
+    for (int k = 0; k < 3; ++k) c[k] = c[k] + rest[3 * (size_t)i + k];
+  for (int k = 0; k < 3; ++k) c[k] = c[k] / (float)V;
+  for (uint32_t i = 0; i < V; ++i) {
+    if (pinned && pinned[i]) continue;
+    float d[3];
+    for (int k = 0; k < 3; ++k) d[k] = rest[3 * (size_t)i + k] - c[k];
+    const float rcp = 1.0f / sqrtf((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+    float r[3] = {0.0f, 0.0f, 0.0f};  // normalize_or_zero
+    if (std::isfinite(rcp) && rcp > 0.0f)
+      for (int k = 0; k < 3; ++k) r[k] = d[k] * rcp;
+    float imp[3];
+    if ((r[0] * r[0] + r[1] * r[1]) + r[2] * r[2] > 1e-4f) {
+      for (int k = 0; k < 3; ++k) imp[k] = r[k] * magnitude;
+    } else {
+      imp[0] = 0.0f * magnitude;
+      imp[1] = 1.0f * magnitude;
+      imp[2] = 0.0f * magnitude;
+    }
+    for (int k = 0; k < 3; ++k) vel[3 * (size_t)i + k] = vel[3 * (size_t)i + k] + imp[k];
+  }
 }
 
 }  // extern "C"
