@@ -62,7 +62,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 def radix_digits(args) -> str:
     """Digit widths of the entry sort's passes over the tile bits, e.g. "7+6"."""
-    tiles = ((args.width + 15) // 16) * ((args.height + 15) // 16)
+    tw, th = {0: (16, 16), 1: (8, 8), 2: (32, 16)}[getattr(args, "tile_shape", 0)]
+    tiles = ((args.width + tw - 1) // tw) * ((args.height + th - 1) // th)
     tile_bits = max(1, (tiles - 1).bit_length())
     rb = args.radix_bits
     if rb == 0:
@@ -96,6 +97,8 @@ def parse():
                     help="tile-entry sort: 0 auto, 1 radix passes, 2 one-pass tile transpose")
     ap.add_argument("--radix-bits", type=int, default=0,
                     help="entry-sort digit width (0 = balanced digits of at most 8 bits)")
+    ap.add_argument("--tile-shape", type=int, default=0,
+                    help="screen tile: 0 = 16x16 (the reference's), 1 = 8x8, 2 = 32x16")
     return ap.parse_args()
 
 
@@ -207,6 +210,7 @@ def config_dict(args, wl, world):
             "cage": "5x5x5 cubes x 6 tets (750 tets, 216 vertices), springs k=40 c=4 dt=1/60",
             "sh_degree": 3, "keys": "32-bit tile|depth", "radix_digits": radix_digits(args),
             "entry_sort": ["auto (radix)", "radix", "tile transpose"][args.entry_sort],
+            "tile": ["16x16", "8x8", "32x16"][args.tile_shape],
             "l2": "inputs larger than L2 (resident scene 255 MB + 26M tile entries)",
             "parallelism": f"replicas x{world} (views sharded, no exchange)"}
 
@@ -268,7 +272,7 @@ def run_ours(args):
                                     wl.strain_split_threshold, wl.mip_filter_3d_var,
                                     1.0 / 255.0, 0.5, profile_stages=profile,
                                     stage_timings=timings, radix_bits=args.radix_bits,
-                                    entry_sort=args.entry_sort)
+                                    entry_sort=args.entry_sort, tile_shape=args.tile_shape)
 
     for _ in range(max(args.warmup, 3)):
         render()
@@ -322,7 +326,8 @@ def run_ours(args):
         cam_c = wl.compositor(cam)
         st.execute_frame_gpu(wl.scene, cages, cam, cam_c, wl.strain_split_threshold,
                              wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, radix_bits=args.radix_bits,
-                             entry_sort=args.entry_sort, stage_timings=False)
+                             entry_sort=args.entry_sort, tile_shape=args.tile_shape,
+                             stage_timings=False)
         wl.step()
         next_verts = wl.cage.vertices()
         st._check(st._lib.cgs_readback_rgba8(st.handle, ctypes.c_void_p(out_np.ctypes.data),
@@ -574,21 +579,22 @@ def run_views(args):
     cages = wl.bind(st)
     imgs = st.view_images(comps)
     pixels = sum(c.screen_width * c.screen_height for c in comps)
-    from cindergs_b200 import autotune
+    from cindergs_b200 import _abi, autotune
     wl.step()
     tuned = autotune.tune_views(st, wl.scene, cages, cams, comps)
-    rbs, ess = autotune.per_view(tuned, comps)
+    tss, rbs, ess = autotune.per_view(tuned, comps)
 
     def per_view_frames():
         wl.step()
         for v, (cam, comp) in enumerate(zip(cams, comps)):
             st.execute_frame_gpu(wl.scene, cages, cam, comp, force_stage3=True,
-                                 stage_timings=False, radix_bits=rbs[v], entry_sort=ess[v])
+                                 stage_timings=False, radix_bits=rbs[v], entry_sort=ess[v],
+                                 tile_shape=tss[v])
 
     def batched(graph):
         wl.step()
         return st.execute_views(wl.scene, cages, cams, comps, imgs, use_graph=graph,
-                                radix_bits=rbs, entry_sort=ess)
+                                radix_bits=rbs, entry_sort=ess, tile_shape=tss)
 
     def timed(fn):
         for _ in range(max(args.warmup, 3)):
@@ -610,7 +616,7 @@ def run_views(args):
     wl.step()
     for v, (cam, comp) in enumerate(zip(cams, comps)):
         st.execute_frame_gpu(wl.scene, cages, cam, comp, force_stage3=True, stage_timings=True,
-                             radix_bits=rbs[v], entry_sort=ess[v])
+                             radix_bits=rbs[v], entry_sort=ess[v], tile_shape=tss[v])
     clock = ClockSampler(0)
     with clock:
         plain_ms, plain_wall, _ = timed(per_view_frames)
@@ -650,8 +656,9 @@ def run_views(args):
                              "graph": graph_wall},
         "speedup_graph_vs_per_view_frames": plain_ms / graph_ms,
         "graph_replays": replays,
-        "autotuned": {f"{w}x{h}": {"radix_bits": rb, "entry_sort": ["auto", "radix", "transpose"][es],
-                                  "stage3_ms": ms} for (w, h), (rb, es, ms) in tuned.items()},
+        "autotuned": {f"{w}x{h}": {"tile": "x".join(map(str, _abi.TILE_SHAPES[ts])),
+                                  "radix_bits": rb, "entry_sort": ["auto", "radix", "transpose"][es],
+                                  "stage34_ms": ms} for (w, h), (ts, rb, es, ms) in tuned.items()},
         "tile_entries_per_step": gst[-1]["total_tile_entries"] if gst else None,
         "cpu_baseline": cpu,
         "clocks": clock.summary(),

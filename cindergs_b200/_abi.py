@@ -70,7 +70,7 @@ class CgsFrameParams(ctypes.Structure):
     _fields_ = [("strain_split_threshold", ctypes.c_float), ("mip_filter_3d_var", ctypes.c_float),
                 ("min_opacity", ctypes.c_float), ("min_radius_px", ctypes.c_float),
                 ("profile_stages", _i32), ("force_stage3", _i32), ("write_f32", _i32),
-                ("radix_bits", _i32), ("entry_sort", _i32)]
+                ("radix_bits", _i32), ("entry_sort", _i32), ("tile_shape", _i32)]
 
 
 class CgsStageTimings(ctypes.Structure):
@@ -83,6 +83,8 @@ class CgsStageTimings(ctypes.Structure):
 
 
 SORT_AUTO, SORT_RADIX, SORT_TRANSPOSE = 0, 1, 2
+TILE_16X16, TILE_8X8, TILE_32X16 = 0, 1, 2
+TILE_SHAPES = {TILE_16X16: (16, 16), TILE_8X8: (8, 8), TILE_32X16: (32, 16)}
 FIELD_PER_FRAME = 1
 
 KERNEL_NAMES = ["clear", "tet_transforms", "deform", "project", "bin", "entry_sort",

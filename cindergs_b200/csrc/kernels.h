@@ -231,6 +231,7 @@ struct BinArgs {
   uint32_t n_rest;
   uint32_t max_n;
   uint32_t width, height, tiles_x, tiles_y;
+  uint32_t tile_w_log2, tile_h_log2;  // screen tile shape (8x8, 16x16 or 32x16 pixels)
   // per slot (depth order): the counting kernel writes the tile count, the
   // scan turns it into the first entry in place
   uint32_t* offsets;            // [max_n]
@@ -394,6 +395,7 @@ struct CompositeArgs {
   const uint32_t* sorted_ids;
   const uint32_t* ranges;
   uint32_t width, height, tiles_x, tiles_y;
+  uint32_t tile_w_log2, tile_h_log2;  // screen tile shape: 8x8, 16x16 or 32x16 pixels
   uint32_t pitch_px;        // RGBA8 row pitch in pixels
   float bg[4];
   uint32_t* out_rgba8;

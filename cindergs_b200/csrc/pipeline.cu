@@ -80,6 +80,7 @@ float bitsf(uint32_t u) {
 // tile entries overflowed the key buffers can be binned and composited again.
 struct FrameDesc {
   uint32_t W = 0, H = 0, tiles_x = 0, tiles_y = 0, total_tiles = 0, pitch = 0;
+  uint32_t tile_lw = 4, tile_lh = 4;  // log2 of the screen tile's width and height
   uint32_t n = 0, max_n = 0;
   bool split_possible = false, key64 = false, write_f32 = false;
   uint32_t tile_bits = 0, depth_bits = 0, sort_bits = 0, radix_bits = 8, depth_base_bits = 0;
@@ -446,6 +447,8 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.height = d.H;
   b.tiles_x = d.tiles_x;
   b.tiles_y = d.tiles_y;
+  b.tile_w_log2 = d.tile_lw;
+  b.tile_h_log2 = d.tile_lh;
   b.offsets = ctx->offsets.as<uint32_t>();
   b.tile_stage = (uint32_t*)(sc + L.btile);
   b.tile_count = b.tile_stage + (size_t)8 * ((d.max_n + 31) / 32);
@@ -562,6 +565,8 @@ int enqueue_stage4(cgs_ctx* ctx, const FrameDesc& d, int result_src) {
   c.height = d.H;
   c.tiles_x = d.tiles_x;
   c.tiles_y = d.tiles_y;
+  c.tile_w_log2 = d.tile_lw;
+  c.tile_h_log2 = d.tile_lh;
   c.pitch_px = d.out_rgba8 ? d.out_pitch : d.pitch;
   std::memcpy(c.bg, d.bg, 16);
   c.out_rgba8 = d.out_rgba8 ? d.out_rgba8 : ctx->fb_rgba8.as<uint32_t>();
@@ -1672,6 +1677,17 @@ int cgs_bind_tets(cgs_ctx* ctx, uint32_t num_tets, const uint32_t* elems, const 
 
 namespace {
 
+// log2 of the screen tile's width and height for CGS_TILE_* (the reference's
+// 16x16 for 0); false for an unknown shape.
+bool tile_shape_log2(int32_t shape, uint32_t* lw, uint32_t* lh) {
+  switch (shape) {
+    case CGS_TILE_16X16: *lw = 4; *lh = 4; return true;
+    case CGS_TILE_8X8: *lw = 3; *lh = 3; return true;
+    case CGS_TILE_32X16: *lw = 5; *lh = 4; return true;
+    default: return false;
+  }
+}
+
 // How a frame is enqueued (cgs_execute_frame, cgs_execute_views).
 struct FrameCtl {
   bool allow_cache = true;     // may reuse the cached Stage 3 lists
@@ -1697,9 +1713,12 @@ int check_frame_args(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composito
     return ctx->fail(CGS_E_ARG, "radix_bits must be 0 or 4..8");
   if (params->entry_sort < CGS_SORT_AUTO || params->entry_sort > CGS_SORT_TRANSPOSE)
     return ctx->fail(CGS_E_ARG, "entry_sort must be one of CGS_SORT_*");
+  uint32_t lw = 4, lh = 4;
+  if (!tile_shape_log2(params->tile_shape, &lw, &lh))
+    return ctx->fail(CGS_E_ARG, "tile_shape must be one of CGS_TILE_*");
   const uint32_t W = comp->screen_width ? comp->screen_width : 1u;
   const uint32_t H = comp->screen_height ? comp->screen_height : 1u;
-  const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+  const uint32_t tiles_x = (W + (1u << lw) - 1) >> lw, tiles_y = (H + (1u << lh) - 1) >> lh;
   const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
   if (total_tiles64 > 0xFFFFFFFFull / 2) return ctx->fail(CGS_E_CAPACITY, "viewport too large");
   if (W >= (1u << 22) || H >= (1u << 22))
@@ -1715,9 +1734,11 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
   cudaStream_t s = ctx->stream;
   const uint32_t W = comp->screen_width ? comp->screen_width : 1u;
   const uint32_t H = comp->screen_height ? comp->screen_height : 1u;
-  const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
-  const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
   FrameDesc d;
+  tile_shape_log2(params->tile_shape, &d.tile_lw, &d.tile_lh);  // validated by the caller
+  const uint32_t tiles_x = (W + (1u << d.tile_lw) - 1) >> d.tile_lw;
+  const uint32_t tiles_y = (H + (1u << d.tile_lh) - 1) >> d.tile_lh;
+  const uint64_t total_tiles64 = (uint64_t)tiles_x * tiles_y;
   d.W = W;
   d.H = H;
   d.tiles_x = tiles_x;
@@ -1797,7 +1818,7 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
   key.mip = mip_bits;
   key.min_opa = fbits(params->min_opacity);
   key.min_rad = fbits(params->min_radius_px);
-  key.radix_bits = d.radix_bits | ((uint32_t)d.entry_sort << 8);
+  key.radix_bits = d.radix_bits | ((uint32_t)d.entry_sort << 8) | (d.tile_lw << 16) | (d.tile_lh << 20);
   bool cached = ctl.allow_cache && !params->force_stage3 && ctx->s3_valid && ctx->s3_key == key;
   if (cached) {
     CGS_TRY(drain(ctx, true));
@@ -2241,9 +2262,13 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
     if (use_graph) {
       // grow the key buffers to the capacity the graph will be captured with
       bool key64 = false;
-      for (uint32_t v = 0; v < num_views; ++v)
-        key64 = key64 || (uint64_t)((comps[v].screen_width + 15) / 16) *
-                                 ((comps[v].screen_height + 15) / 16) > 65535u;
+      for (uint32_t v = 0; v < num_views; ++v) {
+        uint32_t lw = 4, lh = 4;
+        tile_shape_log2(prm[v].tile_shape, &lw, &lh);
+        const uint64_t W = comps[v].screen_width ? comps[v].screen_width : 1u;
+        const uint64_t H = comps[v].screen_height ? comps[v].screen_height : 1u;
+        key64 = key64 || ((W + (1u << lw) - 1) >> lw) * ((H + (1u << lh) - 1) >> lh) > 65535u;
+      }
       CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, key64, ctx->radix_lb_bits ? ctx->radix_lb_bits : 8));
       CGS_TRY(capture_views(ctx, num_views, cameras, comps, prm.data(), d_rgba8));
       ctx->views_key = key_of();

@@ -53,9 +53,10 @@ struct SplatBox {
   float mu_x, mu_y, ca, cb, cc, alpha;
 };
 
-__device__ __forceinline__ uint32_t tile_coord(float v, int32_t hi) {
-  // clamp(floor(v / 16) as i32, 0, hi) with Rust's saturating cast.
-  const float f = floorf(v / 16.0f);
+__device__ __forceinline__ uint32_t tile_coord(float v, int32_t hi, float tile_px) {
+  // clamp(floor(v / tile) as i32, 0, hi) with Rust's saturating cast; the
+  // tile size is a power of two, so the division is exact.
+  const float f = floorf(v / tile_px);
   int32_t i = __float2int_rz(f);  // saturates, NaN -> 0
   i = i < 0 ? 0 : (i > hi ? hi : i);
   return (uint32_t)i;
@@ -79,10 +80,11 @@ __device__ __forceinline__ SplatBox load_box(const BinArgs& a, uint32_t s, uint3
   b.cc = cc4.x;
   b.alpha = cc4.y;
   const int32_t mx = (int32_t)a.tiles_x - 1, my = (int32_t)a.tiles_y - 1;
-  b.x0 = tile_coord(b.mu_x - ext_x, mx);
-  b.x1 = tile_coord(b.mu_x + ext_x, mx);
-  b.y0 = tile_coord(b.mu_y - ext_y, my);
-  b.y1 = tile_coord(b.mu_y + ext_y, my);
+  const float tw = (float)(1u << a.tile_w_log2), th = (float)(1u << a.tile_h_log2);
+  b.x0 = tile_coord(b.mu_x - ext_x, mx, tw);
+  b.x1 = tile_coord(b.mu_x + ext_x, mx, tw);
+  b.y0 = tile_coord(b.mu_y - ext_y, my, th);
+  b.y1 = tile_coord(b.mu_y + ext_y, my, th);
   // ellipse_intersects_tile_gpu returns false for every tile when alpha < 1/255.
   b.valid = !(b.alpha < (1.0f / 255.0f));
   return b;
@@ -126,13 +128,13 @@ __device__ __forceinline__ float div_rcp64(float n, float d, double y) {
 // 1e-12), max(c, 1e-12)), rcp = their binary64 reciprocals (c term, a term),
 // qlim = q_max + 1e-4.
 __device__ __forceinline__ bool tile_hit(uint32_t tx, uint32_t ty, uint32_t wm1, uint32_t hm1,
-                                         const float4 geo, const float4 con, const double2 rcp,
-                                         float qlim) {
-  const uint32_t xs = tx << 4, ys = ty << 4;
+                                         uint32_t lw, uint32_t lh, const float4 geo,
+                                         const float4 con, const double2 rcp, float qlim) {
+  const uint32_t xs = tx << lw, ys = ty << lh;
   const float dx0 = pixel_center(xs) - geo.x;
-  const float dx1 = pixel_center(min(xs + 15u, wm1)) - geo.x;
+  const float dx1 = pixel_center(min(xs + ((1u << lw) - 1u), wm1)) - geo.x;
   const float dy0 = pixel_center(ys) - geo.y;
-  const float dy1 = pixel_center(min(ys + 15u, hm1)) - geo.y;
+  const float dy1 = pixel_center(min(ys + ((1u << lh) - 1u), hm1)) - geo.y;
   const float x_near = clampf(0.0f, dx0, dx1);
   const float y1 = clampf(div_rcp64(geo.z * x_near, con.w, rcp.x), dy0, dy1);
   const float q1 = con.x * x_near * x_near + geo.w * x_near * y1 + con.y * y1 * y1;
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
         const uint32_t ci = item - wbase[o];
         uint32_t tx, ty;
         box_tile(sp.box[warp][o], ci, tx, ty);
-        hit = tile_hit(tx, ty, wm1, hm1, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
+        hit = tile_hit(tx, ty, wm1, hm1, a.tile_w_log2, a.tile_h_log2, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
                        sp.qlim[warp][o]);
         rec = ((KEY64 ? ci : ty * a.tiles_x + tx) << 5) | (uint32_t)o;
       }
@@ -371,7 +373,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
               const int o = find_owner(wbase, item);
               uint32_t tx, ty;
               box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
-              hit = tile_hit(tx, ty, wm1, hm1, sp.geo[warp][o], sp.con[warp][o],
+              hit = tile_hit(tx, ty, wm1, hm1, a.tile_w_log2, a.tile_h_log2, sp.geo[warp][o], sp.con[warp][o],
                              sp.rcp[warp][o], sp.qlim[warp][o]);
             }
             hits = __ballot_sync(0xffffffffu, hit);
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
             const int o = find_owner(wbase, item);
             uint32_t tx, ty;
             box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
-            hit = tile_hit(tx, ty, wm1, hm1, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
+            hit = tile_hit(tx, ty, wm1, hm1, a.tile_w_log2, a.tile_h_log2, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
                            sp.qlim[warp][o]);
           }
           hits = __ballot_sync(0xffffffffu, hit);

@@ -1,8 +1,10 @@
-// Stage 4: 16x16 tile compositor on sm_100a (tile_compositor_v2_kernel,
-// render/kernels/compositor.rs:727-883).
+// Stage 4: tile compositor on sm_100a (tile_compositor_v2_kernel,
+// render/kernels/compositor.rs:727-883) for 16x16 tiles (the reference's)
+// and 8x8 or 32x16 tiles (the autotuner's other shapes).
 //
-// One block of 256 threads per screen tile, one pixel per thread. The tile's
-// depth-sorted splat list is consumed in batches of 256: each batch's 48-byte
+// One block per screen tile, one pixel per thread (64, 256 or 512 threads).
+// The tile's depth-sorted splat list is consumed in batches of 256: each
+// batch's 48-byte
 // splat records are gathered from the Stage 2 record array into shared memory
 // by the Tensor Memory Accelerator's bulk-copy engine (one cp.async.bulk per
 // record, all completing on one mbarrier with an expected byte count), double
@@ -26,7 +28,6 @@
 namespace cgs {
 namespace {
 
-constexpr int kCompThreads = 256;
 constexpr int kBatch = 256;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -72,13 +73,15 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
-__global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs a) {
+template <int LW, int LH>
+__global__ void __launch_bounds__(1 << (LW + LH)) k_composite(const CompositeArgs a) {
+  constexpr uint32_t TW = 1u << LW, TH = 1u << LH, kCompThreads = TW * TH;
   __shared__ __align__(128) SplatRec s_rec[2][kBatch];
   __shared__ __align__(8) uint64_t s_bar[2];
 
   const uint32_t tid = threadIdx.x;
-  const uint32_t px = blockIdx.x * 16u + (tid & 15u);
-  const uint32_t py = blockIdx.y * 16u + (tid >> 4);
+  const uint32_t px = blockIdx.x * TW + (tid & (TW - 1u));
+  const uint32_t py = blockIdx.y * TH + (tid >> LW);
   const bool inside = px < a.width && py < a.height;
   const uint32_t tile_id = blockIdx.y * a.tiles_x + blockIdx.x;
   const uint32_t rs = min(a.ranges[2 * (size_t)tile_id], a.num_entries);
@@ -98,14 +101,14 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
     const uint32_t stage = b & 1u;
     const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
     if (tid == 0) mbar_arrive_expect_tx(&s_bar[stage], cnt * (uint32_t)sizeof(SplatRec));
-    if (tid < cnt) {
-      uint32_t id = a.sorted_ids[rs + b * kBatch + tid];
+    for (uint32_t k = tid; k < cnt; k += kCompThreads) {
+      uint32_t id = a.sorted_ids[rs + b * kBatch + k];
       if (id >= a.num_recs) {  // never let a bad id become an out-of-bounds copy
         if (a.fc) atomicOr(&a.fc->status, kStatusCapacity);
         id = 0;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      bulk_copy_g2s(&s_rec[stage][tid], a.recs + id, (uint32_t)sizeof(SplatRec), &s_bar[stage]);
+      bulk_copy_g2s(&s_rec[stage][k], a.recs + id, (uint32_t)sizeof(SplatRec), &s_bar[stage]);
     }
   };
 
@@ -121,8 +124,8 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
   float pcx = (float)px + 0.5f, pcy = (float)py + 0.5f;
 
   auto finalize = [&](int p, float r_, float g_, float b_, float t_) {
-    const uint32_t x = blockIdx.x * 16u + ((uint32_t)p & 15u);
-    const uint32_t y = blockIdx.y * 16u + ((uint32_t)p >> 4);
+    const uint32_t x = blockIdx.x * TW + ((uint32_t)p & (TW - 1u));
+    const uint32_t y = blockIdx.y * TH + ((uint32_t)p >> LW);
     const float fr = clampf(r_ + t_ * a.bg[0], 0.0f, 1.0f);
     const float fg = clampf(g_ + t_ * a.bg[1], 0.0f, 1.0f);
     const float fb = clampf(b_ + t_ * a.bg[2], 0.0f, 1.0f);
@@ -219,8 +222,8 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
         cg = acc.y;
         cb = acc.z;
         t = acc.w;
-        pcx = (float)(blockIdx.x * 16u + ((uint32_t)pix & 15u)) + 0.5f;
-        pcy = (float)(blockIdx.y * 16u + ((uint32_t)pix >> 4)) + 0.5f;
+        pcx = (float)(blockIdx.x * TW + ((uint32_t)pix & (TW - 1u))) + 0.5f;
+        pcy = (float)(blockIdx.y * TH + ((uint32_t)pix >> LW)) + 0.5f;
       } else {
         pix = -1;
       }
@@ -239,7 +242,14 @@ __global__ void __launch_bounds__(kCompThreads) k_composite(const CompositeArgs 
 cudaError_t launch_composite(const CompositeArgs& a, cudaStream_t s) {
   if (a.tiles_x == 0 || a.tiles_y == 0) return cudaSuccess;
   dim3 grid(a.tiles_x, a.tiles_y);
-  k_composite<<<grid, kCompThreads, 0, s>>>(a);
+  if (a.tile_w_log2 == 3 && a.tile_h_log2 == 3)
+    k_composite<3, 3><<<grid, 64, 0, s>>>(a);
+  else if (a.tile_w_log2 == 5 && a.tile_h_log2 == 4)
+    k_composite<5, 4><<<grid, 512, 0, s>>>(a);
+  else if (a.tile_w_log2 == 4 && a.tile_h_log2 == 4)
+    k_composite<4, 4><<<grid, 256, 0, s>>>(a);
+  else
+    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

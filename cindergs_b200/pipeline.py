@@ -410,7 +410,8 @@ class GpuPipelineState:
                           min_opacity: float = 1.0 / 255.0, min_radius_px: float = 0.5,
                           profile_stages: bool = False, force_stage3: bool = False,
                           write_f32: bool = False, radix_bits: int = 0,
-                          stage_timings: bool = True, entry_sort: int = 0) -> GpuStageTimings:
+                          stage_timings: bool = True, entry_sort: int = 0,
+                          tile_shape: int = 0) -> GpuStageTimings:
         """execute_frame_gpu (gpu_state.rs:613-1243). With stage_timings (the
         default) the call waits for the frame and returns its counts (and, with
         profile_stages, per-stage device ms); with stage_timings=False the frame
@@ -418,14 +419,16 @@ class GpuPipelineState:
         accumulate when profile_stages is set (read them with kernel_profile()),
         and the returned timings are all zero. radix_bits and entry_sort choose
         how the tile entries are sorted (include/cgs.h: CGS_SORT_*); every
-        choice gives the same lists."""
+        choice gives the same lists. tile_shape is the screen tile of Stages 3
+        and 4 (CGS_TILE_*: the reference's 16x16 by default, 8x8 or 32x16)."""
         self.sync_scene_and_cages(scene, cages)
         cam = self._camera(camera)
         comp = self._compositor(compositor)
         params = _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
                                      float(min_opacity), float(min_radius_px),
                                      int(bool(profile_stages)), int(bool(force_stage3)),
-                                     int(bool(write_f32)), int(radix_bits), int(entry_sort))
+                                     int(bool(write_f32)), int(radix_bits), int(entry_sort),
+                                     int(tile_shape))
         t = _abi.CgsStageTimings()
         tp = ctypes.byref(t) if stage_timings else None
         self._check(self._lib.cgs_execute_frame(self._ctx, ctypes.byref(cam), ctypes.byref(comp),
@@ -459,10 +462,10 @@ class GpuPipelineState:
                       compositors, images, use_graph: bool = True,
                       strain_split_threshold: float = 0.0, mip_filter_3d_var: float = 0.0,
                       min_opacity: float = 1.0 / 255.0, min_radius_px: float = 0.5,
-                      radix_bits=0, entry_sort=0) -> dict:
+                      radix_bits=0, entry_sort=0, tile_shape=0) -> dict:
         """One step of many views (cgs_execute_views): Stage 1 once, Stages 2-4
-        per view into images[v] (from view_images). radix_bits and entry_sort
-        are one value for every view or a list with one per view (see
+        per view into images[v] (from view_images). radix_bits, entry_sort and
+        tile_shape are one value for every view or a list with one per view (see
         cindergs_b200.autotune). With use_graph the step is captured as a CUDA
         graph on the first call for a set of views and replayed afterwards.
         Returns the step's stats."""
@@ -473,10 +476,11 @@ class GpuPipelineState:
         outs = (ctypes.c_void_p * n)(*[ctypes.c_void_p(t.data_ptr()) for t in images])
         rbs = list(radix_bits) if hasattr(radix_bits, "__len__") else [radix_bits] * n
         ess = list(entry_sort) if hasattr(entry_sort, "__len__") else [entry_sort] * n
+        tss = list(tile_shape) if hasattr(tile_shape, "__len__") else [tile_shape] * n
         params = (_abi.CgsFrameParams * n)(*[
             _abi.CgsFrameParams(float(strain_split_threshold), float(mip_filter_3d_var),
                                 float(min_opacity), float(min_radius_px), 0, 1, 0, int(rbs[v]),
-                                int(ess[v])) for v in range(n)])
+                                int(ess[v]), int(tss[v])) for v in range(n)])
         st = _abi.CgsViewsStats()
         self._check(self._lib.cgs_execute_views(self._ctx, n, cams, comps, params,
                                                 outs, int(bool(use_graph)), ctypes.byref(st)),

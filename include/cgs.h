@@ -75,7 +75,19 @@ typedef struct cgs_frame_params {
   int32_t radix_bits;           /* entry-sort digit width: 0 = balanced digits of at most
                                    8 bits over the tile bits (13 bits -> 7 + 6), else 4..8 */
   int32_t entry_sort;           /* CGS_SORT_*: how the tile entries are sorted by tile */
+  int32_t tile_shape;           /* CGS_TILE_*: screen tile of Stages 3 and 4 */
 } cgs_frame_params;
+
+/* Screen tile shapes. The reference bins and composites 16x16 tiles
+ * (render/kernels/binning.rs, compositor.rs); 8x8 and 32x16 tiles run the
+ * same ellipse-vs-tile test and blending rules on other rectangles (fewer
+ * candidate pixels per entry, or fewer entries per splat), so a pixel's
+ * colour changes only where the test's rounding admits a splat whose alpha
+ * at that pixel is below the 1/255 cut anyway. Chosen per viewport by the
+ * autotuner. */
+#define CGS_TILE_16X16 0
+#define CGS_TILE_8X8 1
+#define CGS_TILE_32X16 2
 
 /* Entry sort methods (the result is the same, bit for bit). */
 #define CGS_SORT_AUTO 0       /* radix passes */

@@ -99,6 +99,7 @@ def lib():
         L.orc_ref_tet_transforms.argtypes = [_c_u32, _f32p, _u32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_ref_sh_rotate.argtypes = [_c_u32, _f32p, _f32p, _c_u32]
         L.orc_sh_rotation_matrix.argtypes = [_f32p, _c_u32, _f32p]
+        L.orc_set_tile_shape.argtypes = [_c_u32, _c_u32]
         L.orc_spring_frame_damping.restype = _c_f
         L.orc_spring_frame_damping.argtypes = [_c_f, _c_f]
         L.orc_spring_step.argtypes = [_c_u32, _f32p, _f32p, _f32p, _vp, _c_f, _c_f, _c_f, _c_u32,
@@ -249,11 +250,20 @@ def v2_composite(W, H, attrs, sorted_ids, ranges, bg):
 
 
 def v2_frame(scene, cam24, comp, *, mip=0.0, min_opa=1.0 / 255.0, min_rad=0.5, split_thr=0.0,
-             cage=None):
+             cage=None, tile=(16, 16)):
     """Whole v2 frame on the CPU. ``scene`` = dict(pos, cov, opa, sh);
     ``comp`` = dict(width, height, bg, cam_pos, sh_degree); ``cage`` =
-    dict(verts, elems, inv_dm, bind_tet, bind_w) or None. Returns a dict with
-    every intermediate (the same buffers the GPU frame exposes)."""
+    dict(verts, elems, inv_dm, bind_tet, bind_w) or None; ``tile`` = the
+    screen tile (width, height) of Stages 3 and 4. Returns a dict with every
+    intermediate (the same buffers the GPU frame exposes)."""
+    lib().orc_set_tile_shape(int(tile[0]), int(tile[1]))
+    try:
+        return _v2_frame(scene, cam24, comp, mip, min_opa, min_rad, split_thr, cage, tile)
+    finally:
+        lib().orc_set_tile_shape(16, 16)
+
+
+def _v2_frame(scene, cam24, comp, mip, min_opa, min_rad, split_thr, cage, tile):
     W, H = int(comp["width"]), int(comp["height"])
     out = {}
     n = int(np.asarray(scene["opa"]).size)
@@ -276,7 +286,8 @@ def v2_frame(scene, cam24, comp, *, mip=0.0, min_opa=1.0 / 255.0, min_rad=0.5, s
     counts, total = v2_count_tiles(attrs, ext, W, H)
     offsets, total2 = scan(counts)
     assert total == total2
-    tiles = ((W + 15) // 16) * ((H + 15) // 16)
+    tw, th = int(tile[0]), int(tile[1])
+    tiles = ((W + tw - 1) // tw) * ((H + th - 1) // th)
     out.update(attrs=attrs, ext=ext, surviving=surv, counts=counts, offsets=offsets,
                entries=total, total_tiles=tiles)
     if tiles <= 65535:

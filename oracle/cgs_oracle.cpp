@@ -490,14 +490,21 @@ uint32_t project_one(size_t idx, uint32_t n_rest, const float* pos, const float*
 }
 
 // ---------------------------------------------------------------- v2 Stage 3
+// Screen tile of the v2 Stages 3 and 4: the reference's 16x16 pixels unless
+// set otherwise (8x8 and 32x16 are the library's other tile shapes; the
+// functions below keep the reference's formulas on the other rectangle).
+static uint32_t g_tile_w = 16, g_tile_h = 16;
+static uint32_t tiles_across(uint32_t W) { return (W + g_tile_w - 1) / g_tile_w; }
+static uint32_t tiles_down(uint32_t H) { return (H + g_tile_h - 1) / g_tile_h; }
+
 // ellipse_intersects_tile_gpu (render/kernels/binning.rs:37-83).
 bool ellipse_tile(float mu_x, float mu_y, float ca, float cb, float cc, float alpha, uint32_t tx,
                   uint32_t ty, uint32_t W, uint32_t H) {
   if (alpha < (1.0f / 255.0f) || W == 0 || H == 0) return false;
-  uint32_t x_start = tx * 16u, y_start = ty * 16u;
+  uint32_t x_start = tx * g_tile_w, y_start = ty * g_tile_h;
   if (x_start >= W || y_start >= H) return false;
-  uint32_t x_end = std::min(x_start + 15u, W - 1u);
-  uint32_t y_end = std::min(y_start + 15u, H - 1u);
+  uint32_t x_end = std::min(x_start + (g_tile_w - 1u), W - 1u);
+  uint32_t y_end = std::min(y_start + (g_tile_h - 1u), H - 1u);
   float dx0 = ((float)x_start + 0.5f) - mu_x;
   float dx1 = ((float)x_end + 0.5f) - mu_x;
   float dy0 = ((float)y_start + 0.5f) - mu_y;
@@ -520,8 +527,8 @@ struct TileBox {
 // Tile AABB of count_tiles_kernel / emit_tile_keys_kernel (binning.rs:139-142).
 TileBox tile_box(float mu_x, float mu_y, float ext_x, float ext_y, uint32_t tiles_x,
                  uint32_t tiles_y) {
-  auto fl = [](float v, int32_t hi) {
-    float f = std::floor(v / 16.0f);
+  auto fl = [](float v, int32_t hi, uint32_t tile) {
+    float f = std::floor(v / (float)tile);
     int32_t i;
     if (!(f == f)) i = 0;
     else if (f >= 2147483520.0f) i = INT32_MAX;
@@ -530,7 +537,8 @@ TileBox tile_box(float mu_x, float mu_y, float ext_x, float ext_y, uint32_t tile
     return (uint32_t)std::min(std::max(i, 0), hi);
   };
   int32_t mx = (int32_t)tiles_x - 1, my = (int32_t)tiles_y - 1;
-  return {fl(mu_x - ext_x, mx), fl(mu_x + ext_x, mx), fl(mu_y - ext_y, my), fl(mu_y + ext_y, my)};
+  return {fl(mu_x - ext_x, mx, g_tile_w), fl(mu_x + ext_x, mx, g_tile_w),
+          fl(mu_y - ext_y, my, g_tile_h), fl(mu_y + ext_y, my, g_tile_h)};
 }
 
 // ------------------------------------------------------------- ref CPU mode
@@ -1097,6 +1105,12 @@ float mvc_step(uint32_t V, const float* verts) {
 
 extern "C" {
 
+// Screen tile shape of the v2 functions (width, height in pixels).
+void orc_set_tile_shape(uint32_t w, uint32_t h) {
+  g_tile_w = w ? w : 16u;
+  g_tile_h = h ? h : 16u;
+}
+
 void orc_set_threads(int n) { g_threads = n; }
 int orc_get_threads(void) { return num_threads(); }
 
@@ -1171,7 +1185,7 @@ uint64_t orc_project_v2(uint32_t active, uint32_t n_rest, const float* pos, cons
 // count_tiles_kernel (binning.rs:92-164). Returns the sum of counts.
 uint64_t orc_count_tiles(uint32_t n, const float* attrs, const uint32_t* ext, uint32_t W,
                          uint32_t H, uint32_t* counts) {
-  uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+  uint32_t tiles_x = tiles_across(W), tiles_y = tiles_down(H);
   std::atomic<uint64_t> total{0};
   parallel_for(n, [&](size_t b, size_t e) {
     uint64_t local = 0;
@@ -1215,7 +1229,7 @@ void orc_packed_key_bits(uint32_t total_tiles, uint32_t* tile_bits, uint32_t* de
 void orc_emit_keys32(uint32_t n, const float* attrs, const uint32_t* ext, const uint32_t* offsets,
                      uint32_t W, uint32_t H, float near_plane, uint32_t depth_bits,
                      uint32_t* keys, uint32_t* ids) {
-  uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+  uint32_t tiles_x = tiles_across(W), tiles_y = tiles_down(H);
   uint32_t base = f2u(std::fmax(near_plane, 1e-6f)) & 0x7F800000u;
   parallel_for(n, [&](size_t b, size_t e) {
     for (size_t i = b; i < e; ++i) {
@@ -1243,7 +1257,7 @@ void orc_emit_keys32(uint32_t n, const float* attrs, const uint32_t* ext, const 
 // emit_tile_keys_u64_kernel (binning.rs:256-328).
 void orc_emit_keys64(uint32_t n, const float* attrs, const uint32_t* ext, const uint32_t* offsets,
                      uint32_t W, uint32_t H, uint32_t* tiles, uint32_t* depths, uint32_t* ids) {
-  uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+  uint32_t tiles_x = tiles_across(W), tiles_y = tiles_down(H);
   parallel_for(n, [&](size_t b, size_t e) {
     for (size_t i = b; i < e; ++i) {
       uint32_t p = ext[i];
@@ -1326,11 +1340,11 @@ void orc_tile_ranges(uint64_t n, const uint32_t* sorted, uint32_t shift, uint32_
 // output modes: rgba8 tight [H][W][4] (round-half-even, WGSL round) and f32.
 void orc_composite_v2(uint32_t W, uint32_t H, const float* attrs, const uint32_t* sorted_ids,
                       const uint32_t* ranges, const float* bg, uint8_t* rgba8, float* rgba_f32) {
-  uint32_t tiles_x = (W + 15) / 16;
+  uint32_t tiles_x = tiles_across(W);
   parallel_for((size_t)W * H, [&](size_t b, size_t e) {
     for (size_t pix = b; pix < e; ++pix) {
       uint32_t px = (uint32_t)(pix % W), py = (uint32_t)(pix / W);
-      uint32_t tile = (py / 16) * tiles_x + (px / 16);
+      uint32_t tile = (py / g_tile_h) * tiles_x + (px / g_tile_w);
       uint32_t rs = ranges[2 * tile], re = ranges[2 * tile + 1];
       bool empty = rs >= re;
       float cr = 0, cg = 0, cb = 0, t = 1.0f;
