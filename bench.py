@@ -339,6 +339,34 @@ def run_ours(args):
                                 (time.perf_counter() - t0) * 1000.0), device=f"cuda:{local}")
     e2e_value = world * args.steps / (e2e_ms / 1000.0)
 
+    # ---- the same frames with 32x16 screen tiles (the autotuner's choice at
+    # 1080p: fewer tile entries to bin and sort, more candidates per pixel)
+    alt = None
+    if args.tile_shape == 0:
+        def render_alt(count_entries=False):
+            nonlocal frame
+            wl.step()
+            cam = wl.camera(frame)
+            frame += world
+            return st.execute_frame_gpu(wl.scene, cages, cam, wl.compositor(cam),
+                                        wl.strain_split_threshold, wl.mip_filter_3d_var,
+                                        1.0 / 255.0, 0.5, stage_timings=count_entries,
+                                        tile_shape=2)
+        for _ in range(max(args.warmup, 3)):
+            last_alt = render_alt(True)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        a0.record(stream)
+        for _ in range(args.steps):
+            render_alt()
+        a1.record(stream)
+        barrier()
+        alt_ms = max_over_ranks(a0.elapsed_time(a1), device=f"cuda:{local}")
+        alt = {"views_per_s": world * args.steps / (alt_ms / 1000.0),
+               "ms_per_step": alt_ms / args.steps,
+               "tile_entries": last_alt.total_tile_entries}
+
     if rank == 0:
         hbm, peak_kind = peaks()
         kernels = {}
@@ -387,6 +415,8 @@ def run_ours(args):
             "gpu_launches": gpu_launches,
             "clocks": clock.summary(),
         }
+        if alt is not None:
+            line["tile_32x16"] = alt
         if world == 1 and not args.no_cpu_baseline:
             try:
                 bt = cages.bind_tet
