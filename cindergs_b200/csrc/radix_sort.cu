@@ -30,6 +30,7 @@ namespace {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kSortWarps = kSortThreads / 32;
 // Reorder buffers hold one padding word per 32 keys: the lanes of a warp
 // whose keys fall in different digits write positions about one digit run
 // (~32 keys) apart, which without padding map to the same bank.
@@ -62,12 +63,13 @@ struct PassArgs {
 template <int RB, bool PAY2>
 __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const PassArgs a) {
   constexpr uint32_t R = 1u << RB;
+  static_assert(R <= (uint32_t)kSortThreads, "one thread per digit");
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* s_keys = smem;                       // [kSortTileP]
   uint32_t* s_v0 = s_keys + kSortTileP;          // [kSortTileP]
   uint32_t* s_v1 = s_v0 + kSortTileP;            // [kSortTileP] (PAY2)
-  uint32_t* s_whist = s_v0 + (PAY2 ? 2 : 1) * kSortTileP;  // [8][R]
-  uint32_t* s_tstart = s_whist + 8 * R;          // [R]
+  uint32_t* s_whist = s_v0 + (PAY2 ? 2 : 1) * kSortTileP;  // [warps][R]
+  uint32_t* s_tstart = s_whist + kSortWarps * R;  // [R]
   uint32_t* s_goff = s_tstart + R;               // [R]
   uint32_t* s_misc = s_goff + R;                 // [40]: tile, warp sums
 
@@ -76,7 +78,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   if (n > a.capacity) n = a.capacity;
   const uint32_t num_tiles = (n + kSortTile - 1) / kSortTile;
   if (tid == 0) s_misc[0] = atomicAdd(a.tile_ctr, 1u);
-  for (uint32_t k = tid; k < 8 * R; k += kSortThreads) s_whist[k] = 0u;
+  for (uint32_t k = tid; k < kSortWarps * R; k += kSortThreads) s_whist[k] = 0u;
   __syncthreads();
   const uint32_t tile = s_misc[0];
   // Clear this tile's words of the other look-back buffer for the next pass
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   if ((uint32_t)tid < R) {
     uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 0; w < kSortWarps; ++w) {
       const uint32_t c = s_whist[w * R + tid];
       s_whist[w * R + tid] = run;
       run += c;
@@ -233,7 +235,7 @@ __global__ void k_digit_bases(uint32_t* hist, uint32_t radix) {
 template <int RB, bool PAY2>
 size_t onesweep_smem() {
   constexpr uint32_t R = 1u << RB;
-  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTileP + 8 * R + 3 * R + 48);
+  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTileP + kSortWarps * R + 3 * R + 48);
 }
 
 template <int RB, bool PAY2>
