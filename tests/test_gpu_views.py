@@ -87,16 +87,29 @@ def test_replay_overflow_renders_again(setup):
 
 def test_autotuned_views_render_the_same(setup):
     """Per-view digit widths and entry-sort methods chosen by the autotuner
-    give the same images as the defaults."""
-    from cindergs_b200 import autotune
+    on the reference's 16x16 tiles give the same images as the defaults; with
+    tile shapes tuned too, the replayed graph gives the images of an eager
+    batch with the same choices."""
+    from cindergs_b200 import _abi, autotune
     st, wl, cages, cams, comps = setup
     wl.step()
-    best = autotune.tune_views(st, wl.scene, cages, cams, comps, repeats=1)
+    best = autotune.tune_views(st, wl.scene, cages, cams, comps, repeats=1,
+                               tile_shapes=(_abi.TILE_16X16,))
     assert set(best) == {(c.screen_width, c.screen_height) for c in comps}
-    rbs, ess = autotune.per_view(best, comps)
+    tss, rbs, ess = autotune.per_view(best, comps)
+    assert set(tss) == {_abi.TILE_16X16}
     a, b = st.view_images(comps), st.view_images(comps)
     st.execute_views(wl.scene, cages, cams, comps, a, use_graph=False)
     st.execute_views(wl.scene, cages, cams, comps, b, use_graph=True, radix_bits=rbs,
-                     entry_sort=ess)
+                     entry_sort=ess, tile_shape=tss)
     for x, y in zip(images_np(a), images_np(b)):
         np.testing.assert_array_equal(x, y)
+    best = autotune.tune_views(st, wl.scene, cages, cams, comps, repeats=1)
+    tss, rbs, ess = autotune.per_view(best, comps)
+    st.execute_views(wl.scene, cages, cams, comps, a, use_graph=False, radix_bits=rbs,
+                     entry_sort=ess, tile_shape=tss)
+    for _ in range(2):  # capture, then replay
+        st.execute_views(wl.scene, cages, cams, comps, b, use_graph=True, radix_bits=rbs,
+                         entry_sort=ess, tile_shape=tss)
+        for x, y in zip(images_np(a), images_np(b)):
+            np.testing.assert_array_equal(x, y)
