@@ -303,8 +303,12 @@ def run_ours(args):
     value = world * args.steps / (ms / 1000.0)
 
     # ---- e2e: public API with host buffers, copies inside the timed region
-    pinned_out = torch.empty((args.height, args.width, 4), dtype=torch.uint8).pin_memory()
-    out_np = pinned_out.numpy()
+    # two page-locked output images: frame i's pixels are copied to the host
+    # while frame i + 1 renders (cgs_readback_rgba8_async), and each is
+    # waited for before its image is reused
+    pinned_out = [torch.empty((args.height, args.width, 4), dtype=torch.uint8).pin_memory()
+                  for _ in range(2)]
+    out_np = [t.numpy() for t in pinned_out]
     vert_pinned = torch.empty(wl.cage.mesh.rest_vertices.shape, dtype=torch.float32).pin_memory()
     barrier()
     t0 = time.perf_counter()
@@ -314,7 +318,8 @@ def run_ours(args):
     import ctypes
     wl.step()
     vert_pinned.numpy()[:] = wl.cage.vertices()
-    for _ in range(args.steps):
+    prev_ticket = None
+    for step in range(args.steps):
         cam = wl.camera(frame)
         frame += world
         # host vertices -> device (pinned source), then the frame (enqueued),
@@ -328,11 +333,15 @@ def run_ours(args):
                              wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, radix_bits=args.radix_bits,
                              entry_sort=args.entry_sort, tile_shape=args.tile_shape,
                              stage_timings=False)
+        ticket = st.readback_framebuffer_rgba8_async(out_np[step % 2])
         wl.step()
         next_verts = wl.cage.vertices()
-        st._check(st._lib.cgs_readback_rgba8(st.handle, ctypes.c_void_p(out_np.ctypes.data),
-                                             args.width, args.height), "cgs_readback_rgba8")
+        if prev_ticket is not None:
+            st.readback_wait(prev_ticket)  # the previous frame's pixels are on the host
+        prev_ticket = ticket
         vert_pinned.numpy()[:] = next_verts
+    if prev_ticket is not None:
+        st.readback_wait(prev_ticket)
     e2e_end.record(stream)
     barrier()
     e2e_ms = max_over_ranks(max(e2e_start.elapsed_time(e2e_end),

@@ -136,6 +136,8 @@ SIGNATURES = {
                                  ctypes.POINTER(CgsStageTimings)]),
     "cgs_readback_rgba8": (_int, [_vp, _vp, _u32, _u32]),
     "cgs_readback_rgba_f32": (_int, [_vp, _vp, _u32, _u32]),
+    "cgs_readback_rgba8_async": (_i32, [_vp, _vp, _u32, _u32, ctypes.POINTER(_u64)]),
+    "cgs_readback_wait": (_i32, [_vp, _u64]),
     "cgs_framebuffer_device": (_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_u32)]),
     "cgs_invalidate_stage3": (_int, [_vp]),
     "cgs_invalidate": (_int, [_vp]),

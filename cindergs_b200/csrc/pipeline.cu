@@ -256,8 +256,25 @@ struct cgs_ctx {
   uint32_t last_w = 0, last_h = 0, last_pitch = 0, last_active = 0, last_tiles = 0;
   bool last_f32 = false, frame_done = false;
   int latest_slot = -1;
+  uint64_t frame_seq = 0;        // frames enqueued by cgs_execute_frame
+  uint64_t rerun_count = 0;      // Stage 3/4 re-runs after an entry overflow
+  uint64_t rerun_seq = 0;        // frame number of the latest re-run
+  // Asynchronous RGBA8 readbacks (cgs_readback_rgba8_async): a device
+  // snapshot of the framebuffer per slot, copied to the host on rb_stream.
+  struct Readback {
+    DevBuf stage;
+    cudaEvent_t ready = nullptr, done = nullptr;
+    uint64_t ticket = 0, frame_seq = 0, reruns = 0;
+    uint8_t* dst = nullptr;
+    uint32_t W = 0, H = 0;
+    int frame_slot = -1;
+    bool pending = false;
+  } rb[2];
+  cudaStream_t rb_stream = nullptr;
+  uint64_t rb_tickets = 0;
   // in-flight frames
   struct Pending {
+    uint64_t seq = 0;  // frame number (cgs_execute_frame calls)
     bool used = false, stage3_ran = false, profiled = false, need_deform = false;
     bool split_possible = false, key64 = false;
     uint32_t n = 0, cap = 0, sort_passes = 0, splat_passes = 0, total_tiles = 0, W = 0, H = 0;
@@ -610,6 +627,8 @@ int rerun_stage34(cgs_ctx* ctx, uint32_t entries) {
                            cudaMemcpyDeviceToHost, ctx->stream), "read counters");
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "stage 3 re-run");
   ctx->s3_src = src;
+  ++ctx->rerun_count;
+  ctx->rerun_seq = ctx->ring[ctx->latest_slot].seq;
   const FrameCounters& f = ctx->h_ring[ctx->latest_slot].fc;
   if (f.status & kStatusCapacity) return ctx->fail(CGS_E_CAPACITY, "tile entries still exceed the grown buffers");
   return CGS_OK;
@@ -814,6 +833,14 @@ int cgs_ctx_destroy(cgs_ctx* ctx) {
   for (int k = 0; k < kRing; ++k) {
     if (ctx->up.p[k]) cudaFreeHost(ctx->up.p[k]);
     if (ctx->up.ev[k]) cudaEventDestroy(ctx->up.ev[k]);
+  }
+  if (ctx->rb_stream) {
+    cudaStreamSynchronize(ctx->rb_stream);
+    cudaStreamDestroy(ctx->rb_stream);
+  }
+  for (auto& r : ctx->rb) {
+    if (r.ready) cudaEventDestroy(r.ready);
+    if (r.done) cudaEventDestroy(r.done);
   }
   if (ctx->views_exec) cudaGraphExecDestroy(ctx->views_exec);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
@@ -2009,6 +2036,7 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   const uint32_t passes = fi.passes, splat_passes = fi.splat_passes;
   const uint32_t bin_launches = fi.bin_launches, sort_launches = fi.sort_launches;
   P.used = true;
+  P.seq = ++ctx->frame_seq;
   P.stage3_ran = !cached;
   P.profiled = prof;
   P.need_deform = need_deform;
@@ -2304,6 +2332,74 @@ int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t heig
            "framebuffer readback");
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "framebuffer readback");
   return ctx->take_sticky();
+}
+
+int cgs_readback_wait(cgs_ctx* ctx, uint64_t ticket) {
+  if (!ctx) return CGS_E_ARG;
+  cgs_ctx::Readback* r = nullptr;
+  for (auto& x : ctx->rb)
+    if (x.pending && x.ticket == ticket) r = &x;
+  if (!r) {
+    if (ticket == 0 || ticket > ctx->rb_tickets) return ctx->fail(CGS_E_ARG, "unknown readback ticket");
+    return CGS_OK;  // finished and waited for already
+  }
+  cudaSetDevice(ctx->device);
+  r->pending = false;
+  CGS_CUDA(cudaEventSynchronize(r->done), "framebuffer readback");
+  // The copied frame has finished; check its counters now if no call has
+  // (an entry overflow re-renders the latest frame with grown buffers).
+  cgs_ctx::Pending& p = ctx->ring[r->frame_slot];
+  if (p.used && p.seq == r->frame_seq) CGS_TRY(check_slot(ctx, r->frame_slot, true));
+  if (ctx->rerun_count != r->reruns && ctx->rerun_seq == r->frame_seq) {
+    // re-rendered after the snapshot: copy again while it is the last frame
+    if (ctx->latest_slot < 0 || ctx->ring[ctx->latest_slot].seq != r->frame_seq)
+      return ctx->fail(CGS_E_CAPACITY,
+                       "the frame was re-rendered after its readback began and is no longer the last frame");
+    CGS_CUDA(cudaMemcpy2DAsync(r->dst, (size_t)r->W * 4, ctx->fb_rgba8.p, (size_t)ctx->last_pitch * 4,
+                               (size_t)r->W * 4, r->H, cudaMemcpyDeviceToHost, ctx->stream),
+             "framebuffer readback");
+    CGS_CUDA(cudaStreamSynchronize(ctx->stream), "framebuffer readback");
+  }
+  return ctx->take_sticky();
+}
+
+int cgs_readback_rgba8_async(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height,
+                             uint64_t* ticket) {
+  if (!ctx || !dst || !ticket) return CGS_E_ARG;
+  if (!ctx->frame_done || ctx->latest_slot < 0) return ctx->fail(CGS_E_STATE, "no frame rendered");
+  if (width != ctx->last_w || height != ctx->last_h)
+    return ctx->fail(CGS_E_ARG, "size differs from the last frame");
+  cudaSetDevice(ctx->device);
+  if (!ctx->rb_stream)
+    CGS_CUDA(cudaStreamCreateWithFlags(&ctx->rb_stream, cudaStreamNonBlocking), "readback stream");
+  const uint64_t t = ctx->rb_tickets + 1;
+  cgs_ctx::Readback& r = ctx->rb[t & 1];
+  if (r.pending) CGS_TRY(cgs_readback_wait(ctx, r.ticket));  // at most two in flight
+  if (!r.ready) CGS_CUDA(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming), "readback event");
+  if (!r.done) CGS_CUDA(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming), "readback event");
+  const size_t bytes = (size_t)width * height * 4;
+  CGS_TRY(ctx->ensure(r.stage, bytes ? bytes : 4, "readback snapshot"));
+  // snapshot on the frame stream (the next frame may overwrite the
+  // framebuffer), then the host copy on the readback stream
+  CGS_CUDA(cudaMemcpy2DAsync(r.stage.p, (size_t)width * 4, ctx->fb_rgba8.p, (size_t)ctx->last_pitch * 4,
+                             (size_t)width * 4, height, cudaMemcpyDeviceToDevice, ctx->stream),
+           "framebuffer snapshot");
+  CGS_CUDA(cudaEventRecord(r.ready, ctx->stream), "readback event");
+  CGS_CUDA(cudaStreamWaitEvent(ctx->rb_stream, r.ready, 0), "readback event");
+  CGS_CUDA(cudaMemcpyAsync(dst, r.stage.p, bytes, cudaMemcpyDeviceToHost, ctx->rb_stream),
+           "framebuffer readback");
+  CGS_CUDA(cudaEventRecord(r.done, ctx->rb_stream), "readback event");
+  ctx->rb_tickets = t;
+  r.ticket = t;
+  r.frame_slot = ctx->latest_slot;
+  r.frame_seq = ctx->ring[ctx->latest_slot].seq;
+  r.reruns = ctx->rerun_count;
+  r.dst = dst;
+  r.W = width;
+  r.H = height;
+  r.pending = true;
+  *ticket = t;
+  return CGS_OK;
 }
 
 int cgs_readback_rgba_f32(cgs_ctx* ctx, float* dst, uint32_t width, uint32_t height) {

@@ -510,6 +510,23 @@ class GpuPipelineState:
                     "cgs_readback_rgba8")
         return out
 
+    def readback_framebuffer_rgba8_async(self, out: np.ndarray) -> int:
+        """Starts copying the last frame's RGBA8 pixels into `out` ([H, W, 4]
+        uint8, ideally page-locked) without waiting; returns a ticket for
+        readback_wait (cgs_readback_rgba8_async). `out` must stay alive and
+        untouched until then."""
+        if out.dtype != np.uint8 or out.ndim != 3 or out.shape[2] != 4 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous uint8 [H, W, 4] array")
+        ticket = ctypes.c_uint64()
+        self._check(self._lib.cgs_readback_rgba8_async(self._ctx, _p(out), out.shape[1], out.shape[0],
+                                                        ctypes.byref(ticket)),
+                    "cgs_readback_rgba8_async")
+        return int(ticket.value)
+
+    def readback_wait(self, ticket: int) -> None:
+        """Waits until the copy `ticket` has arrived (cgs_readback_wait)."""
+        self._check(self._lib.cgs_readback_wait(self._ctx, int(ticket)), "cgs_readback_wait")
+
     def readback_framebuffer_f32(self, width: int, height: int) -> np.ndarray:
         out = np.empty((height, width, 4), f32)
         self._check(self._lib.cgs_readback_rgba_f32(self._ctx, _p(out), width, height),

@@ -357,6 +357,22 @@ int cgs_execute_views(cgs_ctx* ctx, uint32_t num_views, const cgs_camera* camera
 /* Copies the last frame's RGBA8 pixels into a tight [h][w][4] host buffer
  * (readback_framebuffer_rgba8, gpu_state.rs:1296-1328). */
 int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height);
+/* Starts copying the last frame's RGBA8 pixels into the tight [h][w][4] host
+ * buffer dst and returns without waiting: the pixels are snapshotted on the
+ * device behind the frame and copied to the host on a separate stream, so
+ * the copy overlaps the frames enqueued after it (page-locked dst memory
+ * makes the copy asynchronous). *ticket identifies the copy; dst holds the
+ * pixels once cgs_readback_wait(ctx, ticket) has returned CGS_OK. At most
+ * two copies are in flight: a third call first waits for the oldest. If the
+ * frame overflowed the tile-entry buffers, the wait re-reads it after the
+ * library re-renders it, or returns CGS_E_CAPACITY when newer frames have
+ * replaced it. No reference counterpart: readback_framebuffer_rgba8
+ * (gpu_state.rs:1296-1328) is synchronous. */
+int cgs_readback_rgba8_async(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height,
+                             uint64_t* ticket);
+/* Waits for the copy `ticket` of cgs_readback_rgba8_async (a ticket already
+ * waited for returns CGS_OK at once). */
+int cgs_readback_wait(cgs_ctx* ctx, uint64_t ticket);
 /* Copies the last frame's unquantised RGBA f32 pixels [h][w][4] (written when
  * params.write_f32 was set; render/kernels/compositor.rs f32 output mode). */
 int cgs_readback_rgba_f32(cgs_ctx* ctx, float* dst, uint32_t width, uint32_t height);
