@@ -556,84 +556,132 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Per-frame output layer over cached codes (k_field_infer<true>). Each warp
-// owns a contiguous range of items and streams them through a kApStages-deep
-// ring in shared memory with cp.async: lane l copies 16-byte chunks 2l, 2l+1
-// of the item's 1 KB code (the ones it reads back: hidden units 16 (l % 8)
-// .. + 15 of stream l / 8), lane 0 also the item's rest position. Lane l
-// keeps its 48 projection entries in registers; the eight lanes of a stream
-// reduce their partial P^T code, and lanes 0..11 each form one output float
-// (position + pc + A3 x, gradient + A3) and store the item's 48 bytes
-// together (k_mvc_jacobian's layout).
-constexpr int kApStages = 8, kApWarps = 8, kApStage = 4 * kHid * 2 / 16 + 1;  // uint4 per stage
+// Per-frame output layer over cached codes (k_field_infer<true>) on the
+// tensor cores. An item's code is four rows (h and its three tangents) of
+// 128 bf16; x' and F are those rows times P (128 x 3) plus the affine terms,
+// so four items make one 16-row MMA tile. Each warp owns a contiguous range
+// of items and streams it through a kApStages-deep ring of 4-item stages
+// with cp.async; the 16-byte chunks are placed with an XOR swizzle (chunk j
+// of row r at j ^ (r % 8)) so that the ldmatrix reads are free of bank
+// conflicts. Each stage is multiplied by P with mma.sync m16n8k16 (bf16 in,
+// fp32 accumulate). P is split into three bf16 terms (hi + mid + lo, column
+// n = 4 c + t of B holds term t of P[:, c]) held as B fragments in
+// registers, so each output equals an fp32 dot product to within a few ulp.
+// The kernel is bound by HBM (1,040 bytes per item); the MMAs replace the
+// per-lane multiply-adds (48 per lane and item) that bounded a scalar form.
+// Outputs go out in k_mvc_jacobian's layout: position, then F column-major.
+constexpr int kApStages = 6, kApWarps = 8, kApItems = 4;
+constexpr int kApCodeBytes = kApItems * 4 * kHid * 2;       // 4,096
+constexpr int kApStageBytes = kApCodeBytes + kApItems * 16;  // + rest positions
 
-__global__ void __launch_bounds__(kApWarps * 32) k_field_apply(FieldInfer fi) {
-  extern __shared__ uint4 ap_ring[];
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const uint32_t l = __bfloat16_as_ushort(__float2bfloat16_rn(lo));
+  const uint32_t h = __bfloat16_as_ushort(__float2bfloat16_rn(hi));
+  return l | (h << 16);
+}
+// term t (0 hi, 1 mid, 2 lo) of the three-term bf16 split of v
+__device__ __forceinline__ float bf16_term(float v, int t) {
+  const float hi = __bfloat162float(__float2bfloat16_rn(v));
+  if (t == 0) return hi;
+  const float mid = __bfloat162float(__float2bfloat16_rn(v - hi));
+  if (t == 1) return mid;
+  return v - hi - mid;  // rounded to bf16 when packed
+}
+
+__global__ void __launch_bounds__(kApWarps * 32, 1) k_field_apply(FieldInfer fi) {
+  extern __shared__ __align__(128) unsigned char ap_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint4* ring = ap_ring + (size_t)warp * kApStages * kApStage;
-  const int k0 = (lane & 7) * 16;
-  float pr[16][3];
+  const int g = lane >> 2, q = lane & 3;
+  unsigned char* ring = ap_smem + (size_t)warp * kApStages * kApStageBytes;
+  // B fragments of the split P: k = 16 kk + 2 q (+1) and + 8, n = 8 nt + g
+  uint32_t bfr[8][2][2];
 #pragma unroll
-  for (int i = 0; i < 16; ++i)
+  for (int kk = 0; kk < 8; ++kk)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) pr[i][c] = fi.proj[3 * (k0 + i) + c];
-  // output float o = lane (< 12): 0..2 position, 3 + 3 d + c gradient F[c][d]
-  const int o = lane < 12 ? lane : 0;
-  const int oc = o < 3 ? o : (o - 3) % 3;
-  const int os = o < 3 ? 0 : 1 + (o - 3) / 3;  // stream feeding this output
+    for (int nt = 0; nt < 2; ++nt) {
+      const int n = 8 * nt + g, c = n >> 2, t = n & 3;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int k = 16 * kk + 2 * q + 8 * r;
+        float v0 = 0.0f, v1 = 0.0f;
+        if (c < 3 && t < 3) {
+          v0 = bf16_term(fi.proj[3 * k + c], t);
+          v1 = bf16_term(fi.proj[3 * (k + 1) + c], t);
+        }
+        bfr[kk][nt][r] = pack_bf16x2(v0, v1);
+      }
+    }
   const float* pc = fi.proj + 3 * kHid;
   const float* A3 = pc + 3;
-  const float bias0 = o < 3 ? pc[oc] : A3[3 * oc + (os - 1)];
-  const float a30 = A3[3 * oc], a31 = A3[3 * oc + 1], a32 = A3[3 * oc + 2];
   const uint32_t gw = blockIdx.x * kApWarps + warp, nw = gridDim.x * kApWarps;
   const uint32_t per = (fi.count + nw - 1) / nw;
   const uint32_t i0 = min(fi.count, gw * per), i1 = min(fi.count, i0 + per);
-  auto issue = [&](uint32_t item, int stage) {
-    if (item < i1) {
-      const uint4* src = reinterpret_cast<const uint4*>(fi.codes + (size_t)item * (4 * kHid));
-      uint4* dst = ring + stage * kApStage;
-      cp_async16(dst + 2 * lane, src + 2 * lane);
-      cp_async16(dst + 2 * lane + 1, src + 2 * lane + 1);
-      if (lane == 0) cp_async16(dst + kApStage - 1, fi.code_pos + item);
+  const uint32_t nstages = (i1 - i0 + kApItems - 1) / kApItems;
+  const unsigned char* codes = reinterpret_cast<const unsigned char*>(fi.codes);
+  auto issue = [&](uint32_t sidx) {
+    const uint32_t it = i0 + kApItems * sidx;
+    unsigned char* st = ring + (sidx % kApStages) * kApStageBytes;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t ch = lane + 32 * u;  // 16-byte chunk of the stage's 4 KB
+      if (it + (ch >> 6) < i1) {
+        const uint32_t r = ch >> 4, j = ch & 15;
+        cp_async16(st + r * 256 + ((j ^ (r & 7)) << 4), codes + (size_t)it * 1024 + ch * 16);
+      }
     }
+    if (lane < kApItems && it + lane < i1) cp_async16(st + kApCodeBytes + 16 * lane, fi.code_pos + it + lane);
     cp_async_commit();
   };
 #pragma unroll
-  for (int k = 0; k < kApStages - 1; ++k) issue(i0 + k, k);
-  int stage = 0;
-  for (uint32_t item = i0; item < i1; ++item) {
-    issue(item + kApStages - 1, (stage + kApStages - 1) % kApStages);
+  for (int k = 0; k < kApStages - 1; ++k) issue(k);
+  for (uint32_t sidx = 0; sidx < nstages; ++sidx) {
+    issue(sidx + kApStages - 1);
     cp_async_wait<kApStages - 1>();
-    __syncwarp();  // lane 0's copy of the position
-    const uint4* sb = ring + stage * kApStage;
-    const uint4 q[2] = {sb[2 * lane], sb[2 * lane + 1]};
-    const float4 x4 = *reinterpret_cast<const float4*>(sb + kApStage - 1);
-    float a[3] = {0.0f, 0.0f, 0.0f};
+    __syncwarp();
+    const unsigned char* st = ring + (sidx % kApStages) * kApStageBytes;
+    float d[2][4] = {{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
+    const int mrow = (lane & 7) + ((lane >> 3) & 1) * 8;  // row this lane addresses
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const int j = 2 * kk + (lane >> 4);
+      const uint32_t addr =
+          (uint32_t)__cvta_generic_to_shared(st + mrow * 256 + ((j ^ (mrow & 7)) << 4));
+      uint32_t a0, a1, a2, a3;
+      asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                   : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+                   : "r"(addr));
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+            "{%8,%9}, {%0,%1,%2,%3};\n"
+            : "+f"(d[nt][0]), "+f"(d[nt][1]), "+f"(d[nt][2]), "+f"(d[nt][3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(bfr[kk][nt][0]), "r"(bfr[kk][nt][1]));
+    }
+    // rows g and g + 8 = (item, stream); sum the terms of each output column
+    const uint32_t it = i0 + kApItems * sidx;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const uint32_t u[4] = {q[h].x, q[h].y, q[h].z, q[h].w};
+      float s0 = d[0][2 * h] + d[0][2 * h + 1];  // c = q / 2
+      float s1 = d[1][2 * h] + d[1][2 * h + 1];  // c = 2 (q < 2)
+      s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+      const int row = g + 8 * h, item = row >> 2, stream = row & 3;
+      if ((q & 1) || it + item >= i1) continue;
+      const float4 x = *reinterpret_cast<const float4*>(st + kApCodeBytes + 16 * item);
+      float* out = reinterpret_cast<float*>(fi.xf) + 12 * (size_t)(fi.out_first + it + item);
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float lo = __uint_as_float(u[e] << 16), hi = __uint_as_float(u[e] & 0xFFFF0000u);
-        const int i = 8 * h + 2 * e;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) a[c] += lo * pr[i][c] + hi * pr[i + 1][c];
+      for (int w = 0; w < 2; ++w) {
+        if (w == 1 && q != 0) break;
+        const int c = w == 0 ? (q >> 1) : 2;
+        const float t = w == 0 ? s0 : s1;
+        if (stream == 0)
+          out[c] = (t + pc[c]) + (A3[3 * c] * x.x + A3[3 * c + 1] * x.y + A3[3 * c + 2] * x.z);
+        else
+          out[3 + 3 * (stream - 1) + c] = t + A3[3 * c + stream - 1];
       }
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      a[c] += __shfl_xor_sync(0xffffffffu, a[c], 4);
-      a[c] += __shfl_xor_sync(0xffffffffu, a[c], 2);
-      a[c] += __shfl_xor_sync(0xffffffffu, a[c], 1);
-    }
-    const float t0 = __shfl_sync(0xffffffffu, a[0], 8 * os);
-    const float t1 = __shfl_sync(0xffffffffu, a[1], 8 * os);
-    const float t2 = __shfl_sync(0xffffffffu, a[2], 8 * os);
-    float v = (oc == 0 ? t0 : (oc == 1 ? t1 : t2)) + bias0;
-    if (o < 3) v += a30 * x4.x + a31 * x4.y + a32 * x4.z;
-    if (lane < 12) reinterpret_cast<float*>(fi.xf)[12 * (size_t)(fi.out_first + item) + lane] = v;
     __syncwarp();  // every lane has read this stage before it is refilled
-    stage = stage + 1 == kApStages ? 0 : stage + 1;
   }
   cp_async_wait<0>();
 }
@@ -722,12 +770,12 @@ cudaError_t launch_field_infer(const FieldInfer& fi, cudaStream_t s) {
 cudaError_t launch_field_apply(const FieldInfer& fi, cudaStream_t s) {
   if (fi.count == 0) return cudaSuccess;
   if (!fi.codes || !fi.code_pos) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)kApWarps * kApStages * kApStage * 16;
+  const size_t smem = (size_t)kApWarps * kApStages * kApStageBytes;
   const cudaError_t e =
       cudaFuncSetAttribute(k_field_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  // three blocks per SM (registers and shared memory allow it)
-  const uint32_t blocks = std::min<uint32_t>(148u * 3u, (fi.count + 7) / 8);
+  // one block of eight warps per SM (the rings take 195 KB)
+  const uint32_t blocks = std::min<uint32_t>(148u, (fi.count + kApWarps * kApItems - 1) / (kApWarps * kApItems));
   k_field_apply<<<blocks, kApWarps * 32, smem, s>>>(fi);
   return cudaGetLastError();
 }
