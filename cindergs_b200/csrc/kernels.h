@@ -327,6 +327,9 @@ struct SortArgs {
   // bit (a fixed cost) instead of __match_any_sync (cheap when a warp's keys
   // share few digits, expensive when they are all different)
   uint32_t ballot_mask = ~0u;
+  // bit p: pass p uses shared-memory peer masks instead (one atomicOr and
+  // one warp barrier per key: cheapest for many distinct 8-bit digits)
+  uint32_t smem_mask = 0u;
 };
 // Runs the passes; returns in *out_src the index of the buffer with the result.
 cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s);

@@ -443,6 +443,8 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
     so.num_bits = dbits;
     so.radix_bits = 8;
     so.hist = shist;
+    // depth digits of splats in index order are spread over all 256 values
+    so.smem_mask = ~0u;
     so.status2[0] = ctx->splat_lb[0].as<uint32_t>();
     so.status2[1] = ctx->splat_lb[1].as<uint32_t>();
     so.parity = &ctx->splat_parity;

@@ -7,8 +7,10 @@
 // Per pass and per 4096-key tile (256 threads x 16 keys, warp-striped so a
 // warp's item j is 32 consecutive keys):
 //   1. keys and payloads are loaded coalesced into registers;
-//   2. each warp ranks its 512 keys by digit with __match_any_sync, keeping a
-//      per-warp digit counter in shared memory (stable: ranks follow key order);
+//   2. each warp ranks its 512 keys by digit, 32 at a time (the lanes sharing
+//      a digit found by __match_any_sync, by one ballot per digit bit, or by
+//      shared-memory peer masks, chosen per pass), keeping a per-warp digit
+//      counter in shared memory (stable: ranks follow key order);
 //   3. per-digit counts are published to a chained look-back array, one thread
 //      per digit, and the keys are reordered by digit in shared memory (tile-
 //      local offsets only);
@@ -40,6 +42,12 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
 
+// Ranking modes of a pass: __match_any_sync (cheap when a warp's keys share
+// few digits), one ballot per digit bit (a fixed cost), or shared-memory
+// peer masks (each lane sets its bit in its digit's word; one warp barrier;
+// cheapest for many distinct 8-bit digits).
+constexpr uint32_t kRankMatch = 0, kRankBallot = 1, kRankSmem = 2;
+
 struct PassArgs {
   const uint32_t* keys_in;
   const uint32_t* v0_in;
@@ -57,7 +65,7 @@ struct PassArgs {
   uint32_t grid_tiles;     // tiles covered by the grid (all of clear_next)
   uint32_t* tile_ctr;
   uint32_t* status_word;
-  uint32_t ballot;         // 1: peers from per-bit ballots, 0: __match_any_sync
+  uint32_t rank;           // how a warp finds the lanes sharing a digit: kRank*
 };
 
 template <int RB, bool PAY2>
@@ -72,6 +80,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   uint32_t* s_tstart = s_whist + kSortWarps * R;  // [R]
   uint32_t* s_goff = s_tstart + R;               // [R]
   uint32_t* s_misc = s_goff + R;                 // [40]: tile, warp sums
+  uint32_t* s_wor = s_misc + 48;                 // [warps][3][R] peer masks (kRankSmem)
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   uint32_t n = *a.n_ptr;
@@ -79,6 +88,8 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   const uint32_t num_tiles = (n + kSortTile - 1) / kSortTile;
   if (tid == 0) s_misc[0] = atomicAdd(a.tile_ctr, 1u);
   for (uint32_t k = tid; k < kSortWarps * R; k += kSortThreads) s_whist[k] = 0u;
+  if (a.rank == kRankSmem)
+    for (uint32_t k = tid; k < kSortWarps * 3 * R; k += kSortThreads) s_wor[k] = 0u;
   __syncthreads();
   const uint32_t tile = s_misc[0];
   // Clear this tile's words of the other look-back buffer for the next pass
@@ -116,11 +127,22 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   // highest of them advances.
   uint32_t* wh = s_whist + warp * R;
   const uint32_t lt = lanemask_lt();
+  uint32_t prev_d = 0;
+  bool prev_lead = false;
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t d = (k[j] >> a.shift) & a.dmask;
     uint32_t peers;
-    if (a.ballot) {
+    if (a.rank == kRankSmem) {
+      // a step's words are cleared by their leaders one step later (after
+      // that step's barrier, so every lane has read them); three buffers
+      // keep a word from being reused before it is cleared
+      uint32_t* wo = s_wor + (warp * 3 + (j % 3)) * R;
+      atomicOr(&wo[d], 1u << lane);
+      __syncwarp();
+      peers = wo[d];
+      if (j >= 1 && prev_lead) s_wor[(warp * 3 + ((j + 2) % 3)) * R + prev_d] = 0u;
+    } else if (a.rank == kRankBallot) {
       peers = 0xffffffffu;
 #pragma unroll
       for (int b = 0; b < RB; ++b) {
@@ -131,6 +153,8 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
       peers = __match_any_sync(0xffffffffu, d);
     }
     const int leader = 31 - __clz(peers);
+    prev_lead = lane == leader;
+    prev_d = d;
     uint32_t old = 0;
     if (lane == leader) old = atomicAdd(&wh[d], (uint32_t)__popc(peers));
     old = __shfl_sync(0xffffffffu, old, leader);
@@ -233,14 +257,15 @@ __global__ void k_digit_bases(uint32_t* hist, uint32_t radix) {
 }
 
 template <int RB, bool PAY2>
-size_t onesweep_smem() {
+size_t onesweep_smem(uint32_t rank) {
   constexpr uint32_t R = 1u << RB;
-  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTileP + kSortWarps * R + 3 * R + 48);
+  return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTileP + kSortWarps * R + 3 * R + 48 +
+                             (rank == kRankSmem ? kSortWarps * 3 * R : 0u));
 }
 
 template <int RB, bool PAY2>
 cudaError_t launch_pass(const PassArgs& p, uint32_t grid, cudaStream_t s) {
-  const size_t smem = onesweep_smem<RB, PAY2>();
+  const size_t smem = onesweep_smem<RB, PAY2>(p.rank);
   // per device: set on every launch (a host-side attribute write)
   const cudaError_t e = cudaFuncSetAttribute(k_onesweep<RB, PAY2>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -327,7 +352,7 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.grid_tiles = tiles;
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
-    pa.ballot = (a.ballot_mask >> p) & 1u;
+    pa.rank = ((a.smem_mask >> p) & 1u) ? kRankSmem : (((a.ballot_mask >> p) & 1u) ? kRankBallot : kRankMatch);
     cudaError_t e;
     switch (rb) {
       case 4: e = pay2 ? launch_pass<4, true>(pa, tiles, s) : launch_pass<4, false>(pa, tiles, s); break;
