@@ -429,8 +429,10 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   if (sort_splats) {
     uint32_t* shist = (uint32_t*)(sc + L.shist);
     ctx->kbegin(CGS_K_SPLAT_SORT);
+    // balanced digits of at most 8 bits (19 depth bits -> 7 + 6 + 6)
+    const uint32_t spp = (dbits + 7) / 8, srb = std::max(4u, (dbits + spp - 1) / spp);
     CGS_CUDA(launch_histogram(ctx->skeys[0].as<uint32_t>(), &fc->active, ctx->splat_cap, 0, dbits,
-                              8, shist, s),
+                              srb, shist, s),
              "splat histogram");
     SortArgs so{};
     so.keys[0] = ctx->skeys[0].as<uint32_t>();
@@ -441,9 +443,9 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
     so.capacity = ctx->splat_cap;
     so.first_bit = 0;
     so.num_bits = dbits;
-    so.radix_bits = 8;
+    so.radix_bits = srb;
     so.hist = shist;
-    // depth digits of splats in index order are spread over all 256 values
+    // depth digits of splats in index order are spread over all values
     so.smem_mask = ~0u;
     so.status2[0] = ctx->splat_lb[0].as<uint32_t>();
     so.status2[1] = ctx->splat_lb[1].as<uint32_t>();
@@ -453,7 +455,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
     so.src = 0;
     CGS_CUDA(run_radix_sort(so, &ctx->s3_order_src, s), "splat sort");
     ctx->kend();
-    *splat_passes = sort_passes(dbits, 8);
+    *splat_passes = sort_passes(dbits, srb);
   }
   BinArgs b{};
   b.recs = ctx->recs.as<SplatRec>();

@@ -493,10 +493,10 @@ __global__ void __launch_bounds__(256) k_bin_place(const BinArgs a) {
     const uint32_t dst = a.offsets[32u * t];
     if (src >= cap || dst >= cap) continue;
     const uint32_t m = min(n, min(cap - src, cap - dst));
-    for (uint32_t k0 = 0; k0 < m; k0 += 128) {  // four loads in flight per lane and array
-      uint32_t kk[4], ii[4], dd[4];
+    for (uint32_t k0 = 0; k0 < m; k0 += 256) {  // eight loads in flight per lane and array
+      uint32_t kk[8], ii[8], dd[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const uint32_t k = k0 + 32u * u + lane;
         if (k < m) {
           kk[u] = __ldcs(a.stage_keys + src + k);
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(256) k_bin_place(const BinArgs a) {
         }
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const uint32_t k = k0 + 32u * u + lane;
         if (k < m) {
           a.keys[dst + k] = kk[u];
