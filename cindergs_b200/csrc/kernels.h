@@ -320,6 +320,11 @@ struct SortArgs {
                          // alternately; each pass clears the one it does not
                          // use for the next pass, so no per-frame memset is needed
   int* parity;           // in/out: buffer index the next pass uses (with status2)
+  // words per tile that each pass clears in the status2 buffer it does not
+  // use (0: the radix). A pair shared by sorts of different digit widths sets
+  // the widest radix (256), so that a narrow sort leaves no stale word for a
+  // later wide one to read.
+  uint32_t lb_stride = 0;
   uint32_t* tile_ctr;    // [passes] zeroed
   uint32_t* status_word;
   int src;               // index of the buffer holding the input

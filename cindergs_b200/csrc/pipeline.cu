@@ -450,6 +450,9 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
     so.status2[0] = ctx->splat_lb[0].as<uint32_t>();
     so.status2[1] = ctx->splat_lb[1].as<uint32_t>();
     so.parity = &ctx->splat_parity;
+    // the digit width follows the frame's depth bits (8 at 360p, 7 at 1080p):
+    // clear the full 256-word stride so a narrower sort leaves no stale words
+    so.lb_stride = 256;
     so.tile_ctr = rtiles + kSplatSortTileCtr;
     so.status_word = &fc->status;
     so.src = 0;

@@ -61,7 +61,8 @@ struct PassArgs {
   uint32_t dmask;          // digit mask of this pass (narrower on a final partial pass)
   const uint32_t* dbase;   // this pass's exclusive digit bases (k_digit_bases)
   uint32_t* status;        // this pass's [tiles][radix] look-back words
-  uint32_t* clear_next;    // [tiles][radix] words to zero for the next pass, or null
+  uint32_t* clear_next;    // [tiles][clear_stride] words to zero for the next pass, or null
+  uint32_t clear_stride;   // words per tile of clear_next (>= radix)
   uint32_t grid_tiles;     // tiles covered by the grid (all of clear_next)
   uint32_t* tile_ctr;
   uint32_t* status_word;
@@ -94,8 +95,11 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   const uint32_t tile = s_misc[0];
   // Clear this tile's words of the other look-back buffer for the next pass
   // (the pass that used it has completed: passes are stream-ordered launches).
+  // Every block of the grid clears its stride, so the whole buffer is clean
+  // whatever radix the previous sort on it used.
   if (a.clear_next && tile < a.grid_tiles)
-    for (uint32_t k = tid; k < R; k += kSortThreads) a.clear_next[(size_t)tile * R + k] = 0u;
+    for (uint32_t k = tid; k < a.clear_stride; k += kSortThreads)
+      a.clear_next[(size_t)tile * a.clear_stride + k] = 0u;
   if (tile >= num_tiles) return;
 
   // Load (warp-striped: a warp's item j is 32 consecutive keys). Full tiles,
@@ -344,11 +348,14 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
       const int par = *a.parity;
       pa.status = a.status2[par];
       pa.clear_next = a.status2[par ^ 1];
+      pa.clear_stride = a.lb_stride ? a.lb_stride : R;
       *a.parity = par ^ 1;
     } else {
       pa.status = a.status + (size_t)p * tiles * R;
       pa.clear_next = nullptr;
+      pa.clear_stride = 0;
     }
+    if (pa.clear_stride < R && pa.clear_next) return cudaErrorInvalidValue;
     pa.grid_tiles = tiles;
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;

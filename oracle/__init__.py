@@ -109,6 +109,16 @@ def lib():
         L.orc_ref_frame.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _c_u32, _vp, _vp, _vp, _vp,
                                     _vp, _f32p, _c_u32, _c_u32, _f32p, _f32p, _c_u32, _c_f, _c_f,
                                     _u8p, ctypes.POINTER(_c_u32)]
+        L.orc_ref_ellipse_tile.restype = ctypes.c_int
+        L.orc_ref_ellipse_tile.argtypes = [_c_f] * 6 + [_c_u32] * 4
+        L.orc_ref_tile_bounds_xy.restype = ctypes.c_int
+        L.orc_ref_tile_bounds_xy.argtypes = [_c_f] * 4 + [_c_u32] * 4 + [_u32p]
+        L.orc_pack_depth.restype = _c_u32
+        L.orc_pack_depth.argtypes = [_c_f, _c_f, _c_u32]
+        L.orc_ref_deform.restype = _c_u32
+        L.orc_ref_deform.argtypes = [_c_u32, _f32p, _f32p, _f32p, _f32p, _c_u32, _f32p, _u32p,
+                                     _f32p, _u32p, _f32p, _c_u32, _c_f, _c_f, _f32p, _f32p, _f32p,
+                                     _f32p]
         _lib = L
     return _lib
 
@@ -350,6 +360,47 @@ def ref_render_scene(scene, cam24, W, H, bg, cam_pos, sh_degree):
 def pixel_hash(rgba8) -> int:
     b = np.ascontiguousarray(rgba8, dtype=np.uint8).ravel()
     return int(lib().orc_pixel_hash(b.size, b))
+
+
+def ref_ellipse_tile(mu_x, mu_y, conic, alpha, tx, ty, W, H) -> bool:
+    """ellipse_intersects_tile (render/tiles/mod.rs:139-184), glibc logf cutoff."""
+    return bool(lib().orc_ref_ellipse_tile(mu_x, mu_y, conic[0], conic[1], conic[2], alpha, tx,
+                                           ty, W, H))
+
+
+def ref_tile_bounds_xy(cx, cy, ex, ey, tiles_x, tiles_y, W, H):
+    """compute_gaussian_tile_bounds_xy (render/tiles/mod.rs:97-130): None or
+    (tx0, tx1, ty0, ty1)."""
+    box = np.zeros(4, np.uint32)
+    ok = lib().orc_ref_tile_bounds_xy(cx, cy, ex, ey, tiles_x, tiles_y, W, H, box)
+    return tuple(int(v) for v in box) if ok else None
+
+
+def pack_depth(tz, near_plane, depth_bits) -> int:
+    """pack_relative_depth_bits (render/kernels/binning.rs:25-31)."""
+    return int(lib().orc_pack_depth(float(tz), float(near_plane), int(depth_bits)))
+
+
+def ref_deform(scene, cage, sh_degree=3, split_thr=0.0, mip=0.0):
+    """deform_cage_scene_cpu restated (ref mode, cpu_reference.rs:157-404):
+    dict(pos [m,3], cov [m,6], opa [m], sh [m,48]) with split children
+    appended in parent order. ``cage`` = dict(verts, elems, inv_dm, bind_tet,
+    bind_w) with global tet indices."""
+    n = int(np.asarray(scene["opa"]).size)
+    elems = _u32(cage["elems"]).ravel()
+    op = np.zeros(2 * n * 3, np.float32)
+    oc = np.zeros(2 * n * 6, np.float32)
+    oa = np.zeros(2 * n, np.float32)
+    osh = np.zeros(2 * n * 48, np.float32)
+    m = lib().orc_ref_deform(n, _f32(scene["pos"]).ravel(), _f32(scene["cov"]).ravel(),
+                             _f32(scene["opa"]).ravel(), _f32(scene["sh"]).ravel(),
+                             elems.size // 4, _f32(cage["verts"]).ravel(), elems,
+                             _f32(cage["inv_dm"]).ravel(), _u32(cage["bind_tet"]).ravel(),
+                             _f32(cage["bind_w"]).ravel(), int(sh_degree), float(split_thr),
+                             float(mip), op, oc, oa, osh)
+    m = int(m)
+    return dict(pos=op[:3 * m].reshape(m, 3), cov=oc[:6 * m].reshape(m, 6), opa=oa[:m],
+                sh=osh[:48 * m].reshape(m, 48))
 
 
 def ref_tet_transforms(verts, elems, inv_dm):

@@ -1682,6 +1682,55 @@ uint64_t orc_ref_render_scene(uint32_t n, const float* pos, const float* cov, co
 
 extern "C" {
 
+// ellipse_intersects_tile (render/tiles/mod.rs:139-184): the CPU-side twin of
+// the kernels' test, 16x16 tiles, with the cutoff from glibc logf (Rust's
+// f32::ln on Linux) instead of the deterministic logarithm of the v2 mode.
+int orc_ref_ellipse_tile(float mu_x, float mu_y, float a, float b, float c, float alpha,
+                         uint32_t tx, uint32_t ty, uint32_t W, uint32_t H) {
+  if (alpha < (1.0f / 255.0f) || W == 0 || H == 0) return 0;
+  const uint32_t x_start = tx * 16u, y_start = ty * 16u;
+  if (x_start >= W || y_start >= H) return 0;
+  const float dx0 = ((float)x_start + 0.5f) - mu_x;
+  const float dx1 = ((float)std::min(x_start + 15u, W - 1u) + 0.5f) - mu_x;
+  const float dy0 = ((float)y_start + 0.5f) - mu_y;
+  const float dy1 = ((float)std::min(y_start + 15u, H - 1u) + 0.5f) - mu_y;
+  const float x_near = clampf(0.0f, dx0, dx1);
+  const float y1 = clampf(-b * x_near / std::fmax(c, 1e-12f), dy0, dy1);
+  const float q1 = a * x_near * x_near + 2.0f * b * x_near * y1 + c * y1 * y1;
+  const float y_near = clampf(0.0f, dy0, dy1);
+  const float x2 = clampf(-b * y_near / std::fmax(a, 1e-12f), dx0, dx1);
+  const float q2 = a * x2 * x2 + 2.0f * b * x2 * y_near + c * y_near * y_near;
+  const float q_cut = clampf(2.0f * logf(255.0f * alpha), 0.0f, 8.0f);
+  return std::fmin(q1, q2) <= q_cut + 1e-4f ? 1 : 0;
+}
+
+// compute_gaussian_tile_bounds_xy (render/tiles/mod.rs:97-130), 16x16 tiles:
+// returns 0 when culled or off screen, else 1 with box = tx0, tx1, ty0, ty1.
+int orc_ref_tile_bounds_xy(float cxp, float cyp, float ex, float ey, uint32_t tiles_x,
+                           uint32_t tiles_y, uint32_t W, uint32_t H, uint32_t* box) {
+  const uint32_t tw = g_tile_w, th = g_tile_h;
+  g_tile_w = g_tile_h = 16;
+  TileBox tb{};
+  const bool ok = tile_bounds_xy(cxp, cyp, ex, ey, tiles_x, tiles_y, W, H, &tb);
+  g_tile_w = tw;
+  g_tile_h = th;
+  if (!ok) return 0;
+  box[0] = tb.x0;
+  box[1] = tb.x1;
+  box[2] = tb.y0;
+  box[3] = tb.y1;
+  return 1;
+}
+
+// pack_relative_depth_bits (render/kernels/binning.rs:25-31).
+uint32_t orc_pack_depth(float tz, float near_plane, uint32_t depth_bits) {
+  const uint32_t db = std::min(depth_bits, 28u);
+  const uint32_t base = f2u(std::fmax(near_plane, 1e-6f)) & 0x7F800000u;
+  const uint32_t raw = f2u(std::fmax(tz, 1e-6f));
+  const uint32_t rel = raw > base ? std::min(raw - base, 0x0FFFFFFFu) : 0u;
+  return rel >> (28u - db);
+}
+
 // Reference CPU tet transforms (for tests): J, R column-major, max stretch.
 void orc_ref_tet_transforms(uint32_t T, const float* verts, const uint32_t* elems,
                             const float* inv_dm, float* J, float* R, float* stretch) {
@@ -1710,22 +1759,23 @@ void orc_ref_sh_rotate(uint32_t n, float* sh, const float* R9, uint32_t degree) 
   for (uint32_t i = 0; i < n; ++i) apply_sh_rotation(r, sh + 48 * (size_t)i);
 }
 
-// execute_cpu_reference_with_options (render/pipeline.rs:420-507) for one tet
-// cage set: deform_cage_scene_cpu (SH coefficients rotated per tet, strain
-// split with the f64 eigen-solver, 3D Mip filter), project_scene_cull_cpu
-// (sequential loop, render/mod.rs:226-285), bin_and_sort_active (square radius,
-// tiles/cpu_reference.rs:307-402) and rasterize_scene_cpu. `verts` are the
-// current flattened cage vertices; bind_tet holds global tet indices.
-// Returns the number of tile entries; *out_splits receives the child count.
-uint64_t orc_ref_frame(uint32_t n, const float* pos, const float* cov, const float* opa,
-                       const float* sh, uint32_t T, const float* verts, const uint32_t* elems,
-                       const float* inv_dm, const uint32_t* bind_tet, const float* bind_w,
-                       const float* cam24, uint32_t W, uint32_t H, const float* bg,
-                       const float* cam_pos, uint32_t sh_degree, float split_thr, float mip,
-                       uint8_t* rgba8, uint32_t* out_splits) {
+// deform_cage_scene_cpu (deformation/cpu_reference.rs:157-404) for one tet
+// cage set: position sum, J S J^T with the 1e-4 floor, det-J opacity rule,
+// SH coefficients rotated per tet (degree sh_degree), then the sequential
+// strain split with the f64 eigen-solver and the 3D Mip filter. Children are
+// appended in parent order. Returns the output count (n + children).
+static uint32_t ref_deform_scene(uint32_t n, const float* pos, const float* cov, const float* opa,
+                                 const float* sh, uint32_t T, const float* verts,
+                                 const uint32_t* elems, const float* inv_dm,
+                                 const uint32_t* bind_tet, const float* bind_w,
+                                 uint32_t sh_degree, float split_thr, float mip,
+                                 std::vector<float>& dpos, std::vector<float>& dcov,
+                                 std::vector<float>& dopa, std::vector<float>& dsh) {
+  dpos.assign(pos, pos + 3 * (size_t)n);
+  dcov.assign(cov, cov + 6 * (size_t)n);
+  dopa.assign(opa, opa + n);
+  dsh.assign(sh, sh + 48 * (size_t)n);
   const bool has_cages = T > 0;
-  std::vector<float> dpos(pos, pos + 3 * (size_t)n), dcov(cov, cov + 6 * (size_t)n),
-      dopa(opa, opa + n), dsh(sh, sh + 48 * (size_t)n);
   uint32_t total = n;
   if (has_cages) {
     std::vector<RefTet> tets(T);
@@ -1815,6 +1865,44 @@ uint64_t orc_ref_frame(uint32_t n, const float* pos, const float* cov, const flo
       ++total;
     }
   }
+  return total;
+}
+
+// deform_cage_scene_cpu / deform_scene_adaptive_cpu restated (ref mode, one
+// tet cage set, see ref_deform_scene). Outputs hold 2n slots (out_sh 2n x 48);
+// returns the output count.
+uint32_t orc_ref_deform(uint32_t n, const float* pos, const float* cov, const float* opa,
+                        const float* sh, uint32_t T, const float* verts, const uint32_t* elems,
+                        const float* inv_dm, const uint32_t* bind_tet, const float* bind_w,
+                        uint32_t sh_degree, float split_thr, float mip, float* out_pos,
+                        float* out_cov, float* out_opa, float* out_sh) {
+  std::vector<float> dpos, dcov, dopa, dsh;
+  const uint32_t total = ref_deform_scene(n, pos, cov, opa, sh, T, verts, elems, inv_dm, bind_tet,
+                                          bind_w, sh_degree, split_thr, mip, dpos, dcov, dopa, dsh);
+  std::memcpy(out_pos, dpos.data(), sizeof(float) * 3 * (size_t)total);
+  std::memcpy(out_cov, dcov.data(), sizeof(float) * 6 * (size_t)total);
+  std::memcpy(out_opa, dopa.data(), sizeof(float) * (size_t)total);
+  if (out_sh) std::memcpy(out_sh, dsh.data(), sizeof(float) * 48 * (size_t)total);
+  return total;
+}
+
+// execute_cpu_reference_with_options (render/pipeline.rs:420-507) for one tet
+// cage set: deform_cage_scene_cpu (SH coefficients rotated per tet, strain
+// split with the f64 eigen-solver, 3D Mip filter), project_scene_cull_cpu
+// (sequential loop, render/mod.rs:226-285), bin_and_sort_active (square radius,
+// tiles/cpu_reference.rs:307-402) and rasterize_scene_cpu. `verts` are the
+// current flattened cage vertices; bind_tet holds global tet indices.
+// Returns the number of tile entries; *out_splits receives the child count.
+uint64_t orc_ref_frame(uint32_t n, const float* pos, const float* cov, const float* opa,
+                       const float* sh, uint32_t T, const float* verts, const uint32_t* elems,
+                       const float* inv_dm, const uint32_t* bind_tet, const float* bind_w,
+                       const float* cam24, uint32_t W, uint32_t H, const float* bg,
+                       const float* cam_pos, uint32_t sh_degree, float split_thr, float mip,
+                       uint8_t* rgba8, uint32_t* out_splits) {
+  const bool has_cages = T > 0;
+  std::vector<float> dpos, dcov, dopa, dsh;
+  const uint32_t total = ref_deform_scene(n, pos, cov, opa, sh, T, verts, elems, inv_dm, bind_tet,
+                                          bind_w, sh_degree, split_thr, mip, dpos, dcov, dopa, dsh);
   if (out_splits) *out_splits = total - n;
   // project_scene_cull_cpu: sequential loop (render/mod.rs:248).
   std::vector<float> xy(2 * (size_t)total), depth(total), conic(3 * (size_t)total),

@@ -1,0 +1,172 @@
+"""Parity at the benchmark sizes: the frames behind the reported numbers,
+checked against the oracle (v2 mode) at full size.
+
+* the tet-cage frame exactly as bench.py renders it: 1,100,000 Gaussians,
+  1920x1080, the 750-tet spring cage after a few solver steps (GPU binding,
+  Stage 1 positions/covariances/opacities, Stage 2 records and extents, Stage
+  3 offsets/keys/ids/ranges bit-exact over ~26M tile entries, RGB <= 2e-3);
+* frames alternating 640x360 and 1920x1080 on a 1M-Gaussian scene (the splat
+  depth sort changes digit width between them: 8 bits at 360p, 7 at 1080p);
+* the quantized (f16) scene ingest against the oracle fed the dequantized
+  f32 arrays;
+* one mixed-resolution step of cgs_execute_views (640x360, 1280x720,
+  1920x1080), each view against the oracle;
+* a 7680x4320 frame (129,600 tiles, 64-bit keys) of the large multi-cage
+  scene on a Gaussian subsample, with its four spring-driven tet cages.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cindergs_b200 import (CageScene, GpuPipelineState, QuantizedGaussianSceneSoa, random_scene,
+                           workloads)
+from cindergs_b200 import _abi
+from helpers import assert_stage23_exact, compositor, config0_camera, gpu_buffers, oracle_frame
+
+pytestmark = pytest.mark.gpu
+RGB_TOL = 2e-3
+
+
+def bits(a):
+    return np.asarray(a, np.float32).view(np.uint32)
+
+
+def cage_dict(cages):
+    elems, inv, nverts, bt, bw = cages.flatten()
+    return dict(verts=cages.flat_vertices(), elems=elems, inv_dm=inv, bind_tet=bt, bind_w=bw)
+
+
+def stage1_buffers(st):
+    return dict(pos=st.read_buffer(_abi.BUF_DEFORMED_POS, np.float32),
+                cov=st.read_buffer(_abi.BUF_DEFORMED_COV, np.float32),
+                opa=st.read_buffer(_abi.BUF_DEFORMED_OPA, np.float32))
+
+
+@pytest.fixture(scope="module")
+def st():
+    s = GpuPipelineState(0)
+    yield s
+    s.close()
+
+
+def test_bench_frame_full_size(st):
+    wl = workloads.tet_cage_orbit()
+    st.upload_scene(wl.scene)
+    cages = wl.bind(st)
+    mesh = wl.cage.mesh
+    ot, ow = oracle.bind_points(wl.scene.positions, mesh.rest_vertices, mesh.elements,
+                                mesh.inv_dm, mesh.bounds())
+    np.testing.assert_array_equal(cages.bind_tet, ot, err_msg="bound tets")
+    np.testing.assert_array_equal(bits(cages.bind_w), bits(ow), err_msg="barycentric weights")
+    for _ in range(3):
+        wl.step()
+    cam = wl.camera(3)
+    comp = wl.compositor(cam)
+    t = st.execute_frame_gpu(wl.scene, cages, cam, comp, wl.strain_split_threshold,
+                             wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, force_stage3=True,
+                             write_f32=True)
+    g = gpu_buffers(st)
+    g.update(stage1_buffers(st))
+    img = st.readback_framebuffer_f32(wl.width, wl.height)
+    o = oracle_frame(wl.scene, cam, comp, cage=cage_dict(cages), mip=wl.mip_filter_3d_var,
+                     split_thr=wl.strain_split_threshold)
+    n = wl.scene.count
+    assert t.active_gaussians == n + o["splits"]
+    assert t.total_tile_entries == o["entries"] > 20_000_000
+    np.testing.assert_array_equal(bits(g["pos"][:3 * n]), bits(o["def_pos"][:3 * n]),
+                                  err_msg="deformed positions")
+    np.testing.assert_array_equal(bits(g["cov"][:6 * n]), bits(o["def_cov"][:6 * n]),
+                                  err_msg="deformed covariances")
+    np.testing.assert_array_equal(bits(g["opa"][:n]), bits(o["def_opa"][:n]),
+                                  err_msg="deformed opacities")
+    assert_stage23_exact(g, o)
+    err = float(np.abs(img - o["rgba_f32"]).max())
+    assert err <= RGB_TOL, err
+
+
+def test_alternating_resolutions_1m(st):
+    """360p (8-bit splat-sort digits) and 1080p (7-bit digits) frames in turn:
+    each sort reads look-back words that the previous, differently wide
+    sort left behind, so every frame checks that they were cleared."""
+    scene = random_scene(1_000_000, seed=4)
+    st.upload_scene(scene)
+    st.upload_cages(None)
+    for i, (w, h) in enumerate([(640, 360), (1920, 1080), (640, 360), (1920, 1080)]):
+        cam = config0_camera(w, h)
+        comp = compositor(w, h, cam, deg=3, bg=(0.0, 0.0, 0.0, 1.0))
+        t = st.execute_frame_gpu(scene, None, cam, comp, force_stage3=True, write_f32=True)
+        g = gpu_buffers(st)
+        img = st.readback_framebuffer_f32(w, h)
+        o = oracle_frame(scene, cam, comp)
+        assert t.total_tile_entries == o["entries"] > 1_000_000, (i, w, h)
+        assert_stage23_exact(g, o)
+        assert float(np.abs(img - o["rgba_f32"]).max()) <= RGB_TOL, (i, w, h)
+
+
+def test_quantized_frame_vs_oracle(st):
+    """The f16 ingest (cgs_scene_upload_quantized: covariance pairs and
+    degree-3 SH decoded on the GPU) renders what the oracle renders from the
+    dequantized arrays (binary16 -> binary32 is exact)."""
+    q = QuantizedGaussianSceneSoa.from_soa(random_scene(300_000, seed=8, box=1.0), 3)
+    # the reference's f16 decode cases (tests/gpu_parity_tests.rs:1268-1293)
+    # in the first splats: subnormal, negative subnormal, signed zero and
+    # max-finite halves
+    h = lambda x: int(np.float16(x).view(np.uint16))  # noqa: E731
+    cases = np.array([[h(0.05), 0x0001, 0x8001, h(0.04), 0x03FF, h(0.06)],
+                      [h(12.5), h(-0.75), 0x8000, h(8.0), 0x0000, h(10.0)],
+                      [0x7BFF, 0, 0, h(1.0), 0, h(1.0)]], np.uint32)
+    q.covariances_f16_packed[:3] = cases[:, 0::2] | (cases[:, 1::2] << 16)
+    deq = q.to_soa()
+    st.upload_scene(q)
+    st.upload_cages(None)
+    cam = config0_camera(1920, 1080)
+    comp = compositor(1920, 1080, cam, deg=3, bg=(0.0, 0.0, 0.0, 1.0))
+    t = st.execute_frame_gpu(q, None, cam, comp, force_stage3=True, write_f32=True)
+    g = gpu_buffers(st)
+    img = st.readback_framebuffer_f32(1920, 1080)
+    o = oracle_frame(deq, cam, comp)
+    assert t.total_tile_entries == o["entries"] > 1_000_000
+    assert_stage23_exact(g, o)
+    assert float(np.abs(img - o["rgba_f32"]).max()) <= RGB_TOL
+
+
+def test_mixed_resolution_views_vs_oracle(st):
+    wl, cams, comps = workloads.multiview_cage(n=400_000, views=3)
+    st.upload_scene(wl.scene)
+    cages = wl.bind(st)
+    for _ in range(2):
+        wl.step()
+    imgs = st.view_images(comps)
+    for use_graph in (False, True, True):  # eager, capture, replay
+        stats = st.execute_views(wl.scene, cages, cams, comps, imgs, use_graph=use_graph)
+        assert stats["total_tile_entries"] > 0
+        for v, (cam, comp) in enumerate(zip(cams, comps)):
+            got = imgs[v].cpu().numpy().view(np.uint8).reshape(comp.screen_height,
+                                                               comp.screen_width, 4)
+            o = oracle_frame(wl.scene, cam, comp, cage=cage_dict(cages))
+            d = np.abs(got.astype(np.int32) - o["rgba8"].astype(np.int32))
+            assert d.max() <= 1, (use_graph, v, d.max())
+        wl.step()
+
+
+def test_8k_64bit_multicage_subsample(st):
+    """The large workload's geometry (four 384-tet spring cages over the upper
+    half, 7680x4320, 129,600 tiles, 64-bit keys) on 400,000 of its Gaussians;
+    the quantized layout and the learned polygon cage are checked by their own
+    tests."""
+    wl = workloads.large_multicage(n=400_000)
+    scene = wl.scene.to_soa()
+    st.upload_scene(scene)
+    cs = CageScene.auto_bind(wl.cages, st, scene.count)
+    cs.step(1.0 / 60.0)
+    cs.step(1.0 / 60.0)
+    cam = wl.camera(2)
+    comp = wl.compositor(cam)
+    t = st.execute_frame_gpu(scene, cs, cam, comp, force_stage3=True, write_f32=True)
+    assert t.used_64bit_keys
+    g = gpu_buffers(st, key64=True)
+    img = st.readback_framebuffer_f32(wl.width, wl.height)
+    o = oracle_frame(scene, cam, comp, cage=cage_dict(cs))
+    assert t.total_tile_entries == o["entries"] > 1_000_000
+    assert_stage23_exact(g, o, key64=True)
+    assert float(np.abs(img - o["rgba_f32"]).max()) <= RGB_TOL
