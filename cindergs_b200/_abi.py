@@ -127,6 +127,8 @@ SIGNATURES = {
     "cgs_ctx_synchronize": (_int, [_vp]),
     "cgs_ctx_device_bytes": (_int, [_vp, ctypes.POINTER(_u64)]),
     "cgs_version": (ctypes.c_char_p, []),
+    "cgs_ctx_set_device_budget": (_int, [_vp, _u64]),
+    "cgs_ctx_wait_drill": (_int, [_vp, _u32, ctypes.POINTER(_u32)]),
     "cgs_scene_upload": (_int, [_vp, _u64, _vp, _vp, _vp, _vp, _i32]),
     "cgs_tet_cages_upload": (_int, [_vp, _u32, _vp, _vp, _u32, _vp, _vp]),
     "cgs_cage_vertices_update": (_int, [_vp, _vp, _u32]),

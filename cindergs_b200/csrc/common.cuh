@@ -15,6 +15,10 @@ constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kStatusLookbackTimeout = 1u;
 constexpr uint32_t kStatusCapacity = 2u;
 constexpr uint32_t kStatusBarrierTimeout = 4u;
+// A tensor-core wait gave up twice: MMAs may still be writing tensor memory
+// that the kernel released on exit, so the device state is undefined and the
+// context must be rebuilt.
+constexpr uint32_t kStatusPoisoned = 8u;
 
 // Upper bound on polls of a lookback or mbarrier wait before a kernel gives
 // up, sets a status bit and carries on with whatever it has (the frame's
@@ -29,7 +33,13 @@ struct FrameCounters {
   uint32_t status;       // kStatus* bits
   uint32_t fetched;      // splat records the compositor gathered
   uint32_t tile_ctr[16]; // dynamic tile counters for chained-scan kernels
+  uint32_t pad;
+  unsigned long long stage_ctr;  // binning: staged entries so far (64 bits: never wraps)
 };
+// Largest tile-entry capacity of a frame (32-bit entry indices; a multiple
+// of the radix sort's 4096-entry tiles; the entry sort's look-back words are
+// 64 bits wide, so counts are not limited to 2^30).
+constexpr uint32_t kMaxEntryCap = 0xFFFF0000u;
 
 // Splat record written by Stage 2 and read by Stages 3 and 4: 48 bytes, three
 // 16-byte words so one bulk copy moves a whole record.
@@ -63,6 +73,11 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 }
 __device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
   uint32_t v;
@@ -109,9 +124,10 @@ __device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t v, uint32_t* wa
 // (a dynamic tile counter), so every tile a block waits on is held by a block
 // that is already resident. Called by all lanes of ONE warp; returns the
 // exclusive prefix of `tile` and publishes its inclusive prefix. A wait that
-// exceeds kSpinLimit polls sets kStatusLookbackTimeout and returns 0.
+// exceeds `limit` polls sets kStatusLookbackTimeout and returns 0.
 __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status, uint32_t tile,
-                                                      uint32_t aggregate, uint32_t* status_word) {
+                                                      uint32_t aggregate, uint32_t* status_word,
+                                                      uint32_t limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
     if (lane == 0) st_relaxed_u64(&status[0], (2ull << 32) | aggregate);
@@ -126,7 +142,7 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
     long long mine = pred - lane;
     unsigned long long st = mine >= 0 ? ld_relaxed_u64(&status[mine]) : (2ull << 32);
     while (__any_sync(0xffffffffu, (st >> 32) == 0ull)) {
-      if (++spins > kSpinLimit) {
+      if (++spins > limit) {
         timed_out = true;
         break;
       }

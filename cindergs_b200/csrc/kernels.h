@@ -38,7 +38,14 @@ struct DeformArgs {
   // (9 floats, column-major) out for Stage 2's SH directions
   const float4* mvc_xf;
   float* mvc_R;
+  // 1: the deform launch also computes the tet transforms (its first blocks
+  // take the tets; the Gaussian blocks wait for them), instead of a separate
+  // launch_tet_transforms
+  uint32_t fuse_tets;
 };
+// FrameCounters::tile_ctr slot counting the finished tet blocks of a fused
+// deform launch.
+constexpr int kTetsDoneCtr = 8;
 cudaError_t launch_tet_transforms(const DeformArgs& a, cudaStream_t s);
 
 // ---- MVC (stage1_mvc.cu) -----------------------------------------------------
@@ -237,6 +244,7 @@ struct BinArgs {
   uint32_t* offsets;            // [max_n]
   uint32_t* tile_stage;         // [ceil(max_n/32)] staging start of each 32-slot tile
   uint32_t* tile_count;         // [ceil(max_n/32)] entries of each 32-slot tile
+  const uint32_t* run_start;    // placement: first entry of each 32-slot tile (else offsets)
   FrameCounters* fc;
   int key64;
   uint32_t depth_bits;          // depth bits in a 32-bit key
@@ -264,6 +272,11 @@ struct BinArgs {
 // total -> fc->entries) and places the staged entries (launch_bin_place).
 cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s);
 cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s);
+// first_run[t] = the run holding position t * kRadixTileItems, for every t
+// whose first position lies in a non-empty run (runs: run_start [num_runs]
+// exclusive starts, run_len [num_runs] lengths); at most max_tiles entries.
+cudaError_t launch_run_index(const uint32_t* run_start, const uint32_t* run_len, uint32_t num_runs,
+                             uint32_t* first_run, uint32_t max_tiles, cudaStream_t s);
 // Tile transpose (the entry sort when the tiles fit shared memory): a
 // one-pass stable counting sort of the staged records by tile. Chunk k is the
 // 32-slot tiles [k * chunk_wtiles, (k + 1) * chunk_wtiles); warp w of a chunk
@@ -315,11 +328,14 @@ struct SortArgs {
   uint32_t radix_bits;   // digit width, 4..8
   uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
                          // (turned into exclusive bases in place by the sort)
-  uint32_t* status;      // [passes][tiles][radix] zeroed (when status2 is null)
-  uint32_t* status2[2];  // optional: two [tiles][radix] look-back buffers used
+  void* status;          // [passes][tiles][radix] zeroed look-back words (when status2 is null)
+  void* status2[2];      // optional: two [tiles][radix] look-back buffers used
                          // alternately; each pass clears the one it does not
                          // use for the next pass, so no per-frame memset is needed
   int* parity;           // in/out: buffer index the next pass uses (with status2)
+  // look-back words of 64 bits (any 32-bit count; required above 2^30
+  // elements) instead of 32 bits (counts below 2^30)
+  bool wide_lookback = false;
   // words per tile that each pass clears in the status2 buffer it does not
   // use (0: the radix). A pair shared by sorts of different digit widths sets
   // the widest radix (256), so that a narrow sort leaves no stale word for a
@@ -335,7 +351,27 @@ struct SortArgs {
   // bit p: pass p uses shared-memory peer masks instead (one atomicOr and
   // one warp barrier per key: cheapest for many distinct 8-bit digits)
   uint32_t smem_mask = 0u;
+  // Optional: the input (buffer `src`) is staged in runs: position q of the
+  // input order is element run_src[k] + q - run_start[k] for the run k holding
+  // q (run_start: exclusive scan of the run lengths, runs in input order;
+  // first_run[t]: the run holding position 4096 t, launch_run_index). The
+  // first pass gathers them; no placement pass is needed.
+  const uint32_t* run_start = nullptr;
+  const uint32_t* run_src = nullptr;
+  const uint32_t* first_run = nullptr;
+  uint32_t num_runs = 0;
 };
+// Entries per radix sort tile (the unit of first_run).
+constexpr uint32_t kRadixTileItems = 4096;
+// Wait drills (cgs_ctx_wait_drill): each runs one of the library's bounded
+// device waits against a predecessor or barrier that nothing completes, with
+// `limit` polls, so that it gives up and sets its status bit in *status_word.
+// The look-back arrays must hold two zeroed tiles.
+cudaError_t launch_drill_chained_scan(unsigned long long* status, uint32_t* status_word,
+                                      uint32_t limit, cudaStream_t s);
+cudaError_t launch_drill_digit_lookback(const uint32_t* status, uint32_t radix,
+                                        uint32_t* status_word, uint32_t limit, cudaStream_t s);
+cudaError_t launch_drill_mbarrier(uint32_t* status_word, uint32_t limit, cudaStream_t s);
 // Runs the passes; returns in *out_src the index of the buffer with the result.
 cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s);
 cudaError_t launch_histogram(const uint32_t* keys, const uint32_t* n_ptr, uint32_t capacity,

@@ -417,7 +417,9 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   }
   if (!ok && leader) {
     if (fi.status) atomicOr(fi.status, kStatusBarrierTimeout);
-    mbar_wait(mbar, phase ^ 1u);  // the MMAs given up on, once more (bounded)
+    // the MMAs given up on, once more (bounded); if they still have not
+    // completed, tensor memory may be written after the release below
+    if (!mbar_wait(mbar, phase ^ 1u) && fi.status) atomicOr(fi.status, kStatusPoisoned);
   }
   // release TMEM once every warpgroup is done with it
   tc_fence_before();

@@ -198,6 +198,7 @@ struct cgs_ctx {
   // arena
   DevBuf tet_J, tet_R, tet_S, def_pos, def_cova, def_covb, split_meta, persist;
   DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
+  DevBuf run_index;  // per radix tile of the entry sort: the staged run holding its first entry
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
   // SH coefficient rotation (cgs_sh_rotate, cgs_export_deformed): the band
@@ -290,6 +291,7 @@ struct cgs_ctx {
   bool kprof = false;
   cgs_kernel_profile kp_acc{};
   int sticky = CGS_OK;       // error found while checking an older frame
+  bool poisoned = false;     // kStatusPoisoned seen: frames refuse to run
   std::string sticky_msg;
 
   void kbegin(int id) {
@@ -315,12 +317,20 @@ struct cgs_ctx {
     err = std::string(what) + ": " + cudaGetErrorString(e);
     return CGS_E_CUDA;
   }
+  // Device bytes the arena may hold (cgs_ctx_set_device_budget; 0 = no
+  // limit) and the bytes its growable buffers hold now.
+  uint64_t budget = 0, held = 0;
   int ensure(DevBuf& b, size_t bytes, const char* what) {
     if (bytes <= b.cap && b.p) return CGS_OK;
     size_t nb = grow(b.cap, bytes);
+    if (budget && held - b.cap + nb > budget)
+      return fail(CGS_E_OOM, std::string("device memory budget of ") + std::to_string(budget) +
+                                 " bytes exceeded by " + what + " (" + std::to_string(nb) +
+                                 " bytes with " + std::to_string(held - b.cap) + " held)");
     if (b.p) {
       cudaStreamSynchronize(stream);
       cudaFree(b.p);
+      held -= b.cap;
       b.p = nullptr;
       b.cap = 0;
     }
@@ -332,6 +342,7 @@ struct cgs_ctx {
                                  std::to_string(nb) + " bytes): " + cudaGetErrorString(e));
     }
     b.cap = nb;
+    held += nb;
     return CGS_OK;
   }
   int take_sticky() {
@@ -364,8 +375,9 @@ int ensure_entry_buffers(cgs_ctx* ctx, uint32_t cap, bool key64, uint32_t radix_
     if (key64) CGS_TRY(ctx->ensure(ctx->depths[k], ecap * 4, "sort depths"));
   }
   const uint32_t tiles = sort_tiles((uint32_t)ecap);
+  CGS_TRY(ctx->ensure(ctx->run_index, (size_t)tiles * 4, "entry run index"));
   if (tiles != ctx->radix_lb_tiles || radix_bits != ctx->radix_lb_bits || !ctx->radix_lb[0].p) {
-    const size_t bytes = (size_t)tiles * (1u << radix_bits) * 4;
+    const size_t bytes = (size_t)tiles * (1u << radix_bits) * 8;  // 64-bit look-back words
     for (int k = 0; k < 2; ++k) {
       CGS_TRY(ctx->ensure(ctx->radix_lb[k], bytes, "radix look-back"));
       CGS_CUDA(cudaMemsetAsync(ctx->radix_lb[k].p, 0, bytes, ctx->stream), "clear look-back");
@@ -447,8 +459,8 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
     so.hist = shist;
     // depth digits of splats in index order are spread over all values
     so.smem_mask = ~0u;
-    so.status2[0] = ctx->splat_lb[0].as<uint32_t>();
-    so.status2[1] = ctx->splat_lb[1].as<uint32_t>();
+    so.status2[0] = ctx->splat_lb[0].p;
+    so.status2[1] = ctx->splat_lb[1].p;
     so.parity = &ctx->splat_parity;
     // the digit width follows the frame's depth bits (8 at 360p, 7 at 1080p):
     // clear the full 256-word stride so a narrower sort leaves no stale words
@@ -492,19 +504,37 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.records = transpose ? 1 : 0;
   b.group_shift = 11;  // kTransposeGroupTiles = 2^11
   b.groups = transpose ? (d.total_tiles + kTransposeGroupTiles - 1) / kTransposeGroupTiles : 1u;
-  // count + stage, scan of the per-slot counts (-> first entries, entry
-  // total), and for the radix path the placement of the staged ranges
+  // Count + stage. The tile transpose then scans the per-slot counts in place
+  // (first entries, entry total). The radix path scans the per-32-slot run
+  // lengths instead (run starts, entry total) and indexes the runs by radix
+  // tile: the sort's first pass gathers the staged runs in slot order, so no
+  // placement pass moves them (offsets keep the per-slot counts).
+  const uint32_t nwt = (d.max_n + 31) / 32;
+  uint32_t* run_start = b.tile_stage + nwt;  // unused part of the per-group staging starts
+  const bool gather = !transpose && sort_passes(d.tile_bits, d.radix_bits) > 0;
   ctx->kbegin(CGS_K_BIN);
   CGS_CUDA(launch_bin_count(b, s), "bin count launch");
-  CGS_CUDA(launch_scan_u32(b.offsets, b.offsets, d.max_n, &fc->entries,
-                           (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
-           "offsets scan launch");
-  if (!transpose) CGS_CUDA(launch_bin_place(b, s), "bin place launch");
+  if (transpose) {
+    CGS_CUDA(launch_scan_u32(b.offsets, b.offsets, d.max_n, &fc->entries,
+                             (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
+             "offsets scan launch");
+  } else {
+    CGS_CUDA(launch_scan_u32(b.tile_count, run_start, nwt, &fc->entries,
+                             (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
+             "run scan launch");
+    if (gather) {
+      CGS_CUDA(launch_run_index(run_start, b.tile_count, nwt, ctx->run_index.as<uint32_t>(),
+                                sort_tiles(ctx->entry_cap), s),
+               "run index launch");
+    } else {
+      b.run_start = run_start;  // no sort pass (one screen tile): place the runs
+      CGS_CUDA(launch_bin_place(b, s), "bin place launch");
+    }
+  }
   ctx->kend();
   if (bin_launches) *bin_launches = transpose ? 2u : 3u;
   if (transpose) {
     // one-pass stable counting sort of the staged records by tile
-    const uint32_t nwt = (d.max_n + 31) / 32;
     const uint32_t target = 296;  // chunks: two per SM
     uint32_t m = 8 * ((nwt + 8 * target - 1) / (8 * target));
     m = std::min<uint32_t>(std::max<uint32_t>(m, 8u), 2040u);
@@ -560,13 +590,20 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.first_bit = d.key64 ? 0u : d.depth_bits;
   sa.num_bits = d.tile_bits;
   sa.radix_bits = d.radix_bits;
-  sa.status2[0] = ctx->radix_lb[0].as<uint32_t>();
-  sa.status2[1] = ctx->radix_lb[1].as<uint32_t>();
+  sa.status2[0] = ctx->radix_lb[0].p;
+  sa.status2[1] = ctx->radix_lb[1].p;
+  sa.wide_lookback = true;  // frames may hold more than 2^30 tile entries
   sa.parity = &ctx->radix_parity;
   sa.tile_ctr = rtiles;
   sa.status_word = &fc->status;
   sa.hist = d_hist;
-  sa.src = 0;
+  sa.src = gather ? 1 : 0;
+  if (gather) {
+    sa.run_start = run_start;
+    sa.run_src = b.tile_stage;
+    sa.first_run = ctx->run_index.as<uint32_t>();
+    sa.num_runs = nwt;
+  }
   // The entries' first digit (the low tile bits) differs from lane to lane,
   // so that pass ranks with per-bit ballots; after it a warp's keys mostly
   // share their higher digits, which __match_any_sync groups more cheaply.
@@ -612,7 +649,7 @@ int enqueue_stage4(cgs_ctx* ctx, const FrameDesc& d, int result_src) {
 // key buffers (capacity already grown), synchronously.
 int rerun_stage34(cgs_ctx* ctx, uint32_t entries) {
   const FrameDesc& d = ctx->last_desc;
-  ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)entries + entries / 4 + 4096, 0x3FFFFFFFull);
+  ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)entries + entries / 4 + 4096, (uint64_t)kMaxEntryCap);
   CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, d.key64, d.radix_bits));
   const ScratchLayout L(d.n, d.max_n ? d.max_n : 1u);
   char* sc = ctx->scratch.as<char>();
@@ -661,6 +698,7 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
     ctx->sticky = CGS_E_TIMEOUT;
     ctx->sticky_msg = "a bounded device-side wait gave up during a frame";
   }
+  if (status & kStatusPoisoned) ctx->poisoned = true;
   if (p.stage3_ran && (status & kStatusCapacity || entries > p.cap)) {
     if (k == ctx->latest_slot) {
       CGS_TRY(rerun_stage34(ctx, entries));
@@ -669,11 +707,11 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       ctx->sticky = CGS_E_CAPACITY;
       ctx->sticky_msg = "an earlier frame's tile entries exceeded the key buffers";
       ctx->entry_cap = std::max(ctx->entry_cap,
-                                (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, 0x3FFFFFFFull));
+                                (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, (uint64_t)kMaxEntryCap));
     }
   } else if (p.stage3_ran && entries > ctx->entry_cap / 10 * 8) {
     // keep 25% headroom for the next frames
-    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, 0x3FFFFFFFull);
+    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, (uint64_t)kMaxEntryCap);
   }
   if (k == ctx->latest_slot) {
     if (p.stage3_ran) {
@@ -715,8 +753,10 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       }
     }
     if (p.need_deform) {
-      kp.alg_bytes[CGS_K_TET_TRANSFORMS] += T * (16 + 36 + 48 + 76);
-      kp.alg_bytes[CGS_K_DEFORM] += (uint64_t)p.n * 60 + A * 40 + (A - p.n) * 8;
+      // tet transforms (fused into the deform launch): 16 B elements + 36 B
+      // D_m^-1 + 48 B corner vertices in, J, R (36 B each) and sigma_1 out
+      kp.alg_bytes[CGS_K_DEFORM] += T * (16 + 36 + 48 + 76) + (uint64_t)p.n * 60 + A * 40 +
+                                    (A - p.n) * 8;
     }
     kp.alg_bytes[CGS_K_PROJECT] += A * 40 + S * (shb + 48) + (A - S) * 16 + (p.stage3_ran ? A * 8 : 0);
     if (p.stage3_ran) {
@@ -870,6 +910,45 @@ int cgs_ctx_synchronize(cgs_ctx* ctx) {
   return ctx->take_sticky();
 }
 
+int cgs_ctx_set_device_budget(cgs_ctx* ctx, uint64_t bytes) {
+  if (!ctx) return CGS_E_ARG;
+  ctx->budget = bytes;
+  return CGS_OK;
+}
+
+// Each drill's scratch: two tiles of 64-bit chained-scan words, two tiles of
+// 256 digit words and the status word, zeroed, in a buffer of its own.
+int cgs_ctx_wait_drill(cgs_ctx* ctx, uint32_t polls, uint32_t* out_gave_up) {
+  if (!ctx) return CGS_E_ARG;
+  if (polls == 0 || polls > kSpinLimit) return ctx->fail(CGS_E_ARG, "polls must be in [1, 2^22]");
+  cudaSetDevice(ctx->device);
+  CGS_TRY(drain(ctx, true));
+  const size_t bytes = 2 * sizeof(unsigned long long) + 2 * 256 * sizeof(uint32_t) + 16;
+  DevBuf buf;
+  CGS_CUDA(cudaMalloc(&buf.p, 3 * bytes), "drill scratch");
+  CGS_CUDA(cudaMemsetAsync(buf.p, 0, 3 * bytes, ctx->stream), "clear drill scratch");
+  uint32_t gave_up = 0;
+  for (int k = 0; k < 3; ++k) {
+    char* base = buf.as<char>() + k * bytes;
+    unsigned long long* scan_status = (unsigned long long*)base;
+    uint32_t* digits = (uint32_t*)(base + 2 * sizeof(unsigned long long));
+    uint32_t* word = digits + 2 * 256;
+    cudaError_t e = k == 0   ? launch_drill_chained_scan(scan_status, word, polls, ctx->stream)
+                    : k == 1 ? launch_drill_digit_lookback(digits, 256, word, polls, ctx->stream)
+                             : launch_drill_mbarrier(word, polls, ctx->stream);
+    CGS_CUDA(e, "drill launch");
+    uint32_t w = 0;
+    CGS_CUDA(cudaMemcpyAsync(&w, word, 4, cudaMemcpyDeviceToHost, ctx->stream), "drill status");
+    CGS_CUDA(cudaStreamSynchronize(ctx->stream), "drill");
+    const uint32_t want = k == 2 ? kStatusBarrierTimeout : kStatusLookbackTimeout;
+    if (w & want) gave_up |= 1u << k;
+  }
+  if (out_gave_up) *out_gave_up = gave_up;
+  if (gave_up) return ctx->fail(CGS_E_TIMEOUT, "bounded device waits gave up (drill mask " +
+                                                   std::to_string(gave_up) + ")");
+  return CGS_OK;
+}
+
 int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out) {
   if (!ctx || !out) return CGS_E_ARG;
   const DevBuf* bufs[] = {&ctx->rest_pos, &ctx->rest_cova, &ctx->rest_covb, &ctx->rest_sh,
@@ -896,6 +975,7 @@ int cgs_scene_upload(cgs_ctx* ctx, uint64_t n, const float* pos, const float* co
   if (n >= (1ull << 30)) return ctx->fail(CGS_E_CAPACITY, "scene exceeds 2^30 Gaussians");
   if (n > 0 && (!pos || !cov || !opa || !sh)) return ctx->fail(CGS_E_ARG, "null scene array");
   cudaSetDevice(ctx->device);
+  ctx->scene_ready = false;  // until the new scene is resident (a failed growth loses the old one)
   const size_t shb = (size_t)n * 48 * (sh_format == CGS_SH_F16 ? 2 : 4);
   const size_t nn = n ? n : 1;
   CGS_TRY(ctx->ensure(ctx->rest_pos, nn * 16, "rest positions"));
@@ -947,6 +1027,7 @@ int cgs_scene_upload_quantized(cgs_ctx* ctx, uint64_t n, const float* pos,
   if (n > 0 && (!pos || !cov_f16x2 || !opa || !sh_f16x2))
     return ctx->fail(CGS_E_ARG, "null scene array");
   cudaSetDevice(ctx->device);
+  ctx->scene_ready = false;  // until the new scene is resident (a failed growth loses the old one)
   const size_t nn = n ? n : 1;
   const size_t bases = sh_degree == 0 ? 1 : (sh_degree == 1 ? 4 : (sh_degree == 2 ? 9 : 16));
   const size_t words = (bases * 3 + 1) / 2;
@@ -1268,6 +1349,7 @@ int mvc_bind(cgs_ctx* ctx, bool learned, float threshold, bool cache, uint32_t* 
         if (learned && e == cudaSuccess && rc == CGS_OK) {
           uint32_t fst = 0;
           e = cudaMemcpy(&fst, ctx->field.status.p, 4, cudaMemcpyDeviceToHost);
+          if (e == cudaSuccess && (fst & kStatusPoisoned)) ctx->poisoned = true;
           if (e == cudaSuccess && fst)
             rc = ctx->fail(CGS_E_TIMEOUT, "field inference gave up waiting for the tensor cores");
         }
@@ -1455,6 +1537,7 @@ int cgs_mvc_field_infer(cgs_ctx* ctx, uint64_t n, const float* d_points, int32_t
   uint32_t fst = 0;
   CGS_CUDA(cudaMemcpyAsync(&fst, f.status.p, 4, cudaMemcpyDeviceToHost, s), "field inference");
   CGS_CUDA(cudaStreamSynchronize(s), "field inference");
+  if (fst & kStatusPoisoned) ctx->poisoned = true;
   if (fst) return ctx->fail(CGS_E_TIMEOUT, "field inference gave up waiting for the tensor cores");
   return CGS_OK;
 }
@@ -1864,7 +1947,7 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
   }
   if (!cached) {
     if (ctx->entry_cap == 0)
-      ctx->entry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(32ull * mn, 1u << 20), 0x3FFFFFFFull);
+      ctx->entry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(32ull * mn, 1u << 20), (uint64_t)kMaxEntryCap);
     CGS_TRY(ensure_entry_buffers(ctx, ctx->entry_cap, d.key64, d.radix_bits));
     CGS_TRY(ensure_splat_buffers(ctx, mn));
   }
@@ -1925,11 +2008,8 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
         ctx->kend();
       }
     }
-    if (has_cages) {
-      ctx->kbegin(CGS_K_TET_TRANSFORMS);
-      CGS_CUDA(launch_tet_transforms(da, s), "tet transforms launch");
-      ctx->kend();
-    }
+    // the tet transforms run in the deform launch's first blocks
+    da.fuse_tets = has_cages ? 1u : 0u;
     ctx->kbegin(CGS_K_DEFORM);
     CGS_CUDA(launch_deform(da, s), "deform launch");
     ctx->kend();
@@ -2014,6 +2094,9 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
 int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* comp,
                       const cgs_frame_params* params, cgs_stage_timings* timings) {
   CGS_TRY(check_frame_args(ctx, camera, comp, params));
+  if (ctx->poisoned)
+    return ctx->fail(CGS_E_STATE, "a tensor-core wait gave up twice in an earlier frame; the "
+                                  "device state is undefined: destroy and recreate the context");
   cudaSetDevice(ctx->device);
   cgs_stage_timings tm{};
   const bool prof = params->profile_stages != 0;
@@ -2112,6 +2195,7 @@ int check_views(cgs_ctx* ctx, uint32_t nv, const uint32_t* cap_used,
   overflowed->clear();
   for (uint32_t v = 0; v < nv; ++v) {
     const FrameCounters& fc = ctx->h_views[v].fc;
+    if (fc.status & kStatusPoisoned) ctx->poisoned = true;
     if (fc.status & (kStatusLookbackTimeout | kStatusBarrierTimeout))
       return ctx->fail(CGS_E_TIMEOUT, "a bounded device-side wait gave up during a view");
     if ((fc.status & kStatusCapacity) || fc.entries > cap_used[v]) overflowed->push_back(v);
@@ -2119,7 +2203,7 @@ int check_views(cgs_ctx* ctx, uint32_t nv, const uint32_t* cap_used,
     *total_entries += fc.entries;
   }
   if (most > ctx->entry_cap / 10 * 8)
-    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)most * 13 / 10 + 4096, 0x3FFFFFFFull);
+    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)most * 13 / 10 + 4096, (uint64_t)kMaxEntryCap);
   return CGS_OK;
 }
 
@@ -2542,9 +2626,10 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
       const uint32_t* ord = (const uint32_t*)tmp.data();
       std::vector<uint32_t> cnt(sa, 0);
       for (size_t j = 0; j < sa; ++j) {
+        // the tile transpose leaves the scanned offsets, the radix path the counts
         const uint32_t next = j + 1 < sa ? off[j + 1] : (uint32_t)entries;
         if (ord[j] >= sa) return ctx->fail(CGS_E_STATE, "splat order out of range");
-        cnt[ord[j]] = next - off[j];
+        cnt[ord[j]] = ctx->s3_transpose ? next - off[j] : off[j];
       }
       out.resize(sa * 4);
       uint32_t* o = (uint32_t*)out.data();
@@ -2845,7 +2930,7 @@ static int sort_common(cgs_ctx* ctx, uint32_t* d_keys, uint32_t* d_vals, uint32_
   sa.num_bits = key_bits;
   sa.radix_bits = rb;
   sa.hist = hist;
-  sa.status = (uint32_t*)(b + hdr);
+  sa.status = b + hdr;
   sa.tile_ctr = words + 2;
   sa.status_word = words + 1;
   sa.src = 0;

@@ -38,9 +38,31 @@ constexpr int kSortWarps = kSortThreads / 32;
 // (~32 keys) apart, which without padding map to the same bank.
 constexpr uint32_t kSortTileP = kSortTile + kSortTile / 32;
 __device__ __forceinline__ uint32_t padded(uint32_t i) { return i + (i >> 5); }
-constexpr uint32_t kFlagAgg = 1u << 30;
-constexpr uint32_t kFlagPre = 2u << 30;
-constexpr uint32_t kValueMask = (1u << 30) - 1u;
+// Look-back words: a flag (tile count published / inclusive prefix
+// published) above the count. 32-bit words carry counts below 2^30 (splat
+// sorts, the stand-alone sorts); 64-bit words any 32-bit count (the frame's
+// tile entries, which may exceed 2^30).
+template <typename W>
+struct Lb;
+template <>
+struct Lb<uint32_t> {
+  static constexpr uint32_t kAgg = 1u << 30, kPre = 2u << 30, kMask = (1u << 30) - 1u;
+  static __device__ __forceinline__ uint32_t load(const uint32_t* p) { return ld_relaxed_u32(p); }
+  static __device__ __forceinline__ void store(uint32_t* p, uint32_t w) { st_relaxed_u32(p, w); }
+  static __device__ __forceinline__ uint32_t flag(uint32_t w) { return w & ~kMask; }
+  static __device__ __forceinline__ uint32_t value(uint32_t w) { return w & kMask; }
+  static __device__ __forceinline__ uint32_t make(uint32_t f, uint32_t v) { return f | (v & kMask); }
+};
+template <>
+struct Lb<unsigned long long> {
+  using W = unsigned long long;
+  static constexpr W kAgg = 1ull << 32, kPre = 2ull << 32, kMask = 0xFFFFFFFFull;
+  static __device__ __forceinline__ W load(const W* p) { return ld_relaxed_u64(p); }
+  static __device__ __forceinline__ void store(W* p, W w) { st_relaxed_u64(p, w); }
+  static __device__ __forceinline__ W flag(W w) { return w & ~kMask; }
+  static __device__ __forceinline__ uint32_t value(W w) { return (uint32_t)w; }
+  static __device__ __forceinline__ W make(W f, uint32_t v) { return f | (W)v; }
+};
 
 // Ranking modes of a pass: __match_any_sync (cheap when a warp's keys share
 // few digits), one ballot per digit bit (a fixed cost), or shared-memory
@@ -60,18 +82,73 @@ struct PassArgs {
   uint32_t shift;
   uint32_t dmask;          // digit mask of this pass (narrower on a final partial pass)
   const uint32_t* dbase;   // this pass's exclusive digit bases (k_digit_bases)
-  uint32_t* status;        // this pass's [tiles][radix] look-back words
-  uint32_t* clear_next;    // [tiles][clear_stride] words to zero for the next pass, or null
+  void* status;            // this pass's [tiles][radix] look-back words (32- or 64-bit)
+  void* clear_next;        // [tiles][clear_stride] words to zero for the next pass, or null
   uint32_t clear_stride;   // words per tile of clear_next (>= radix)
   uint32_t grid_tiles;     // tiles covered by the grid (all of clear_next)
   uint32_t* tile_ctr;
   uint32_t* status_word;
   uint32_t rank;           // how a warp finds the lanes sharing a digit: kRank*
+  // Gather mode (a first pass that reads staged runs instead of a contiguous
+  // input): position q of the input order is element run_src[k] + (q -
+  // run_start[k]) of keys_in / v0_in / v1_in, for the run k with run_start[k]
+  // <= q < run_start[k + 1] (run_start is the exclusive scan of the run
+  // lengths, runs in input order); first_run[t] is the run holding position
+  // t * 4096. Null run_start: contiguous input.
+  const uint32_t* run_start;
+  const uint32_t* run_src;
+  const uint32_t* first_run;
+  uint32_t num_runs;
 };
 
-template <int RB, bool PAY2>
+// Exclusive prefix of digit d over the tiles before `tile`: walks back from
+// tile - 1, adding published tile counts until a tile with its inclusive
+// prefix. A word with neither flag is polled again (its tile is held by a
+// resident block); after `limit` polls the wait gives up, sets
+// kStatusLookbackTimeout and returns what it has. The words of four
+// predecessors are read at once (independent loads), so a walk over tiles
+// that have published only their counts costs one load latency per four
+// tiles instead of one per tile.
+template <typename W>
+__device__ __forceinline__ uint32_t digit_lookback(const W* status, uint32_t tile, uint32_t R,
+                                                   uint32_t d, uint32_t* status_word,
+                                                   uint32_t limit) {
+  constexpr int kAhead = 4;
+  uint32_t excl = 0;
+  long long pred = (long long)tile - 1;
+  uint32_t spins = 0;
+  while (pred >= 0) {
+    W w[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k)
+      w[k] = pred - k >= 0 ? Lb<W>::load(status + (size_t)(pred - k) * R + d) : W(0);
+    int used = 0;
+    bool done = false;
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) {
+      if (done || used < k || pred - k < 0) continue;
+      if (Lb<W>::flag(w[k]) == 0) continue;  // not published: wait on it below
+      excl += Lb<W>::value(w[k]);
+      used = k + 1;
+      if (Lb<W>::flag(w[k]) == Lb<W>::kPre) done = true;
+    }
+    if (done) break;
+    pred -= used;
+    if (used == 0) {  // the nearest unread predecessor has published nothing yet
+      if (++spins > limit) {
+        atomicOr(status_word, kStatusLookbackTimeout);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  return excl;
+}
+
+template <int RB, bool PAY2, typename W>
 __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const PassArgs a) {
   constexpr uint32_t R = 1u << RB;
+  W* const lb = static_cast<W*>(a.status);
   static_assert(R <= (uint32_t)kSortThreads, "one thread per digit");
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* s_keys = smem;                       // [kSortTileP]
@@ -99,7 +176,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   // whatever radix the previous sort on it used.
   if (a.clear_next && tile < a.grid_tiles)
     for (uint32_t k = tid; k < a.clear_stride; k += kSortThreads)
-      a.clear_next[(size_t)tile * a.clear_stride + k] = 0u;
+      static_cast<W*>(a.clear_next)[(size_t)tile * a.clear_stride + k] = W(0);
   if (tile >= num_tiles) return;
 
   // Load (warp-striped: a warp's item j is 32 consecutive keys). Full tiles,
@@ -109,7 +186,59 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   const size_t first = tile_base + (size_t)warp * (32 * kSortItems) + lane;
   uint32_t k[kSortItems], v0[kSortItems], v1[kSortItems];
   uint32_t rk[kSortItems / 2];  // two 16-bit in-warp ranks per word (ranks < 512)
-  if (full) {
+  if (a.run_start) {
+    // Gather mode: the runs overlapping this tile's positions, from the one
+    // holding its first position, go to shared memory (the reorder buffers,
+    // unused until after ranking) 256 at a time until one starts past the
+    // tile; each lane then walks forward through them as its positions grow.
+    uint32_t* s_rs = s_keys;  // run starts
+    uint32_t* s_rsrc = s_v0;  // their staged positions
+    const uint32_t tile_end = (uint32_t)min((size_t)n, tile_base + kSortTile);
+    const uint32_t k0 = __ldcg(a.first_run + tile);
+    uint32_t nwin = 0;
+    for (;;) {
+      const uint32_t kk = k0 + nwin + (uint32_t)tid;
+      const bool in = kk < a.num_runs;
+      s_rs[nwin + tid] = in ? __ldcg(a.run_start + kk) : 0xFFFFFFFFu;
+      s_rsrc[nwin + tid] = in ? __ldcg(a.run_src + kk) : 0u;
+      nwin += kSortThreads;
+      __syncthreads();
+      if (nwin >= kSortTile || s_rs[nwin - 1] >= tile_end) break;
+    }
+    const bool covered = s_rs[nwin - 1] >= tile_end;
+    uint32_t r = 0;
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+      const size_t q = first + 32 * j;
+      k[j] = 0xFFFFFFFFu;
+      v0[j] = 0u;
+      if (PAY2) v1[j] = 0u;
+      if (q < (size_t)n) {
+        uint32_t src;
+        if (covered) {
+          while (r + 1 < nwin && s_rs[r + 1] <= (uint32_t)q) ++r;
+          src = s_rsrc[r] + ((uint32_t)q - s_rs[r]);
+        } else {
+          // more runs than the window holds (many empty ones): search the
+          // run starts in memory
+          uint32_t lo = k0, hi = a.num_runs;  // last run with start <= q
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldcg(a.run_start + mid) <= (uint32_t)q) lo = mid; else hi = mid;
+          }
+          src = __ldcg(a.run_src + lo) + ((uint32_t)q - __ldcg(a.run_start + lo));
+        }
+        if (src < a.capacity) {
+          k[j] = __ldcs(a.keys_in + src);
+          v0[j] = __ldcs(a.v0_in + src);
+          if (PAY2) v1[j] = __ldcs(a.v1_in + src);
+        } else {
+          atomicOr(a.status_word, kStatusCapacity);
+        }
+      }
+    }
+    __syncthreads();  // the window is read before the reorder reuses the buffers
+  } else if (full) {
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
       k[j] = __ldcs(a.keys_in + first + 32 * j);
@@ -194,7 +323,8 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     // Padding keys (past n) carry the largest digit and sit at the end of it.
     agg = my_count;
     if ((uint32_t)tid == a.dmask) agg -= (kSortTile - tile_valid);
-    st_relaxed_u32(a.status + (size_t)tile * R + tid, (tile == 0 ? kFlagPre : kFlagAgg) | agg);
+    Lb<W>::store(lb + (size_t)tile * R + tid,
+                 Lb<W>::make(tile == 0 ? Lb<W>::kPre : Lb<W>::kAgg, agg));
   }
   __syncthreads();
 #pragma unroll
@@ -209,23 +339,8 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   if ((uint32_t)tid < R) {
     uint32_t excl = 0;
     if (tile != 0) {
-      long long pred = (long long)tile - 1;
-      uint32_t spins = 0;
-      while (pred >= 0) {
-        const uint32_t w = ld_relaxed_u32(a.status + (size_t)pred * R + tid);
-        if ((w & ~kValueMask) == 0u) {
-          if (++spins > kSpinLimit) {
-            atomicOr(a.status_word, kStatusLookbackTimeout);
-            break;
-          }
-          __nanosleep(32);
-          continue;
-        }
-        excl += w & kValueMask;
-        if ((w & ~kValueMask) == kFlagPre) break;
-        --pred;
-      }
-      st_relaxed_u32(a.status + (size_t)tile * R + tid, kFlagPre | ((excl + agg) & kValueMask));
+      excl = digit_lookback<W>(lb, tile, R, (uint32_t)tid, a.status_word, kSpinLimit);
+      Lb<W>::store(lb + (size_t)tile * R + tid, Lb<W>::make(Lb<W>::kPre, excl + agg));
     }
     s_goff[tid] = a.dbase[tid] + excl - tstart;
   }
@@ -267,15 +382,21 @@ size_t onesweep_smem(uint32_t rank) {
                              (rank == kRankSmem ? kSortWarps * 3 * R : 0u));
 }
 
-template <int RB, bool PAY2>
-cudaError_t launch_pass(const PassArgs& p, uint32_t grid, cudaStream_t s) {
+template <int RB, bool PAY2, typename W>
+cudaError_t launch_pass_w(const PassArgs& p, uint32_t grid, cudaStream_t s) {
   const size_t smem = onesweep_smem<RB, PAY2>(p.rank);
   // per device: set on every launch (a host-side attribute write)
-  const cudaError_t e = cudaFuncSetAttribute(k_onesweep<RB, PAY2>,
+  const cudaError_t e = cudaFuncSetAttribute(k_onesweep<RB, PAY2, W>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_onesweep<RB, PAY2><<<grid, kSortThreads, smem, s>>>(p);
+  k_onesweep<RB, PAY2, W><<<grid, kSortThreads, smem, s>>>(p);
   return cudaGetLastError();
+}
+
+template <int RB, bool PAY2>
+cudaError_t launch_pass(const PassArgs& p, uint32_t grid, bool wide, cudaStream_t s) {
+  return wide ? launch_pass_w<RB, PAY2, unsigned long long>(p, grid, s)
+              : launch_pass_w<RB, PAY2, uint32_t>(p, grid, s);
 }
 
 // Digit histograms of every pass in one read of the keys.
@@ -303,7 +424,22 @@ __global__ void k_histogram(const uint32_t* __restrict__ keys, const uint32_t* _
     if (s_hist[k]) atomicAdd(&hist[k], s_hist[k]);
 }
 
+// Wait drill: one thread per digit walks back from tile 1 to a tile 0 whose
+// words nothing publishes (status holds 2 x R zeroed words), so every walk
+// polls until its limit and sets the timeout bit.
+__global__ void k_drill_digit_lookback(const uint32_t* status, uint32_t R, uint32_t* status_word,
+                                       uint32_t limit) {
+  if (threadIdx.x < R) digit_lookback<uint32_t>(status, 1u, R, threadIdx.x, status_word, limit);
+}
+
 }  // namespace
+
+cudaError_t launch_drill_digit_lookback(const uint32_t* status, uint32_t radix,
+                                        uint32_t* status_word, uint32_t limit, cudaStream_t s) {
+  if (radix == 0 || radix > 256) return cudaErrorInvalidValue;
+  k_drill_digit_lookback<<<1, 256, 0, s>>>(status, radix, status_word, limit);
+  return cudaGetLastError();
+}
 
 uint32_t sort_tiles(uint32_t capacity) { return (capacity + kSortTile - 1) / kSortTile; }
 
@@ -326,6 +462,8 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
   const uint32_t tiles = sort_tiles(a.capacity);
   int src = a.src;
   const bool pay2 = a.vals2[0] != nullptr;
+  const bool wide = a.wide_lookback;
+  if (!wide && a.capacity > (1u << 30)) return cudaErrorInvalidValue;  // 30-bit counts
   // counts -> exclusive bases (in place)
   k_digit_bases<<<passes, 256, 0, s>>>(a.hist, R);
   cudaError_t le = cudaGetLastError();
@@ -351,7 +489,7 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
       pa.clear_stride = a.lb_stride ? a.lb_stride : R;
       *a.parity = par ^ 1;
     } else {
-      pa.status = a.status + (size_t)p * tiles * R;
+      pa.status = static_cast<char*>(a.status) + (size_t)p * tiles * R * (wide ? 8 : 4);
       pa.clear_next = nullptr;
       pa.clear_stride = 0;
     }
@@ -359,14 +497,18 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.grid_tiles = tiles;
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
+    pa.run_start = p == 0 ? a.run_start : nullptr;
+    pa.run_src = a.run_src;
+    pa.first_run = a.first_run;
+    pa.num_runs = a.num_runs;
     pa.rank = ((a.smem_mask >> p) & 1u) ? kRankSmem : (((a.ballot_mask >> p) & 1u) ? kRankBallot : kRankMatch);
     cudaError_t e;
     switch (rb) {
-      case 4: e = pay2 ? launch_pass<4, true>(pa, tiles, s) : launch_pass<4, false>(pa, tiles, s); break;
-      case 5: e = pay2 ? launch_pass<5, true>(pa, tiles, s) : launch_pass<5, false>(pa, tiles, s); break;
-      case 6: e = pay2 ? launch_pass<6, true>(pa, tiles, s) : launch_pass<6, false>(pa, tiles, s); break;
-      case 7: e = pay2 ? launch_pass<7, true>(pa, tiles, s) : launch_pass<7, false>(pa, tiles, s); break;
-      default: e = pay2 ? launch_pass<8, true>(pa, tiles, s) : launch_pass<8, false>(pa, tiles, s); break;
+      case 4: e = pay2 ? launch_pass<4, true>(pa, tiles, wide, s) : launch_pass<4, false>(pa, tiles, wide, s); break;
+      case 5: e = pay2 ? launch_pass<5, true>(pa, tiles, wide, s) : launch_pass<5, false>(pa, tiles, wide, s); break;
+      case 6: e = pay2 ? launch_pass<6, true>(pa, tiles, wide, s) : launch_pass<6, false>(pa, tiles, wide, s); break;
+      case 7: e = pay2 ? launch_pass<7, true>(pa, tiles, wide, s) : launch_pass<7, false>(pa, tiles, wide, s); break;
+      default: e = pay2 ? launch_pass<8, true>(pa, tiles, wide, s) : launch_pass<8, false>(pa, tiles, wide, s); break;
     }
     if (e != cudaSuccess) return e;
     src = 1 - src;

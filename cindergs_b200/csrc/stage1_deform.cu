@@ -4,6 +4,10 @@
 //                    Cardano on J^T J, rotation by 5 Newton-Schulz polar
 //                    steps with chirality fix
 //                    (render/kernels/deformation.rs:684-865).
+//                    In frames the first blocks of the k_deform launch run
+//                    these transforms (tet_transform) and publish a count;
+//                    the Gaussian blocks wait for it (bounded), so Stage 1 is
+//                    one launch.
 //  k_deform<SPLIT>   per Gaussian: x' = sum w_k x_k, M = J S J^T (diag >= 1e-4,
 //                    symmetrised), det-J opacity, 3D Mip filter, strain split
 //                    along the major eigenvector
@@ -29,14 +33,13 @@ namespace {
 
 constexpr int kDeformThreads = 256;
 
-__global__ void __launch_bounds__(128) k_tet_transforms(uint32_t T, const float* __restrict__ verts,
-                                                        const uint4* __restrict__ elems,
-                                                        const float* __restrict__ inv_dm,
-                                                        float* __restrict__ J_out,
-                                                        float* __restrict__ R_out,
-                                                        float* __restrict__ S_out) {
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T) return;
+// J, sigma_1 and R of tet t (compute_tet_transforms_kernel,
+// deformation.rs:684-865).
+__device__ __forceinline__ void tet_transform(uint32_t t, const float* __restrict__ verts,
+                                              const uint4* __restrict__ elems,
+                                              const float* __restrict__ inv_dm,
+                                              float* __restrict__ J_out, float* __restrict__ R_out,
+                                              float* __restrict__ S_out) {
   const uint4 e = elems[t];
   const float* x0 = verts + 3 * (size_t)e.x;
   const float* x1 = verts + 3 * (size_t)e.y;
@@ -136,6 +139,16 @@ __global__ void __launch_bounds__(128) k_tet_transforms(uint32_t T, const float*
   }
   R[0] = r00; R[1] = r10; R[2] = r20; R[3] = r01; R[4] = r11; R[5] = r21;
   R[6] = r02; R[7] = r12; R[8] = r22;
+}
+
+__global__ void __launch_bounds__(128) k_tet_transforms(uint32_t T, const float* __restrict__ verts,
+                                                        const uint4* __restrict__ elems,
+                                                        const float* __restrict__ inv_dm,
+                                                        float* __restrict__ J_out,
+                                                        float* __restrict__ R_out,
+                                                        float* __restrict__ S_out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < T) tet_transform(t, verts, elems, inv_dm, J_out, R_out, S_out);
 }
 
 // 3D Mip filter Sigma + s I with opacity * sqrt(det / det_reg), in the operand
@@ -303,14 +316,42 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_sums[32];
   __shared__ uint32_t s_base;
-  uint32_t tile;
-  if (SPLIT) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&a.fc->tile_ctr[0], 1u);
+  // Tickets in launch order: the first tet_blocks tickets compute the tet
+  // transforms, the others are Gaussian tiles in increasing order (the chained
+  // scan of the split children needs that order; every tile a block waits on
+  // belongs to a block that took its ticket earlier, so it is resident).
+  if (threadIdx.x == 0) s_tile = atomicAdd(&a.fc->tile_ctr[0], 1u);
+  __syncthreads();
+  uint32_t tile = s_tile;
+  const uint32_t tet_blocks = a.fuse_tets ? (a.num_tets + kDeformThreads - 1) / kDeformThreads : 0u;
+  if (tile < tet_blocks) {
+    const uint32_t t = tile * kDeformThreads + threadIdx.x;
+    if (t < a.num_tets)
+      tet_transform(t, a.verts, a.elems, a.inv_dm, a.tet_J, a.tet_R, a.tet_stretch);
     __syncthreads();
-    tile = s_tile;
-  } else {
-    tile = blockIdx.x;
-    if (tile == 0 && threadIdx.x == 0) *a.split_count = 0u;
+    if (threadIdx.x == 0) {
+      __threadfence();  // this block's J, R, sigma_1 before its completion count
+      atomicAdd(&a.fc->tile_ctr[kTetsDoneCtr], 1u);
+    }
+    return;
+  }
+  tile -= tet_blocks;
+  if (!SPLIT && tile == 0 && threadIdx.x == 0) *a.split_count = 0u;
+  if (tet_blocks) {
+    // Wait (bounded) until every tet block has published; the tet data is
+    // then read through L2 (ld.global.cg), never through the incoherent
+    // read-only path.
+    if (threadIdx.x == 0) {
+      uint32_t spins = 0;
+      while (ld_acquire_u32(&a.fc->tile_ctr[kTetsDoneCtr]) < tet_blocks) {
+        if (++spins > kSpinLimit) {
+          atomicOr(&a.fc->status, kStatusLookbackTimeout);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __syncthreads();
   }
   const uint32_t i = tile * kDeformThreads + threadIdx.x;
   bool split = false;
@@ -397,9 +438,9 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
       const float pz =
           w.x * __ldg(v0 + 2) + w.y * __ldg(v1 + 2) + w.z * __ldg(v2 + 2) + w.w * __ldg(v3 + 2);
       const float* J = a.tet_J + 9 * (size_t)tet_raw;
-      const float j_00 = __ldg(J + 0), j_10 = __ldg(J + 1), j_20 = __ldg(J + 2);
-      const float j_01 = __ldg(J + 3), j_11 = __ldg(J + 4), j_21 = __ldg(J + 5);
-      const float j_02 = __ldg(J + 6), j_12 = __ldg(J + 7), j_22 = __ldg(J + 8);
+      const float j_00 = __ldcg(J + 0), j_10 = __ldcg(J + 1), j_20 = __ldcg(J + 2);
+      const float j_01 = __ldcg(J + 3), j_11 = __ldcg(J + 4), j_21 = __ldcg(J + 5);
+      const float j_02 = __ldcg(J + 6), j_12 = __ldcg(J + 7), j_22 = __ldcg(J + 8);
       const float s_xx = rca.x, s_xy = rca.y, s_xz = rca.z, s_yy = rca.w, s_yz = rcb.x,
                   s_zz = rcb.y;
       const float k_00 = j_00 * s_xx + j_01 * s_xy + j_02 * s_xz;
@@ -425,7 +466,7 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
       const float s_det = clampf(det_j, 0.6f, 1.8f);
       const float safe_base = clampf(1.0f - rp.w, 1e-4f, 0.999f);
       const float alpha_prime = clampf(1.0f - cgs_powf(safe_base, 1.0f / s_det), 0.05f, 0.99f);
-      split = SPLIT && a.split_threshold > 0.0f && __ldg(&a.tet_stretch[tet_raw]) > a.split_threshold;
+      split = SPLIT && a.split_threshold > 0.0f && __ldcg(&a.tet_stretch[tet_raw]) > a.split_threshold;
       if (!split) {
         float xx = m00, yy = m11, zz = m22, alpha = alpha_prime;
         if (a.mip > 0.0f) mip3d(xx, m01, m02, yy, m12, zz, alpha, a.mip);
@@ -619,8 +660,9 @@ cudaError_t launch_tet_transforms(const DeformArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s) {
-  if (a.n == 0) return cudaSuccess;
-  const uint32_t blocks = (a.n + kDeformThreads - 1) / kDeformThreads;
+  if (a.n == 0) return a.fuse_tets ? launch_tet_transforms(a, s) : cudaSuccess;
+  const uint32_t tet_blocks = a.fuse_tets ? (a.num_tets + kDeformThreads - 1) / kDeformThreads : 0u;
+  const uint32_t blocks = (a.n + kDeformThreads - 1) / kDeformThreads + tet_blocks;
   if (a.split_threshold > 0.0f)
     k_deform<true><<<blocks, kDeformThreads, 0, s>>>(a);
   else

@@ -16,8 +16,18 @@
 // entry's rank inside its splat). A splat with thousands of candidate tiles
 // is spread over all 32 lanes instead of serialising one lane.
 //
-// Compiled with -fmad=false: the ellipse test's quadratic is rounded term by
-// term as in the reference, so counts, offsets and keys are bit-exact.
+// Term tables: the reference's test evaluates the conic's quadratic at two
+// points of a tile -- one whose x is the tile column's nearest x to the
+// centre, one whose y is the tile row's nearest y -- each with a division
+// that depends on the column alone or on the row alone. A warp therefore
+// first evaluates, per splat, every column term (x edges, nearest x, the
+// clamped-y division, a x^2) and every row term (y edges, nearest y, the
+// clamped-x division, c y^2) of its 32 splats' tile boxes into shared memory;
+// each candidate tile then combines one column and one row entry with ~20
+// floating-point operations instead of evaluating the whole test. Every
+// product and sum is rounded separately (explicit __fmul_rn/__fadd_rn, in the
+// reference's operand order), so the test's result is the reference formula's
+// bit for bit; counts, offsets and keys are bit-exact.
 #include <algorithm>
 
 #include "kernels.h"
@@ -28,23 +38,28 @@ namespace {
 constexpr int kBinThreads = 256;
 constexpr int kBinWarps = kBinThreads / 32;
 constexpr int kMaskCap = 64;   // stored ballot masks per warp (2,048 candidates)
-constexpr int kHitCap = 896;   // stored hit records per warp (4 blocks fit an SM); a warp's
-                               // 32 splats emit ~770 entries at 1080p on average
+constexpr int kHitCap = 640;   // stored hit records per warp; a warp's 32 splats emit ~770
+                               // entries at 1080p on average, the rest walk the masks again
+constexpr int kTabCap = 384;   // term-table entries (tile columns + rows) per warp
 constexpr uint32_t kMaxGroups = 8;  // tile groups of the record mode
 
 // Per-splat constants of a warp's 32 splats, read by the lane that tests one
-// of the splat's candidate tiles (three 128-bit loads and two 32-bit loads).
+// of the splat's candidate tiles.
 struct BinSplats {
   double2 rcp[kBinWarps][32]; // RN64(1 / max(c, 1e-12)), RN64(1 / max(a, 1e-12))
   uint4 box[kBinWarps][32];   // x0, y0, width (tiles), ceil(2^32 / width)
   float4 geo[kBinWarps][32];  // mu_x, mu_y, -b, 2b
   float4 con[kBinWarps][32];  // a, c, max(a, 1e-12), max(c, 1e-12)
-  float qlim[kBinWarps][32];  // q_max + 1e-4
+  float4 kq[kBinWarps][32];   // a, 2b, c, q_max + 1e-4 (the term-table test)
+  uint2 tb[kBinWarps][32];    // first column entry, first row entry in the term table
   uint32_t base[kBinWarps][32];  // exclusive prefix of the candidate counts
+  uint32_t cpre[kBinWarps][32];  // exclusive prefix of the tile-box widths
+  uint32_t rpre[kBinWarps][32];  // exclusive prefix of the tile-box heights
   uint32_t dq[kBinWarps][32];    // depth part of the key
   uint32_t sid[kBinWarps][32];   // splat index
 };
 constexpr size_t kBinSmem = sizeof(BinSplats) + sizeof(uint32_t) * kBinWarps * (2 * kMaskCap + kHitCap) +
+                            sizeof(float4) * kBinWarps * kTabCap +
                             sizeof(uint32_t) * 1024;  // + tile-digit histograms (<= 4 x 256)
 
 struct SplatBox {
@@ -53,10 +68,10 @@ struct SplatBox {
   float mu_x, mu_y, ca, cb, cc, alpha;
 };
 
-__device__ __forceinline__ uint32_t tile_coord(float v, int32_t hi, float tile_px) {
+__device__ __forceinline__ uint32_t tile_coord(float v, int32_t hi, float inv_tile) {
   // clamp(floor(v / tile) as i32, 0, hi) with Rust's saturating cast; the
-  // tile size is a power of two, so the division is exact.
-  const float f = floorf(v / tile_px);
+  // tile size is a power of two, so v * (1 / tile) is the exact quotient.
+  const float f = floorf(__fmul_rn(v, inv_tile));
   int32_t i = __float2int_rz(f);  // saturates, NaN -> 0
   i = i < 0 ? 0 : (i > hi ? hi : i);
   return (uint32_t)i;
@@ -80,11 +95,12 @@ __device__ __forceinline__ SplatBox load_box(const BinArgs& a, uint32_t s, uint3
   b.cc = cc4.x;
   b.alpha = cc4.y;
   const int32_t mx = (int32_t)a.tiles_x - 1, my = (int32_t)a.tiles_y - 1;
-  const float tw = (float)(1u << a.tile_w_log2), th = (float)(1u << a.tile_h_log2);
-  b.x0 = tile_coord(b.mu_x - ext_x, mx, tw);
-  b.x1 = tile_coord(b.mu_x + ext_x, mx, tw);
-  b.y0 = tile_coord(b.mu_y - ext_y, my, th);
-  b.y1 = tile_coord(b.mu_y + ext_y, my, th);
+  const float itw = __uint_as_float((127u - a.tile_w_log2) << 23);  // 2^-lw
+  const float ith = __uint_as_float((127u - a.tile_h_log2) << 23);
+  b.x0 = tile_coord(__fsub_rn(b.mu_x, ext_x), mx, itw);
+  b.x1 = tile_coord(__fadd_rn(b.mu_x, ext_x), mx, itw);
+  b.y0 = tile_coord(__fsub_rn(b.mu_y, ext_y), my, ith);
+  b.y1 = tile_coord(__fadd_rn(b.mu_y, ext_y), my, ith);
   // ellipse_intersects_tile_gpu returns false for every tile when alpha < 1/255.
   b.valid = !(b.alpha < (1.0f / 255.0f));
   return b;
@@ -94,7 +110,7 @@ __device__ __forceinline__ SplatBox load_box(const BinArgs& a, uint32_t s, uint3
 // the subtraction of 2^23 - 0.5 is exact (Sterbenz), so the result equals the
 // reference's integer-to-float conversion plus one half without a conversion.
 __device__ __forceinline__ float pixel_center(uint32_t v) {
-  return __int_as_float(0x4B000000u | v) - 8388607.5f;
+  return __fsub_rn(__int_as_float(0x4B000000u | v), 8388607.5f);
 }
 
 // n / d correctly rounded to binary32, for d > 0, from y = RN64(1 / d) (one
@@ -108,10 +124,10 @@ __device__ __forceinline__ float pixel_center(uint32_t v) {
 // binary32 value. Results below 2^-125 in magnitude, where the binary32 grid
 // is finer relative to the value than that argument assumes, use the binary32
 // division itself; zero stays a signed zero.
-__device__ __noinline__ float div_ieee(float n, float d) { return n / d; }
+__device__ __noinline__ float div_ieee(float n, float d) { return __fdiv_rn(n, d); }
 
 __device__ __forceinline__ float div_rcp64(float n, float d, double y) {
-  const double q = (double)n * y;
+  const double q = __dmul_rn((double)n, y);
   float r = __double2float_rn(q);
   // a call, so that the compiler cannot turn the rare case into a division
   // on every lane
@@ -120,28 +136,73 @@ __device__ __forceinline__ float div_rcp64(float n, float d, double y) {
 }
 
 // ellipse_intersects_tile_gpu (binning.rs:37-96) for tile (tx, ty) of the
-// splat's tile box, in the reference's operand order (compiled without FMA
-// contraction): the quadratic form is evaluated at the tile point nearest the
+// splat's tile box, in the reference's operand order, every operation rounded
+// separately: the quadratic form is evaluated at the tile point nearest the
 // centre along x (y minimised, clamped) and along y (x minimised, clamped).
 // The reference's "tile starts outside the viewport" exit never fires for a
 // tile of the clamped box. geo = (mu_x, mu_y, -b, 2b), con = (a, c, max(a,
 // 1e-12), max(c, 1e-12)), rcp = their binary64 reciprocals (c term, a term),
-// qlim = q_max + 1e-4.
+// qlim = q_max + 1e-4. Used for warps whose term tables do not fit.
 __device__ __forceinline__ bool tile_hit(uint32_t tx, uint32_t ty, uint32_t wm1, uint32_t hm1,
                                          uint32_t lw, uint32_t lh, const float4 geo,
                                          const float4 con, const double2 rcp, float qlim) {
   const uint32_t xs = tx << lw, ys = ty << lh;
-  const float dx0 = pixel_center(xs) - geo.x;
-  const float dx1 = pixel_center(min(xs + ((1u << lw) - 1u), wm1)) - geo.x;
-  const float dy0 = pixel_center(ys) - geo.y;
-  const float dy1 = pixel_center(min(ys + ((1u << lh) - 1u), hm1)) - geo.y;
+  const float dx0 = __fsub_rn(pixel_center(xs), geo.x);
+  const float dx1 = __fsub_rn(pixel_center(min(xs + ((1u << lw) - 1u), wm1)), geo.x);
+  const float dy0 = __fsub_rn(pixel_center(ys), geo.y);
+  const float dy1 = __fsub_rn(pixel_center(min(ys + ((1u << lh) - 1u), hm1)), geo.y);
   const float x_near = clampf(0.0f, dx0, dx1);
-  const float y1 = clampf(div_rcp64(geo.z * x_near, con.w, rcp.x), dy0, dy1);
-  const float q1 = con.x * x_near * x_near + geo.w * x_near * y1 + con.y * y1 * y1;
+  const float y1 = clampf(div_rcp64(__fmul_rn(geo.z, x_near), con.w, rcp.x), dy0, dy1);
+  const float q1 = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(con.x, x_near), x_near),
+                                       __fmul_rn(__fmul_rn(geo.w, x_near), y1)),
+                             __fmul_rn(__fmul_rn(con.y, y1), y1));
   const float y_near = clampf(0.0f, dy0, dy1);
-  const float x2 = clampf(div_rcp64(geo.z * y_near, con.z, rcp.y), dx0, dx1);
-  const float q2 = con.x * x2 * x2 + geo.w * x2 * y_near + con.y * y_near * y_near;
+  const float x2 = clampf(div_rcp64(__fmul_rn(geo.z, y_near), con.z, rcp.y), dx0, dx1);
+  const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(con.x, x2), x2),
+                                       __fmul_rn(__fmul_rn(geo.w, x2), y_near)),
+                             __fmul_rn(__fmul_rn(con.y, y_near), y_near));
   return fminf(q1, q2) <= qlim;
+}
+
+// Column terms of a splat's tile column tx (the parts of tile_hit that depend
+// on the column alone): x edges, the y minimiser at the column's nearest x
+// (before its clamp to the row), a x_near^2.
+__device__ __forceinline__ float4 col_terms(uint32_t tx, uint32_t lw, uint32_t wm1, const float4 geo,
+                                            const float4 con, const double2 rcp) {
+  const uint32_t xs = tx << lw;
+  const float dx0 = __fsub_rn(pixel_center(xs), geo.x);
+  const float dx1 = __fsub_rn(pixel_center(min(xs + ((1u << lw) - 1u), wm1)), geo.x);
+  const float x_near = clampf(0.0f, dx0, dx1);
+  return make_float4(dx0, dx1, div_rcp64(__fmul_rn(geo.z, x_near), con.w, rcp.x),
+                     __fmul_rn(__fmul_rn(con.x, x_near), x_near));
+}
+
+// Row terms of tile row ty: y edges, the x minimiser at the row's nearest y
+// (before its clamp to the column), c y_near^2.
+__device__ __forceinline__ float4 row_terms(uint32_t ty, uint32_t lh, uint32_t hm1, const float4 geo,
+                                            const float4 con, const double2 rcp) {
+  const uint32_t ys = ty << lh;
+  const float dy0 = __fsub_rn(pixel_center(ys), geo.y);
+  const float dy1 = __fsub_rn(pixel_center(min(ys + ((1u << lh) - 1u), hm1)), geo.y);
+  const float y_near = clampf(0.0f, dy0, dy1);
+  return make_float4(dy0, dy1, div_rcp64(__fmul_rn(geo.z, y_near), con.z, rcp.y),
+                     __fmul_rn(__fmul_rn(con.y, y_near), y_near));
+}
+
+// tile_hit from a column entry, a row entry and kq = (a, 2b, c, qlim): the
+// same operations on the same operands, the column/row-only ones taken from
+// the tables.
+__device__ __forceinline__ bool tab_hit(const float4 col, const float4 row, const float4 kq) {
+  const float x_near = clampf(0.0f, col.x, col.y);
+  const float y_near = clampf(0.0f, row.x, row.y);
+  const float y1 = clampf(col.z, row.x, row.y);
+  const float q1 = __fadd_rn(__fadd_rn(col.w, __fmul_rn(__fmul_rn(kq.y, x_near), y1)),
+                             __fmul_rn(__fmul_rn(kq.z, y1), y1));
+  const float x2 = clampf(row.z, col.x, col.y);
+  const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(kq.x, x2), x2),
+                                       __fmul_rn(__fmul_rn(kq.y, x2), y_near)),
+                             row.w);
+  return fminf(q1, q2) <= kq.w;
 }
 
 __device__ __forceinline__ uint32_t seg_mask(int lo, int hi) {
@@ -152,9 +213,9 @@ __device__ __forceinline__ uint32_t seg_mask(int lo, int hi) {
   return upper & ~lower;
 }
 
-// Lane of the warp's splat that owns candidate `item`: the last lane whose
-// exclusive candidate prefix is <= item (lanes with no candidates share the
-// next lane's prefix and are skipped by "last").
+// Lane of the warp's splat that owns item `item` of a concatenation: the last
+// lane whose exclusive prefix is <= item (lanes with no items share the next
+// lane's prefix and are skipped by "last").
 __device__ __forceinline__ int find_owner(const uint32_t* base, uint32_t item) {
   int o = 0;
 #pragma unroll
@@ -163,11 +224,10 @@ __device__ __forceinline__ int find_owner(const uint32_t* base, uint32_t item) {
   return o;
 }
 
-// Candidate `c` of a splat's tile box (row-major) -> tile coordinates.
-__device__ __forceinline__ void box_tile(const uint4 box, uint32_t c, uint32_t& tx, uint32_t& ty) {
-  const uint32_t r = box.z <= 1u ? c : __umulhi(c, box.w);
-  tx = box.x + (c - r * box.z);
-  ty = box.y + r;
+// Candidate `c` of a splat's tile box (row-major) -> row and column in the box.
+__device__ __forceinline__ void box_rc(const uint4 box, uint32_t c, uint32_t& r, uint32_t& col) {
+  r = box.z <= 1u ? c : __umulhi(c, box.w);
+  col = c - r * box.z;
 }
 
 // Binning in depth-key order, part 1 (slot s is splat order_ids[s]; Stage 2's
@@ -177,11 +237,12 @@ __device__ __forceinline__ void box_tile(const uint4 box, uint32_t c, uint32_t& 
 // The 32 splats' candidate tiles (each splat's tile box, row-major) are
 // concatenated and tested 32 at a time, one per lane, so large and small
 // splats share the lanes evenly.
+//   0. term tables: the column and row terms of the 32 tile boxes (when they
+//      fit; otherwise every candidate evaluates the whole test).
 //   1. counting: ballot per 32 candidates; the masks, the hits before each
 //      mask, and one record per hit (tile id or candidate index, owner lane)
 //      are kept in shared memory. A slot's count is the number of hits inside
-//      its candidate range, read from the masks, and is written to `offsets`
-//      (scanned in place afterwards).
+//      its candidate range, read from the masks, and is written to `offsets`.
 //   2. staging: the tile's hits, in candidate order (= the reference's
 //      emission order: splat by splat, row-major), get a contiguous range of
 //      the staging buffers from an atomic counter and are written there with
@@ -189,17 +250,19 @@ __device__ __forceinline__ void box_tile(const uint4 box, uint32_t c, uint32_t& 
 //      tiles, (tile, raw depth bits) pairs; the block's digit histograms of
 //      the tile bits are accumulated. Warps with more hits or candidates than
 //      the shared-memory stores hold walk their candidates again for the rest.
-// The staging order of the tiles is whatever the counter gave; k_bin_place
-// moves each tile's range to its scanned offset, which restores the
-// (depth, splat index) order, and a stable sort on the tile bits alone then
-// yields the reference's (tile, depth, splat index) order. Entries at or
-// beyond the buffer capacity are not written and set the capacity status bit
-// (the host grows the buffers and runs Stage 3 again).
+// The staging order of the tiles is whatever the counter gave; the entry
+// sort's first pass reads each 32-slot tile's staged run in slot order (or
+// k_bin_place moves it to its scanned offset), which restores the (depth,
+// splat index) order, and a stable sort on the tile bits alone then yields
+// the reference's (tile, depth, splat index) order. Entries at or beyond the
+// buffer capacity are not written and set the capacity status bit (the host
+// grows the buffers and runs Stage 3 again).
 template <bool KEY64>
-__global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
+__global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
   extern __shared__ __align__(16) unsigned char bin_smem[];
   BinSplats& sp = *reinterpret_cast<BinSplats*>(bin_smem);
-  uint32_t* s_mask = reinterpret_cast<uint32_t*>(bin_smem + sizeof(BinSplats));  // [w][kMaskCap]
+  float4* s_tab = reinterpret_cast<float4*>(bin_smem + sizeof(BinSplats));  // [w][kTabCap]
+  uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_tab + kBinWarps * kTabCap);  // [w][kMaskCap]
   uint32_t* s_mrun = s_mask + kBinWarps * kMaskCap;  // [w][kMaskCap] hits before mask c
   uint32_t* s_hits = s_mrun + kBinWarps * kMaskCap;  // [w][kHitCap]
   uint32_t* s_hist = s_hits + kBinWarps * kHitCap;   // [passes][radix]
@@ -209,6 +272,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
   const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
   const uint32_t nbins = passes * radix;
   const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
+  const uint32_t lw = a.tile_w_log2, lh = a.tile_h_log2;
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
   // Record mode: per warp, per tile group, the hits counted, the staging
@@ -222,6 +286,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
   const uint32_t num_tiles = (a.max_n + 31u) / 32u;
   const uint32_t* wbase = sp.base[warp];
+  float4* wtab = s_tab + warp * kTabCap;
   uint32_t* wmask = s_mask + warp * kMaskCap;
   uint32_t* wmrun = s_mrun + warp * kMaskCap;
   uint32_t* whits = s_hits + warp * kHitCap;
@@ -242,32 +307,78 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
     const SplatBox b = load_box(a, sid, active);
 
     // Stage the warp's splats.
-    const uint32_t ncand = b.valid ? (b.x1 - b.x0 + 1u) * (b.y1 - b.y0 + 1u) : 0u;
-    uint32_t incl = ncand;
+    const uint32_t bw = b.valid ? (b.x1 - b.x0 + 1u) : 0u;
+    const uint32_t bh = b.valid ? (b.y1 - b.y0 + 1u) : 0u;
+    const uint32_t ncand = bw * bh;
+    uint32_t incl = ncand, cincl = bw, rincl = bh;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
+      const uint32_t yc = __shfl_up_sync(0xffffffffu, cincl, o);
+      const uint32_t yr = __shfl_up_sync(0xffffffffu, rincl, o);
+      if (lane >= o) {
+        incl += y;
+        cincl += yc;
+        rincl += yr;
+      }
     }
     const uint32_t base = incl - ncand;
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t wt = __shfl_sync(0xffffffffu, cincl, 31);
+    const uint32_t ht = __shfl_sync(0xffffffffu, rincl, 31);
+    const bool tab = wt + ht <= (uint32_t)kTabCap;  // warp-uniform
     __syncwarp();  // the previous tile's readers are done with the warp's shared memory
     {
-      const uint32_t w = b.valid ? (b.x1 - b.x0 + 1u) : 1u;
+      const uint32_t w = b.valid ? bw : 1u;
       const float ca_ = fmaxf(b.ca, 1e-12f), cc_ = fmaxf(b.cc, 1e-12f);
+      const float cb2 = __fmul_rn(2.0f, b.cb);
+      const float qlim =
+          __fadd_rn(b.valid ? clampf(__fmul_rn(2.0f, cgs_logf(__fmul_rn(255.0f, b.alpha))), 0.0f, 8.0f)
+                            : 0.0f,
+                    1e-4f);
       sp.box[warp][lane] =
           make_uint4(b.x0, b.y0, w, w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w));
-      sp.geo[warp][lane] = make_float4(b.mu_x, b.mu_y, -b.cb, 2.0f * b.cb);
+      sp.geo[warp][lane] = make_float4(b.mu_x, b.mu_y, -b.cb, cb2);
       sp.con[warp][lane] = make_float4(b.ca, b.cc, ca_, cc_);
+      sp.kq[warp][lane] = make_float4(b.ca, cb2, b.cc, qlim);
       sp.rcp[warp][lane] = make_double2(1.0 / (double)cc_, 1.0 / (double)ca_);
-      sp.qlim[warp][lane] =
-          (b.valid ? clampf(2.0f * cgs_logf(255.0f * b.alpha), 0.0f, 8.0f) : 0.0f) + 1e-4f;
+      sp.tb[warp][lane] = make_uint2(cincl - bw, wt + rincl - bh);
       sp.base[warp][lane] = base;
+      sp.cpre[warp][lane] = cincl - bw;
+      sp.rpre[warp][lane] = rincl - bh;
       sp.dq[warp][lane] = dq;
       sp.sid[warp][lane] = sid;
     }
     if (rec_mode && lane < (int)kMaxGroups) s_gcnt[lane] = 0u;
     __syncwarp();
+    if (tab) {
+      // 0. term tables: columns [0, wt), rows [wt, wt + ht)
+      for (uint32_t i = lane; i < wt; i += 32) {
+        const int o = find_owner(sp.cpre[warp], i);
+        wtab[i] = col_terms(sp.box[warp][o].x + (i - sp.cpre[warp][o]), lw, wm1, sp.geo[warp][o],
+                            sp.con[warp][o], sp.rcp[warp][o]);
+      }
+      for (uint32_t i = lane; i < ht; i += 32) {
+        const int o = find_owner(sp.rpre[warp], i);
+        wtab[wt + i] = row_terms(sp.box[warp][o].y + (i - sp.rpre[warp][o]), lh, hm1,
+                                 sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o]);
+      }
+      __syncwarp();
+    }
+    // the exact test of candidate ci of lane o's splat; tx, ty its tile
+    auto test = [&](int o, uint32_t ci, uint32_t& tx, uint32_t& ty) -> bool {
+      const uint4 bx = sp.box[warp][o];
+      uint32_t r, c;
+      box_rc(bx, ci, r, c);
+      tx = bx.x + c;
+      ty = bx.y + r;
+      if (tab) {
+        const uint2 t = sp.tb[warp][o];
+        return tab_hit(wtab[t.x + c], wtab[t.y + r], sp.kq[warp][o]);
+      }
+      return tile_hit(tx, ty, wm1, hm1, lw, lh, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
+                      sp.kq[warp][o].w);
+    };
     const bool big = total > (uint32_t)kMaskCap * 32u;  // warp-uniform
 
     // 1. count
@@ -281,9 +392,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
         const int o = find_owner(wbase, item);
         const uint32_t ci = item - wbase[o];
         uint32_t tx, ty;
-        box_tile(sp.box[warp][o], ci, tx, ty);
-        hit = tile_hit(tx, ty, wm1, hm1, a.tile_w_log2, a.tile_h_log2, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
-                       sp.qlim[warp][o]);
+        hit = test(o, ci, tx, ty);
         rec = ((KEY64 ? ci : ty * a.tiles_x + tx) << 5) | (uint32_t)o;
       }
       const uint32_t hits = __ballot_sync(0xffffffffu, hit);
@@ -292,7 +401,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
         wmrun[c] = run;
       }
       if (hit) {
-        const uint32_t k = run + __popc(hits & lanemask_lt());
+        const uint32_t k = run + __popc(hits & lt);
         if (k < (uint32_t)kHitCap) whits[k] = rec;
       }
       if (big) {
@@ -328,7 +437,9 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
       // slot lane.
       if (lane < (int)G) {
         const uint32_t gc = s_gcnt[lane];
-        const uint32_t gb = gc ? atomicAdd(&a.fc->tile_ctr[2], gc) : 0u;
+        const unsigned long long gb64 =
+            gc ? atomicAdd(&a.fc->stage_ctr, (unsigned long long)gc) : 0ull;
+        const uint32_t gb = gb64 >= cap ? cap : (uint32_t)gb64;  // at or past cap: not staged
         a.tile_stage[(size_t)tile * G + lane] = gb;
         a.tile_count[(size_t)tile * G + lane] = gc;
         s_gbase[lane] = gb;
@@ -340,7 +451,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
         const uint32_t g = h ? (rec >> 5) >> gshift : 0xFFFFFFFFu;
         const uint32_t peers = __match_any_sync(0xffffffffu, g);
         if (h) {
-          const uint32_t pos = s_gbase[g] + s_grun[g] + __popc(peers & lt);
+          const uint64_t pos = (uint64_t)s_gbase[g] + s_grun[g] + __popc(peers & lt);
           if (pos < cap)
             a.stage_keys[pos] = rec;
           else
@@ -372,9 +483,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
             if (item < total) {
               const int o = find_owner(wbase, item);
               uint32_t tx, ty;
-              box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
-              hit = tile_hit(tx, ty, wm1, hm1, a.tile_w_log2, a.tile_h_log2, sp.geo[warp][o], sp.con[warp][o],
-                             sp.rcp[warp][o], sp.qlim[warp][o]);
+              hit = test(o, item - wbase[o], tx, ty);
             }
             hits = __ballot_sync(0xffffffffu, hit);
           }
@@ -383,9 +492,9 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
           uint32_t rec = 0;
           if (sel) {
             const int o = find_owner(wbase, item);
-            uint32_t tx, ty;
-            box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
-            rec = ((ty * a.tiles_x + tx) << 5) | (uint32_t)o;
+            uint32_t r, cc;
+            box_rc(sp.box[warp][o], item - wbase[o], r, cc);
+            rec = (((sp.box[warp][o].y + r) * a.tiles_x + sp.box[warp][o].x + cc) << 5) | (uint32_t)o;
           }
           put_rec(sel, rec);
           hrun += __popc(hits);
@@ -395,13 +504,15 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
     }
     uint32_t sbase = 0;
     if (lane == 0) {
-      sbase = run ? atomicAdd(&a.fc->tile_ctr[2], run) : 0u;
+      const unsigned long long sb64 =
+          run ? atomicAdd(&a.fc->stage_ctr, (unsigned long long)run) : 0ull;
+      sbase = sb64 >= cap ? cap : (uint32_t)sb64;  // at or past cap: nothing is staged
       a.tile_stage[tile] = sbase;
       a.tile_count[tile] = run;
     }
     sbase = __shfl_sync(0xffffffffu, sbase, 0);
     auto put = [&](uint32_t k, uint32_t tile_id, int o) {
-      const uint32_t pos = sbase + k;
+      const uint64_t pos = (uint64_t)sbase + k;
       if (pos >= cap) {
         overflow = true;
         return;
@@ -425,9 +536,9 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
       const int o = (int)(v & 31u);
       uint32_t tile_id = v >> 5;
       if (KEY64) {
-        uint32_t tx, ty;
-        box_tile(sp.box[warp][o], tile_id, tx, ty);
-        tile_id = ty * a.tiles_x + tx;
+        uint32_t r, cc;
+        box_rc(sp.box[warp][o], tile_id, r, cc);
+        tile_id = (sp.box[warp][o].y + r) * a.tiles_x + sp.box[warp][o].x + cc;
       }
       put(k, tile_id, o);
     }
@@ -450,18 +561,16 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_count(const BinArgs a) {
           if (item < total) {
             const int o = find_owner(wbase, item);
             uint32_t tx, ty;
-            box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
-            hit = tile_hit(tx, ty, wm1, hm1, a.tile_w_log2, a.tile_h_log2, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
-                           sp.qlim[warp][o]);
+            hit = test(o, item - wbase[o], tx, ty);
           }
           hits = __ballot_sync(0xffffffffu, hit);
         }
-        const uint32_t k = hrun + __popc(hits & lanemask_lt());
+        const uint32_t k = hrun + __popc(hits & lt);
         if (((hits >> lane) & 1u) && k >= (uint32_t)kHitCap) {
           const int o = find_owner(wbase, item);
-          uint32_t tx, ty;
-          box_tile(sp.box[warp][o], item - wbase[o], tx, ty);
-          put(k, ty * a.tiles_x + tx, o);
+          uint32_t r, cc;
+          box_rc(sp.box[warp][o], item - wbase[o], r, cc);
+          put(k, (sp.box[warp][o].y + r) * a.tiles_x + sp.box[warp][o].x + cc, o);
         }
         hrun += __popc(hits);
       }
@@ -490,7 +599,7 @@ __global__ void __launch_bounds__(256) k_bin_place(const BinArgs a) {
     const uint32_t n = a.tile_count[t];
     if (n == 0) continue;
     const uint32_t src = a.tile_stage[t];
-    const uint32_t dst = a.offsets[32u * t];
+    const uint32_t dst = a.run_start ? a.run_start[t] : a.offsets[32u * t];
     if (src >= cap || dst >= cap) continue;
     const uint32_t m = min(n, min(cap - src, cap - dst));
     for (uint32_t k0 = 0; k0 < m; k0 += 256) {  // eight loads in flight per lane and array
@@ -804,7 +913,43 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_u32(const uint32_t* __res
   if (tile == num_tiles - 1 && threadIdx.x == 0) *d_total = s_base + agg;
 }
 
+// Wait drill: one warp runs the chained scan as tile 1 of a status array
+// whose tile 0 nothing publishes (two zeroed 64-bit words), so its look-back
+// polls until `limit` and sets the timeout bit.
+__global__ void k_drill_chained_scan(unsigned long long* status, uint32_t* status_word,
+                                     uint32_t limit) {
+  chained_scan_warp(status, 1u, 1u, status_word, limit);
+}
+
+// first_run[b] for the radix tiles whose first position lies in run k.
+__global__ void k_run_index(const uint32_t* __restrict__ run_start,
+                            const uint32_t* __restrict__ run_len, uint32_t num_runs,
+                            uint32_t* __restrict__ first_run, uint32_t max_tiles) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < num_runs;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t len = run_len[k];
+    if (len == 0) continue;
+    const uint64_t st = run_start[k], en = st + len;
+    const uint64_t b0 = (st + kRadixTileItems - 1) / kRadixTileItems;
+    const uint64_t b1 = (en - 1) / kRadixTileItems;
+    for (uint64_t b = b0; b <= b1 && b < max_tiles; ++b) first_run[b] = k;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_drill_chained_scan(unsigned long long* status, uint32_t* status_word,
+                                      uint32_t limit, cudaStream_t s) {
+  k_drill_chained_scan<<<1, 32, 0, s>>>(status, status_word, limit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_run_index(const uint32_t* run_start, const uint32_t* run_len, uint32_t num_runs,
+                             uint32_t* first_run, uint32_t max_tiles, cudaStream_t s) {
+  if (num_runs == 0) return cudaSuccess;
+  k_run_index<<<148 * 4, 256, 0, s>>>(run_start, run_len, num_runs, first_run, max_tiles);
+  return cudaGetLastError();
+}
 
 // Persistent grid: as many blocks as fit on the device at once (at most one
 // warp per 32-slot tile).

@@ -58,10 +58,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for a phase; returns false (and the caller flags it) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t limit = kSpinLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+
+// Wait drill: an mbarrier expecting one arrival that never comes; the bounded
+// wait gives up after `limit` tries and the timeout bit is set.
+__global__ void k_drill_mbarrier(uint32_t* status_word, uint32_t limit) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, limit)) atomicOr(status_word, kStatusBarrierTimeout);
 }
 
 __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
@@ -238,6 +251,11 @@ __global__ void __launch_bounds__(1 << (LW + LH)) k_composite(const CompositeArg
 }
 
 }  // namespace
+
+cudaError_t launch_drill_mbarrier(uint32_t* status_word, uint32_t limit, cudaStream_t s) {
+  k_drill_mbarrier<<<1, 32, 0, s>>>(status_word, limit);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_composite(const CompositeArgs& a, cudaStream_t s) {
   if (a.tiles_x == 0 || a.tiles_y == 0) return cudaSuccess;

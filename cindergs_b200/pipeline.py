@@ -551,6 +551,20 @@ class GpuPipelineState:
                     "cgs_ctx_device_bytes")
         return int(v.value)
 
+    def set_device_budget(self, nbytes: int) -> None:
+        """Caps the device memory of the scene residency and frame arena
+        (cgs_ctx_set_device_budget; 0 = no cap). Growth past it raises
+        CgsError with code CGS_E_OOM."""
+        self._check(self._lib.cgs_ctx_set_device_budget(self._ctx, int(nbytes)),
+                    "cgs_ctx_set_device_budget")
+
+    def wait_drill(self, polls: int = 1 << 16) -> tuple:
+        """Runs the bounded-wait drill (cgs_ctx_wait_drill); returns (status,
+        mask of the waits that gave up). CGS_E_TIMEOUT is the expected status."""
+        m = ctypes.c_uint32()
+        rc = self._lib.cgs_ctx_wait_drill(self._ctx, int(polls), ctypes.byref(m))
+        return int(rc), int(m.value)
+
     def kernel_profile(self) -> dict:
         """Per-kernel device ms, launches and algorithmic HBM bytes accumulated
         over the frames run with profile_stages=True since the last reset."""

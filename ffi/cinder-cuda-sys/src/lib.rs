@@ -187,6 +187,8 @@ extern "C" {
     pub fn cgs_ctx_synchronize(ctx: *mut cgs_ctx) -> c_int;
     pub fn cgs_ctx_device_bytes(ctx: *const cgs_ctx, out_bytes: *mut u64) -> c_int;
     pub fn cgs_version() -> *const c_char;
+    pub fn cgs_ctx_set_device_budget(ctx: *mut cgs_ctx, bytes: u64) -> c_int;
+    pub fn cgs_ctx_wait_drill(ctx: *mut cgs_ctx, polls: u32, out_gave_up: *mut u32) -> c_int;
 
     // ---- scene residency (GpuSceneState, render/gpu_state.rs:95-343)
     pub fn cgs_scene_upload(ctx: *mut cgs_ctx, n: u64, pos: *const f32, cov: *const f32,

@@ -34,7 +34,10 @@ extern "C" {
 #define CGS_E_ARG -1       /* invalid argument (null pointer, bad size, bad enum) */
 #define CGS_E_OOM -2       /* device or pinned-host allocation failed */
 #define CGS_E_CUDA -3      /* a CUDA runtime call failed */
-#define CGS_E_TIMEOUT -4   /* a bounded device-side wait gave up (status word set) */
+#define CGS_E_TIMEOUT -4   /* a bounded device-side wait gave up (status word set); the
+                              frame's results are undefined. If a tensor-core wait gave up
+                              twice, later frames return CGS_E_STATE: destroy and recreate
+                              the context */
 #define CGS_E_CAPACITY -5  /* a size exceeds a documented hard limit */
 #define CGS_E_STATE -6     /* call order violated (e.g. frame before scene upload) */
 
@@ -125,6 +128,21 @@ int cgs_ctx_synchronize(cgs_ctx* ctx);
 int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out_bytes);
 /* Library version string. */
 const char* cgs_version(void);
+/* Caps the device memory the context's growable buffers (scene residency and
+ * frame arena) may hold; 0 (the default) removes the cap. A call that would
+ * grow past it fails with CGS_E_OOM and leaves the context usable. No
+ * reference counterpart: the reference's arena grows by 1.5x without a limit
+ * (render/gpu_pool.rs:43-49). */
+int cgs_ctx_set_device_budget(cgs_ctx* ctx, uint64_t bytes);
+/* Failure drill for the bounded device waits: runs the chained-scan look-back
+ * (bit 0), the radix sort's digit look-back (bit 1) and the compositor's
+ * mbarrier wait (bit 2), each against a predecessor or barrier that nothing
+ * completes and with `polls` polls (1..2^22) instead of the kernels' 2^22.
+ * Each wait gives up, sets its status bit and returns; *out_gave_up receives
+ * the mask of drills that gave up. Returns CGS_E_TIMEOUT when any did (the
+ * expected outcome) and leaves the context usable. No reference counterpart:
+ * the reference's waits are unbounded. */
+int cgs_ctx_wait_drill(cgs_ctx* ctx, uint32_t polls, uint32_t* out_gave_up);
 
 /* ---- scene residency (GpuSceneState, render/gpu_state.rs:95-343) ---- */
 
