@@ -7,6 +7,14 @@ layer pinned, stiffness 40, damping 4/s, dt 1/60), 1920x1080, a camera
 orbiting at radius 4. One step = one frame: a host spring step, then Stage 1
 (deform), Stage 2 (project), Stage 3 (bin + sort) and Stage 4 (composite).
 
+The default line also carries, at 1 GPU: `stage4` ((pixel, entry) pairs/s and
+the compositor's FP32 issue fraction), `error_floor` (a float64 evaluation of
+the frame's formulas on a sample, against the f32 frame), `mvc` (the
+polygon-cage leg below, with fewer frames) and `views` (the multi-view leg
+below); `--no-legs` leaves them out. `e2e` runs the same frames through the C
+ABI with the cage vertices uploaded and the RGBA8 frame read back every step,
+and reports the host time per step by part.
+
 Arms:
   python bench.py [--gpus N --steps K --warmup W]     this library (CUDA, sm_100a)
   python bench.py --impl reference ...                the reference's CPU path
@@ -94,6 +102,9 @@ def parse():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="default workload only: skip the error floor and the MVC and "
+                         "multi-view legs")
     ap.add_argument("--entry-sort", type=int, default=0,
                     help="tile-entry sort: 0 auto, 1 radix passes, 2 one-pass tile transpose")
     ap.add_argument("--radix-bits", type=int, default=0,
@@ -303,51 +314,69 @@ def run_ours(args):
     kp = st.kernel_profile()
     value = world * args.steps / (ms / 1000.0)
 
-    # ---- e2e: public API with host buffers, copies inside the timed region
-    # two page-locked output images: frame i's pixels are copied to the host
-    # while frame i + 1 renders (cgs_readback_rgba8_async), and each is
-    # waited for before its image is reused
+    # ---- e2e: through the C ABI with host buffers, copies inside the timed
+    # region. Per step: the host spring step, the cage vertices uploaded
+    # (cgs_cage_vertices_update), the frame enqueued (cgs_execute_frame, no
+    # host wait), and the RGBA8 frame read back into page-locked host memory
+    # (cgs_readback_rgba8_async: frame i's copy runs while frame i + 1
+    # renders; each image is waited for before it is reused). Cameras and
+    # compositor blocks are host inputs prepared like the caller's own
+    # structs; the host time per step is reported by part.
+    import ctypes
+    from cindergs_b200 import _abi
+    lib, ctx = st._lib, st.handle
+    e2e_frames = [frame + world * i for i in range(args.steps)]
+    cams_c = [st._camera(wl.camera(f)) for f in e2e_frames]
+    comps_c = [st._compositor(wl.compositor(wl.camera(f))) for f in e2e_frames]
+    params_c = _abi.CgsFrameParams(float(wl.strain_split_threshold), float(wl.mip_filter_3d_var),
+                                   1.0 / 255.0, 0.5, 0, 0, 0, int(args.radix_bits),
+                                   int(args.entry_sort), int(args.tile_shape))
     pinned_out = [torch.empty((args.height, args.width, 4), dtype=torch.uint8).pin_memory()
                   for _ in range(2)]
-    out_np = [t.numpy() for t in pinned_out]
-    vert_pinned = torch.empty(wl.cage.mesh.rest_vertices.shape, dtype=torch.float32).pin_memory()
+    out_ptr = [ctypes.c_void_p(t.data_ptr()) for t in pinned_out]
+    nverts = wl.cage.mesh.rest_vertices.shape[0]
+    vert_host = np.empty((nverts, 3), np.float32)
+    ticket = ctypes.c_uint64()
+    host_ms = {"spring_step": 0.0, "enqueue": 0.0, "readback_wait": 0.0}
     barrier()
     t0 = time.perf_counter()
     e2e_start = torch.cuda.Event(enable_timing=True)
     e2e_end = torch.cuda.Event(enable_timing=True)
     e2e_start.record(stream)
-    import ctypes
-    wl.step()
-    vert_pinned.numpy()[:] = wl.cage.vertices()
     prev_ticket = None
     for step in range(args.steps):
-        cam = wl.camera(frame)
-        frame += world
-        # host vertices -> device (pinned source), then the frame (enqueued),
-        # the next step's spring update on the host while it renders, then the
-        # pixels back
-        st._check(st._lib.cgs_cage_vertices_update(
-            st.handle, ctypes.c_void_p(vert_pinned.data_ptr()), vert_pinned.shape[0]),
-            "cgs_cage_vertices_update")
-        cam_c = wl.compositor(cam)
-        st.execute_frame_gpu(wl.scene, cages, cam, cam_c, wl.strain_split_threshold,
-                             wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, radix_bits=args.radix_bits,
-                             entry_sort=args.entry_sort, tile_shape=args.tile_shape,
-                             stage_timings=False)
-        ticket = st.readback_framebuffer_rgba8_async(out_np[step % 2])
+        ta = time.perf_counter()
         wl.step()
-        next_verts = wl.cage.vertices()
-        if prev_ticket is not None:
-            st.readback_wait(prev_ticket)  # the previous frame's pixels are on the host
-        prev_ticket = ticket
-        vert_pinned.numpy()[:] = next_verts
+        vert_host[:] = wl.cage.vertices()
+        tb = time.perf_counter()
+        _abi.check(lib.cgs_cage_vertices_update(ctx, vert_host.ctypes.data_as(ctypes.c_void_p),
+                                                nverts), "cgs_cage_vertices_update", ctx)
+        _abi.check(lib.cgs_execute_frame(ctx, ctypes.byref(cams_c[step]),
+                                         ctypes.byref(comps_c[step]), ctypes.byref(params_c),
+                                         None), "cgs_execute_frame", ctx)
+        _abi.check(lib.cgs_readback_rgba8_async(ctx, out_ptr[step % 2], args.width, args.height,
+                                                ctypes.byref(ticket)),
+                   "cgs_readback_rgba8_async", ctx)
+        tc = time.perf_counter()
+        if prev_ticket is not None:  # the previous frame's pixels are on the host
+            _abi.check(lib.cgs_readback_wait(ctx, prev_ticket), "cgs_readback_wait", ctx)
+        prev_ticket = ticket.value
+        td = time.perf_counter()
+        host_ms["spring_step"] += (tb - ta) * 1000.0
+        host_ms["enqueue"] += (tc - tb) * 1000.0
+        host_ms["readback_wait"] += (td - tc) * 1000.0
     if prev_ticket is not None:
-        st.readback_wait(prev_ticket)
+        _abi.check(lib.cgs_readback_wait(ctx, prev_ticket), "cgs_readback_wait", ctx)
     e2e_end.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(max(e2e_start.elapsed_time(e2e_end),
-                                (time.perf_counter() - t0) * 1000.0), device=f"cuda:{local}")
+    frame += world * args.steps
+    e2e_wall = (time.perf_counter() - t0) * 1000.0
+    e2e_dev = e2e_start.elapsed_time(e2e_end)
+    e2e_ms = max_over_ranks(max(e2e_dev, e2e_wall), device=f"cuda:{local}")
     e2e_value = world * args.steps / (e2e_ms / 1000.0)
+    e2e_parts = {k: v / args.steps for k, v in host_ms.items()}
+    e2e_parts["wall_ms_per_step"] = e2e_wall / args.steps
+    e2e_parts["device_ms_per_step"] = e2e_dev / args.steps
 
     # ---- the same frames with 32x16 screen tiles (the autotuner's choice at
     # 1080p: fewer tile entries to bin and sort, more candidates per pixel)
@@ -376,6 +405,19 @@ def run_ours(args):
         alt = {"views_per_s": world * args.steps / (alt_ms / 1000.0),
                "ms_per_step": alt_ms / args.steps,
                "tile_entries": last_alt.total_tile_entries}
+
+    # ---- one more frame of the workload with the f32 image written: the
+    # float64 error floor of its formulas on a sample (1 GPU)
+    floor = None
+    if world == 1 and not args.no_legs and args.tile_shape == 0:
+        from cindergs_b200 import error_floor
+        wl.step()
+        cam_f = wl.camera(frame)
+        comp_f = wl.compositor(cam_f)
+        st.execute_frame_gpu(wl.scene, cages, cam_f, comp_f, wl.strain_split_threshold,
+                             wl.mip_filter_3d_var, 1.0 / 255.0, 0.5, force_stage3=True,
+                             write_f32=True)
+        floor = error_floor.frame_floor(st, wl.scene, cages, cam_f, comp_f)
 
     if rank == 0:
         hbm, peak_kind = peaks()
@@ -420,13 +462,53 @@ def run_ours(args):
                          "frac": (per_launch_bytes / (per_launch_ms / 1000.0) / 1e9) / hbm,
                          "traffic": traffic, "alg_bytes_per_launch": per_launch_bytes},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step":
-                    int(wl.cage.mesh.rest_vertices.nbytes),
-                    "d2h_bytes_per_step": int(args.width * args.height * 4 + 36)},
+                    int(wl.cage.mesh.rest_vertices.nbytes) + 96 + 48 + 40,
+                    "d2h_bytes_per_step": int(args.width * args.height * 4 + 36),
+                    "host_ms_per_step": e2e_parts,
+                    "path": "C ABI: cage vertices up, frame, asynchronous RGBA8 readback"},
             "gpu_launches": gpu_launches,
             "clocks": clock.summary(),
         }
         if alt is not None:
             line["tile_32x16"] = alt
+        # Stage 4 is FP32/SFU issue-bound: (pixel, entry) pairs per second,
+        # from the entries the compositor gathered (its algorithmic bytes are
+        # 52 B per gathered entry + 8 B per tile + 4 B per pixel), and the FP32
+        # issue rate those pairs need at 24 FP32 operations each (the blend
+        # loop's arithmetic per pair that passes the opacity and q cuts)
+        # against 128 FP32 lanes per SM at the sampled SM clock.
+        ck = kp.get("composite")
+        if ck and ck["launches"]:
+            tw, th = {0: (16, 16), 1: (8, 8), 2: (32, 16)}[args.tile_shape]
+            tiles = ((args.width + tw - 1) // tw) * ((args.height + th - 1) // th)
+            fetched = max(ck["alg_bytes"] / max(args.steps, 1) - 4 * args.width * args.height
+                          - 8 * tiles, 0) / 52.0
+            pairs = fetched * tw * th
+            cms = ck["ms"] / max(args.steps, 1)
+            clk = (line["clocks"].get("sm_mhz") or 1965.0) * 1e6
+            pps = pairs / (cms / 1000.0)
+            line["stage4"] = {"ms_per_frame": cms, "entries_gathered_per_frame": fetched,
+                              "pixel_entry_pairs_per_frame": pairs, "pairs_per_s": pps,
+                              "fp32_ops_per_pair": 24,
+                              "fp32_issue_frac": pps * 24 / (148 * 128 * clk),
+                              "hbm_frac": kernels.get("composite", {}).get("hbm_frac")}
+        if floor is not None:
+            line["error_floor"] = floor
+        if world == 1 and not args.no_legs:
+            st.close()
+            st = None
+            torch.cuda.empty_cache()
+            # the legs' own CPU baselines run in their standalone workloads
+            for name, fn, over in (("mvc", mvc_result, {"steps": min(args.steps, 10)}),
+                                   ("views", views_result, {"steps": min(args.steps, 5)})):
+                try:
+                    sub = argparse.Namespace(**{**vars(args), **over, "gaussians": None,
+                                                "no_cpu_baseline": True, "width": 1920,
+                                                "height": 1080})
+                    line[name] = fn(sub)
+                except Exception as exc:  # a leg that fails is reported, not fatal
+                    line[name] = {"failed": f"{type(exc).__name__}: {exc}"}
+                torch.cuda.empty_cache()
         if world == 1 and not args.no_cpu_baseline:
             try:
                 bt = cages.bind_tet
@@ -440,7 +522,8 @@ def run_ours(args):
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
                                         "kind": "port", "sample": f"failed: {exc}"}
         print(json.dumps(line), flush=True)
-    st.close()
+    if st is not None:
+        st.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -449,6 +532,14 @@ def run_ours(args):
 
 def run_mvc(args):
     """Exact vs learned MVC Stage 1 on the polygon-cage workload (1 GPU)."""
+    print(json.dumps(mvc_result(args)), flush=True)
+    return 0
+
+
+def mvc_result(args) -> dict:
+    """The polygon-cage leg: exact stored bindings vs the learned field
+    (cached codes and per-frame network), the learned error judged by the
+    exact deformation of the same frames."""
     import torch
     from cindergs_b200 import GpuPipelineState, _abi, workloads
     torch.cuda.set_device(0)
@@ -606,13 +697,19 @@ def run_mvc(args):
                           "bytes_per_launch": mk.get("alg_bytes")},
             "peak_kind": pk["kind"]},
     }
-    print(json.dumps(line), flush=True)
     st.close()
-    return 0
+    return line
 
 
 def run_views(args):
     """Per-view frames vs batched views vs a replayed CUDA graph (1 GPU)."""
+    print(json.dumps(views_result(args)), flush=True)
+    return 0
+
+
+def views_result(args) -> dict:
+    """The batched multi-view leg: 64 autotuned views per step as per-view
+    frame calls, one batched call and one replayed CUDA graph."""
     import torch
     from cindergs_b200 import GpuPipelineState, workloads
     torch.cuda.set_device(0)
@@ -708,9 +805,8 @@ def run_views(args):
         "cpu_baseline": cpu,
         "clocks": clock.summary(),
     }
-    print(json.dumps(line), flush=True)
     st.close()
-    return 0
+    return line
 
 
 def run_large(args):
