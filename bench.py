@@ -288,6 +288,13 @@ def run_ours(args):
 
     for _ in range(max(args.warmup, 3)):
         render()
+    # Kernel launch shapes (block sizes) chosen by the autotuner on the
+    # workload's current frame; every shape renders the same frame.
+    from cindergs_b200 import autotune
+    cam_t = wl.camera(frame)
+    shape, _ = autotune.tune_launch_shape(st, wl.scene, cages, cam_t, wl.compositor(cam_t),
+                                          radix_bits=args.radix_bits, entry_sort=args.entry_sort,
+                                          tile_shape=args.tile_shape)
     # Per-stage device times of a few representative frames (not timed).
     stage_rows = [render(profile=True, timings=True) for _ in range(3)]
     st.synchronize()
@@ -450,7 +457,8 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_dict(args, wl, world),
+            "data": "synthetic", "config": dict(config_dict(args, wl, world),
+                                                launch_shape=shape),
             "stages_ms": stages,
             "frame_counts": {"active_gaussians": last.active_gaussians,
                              "surviving_gaussians": last.surviving_gaussians,

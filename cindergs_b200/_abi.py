@@ -116,6 +116,12 @@ class CgsCollisionPlane(ctypes.Structure):
                 ("pad", ctypes.c_float * 2)]
 
 
+class CgsLaunchShape(ctypes.Structure):
+    """cgs_launch_shape: block sizes of the frame's kernels (0 = default)."""
+    _fields_ = [("project_threads", _u32), ("bin_blocks_per_sm", _u32),
+                ("ranges_blocks", _u32), ("pad", _u32)]
+
+
 assert ctypes.sizeof(CgsSpringCage) == 32 and ctypes.sizeof(CgsCollisionPlane) == 32
 assert ctypes.sizeof(CgsCamera) == 96
 assert ctypes.sizeof(CgsCompositor) == 48
@@ -128,6 +134,7 @@ SIGNATURES = {
     "cgs_ctx_device_bytes": (_int, [_vp, ctypes.POINTER(_u64)]),
     "cgs_version": (ctypes.c_char_p, []),
     "cgs_ctx_set_device_budget": (_int, [_vp, _u64]),
+    "cgs_ctx_set_launch_shape": (_int, [_vp, ctypes.POINTER(CgsLaunchShape)]),
     "cgs_ctx_wait_drill": (_int, [_vp, _u32, ctypes.POINTER(_u32)]),
     "cgs_scene_upload": (_int, [_vp, _u64, _vp, _vp, _vp, _vp, _i32]),
     "cgs_tet_cages_upload": (_int, [_vp, _u32, _vp, _vp, _u32, _vp, _vp]),

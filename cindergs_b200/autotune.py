@@ -1,4 +1,5 @@
-"""Per-resolution tuning of the frame's free parameters.
+"""Per-resolution tuning of the frame's free parameters, and of its kernels'
+launch shapes.
 
 Three parameters are tuned per viewport: the screen tile shape of Stages 3
 and 4 (the reference's 16 x 16 pixels, 8 x 8 or 32 x 16: larger tiles give
@@ -12,6 +13,12 @@ alpha is below the 1/255 cut there anyway. For each distinct viewport of a
 set of views, one representative view is rendered with every candidate and
 the candidate with the smallest median Stage 3 + Stage 4 device time is
 kept.
+
+Launch shapes (`tune_launch_shape`): the Stage 2 block size (128, 256 or 512
+threads), the binning kernel's resident blocks per SM (1 or 2) and the
+tile-range kernel's grid are tuned one after another (coordinate descent,
+each over the others' current best) on one view, by the median Stage 2 + 3 +
+4 device time; every shape gives the same frame bit for bit.
 """
 from __future__ import annotations
 
@@ -70,3 +77,33 @@ def per_view(best: dict, compositors):
         rbs.append(rb)
         ess.append(es)
     return tss, rbs, ess
+
+
+LAUNCH_CHOICES = {"project_threads": (256, 128, 512), "bin_blocks_per_sm": (2, 1),
+                  "ranges_blocks": (1184, 592, 2368)}
+
+
+def tune_launch_shape(state, scene, cages, camera, compositor, repeats: int = 3, **frame_kw):
+    """Chooses the launch shape for frames like (camera, compositor) and sets
+    it on `state`; returns (shape dict, median Stage 2-4 ms)."""
+    best = {k: v[0] for k, v in LAUNCH_CHOICES.items()}
+
+    def cost(shape):
+        state.set_launch_shape(**shape)
+        state.execute_frame_gpu(scene, cages, camera, compositor, force_stage3=True, **frame_kw)
+        ms = []
+        for _ in range(repeats):
+            t = state.execute_frame_gpu(scene, cages, camera, compositor, force_stage3=True,
+                                        profile_stages=True, **frame_kw)
+            ms.append(t.stage2_project_ms + t.stage3_bin_sort_ms + t.stage4_composite_ms)
+        return statistics.median(ms)
+
+    best_ms = cost(best)
+    for key, values in LAUNCH_CHOICES.items():
+        for v in values[1:]:
+            trial = dict(best, **{key: v})
+            ms = cost(trial)
+            if ms < best_ms:
+                best, best_ms = trial, ms
+    state.set_launch_shape(**best)
+    return best, best_ms

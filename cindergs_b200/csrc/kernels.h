@@ -182,6 +182,7 @@ cudaError_t launch_bind(const BindArgs& a, cudaStream_t s);
 
 // ---- Stage 2 (stage2_project.cu) -------------------------------------------
 struct ProjectArgs {
+  uint32_t threads;           // block size: 128, 256 (0) or 512
   const float4* pos;          // [max_n] xyz + opacity
   const float4* cova;         // [max_n]
   const float2* covb;         // [max_n]
@@ -245,6 +246,7 @@ struct BinArgs {
   uint32_t* tile_stage;         // [ceil(max_n/32)] staging start of each 32-slot tile
   uint32_t* tile_count;         // [ceil(max_n/32)] entries of each 32-slot tile
   const uint32_t* run_start;    // placement: first entry of each 32-slot tile (else offsets)
+  uint32_t blocks_per_sm;       // resident blocks per SM of the count kernel (0: all that fit)
   FrameCounters* fc;
   int key64;
   uint32_t depth_bits;          // depth bits in a 32-bit key
@@ -309,7 +311,7 @@ cudaError_t launch_chunk_place(const TransposeArgs& a, cudaStream_t s);
 // min(*n_ptr, capacity) words. ranges zeroed.
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
                                uint32_t capacity, uint32_t total_tiles, uint32_t* ranges,
-                               cudaStream_t s);
+                               uint32_t blocks, cudaStream_t s);
 // Generic exclusive scan of n u32 (chained scan); total -> *d_total.
 cudaError_t launch_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* d_total,
                             unsigned long long* status, uint32_t* tile_ctr, uint32_t* status_word,

@@ -320,6 +320,7 @@ struct cgs_ctx {
   // Device bytes the arena may hold (cgs_ctx_set_device_budget; 0 = no
   // limit) and the bytes its growable buffers hold now.
   uint64_t budget = 0, held = 0;
+  cgs_launch_shape shape{};  // cgs_ctx_set_launch_shape (zeros: defaults)
   int ensure(DevBuf& b, size_t bytes, const char* what) {
     if (bytes <= b.cap && b.p) return CGS_OK;
     size_t nb = grow(b.cap, bytes);
@@ -473,6 +474,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
     *splat_passes = sort_passes(dbits, srb);
   }
   BinArgs b{};
+  b.blocks_per_sm = ctx->shape.bin_blocks_per_sm;
   b.recs = ctx->recs.as<SplatRec>();
   b.order_keys = ctx->skeys[ctx->s3_order_src].as<uint32_t>();
   b.order_ids = ctx->sids[ctx->s3_order_src].as<uint32_t>();
@@ -614,7 +616,8 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   ctx->kend();
   ctx->kbegin(CGS_K_TILE_RANGES);
   CGS_CUDA(launch_tile_ranges(ctx->keys[*result_src].as<uint32_t>(), d.key64 ? 0u : d.depth_bits,
-                              n_ptr, ctx->entry_cap, d.total_tiles, ctx->ranges.as<uint32_t>(), s),
+                              n_ptr, ctx->entry_cap, d.total_tiles, ctx->ranges.as<uint32_t>(),
+                              ctx->shape.ranges_blocks, s),
            "ranges launch");
   ctx->kend();
   return CGS_OK;
@@ -908,6 +911,18 @@ int cgs_ctx_synchronize(cgs_ctx* ctx) {
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
   CGS_TRY(drain(ctx, true));
   return ctx->take_sticky();
+}
+
+int cgs_ctx_set_launch_shape(cgs_ctx* ctx, const cgs_launch_shape* shape) {
+  if (!ctx || !shape) return CGS_E_ARG;
+  const uint32_t t = shape->project_threads;
+  if (t != 0 && t != 128 && t != 256 && t != 512)
+    return ctx->fail(CGS_E_ARG, "project_threads must be 0, 128, 256 or 512");
+  if (shape->bin_blocks_per_sm > 8) return ctx->fail(CGS_E_ARG, "bin_blocks_per_sm must be <= 8");
+  if (shape->ranges_blocks > 65535) return ctx->fail(CGS_E_ARG, "ranges_blocks must be <= 65535");
+  ctx->shape = *shape;
+  ++ctx->state_epoch;  // launch shapes are part of a captured view graph
+  return CGS_OK;
 }
 
 int cgs_ctx_set_device_budget(cgs_ctx* ctx, uint64_t bytes) {
@@ -2021,6 +2036,7 @@ int enqueue_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_compositor* 
 
   // ---------------- Stage 2
   ProjectArgs p{};
+  p.threads = ctx->shape.project_threads;
   if (deform_on) {
     p.pos = ctx->def_pos.as<float4>();
     p.cova = ctx->def_cova.as<float4>();

@@ -21,7 +21,8 @@
 namespace cgs {
 namespace {
 
-constexpr int kProjectThreads = 256;
+constexpr int kProjectThreads = 256;     // default block size
+constexpr int kProjectMaxThreads = 512;  // largest block size a launch shape may ask for
 
 struct ShCoeffs {
   float c[48];
@@ -104,8 +105,8 @@ __device__ __forceinline__ float3 eval_sh(const float* c, float dx, float dy, fl
                      clampf(b + 0.5f, 0.0f, 1.0f));
 }
 
-__global__ void __launch_bounds__(kProjectThreads) k_project(const ProjectArgs a) {
-  const uint32_t idx = blockIdx.x * kProjectThreads + threadIdx.x;
+__global__ void __launch_bounds__(kProjectMaxThreads) k_project(const ProjectArgs a) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
   bool visible = false;
   if (idx < active && idx < a.max_n) {
@@ -351,7 +352,9 @@ cudaError_t launch_scene_decode_quantized(uint32_t n, const float* pos, const ui
 
 cudaError_t launch_project(const ProjectArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
-  k_project<<<(a.max_n + kProjectThreads - 1) / kProjectThreads, kProjectThreads, 0, s>>>(a);
+  const uint32_t t = a.threads ? a.threads : kProjectThreads;
+  if (t != 128 && t != 256 && t != 512) return cudaErrorInvalidValue;
+  k_project<<<(a.max_n + t - 1) / t, t, 0, s>>>(a);
   return cudaGetLastError();
 }
 

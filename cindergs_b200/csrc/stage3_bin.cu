@@ -956,6 +956,7 @@ cudaError_t launch_run_index(const uint32_t* run_start, const uint32_t* run_len,
 template <bool KEY64>
 cudaError_t launch_bin_count_t(const BinArgs& a, cudaStream_t s) {
   static int resident = 0;  // blocks of k_bin_count<KEY64> the device runs at once
+  static int sm_count = 0;
   if (resident == 0) {
     cudaError_t e = cudaFuncSetAttribute(k_bin_count<KEY64>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBinSmem);
@@ -967,9 +968,13 @@ cudaError_t launch_bin_count_t(const BinArgs& a, cudaStream_t s) {
                                                            kBinSmem)) != cudaSuccess)
       return e;
     resident = std::max(1, sms * std::max(per_sm, 1));
+    sm_count = std::max(1, sms);
   }
+  // a launch shape may ask for fewer resident blocks per SM than fit
+  uint32_t want = (uint32_t)resident;
+  if (a.blocks_per_sm) want = std::min<uint32_t>(want, a.blocks_per_sm * (uint32_t)sm_count);
   const uint32_t tiles = (a.max_n + 31u) / 32u;
-  const uint32_t blocks = std::min<uint32_t>((uint32_t)resident, (tiles + kBinWarps - 1) / kBinWarps);
+  const uint32_t blocks = std::min<uint32_t>(want, (tiles + kBinWarps - 1) / kBinWarps);
   k_bin_count<KEY64><<<blocks, kBinThreads, kBinSmem, s>>>(a);
   return cudaGetLastError();
 }
@@ -1016,8 +1021,9 @@ cudaError_t launch_chunk_place(const TransposeArgs& a, cudaStream_t s) {
 
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
                                uint32_t capacity, uint32_t total_tiles, uint32_t* ranges,
-                               cudaStream_t s) {
-  k_tile_ranges<<<148 * 8, 256, 0, s>>>(sorted, shift, n_ptr, capacity, total_tiles, ranges);
+                               uint32_t blocks, cudaStream_t s) {
+  k_tile_ranges<<<blocks ? blocks : 148 * 8, 256, 0, s>>>(sorted, shift, n_ptr, capacity,
+                                                         total_tiles, ranges);
   return cudaGetLastError();
 }
 

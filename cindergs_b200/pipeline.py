@@ -551,6 +551,14 @@ class GpuPipelineState:
                     "cgs_ctx_device_bytes")
         return int(v.value)
 
+    def set_launch_shape(self, project_threads: int = 0, bin_blocks_per_sm: int = 0,
+                         ranges_blocks: int = 0) -> None:
+        """Block sizes of the frame's kernels (cgs_ctx_set_launch_shape; 0 =
+        the library's default); chosen by cindergs_b200.autotune."""
+        shp = _abi.CgsLaunchShape(int(project_threads), int(bin_blocks_per_sm), int(ranges_blocks), 0)
+        self._check(self._lib.cgs_ctx_set_launch_shape(self._ctx, ctypes.byref(shp)),
+                    "cgs_ctx_set_launch_shape")
+
     def set_device_budget(self, nbytes: int) -> None:
         """Caps the device memory of the scene residency and frame arena
         (cgs_ctx_set_device_budget; 0 = no cap). Growth past it raises

@@ -156,6 +156,16 @@ pub struct cgs_collision_plane {
     pub pad: [f32; 2],
 }
 
+/// Launch shapes of the frame's kernels (cgs_ctx_set_launch_shape).
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct cgs_launch_shape {
+    pub project_threads: u32,
+    pub bin_blocks_per_sm: u32,
+    pub ranges_blocks: u32,
+    pub pad: u32,
+}
+
 /// Statistics of one cgs_execute_views step.
 #[repr(C)]
 #[derive(Clone, Copy, Debug, Default)]
@@ -187,6 +197,7 @@ extern "C" {
     pub fn cgs_ctx_synchronize(ctx: *mut cgs_ctx) -> c_int;
     pub fn cgs_ctx_device_bytes(ctx: *const cgs_ctx, out_bytes: *mut u64) -> c_int;
     pub fn cgs_version() -> *const c_char;
+    pub fn cgs_ctx_set_launch_shape(ctx: *mut cgs_ctx, shape: *const cgs_launch_shape) -> c_int;
     pub fn cgs_ctx_set_device_budget(ctx: *mut cgs_ctx, bytes: u64) -> c_int;
     pub fn cgs_ctx_wait_drill(ctx: *mut cgs_ctx, polls: u32, out_gave_up: *mut u32) -> c_int;
 

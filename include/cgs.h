@@ -128,6 +128,19 @@ int cgs_ctx_synchronize(cgs_ctx* ctx);
 int cgs_ctx_device_bytes(const cgs_ctx* ctx, uint64_t* out_bytes);
 /* Library version string. */
 const char* cgs_version(void);
+/* Launch shapes of the frame's kernels: the block sizes the autotuner picks
+ * (cindergs_b200/autotune.py). Zero fields keep the library's defaults. No
+ * reference counterpart: the reference launches fixed CubeDims. */
+typedef struct cgs_launch_shape {
+  uint32_t project_threads;    /* Stage 2 block: 128, 256 (default) or 512 threads */
+  uint32_t bin_blocks_per_sm;  /* Stage 3 binning: resident 256-thread blocks per SM
+                                  (default: as many as fit, 2) */
+  uint32_t ranges_blocks;      /* tile-range kernel: blocks of 256 threads (default 1184) */
+  uint32_t pad;
+} cgs_launch_shape;
+/* Sets the launch shape of the following frames and view steps (a captured
+ * view graph is rebuilt). CGS_E_ARG for a value outside the ranges above. */
+int cgs_ctx_set_launch_shape(cgs_ctx* ctx, const cgs_launch_shape* shape);
 /* Caps the device memory the context's growable buffers (scene residency and
  * frame arena) may hold; 0 (the default) removes the cap. A call that would
  * grow past it fails with CGS_E_OOM and leaves the context usable. No
