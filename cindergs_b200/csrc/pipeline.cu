@@ -285,7 +285,19 @@ struct cgs_ctx {
     cudaEvent_t kev[2 * kMaxMarks] = {};
     int kid[kMaxMarks] = {};
     int kcount = 0;
+    // what it takes to render the frame again after its tile entries
+    // overflowed while later frames were in flight: its arguments and the
+    // cage vertices it deformed with (device snapshots)
+    cgs_camera cam{};
+    cgs_compositor comp{};
+    cgs_frame_params params{};
+    DevBuf verts_snap, mvc_snap;
+    size_t verts_bytes = 0, mvc_bytes = 0;
+    bool overflowed = false;
   } ring[kRing];
+  // The arena holds an earlier frame's intermediates (a re-render), not the
+  // last frame's, until the next frame.
+  bool arena_rerendered = false;
   int next_slot = 0;
   int cur = -1;              // slot of the frame being enqueued
   bool kprof = false;
@@ -707,8 +719,9 @@ int check_slot(cgs_ctx* ctx, int k, bool block) {
       CGS_TRY(rerun_stage34(ctx, entries));
       entries = ctx->h_ring[k].fc.entries;
     } else {
-      ctx->sticky = CGS_E_CAPACITY;
-      ctx->sticky_msg = "an earlier frame's tile entries exceeded the key buffers";
+      // a later frame is in flight: its pixels are rendered again if a
+      // readback waits for them (rerender_slot); the buffers grow now
+      p.overflowed = true;
       ctx->entry_cap = std::max(ctx->entry_cap,
                                 (uint32_t)std::min<uint64_t>((uint64_t)entries * 13 / 10 + 4096, (uint64_t)kMaxEntryCap));
     }
@@ -2158,6 +2171,24 @@ int cgs_execute_frame(cgs_ctx* ctx, const cgs_camera* camera, const cgs_composit
   P.W = W;
   P.H = H;
   P.write_f32 = d.write_f32;
+  P.overflowed = false;
+  P.cam = *camera;
+  P.comp = *comp;
+  P.params = *params;
+  P.verts_bytes = P.mvc_bytes = 0;
+  if (ctx->has_cages && ctx->cage_verts.p) {
+    P.verts_bytes = (size_t)ctx->num_verts * 12;
+    CGS_TRY(ctx->ensure(P.verts_snap, P.verts_bytes ? P.verts_bytes : 4, "frame vertex snapshot"));
+    CGS_CUDA(cudaMemcpyAsync(P.verts_snap.p, ctx->cage_verts.p, P.verts_bytes,
+                             cudaMemcpyDeviceToDevice, ctx->stream), "vertex snapshot");
+  }
+  if (ctx->mvc_nb > 0 && ctx->mvc_verts.p) {
+    P.mvc_bytes = (size_t)ctx->mvc_V * 16;
+    CGS_TRY(ctx->ensure(P.mvc_snap, P.mvc_bytes ? P.mvc_bytes : 4, "frame vertex snapshot"));
+    CGS_CUDA(cudaMemcpyAsync(P.mvc_snap.p, ctx->mvc_verts.p, P.mvc_bytes,
+                             cudaMemcpyDeviceToDevice, ctx->stream), "vertex snapshot");
+  }
+  ctx->arena_rerendered = false;
   ctx->cur = -1;
   ctx->latest_slot = slot;
   if (!cached) ctx->last_desc = d;
@@ -2441,6 +2472,79 @@ int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t heig
   return ctx->take_sticky();
 }
 
+namespace {
+
+// Renders frame slot k again (Stages 1-4 from its stored arguments and cage
+// vertex snapshots, with the grown key buffers) into out (rows of `pitch`
+// pixels), synchronously; the current cage vertices are restored after, and
+// the next frame deforms and bins afresh.
+int rerender_slot(cgs_ctx* ctx, int k, uint32_t* out, uint32_t pitch) {
+  cgs_ctx::Pending& p = ctx->ring[k];
+  cudaStream_t s = ctx->stream;
+  CGS_TRY(drain(ctx, true));  // every frame checked (a latest-frame re-run happens first)
+  DevBuf save_t, save_m;
+  if (p.verts_bytes) {
+    CGS_CUDA(cudaMalloc(&save_t.p, p.verts_bytes), "vertex save");
+    CGS_CUDA(cudaMemcpyAsync(save_t.p, ctx->cage_verts.p, p.verts_bytes, cudaMemcpyDeviceToDevice, s),
+             "vertex save");
+    CGS_CUDA(cudaMemcpyAsync(ctx->cage_verts.p, p.verts_snap.p, p.verts_bytes,
+                             cudaMemcpyDeviceToDevice, s), "vertex restore");
+  }
+  if (p.mvc_bytes) {
+    CGS_CUDA(cudaMalloc(&save_m.p, p.mvc_bytes), "vertex save");
+    CGS_CUDA(cudaMemcpyAsync(save_m.p, ctx->mvc_verts.p, p.mvc_bytes, cudaMemcpyDeviceToDevice, s),
+             "vertex save");
+    CGS_CUDA(cudaMemcpyAsync(ctx->mvc_verts.p, p.mvc_snap.p, p.mvc_bytes,
+                             cudaMemcpyDeviceToDevice, s), "vertex restore");
+  }
+  cgs_frame_params prm = p.params;
+  prm.force_stage3 = 1;
+  prm.profile_stages = 0;
+  prm.write_f32 = 0;
+  FrameCtl ctl;
+  ctl.allow_cache = false;
+  ctl.force_stage1 = true;
+  ctl.counters = &ctx->h_ring[k];
+  ctl.out_rgba8 = out;
+  ctl.out_pitch = pitch;
+  const bool kp = ctx->kprof;
+  ctx->kprof = false;
+  ctx->cur = -1;
+  int rc = CGS_OK;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    FrameInfo fi;
+    rc = enqueue_frame(ctx, &p.cam, &p.comp, &prm, ctl, &fi);
+    if (rc != CGS_OK) break;
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = ctx->fail(CGS_E_CUDA, "re-render of an earlier frame failed");
+      break;
+    }
+    const FrameCounters& f = ctx->h_ring[k].fc;
+    if (f.status & (kStatusLookbackTimeout | kStatusBarrierTimeout)) {
+      rc = ctx->fail(CGS_E_TIMEOUT, "a bounded device-side wait gave up during a re-render");
+      break;
+    }
+    if (!(f.status & kStatusCapacity) && f.entries <= ctx->entry_cap) break;
+    ctx->entry_cap = (uint32_t)std::min<uint64_t>((uint64_t)f.entries * 13 / 10 + 4096,
+                                                  (uint64_t)kMaxEntryCap);
+    rc = ctx->fail(CGS_E_CAPACITY, "tile entries exceed the largest key buffers");
+  }
+  ctx->kprof = kp;
+  if (p.verts_bytes)
+    cudaMemcpyAsync(ctx->cage_verts.p, save_t.p, p.verts_bytes, cudaMemcpyDeviceToDevice, s);
+  if (p.mvc_bytes)
+    cudaMemcpyAsync(ctx->mvc_verts.p, save_m.p, p.mvc_bytes, cudaMemcpyDeviceToDevice, s);
+  CGS_CUDA(cudaStreamSynchronize(s), "vertex restore");
+  ctx->deformed_valid = false;
+  ctx->s3_valid = false;
+  ctx->arena_rerendered = true;
+  p.overflowed = false;
+  ++ctx->rerun_count;
+  return rc;
+}
+
+}  // namespace
+
 int cgs_readback_wait(cgs_ctx* ctx, uint64_t ticket) {
   if (!ctx) return CGS_E_ARG;
   cgs_ctx::Readback* r = nullptr;
@@ -2457,6 +2561,15 @@ int cgs_readback_wait(cgs_ctx* ctx, uint64_t ticket) {
   // (an entry overflow re-renders the latest frame with grown buffers).
   cgs_ctx::Pending& p = ctx->ring[r->frame_slot];
   if (p.used && p.seq == r->frame_seq) CGS_TRY(check_slot(ctx, r->frame_slot, true));
+  if (p.overflowed && p.seq == r->frame_seq) {
+    // its entries overflowed while a later frame was in flight: render it
+    // again into the snapshot buffer, then copy that
+    CGS_TRY(rerender_slot(ctx, r->frame_slot, r->stage.as<uint32_t>(), r->W));
+    CGS_CUDA(cudaMemcpyAsync(r->dst, r->stage.p, (size_t)r->W * r->H * 4, cudaMemcpyDeviceToHost,
+                             ctx->stream), "framebuffer readback");
+    CGS_CUDA(cudaStreamSynchronize(ctx->stream), "framebuffer readback");
+    return ctx->take_sticky();
+  }
   if (ctx->rerun_count != r->reruns && ctx->rerun_seq == r->frame_seq) {
     // re-rendered after the snapshot: copy again while it is the last frame
     if (ctx->latest_slot < 0 || ctx->ring[ctx->latest_slot].seq != r->frame_seq)
@@ -2556,6 +2669,9 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
                           uint64_t* out_bytes) {
   if (!ctx || !out_bytes) return CGS_E_ARG;
   if (!ctx->frame_done) return ctx->fail(CGS_E_STATE, "no frame rendered");
+  if (ctx->arena_rerendered)
+    return ctx->fail(CGS_E_STATE, "an earlier frame was rendered again since the last frame; "
+                                  "its intermediates replaced the last frame's");
   cudaSetDevice(ctx->device);
   CGS_TRY(drain(ctx, true));
   CGS_CUDA(cudaStreamSynchronize(ctx->stream), "read frame buffer");

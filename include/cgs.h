@@ -396,9 +396,11 @@ int cgs_readback_rgba8(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t heig
  * pixels once cgs_readback_wait(ctx, ticket) has returned CGS_OK. At most
  * two copies are in flight: a third call first waits for the oldest. If the
  * frame overflowed the tile-entry buffers, the wait re-reads it after the
- * library re-renders it, or returns CGS_E_CAPACITY when newer frames have
- * replaced it. No reference counterpart: readback_framebuffer_rgba8
- * (gpu_state.rs:1296-1328) is synchronous. */
+ * library re-renders it with grown buffers; when later frames were already
+ * in flight, the wait renders it again from its stored arguments and cage
+ * vertices (the next frame then deforms and bins afresh, and
+ * cgs_read_frame_buffer refuses until it has run). No reference counterpart:
+ * readback_framebuffer_rgba8 (gpu_state.rs:1296-1328) is synchronous. */
 int cgs_readback_rgba8_async(cgs_ctx* ctx, uint8_t* dst, uint32_t width, uint32_t height,
                              uint64_t* ticket);
 /* Waits for the copy `ticket` of cgs_readback_rgba8_async (a ticket already

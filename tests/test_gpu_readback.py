@@ -74,3 +74,60 @@ def test_third_copy_waits_for_the_oldest(gpu_state):
     with pytest.raises(_abi.CgsError) as e:
         st.readback_framebuffer_rgba8_async(np.empty((h + 1, w, 4), np.uint8))
     assert e.value.code == _abi.CGS_E_ARG
+
+
+def test_overflowed_earlier_frame_is_rendered_again():
+    """A frame whose tile entries outgrow the key buffers while a later frame
+    is already in flight is rendered again, from its own camera and cage
+    vertices, when its asynchronous readback is waited for: the pixels equal
+    a synchronous render of that frame by another context."""
+    from cindergs_b200 import GpuPipelineState, workloads
+    w, h = 1280, 720
+    wl = workloads.tet_cage_orbit(n=40_000, width=w, height=h)
+    wl.scene.covariances_3d[:] *= np.float32(40.0)  # large splats: many entries close up
+    sim = wl.cage.simulator
+    rest = wl.cage.mesh.rest_vertices.copy()
+    rng = np.random.default_rng(3)
+    verts = [(rest + rng.normal(0, 0.04, rest.shape)).astype(np.float32) for _ in range(3)]
+    from cindergs_b200 import CameraUniforms
+    far = CameraUniforms.from_look_at((0.0, 0.5, 40.0), (0, 0, 0), (0, 1, 0), np.deg2rad(60), w, h,
+                                      0.2)
+    near = CameraUniforms.from_look_at((0.0, 0.3, 2.2), (0, 0, 0), (0, 1, 0), np.deg2rad(60), w, h,
+                                       0.2)
+    # the expected pixels of the big frame, from a context sized by it
+    ref = GpuPipelineState(0)
+    try:
+        ref.upload_scene(wl.scene)
+        cages_r = wl.bind(ref)
+        sim.current_positions = verts[1]
+        ref.execute_frame_gpu(wl.scene, cages_r, near, compositor(w, h, near, deg=3),
+                              force_stage3=True)
+        want = ref.readback_framebuffer_rgba8(w, h)
+    finally:
+        ref.close()
+    st = GpuPipelineState(0)
+    try:
+        st.upload_scene(wl.scene)
+        cages = wl.cages  # the bindings made above, uploaded to this context too
+        sim.current_positions = verts[0]
+        t0 = st.execute_frame_gpu(wl.scene, cages, far, compositor(w, h, far, deg=3),
+                                  force_stage3=True)
+        out = torch.empty((h, w, 4), dtype=torch.uint8).pin_memory().numpy()
+        sim.current_positions = verts[1]
+        st.execute_frame_gpu(wl.scene, cages, near, compositor(w, h, near, deg=3),
+                             force_stage3=True, stage_timings=False)
+        ticket = st.readback_framebuffer_rgba8_async(out)
+        sim.current_positions = verts[2]
+        st.execute_frame_gpu(wl.scene, cages, far, compositor(w, h, far, deg=3),
+                             force_stage3=True, stage_timings=False)
+        st.readback_wait(ticket)
+        np.testing.assert_array_equal(out, want)
+        assert want[..., :3].max() > 0
+        # the frame after it renders as usual
+        sim.current_positions = verts[1]
+        st.execute_frame_gpu(wl.scene, cages, near, compositor(w, h, near, deg=3),
+                             force_stage3=True)
+        np.testing.assert_array_equal(st.readback_framebuffer_rgba8(w, h), want)
+        assert t0.total_tile_entries < 1_000_000
+    finally:
+        st.close()
