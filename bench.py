@@ -35,7 +35,7 @@ CUDA graph. One JSON line, 1 GPU.
   python bench.py --workload large [--steps K --warmup W]
 Large-scene workload (6,000,000 Gaussians in the quantized f16 layout, four
 384-tet spring cages over the upper half, the learned polygon cage for the
-rest, 7680x4320 with 64-bit keys, camera orbiting at radius 8): frames/s and
+rest, 7680x4320 with 64-bit keys, camera orbiting at radius 4): frames/s and
 per-stage times. One JSON line, 1 GPU.
 
   python bench.py --workload mvc [--steps K --warmup W]

@@ -152,7 +152,7 @@ def spring_cage(lo, hi, cells: int, rng: np.random.Generator) -> Cage:
 
 
 def large_multicage(n: int = 6_000_000, seed: int = 0, width: int = 7680, height: int = 4320,
-                    frames: int = 30, radius: float = 8.0) -> LargeMultiCageWorkload:
+                    frames: int = 30, radius: float = 4.0) -> LargeMultiCageWorkload:
     """The large-scene workload: Gaussians drawn as in ``random_scene`` and
     scaled into [-1, 1]^3, stored as a QuantizedGaussianSceneSoa (f16
     covariances and SH degree 3); four 4x4x4-cube (384-tet) spring cages over

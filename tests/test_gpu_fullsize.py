@@ -154,7 +154,7 @@ def test_8k_64bit_multicage_subsample(st):
     half, 7680x4320, 129,600 tiles, 64-bit keys) on 400,000 of its Gaussians;
     the quantized layout and the learned polygon cage are checked by their own
     tests."""
-    wl = workloads.large_multicage(n=400_000)
+    wl = workloads.large_multicage(n=400_000, radius=8.0)  # ~29M entries: the oracle's size
     scene = wl.scene.to_soa()
     st.upload_scene(scene)
     cs = CageScene.auto_bind(wl.cages, st, scene.count)
