@@ -109,6 +109,8 @@ def parse():
                     help="tile-entry sort: 0 auto, 1 radix passes, 2 one-pass tile transpose")
     ap.add_argument("--radix-bits", type=int, default=0,
                     help="entry-sort digit width (0 = balanced digits of at most 8 bits)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (a stable launch list for profiling)")
     ap.add_argument("--tile-shape", type=int, default=0,
                     help="screen tile: 0 = 16x16 (the reference's), 1 = 8x8, 2 = 32x16")
     return ap.parse_args()
@@ -292,9 +294,14 @@ def run_ours(args):
     # workload's current frame; every shape renders the same frame.
     from cindergs_b200 import autotune
     cam_t = wl.camera(frame)
-    shape, _ = autotune.tune_launch_shape(st, wl.scene, cages, cam_t, wl.compositor(cam_t),
-                                          radix_bits=args.radix_bits, entry_sort=args.entry_sort,
-                                          tile_shape=args.tile_shape)
+    if args.no_tune:
+        shape = {k: v[0] for k, v in autotune.LAUNCH_CHOICES.items()}
+        st.set_launch_shape(**shape)
+    else:
+        shape, _ = autotune.tune_launch_shape(st, wl.scene, cages, cam_t, wl.compositor(cam_t),
+                                              radix_bits=args.radix_bits,
+                                              entry_sort=args.entry_sort,
+                                              tile_shape=args.tile_shape)
     # Per-stage device times of a few representative frames (not timed).
     stage_rows = [render(profile=True, timings=True) for _ in range(3)]
     st.synchronize()
