@@ -781,6 +781,25 @@ def views_result(args) -> dict:
         graph_ms, graph_wall, gst = timed(lambda: batched(True))
     replays = sum(1 for x in gst if x["graph_replayed"])
     nv = len(cams)
+    # Per-kernel device time and algorithmic HBM bytes of one step of
+    # per-view frames: the step's floor is the sum over kernels of bytes /
+    # the measured copy bandwidth, a bound for any batching of the views.
+    st.kernel_profile_reset()
+    wl.step()
+    for v, (cam, comp) in enumerate(zip(cams, comps)):
+        st.execute_frame_gpu(wl.scene, cages, cam, comp, force_stage3=True, profile_stages=True,
+                             radix_bits=rbs[v], entry_sort=ess[v], tile_shape=tss[v])
+    st.synchronize()
+    hbm = peaks()[0]
+    per_kernel, floor_ms = {}, 0.0
+    for name, k in st.kernel_profile().items():
+        if k["launches"] == 0:
+            continue
+        f = k["alg_bytes"] / (hbm * 1e9) * 1e3
+        floor_ms += f
+        per_kernel[name] = {"ms": k["ms"], "launches": k["launches"],
+                            "alg_bytes": k["alg_bytes"], "hbm_floor_ms": f,
+                            "frac": f / k["ms"] if k["ms"] > 0 else None}
     cpu = None
     if not args.no_cpu_baseline:
         # one 1280x720 view through the restated reference CPU backend
@@ -817,6 +836,9 @@ def views_result(args) -> dict:
                                   "radix_bits": rb, "entry_sort": ["auto", "radix", "transpose"][es],
                                   "stage34_ms": ms} for (w, h), (ts, rb, es, ms) in tuned.items()},
         "tile_entries_per_step": gst[-1]["total_tile_entries"] if gst else None,
+        "per_kernel_one_step": per_kernel,
+        "hbm_floor_ms_per_step": floor_ms,
+        "max_speedup_over_per_view_frames_at_hbm_floor": plain_ms / floor_ms if floor_ms else None,
         "cpu_baseline": cpu,
         "clocks": clock.summary(),
     }

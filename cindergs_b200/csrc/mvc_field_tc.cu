@@ -4,24 +4,30 @@
 // (x' = Pc^T h + pc + A3 x, F = Pc^T dh + A3; k_mvc_jacobian's layout) or the
 // last hidden layer and its tangents as the cached code (bf16 [4][128]).
 //
-// One CTA per SM, two warpgroups; each warpgroup owns a tile of 32 items =
-// 128 rows, stream-major (row 32 s + p: item p, stream s = value, d/dx,
-// d/dy, d/dz), i.e. one M = 128 tcgen05.mma tile in which warp s of the
-// warpgroup reads stream s of every item (tcgen05.ld 32x32b, lane = row).
-// Per layer one elected thread issues the K = 16 steps into the
-// warpgroup's 128-column TMEM accumulator and commits them to an mbarrier;
-// then, 32 columns at a time, the value warp stages the pre-activations in
-// shared memory, each of the four warps evaluates the SiLU and its slope for
-// 8 of the columns of every item, and each warp takes back what its stream
-// needs (the activation, or the slope times its tangent) and writes the
-// bf16 result as the next layer's A operand. The sine/cosine pairs of the
-// Fourier features are likewise computed once per item, 6 of the 24 pairs
-// by each warp. Operands live in shared memory in
-// the K-major, 128-byte-swizzle canonical layout: rows of 64 bf16 (128 B),
-// 8-row atoms of 1024 B, 16-byte chunk c of row r stored at chunk
-// c ^ (r % 8). The output projection is one more MMA with N = 16 against
-// Pc split into three bf16 terms (columns 0-2, 3-5, 6-8), so that the
-// products are exact and only the fp32 accumulation rounds.
+// One CTA per SM, three warpgroups; each warpgroup owns a tile of 32 items
+// = 128 columns n = 4 p + s (item p, stream s = value, d/dx, d/dy, d/dz).
+// A hidden layer is one M = 128, N = 128 product per tile with the weights
+// as A (K-major, as stored) and the activations as B in MN-major order
+// (row k of the operand holds input k of every column), so the accumulator
+// has TMEM lane = hidden unit and column = (item, stream): the thread that
+// owns lane j reads the pre-activation and the three tangents of unit j of
+// an item side by side, evaluates the SiLU and its slope once and scales
+// its own tangents, and writes row j of the next layer's operand -- no
+// exchange between threads and no barrier inside the epilogue. One elected
+// thread per warpgroup issues the K = 16 steps and commits them to the
+// warpgroup's mbarrier; the three warpgroups' products queue on the tensor
+// pipe while the other warpgroups run their epilogues. The output
+// projection takes the same shared-memory tile as an MN-major A operand
+// (M = 128 columns of the tile) against Pc split into three bf16 terms
+// (N = 16: columns 0-2, 3-5, 6-8), so that the products are exact and only
+// the fp32 accumulation rounds; lane n of its accumulator is column n.
+//
+// Shared-memory operands use the 128-byte-swizzle canonical layouts:
+// K-major (weights, Pc): rows of 64 bf16 (128 B), 8-row atoms of 1024 B,
+// 16-byte chunk c of row r stored at chunk c ^ (r % 8); MN-major
+// (activations): 128-byte rows of 64 consecutive columns, one row per input
+// k, 8-row atoms of 1024 B (stride byte offset), the second 64 columns
+// 16 KB further on (leading byte offset), chunk c of row k at c ^ (k % 8).
 //
 // Every mbarrier wait is bounded; a wait that gives up sets the status word
 // and the warpgroup stops issuing work (TMEM is released at the end).
@@ -35,9 +41,12 @@ namespace cgs {
 namespace {
 
 constexpr int kHid = kFieldHid, kIn = kFieldIn;
-constexpr int kTcWG = 2;                 // warpgroups (tiles in flight) per CTA
-constexpr uint32_t kTcCols = 256;        // TMEM columns per warpgroup (128 hidden + 16 proj)
+constexpr int kTcWG = 3;                 // warpgroups (tiles in flight) per CTA
+constexpr uint32_t kTcCols = 128;        // TMEM columns per warpgroup
+constexpr uint32_t kTcAlloc = 512;       // power of two >= kTcWG * kTcCols
 constexpr uint32_t kTcWaitLimit = 1u << 20;
+constexpr uint32_t kItems = 32;          // items per tile
+constexpr uint32_t kMnBlock = 16384;     // bytes between the two 64-column halves of a tile
 
 // shared memory map (bytes from the 1024-aligned base)
 constexpr uint32_t kOffW1 = 0;                        // [128 x 64]   16 KB
@@ -45,14 +54,14 @@ constexpr uint32_t kOffW2 = kOffW1 + 128 * 64 * 2;    // [128 x 128]  32 KB each
 constexpr uint32_t kOffW3 = kOffW2 + 128 * 128 * 2;
 constexpr uint32_t kOffW4 = kOffW3 + 128 * 128 * 2;
 constexpr uint32_t kOffP = kOffW4 + 128 * 128 * 2;    // [16 x 128]   4 KB
-constexpr uint32_t kOffA = kOffP + 16 * 128 * 2;      // [128 x 128] per warpgroup
-constexpr uint32_t kOffBias = kOffA + kTcWG * 128 * 128 * 2;  // 4 x 128 f32
-constexpr uint32_t kChunk = 64;                        // columns per epilogue step
-constexpr uint32_t kXStride = kChunk + 4;                // floats per item row (bank spread)
-constexpr uint32_t kOffX = kOffBias + 4 * 128 * 4;    // per warpgroup: exchange area
-constexpr uint32_t kXBytes = 2 * 32 * kXStride * 4;      //   pre (then act), slope [32 item][68]
-constexpr uint32_t kOffMisc = kOffX + kTcWG * kXBytes;   // pc, A3, mbarriers, tmem
-constexpr uint32_t kTcSmem = kOffMisc + 256 + 1024;      // + alignment slack
+constexpr uint32_t kOffB = kOffP + 16 * 128 * 2;      // activation tile [128 k][128 n] per warpgroup
+constexpr uint32_t kBTile = 128 * 128 * 2;
+constexpr uint32_t kOffBias = kOffB + kTcWG * kBTile;  // 4 x 128 f32
+constexpr uint32_t kOffMisc = kOffBias + 4 * 128 * 4;  // pc, A3, mbarriers, tmem
+constexpr uint32_t kTcSmem = kOffMisc + 256 + 1024;    // + alignment slack
+static_assert(kTcSmem <= 232448, "shared memory per CTA");
+static_assert(kTcWG * kTcCols <= kTcAlloc, "TMEM columns");
+static_assert(kOffB % 1024 == 0 && kBTile % 1024 == 0, "swizzle atoms are 1024-byte aligned");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -65,19 +74,31 @@ __device__ __forceinline__ uint32_t sw_off(uint32_t R, uint32_t r, uint32_t k) {
   return kb * (R * 128) + (r >> 3) * 1024 + (r & 7) * 128 + chunk * 16 + (kk & 7) * 2;
 }
 
-// Shared memory matrix descriptor: K-major, 128-byte swizzle, SBO = 1024 B.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// Byte offset of the 16-byte chunk holding columns 8 c .. 8 c + 7 (c < 16)
+// of row k of an MN-major activation tile.
+__device__ __forceinline__ uint32_t mn_chunk(uint32_t k, uint32_t c) {
+  return (c >> 3) * kMnBlock + (k >> 3) * 1024 + (k & 7) * 128 + (((c & 7) ^ (k & 7)) << 4);
+}
+
+// Shared memory matrix descriptor, 128-byte swizzle: K-major operands
+// (stride byte offset 1024 = next 8-row atom; the leading offset is unused)
+// and MN-major operands (stride byte offset 1024 = next 8 rows of K, leading
+// byte offset = next 64 columns of M or N).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr, uint32_t lbo = 16) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1 << 16;              // leading byte offset (unused for this layout)
-  d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset: next 8-row atom
-  d |= (uint64_t)1 << 46;              // descriptor version
-  d |= (uint64_t)2 << 61;              // 128-byte swizzle
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;  // leading byte offset
+  d |= (uint64_t)(1024 >> 4) << 32;             // stride byte offset
+  d |= (uint64_t)1 << 46;                       // descriptor version
+  d |= (uint64_t)2 << 61;                       // 128-byte swizzle
   return d;
 }
 
-// Instruction descriptor: kind::f16, bf16 A and B (K-major), f32 accumulate.
-__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+// Instruction descriptor: kind::f16, bf16 A and B, f32 accumulate; a_mn / b_mn
+// select MN-major A / B.
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N, uint32_t a_mn,
+                                                  uint32_t b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (a_mn << 15) | (b_mn << 16) | ((N >> 3) << 17) |
+         ((M >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16_tc(uint32_t d_tmem, uint64_t a, uint64_t b,
@@ -120,15 +141,17 @@ __device__ __forceinline__ void tc_fence_before() {
 
 #define CGS_R8(i) "=r"(v[i]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), \
                   "=r"(v[i + 5]), "=r"(v[i + 6]), "=r"(v[i + 7])
-// 32 consecutive TMEM columns of this thread's lane.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// 32 consecutive TMEM columns of this thread's lane into v[O .. O + 31]
+// (no wait: the caller waits once for several loads).
+template <int O, int NV>
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&v)[NV]) {
+  static_assert(O + 32 <= NV, "tmem_ld32 range");
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
       "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
       "%28, %29, %30, %31}, [%32];\n"
-      : CGS_R8(0), CGS_R8(8), CGS_R8(16), CGS_R8(24)
+      : CGS_R8(O), CGS_R8(O + 8), CGS_R8(O + 16), CGS_R8(O + 24)
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile(
@@ -138,11 +161,24 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
 #undef CGS_R8
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ float3 item_position(const FieldInfer& fi, uint32_t k_item) {
+  const uint32_t gi = fi.gauss ? fi.gauss[fi.first + k_item] : fi.first + k_item;
+  if (fi.points4) {
+    const float4 x4 = fi.points4[gi];
+    return make_float3(x4.x, x4.y, x4.z);
+  }
+  return make_float3(fi.points3[3 * (size_t)gi], fi.points3[3 * (size_t)gi + 1],
+                     fi.points3[3 * (size_t)gi + 2]);
 }
 
 template <bool CODES>
@@ -156,11 +192,8 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kOffMisc + 128);
   volatile uint32_t* s_ok = reinterpret_cast<uint32_t*>(sm + kOffMisc + 144);  // [kTcWG]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wg = warp >> 2, r = tid & 127;  // warpgroup, row within its tile
-  const int s_st = warp & 3, p = lane;      // stream (warp in the warpgroup), item (lane)
-  float* X = reinterpret_cast<float*>(sm + kOffX + (uint32_t)wg * kXBytes);
-  float* X_pre = X + p * kXStride;                 // this item's row: pre-activation, then act
-  float* X_slp = X + (32 + p) * kXStride;          // this item's row: SiLU slope
+  const int wg = warp >> 2, q4 = warp & 3;  // warpgroup, warp within it (TMEM lane quarter)
+  const uint32_t j = 32u * (uint32_t)q4 + (uint32_t)lane;  // TMEM lane of this thread
 
   // ---- weights, biases and the projection into shared memory
   auto put_w = [&](uint32_t off, const __nv_bfloat16* W, uint32_t R, uint32_t K) {
@@ -201,7 +234,7 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(s_tmem)),
-                 "r"(kTcCols * kTcWG));
+                 "r"(kTcAlloc));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -210,12 +243,12 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem + (uint32_t)wg * kTcCols;
-  const uint32_t t_row = tmem + ((uint32_t)(warp & 3) * 32u << 16);  // this warp's lanes
+  const uint32_t t_row = tmem + ((uint32_t)q4 * 32u << 16);  // this warp's lanes
   const uint32_t mbar = smem_u32(&s_mbar[wg]);
-  unsigned char* A = sm + kOffA + (uint32_t)wg * 128 * 128 * 2;
-  const uint32_t a_addr = smem_u32(A);
+  unsigned char* Bt = sm + kOffB + (uint32_t)wg * kBTile;
+  const uint32_t b_addr = smem_u32(Bt);
   const uint32_t base_addr = smem_u32(sm);
-  const uint32_t id_h = idesc_bf16(128, 128), id_p = idesc_bf16(128, 16);
+  const uint32_t id_h = idesc_bf16(128, 128, 0, 1), id_p = idesc_bf16(128, 16, 1, 0);
   const bool leader = (tid & 127) == 0;
   uint32_t phase = 0;
   bool ok = true;
@@ -230,72 +263,54 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
     tc_fence_after();
     return ok;
   };
+  // row j of the activation tile: 8 chunks of 16 B per 64-column half
+  unsigned char* rowj = Bt + (j >> 3) * 1024 + (j & 7) * 128;
+  const uint32_t swz = j & 7;
 
-  const uint32_t tiles = (fi.count + 31) / 32;
+  const uint32_t tiles = (fi.count + kItems - 1) / kItems;
   for (uint32_t t = blockIdx.x * kTcWG + wg; t < tiles && ok; t += gridDim.x * kTcWG) {
-    const uint32_t k_item = t * 32 + p;
-    const bool valid = k_item < fi.count;
-    float xr[3] = {0.0f, 0.0f, 0.0f};
-    if (valid) {
-      const uint32_t gi = fi.gauss ? fi.gauss[fi.first + k_item] : fi.first + k_item;
-      if (fi.points4) {
-        const float4 x4 = fi.points4[gi];
-        xr[0] = x4.x;
-        xr[1] = x4.y;
-        xr[2] = x4.z;
-      } else {
-        xr[0] = fi.points3[3 * (size_t)gi];
-        xr[1] = fi.points3[3 * (size_t)gi + 1];
-        xr[2] = fi.points3[3 * (size_t)gi + 2];
-      }
-    }
-    // ---- layer-1 input row: features (value row) or their derivative along
-    // one axis (tangent rows), bf16, K = 64. Pair i = 3 b + d (band b, axis
-    // d): warp w computes pairs 6w .. 6w + 5 of every item.
+    // ---- layer-1 operand: row k = feature k; column 4 p + s = the feature
+    // of item p (s = 0) or its derivative along axis s - 1. Thread (q4, p)
+    // evaluates the sine/cosine pairs i = 6 q4 .. 6 q4 + 5 (band i / 3,
+    // axis i % 3) of item p and rows 4 q4 .. 4 q4 + 3 of {0, 1, 2, 51..63}.
+    // (The previous tile's last product, which read this operand, has
+    // completed: its wait came before.)
     {
+      const uint32_t p = (uint32_t)lane, k_item = t * kItems + p;
+      float3 x3 = make_float3(0.0f, 0.0f, 0.0f);
+      if (k_item < fi.count) x3 = item_position(fi, k_item);
+      if (CODES && q4 == 0 && k_item < fi.count)
+        fi.code_pos[k_item] = make_float4(x3.x, x3.y, x3.z, 0.0f);
       const float inv_s = fi.enc[3];
-      const float xh[3] = {(xr[0] - fi.enc[0]) * inv_s, (xr[1] - fi.enc[1]) * inv_s,
-                           (xr[2] - fi.enc[2]) * inv_s};
-      float* S = X;  // [24 pairs][32 items] x (sin, cos)
-      wg_sync(wg);   // the previous tile's readers of the exchange area are done
+      const float xh[3] = {(x3.x - fi.enc[0]) * inv_s, (x3.y - fi.enc[1]) * inv_s,
+                           (x3.z - fi.enc[2]) * inv_s};
+      // the 8-byte slot of column 4 p in row k
+      auto put4 = [&](uint32_t k, float a, float b, float c, float d) {
+        *reinterpret_cast<uint2*>(Bt + mn_chunk(k, p >> 1) + (p & 1) * 8) =
+            make_uint2(pack2(a, b), pack2(c, d));
+      };
 #pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const int i = 6 * s_st + k, b = i / 3, d = i % 3;
+      for (int kk = 0; kk < 6; ++kk) {
+        const int i = 6 * q4 + kk, b = i / 3, d = i - 3 * b;
         const float w = (float)(1 << b) * 1.57079632679489662f;
         float sn, cs;
         sincosf(w * (d == 0 ? xh[0] : (d == 1 ? xh[1] : xh[2])), &sn, &cs);
-        S[(2 * i) * 32 + p] = sn;
-        S[(2 * i + 1) * 32 + p] = cs;
+        const float ds = w * cs * inv_s, dc = -w * sn * inv_s;
+        const uint32_t ks = 3u + 6u * (uint32_t)b + 2u * (uint32_t)d;
+        put4(ks, sn, d == 0 ? ds : 0.0f, d == 1 ? ds : 0.0f, d == 2 ? ds : 0.0f);
+        put4(ks + 1, cs, d == 0 ? dc : 0.0f, d == 1 ? dc : 0.0f, d == 2 ? dc : 0.0f);
       }
-      wg_sync(wg);
-      const int ax = s_st - 1;  // tangent axis (-1 for the value row)
-#pragma unroll 1
-      for (int c = 0; c < kIn / 8; ++c) {
-        float f8[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int j = c * 8 + e;
-          float f = 0.0f;
-          if (j < 3) {
-            f = s_st == 0 ? xh[j] : (j == ax ? inv_s : 0.0f);
-          } else if (j < 3 + 6 * kFieldBands) {
-            const int q = j - 3, b = q / 6, d = (q % 6) >> 1, i = 3 * b + d;
-            const bool is_cos = q & 1;
-            if (s_st == 0) {
-              f = S[(2 * i + (is_cos ? 1 : 0)) * 32 + p];
-            } else if (d == ax) {
-              const float w = (float)(1 << b) * 1.57079632679489662f;
-              f = is_cos ? -w * S[(2 * i) * 32 + p] * inv_s : w * S[(2 * i + 1) * 32 + p] * inv_s;
-            }
-          }
-          f8[e] = f;
-        }
-        *reinterpret_cast<uint4*>(A + sw_off(128, r, c * 8)) =
-            make_uint4(pack2(f8[0], f8[1]), pack2(f8[2], f8[3]), pack2(f8[4], f8[5]),
-                       pack2(f8[6], f8[7]));
+      for (int kk = 0; kk < 4; ++kk) {
+        const int idx = 4 * q4 + kk;
+        if (idx < 3)
+          put4((uint32_t)idx, xh[idx], idx == 0 ? inv_s : 0.0f, idx == 1 ? inv_s : 0.0f,
+               idx == 2 ? inv_s : 0.0f);
+        else
+          put4((uint32_t)(48 + idx), 0.0f, 0.0f, 0.0f, 0.0f);
       }
     }
-    // ---- four hidden layers
+    // ---- four hidden layers: D[j][n] = sum_k W[j][k] X[k][n]
 #pragma unroll 1
     for (int l = 0; l < 4 && ok; ++l) {
       fence_async_smem();
@@ -307,85 +322,56 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
         const uint32_t K = l == 0 ? kIn : kHid;
         for (uint32_t ks = 0; ks < K / 16; ++ks) {
           const uint32_t kb = ks >> 2, kin = (ks & 3) * 32;
-          mma_bf16_tc(tmem, sw128_desc(a_addr + kb * 16384 + kin),
-                      sw128_desc(base_addr + woff + kb * 16384 + kin), id_h, ks > 0);
+          mma_bf16_tc(tmem, sw128_desc(base_addr + woff + kb * 16384 + kin),
+                      sw128_desc(b_addr + ks * 2048, kMnBlock), id_h, ks > 0);
         }
         mma_commit(mbar);
       }
       if (!wait_mma()) break;
-      const float* bias = s_bias + l * kHid;
+      const float bj = s_bias[l * kHid + j];
       const bool last = l == 3;
 #pragma unroll 1
-      for (int q = 0; q < kHid / (int)kChunk; ++q) {
-        uint32_t v[kChunk];
-        {
-          uint32_t (&v0)[32] = *reinterpret_cast<uint32_t(*)[32]>(&v[0]);
-          uint32_t (&v1)[32] = *reinterpret_cast<uint32_t(*)[32]>(&v[32]);
-          tmem_ld32(t_row + (uint32_t)q * kChunk, v0);
-          tmem_ld32(t_row + (uint32_t)q * kChunk + 32, v1);
+      for (int h = 0; h < 2; ++h) {  // columns 64 h .. 64 h + 63 = items 16 h .. 16 h + 15
+        uint32_t v[64];
+        tmem_ld32_nowait<0>(t_row + (uint32_t)h * 64u, v);
+        tmem_ld32_nowait<32>(t_row + (uint32_t)h * 64u + 32u, v);
+        tmem_wait_ld();
+        uint32_t o[32];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const float pre = __uint_as_float(v[4 * i]) + bj;
+          const float sg = __fdividef(1.0f, 1.0f + __expf(-pre));
+          const float sl = sg * (1.0f + pre * (1.0f - sg));
+          o[2 * i] = pack2(pre * sg, __uint_as_float(v[4 * i + 1]) * sl);
+          o[2 * i + 1] =
+              pack2(__uint_as_float(v[4 * i + 2]) * sl, __uint_as_float(v[4 * i + 3]) * sl);
         }
-        const float* bq = bias + q * kChunk;
-        if (s_st == 0) {
+        if (CODES && last) {
+          // code of an item: [stream][unit] bf16
 #pragma unroll
-          for (int j = 0; j < (int)kChunk; j += 4)
-            *reinterpret_cast<float4*>(X_pre + j) =
-                make_float4(__uint_as_float(v[j]) + bq[j], __uint_as_float(v[j + 1]) + bq[j + 1],
-                            __uint_as_float(v[j + 2]) + bq[j + 2], __uint_as_float(v[j + 3]) + bq[j + 3]);
-        }
-        wg_sync(wg);
-        // SiLU and its slope for columns 16 w .. 16 w + 15 of this item (the
-        // activation replaces the pre-activation)
-#pragma unroll
-        for (int k = 0; k < 16; k += 4) {
-          const int j = 16 * s_st + k;
-          const float4 pre4 = *reinterpret_cast<const float4*>(X_pre + j);
-          const float pr[4] = {pre4.x, pre4.y, pre4.z, pre4.w};
-          float ac[4], sl[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const float sg = __fdividef(1.0f, 1.0f + __expf(-pr[e]));
-            ac[e] = pr[e] * sg;
-            sl[e] = sg * (1.0f + pr[e] * (1.0f - sg));
+          for (int i = 0; i < 16; ++i) {
+            const uint32_t k_item = t * kItems + 16u * (uint32_t)h + (uint32_t)i;
+            if (k_item < fi.count) {
+              unsigned short* dst =
+                  reinterpret_cast<unsigned short*>(fi.codes + (size_t)k_item * (4 * kHid)) + j;
+              dst[0] = (unsigned short)(o[2 * i] & 0xFFFFu);
+              dst[kHid] = (unsigned short)(o[2 * i] >> 16);
+              dst[2 * kHid] = (unsigned short)(o[2 * i + 1] & 0xFFFFu);
+              dst[3 * kHid] = (unsigned short)(o[2 * i + 1] >> 16);
+            }
           }
-          *reinterpret_cast<float4*>(X_pre + j) = make_float4(ac[0], ac[1], ac[2], ac[3]);
-          *reinterpret_cast<float4*>(X_slp + j) = make_float4(sl[0], sl[1], sl[2], sl[3]);
-        }
-        wg_sync(wg);
-        uint32_t outw[kChunk / 2];
-        const float* src = s_st == 0 ? X_pre : X_slp;
+        } else {
+          unsigned char* rp = rowj + (uint32_t)h * kMnBlock;
 #pragma unroll
-        for (int j = 0; j < (int)kChunk; j += 4) {
-          const float4 w4 = *reinterpret_cast<const float4*>(src + j);
-          if (s_st == 0) {
-            outw[j >> 1] = pack2(w4.x, w4.y);
-            outw[(j >> 1) + 1] = pack2(w4.z, w4.w);
-          } else {
-            outw[j >> 1] = pack2(__uint_as_float(v[j]) * w4.x, __uint_as_float(v[j + 1]) * w4.y);
-            outw[(j >> 1) + 1] =
-                pack2(__uint_as_float(v[j + 2]) * w4.z, __uint_as_float(v[j + 3]) * w4.w);
-          }
+          for (int c = 0; c < 8; ++c)
+            *reinterpret_cast<uint4*>(rp + (((uint32_t)c ^ swz) << 4)) =
+                make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
         }
-#pragma unroll
-        for (int c4 = 0; c4 < (int)kChunk / 8; ++c4)
-          *reinterpret_cast<uint4*>(A + sw_off(128, r, q * kChunk + c4 * 8)) =
-              make_uint4(outw[4 * c4], outw[4 * c4 + 1], outw[4 * c4 + 2], outw[4 * c4 + 3]);
-        if (CODES && last && valid) {
-          uint4* dst = reinterpret_cast<uint4*>(fi.codes + (size_t)k_item * (4 * kHid) +
-                                                s_st * kHid + q * kChunk);
-#pragma unroll
-          for (int c4 = 0; c4 < (int)kChunk / 8; ++c4)
-            dst[c4] = make_uint4(outw[4 * c4], outw[4 * c4 + 1], outw[4 * c4 + 2], outw[4 * c4 + 3]);
-        }
-        // (the next chunk's first writes come after every warp passed this
-        // chunk's second barrier, i.e. after all reads of the pre-activations)
       }
     }
     if (!ok) break;
-    if (CODES) {
-      if (valid && s_st == 0) fi.code_pos[k_item] = make_float4(xr[0], xr[1], xr[2], 0.0f);
-      continue;
-    }
-    // ---- output projection: N = 16 against the split Pc
+    if (CODES) continue;
+    // ---- output projection: D[n][c] = sum_k X[k][n] Pc'[c][k], N = 16
     fence_async_smem();
     tc_fence_before();
     wg_sync(wg);
@@ -393,25 +379,34 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
       tc_fence_after();
       for (uint32_t ks = 0; ks < kHid / 16; ++ks) {
         const uint32_t kb = ks >> 2, kin = (ks & 3) * 32;
-        mma_bf16_tc(tmem + kHid, sw128_desc(a_addr + kb * 16384 + kin),
+        mma_bf16_tc(tmem, sw128_desc(b_addr + ks * 2048, kMnBlock),
                     sw128_desc(base_addr + kOffP + kb * 2048 + kin), id_p, ks > 0);
       }
       mma_commit(mbar);
     }
     if (!wait_mma()) break;
     uint32_t v[16];
-    tmem_ld16(t_row + kHid, v);
-    if (valid) {
+    tmem_ld16(t_row, v);
+    const uint32_t k_item = t * kItems + (j >> 2), s_st = j & 3;
+    if (k_item < fi.count) {
       float* out = reinterpret_cast<float*>(fi.xf) + 12 * (size_t)(fi.out_first + k_item);
       const float* pc = s_misc;
       const float* A3 = s_misc + 3;
+      if (s_st == 0) {
+        const float3 x3 = item_position(fi, k_item);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float y = (__uint_as_float(v[c]) + __uint_as_float(v[3 + c])) + __uint_as_float(v[6 + c]);
-        if (s_st == 0)
-          out[c] = y + pc[c] + (A3[3 * c] * xr[0] + A3[3 * c + 1] * xr[1] + A3[3 * c + 2] * xr[2]);
-        else
+        for (int c = 0; c < 3; ++c) {
+          const float y =
+              (__uint_as_float(v[c]) + __uint_as_float(v[3 + c])) + __uint_as_float(v[6 + c]);
+          out[c] = y + pc[c] + (A3[3 * c] * x3.x + A3[3 * c + 1] * x3.y + A3[3 * c + 2] * x3.z);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float y =
+              (__uint_as_float(v[c]) + __uint_as_float(v[3 + c])) + __uint_as_float(v[6 + c]);
           out[3 + 3 * (s_st - 1) + c] = y + A3[3 * c + (s_st - 1)];
+        }
       }
     }
   }
@@ -427,7 +422,7 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   tc_fence_after();
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*s_tmem),
-                 "r"(kTcCols * kTcWG));
+                 "r"(kTcAlloc));
   }
 }
 
@@ -441,8 +436,15 @@ cudaError_t launch_field_infer_tc(const FieldInfer& fi, cudaStream_t s) {
                : cudaFuncSetAttribute(k_field_infer_tc<false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
   if (e != cudaSuccess) return e;
-  const uint32_t tiles = (fi.count + 31) / 32;
-  const uint32_t blocks = std::min<uint32_t>(148u, (tiles + kTcWG - 1) / kTcWG);
+  static int sm_count = 0;
+  if (sm_count == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sm_count = 148;
+  }
+  const uint32_t tiles = (fi.count + kItems - 1) / kItems;
+  const uint32_t blocks = std::min<uint32_t>((uint32_t)sm_count, (tiles + kTcWG - 1) / kTcWG);
   if (fi.codes)
     k_field_infer_tc<true><<<blocks, kTcWG * 128, kTcSmem, s>>>(fi);
   else
