@@ -12,7 +12,9 @@ checked against the oracle (v2 mode) at full size.
 * one mixed-resolution step of cgs_execute_views (640x360, 1280x720,
   1920x1080), each view against the oracle;
 * a 7680x4320 frame (129,600 tiles, 64-bit keys) of the large multi-cage
-  scene on a Gaussian subsample, with its four spring-driven tet cages.
+  scene on a Gaussian subsample, with its four spring-driven tet cages;
+* the 3M-Gaussian polygon-cage (MVC) frame: exact stored bindings against the
+  oracle on a sample, the learned field against the exact frame.
 """
 import numpy as np
 import pytest
@@ -170,3 +172,70 @@ def test_8k_64bit_multicage_subsample(st):
     assert t.total_tile_entries == o["entries"] > 1_000_000
     assert_stage23_exact(g, o, key64=True)
     assert float(np.abs(img - o["rgba_f32"]).max()) <= RGB_TOL
+
+
+def test_mvc_polygon_cage_full_size(st):
+    """The polygon-cage workload at its benchmark size: 3,000,000 Gaussians in
+    the unit ball, the 642-vertex displaced icosphere cage, 1920x1080.
+    Exact stored bindings: the deformed means and covariances of a
+    10,000-Gaussian sample against the oracle's deform_scene_cpu restatement
+    with the oracle's own bindings (its weights agree with the GPU's to 5e-5,
+    so the comparison is statistical). Learned field, trained as the
+    benchmark trains it: the error of its frame against the exact frame, and
+    the per-frame network against the cached codes on the same frame."""
+    import torch
+    n = 3_000_000
+    wl = workloads.mvc_cage_sphere(n=n)
+    st.upload_scene(wl.scene)
+    st.upload_cages(None)
+    st.mvc_cage_upload(wl.cage)
+    assert st.mvc_bind() > 0
+    verts = wl.vertices(1)
+    cam = wl.camera(1)
+    comp = wl.compositor(cam)
+
+    def frame():
+        st.mvc_vertices_update(verts)
+        st.execute_frame_gpu(wl.scene, None, cam, comp, 0.0, 0.0, force_stage3=True)
+        pos = st.read_buffer(_abi.BUF_DEFORMED_POS, np.float32).reshape(-1, 3)[:n].copy()
+        cov = st.read_buffer(_abi.BUF_DEFORMED_COV, np.float32).reshape(-1, 6)[:n].copy()
+        return pos, cov
+
+    pos_e, cov_e = frame()
+    sidx = np.sort(np.random.default_rng(3).choice(n, 10_000, replace=False))
+    inside, wg = oracle.mvc_bind(wl.scene.positions[sidx], wl.cage.rest_vertices,
+                                 wl.cage.triangles)
+    o = oracle.mvc_deform(wl.scene.positions[sidx], wl.scene.covariances_3d[sidx],
+                          wl.scene.opacities[sidx], inside, wg, verts)
+    m = len(sidx)
+    dp = np.linalg.norm(pos_e[sidx].astype(np.float64) - o["pos"][:m], axis=1)
+    print(f"\nexact MVC at 3M vs oracle (10k sample): position mean {dp.mean():.2e} "
+          f"p99.9 {np.quantile(dp, 0.999):.2e} max {dp.max():.2e}")
+    assert dp.mean() < 1e-5 and np.quantile(dp, 0.999) < 1e-4 and dp.max() < 1e-3
+    out = ~inside.astype(bool)
+    np.testing.assert_array_equal(pos_e[sidx][out], wl.scene.positions[sidx][out])
+    scale = np.abs(o["cov"][:m]).max(axis=1) + 1e-30
+    dc = np.abs(cov_e[sidx].astype(np.float64) - o["cov"][:m]).max(axis=1) / scale
+    assert dc.mean() < 1e-4 and np.quantile(dc, 0.999) < 1e-2, (dc.mean(), dc.max())
+
+    pts = torch.from_numpy(wl.training_points(2_000_000)).to("cuda:0")
+    w = st.mvc_weights(pts)
+    st.mvc_field_create(seed=1)
+    st.mvc_field_train(pts, w, steps=6000, batch=4096, lr=2e-3, lam=0.05, seed=5)
+    del w, pts
+    torch.cuda.empty_cache()
+    _, _, enc = st.mvc_field_layout()
+    s = 1.0 / float(enc[3])
+    sample = wl.scene.positions[np.random.default_rng(7).choice(n, 200_000, replace=False)]
+    raw, _ = st.mvc_field_infer(sample, rest=True)
+    thr = float(np.quantile(np.linalg.norm(raw - sample, axis=1) / s, 0.99))
+    st.mvc_bind_learned(thr, per_frame=True)
+    pos_pf, _ = frame()
+    st.mvc_bind_learned(thr)
+    pos_l, _ = frame()
+    mode = np.linalg.norm(pos_l.astype(np.float64) - pos_pf, axis=1) / s
+    err = np.linalg.norm(pos_l.astype(np.float64) - pos_e, axis=1) / s
+    print(f"learned at 3M: error vs exact mean {err.mean():.2e} p99 {np.quantile(err, 0.99):.2e} "
+          f"max {err.max():.2e} (of s); per-frame network vs codes max {mode.max():.2e}")
+    assert mode.max() < 1e-6
+    assert err.mean() < 1e-3 and np.quantile(err, 0.99) < 4e-3
