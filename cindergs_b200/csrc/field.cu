@@ -176,6 +176,7 @@ cudaError_t FieldState::ensure_batch(uint32_t B) {
   FIELD_TRY(dpreb.ensure(b * H * 2));
   FIELD_TRY(dpreT.ensure(H * b * 2));
   FIELD_TRY(dh.ensure(b * H * 4));
+  FIELD_TRY(gemm_ws.ensure((size_t)16 * std::max<uint32_t>(ldV, kFieldHid) * H * 4));
   Bcap = B;
   return cudaSuccess;
 }
@@ -202,6 +203,7 @@ cudaError_t FieldState::forward(const float* points, const float* target, uint32
   const float* bias[4] = {nt.b1, nt.b2, nt.b3, nt.b4};
   for (int l = 0; l < 4; ++l) {
     GemmArgs g{};
+    g.status = status.as<uint32_t>();
     g.A = l == 0 ? a0.as<__nv_bfloat16>() : h[l - 1].as<__nv_bfloat16>();
     g.lda = g.K = l == 0 ? kFieldIn : kFieldHid;
     g.B = W[l];
@@ -216,6 +218,7 @@ cudaError_t FieldState::forward(const float* points, const float* target, uint32
     FIELD_TRY(launch_gemm_nt(g, kEpiBiasSilu, s));
   }
   GemmArgs g{};
+  g.status = status.as<uint32_t>();
   g.A = h[3].as<__nv_bfloat16>();
   g.lda = g.K = kFieldHid;
   g.B = nt.W5b;
@@ -255,6 +258,9 @@ cudaError_t FieldState::backward(uint32_t B, cudaStream_t s) {
   FIELD_TRY(launch_transpose_bf16(h[3].as<__nv_bfloat16>(), B, kFieldHid, kFieldHid,
                                   hT.as<__nv_bfloat16>(), B, s));
   GemmArgs gw{};
+  gw.status = status.as<uint32_t>();
+  gw.ws = gemm_ws.as<float>();
+  gw.ws_floats = gemm_ws.cap / 4;
   gw.A = dzT.as<__nv_bfloat16>();
   gw.lda = B;
   gw.B = hT.as<__nv_bfloat16>();
@@ -268,6 +274,7 @@ cudaError_t FieldState::backward(uint32_t B, cudaStream_t s) {
   FIELD_TRY(launch_colsum(dz.as<float>(), B, V, ldV, g + off[kB5], s));
   FIELD_TRY(launch_transpose_bf16(nt.W5b, V, kFieldHid, kFieldHid, wTb, ldV, s));
   GemmArgs gd{};
+  gd.status = status.as<uint32_t>();
   gd.A = dzb.as<__nv_bfloat16>();
   gd.lda = ldV;
   gd.B = wTb;
@@ -289,6 +296,9 @@ cudaError_t FieldState::backward(uint32_t B, cudaStream_t s) {
     const __nv_bfloat16* in = l == 0 ? a0.as<__nv_bfloat16>() : h[l - 1].as<__nv_bfloat16>();
     FIELD_TRY(launch_transpose_bf16(in, B, kin, kin, hT.as<__nv_bfloat16>(), B, s));
     GemmArgs gl{};
+    gl.status = status.as<uint32_t>();
+    gl.ws = gemm_ws.as<float>();
+    gl.ws_floats = gemm_ws.cap / 4;
     gl.A = dpreT.as<__nv_bfloat16>();
     gl.lda = B;
     gl.B = hT.as<__nv_bfloat16>();
@@ -303,6 +313,7 @@ cudaError_t FieldState::backward(uint32_t B, cudaStream_t s) {
     if (l > 0) {
       FIELD_TRY(launch_transpose_bf16(Wl[l], kFieldHid, kFieldHid, kFieldHid, wTb, kFieldHid, s));
       GemmArgs gh{};
+      gh.status = status.as<uint32_t>();
       gh.A = dpreb.as<__nv_bfloat16>();
       gh.lda = kFieldHid;
       gh.B = wTb;

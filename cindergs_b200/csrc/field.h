@@ -40,6 +40,7 @@ struct FieldState {
   // training batch (B rows)
   uint32_t Bcap = 0;
   FieldBuf x, wt, a0, pre[4], h[4], z, dz, dzb, dzT, hT, dpre, dpreb, dpreT, dh;
+  FieldBuf gemm_ws;  // split-K partial sums of the weight gradients (K = batch)
 
   uint32_t total() const { return off[kFieldParams]; }
   // New network for a cage of V vertices with the given rest vertices [V*4]

@@ -92,7 +92,7 @@ struct FieldNet {  // device pointers into one parameter block
   const __nv_bfloat16 *W1b, *W2b, *W3b, *W4b, *W5b;
   const float *b1, *b2, *b3, *b4, *b5;
 };
-struct GemmArgs {  // C = A B^T (+ bias), D = bf16(silu(C))
+struct GemmArgs {  // C = A B^T (+ bias), D = bf16(silu(C)); tcgen05 (mvc_field_tc.cu)
   const __nv_bfloat16* A;
   const __nv_bfloat16* B;
   uint32_t M, N, K, lda, ldb;
@@ -101,6 +101,9 @@ struct GemmArgs {  // C = A B^T (+ bias), D = bf16(silu(C))
   const float* bias;
   __nv_bfloat16* D;
   uint32_t ldd;
+  uint32_t* status;      // kStatusBarrierTimeout / kStatusPoisoned on a failed wait, or null
+  float* ws;             // split-K partial sums (F32 epilogue), or null: no split
+  size_t ws_floats;
 };
 struct FieldBatch {
   const float* points;   // [n*3]

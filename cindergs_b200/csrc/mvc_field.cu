@@ -43,18 +43,7 @@ namespace {
 constexpr int kIn = kFieldIn;    // 64 features
 constexpr int kHid = kFieldHid;  // 128
 
-// D += A B, m16n8k16, A row-major, B column-major, bf16 in, fp32 accumulate.
-__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
 __device__ __forceinline__ float sigmoid_fast(float x) { return 1.0f / (1.0f + __expf(-x)); }
-__device__ __forceinline__ float silu(float x) { return x * sigmoid_fast(x); }
 __device__ __forceinline__ float silu_grad(float x) {
   const float s = sigmoid_fast(x);
   return s * (1.0f + x * (1.0f - s));
@@ -115,100 +104,6 @@ __global__ void k_field_gather(FieldBatch fb) {
     feature(j, xh, fb.enc[3], f, df);
     fb.a0[(size_t)r * kIn + j] = __float2bfloat16_rn(f);
   }
-}
-
-// C = A * B^T: A [M x K] bf16 (lda), B [N x K] bf16 (ldb), fp32 accumulate.
-// 64 x 64 tiles, 4 warps of 32 x 32, K in steps of 32 through shared memory
-// (rows padded by 8 bf16, so the fragment loads hit distinct banks).
-// lda, ldb multiples of 8 and 16-byte-aligned rows; edges zero-filled.
-constexpr int kBM = 64, kBN = 64, kBK = 32, kPad = 8;
-
-template <int EPI>
-__global__ void __launch_bounds__(128) k_gemm_nt(GemmArgs g) {
-  __shared__ __align__(16) __nv_bfloat16 As[kBM][kBK + kPad];
-  __shared__ __align__(16) __nv_bfloat16 Bs[kBN][kBK + kPad];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int gq = lane >> 2, tq = lane & 3;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const uint32_t m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.0f;
-  for (uint32_t k0 = 0; k0 < g.K; k0 += kBK) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int c = tid * 2 + h;  // 16-byte chunk 0..255
-      const int row = c >> 2, col = (c & 3) * 8;
-      const uint32_t ka = k0 + col;
-      uint4 va = make_uint4(0, 0, 0, 0), vb = make_uint4(0, 0, 0, 0);
-      if (m0 + row < g.M) {
-        const __nv_bfloat16* p = g.A + (size_t)(m0 + row) * g.lda + ka;
-        if (ka + 8 <= g.K) {
-          va = *reinterpret_cast<const uint4*>(p);
-        } else {
-          __align__(16) __nv_bfloat16 t[8];
-          for (int e = 0; e < 8; ++e) t[e] = ka + e < g.K ? p[e] : __float2bfloat16_rn(0.0f);
-          va = *reinterpret_cast<const uint4*>(t);
-        }
-      }
-      if (n0 + row < g.N) {
-        const __nv_bfloat16* p = g.B + (size_t)(n0 + row) * g.ldb + ka;
-        if (ka + 8 <= g.K) {
-          vb = *reinterpret_cast<const uint4*>(p);
-        } else {
-          __align__(16) __nv_bfloat16 t[8];
-          for (int e = 0; e < 8; ++e) t[e] = ka + e < g.K ? p[e] : __float2bfloat16_rn(0.0f);
-          vb = *reinterpret_cast<const uint4*>(t);
-        }
-      }
-      *reinterpret_cast<uint4*>(&As[row][col]) = va;
-      *reinterpret_cast<uint4*>(&Bs[row][col]) = vb;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 16) {
-      uint32_t af[2][4];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm + i * 16 + gq;
-        af[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * tq]);
-        af[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * tq]);
-        af[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 8 + 2 * tq]);
-        af[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 8 + 2 * tq]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int n = wn + j * 8 + gq;
-        const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 2 * tq]);
-        const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 8 + 2 * tq]);
-#pragma unroll
-        for (int i = 0; i < 2; ++i) mma_bf16(acc[i][j], af[i], b0, b1);
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const uint32_t row = m0 + wm + i * 16 + gq + h * 8;
-        if (row >= g.M) continue;
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const uint32_t col = n0 + wn + j * 8 + 2 * tq + e;
-          if (col >= g.N) continue;
-          float v = acc[i][j][2 * h + e];
-          if (EPI != kEpiF32) v += g.bias[col];
-          g.C[(size_t)row * g.ldc + col] = v;
-          if (EPI == kEpiBiasSilu) g.D[(size_t)row * g.ldd + col] = __float2bfloat16_rn(silu(v));
-        }
-      }
 }
 
 // out [C x R] bf16 = transpose of in [R x C] (fp32 or bf16).
@@ -691,19 +586,6 @@ __global__ void __launch_bounds__(kApWarps * 32, 1) k_field_apply(FieldInfer fi)
 cudaError_t launch_field_gather(const FieldBatch& b, cudaStream_t s) {
   if (b.B == 0) return cudaSuccess;
   k_field_gather<<<b.B, 128, 0, s>>>(b);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_gemm_nt(const GemmArgs& g, int epi, cudaStream_t s) {
-  if (g.M == 0 || g.N == 0) return cudaSuccess;
-  if ((g.lda & 7) || (g.ldb & 7)) return cudaErrorInvalidValue;
-  const dim3 grid((g.N + kBN - 1) / kBN, (g.M + kBM - 1) / kBM);
-  if (epi == kEpiF32)
-    k_gemm_nt<kEpiF32><<<grid, 128, 0, s>>>(g);
-  else if (epi == kEpiBias)
-    k_gemm_nt<kEpiBias><<<grid, 128, 0, s>>>(g);
-  else
-    k_gemm_nt<kEpiBiasSilu><<<grid, 128, 0, s>>>(g);
   return cudaGetLastError();
 }
 

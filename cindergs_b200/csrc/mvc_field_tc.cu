@@ -426,6 +426,215 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
   }
 }
 
+// ---- training GEMMs: C = A B^T (+ bias), D = bf16(silu(C)) -------------------
+// One CTA of 128 threads per 128 x 128 output tile. K is consumed in 64-wide
+// blocks through a 4-stage ring: every thread copies its share of a block's
+// A and B rows into shared memory with 16-byte cp.async (rows past M or N and
+// columns past K zero-filled) in the K-major 128-byte-swizzle layout, one
+// elected thread issues the block's four K = 16 tcgen05 MMAs into a 128-column
+// TMEM accumulator and commits them to the stage's mbarrier, and the copies
+// run two blocks ahead of the MMAs; a stage is refilled once the MMAs that
+// read it have completed. The epilogue reads the accumulator row by row
+// (TMEM lane = output row) and applies the bias and SiLU.
+constexpr uint32_t kGmTile = 128, kGmBK = 64, kGmStages = 4, kGmAhead = 2;
+constexpr uint32_t kGmStageBytes = 2 * kGmTile * kGmBK * 2;   // A and B, 32 KB
+constexpr uint32_t kGmSmem = kGmStages * kGmStageBytes + 256 + 1024;
+
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr uint32_t kGmMaxSplits = 16;
+
+// C[r][c] = sum over splits z (in order) of ws[z][r][c].
+__global__ void k_split_reduce(const float* __restrict__ ws, uint32_t splits, uint32_t M,
+                               uint32_t N, float* __restrict__ C, uint32_t ldc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M * N) return;
+  float acc = 0.0f;
+  for (uint32_t z = 0; z < splits; ++z) acc += ws[(size_t)z * M * N + i];
+  C[(size_t)(i / N) * ldc + i % N] = acc;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(GemmArgs g) {
+  extern __shared__ unsigned char gm_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(gm_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* s_bar = reinterpret_cast<uint64_t*>(sm + kGmStages * kGmStageBytes);  // [stages]
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_bar + kGmStages);
+  volatile uint32_t* s_ok = s_tmem + 1;  // [2], alternating by block
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t m0 = blockIdx.y * kGmTile, n0 = blockIdx.x * kGmTile;
+  // split z of K: blocks [kb0, kb0 + nk) of the K range
+  const uint32_t nkb = (g.K + kGmBK - 1) / kGmBK, per = (nkb + gridDim.z - 1) / gridDim.z;
+  const uint32_t kb0 = min(nkb, blockIdx.z * per), nk = min(nkb, kb0 + per) - kb0;
+  const bool split = gridDim.z > 1;
+  if (tid < (int)kGmStages)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s_bar[tid])));
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(s_tmem)),
+                 "r"(kGmTile));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const uint32_t base = smem_u32(sm);
+  const uint32_t idesc = idesc_bf16(kGmTile, kGmTile, 0, 0);
+
+  // block kb of A rows m0.. and B rows n0.. into stage kb % stages
+  auto load = [&](uint32_t kb) {
+    const uint32_t st = base + (kb % kGmStages) * kGmStageBytes, k0 = (kb0 + kb) * kGmBK;
+#pragma unroll 4
+    for (uint32_t c = (uint32_t)tid; c < 2 * kGmTile * 8; c += 128) {
+      const bool isb = c >= kGmTile * 8;
+      const uint32_t cc = isb ? c - kGmTile * 8 : c, row = cc >> 3, ch = cc & 7;
+      const uint32_t grow = (isb ? n0 : m0) + row, R = isb ? g.N : g.M, k = k0 + ch * 8;
+      const __nv_bfloat16* mat = isb ? g.B : g.A;
+      const void* src = mat;
+      uint32_t bytes = 0;
+      if (grow < R && k < g.K) {
+        bytes = min(8u, g.K - k) * 2u;
+        src = mat + (size_t)grow * (isb ? g.ldb : g.lda) + k;
+      }
+      cp_async16_zfill(st + (isb ? kGmTile * 128 : 0) + (row >> 3) * 1024 + (row & 7) * 128 +
+                           ((ch ^ (row & 7)) << 4),
+                       src, bytes);
+    }
+  };
+#pragma unroll
+  for (uint32_t p = 0; p < kGmAhead; ++p) {
+    if (p < nk) load(p);
+    cp_async_commit();
+  }
+  bool ok = true;
+  uint32_t issued = 0;  // blocks whose MMAs were issued (block-uniform)
+  for (uint32_t kb = 0; kb < nk; ++kb) {
+    cp_async_wait<kGmAhead - 1>();  // this thread's copies of block kb have landed
+    fence_async_smem();
+    // the stage refilled below was read by the MMAs of block kb - ahead
+    if (tid == 0 && kb >= kGmAhead) {
+      const uint32_t q = kb - kGmAhead;
+      s_ok[kb & 1u] = mbar_wait(smem_u32(&s_bar[q % kGmStages]), (q / kGmStages) & 1u) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (kb >= kGmAhead && s_ok[kb & 1u] == 0u) {
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a = base + (kb % kGmStages) * kGmStageBytes, b = a + kGmTile * 128;
+#pragma unroll
+      for (uint32_t k16 = 0; k16 < kGmBK / 16; ++k16)
+        mma_bf16_tc(tmem, sw128_desc(a + k16 * 32), sw128_desc(b + k16 * 32), idesc,
+                    (kb > 0 || k16 > 0) ? 1u : 0u);
+      mma_commit(smem_u32(&s_bar[kb % kGmStages]));
+    }
+    issued = kb + 1;
+    if (kb + kGmAhead < nk) load(kb + kGmAhead);
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  // the last commit covers every MMA issued before it
+  if (tid == 0) {
+    bool done = true;
+    if (issued > 0) {
+      const uint32_t q = issued - 1;
+      done = mbar_wait(smem_u32(&s_bar[q % kGmStages]), (q / kGmStages) & 1u);
+    }
+    s_ok[0] = (ok && done) ? 1u : 0u;
+    if ((!ok || !done) && g.status) {
+      atomicOr(g.status, kStatusBarrierTimeout);
+      // MMAs still running may write tensor memory after its release below
+      if (!done) atomicOr(g.status, kStatusPoisoned);
+    }
+  }
+  __syncthreads();
+  ok = s_ok[0] != 0u;
+  tc_fence_after();
+  if (ok) {
+    const uint32_t row = m0 + 32u * (uint32_t)warp + (uint32_t)lane;
+    const uint32_t t_row = tmem + ((uint32_t)warp * 32u << 16);
+    const bool vec_c = ((g.ldc & 3u) == 0u) && (((uintptr_t)g.C & 15u) == 0u);
+    const bool vec_d = ((g.ldd & 7u) == 0u) && (((uintptr_t)g.D & 15u) == 0u);
+#pragma unroll 1
+    for (uint32_t c0 = 0; c0 < kGmTile; c0 += 32) {
+      uint32_t v[32];
+      if (nk > 0) {
+        tmem_ld32_nowait<0>(t_row + c0, v);  // every lane of the warp loads (aligned)
+        tmem_wait_ld();
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = 0u;
+      }
+      const uint32_t col0 = n0 + c0;
+      if (row >= g.M || col0 >= g.N) continue;
+      float x[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        x[i] = __uint_as_float(v[i]);
+        if (EPI != kEpiF32 && col0 + i < g.N) x[i] += g.bias[col0 + i];
+      }
+      // a split's partial sums go to its slice of the workspace ([M][N] each)
+      float* crow = split ? g.ws + ((size_t)blockIdx.z * g.M + row) * g.N + col0
+                          : g.C + (size_t)row * g.ldc + col0;
+      if (split) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col0 + i < g.N) crow[i] = x[i];
+        continue;
+      }
+      if (vec_c && col0 + 32 <= g.N) {
+#pragma unroll
+        for (int i = 0; i < 32; i += 4)
+          *reinterpret_cast<float4*>(crow + i) = make_float4(x[i], x[i + 1], x[i + 2], x[i + 3]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col0 + i < g.N) crow[i] = x[i];
+      }
+      if (EPI == kEpiBiasSilu) {
+        __nv_bfloat16* drow = g.D + (size_t)row * g.ldd + col0;
+        if (vec_d && col0 + 32 <= g.N) {
+#pragma unroll
+          for (int i = 0; i < 32; i += 8) {
+            uint32_t w[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float a0 = x[i + 2 * e], a1 = x[i + 2 * e + 1];
+              w[e] = pack2(a0 * (1.0f / (1.0f + __expf(-a0))), a1 * (1.0f / (1.0f + __expf(-a1))));
+            }
+            *reinterpret_cast<uint4*>(drow + i) = make_uint4(w[0], w[1], w[2], w[3]);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (col0 + i < g.N) drow[i] = __float2bfloat16_rn(x[i] * (1.0f / (1.0f + __expf(-x[i]))));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(kGmTile));
+}
+
 }  // namespace
 
 cudaError_t launch_field_infer_tc(const FieldInfer& fi, cudaStream_t s) {
@@ -450,6 +659,50 @@ cudaError_t launch_field_infer_tc(const FieldInfer& fi, cudaStream_t s) {
   else
     k_field_infer_tc<false><<<blocks, kTcWG * 128, kTcSmem, s>>>(fi);
   return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_nt(const GemmArgs& g, int epi, cudaStream_t s) {
+  if (g.M == 0 || g.N == 0) return cudaSuccess;
+  if ((g.lda & 7) || (g.ldb & 7)) return cudaErrorInvalidValue;
+  if (((uintptr_t)g.A & 15) || ((uintptr_t)g.B & 15)) return cudaErrorInvalidValue;
+  static int sm_count = 0;
+  if (sm_count == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sm_count = 148;
+  }
+  dim3 grid((g.N + kGmTile - 1) / kGmTile, (g.M + kGmTile - 1) / kGmTile, 1);
+  // Long K over few tiles (the weight gradients: K = the batch): split K so
+  // that the grid covers the SMs; the partial sums are added in split order
+  // (deterministic) by k_split_reduce.
+  const uint32_t tiles = grid.x * grid.y, nkb = (g.K + kGmBK - 1) / kGmBK;
+  if (epi == kEpiF32 && g.ws && tiles * 2 <= (uint32_t)sm_count && nkb >= 8) {
+    uint32_t z = std::min<uint32_t>({(uint32_t)sm_count / tiles, nkb / 4, kGmMaxSplits});
+    while (z > 1 && (size_t)z * g.M * g.N > g.ws_floats) --z;
+    grid.z = std::max<uint32_t>(1, z);
+  }
+  cudaError_t e;
+  if (epi == kEpiF32) {
+    e = cudaFuncSetAttribute(k_gemm_tc<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kGmSmem);
+    if (e == cudaSuccess) k_gemm_tc<kEpiF32><<<grid, 128, kGmSmem, s>>>(g);
+    if (e == cudaSuccess && grid.z > 1) {
+      e = cudaGetLastError();
+      const uint32_t n = g.M * g.N;
+      if (e == cudaSuccess)
+        k_split_reduce<<<(n + 255) / 256, 256, 0, s>>>(g.ws, grid.z, g.M, g.N, g.C, g.ldc);
+    }
+  } else if (epi == kEpiBias) {
+    e = cudaFuncSetAttribute(k_gemm_tc<kEpiBias>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kGmSmem);
+    if (e == cudaSuccess) k_gemm_tc<kEpiBias><<<grid, 128, kGmSmem, s>>>(g);
+  } else {
+    e = cudaFuncSetAttribute(k_gemm_tc<kEpiBiasSilu>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGmSmem);
+    if (e == cudaSuccess) k_gemm_tc<kEpiBiasSilu><<<grid, 128, kGmSmem, s>>>(g);
+  }
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace cgs

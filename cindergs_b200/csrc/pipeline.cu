@@ -1469,6 +1469,19 @@ int cgs_mvc_field_params(cgs_ctx* ctx, float* dst, const float* src) {
   return CGS_OK;
 }
 
+// Waits for the field's stream and turns its status word into the call's
+// result: a bounded wait for the tensor cores gave up (CGS_E_TIMEOUT), and if
+// MMAs may still have been running when their tensor memory was released,
+// the context is unusable from then on.
+static int field_status(cgs_ctx* ctx, const char* what) {
+  uint32_t fst = 0;
+  CGS_CUDA(cudaMemcpyAsync(&fst, ctx->field.status.p, 4, cudaMemcpyDeviceToHost, ctx->stream), what);
+  CGS_CUDA(cudaStreamSynchronize(ctx->stream), what);
+  if (fst & kStatusPoisoned) ctx->poisoned = true;
+  if (fst) return ctx->fail(CGS_E_TIMEOUT, "gave up waiting for the tensor cores");
+  return CGS_OK;
+}
+
 int cgs_mvc_field_train(cgs_ctx* ctx, uint64_t n, const float* d_points, const float* d_weights,
                         uint32_t steps, uint32_t batch, float lr, float lambda, uint64_t seed,
                         float* out_loss) {
@@ -1482,6 +1495,7 @@ int cgs_mvc_field_train(cgs_ctx* ctx, uint64_t n, const float* d_points, const f
   cudaStream_t s = ctx->stream;
   const uint32_t tail = std::max<uint32_t>(1, steps / 10);
   CGS_CUDA(cudaMemsetAsync(f.loss.p, 0, 8, s), "field train");
+  CGS_CUDA(cudaMemsetAsync(f.status.p, 0, 4, s), "field train");
   uint64_t st = seed ^ 0xD1B54A32D192ED03ull;
   for (uint32_t t = 0; t < steps; ++t) {
     if (t == steps - tail) CGS_CUDA(cudaMemsetAsync(f.loss.p, 0, 8, s), "field train");
@@ -1498,7 +1512,7 @@ int cgs_mvc_field_train(cgs_ctx* ctx, uint64_t n, const float* d_points, const f
   }
   float hl[2] = {0.0f, 0.0f};
   CGS_CUDA(cudaMemcpyAsync(hl, f.loss.p, 8, cudaMemcpyDeviceToHost, s), "field train");
-  CGS_CUDA(cudaStreamSynchronize(s), "field train");
+  CGS_TRY(field_status(ctx, "field training"));
   if (out_loss) {
     out_loss[0] = steps ? hl[0] / (float)tail : 0.0f;
     out_loss[1] = steps ? hl[1] / (float)tail : 0.0f;
@@ -1514,12 +1528,13 @@ int cgs_mvc_field_grads(cgs_ctx* ctx, uint64_t n, const float* d_points, const f
   FieldState& f = ctx->field;
   cudaStream_t s = ctx->stream;
   CGS_CUDA(cudaMemsetAsync(f.loss.p, 0, 8, s), "field grads");
+  CGS_CUDA(cudaMemsetAsync(f.status.p, 0, 4, s), "field grads");
   CGS_CUDA(f.forward(d_points, d_weights, (uint32_t)n, (uint32_t)n, 0, ctx->mvc_rest.as<float4>(),
                      lambda, s), "field forward");
   CGS_CUDA(f.backward((uint32_t)n, s), "field backward");
   float hl[2];
   CGS_CUDA(cudaMemcpyAsync(hl, f.loss.p, 8, cudaMemcpyDeviceToHost, s), "field grads");
-  CGS_CUDA(cudaStreamSynchronize(s), "field grads");
+  CGS_TRY(field_status(ctx, "field gradients"));
   if (grads)
     CGS_CUDA(cudaMemcpy(grads, f.g32.p, (size_t)f.total() * 4, cudaMemcpyDeviceToHost),
              "field grads");
@@ -1535,9 +1550,9 @@ int cgs_mvc_field_eval(cgs_ctx* ctx, uint64_t n, const float* d_points, float* d
   if (n == 0) return CGS_OK;
   if (!d_points || !d_weights) return CGS_E_ARG;
   if (n > 0xFFFFFFFFull) return ctx->fail(CGS_E_CAPACITY, "at most 2^32 - 1 points");
+  CGS_CUDA(cudaMemsetAsync(ctx->field.status.p, 0, 4, ctx->stream), "field eval");
   CGS_CUDA(ctx->field.eval((uint32_t)n, d_points, d_weights, ctx->stream), "field eval");
-  CGS_CUDA(cudaStreamSynchronize(ctx->stream), "field eval");
-  return CGS_OK;
+  return field_status(ctx, "field evaluation");
 }
 
 int cgs_mvc_field_infer(cgs_ctx* ctx, uint64_t n, const float* d_points, int32_t use_rest,
