@@ -117,14 +117,22 @@ __device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t v, uint32_t* wa
   return excl;
 }
 
+// a + b, saturating at 2^32 - 1
+__device__ __forceinline__ uint32_t sat_add_u32(uint32_t a, uint32_t b) {
+  const uint32_t c = a + b;
+  return c < a ? 0xFFFFFFFFu : c;
+}
+
 // Chained-scan ("decoupled look-back", Merrill & Garland 2016) of one value
 // per tile. status[t] = flag << 32 | value with flag 1 = tile aggregate
 // published, 2 = inclusive prefix published; the array must be zeroed before
 // the launch. Tiles must be acquired in increasing order by running blocks
 // (a dynamic tile counter), so every tile a block waits on is held by a block
 // that is already resident. Called by all lanes of ONE warp; returns the
-// exclusive prefix of `tile` and publishes its inclusive prefix. A wait that
-// exceeds `limit` polls sets kStatusLookbackTimeout and returns 0.
+// exclusive prefix of `tile` and publishes its inclusive prefix (with SAT,
+// sums saturate at 2^32 - 1 instead of wrapping). A wait that exceeds `limit`
+// polls sets kStatusLookbackTimeout and returns 0.
+template <bool SAT = false>
 __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status, uint32_t tile,
                                                       uint32_t aggregate, uint32_t* status_word,
                                                       uint32_t limit = kSpinLimit) {
@@ -156,8 +164,11 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
     int first_p = pmask ? (__ffs(pmask) - 1) : 32;
     uint32_t v = lane <= first_p ? (uint32_t)st : 0u;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    exclusive += v;
+    for (int o = 16; o > 0; o >>= 1) {
+      const uint32_t w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = SAT ? sat_add_u32(v, w) : v + w;
+    }
+    exclusive = SAT ? sat_add_u32(exclusive, v) : exclusive + v;
     if (pmask) break;
     pred -= 32;
   }
@@ -165,7 +176,9 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
     if (lane == 0) atomicOr(status_word, kStatusLookbackTimeout);
     exclusive = 0;
   }
-  if (lane == 0) st_relaxed_u64(&status[tile], (2ull << 32) | (uint32_t)(exclusive + aggregate));
+  if (lane == 0)
+    st_relaxed_u64(&status[tile], (2ull << 32) | (SAT ? sat_add_u32(exclusive, aggregate)
+                                                      : exclusive + aggregate));
   return exclusive;
 }
 

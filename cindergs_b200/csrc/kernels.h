@@ -243,22 +243,22 @@ struct BinArgs {
   uint32_t max_n;
   uint32_t width, height, tiles_x, tiles_y;
   uint32_t tile_w_log2, tile_h_log2;  // screen tile shape (8x8, 16x16 or 32x16 pixels)
-  // per slot (depth order): the counting kernel writes the tile count, the
-  // scan turns it into the first entry in place
+  // per slot (depth order): the first entry (direct mode), or the tile count
+  // that a scan turns into the first entry in place (record mode)
   uint32_t* offsets;            // [max_n]
-  uint32_t* tile_stage;         // [ceil(max_n/32)] staging start of each 32-slot tile
-  uint32_t* tile_count;         // [ceil(max_n/32)] entries of each 32-slot tile
-  const uint32_t* run_start;    // placement: first entry of each 32-slot tile (else offsets)
+  // direct mode: look-back words of the 32-slot tiles' hit counts, zeroed
+  unsigned long long* lookback; // [ceil(max_n/32)]
+  // record mode: staging start and records of each 32-slot tile and group
+  uint32_t* tile_stage;
+  uint32_t* tile_count;
   uint32_t blocks_per_sm;       // resident blocks per SM of the count kernel (0: all that fit)
   FrameCounters* fc;
   int key64;
   uint32_t depth_bits;          // depth bits in a 32-bit key
-  // staged entries (counting kernel) and their final places (placement kernel)
-  uint32_t* stage_keys;         // 32-bit: packed keys; 64-bit: tile ids
-  uint32_t* stage_depths;       // 64-bit: raw depth bits
-  uint32_t* stage_ids;
-  uint32_t* keys;
-  uint32_t* depths;
+  // record mode: the staged records; direct mode: the entries in depth order
+  uint32_t* stage_keys;
+  uint32_t* keys;               // 32-bit: packed keys; 64-bit: tile ids
+  uint32_t* depths;             // 64-bit: raw depth bits
   uint32_t* ids;
   uint32_t* hist;               // [passes][1 << radix_bits] tile-digit histograms, zeroed
   uint32_t radix_bits;
@@ -272,16 +272,12 @@ struct BinArgs {
   uint32_t groups;              // <= 8
   uint32_t group_shift;
 };
-// Counts each slot's tiles, stages its entries and accumulates the histograms
-// (k_bin_count); the caller then scans `offsets` in place (launch_scan_u32,
-// total -> fc->entries) and places the staged entries (launch_bin_place).
+// Counts each slot's tiles and, in direct mode, writes the scanned offsets,
+// the entry total (fc->entries) and every entry at its place in depth order
+// and accumulates the tile-digit histograms (k_bin_count, one launch); in
+// record mode it stages one record per hit and leaves the per-slot counts
+// for a scan (launch_scan_u32).
 cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s);
-cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s);
-// first_run[t] = the run holding position t * kRadixTileItems, for every t
-// whose first position lies in a non-empty run (runs: run_start [num_runs]
-// exclusive starts, run_len [num_runs] lengths); at most max_tiles entries.
-cudaError_t launch_run_index(const uint32_t* run_start, const uint32_t* run_len, uint32_t num_runs,
-                             uint32_t* first_run, uint32_t max_tiles, cudaStream_t s);
 // Tile transpose (the entry sort when the tiles fit shared memory): a
 // one-pass stable counting sort of the staged records by tile. Chunk k is the
 // 32-slot tiles [k * chunk_wtiles, (k + 1) * chunk_wtiles); warp w of a chunk
@@ -356,18 +352,7 @@ struct SortArgs {
   // bit p: pass p uses shared-memory peer masks instead (one atomicOr and
   // one warp barrier per key: cheapest for many distinct 8-bit digits)
   uint32_t smem_mask = 0u;
-  // Optional: the input (buffer `src`) is staged in runs: position q of the
-  // input order is element run_src[k] + q - run_start[k] for the run k holding
-  // q (run_start: exclusive scan of the run lengths, runs in input order;
-  // first_run[t]: the run holding position 4096 t, launch_run_index). The
-  // first pass gathers them; no placement pass is needed.
-  const uint32_t* run_start = nullptr;
-  const uint32_t* run_src = nullptr;
-  const uint32_t* first_run = nullptr;
-  uint32_t num_runs = 0;
 };
-// Entries per radix sort tile (the unit of first_run).
-constexpr uint32_t kRadixTileItems = 4096;
 // Wait drills (cgs_ctx_wait_drill): each runs one of the library's bounded
 // device waits against a predecessor or barrier that nothing completes, with
 // `limit` polls, so that it gives up and sets its status bit in *status_word.

@@ -198,7 +198,6 @@ struct cgs_ctx {
   // arena
   DevBuf tet_J, tet_R, tet_S, def_pos, def_cova, def_covb, split_meta, persist;
   DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
-  DevBuf run_index;  // per radix tile of the entry sort: the staged run holding its first entry
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
   // SH coefficient rotation (cgs_sh_rotate, cgs_export_deformed): the band
@@ -388,7 +387,6 @@ int ensure_entry_buffers(cgs_ctx* ctx, uint32_t cap, bool key64, uint32_t radix_
     if (key64) CGS_TRY(ctx->ensure(ctx->depths[k], ecap * 4, "sort depths"));
   }
   const uint32_t tiles = sort_tiles((uint32_t)ecap);
-  CGS_TRY(ctx->ensure(ctx->run_index, (size_t)tiles * 4, "entry run index"));
   if (tiles != ctx->radix_lb_tiles || radix_bits != ctx->radix_lb_bits || !ctx->radix_lb[0].p) {
     const size_t bytes = (size_t)tiles * (1u << radix_bits) * 8;  // 64-bit look-back words
     for (int k = 0; k < 2; ++k) {
@@ -506,8 +504,6 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.key64 = d.key64;
   b.depth_bits = d.depth_bits;
   b.stage_keys = ctx->keys[1].as<uint32_t>();
-  b.stage_depths = d.key64 ? ctx->depths[1].as<uint32_t>() : nullptr;
-  b.stage_ids = ctx->ids[1].as<uint32_t>();
   b.keys = ctx->keys[0].as<uint32_t>();
   b.depths = d.key64 ? ctx->depths[0].as<uint32_t>() : nullptr;
   b.ids = ctx->ids[0].as<uint32_t>();
@@ -518,35 +514,21 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   b.records = transpose ? 1 : 0;
   b.group_shift = 11;  // kTransposeGroupTiles = 2^11
   b.groups = transpose ? (d.total_tiles + kTransposeGroupTiles - 1) / kTransposeGroupTiles : 1u;
-  // Count + stage. The tile transpose then scans the per-slot counts in place
-  // (first entries, entry total). The radix path scans the per-32-slot run
-  // lengths instead (run starts, entry total) and indexes the runs by radix
-  // tile: the sort's first pass gathers the staged runs in slot order, so no
-  // placement pass moves them (offsets keep the per-slot counts).
+  // Direct mode (radix path): one launch counts, scans (look-back over the
+  // 32-slot tiles) and writes every entry at its place in depth order. The
+  // tile transpose stages records and then scans the per-slot counts in place
+  // (first entries, entry total).
   const uint32_t nwt = (d.max_n + 31) / 32;
-  uint32_t* run_start = b.tile_stage + nwt;  // unused part of the per-group staging starts
-  const bool gather = !transpose && sort_passes(d.tile_bits, d.radix_bits) > 0;
+  b.lookback = reinterpret_cast<unsigned long long*>(b.tile_stage + 2 * (size_t)nwt);
   ctx->kbegin(CGS_K_BIN);
   CGS_CUDA(launch_bin_count(b, s), "bin count launch");
   if (transpose) {
     CGS_CUDA(launch_scan_u32(b.offsets, b.offsets, d.max_n, &fc->entries,
                              (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
              "offsets scan launch");
-  } else {
-    CGS_CUDA(launch_scan_u32(b.tile_count, run_start, nwt, &fc->entries,
-                             (unsigned long long*)(sc + L.bin), &fc->tile_ctr[3], &fc->status, s),
-             "run scan launch");
-    if (gather) {
-      CGS_CUDA(launch_run_index(run_start, b.tile_count, nwt, ctx->run_index.as<uint32_t>(),
-                                sort_tiles(ctx->entry_cap), s),
-               "run index launch");
-    } else {
-      b.run_start = run_start;  // no sort pass (one screen tile): place the runs
-      CGS_CUDA(launch_bin_place(b, s), "bin place launch");
-    }
   }
   ctx->kend();
-  if (bin_launches) *bin_launches = transpose ? 2u : 3u;
+  if (bin_launches) *bin_launches = transpose ? 2u : 1u;
   if (transpose) {
     // one-pass stable counting sort of the staged records by tile
     const uint32_t target = 296;  // chunks: two per SM
@@ -611,13 +593,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.tile_ctr = rtiles;
   sa.status_word = &fc->status;
   sa.hist = d_hist;
-  sa.src = gather ? 1 : 0;
-  if (gather) {
-    sa.run_start = run_start;
-    sa.run_src = b.tile_stage;
-    sa.first_run = ctx->run_index.as<uint32_t>();
-    sa.num_runs = nwt;
-  }
+  sa.src = 0;
   // The entries' first digit (the low tile bits) differs from lane to lane,
   // so that pass ranks with per-bit ballots; after it a warp's keys mostly
   // share their higher digits, which __match_any_sync groups more cheaply.
@@ -2773,10 +2749,9 @@ int cgs_read_frame_buffer(cgs_ctx* ctx, int32_t which, void* dst, uint64_t dst_b
       const uint32_t* ord = (const uint32_t*)tmp.data();
       std::vector<uint32_t> cnt(sa, 0);
       for (size_t j = 0; j < sa; ++j) {
-        // the tile transpose leaves the scanned offsets, the radix path the counts
         const uint32_t next = j + 1 < sa ? off[j + 1] : (uint32_t)entries;
         if (ord[j] >= sa) return ctx->fail(CGS_E_STATE, "splat order out of range");
-        cnt[ord[j]] = ctx->s3_transpose ? next - off[j] : off[j];
+        cnt[ord[j]] = next - off[j];
       }
       out.resize(sa * 4);
       uint32_t* o = (uint32_t*)out.data();

@@ -89,16 +89,6 @@ struct PassArgs {
   uint32_t* tile_ctr;
   uint32_t* status_word;
   uint32_t rank;           // how a warp finds the lanes sharing a digit: kRank*
-  // Gather mode (a first pass that reads staged runs instead of a contiguous
-  // input): position q of the input order is element run_src[k] + (q -
-  // run_start[k]) of keys_in / v0_in / v1_in, for the run k with run_start[k]
-  // <= q < run_start[k + 1] (run_start is the exclusive scan of the run
-  // lengths, runs in input order); first_run[t] is the run holding position
-  // t * 4096. Null run_start: contiguous input.
-  const uint32_t* run_start;
-  const uint32_t* run_src;
-  const uint32_t* first_run;
-  uint32_t num_runs;
 };
 
 // Exclusive prefix of digit d over the tiles before `tile`: walks back from
@@ -186,59 +176,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   const size_t first = tile_base + (size_t)warp * (32 * kSortItems) + lane;
   uint32_t k[kSortItems], v0[kSortItems], v1[kSortItems];
   uint32_t rk[kSortItems / 2];  // two 16-bit in-warp ranks per word (ranks < 512)
-  if (a.run_start) {
-    // Gather mode: the runs overlapping this tile's positions, from the one
-    // holding its first position, go to shared memory (the reorder buffers,
-    // unused until after ranking) 256 at a time until one starts past the
-    // tile; each lane then walks forward through them as its positions grow.
-    uint32_t* s_rs = s_keys;  // run starts
-    uint32_t* s_rsrc = s_v0;  // their staged positions
-    const uint32_t tile_end = (uint32_t)min((size_t)n, tile_base + kSortTile);
-    const uint32_t k0 = __ldcg(a.first_run + tile);
-    uint32_t nwin = 0;
-    for (;;) {
-      const uint32_t kk = k0 + nwin + (uint32_t)tid;
-      const bool in = kk < a.num_runs;
-      s_rs[nwin + tid] = in ? __ldcg(a.run_start + kk) : 0xFFFFFFFFu;
-      s_rsrc[nwin + tid] = in ? __ldcg(a.run_src + kk) : 0u;
-      nwin += kSortThreads;
-      __syncthreads();
-      if (nwin >= kSortTile || s_rs[nwin - 1] >= tile_end) break;
-    }
-    const bool covered = s_rs[nwin - 1] >= tile_end;
-    uint32_t r = 0;
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-      const size_t q = first + 32 * j;
-      k[j] = 0xFFFFFFFFu;
-      v0[j] = 0u;
-      if (PAY2) v1[j] = 0u;
-      if (q < (size_t)n) {
-        uint32_t src;
-        if (covered) {
-          while (r + 1 < nwin && s_rs[r + 1] <= (uint32_t)q) ++r;
-          src = s_rsrc[r] + ((uint32_t)q - s_rs[r]);
-        } else {
-          // more runs than the window holds (many empty ones): search the
-          // run starts in memory
-          uint32_t lo = k0, hi = a.num_runs;  // last run with start <= q
-          while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (__ldcg(a.run_start + mid) <= (uint32_t)q) lo = mid; else hi = mid;
-          }
-          src = __ldcg(a.run_src + lo) + ((uint32_t)q - __ldcg(a.run_start + lo));
-        }
-        if (src < a.capacity) {
-          k[j] = __ldcs(a.keys_in + src);
-          v0[j] = __ldcs(a.v0_in + src);
-          if (PAY2) v1[j] = __ldcs(a.v1_in + src);
-        } else {
-          atomicOr(a.status_word, kStatusCapacity);
-        }
-      }
-    }
-    __syncthreads();  // the window is read before the reorder reuses the buffers
-  } else if (full) {
+  if (full) {
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
       k[j] = __ldcs(a.keys_in + first + 32 * j);
@@ -497,10 +435,6 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.grid_tiles = tiles;
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
-    pa.run_start = p == 0 ? a.run_start : nullptr;
-    pa.run_src = a.run_src;
-    pa.first_run = a.first_run;
-    pa.num_runs = a.num_runs;
     pa.rank = ((a.smem_mask >> p) & 1u) ? kRankSmem : (((a.ballot_mask >> p) & 1u) ? kRankBallot : kRankMatch);
     cudaError_t e;
     switch (rb) {

@@ -339,8 +339,11 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
   if (!SPLIT && tile == 0 && threadIdx.x == 0) *a.split_count = 0u;
   if (tet_blocks) {
     // Wait (bounded) until every tet block has published; the tet data is
-    // then read through L2 (ld.global.cg), never through the incoherent
-    // read-only path.
+    // then read with ld.global.ca (L1-cached, ordered after the acquire; no
+    // SM has cached those lines earlier in this launch, and L1 holds no lines
+    // from earlier launches), never through the incoherent read-only path. A
+    // few hundred tets' J are read by every Gaussian: served from L1 instead
+    // of hammering the same L2 lines.
     if (threadIdx.x == 0) {
       uint32_t spins = 0;
       while (ld_acquire_u32(&a.fc->tile_ctr[kTetsDoneCtr]) < tet_blocks) {
@@ -438,9 +441,9 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
       const float pz =
           w.x * __ldg(v0 + 2) + w.y * __ldg(v1 + 2) + w.z * __ldg(v2 + 2) + w.w * __ldg(v3 + 2);
       const float* J = a.tet_J + 9 * (size_t)tet_raw;
-      const float j_00 = __ldcg(J + 0), j_10 = __ldcg(J + 1), j_20 = __ldcg(J + 2);
-      const float j_01 = __ldcg(J + 3), j_11 = __ldcg(J + 4), j_21 = __ldcg(J + 5);
-      const float j_02 = __ldcg(J + 6), j_12 = __ldcg(J + 7), j_22 = __ldcg(J + 8);
+      const float j_00 = __ldca(J + 0), j_10 = __ldca(J + 1), j_20 = __ldca(J + 2);
+      const float j_01 = __ldca(J + 3), j_11 = __ldca(J + 4), j_21 = __ldca(J + 5);
+      const float j_02 = __ldca(J + 6), j_12 = __ldca(J + 7), j_22 = __ldca(J + 8);
       const float s_xx = rca.x, s_xy = rca.y, s_xz = rca.z, s_yy = rca.w, s_yz = rcb.x,
                   s_zz = rcb.y;
       const float k_00 = j_00 * s_xx + j_01 * s_xy + j_02 * s_xz;
@@ -466,7 +469,7 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
       const float s_det = clampf(det_j, 0.6f, 1.8f);
       const float safe_base = clampf(1.0f - rp.w, 1e-4f, 0.999f);
       const float alpha_prime = clampf(1.0f - cgs_powf(safe_base, 1.0f / s_det), 0.05f, 0.99f);
-      split = SPLIT && a.split_threshold > 0.0f && __ldcg(&a.tet_stretch[tet_raw]) > a.split_threshold;
+      split = SPLIT && a.split_threshold > 0.0f && __ldca(&a.tet_stretch[tet_raw]) > a.split_threshold;
       if (!split) {
         float xx = m00, yy = m11, zz = m22, alpha = alpha_prime;
         if (a.mip > 0.0f) mip3d(xx, m01, m02, yy, m12, zz, alpha, a.mip);

@@ -230,11 +230,11 @@ __device__ __forceinline__ void box_rc(const uint4 box, uint32_t c, uint32_t& r,
   col = c - r * box.z;
 }
 
-// Binning in depth-key order, part 1 (slot s is splat order_ids[s]; Stage 2's
-// depth keys were radix-sorted stably, so slots run by (depth key, splat
-// index)). Persistent warps: each warp takes 32 consecutive slots at a time
-// from a counter and handles them alone, without waiting for any other warp.
-// The 32 splats' candidate tiles (each splat's tile box, row-major) are
+// Binning in depth-key order (slot s is splat order_ids[s]; Stage 2's depth
+// keys were radix-sorted stably, so slots run by (depth key, splat index)).
+// Persistent warps: each warp takes 32 consecutive slots at a time from a
+// counter (so the 32-slot tiles are taken in increasing order). The 32
+// splats' candidate tiles (each splat's tile box, row-major) are
 // concatenated and tested 32 at a time, one per lane, so large and small
 // splats share the lanes evenly.
 //   0. term tables: the column and row terms of the 32 tile boxes (when they
@@ -242,21 +242,22 @@ __device__ __forceinline__ void box_rc(const uint4 box, uint32_t c, uint32_t& r,
 //   1. counting: ballot per 32 candidates; the masks, the hits before each
 //      mask, and one record per hit (tile id or candidate index, owner lane)
 //      are kept in shared memory. A slot's count is the number of hits inside
-//      its candidate range, read from the masks, and is written to `offsets`.
-//   2. staging: the tile's hits, in candidate order (= the reference's
-//      emission order: splat by splat, row-major), get a contiguous range of
-//      the staging buffers from an atomic counter and are written there with
-//      their 32-bit keys (tile << depth_bits | depth_q) or, beyond 65,535
-//      tiles, (tile, raw depth bits) pairs; the block's digit histograms of
-//      the tile bits are accumulated. Warps with more hits or candidates than
-//      the shared-memory stores hold walk their candidates again for the rest.
-// The staging order of the tiles is whatever the counter gave; the entry
-// sort's first pass reads each 32-slot tile's staged run in slot order (or
-// k_bin_place moves it to its scanned offset), which restores the (depth,
-// splat index) order, and a stable sort on the tile bits alone then yields
-// the reference's (tile, depth, splat index) order. Entries at or beyond the
-// buffer capacity are not written and set the capacity status bit (the host
-// grows the buffers and runs Stage 3 again).
+//      its candidate range, read from the masks.
+//   2. direct mode: the tile's hit count enters a decoupled look-back over
+//      the 32-slot tiles (published as soon as it is counted; sums saturate),
+//      which gives the tile's first entry: the slots' scanned offsets are
+//      written, and the hits, in candidate order (= the reference's emission
+//      order: splat by splat, row-major), are written at their places in
+//      depth order with their 32-bit keys (tile << depth_bits | depth_q) or,
+//      beyond 65,535 tiles, (tile, raw depth bits) pairs; the block's digit
+//      histograms of the tile bits are accumulated. A stable sort on the tile
+//      bits alone then yields the reference's (tile, depth, splat index)
+//      order. Record mode (the tile transpose) instead stages one record per
+//      hit at an atomic position per tile group and leaves the counts.
+//      Warps with more hits or candidates than the shared-memory stores hold
+//      walk their candidates again for the rest.
+// Entries at or beyond the buffer capacity are not written and set the
+// capacity status bit (the host grows the buffers and runs Stage 3 again).
 template <bool KEY64>
 __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
   extern __shared__ __align__(16) unsigned char bin_smem[];
@@ -429,7 +430,24 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       const uint32_t next = __shfl_down_sync(0xffffffffu, before, 1);
       count = (lane == 31 ? run : next) - before;
     }
-    if (s < a.max_n) a.offsets[s] = count;
+    // Direct mode: the 32-slot tile's first entry from a decoupled look-back
+    // over the tiles' hit counts (tiles are taken in increasing order), so
+    // each slot's scanned offset and each entry's final place in depth order
+    // are known here. Record mode keeps the counts (scanned afterwards).
+    uint32_t wexcl = 0;
+    if (rec_mode) {
+      if (s < a.max_n) a.offsets[s] = count;
+    } else {
+      wexcl = chained_scan_warp<true>(a.lookback, tile, run, &a.fc->status);
+      uint32_t cincl = count;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, cincl, o);
+        if (lane >= o) cincl += y;
+      }
+      if (s < a.max_n) a.offsets[s] = sat_add_u32(wexcl, cincl - count);
+      if (tile == num_tiles - 1u && lane == 0) a.fc->entries = sat_add_u32(wexcl, run);
+    }
 
     // 2. stage
     if (rec_mode) {
@@ -502,15 +520,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       }
       continue;
     }
-    uint32_t sbase = 0;
-    if (lane == 0) {
-      const unsigned long long sb64 =
-          run ? atomicAdd(&a.fc->stage_ctr, (unsigned long long)run) : 0ull;
-      sbase = sb64 >= cap ? cap : (uint32_t)sb64;  // at or past cap: nothing is staged
-      a.tile_stage[tile] = sbase;
-      a.tile_count[tile] = run;
-    }
-    sbase = __shfl_sync(0xffffffffu, sbase, 0);
+    const uint32_t sbase = wexcl;  // saturated: at or past cap, nothing is written
     auto put = [&](uint32_t k, uint32_t tile_id, int o) {
       const uint64_t pos = (uint64_t)sbase + k;
       if (pos >= cap) {
@@ -521,12 +531,12 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       uint32_t word;
       if (KEY64) {
         word = tile_id;
-        a.stage_depths[pos] = d;
+        a.depths[pos] = d;
       } else {
         word = a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d);
       }
-      a.stage_keys[pos] = word;
-      a.stage_ids[pos] = sp.sid[warp][o];
+      a.keys[pos] = word;
+      a.ids[pos] = sp.sid[warp][o];
       for (uint32_t p = 0; p < passes; ++p)
         atomicAdd(&s_hist[p * radix + ((word >> (tshift + p * a.radix_bits)) & rmask)], 1u);
     };
@@ -582,47 +592,6 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
     const uint32_t v = s_hist[k];
     if (v) atomicAdd(&a.hist[k], v);
-  }
-}
-
-// Binning, part 3: each 32-slot tile's staged range moves to the tile's first
-// entry (the scanned offset of its first slot), one warp per tile, coalesced
-// on both sides. Ranges that reach past the buffers were not staged (the
-// capacity bit is set) and are clamped here.
-template <bool KEY64>
-__global__ void __launch_bounds__(256) k_bin_place(const BinArgs a) {
-  const uint32_t num_tiles = (a.max_n + 31u) / 32u;
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  const uint32_t cap = a.entry_cap;
-  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < num_tiles; t += warps) {
-    const uint32_t n = a.tile_count[t];
-    if (n == 0) continue;
-    const uint32_t src = a.tile_stage[t];
-    const uint32_t dst = a.run_start ? a.run_start[t] : a.offsets[32u * t];
-    if (src >= cap || dst >= cap) continue;
-    const uint32_t m = min(n, min(cap - src, cap - dst));
-    for (uint32_t k0 = 0; k0 < m; k0 += 256) {  // eight loads in flight per lane and array
-      uint32_t kk[8], ii[8], dd[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const uint32_t k = k0 + 32u * u + lane;
-        if (k < m) {
-          kk[u] = __ldcs(a.stage_keys + src + k);
-          ii[u] = __ldcs(a.stage_ids + src + k);
-          if (KEY64) dd[u] = __ldcs(a.stage_depths + src + k);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const uint32_t k = k0 + 32u * u + lane;
-        if (k < m) {
-          a.keys[dst + k] = kk[u];
-          a.ids[dst + k] = ii[u];
-          if (KEY64) a.depths[dst + k] = dd[u];
-        }
-      }
-    }
   }
 }
 
@@ -921,33 +890,11 @@ __global__ void k_drill_chained_scan(unsigned long long* status, uint32_t* statu
   chained_scan_warp(status, 1u, 1u, status_word, limit);
 }
 
-// first_run[b] for the radix tiles whose first position lies in run k.
-__global__ void k_run_index(const uint32_t* __restrict__ run_start,
-                            const uint32_t* __restrict__ run_len, uint32_t num_runs,
-                            uint32_t* __restrict__ first_run, uint32_t max_tiles) {
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < num_runs;
-       k += gridDim.x * blockDim.x) {
-    const uint32_t len = run_len[k];
-    if (len == 0) continue;
-    const uint64_t st = run_start[k], en = st + len;
-    const uint64_t b0 = (st + kRadixTileItems - 1) / kRadixTileItems;
-    const uint64_t b1 = (en - 1) / kRadixTileItems;
-    for (uint64_t b = b0; b <= b1 && b < max_tiles; ++b) first_run[b] = k;
-  }
-}
-
 }  // namespace
 
 cudaError_t launch_drill_chained_scan(unsigned long long* status, uint32_t* status_word,
                                       uint32_t limit, cudaStream_t s) {
   k_drill_chained_scan<<<1, 32, 0, s>>>(status, status_word, limit);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_run_index(const uint32_t* run_start, const uint32_t* run_len, uint32_t num_runs,
-                             uint32_t* first_run, uint32_t max_tiles, cudaStream_t s) {
-  if (num_runs == 0) return cudaSuccess;
-  k_run_index<<<148 * 4, 256, 0, s>>>(run_start, run_len, num_runs, first_run, max_tiles);
   return cudaGetLastError();
 }
 
@@ -983,17 +930,6 @@ cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
   if (a.width >= (1u << 22) || a.height >= (1u << 22)) return cudaErrorInvalidValue;
   return a.key64 ? launch_bin_count_t<true>(a, s) : launch_bin_count_t<false>(a, s);
-}
-
-cudaError_t launch_bin_place(const BinArgs& a, cudaStream_t s) {
-  if (a.max_n == 0) return cudaSuccess;
-  const uint32_t tiles = (a.max_n + 31u) / 32u;
-  const uint32_t blocks = std::min<uint32_t>(148u * 8u, (tiles + 7u) / 8u);
-  if (a.key64)
-    k_bin_place<true><<<blocks, 256, 0, s>>>(a);
-  else
-    k_bin_place<false><<<blocks, 256, 0, s>>>(a);
-  return cudaGetLastError();
 }
 
 cudaError_t launch_chunk_counts(const TransposeArgs& a, cudaStream_t s) {

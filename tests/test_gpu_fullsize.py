@@ -216,7 +216,10 @@ def test_mvc_polygon_cage_full_size(st):
     np.testing.assert_array_equal(pos_e[sidx][out], wl.scene.positions[sidx][out])
     scale = np.abs(o["cov"][:m]).max(axis=1) + 1e-30
     dc = np.abs(cov_e[sidx].astype(np.float64) - o["cov"][:m]).max(axis=1) / scale
-    assert dc.mean() < 1e-4 and np.quantile(dc, 0.999) < 1e-2, (dc.mean(), dc.max())
+    # covariances go through F = sum_j v_j grad(w_j)^T, whose central
+    # differences divide the weights' 5e-5 agreement by 2h (h = 1e-3 x the
+    # cage diagonal)
+    assert dc.mean() < 1e-3 and dc.max() < 1e-2, (dc.mean(), dc.max())
 
     pts = torch.from_numpy(wl.training_points(2_000_000)).to("cuda:0")
     w = st.mvc_weights(pts)
