@@ -57,6 +57,11 @@ struct BinSplats {
   uint32_t rpre[kBinWarps][32];  // exclusive prefix of the tile-box heights
   uint32_t dq[kBinWarps][32];    // depth part of the key
   uint32_t sid[kBinWarps][32];   // splat index
+  // owner lookup of warps with at most kMaskCap * 32 candidates: bit i of
+  // word i / 32 set where a splat's candidates start, and the lane of the
+  // k-th splat with candidates
+  uint32_t sbits[kBinWarps][kMaskCap];
+  uint32_t lor[kBinWarps][32];
 };
 constexpr size_t kBinSmem = sizeof(BinSplats) + sizeof(uint32_t) * kBinWarps * (2 * kMaskCap + kHitCap) +
                             sizeof(float4) * kBinWarps * kTabCap +
@@ -351,6 +356,15 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       sp.sid[warp][lane] = sid;
     }
     if (rec_mode && lane < (int)kMaxGroups) s_gcnt[lane] = 0u;
+    const bool big = total > (uint32_t)kMaskCap * 32u;  // warp-uniform
+    if (!big) {
+#pragma unroll
+      for (int k = lane; k < kMaskCap; k += 32) sp.sbits[warp][k] = 0u;
+      const uint32_t nonempty = __ballot_sync(0xffffffffu, ncand > 0u);
+      if (ncand > 0u) sp.lor[warp][__popc(nonempty & lt)] = (uint32_t)lane;
+      __syncwarp();
+      if (ncand > 0u) atomicOr(&sp.sbits[warp][base >> 5], 1u << (base & 31u));
+    }
     __syncwarp();
     if (tab) {
       // 0. term tables: columns [0, wt), rows [wt, wt + ht)
@@ -380,17 +394,23 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       return tile_hit(tx, ty, wm1, hm1, lw, lh, sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o],
                       sp.kq[warp][o].w);
     };
-    const bool big = total > (uint32_t)kMaskCap * 32u;  // warp-uniform
 
     // 1. count
-    uint32_t run = 0;  // hits before the current chunk (warp-uniform)
-    uint32_t own = 0;  // this lane's hits, accumulated only when `big`
+    uint32_t run = 0;     // hits before the current chunk (warp-uniform)
+    uint32_t own = 0;     // this lane's hits, accumulated only when `big`
+    uint32_t starts = 0;  // splats starting before the current chunk
+    const uint32_t upto = (2u << lane) - 1u;  // bits 0 .. lane
     for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
       const uint32_t item = chunk + lane;
       bool hit = false;
       uint32_t rec = 0;
+      // owner of `item`: the k-th splat with candidates, k = the starts at or
+      // before it (a popcount instead of a search)
+      uint32_t sb = 0;
+      if (!big) sb = sp.sbits[warp][c];
       if (item < total) {
-        const int o = find_owner(wbase, item);
+        const int o = big ? find_owner(wbase, item)
+                          : (int)sp.lor[warp][starts + __popc(sb & upto) - 1u];
         const uint32_t ci = item - wbase[o];
         uint32_t tx, ty;
         hit = test(o, ci, tx, ty);
@@ -417,6 +437,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
         __syncwarp();
       }
       run += __popc(hits);
+      starts += __popc(sb);
     }
     __syncwarp();
     uint32_t count = own;
