@@ -616,6 +616,298 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
   }
 }
 
+// ---- Binning, direct mode ---------------------------------------------------
+// The radix path's binning in one launch (the record mode of the tile
+// transpose stays with k_bin_count). Per 32-slot tile (a warp's 32 splats in
+// depth order, tiles taken from a counter in increasing order):
+//   setup:  tile boxes, candidate and box-edge prefixes, per-splat constants
+//           in shared memory; a start bit at each splat's first candidate and
+//           the lane of each splat with candidates, so that a candidate's
+//           splat is found by a popcount (no search);
+//   tables: the column and row terms of the 32 tile boxes (tile_hit's
+//           column-only and row-only parts);
+//   count:  32 candidates per step, one per lane, ~20 rounded operations
+//           each against the tables (the whole test when the tables do not
+//           fit); the ballot masks and the hits before each are kept;
+//   scan:   the tile's hit count enters a decoupled look-back over the 32-slot
+//           tiles (saturating sums): the slots' scanned offsets and the tile's
+//           first entry;
+//   write:  the stored masks are walked again and every hit is written at
+//           its place in depth order (key, splat index, 64-bit: depth word);
+//           the tile-digit histograms count pass 0 per entry and the higher
+//           passes per run of lanes with one digit (a splat's row of tiles
+//           shares its high digits), one shared atomic per run.
+// Warps with more candidates than the masks hold test the rest again in the
+// write step. Entries at or beyond the capacity are not written and set the
+// capacity bit.
+constexpr int kDirMaskCap = 96;   // stored ballot masks per warp (3,072 candidates)
+constexpr int kDirTabCap = 448;   // term-table entries per warp
+
+struct DirSplats {
+  uint4 own[kBinWarps][32];    // first candidate, ceil(2^32 / width) (0 if width 1), width, first tile id
+  uint2 tb[kBinWarps][32];     // first column entry, first row entry in the term table
+  uint2 xy[kBinWarps][32];     // box origin (tiles)
+  float4 kq[kBinWarps][32];    // a, 2b, c, q_max + 1e-4
+  float4 geo[kBinWarps][32];   // mu_x, mu_y, -b, 2b
+  float4 con[kBinWarps][32];   // a, c, max(a, 1e-12), max(c, 1e-12)
+  double2 rcp[kBinWarps][32];  // RN64(1 / max(c, 1e-12)), RN64(1 / max(a, 1e-12))
+  uint32_t base[kBinWarps][32];
+  uint32_t cpre[kBinWarps][32];
+  uint32_t rpre[kBinWarps][32];
+  uint32_t dq[kBinWarps][32];
+  uint32_t sid[kBinWarps][32];
+  uint32_t lor[kBinWarps][32];           // lane of the k-th splat with candidates
+  uint32_t sbits[kBinWarps][kDirMaskCap];  // start bit per splat's first candidate
+  uint32_t mask[kBinWarps][kDirMaskCap];   // hit ballots
+  uint32_t mrun[kBinWarps][kDirMaskCap];   // hits before each ballot
+};
+constexpr size_t kDirSmem = sizeof(DirSplats) + sizeof(float4) * kBinWarps * kDirTabCap +
+                            sizeof(uint32_t) * 1024;  // + tile-digit histograms (<= 4 x 256)
+
+template <bool KEY64>
+__global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) {
+  extern __shared__ __align__(16) unsigned char dir_smem[];
+  DirSplats& sp = *reinterpret_cast<DirSplats*>(dir_smem);
+  float4* s_tab = reinterpret_cast<float4*>(dir_smem + sizeof(DirSplats));  // [w][kDirTabCap]
+  uint32_t* s_hist = reinterpret_cast<uint32_t*>(s_tab + kBinWarps * kDirTabCap);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
+  const uint32_t passes = (a.tile_bits + a.radix_bits - 1u) / a.radix_bits;
+  const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
+  const uint32_t nbins = passes * radix;
+  const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
+  const uint32_t lw = a.tile_w_log2, lh = a.tile_h_log2;
+  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
+  __syncthreads();
+  const uint32_t lt = lanemask_lt();
+  const uint32_t upto = (2u << lane) - 1u;  // lanes 0 .. lane
+  const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
+  const uint32_t num_tiles = (a.max_n + 31u) / 32u;
+  const uint32_t* wbase = sp.base[warp];
+  float4* wtab = s_tab + warp * kDirTabCap;
+  uint32_t* wmask = sp.mask[warp];
+  uint32_t* wmrun = sp.mrun[warp];
+  const uint32_t cap = a.entry_cap;
+  bool overflow = false;
+
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= num_tiles) break;
+    const uint32_t s = tile * 32u + lane;  // slot in depth order
+    uint32_t sid = kInvalid, dq = 0;
+    if (s < active && s < a.max_n) {
+      sid = a.order_ids[s];
+      dq = a.order_keys[s];
+    }
+    const SplatBox b = load_box(a, sid, active);
+
+    // ---- setup
+    const uint32_t bw = b.valid ? (b.x1 - b.x0 + 1u) : 0u;
+    const uint32_t bh = b.valid ? (b.y1 - b.y0 + 1u) : 0u;
+    const uint32_t ncand = bw * bh;
+    uint32_t incl = ncand, cincl = bw, rincl = bh;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      const uint32_t yc = __shfl_up_sync(0xffffffffu, cincl, o);
+      const uint32_t yr = __shfl_up_sync(0xffffffffu, rincl, o);
+      if (lane >= o) {
+        incl += y;
+        cincl += yc;
+        rincl += yr;
+      }
+    }
+    const uint32_t base = incl - ncand;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t wt = __shfl_sync(0xffffffffu, cincl, 31);
+    const uint32_t ht = __shfl_sync(0xffffffffu, rincl, 31);
+    const bool tab = wt + ht <= (uint32_t)kDirTabCap;            // warp-uniform
+    const bool big = total > (uint32_t)kDirMaskCap * 32u;        // warp-uniform
+    const uint32_t nonempty = __ballot_sync(0xffffffffu, ncand > 0u);
+    __syncwarp();  // the previous tile's readers are done with the warp's shared memory
+    {
+      const uint32_t w = b.valid ? bw : 1u;
+      const float ca_ = fmaxf(b.ca, 1e-12f), cc_ = fmaxf(b.cc, 1e-12f);
+      const float cb2 = __fmul_rn(2.0f, b.cb);
+      const float qlim =
+          __fadd_rn(b.valid ? clampf(__fmul_rn(2.0f, cgs_logf(__fmul_rn(255.0f, b.alpha))), 0.0f, 8.0f)
+                            : 0.0f,
+                    1e-4f);
+      sp.own[warp][lane] =
+          make_uint4(base, w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w), w,
+                     b.y0 * a.tiles_x + b.x0);
+      sp.tb[warp][lane] = make_uint2(cincl - bw, wt + rincl - bh);
+      sp.xy[warp][lane] = make_uint2(b.x0, b.y0);
+      sp.kq[warp][lane] = make_float4(b.ca, cb2, b.cc, qlim);
+      sp.geo[warp][lane] = make_float4(b.mu_x, b.mu_y, -b.cb, cb2);
+      sp.con[warp][lane] = make_float4(b.ca, b.cc, ca_, cc_);
+      sp.rcp[warp][lane] = make_double2(1.0 / (double)cc_, 1.0 / (double)ca_);
+      sp.base[warp][lane] = base;
+      sp.cpre[warp][lane] = cincl - bw;
+      sp.rpre[warp][lane] = rincl - bh;
+      sp.dq[warp][lane] = dq;
+      sp.sid[warp][lane] = sid;
+      if (ncand > 0u) sp.lor[warp][__popc(nonempty & lt)] = (uint32_t)lane;
+      if (!big) {
+#pragma unroll
+        for (int k = lane; k < kDirMaskCap; k += 32) sp.sbits[warp][k] = 0u;
+      }
+    }
+    __syncwarp();
+    if (!big && ncand > 0u) atomicOr(&sp.sbits[warp][base >> 5], 1u << (base & 31u));
+    // ---- tables: columns [0, wt), rows [wt, wt + ht)
+    if (tab) {
+      for (uint32_t i = lane; i < wt; i += 32) {
+        const int o = find_owner(sp.cpre[warp], i);
+        wtab[i] = col_terms(sp.xy[warp][o].x + (i - sp.cpre[warp][o]), lw, wm1, sp.geo[warp][o],
+                            sp.con[warp][o], sp.rcp[warp][o]);
+      }
+      for (uint32_t i = lane; i < ht; i += 32) {
+        const int o = find_owner(sp.rpre[warp], i);
+        wtab[wt + i] = row_terms(sp.xy[warp][o].y + (i - sp.rpre[warp][o]), lh, hm1,
+                                 sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o]);
+      }
+    }
+    __syncwarp();
+    // owner (lane) of candidate `item`; sb = start bits of its chunk, starts =
+    // splats starting before the chunk
+    auto owner = [&](uint32_t item, uint32_t sb, uint32_t starts) -> int {
+      return big ? find_owner(wbase, item) : (int)sp.lor[warp][starts + __popc(sb & upto) - 1u];
+    };
+    // the test of candidate item of splat o; r, c its row and column in the box
+    auto test = [&](int o, uint32_t item, uint32_t& r, uint32_t& c) -> bool {
+      const uint4 ow = sp.own[warp][o];
+      const uint32_t ci = item - ow.x;
+      r = ow.y ? __umulhi(ci, ow.y) : ci;
+      c = ci - r * ow.z;
+      if (tab) {
+        const uint2 t = sp.tb[warp][o];
+        return tab_hit(wtab[t.x + c], wtab[t.y + r], sp.kq[warp][o]);
+      }
+      const uint2 xy = sp.xy[warp][o];
+      return tile_hit(xy.x + c, xy.y + r, wm1, hm1, lw, lh, sp.geo[warp][o], sp.con[warp][o],
+                      sp.rcp[warp][o], sp.kq[warp][o].w);
+    };
+
+    // ---- count
+    uint32_t run = 0;     // hits before the current chunk (warp-uniform)
+    uint32_t own = 0;     // this lane's hits, accumulated only when `big`
+    uint32_t starts = 0;  // splats starting before the current chunk
+    for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
+      const uint32_t item = chunk + lane;
+      const uint32_t sb = big ? 0u : sp.sbits[warp][c];
+      bool hit = false;
+      if (item < total) {
+        uint32_t r, cc;
+        hit = test(owner(item, sb, starts), item, r, cc);
+      }
+      const uint32_t hits = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0 && c < (uint32_t)kDirMaskCap) {
+        wmask[c] = hits;
+        wmrun[c] = run;
+      }
+      if (big) {
+        const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
+        const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
+        own += __popc(hits & seg_mask(lo, hi));
+      }
+      run += __popc(hits);
+      starts += __popc(sb);
+    }
+    __syncwarp();
+    uint32_t count = own;
+    if (!big) {
+      // hits before this lane's first candidate, from the stored masks
+      uint32_t before = run;
+      if (base < total) {
+        const uint32_t c = base >> 5;
+        before = wmrun[c] + __popc(wmask[c] & ((1u << (base & 31u)) - 1u));
+      }
+      const uint32_t next = __shfl_down_sync(0xffffffffu, before, 1);
+      count = (lane == 31 ? run : next) - before;
+    }
+
+    // ---- scan
+    const uint32_t wexcl = chained_scan_warp<true>(a.lookback, tile, run, &a.fc->status);
+    {
+      uint32_t cincl2 = count;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, cincl2, o);
+        if (lane >= o) cincl2 += y;
+      }
+      if (s < a.max_n) a.offsets[s] = sat_add_u32(wexcl, cincl2 - count);
+      if (tile == num_tiles - 1u && lane == 0) a.fc->entries = sat_add_u32(wexcl, run);
+    }
+
+    // ---- write
+    uint32_t hrun = 0;
+    starts = 0;
+    for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
+      const uint32_t item = chunk + lane;
+      const uint32_t sb = big ? 0u : sp.sbits[warp][c];
+      uint32_t hits;
+      if (c < (uint32_t)kDirMaskCap) {
+        hits = wmask[c];
+      } else {
+        bool h = false;
+        if (item < total) {
+          uint32_t r, cc;
+          h = test(owner(item, sb, starts), item, r, cc);
+        }
+        hits = __ballot_sync(0xffffffffu, h);
+      }
+      const bool hit = (hits >> lane) & 1u;
+      uint32_t word = 0;
+      if (hit) {
+        const int o = owner(item, sb, starts);
+        const uint4 ow = sp.own[warp][o];
+        const uint32_t ci = item - ow.x;
+        const uint32_t r = ow.y ? __umulhi(ci, ow.y) : ci;
+        const uint32_t cc = ci - r * ow.z;
+        const uint32_t tile_id = ow.w + r * a.tiles_x + cc;
+        const uint32_t d = sp.dq[warp][o];
+        word = KEY64 ? tile_id : (a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d));
+        const uint64_t pos = (uint64_t)wexcl + hrun + __popc(hits & lt);
+        if (pos < cap) {
+          a.keys[pos] = word;
+          a.ids[pos] = sp.sid[warp][o];
+          if (KEY64) a.depths[pos] = d;
+        } else {
+          overflow = true;
+        }
+      }
+      // tile-digit histograms: pass 0 per entry; the higher passes per run of
+      // consecutive lanes holding one digit
+      for (uint32_t p = 0; p < passes; ++p) {
+        const uint32_t dg = hit ? (word >> (tshift + p * a.radix_bits)) & rmask : 0xFFFFFFFFu;
+        if (p == 0) {
+          if (hit) atomicAdd(&s_hist[dg], 1u);
+          continue;
+        }
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, dg, 1);
+        const bool first = lane == 0 || dg != prev;
+        const uint32_t bnd = __ballot_sync(0xffffffffu, first);
+        if (hit && first) {
+          const uint32_t after = bnd & ~upto;
+          const uint32_t len = (after ? (uint32_t)(__ffs(after) - 1) : 32u) - (uint32_t)lane;
+          atomicAdd(&s_hist[p * radix + dg], len);
+        }
+      }
+      hrun += __popc(hits);
+      starts += __popc(sb);
+    }
+  }
+  if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
+    const uint32_t v = s_hist[k];
+    if (v) atomicAdd(&a.hist[k], v);
+  }
+}
+
 // ---- Tile transpose ---------------------------------------------------------
 // The binning kernel stages each 32-slot tile's hits in the reference's
 // emission order. Sorting them stably by tile is a transpose of the
@@ -921,36 +1213,40 @@ cudaError_t launch_drill_chained_scan(unsigned long long* status, uint32_t* stat
 
 // Persistent grid: as many blocks as fit on the device at once (at most one
 // warp per 32-slot tile).
-template <bool KEY64>
-cudaError_t launch_bin_count_t(const BinArgs& a, cudaStream_t s) {
-  static int resident = 0;  // blocks of k_bin_count<KEY64> the device runs at once
-  static int sm_count = 0;
-  if (resident == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_bin_count<KEY64>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBinSmem);
+// Persistent grid of kernel K (k_bin_count or k_bin_direct) with `smem`
+// bytes per block: as many blocks as fit on the device at once (at most one
+// warp per 32-slot tile), or fewer when the launch shape asks.
+template <typename K>
+cudaError_t launch_persistent_bin(K kernel, size_t smem, int* resident, int* sm_count,
+                                  const BinArgs& a, cudaStream_t s) {
+  if (*resident == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_count<KEY64>, kBinThreads,
-                                                           kBinSmem)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBinThreads, smem)) !=
+        cudaSuccess)
       return e;
-    resident = std::max(1, sms * std::max(per_sm, 1));
-    sm_count = std::max(1, sms);
+    *resident = std::max(1, sms * std::max(per_sm, 1));
+    *sm_count = std::max(1, sms);
   }
-  // a launch shape may ask for fewer resident blocks per SM than fit
-  uint32_t want = (uint32_t)resident;
-  if (a.blocks_per_sm) want = std::min<uint32_t>(want, a.blocks_per_sm * (uint32_t)sm_count);
+  uint32_t want = (uint32_t)*resident;
+  if (a.blocks_per_sm) want = std::min<uint32_t>(want, a.blocks_per_sm * (uint32_t)*sm_count);
   const uint32_t tiles = (a.max_n + 31u) / 32u;
   const uint32_t blocks = std::min<uint32_t>(want, (tiles + kBinWarps - 1) / kBinWarps);
-  k_bin_count<KEY64><<<blocks, kBinThreads, kBinSmem, s>>>(a);
+  kernel<<<blocks, kBinThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
   if (a.width >= (1u << 22) || a.height >= (1u << 22)) return cudaErrorInvalidValue;
-  return a.key64 ? launch_bin_count_t<true>(a, s) : launch_bin_count_t<false>(a, s);
+  static int res[4] = {0, 0, 0, 0}, sms[4] = {0, 0, 0, 0};
+  if (a.records) return launch_persistent_bin(k_bin_count<false>, kBinSmem, &res[0], &sms[0], a, s);
+  if (!a.lookback) return cudaErrorInvalidValue;
+  return a.key64 ? launch_persistent_bin(k_bin_direct<true>, kDirSmem, &res[3], &sms[3], a, s)
+                 : launch_persistent_bin(k_bin_direct<false>, kDirSmem, &res[2], &sms[2], a, s);
 }
 
 cudaError_t launch_chunk_counts(const TransposeArgs& a, cudaStream_t s) {
