@@ -329,6 +329,9 @@ struct SortArgs {
   uint32_t radix_bits;   // digit width, 4..8
   uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
                          // (turned into exclusive bases in place by the sort)
+  // true: only pass 0's counts are filled before the sort; the first pass
+  // counts the later passes' digits of the keys it reads (zeroed slots)
+  bool later_hist = false;
   void* status;          // [passes][tiles][radix] zeroed look-back words (when status2 is null)
   void* status2[2];      // optional: two [tiles][radix] look-back buffers used
                          // alternately; each pass clears the one it does not

@@ -593,6 +593,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.tile_ctr = rtiles;
   sa.status_word = &fc->status;
   sa.hist = d_hist;
+  sa.later_hist = !transpose;  // the binning counted the first digit only
   sa.src = 0;
   // The entries' first digit (the low tile bits) differs from lane to lane,
   // so that pass ranks with per-bit ballots; after it a warp's keys mostly

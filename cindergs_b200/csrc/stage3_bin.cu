@@ -633,10 +633,9 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
 //           tiles (saturating sums): the slots' scanned offsets and the tile's
 //           first entry;
 //   write:  the stored masks are walked again and every hit is written at
-//           its place in depth order (key, splat index, 64-bit: depth word);
-//           the tile-digit histograms count pass 0 per entry and the higher
-//           passes per run of lanes with one digit (a splat's row of tiles
-//           shares its high digits), one shared atomic per run.
+//           its place in depth order (key, splat index, 64-bit: depth word)
+//           and counted in a per-warp histogram of the entry sort's first
+//           digit (its first pass counts the later digits).
 // Warps with more candidates than the masks hold test the rest again in the
 // write step. Entries at or beyond the capacity are not written and set the
 // capacity bit.
@@ -661,8 +660,12 @@ struct DirSplats {
   uint32_t mask[kBinWarps][kDirMaskCap];   // hit ballots
   uint32_t mrun[kBinWarps][kDirMaskCap];   // hits before each ballot
 };
+// tile-digit histograms: one per warp when a histogram has at most
+// kDirWarpBins bins (no contention between warps), else one per block
+constexpr uint32_t kDirWarpBins = 256;
 constexpr size_t kDirSmem = sizeof(DirSplats) + sizeof(float4) * kBinWarps * kDirTabCap +
-                            sizeof(uint32_t) * 1024;  // + tile-digit histograms (<= 4 x 256)
+                            sizeof(uint32_t) * kBinWarps * kDirWarpBins;
+static_assert(kBinWarps * kDirWarpBins >= 1024, "a block histogram of 4 x 256 bins fits");
 
 template <bool KEY64>
 __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) {
@@ -672,13 +675,15 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(s_tab + kBinWarps * kDirTabCap);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
-  const uint32_t passes = (a.tile_bits + a.radix_bits - 1u) / a.radix_bits;
   const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
-  const uint32_t nbins = passes * radix;
+  const uint32_t nbins = radix;  // pass 0's digits
   const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
   const uint32_t lw = a.tile_w_log2, lh = a.tile_h_log2;
-  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
+  const bool warp_hist = nbins <= kDirWarpBins;
+  const uint32_t hist_words = warp_hist ? kBinWarps * nbins : nbins;
+  for (uint32_t k = threadIdx.x; k < hist_words; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
+  uint32_t* whist = warp_hist ? s_hist + warp * nbins : s_hist;
   const uint32_t lt = lanemask_lt();
   const uint32_t upto = (2u << lane) - 1u;  // lanes 0 .. lane
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
@@ -879,23 +884,9 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
           overflow = true;
         }
       }
-      // tile-digit histograms: pass 0 per entry; the higher passes per run of
-      // consecutive lanes holding one digit
-      for (uint32_t p = 0; p < passes; ++p) {
-        const uint32_t dg = hit ? (word >> (tshift + p * a.radix_bits)) & rmask : 0xFFFFFFFFu;
-        if (p == 0) {
-          if (hit) atomicAdd(&s_hist[dg], 1u);
-          continue;
-        }
-        const uint32_t prev = __shfl_up_sync(0xffffffffu, dg, 1);
-        const bool first = lane == 0 || dg != prev;
-        const uint32_t bnd = __ballot_sync(0xffffffffu, first);
-        if (hit && first) {
-          const uint32_t after = bnd & ~upto;
-          const uint32_t len = (after ? (uint32_t)(__ffs(after) - 1) : 32u) - (uint32_t)lane;
-          atomicAdd(&s_hist[p * radix + dg], len);
-        }
-      }
+      // the first sort pass's digit (the entry sort's first pass counts the
+      // later passes' digits of the keys it reads)
+      if (hit) atomicAdd(&whist[(word >> tshift) & rmask], 1u);
       hrun += __popc(hits);
       starts += __popc(sb);
     }
@@ -903,7 +894,12 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
   if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
-    const uint32_t v = s_hist[k];
+    uint32_t v = 0;
+    if (warp_hist) {
+      for (int w = 0; w < kBinWarps; ++w) v += s_hist[w * nbins + k];
+    } else {
+      v = s_hist[k];
+    }
     if (v) atomicAdd(&a.hist[k], v);
   }
 }
