@@ -128,20 +128,24 @@ __device__ __forceinline__ uint32_t sat_add_u32(uint32_t a, uint32_t b) {
 // published, 2 = inclusive prefix published; the array must be zeroed before
 // the launch. Tiles must be acquired in increasing order by running blocks
 // (a dynamic tile counter), so every tile a block waits on is held by a block
-// that is already resident. Called by all lanes of ONE warp; returns the
-// exclusive prefix of `tile` and publishes its inclusive prefix (with SAT,
-// sums saturate at 2^32 - 1 instead of wrapping). A wait that exceeds `limit`
-// polls sets kStatusLookbackTimeout and returns 0.
+// that is already resident and publishes its aggregate without waiting.
+// Called by all lanes of ONE warp. chained_publish publishes the tile's
+// aggregate (tile 0: its inclusive prefix); chained_resolve then walks back
+// for its exclusive prefix, publishes the inclusive one and returns the
+// exclusive one (with SAT, sums saturate at 2^32 - 1 instead of wrapping). A
+// wait that exceeds `limit` polls sets kStatusLookbackTimeout and returns 0.
+__device__ __forceinline__ void chained_publish(unsigned long long* status, uint32_t tile,
+                                                uint32_t aggregate) {
+  if ((threadIdx.x & 31) == 0)
+    st_relaxed_u64(&status[tile], ((tile == 0 ? 2ull : 1ull) << 32) | aggregate);
+}
+
 template <bool SAT = false>
-__device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status, uint32_t tile,
-                                                      uint32_t aggregate, uint32_t* status_word,
-                                                      uint32_t limit = kSpinLimit) {
+__device__ __forceinline__ uint32_t chained_resolve(unsigned long long* status, uint32_t tile,
+                                                    uint32_t aggregate, uint32_t* status_word,
+                                                    uint32_t limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
-  if (tile == 0) {
-    if (lane == 0) st_relaxed_u64(&status[0], (2ull << 32) | aggregate);
-    return 0u;
-  }
-  if (lane == 0) st_relaxed_u64(&status[tile], (1ull << 32) | aggregate);
+  if (tile == 0) return 0u;
   uint32_t exclusive = 0;
   long long pred = (long long)tile - 1;
   uint32_t spins = 0;
@@ -180,6 +184,14 @@ __device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status
     st_relaxed_u64(&status[tile], (2ull << 32) | (SAT ? sat_add_u32(exclusive, aggregate)
                                                       : exclusive + aggregate));
   return exclusive;
+}
+
+template <bool SAT = false>
+__device__ __forceinline__ uint32_t chained_scan_warp(unsigned long long* status, uint32_t tile,
+                                                      uint32_t aggregate, uint32_t* status_word,
+                                                      uint32_t limit = kSpinLimit) {
+  chained_publish(status, tile, aggregate);
+  return chained_resolve<SAT>(status, tile, aggregate, status_word, limit);
 }
 
 }  // namespace cgs

@@ -248,6 +248,11 @@ struct BinArgs {
   uint32_t* offsets;            // [max_n]
   // direct mode: look-back words of the 32-slot tiles' hit counts, zeroed
   unsigned long long* lookback; // [ceil(max_n/32)]
+  // direct mode: two scratch runs of run_cap staged entries (keys, splat
+  // indices, depth words) per counting warp of the grid:
+  // kBinDirectRunWarpsPerSm x SMs x 2 x 3 x run_cap words
+  uint32_t* run_scratch;
+  uint32_t run_cap;
   // record mode: staging start and records of each 32-slot tile and group
   uint32_t* tile_stage;
   uint32_t* tile_count;
@@ -278,6 +283,11 @@ struct BinArgs {
 // record mode it stages one record per hit and leaves the per-slot counts
 // for a scan (launch_scan_u32).
 cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s);
+// Direct-mode grid bound: blocks per SM and counting warps per block (the
+// scratch runs of BinArgs are sized for them).
+constexpr uint32_t kBinDirectMaxBlocksPerSm = 2;
+constexpr uint32_t kBinDirectRunWarpsPerSm = kBinDirectMaxBlocksPerSm * 8;
+constexpr uint32_t kBinDirectRunCap = 2048;
 // Tile transpose (the entry sort when the tiles fit shared memory): a
 // one-pass stable counting sort of the staged records by tile. Chunk k is the
 // 32-slot tiles [k * chunk_wtiles, (k + 1) * chunk_wtiles); warp w of a chunk

@@ -198,6 +198,7 @@ struct cgs_ctx {
   // arena
   DevBuf tet_J, tet_R, tet_S, def_pos, def_cova, def_covb, split_meta, persist;
   DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
+  DevBuf bin_runs;  // the direct binning's per-warp scratch runs
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
   // SH coefficient rotation (cgs_sh_rotate, cgs_export_deformed): the band
@@ -520,6 +521,16 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   // (first entries, entry total).
   const uint32_t nwt = (d.max_n + 31) / 32;
   b.lookback = reinterpret_cast<unsigned long long*>(b.tile_stage + 2 * (size_t)nwt);
+  if (!transpose) {
+    int sms = 0;
+    CGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device),
+             "device attribute");
+    CGS_TRY(ctx->ensure(ctx->bin_runs,
+                        (size_t)sms * kBinDirectRunWarpsPerSm * 2 * 3 * kBinDirectRunCap * 4,
+                        "binning scratch runs"));
+    b.run_scratch = ctx->bin_runs.as<uint32_t>();
+    b.run_cap = kBinDirectRunCap;
+  }
   ctx->kbegin(CGS_K_BIN);
   CGS_CUDA(launch_bin_count(b, s), "bin count launch");
   if (transpose) {
