@@ -248,11 +248,6 @@ struct BinArgs {
   uint32_t* offsets;            // [max_n]
   // direct mode: look-back words of the 32-slot tiles' hit counts, zeroed
   unsigned long long* lookback; // [ceil(max_n/32)]
-  // direct mode: two scratch runs of run_cap staged entries (keys, splat
-  // indices, depth words) per counting warp of the grid:
-  // kBinDirectRunWarpsPerSm x SMs x 2 x 3 x run_cap words
-  uint32_t* run_scratch;
-  uint32_t run_cap;
   // record mode: staging start and records of each 32-slot tile and group
   uint32_t* tile_stage;
   uint32_t* tile_count;
@@ -283,11 +278,6 @@ struct BinArgs {
 // record mode it stages one record per hit and leaves the per-slot counts
 // for a scan (launch_scan_u32).
 cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s);
-// Direct-mode grid bound: blocks per SM and counting warps per block (the
-// scratch runs of BinArgs are sized for them).
-constexpr uint32_t kBinDirectMaxBlocksPerSm = 2;
-constexpr uint32_t kBinDirectRunWarpsPerSm = kBinDirectMaxBlocksPerSm * 8;
-constexpr uint32_t kBinDirectRunCap = 2048;
 // Tile transpose (the entry sort when the tiles fit shared memory): a
 // one-pass stable counting sort of the staged records by tile. Chunk k is the
 // 32-slot tiles [k * chunk_wtiles, (k + 1) * chunk_wtiles); warp w of a chunk
@@ -318,6 +308,9 @@ cudaError_t launch_chunk_place(const TransposeArgs& a, cudaStream_t s);
 
 // Per-tile [start, end) from sorted words: tile = word >> shift, over
 // min(*n_ptr, capacity) words. ranges zeroed.
+// Turns the last sort pass's range words (complemented first entries, ends)
+// into [first, end) per screen tile; empty tiles stay (0, 0).
+cudaError_t launch_ranges_fixup(uint32_t* ranges, uint32_t num_tiles, cudaStream_t s);
 cudaError_t launch_tile_ranges(const uint32_t* sorted, uint32_t shift, const uint32_t* n_ptr,
                                uint32_t capacity, uint32_t total_tiles, uint32_t* ranges,
                                uint32_t blocks, cudaStream_t s);
@@ -342,6 +335,12 @@ struct SortArgs {
   // true: only pass 0's counts are filled before the sort; the first pass
   // counts the later passes' digits of the keys it reads (zeroed slots)
   bool later_hist = false;
+  // optional: the last pass also finds the [first, end) entries of every
+  // screen tile (key >> tile_shift) into ranges[2 t], ranges[2 t + 1]
+  // (zeroed before the sort; finish with launch_ranges_fixup)
+  uint32_t* ranges = nullptr;
+  uint32_t tile_shift = 0;
+  uint32_t num_tiles = 0;
   void* status;          // [passes][tiles][radix] zeroed look-back words (when status2 is null)
   void* status2[2];      // optional: two [tiles][radix] look-back buffers used
                          // alternately; each pass clears the one it does not

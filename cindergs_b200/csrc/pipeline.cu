@@ -198,7 +198,6 @@ struct cgs_ctx {
   // arena
   DevBuf tet_J, tet_R, tet_S, def_pos, def_cova, def_covb, split_meta, persist;
   DevBuf recs, offsets, scratch, ranges, keys[2], ids[2], depths[2], radix_lb[2];
-  DevBuf bin_runs;  // the direct binning's per-warp scratch runs
   DevBuf fb_rgba8, fb_f32;
   DevBuf prim[4];  // scratch for the stand-alone scan/sort entry points
   // SH coefficient rotation (cgs_sh_rotate, cgs_export_deformed): the band
@@ -521,16 +520,6 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   // (first entries, entry total).
   const uint32_t nwt = (d.max_n + 31) / 32;
   b.lookback = reinterpret_cast<unsigned long long*>(b.tile_stage + 2 * (size_t)nwt);
-  if (!transpose) {
-    int sms = 0;
-    CGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device),
-             "device attribute");
-    CGS_TRY(ctx->ensure(ctx->bin_runs,
-                        (size_t)sms * kBinDirectRunWarpsPerSm * 2 * 3 * kBinDirectRunCap * 4,
-                        "binning scratch runs"));
-    b.run_scratch = ctx->bin_runs.as<uint32_t>();
-    b.run_cap = kBinDirectRunCap;
-  }
   ctx->kbegin(CGS_K_BIN);
   CGS_CUDA(launch_bin_count(b, s), "bin count launch");
   if (transpose) {
@@ -605,6 +594,13 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.status_word = &fc->status;
   sa.hist = d_hist;
   sa.later_hist = !transpose;  // the binning counted the first digit only
+  // the last pass finds the tile ranges (the ranges were zeroed above)
+  const bool pass_ranges = *passes > 0;
+  if (pass_ranges) {
+    sa.ranges = ctx->ranges.as<uint32_t>();
+    sa.tile_shift = d.key64 ? 0u : d.depth_bits;
+    sa.num_tiles = d.total_tiles;
+  }
   sa.src = 0;
   // The entries' first digit (the low tile bits) differs from lane to lane,
   // so that pass ranks with per-bit ballots; after it a warp's keys mostly
@@ -615,10 +611,13 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   if (sort_launches) *sort_launches = 1 + *passes;
   ctx->kend();
   ctx->kbegin(CGS_K_TILE_RANGES);
-  CGS_CUDA(launch_tile_ranges(ctx->keys[*result_src].as<uint32_t>(), d.key64 ? 0u : d.depth_bits,
-                              n_ptr, ctx->entry_cap, d.total_tiles, ctx->ranges.as<uint32_t>(),
-                              ctx->shape.ranges_blocks, s),
-           "ranges launch");
+  if (pass_ranges)
+    CGS_CUDA(launch_ranges_fixup(ctx->ranges.as<uint32_t>(), d.total_tiles, s), "ranges fix-up");
+  else
+    CGS_CUDA(launch_tile_ranges(ctx->keys[*result_src].as<uint32_t>(), d.key64 ? 0u : d.depth_bits,
+                                n_ptr, ctx->entry_cap, d.total_tiles, ctx->ranges.as<uint32_t>(),
+                                ctx->shape.ranges_blocks, s),
+             "ranges launch");
   ctx->kend();
   return CGS_OK;
 }

@@ -95,6 +95,12 @@ struct PassArgs {
   uint32_t* later_hist;
   uint32_t later_passes;
   uint32_t num_bits;
+  // last pass of a sort with ranges: per screen tile (key >> tile_shift,
+  // below num_tiles), atomicMax of the complemented first entry and of the
+  // end of every run of one tile in this block's output
+  uint32_t* ranges;
+  uint32_t tile_shift;
+  uint32_t num_tiles;
 };
 
 // Exclusive prefix of digit d over the tiles before `tile`: walks back from
@@ -318,6 +324,25 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
       bad = true;
       continue;
     }
+    if (a.ranges) {
+      // runs of one tile are contiguous here (one digit run, in input order,
+      // which the earlier passes sorted by the lower tile bits) and in the
+      // output (the run's positions are consecutive)
+      const uint32_t t = a.tile_shift >= 32u ? 0u : key >> a.tile_shift;
+      bool first = i == 0, last = i + 1 == tile_valid;
+      if (!first) {
+        const uint32_t pk = s_keys[padded(i - 1)];
+        first = (a.tile_shift >= 32u ? 0u : pk >> a.tile_shift) != t;
+      }
+      if (!last) {
+        const uint32_t nk = s_keys[padded(i + 1)];
+        last = (a.tile_shift >= 32u ? 0u : nk >> a.tile_shift) != t;
+      }
+      if (t < a.num_tiles) {
+        if (first) atomicMax(&a.ranges[2 * (size_t)t], ~g);
+        if (last) atomicMax(&a.ranges[2 * (size_t)t + 1], g + 1u);
+      }
+    }
     a.keys_out[g] = key;
     a.v0_out[g] = s_v0[padded(i)];
     if (PAY2) a.v1_out[g] = s_v1[padded(i)];
@@ -473,6 +498,9 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.tile_ctr = a.tile_ctr + p;
     pa.status_word = a.status_word;
     pa.rank = ((a.smem_mask >> p) & 1u) ? kRankSmem : (((a.ballot_mask >> p) & 1u) ? kRankBallot : kRankMatch);
+    pa.ranges = p + 1 == passes ? a.ranges : nullptr;
+    pa.tile_shift = a.tile_shift;
+    pa.num_tiles = a.num_tiles;
     pa.later_hist = later && p == 0 ? a.hist + R : nullptr;
     pa.later_passes = later && p == 0 ? passes - 1 : 0u;
     pa.num_bits = a.num_bits;

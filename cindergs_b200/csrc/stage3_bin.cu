@@ -628,28 +628,17 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
 //           column-only and row-only parts);
 //   count:  32 candidates per step, one per lane, ~20 rounded operations
 //           each against the tables (the whole test when the tables do not
-//           fit); the ballot masks and the hits before each are kept, and
-//           each hit's key and splat index are staged in the warp's scratch
-//           run (global memory, L2-resident), in candidate order (= the
-//           reference's emission order: splat by splat, row-major);
-//   scan:   the tile's hit count is published at once for a decoupled
-//           look-back over the 32-slot tiles (saturating sums), and the tile
-//           is handed to the block's resolver warp, while the counting warp
-//           takes its next tile;
-//   resolve: a ninth warp per block walks back for each handed tile's first
-//           entry (its tiles in increasing order, as soon as they are
-//           counted), copies the staged run to its place in depth order (keys,
-//           splat indices; 64-bit keys: depth words), writes the slots'
-//           scanned offsets and counts the entry sort's first digit (its first
-//           pass counts the later digits), then frees the run.
-// So the counting warps never wait on other tiles: a counting warp waits
-// only for one of its two scratch runs to be free, and only before it takes a
-// tile; the resolver waits only on the counts of tiles already taken, whose
-// warps publish them without waiting (no cycle). A tile with more hits than a
-// scratch run holds is finished by its own warp (look-back, then a second walk
-// over its stored ballots; warps with more candidates than the ballots hold
-// test the rest again there). Entries at or beyond the capacity are not
-// written and set the capacity bit.
+//           fit); the ballot masks and the hits before each are kept;
+//   scan:   the tile's hit count enters a decoupled look-back over the 32-slot
+//           tiles (saturating sums): the slots' scanned offsets and the tile's
+//           first entry;
+//   write:  the stored masks are walked again and every hit is written at
+//           its place in depth order (key, splat index, 64-bit: depth word)
+//           and counted in a per-warp histogram of the entry sort's first
+//           digit (its first pass counts the later digits).
+// Warps with more candidates than the masks hold test the rest again in the
+// write step. Entries at or beyond the capacity are not written and set the
+// capacity bit.
 constexpr int kDirMaskCap = 96;   // stored ballot masks per warp (3,072 candidates)
 constexpr int kDirTabCap = 448;   // term-table entries per warp
 
@@ -670,19 +659,16 @@ struct DirSplats {
   uint32_t sbits[kBinWarps][kDirMaskCap];  // start bit per splat's first candidate
   uint32_t mask[kBinWarps][kDirMaskCap];   // hit ballots
   uint32_t mrun[kBinWarps][kDirMaskCap];   // hits before each ballot
-  // hand-off of counted tiles to the resolver: per counting warp and run
-  uint32_t q_tile[kBinWarps][2];
-  uint32_t q_run[kBinWarps][2];
-  uint32_t q_state[kBinWarps][2];          // 0 free, 1 handed over
-  uint32_t q_count[kBinWarps][2][32];      // the tile's slot counts
-  uint32_t done;                           // counting warps that have finished
 };
-constexpr int kDirThreads = kBinThreads + 32;  // eight counting warps + the resolver
+// tile-digit histograms: one per warp when a histogram has at most
+// kDirWarpBins bins (no contention between warps), else one per block
+constexpr uint32_t kDirWarpBins = 256;
 constexpr size_t kDirSmem = sizeof(DirSplats) + sizeof(float4) * kBinWarps * kDirTabCap +
-                            sizeof(uint32_t) * 256;  // + the first digit's histogram
+                            sizeof(uint32_t) * kBinWarps * kDirWarpBins;
+static_assert(kBinWarps * kDirWarpBins >= 1024, "a block histogram of 4 x 256 bins fits");
 
 template <bool KEY64>
-__global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) {
+__global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) {
   extern __shared__ __align__(16) unsigned char dir_smem[];
   DirSplats& sp = *reinterpret_cast<DirSplats*>(dir_smem);
   float4* s_tab = reinterpret_cast<float4*>(dir_smem + sizeof(DirSplats));  // [w][kDirTabCap]
@@ -690,146 +676,26 @@ __global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
   const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
+  const uint32_t nbins = radix;  // pass 0's digits
   const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
   const uint32_t lw = a.tile_w_log2, lh = a.tile_h_log2;
-  for (uint32_t k = threadIdx.x; k < radix; k += kDirThreads) s_hist[k] = 0u;
-  if (threadIdx.x < kBinWarps * 2) (&sp.q_state[0][0])[threadIdx.x] = 0u;
-  if (threadIdx.x == 0) sp.done = 0u;
+  const bool warp_hist = nbins <= kDirWarpBins;
+  const uint32_t hist_words = warp_hist ? kBinWarps * nbins : nbins;
+  for (uint32_t k = threadIdx.x; k < hist_words; k += kBinThreads) s_hist[k] = 0u;
   __syncthreads();
+  uint32_t* whist = warp_hist ? s_hist + warp * nbins : s_hist;
   const uint32_t lt = lanemask_lt();
   const uint32_t upto = (2u << lane) - 1u;  // lanes 0 .. lane
-  const uint32_t num_tiles = (a.max_n + 31u) / 32u;
-  const uint32_t cap = a.entry_cap;
-  const uint32_t wcap = a.run_cap;  // entries of a scratch run
-  bool overflow = false;
-  volatile uint32_t* q_state = &sp.q_state[0][0];
-
-  // Look-back, offsets and the entry total of a counted tile (all lanes of a
-  // warp); returns its first entry.
-  auto resolve = [&](uint32_t tile, uint32_t run, uint32_t count) -> uint32_t {
-    const uint32_t wexcl = chained_resolve<true>(a.lookback, tile, run, &a.fc->status);
-    uint32_t cincl = count;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, cincl, o);
-      if (lane >= o) cincl += y;
-    }
-    const uint32_t s = tile * 32u + (uint32_t)lane;
-    if (s < a.max_n) a.offsets[s] = sat_add_u32(wexcl, cincl - count);
-    if (tile == num_tiles - 1u && lane == 0) a.fc->entries = sat_add_u32(wexcl, run);
-    return wexcl;
-  };
-  auto put = [&](uint64_t pos, uint32_t word, uint32_t id, uint32_t d) {
-    if (pos < cap) {
-      a.keys[pos] = word;
-      a.ids[pos] = id;
-      if (KEY64) a.depths[pos] = d;
-    } else {
-      overflow = true;
-    }
-    atomicAdd(&s_hist[(word >> tshift) & rmask], 1u);
-  };
-
-  if (warp == kBinWarps) {
-    // ---- the resolver: handed tiles in increasing order
-    uint32_t spins = 0;
-    for (;;) {
-      const uint32_t st = lane < kBinWarps * 2 ? q_state[lane] : 0u;
-      const uint32_t ready = __ballot_sync(0xffffffffu, st == 1u);
-      if (!ready) {
-        const uint32_t fin = *(volatile uint32_t*)&sp.done;
-        __threadfence_block();
-        const uint32_t again = __ballot_sync(
-            0xffffffffu, lane < kBinWarps * 2 && q_state[lane] == 1u);
-        if (fin == (uint32_t)kBinWarps && !again) break;
-        if (!again) {
-          if (++spins > kSpinLimit) {
-            if (lane == 0) atomicOr(&a.fc->status, kStatusLookbackTimeout);
-            break;
-          }
-          __nanosleep(64);
-        }
-        continue;
-      }
-      spins = 0;
-      __threadfence_block();
-      // the handed tile with the smallest number
-      uint32_t key = ((ready >> lane) & 1u) ? (&sp.q_tile[0][0])[lane] : 0xFFFFFFFFu;
-      uint32_t best = key;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
-      const int q = __ffs(__ballot_sync(0xffffffffu, key == best)) - 1;  // slot: warp q / 2, run q % 2
-      const uint32_t tile = best, run = (&sp.q_run[0][0])[q];
-      const uint32_t count = sp.q_count[q >> 1][q & 1][lane];
-      const uint32_t wexcl = resolve(tile, run, count);
-      const uint32_t* sk = a.run_scratch +
-                           ((size_t)(blockIdx.x * kBinWarps + (q >> 1)) * 2u + (q & 1)) * 3u * wcap;
-      const uint32_t* si = sk + wcap;
-      const uint32_t* sd = si + wcap;
-      for (uint32_t k0 = 0; k0 < run; k0 += 128) {
-        uint32_t kw[4], iw[4], dw[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const uint32_t k = k0 + 32u * u + (uint32_t)lane;
-          if (k < run) {
-            kw[u] = __ldcg(sk + k);
-            iw[u] = __ldcg(si + k);
-            dw[u] = KEY64 ? __ldcg(sd + k) : 0u;
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const uint32_t k = k0 + 32u * u + (uint32_t)lane;
-          if (k < run) put((uint64_t)wexcl + k, kw[u], iw[u], dw[u]);
-        }
-      }
-      __syncwarp();
-      if (lane == 0) {
-        __threadfence_block();
-        q_state[q] = 0u;  // the run may be refilled
-      }
-    }
-    if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
-    __syncthreads();  // every counting warp has finished (their overflow writes counted too)
-    for (uint32_t k = (uint32_t)lane; k < radix; k += 32)
-      if (s_hist[k]) atomicAdd(&a.hist[k], s_hist[k]);
-    return;
-  }
-
-  // ---- the counting warps
   const uint32_t active = a.n_rest + (a.split_count ? *a.split_count : 0u);
+  const uint32_t num_tiles = (a.max_n + 31u) / 32u;
   const uint32_t* wbase = sp.base[warp];
   float4* wtab = s_tab + warp * kDirTabCap;
   uint32_t* wmask = sp.mask[warp];
   uint32_t* wmrun = sp.mrun[warp];
-  uint32_t* const wscr = a.run_scratch + ((size_t)blockIdx.x * kBinWarps + warp) * 2u * 3u * (size_t)wcap;
-  uint32_t buf = 0;
-  bool gave_up = false;
+  const uint32_t cap = a.entry_cap;
+  bool overflow = false;
+
   for (;;) {
-    // a free scratch run, before taking a tile (a warp holding a tile never
-    // waits before publishing its count)
-    {
-      uint32_t spins = 0;
-      bool freed = false;
-      for (;;) {
-        if (lane == 0) freed = q_state[warp * 2 + buf] == 0u;
-        freed = __shfl_sync(0xffffffffu, freed, 0);
-        if (freed) break;
-        if (lane == 0) freed = q_state[warp * 2 + (buf ^ 1u)] == 0u;
-        freed = __shfl_sync(0xffffffffu, freed, 0);
-        if (freed) {
-          buf ^= 1u;
-          break;
-        }
-        if (++spins > kSpinLimit) break;
-        __nanosleep(64);
-      }
-      if (!freed) {
-        gave_up = true;
-        break;
-      }
-      __threadfence_block();
-    }
     uint32_t tile = 0;
     if (lane == 0) tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
     tile = __shfl_sync(0xffffffffu, tile, 0);
@@ -915,13 +781,12 @@ __global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) 
     auto owner = [&](uint32_t item, uint32_t sb, uint32_t starts) -> int {
       return big ? find_owner(wbase, item) : (int)sp.lor[warp][starts + __popc(sb & upto) - 1u];
     };
-    // the test of candidate item of splat o; tile_id its screen tile
-    auto test = [&](int o, uint32_t item, uint32_t& tile_id) -> bool {
+    // the test of candidate item of splat o; r, c its row and column in the box
+    auto test = [&](int o, uint32_t item, uint32_t& r, uint32_t& c) -> bool {
       const uint4 ow = sp.own[warp][o];
       const uint32_t ci = item - ow.x;
-      const uint32_t r = ow.y ? __umulhi(ci, ow.y) : ci;
-      const uint32_t c = ci - r * ow.z;
-      tile_id = ow.w + r * a.tiles_x + c;
+      r = ow.y ? __umulhi(ci, ow.y) : ci;
+      c = ci - r * ow.z;
       if (tab) {
         const uint2 t = sp.tb[warp][o];
         return tab_hit(wtab[t.x + c], wtab[t.y + r], sp.kq[warp][o]);
@@ -930,15 +795,8 @@ __global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) 
       return tile_hit(xy.x + c, xy.y + r, wm1, hm1, lw, lh, sp.geo[warp][o], sp.con[warp][o],
                       sp.rcp[warp][o], sp.kq[warp][o].w);
     };
-    auto key_word = [&](int o, uint32_t tile_id, uint32_t& d) -> uint32_t {
-      d = sp.dq[warp][o];
-      return KEY64 ? tile_id : (a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d));
-    };
 
-    // ---- count, staging the hits in scratch run `buf`
-    uint32_t* sk = wscr + (size_t)buf * 3u * wcap;
-    uint32_t* si = sk + wcap;
-    uint32_t* sd = si + wcap;
+    // ---- count
     uint32_t run = 0;     // hits before the current chunk (warp-uniform)
     uint32_t own = 0;     // this lane's hits, accumulated only when `big`
     uint32_t starts = 0;  // splats starting before the current chunk
@@ -947,25 +805,14 @@ __global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) 
       const uint32_t item = chunk + lane;
       const uint32_t sb = big ? 0u : sp.sbits[warp][c];
       bool hit = false;
-      int o = 0;
-      uint32_t tile_id = 0;
       if (item < total) {
-        o = owner(item, sb, starts);
-        hit = test(o, item, tile_id);
+        uint32_t r, cc;
+        hit = test(owner(item, sb, starts), item, r, cc);
       }
       const uint32_t hits = __ballot_sync(0xffffffffu, hit);
       if (lane == 0 && c < (uint32_t)kDirMaskCap) {
         wmask[c] = hits;
         wmrun[c] = run;
-      }
-      if (hit) {
-        const uint32_t k = run + __popc(hits & lt);
-        if (k < wcap) {
-          uint32_t d;
-          sk[k] = key_word(o, tile_id, d);
-          si[k] = sp.sid[warp][o];
-          if (KEY64) sd[k] = d;
-        }
       }
       if (big) {
         const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
@@ -988,27 +835,23 @@ __global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) 
       count = (lane == 31 ? run : next) - before;
     }
 
-    // ---- scan: publish the count now; the resolver walks back for it
-    chained_publish(a.lookback, tile, run);
-    if (run <= wcap) {
-      sp.q_count[warp][buf][lane] = count;
-      if (lane == 0) {
-        sp.q_tile[warp][buf] = tile;
-        sp.q_run[warp][buf] = run;
+    // ---- scan
+    const uint32_t wexcl = chained_scan_warp<true>(a.lookback, tile, run, &a.fc->status);
+    {
+      uint32_t cincl2 = count;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, cincl2, o);
+        if (lane >= o) cincl2 += y;
       }
-      __syncwarp();
-      if (lane == 0) {
-        __threadfence_block();
-        q_state[warp * 2 + buf] = 1u;
-      }
-      buf ^= 1u;
-      continue;
+      if (s < a.max_n) a.offsets[s] = sat_add_u32(wexcl, cincl2 - count);
+      if (tile == num_tiles - 1u && lane == 0) a.fc->entries = sat_add_u32(wexcl, run);
     }
-    // More hits than a scratch run holds: finish this tile here, from its
-    // stored ballots (and tests beyond them).
-    const uint32_t wexcl = resolve(tile, run, count);
+
+    // ---- write
     uint32_t hrun = 0;
     starts = 0;
+#pragma unroll 2
     for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
       const uint32_t item = chunk + lane;
       const uint32_t sb = big ? 0u : sp.sbits[warp][c];
@@ -1018,31 +861,49 @@ __global__ void __launch_bounds__(kDirThreads, 2) k_bin_direct(const BinArgs a) 
       } else {
         bool h = false;
         if (item < total) {
-          uint32_t tid_;
-          h = test(owner(item, sb, starts), item, tid_);
+          uint32_t r, cc;
+          h = test(owner(item, sb, starts), item, r, cc);
         }
         hits = __ballot_sync(0xffffffffu, h);
       }
-      if ((hits >> lane) & 1u) {
+      const bool hit = (hits >> lane) & 1u;
+      uint32_t word = 0;
+      if (hit) {
         const int o = owner(item, sb, starts);
-        uint32_t tile_id;
-        test(o, item, tile_id);
-        uint32_t d;
-        const uint32_t word = key_word(o, tile_id, d);
-        put((uint64_t)wexcl + hrun + __popc(hits & lt), word, sp.sid[warp][o], d);
+        const uint4 ow = sp.own[warp][o];
+        const uint32_t ci = item - ow.x;
+        const uint32_t r = ow.y ? __umulhi(ci, ow.y) : ci;
+        const uint32_t cc = ci - r * ow.z;
+        const uint32_t tile_id = ow.w + r * a.tiles_x + cc;
+        const uint32_t d = sp.dq[warp][o];
+        word = KEY64 ? tile_id : (a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d));
+        const uint64_t pos = (uint64_t)wexcl + hrun + __popc(hits & lt);
+        if (pos < cap) {
+          a.keys[pos] = word;
+          a.ids[pos] = sp.sid[warp][o];
+          if (KEY64) a.depths[pos] = d;
+        } else {
+          overflow = true;
+        }
       }
+      // the first sort pass's digit (the entry sort's first pass counts the
+      // later passes' digits of the keys it reads)
+      if (hit) atomicAdd(&whist[(word >> tshift) & rmask], 1u);
       hrun += __popc(hits);
       starts += __popc(sb);
     }
   }
-  if (gave_up && lane == 0) atomicOr(&a.fc->status, kStatusLookbackTimeout);
   if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
-  __syncwarp();
-  if (lane == 0) {
-    __threadfence_block();
-    atomicAdd(&sp.done, 1u);
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
+    uint32_t v = 0;
+    if (warp_hist) {
+      for (int w = 0; w < kBinWarps; ++w) v += s_hist[w * nbins + k];
+    } else {
+      v = s_hist[k];
+    }
+    if (v) atomicAdd(&a.hist[k], v);
   }
-  __syncthreads();  // the resolver's histogram flush follows this barrier
 }
 
 // ---- Tile transpose ---------------------------------------------------------
@@ -1290,6 +1151,15 @@ __global__ void k_tile_ranges(const uint32_t* __restrict__ sorted, uint32_t shif
   }
 }
 
+// [first, end) of every screen tile from the last sort pass's words:
+// ranges[2 t] = ~first (0 when the tile is empty), ranges[2 t + 1] = end.
+__global__ void k_ranges_fixup(uint32_t* __restrict__ ranges, uint32_t num_tiles) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= num_tiles) return;
+  const uint32_t x = ranges[2 * (size_t)t];
+  if (x != 0u) ranges[2 * (size_t)t] = ~x;
+}
+
 // Generic single-pass exclusive scan: 4096 elements per tile (16 per thread,
 // blocked), chained across tiles.
 constexpr int kScanThreads = 256;
@@ -1354,15 +1224,15 @@ cudaError_t launch_drill_chained_scan(unsigned long long* status, uint32_t* stat
 // bytes per block: as many blocks as fit on the device at once (at most one
 // warp per 32-slot tile), or fewer when the launch shape asks.
 template <typename K>
-cudaError_t launch_persistent_bin(K kernel, int threads, size_t smem, int* resident,
-                                  int* sm_count, const BinArgs& a, cudaStream_t s) {
+cudaError_t launch_persistent_bin(K kernel, size_t smem, int* resident, int* sm_count,
+                                  const BinArgs& a, cudaStream_t s) {
   if (*resident == 0) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem)) !=
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBinThreads, smem)) !=
         cudaSuccess)
       return e;
     *resident = std::max(1, sms * std::max(per_sm, 1));
@@ -1371,10 +1241,8 @@ cudaError_t launch_persistent_bin(K kernel, int threads, size_t smem, int* resid
   uint32_t want = (uint32_t)*resident;
   if (a.blocks_per_sm) want = std::min<uint32_t>(want, a.blocks_per_sm * (uint32_t)*sm_count);
   const uint32_t tiles = (a.max_n + 31u) / 32u;
-  uint32_t blocks = std::min<uint32_t>(want, (tiles + kBinWarps - 1) / kBinWarps);
-  // the direct kernel's scratch runs are sized for kBinDirectMaxBlocksPerSm
-  if (a.run_scratch) blocks = std::min<uint32_t>(blocks, kBinDirectMaxBlocksPerSm * (uint32_t)*sm_count);
-  kernel<<<blocks, threads, smem, s>>>(a);
+  const uint32_t blocks = std::min<uint32_t>(want, (tiles + kBinWarps - 1) / kBinWarps);
+  kernel<<<blocks, kBinThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -1382,11 +1250,10 @@ cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
   if (a.width >= (1u << 22) || a.height >= (1u << 22)) return cudaErrorInvalidValue;
   static int res[4] = {0, 0, 0, 0}, sms[4] = {0, 0, 0, 0};
-  if (a.records)
-    return launch_persistent_bin(k_bin_count<false>, kBinThreads, kBinSmem, &res[0], &sms[0], a, s);
-  if (!a.lookback || !a.run_scratch || a.run_cap == 0) return cudaErrorInvalidValue;
-  return a.key64 ? launch_persistent_bin(k_bin_direct<true>, kDirThreads, kDirSmem, &res[3], &sms[3], a, s)
-                 : launch_persistent_bin(k_bin_direct<false>, kDirThreads, kDirSmem, &res[2], &sms[2], a, s);
+  if (a.records) return launch_persistent_bin(k_bin_count<false>, kBinSmem, &res[0], &sms[0], a, s);
+  if (!a.lookback) return cudaErrorInvalidValue;
+  return a.key64 ? launch_persistent_bin(k_bin_direct<true>, kDirSmem, &res[3], &sms[3], a, s)
+                 : launch_persistent_bin(k_bin_direct<false>, kDirSmem, &res[2], &sms[2], a, s);
 }
 
 cudaError_t launch_chunk_counts(const TransposeArgs& a, cudaStream_t s) {
@@ -1409,6 +1276,12 @@ cudaError_t launch_chunk_place(const TransposeArgs& a, cudaStream_t s) {
       a.chunk_wtiles % kPlaceWarps != 0 || a.chunk_wtiles > 2040u)
     return cudaErrorInvalidValue;
   k_chunk_place<<<dim3(a.num_chunks, a.groups), kPlaceWarps * 32, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ranges_fixup(uint32_t* ranges, uint32_t num_tiles, cudaStream_t s) {
+  if (num_tiles == 0) return cudaSuccess;
+  k_ranges_fixup<<<(num_tiles + 255) / 256, 256, 0, s>>>(ranges, num_tiles);
   return cudaGetLastError();
 }
 
