@@ -588,7 +588,10 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.radix_bits = d.radix_bits;
   sa.status2[0] = ctx->radix_lb[0].p;
   sa.status2[1] = ctx->radix_lb[1].p;
-  sa.wide_lookback = true;  // frames may hold more than 2^30 tile entries
+  // 64-bit look-back words only when the buffers may hold more than 2^30
+  // entries (32-bit words carry 30-bit counts); the width follows the
+  // capacity, whose every change clears the look-back buffers
+  sa.wide_lookback = ctx->entry_cap > (1u << 30);
   sa.parity = &ctx->radix_parity;
   sa.tile_ctr = rtiles;
   sa.status_word = &fc->status;
