@@ -634,8 +634,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
 //           first entry;
 //   write:  the stored masks are walked again and every hit is written at
 //           its place in depth order (key, splat index, 64-bit: depth word)
-//           and counted in a per-warp histogram of the entry sort's first
-//           digit (its first pass counts the later digits).
+//           and counted in per-warp histograms of the entry sort's digits.
 // Warps with more candidates than the masks hold test the rest again in the
 // write step. Entries at or beyond the capacity are not written and set the
 // capacity bit.
@@ -676,7 +675,8 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
   const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
-  const uint32_t nbins = radix;  // pass 0's digits
+  const uint32_t passes = (a.tile_bits + a.radix_bits - 1u) / a.radix_bits;
+  const uint32_t nbins = passes * radix;
   const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
   const uint32_t lw = a.tile_w_log2, lh = a.tile_h_log2;
   const bool warp_hist = nbins <= kDirWarpBins;
@@ -886,9 +886,12 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
           overflow = true;
         }
       }
-      // the first sort pass's digit (the entry sort's first pass counts the
-      // later passes' digits of the keys it reads)
-      if (hit) atomicAdd(&whist[(word >> tshift) & rmask], 1u);
+      // the entry sort's digits (per-warp histograms)
+      if (hit) {
+        atomicAdd(&whist[(word >> tshift) & rmask], 1u);
+        for (uint32_t p = 1; p < passes; ++p)
+          atomicAdd(&whist[p * radix + ((word >> (tshift + p * a.radix_bits)) & rmask)], 1u);
+      }
       hrun += __popc(hits);
       starts += __popc(sb);
     }
