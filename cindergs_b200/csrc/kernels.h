@@ -332,9 +332,6 @@ struct SortArgs {
   uint32_t radix_bits;   // digit width, 4..8
   uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
                          // (turned into exclusive bases in place by the sort)
-  // true: only pass 0's counts are filled before the sort; the first pass
-  // counts the later passes' digits of the keys it reads (zeroed slots)
-  bool later_hist = false;
   // optional: the last pass also finds the [first, end) entries of every
   // screen tile (key >> tile_shift) into ranges[2 t], ranges[2 t + 1]
   // (zeroed before the sort; finish with launch_ranges_fixup)

@@ -596,7 +596,6 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.tile_ctr = rtiles;
   sa.status_word = &fc->status;
   sa.hist = d_hist;
-  sa.later_hist = false;  // the binning counted every pass's digits
   // the last pass finds the tile ranges (the ranges were zeroed above)
   const bool pass_ranges = *passes > 0;
   if (pass_ranges) {

@@ -89,12 +89,6 @@ struct PassArgs {
   uint32_t* tile_ctr;
   uint32_t* status_word;
   uint32_t rank;           // how a warp finds the lanes sharing a digit: kRank*
-  // first pass of a sort with later_hist: counts of the digits of passes
-  // 1 .. later_passes of every key read ([pass][radix] slots after this
-  // pass's), whose fields follow this pass's field, `num_bits` key bits in all
-  uint32_t* later_hist;
-  uint32_t later_passes;
-  uint32_t num_bits;
   // last pass of a sort with ranges: per screen tile (key >> tile_shift,
   // below num_tiles), atomicMax of the complemented first entry and of the
   // end of every run of one tile in this block's output
@@ -161,7 +155,6 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   uint32_t* s_goff = s_tstart + R;               // [R]
   uint32_t* s_misc = s_goff + R;                 // [40]: tile, warp sums
   uint32_t* s_wor = s_misc + 48;                 // [warps][3][R] peer masks (kRankSmem)
-  uint32_t* s_later = s_wor + (a.rank == kRankSmem ? kSortWarps * 3 * R : 0u);  // [later][R]
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   uint32_t n = *a.n_ptr;
@@ -171,8 +164,6 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
   for (uint32_t k = tid; k < kSortWarps * R; k += kSortThreads) s_whist[k] = 0u;
   if (a.rank == kRankSmem)
     for (uint32_t k = tid; k < kSortWarps * 3 * R; k += kSortThreads) s_wor[k] = 0u;
-  if (a.later_hist)
-    for (uint32_t k = tid; k < a.later_passes * R; k += kSortThreads) s_later[k] = 0u;
   __syncthreads();
   const uint32_t tile = s_misc[0];
   // Clear this tile's words of the other look-back buffer for the next pass
@@ -208,20 +199,6 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     }
   }
 
-  // Digits of the later passes (first pass of a later_hist sort).
-  if (a.later_hist) {
-    const uint32_t valid_n = full ? kSortTile : (uint32_t)((size_t)n - tile_base);
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-      const uint32_t i = (uint32_t)(warp * (32 * kSortItems) + lane + 32 * j);
-      if (i >= valid_n) continue;
-      for (uint32_t q = 1; q <= a.later_passes; ++q) {
-        const uint32_t rem = a.num_bits - q * RB;
-        const uint32_t dm = (1u << (rem < RB ? rem : RB)) - 1u;
-        atomicAdd(&s_later[(q - 1) * R + ((k[j] >> (a.shift + q * RB)) & dm)], 1u);
-      }
-    }
-  }
   // Warp-level stable ranking by digit: the lanes holding the same digit
   // (match) take consecutive ranks after the warp's running count, which the
   // highest of them advances.
@@ -348,13 +325,6 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     if (PAY2) a.v1_out[g] = s_v1[padded(i)];
   }
   if (bad) atomicOr(a.status_word, kStatusCapacity);
-  if (a.later_hist) {
-    __syncthreads();
-    for (uint32_t k2 = tid; k2 < a.later_passes * R; k2 += kSortThreads) {
-      const uint32_t v = s_later[k2];
-      if (v) atomicAdd(&a.later_hist[k2], v);
-    }
-  }
 }
 
 // Exclusive digit bases of every pass from the digit counts, in place: block
@@ -372,7 +342,7 @@ template <int RB, bool PAY2>
 size_t onesweep_smem(uint32_t rank) {
   constexpr uint32_t R = 1u << RB;
   return sizeof(uint32_t) * ((PAY2 ? 3 : 2) * kSortTileP + kSortWarps * R + 3 * R + 48 +
-                             (rank == kRankSmem ? kSortWarps * 3 * R : 0u) + 3 * R);
+                             (rank == kRankSmem ? kSortWarps * 3 * R : 0u));
 }
 
 template <int RB, bool PAY2, typename W>
@@ -457,18 +427,11 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
   const bool pay2 = a.vals2[0] != nullptr;
   const bool wide = a.wide_lookback;
   if (!wide && a.capacity > (1u << 30)) return cudaErrorInvalidValue;  // 30-bit counts
-  // counts -> exclusive bases (in place); with later_hist, pass 0's now and
-  // the later passes' once the first pass has counted them
-  const bool later = a.later_hist && passes > 1;
-  if (later && passes - 1 > 3) return cudaErrorInvalidValue;  // shared-memory slots
-  k_digit_bases<<<later ? 1u : passes, 256, 0, s>>>(a.hist, R);
+  // counts -> exclusive bases (in place)
+  k_digit_bases<<<passes, 256, 0, s>>>(a.hist, R);
   cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) return le;
   for (uint32_t p = 0; p < passes; ++p) {
-    if (later && p == 1) {
-      k_digit_bases<<<passes - 1, 256, 0, s>>>(a.hist + R, R);
-      if ((le = cudaGetLastError()) != cudaSuccess) return le;
-    }
     PassArgs pa;
     pa.keys_in = a.keys[src];
     pa.v0_in = a.vals[src];
@@ -501,9 +464,6 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
     pa.ranges = p + 1 == passes ? a.ranges : nullptr;
     pa.tile_shift = a.tile_shift;
     pa.num_tiles = a.num_tiles;
-    pa.later_hist = later && p == 0 ? a.hist + R : nullptr;
-    pa.later_passes = later && p == 0 ? passes - 1 : 0u;
-    pa.num_bits = a.num_bits;
     cudaError_t e;
     switch (rb) {
       case 4: e = pay2 ? launch_pass<4, true>(pa, tiles, wide, s) : launch_pass<4, false>(pa, tiles, wide, s); break;

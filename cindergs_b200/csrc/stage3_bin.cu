@@ -263,7 +263,6 @@ __device__ __forceinline__ void box_rc(const uint4 box, uint32_t c, uint32_t& r,
 //      walk their candidates again for the rest.
 // Entries at or beyond the buffer capacity are not written and set the
 // capacity status bit (the host grows the buffers and runs Stage 3 again).
-template <bool KEY64>
 __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
   extern __shared__ __align__(16) unsigned char bin_smem[];
   BinSplats& sp = *reinterpret_cast<BinSplats*>(bin_smem);
@@ -271,21 +270,14 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
   uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_tab + kBinWarps * kTabCap);  // [w][kMaskCap]
   uint32_t* s_mrun = s_mask + kBinWarps * kMaskCap;  // [w][kMaskCap] hits before mask c
   uint32_t* s_hits = s_mrun + kBinWarps * kMaskCap;  // [w][kHitCap]
-  uint32_t* s_hist = s_hits + kBinWarps * kHitCap;   // [passes][radix]
+  uint32_t* s_grp = s_hits + kBinWarps * kHitCap;    // [warps][3][kMaxGroups]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t radix = 1u << a.radix_bits, rmask = radix - 1u;
-  const uint32_t passes = (a.tile_bits + a.radix_bits - 1u) / a.radix_bits;
-  const uint32_t tshift = KEY64 ? 0u : a.depth_bits;  // tile bits of the sort word
-  const uint32_t nbins = passes * radix;
   const uint32_t wm1 = a.width - 1u, hm1 = a.height - 1u;
   const uint32_t lw = a.tile_w_log2, lh = a.tile_h_log2;
-  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) s_hist[k] = 0u;
-  __syncthreads();
-  // Record mode: per warp, per tile group, the hits counted, the staging
-  // start and the records written (in the histogram area, unused here).
-  const bool rec_mode = !KEY64 && a.records;
+  // per warp, per tile group: the hits counted, the staging start and the
+  // records written
   const uint32_t G = a.groups, gshift = a.group_shift;
-  uint32_t* s_gcnt = s_hist + warp * 3 * kMaxGroups;
+  uint32_t* s_gcnt = s_grp + warp * 3 * kMaxGroups;
   uint32_t* s_gbase = s_gcnt + kMaxGroups;
   uint32_t* s_grun = s_gbase + kMaxGroups;
   const uint32_t lt = lanemask_lt();
@@ -355,7 +347,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       sp.dq[warp][lane] = dq;
       sp.sid[warp][lane] = sid;
     }
-    if (rec_mode && lane < (int)kMaxGroups) s_gcnt[lane] = 0u;
+    if (lane < (int)kMaxGroups) s_gcnt[lane] = 0u;
     const bool big = total > (uint32_t)kMaskCap * 32u;  // warp-uniform
     if (!big) {
 #pragma unroll
@@ -414,7 +406,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
         const uint32_t ci = item - wbase[o];
         uint32_t tx, ty;
         hit = test(o, ci, tx, ty);
-        rec = ((KEY64 ? ci : ty * a.tiles_x + tx) << 5) | (uint32_t)o;
+        rec = ((ty * a.tiles_x + tx) << 5) | (uint32_t)o;
       }
       const uint32_t hits = __ballot_sync(0xffffffffu, hit);
       if (lane == 0 && c < (uint32_t)kMaskCap) {
@@ -430,7 +422,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
         const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
         own += __popc(hits & seg_mask(lo, hi));
       }
-      if (rec_mode) {  // hits per tile group (one counter update per group present)
+      {  // hits per tile group (one counter update per group present)
         const uint32_t g = hit ? (rec >> 5) >> gshift : 0xFFFFFFFFu;
         const uint32_t peers = __match_any_sync(0xffffffffu, g);
         if (hit && lane == 31 - __clz(peers)) s_gcnt[g] += __popc(peers);
@@ -451,29 +443,11 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
       const uint32_t next = __shfl_down_sync(0xffffffffu, before, 1);
       count = (lane == 31 ? run : next) - before;
     }
-    // Direct mode: the 32-slot tile's first entry from a decoupled look-back
-    // over the tiles' hit counts (tiles are taken in increasing order), so
-    // each slot's scanned offset and each entry's final place in depth order
-    // are known here. Record mode keeps the counts (scanned afterwards).
-    uint32_t wexcl = 0;
-    if (rec_mode) {
-      if (s < a.max_n) a.offsets[s] = count;
-    } else {
-      wexcl = chained_scan_warp<true>(a.lookback, tile, run, &a.fc->status);
-      uint32_t cincl = count;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, cincl, o);
-        if (lane >= o) cincl += y;
-      }
-      if (s < a.max_n) a.offsets[s] = sat_add_u32(wexcl, cincl - count);
-      if (tile == num_tiles - 1u && lane == 0) a.fc->entries = sat_add_u32(wexcl, run);
-    }
+    if (s < a.max_n) a.offsets[s] = count;  // scanned afterwards
 
-    // 2. stage
-    if (rec_mode) {
-      // One run per tile group, each in the hits' order: record = tile << 5 |
-      // slot lane.
+    // 2. stage: one run per tile group, each in the hits' order: record =
+    // tile << 5 | slot lane.
+    {
       if (lane < (int)G) {
         const uint32_t gc = s_gcnt[lane];
         const unsigned long long gb64 =
@@ -539,81 +513,9 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
           hrun += __popc(hits);
         }
       }
-      continue;
-    }
-    const uint32_t sbase = wexcl;  // saturated: at or past cap, nothing is written
-    auto put = [&](uint32_t k, uint32_t tile_id, int o) {
-      const uint64_t pos = (uint64_t)sbase + k;
-      if (pos >= cap) {
-        overflow = true;
-        return;
-      }
-      const uint32_t d = sp.dq[warp][o];
-      uint32_t word;
-      if (KEY64) {
-        word = tile_id;
-        a.depths[pos] = d;
-      } else {
-        word = a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d);
-      }
-      a.keys[pos] = word;
-      a.ids[pos] = sp.sid[warp][o];
-      for (uint32_t p = 0; p < passes; ++p)
-        atomicAdd(&s_hist[p * radix + ((word >> (tshift + p * a.radix_bits)) & rmask)], 1u);
-    };
-    const uint32_t stored = min(run, (uint32_t)kHitCap);
-    for (uint32_t k = lane; k < stored; k += 32) {
-      const uint32_t v = whits[k];
-      const int o = (int)(v & 31u);
-      uint32_t tile_id = v >> 5;
-      if (KEY64) {
-        uint32_t r, cc;
-        box_rc(sp.box[warp][o], tile_id, r, cc);
-        tile_id = (sp.box[warp][o].y + r) * a.tiles_x + sp.box[warp][o].x + cc;
-      }
-      put(k, tile_id, o);
-    }
-    if (run > (uint32_t)kHitCap) {
-      // Hits beyond the stored records: walk the candidates again, using the
-      // stored masks where there are any.
-      uint32_t hrun = 0;
-      for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
-        uint32_t hits;
-        const uint32_t item = chunk + lane;
-        if (c < (uint32_t)kMaskCap) {
-          hits = wmask[c];
-          hrun = wmrun[c];
-          if (hrun + __popc(hits) <= (uint32_t)kHitCap) {
-            hrun += __popc(hits);
-            continue;
-          }
-        } else {
-          bool hit = false;
-          if (item < total) {
-            const int o = find_owner(wbase, item);
-            uint32_t tx, ty;
-            hit = test(o, item - wbase[o], tx, ty);
-          }
-          hits = __ballot_sync(0xffffffffu, hit);
-        }
-        const uint32_t k = hrun + __popc(hits & lt);
-        if (((hits >> lane) & 1u) && k >= (uint32_t)kHitCap) {
-          const int o = find_owner(wbase, item);
-          uint32_t r, cc;
-          box_rc(sp.box[warp][o], item - wbase[o], r, cc);
-          put(k, (sp.box[warp][o].y + r) * a.tiles_x + sp.box[warp][o].x + cc, o);
-        }
-        hrun += __popc(hits);
-      }
     }
   }
   if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
-  if (rec_mode) return;  // no histograms (the area held the group counters)
-  __syncthreads();
-  for (uint32_t k = threadIdx.x; k < nbins; k += kBinThreads) {
-    const uint32_t v = s_hist[k];
-    if (v) atomicAdd(&a.hist[k], v);
-  }
 }
 
 // ---- Binning, direct mode ---------------------------------------------------
@@ -1253,7 +1155,10 @@ cudaError_t launch_bin_count(const BinArgs& a, cudaStream_t s) {
   if (a.max_n == 0) return cudaSuccess;
   if (a.width >= (1u << 22) || a.height >= (1u << 22)) return cudaErrorInvalidValue;
   static int res[4] = {0, 0, 0, 0}, sms[4] = {0, 0, 0, 0};
-  if (a.records) return launch_persistent_bin(k_bin_count<false>, kBinSmem, &res[0], &sms[0], a, s);
+  if (a.records) {
+    if (a.key64) return cudaErrorInvalidValue;  // records hold 27-bit tile ids
+    return launch_persistent_bin(k_bin_count, kBinSmem, &res[0], &sms[0], a, s);
+  }
   if (!a.lookback) return cudaErrorInvalidValue;
   return a.key64 ? launch_persistent_bin(k_bin_direct<true>, kDirSmem, &res[3], &sms[3], a, s)
                  : launch_persistent_bin(k_bin_direct<false>, kDirSmem, &res[2], &sms[2], a, s);
