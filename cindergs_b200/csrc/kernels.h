@@ -331,7 +331,7 @@ struct SortArgs {
   uint32_t num_bits;     // bits to sort on (from first_bit)
   uint32_t radix_bits;   // digit width, 4..8
   uint32_t* hist;        // [passes][radix] counts of the digits, filled before the passes
-                         // (turned into exclusive bases in place by the sort)
+                         // (each block of a pass scans its pass's counts)
   // optional: the last pass also finds the [first, end) entries of every
   // screen tile (key >> tile_shift) into ranges[2 t], ranges[2 t + 1]
   // (zeroed before the sort; finish with launch_ranges_fixup)

@@ -81,7 +81,7 @@ struct PassArgs {
   uint32_t capacity;
   uint32_t shift;
   uint32_t dmask;          // digit mask of this pass (narrower on a final partial pass)
-  const uint32_t* dbase;   // this pass's exclusive digit bases (k_digit_bases)
+  const uint32_t* dbase;   // this pass's digit counts (each block scans them)
   void* status;            // this pass's [tiles][radix] look-back words (32- or 64-bit)
   void* clear_next;        // [tiles][clear_stride] words to zero for the next pass, or null
   uint32_t clear_stride;   // words per tile of clear_next (>= radix)
@@ -174,6 +174,13 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     for (uint32_t k = tid; k < a.clear_stride; k += kSortThreads)
       static_cast<W*>(a.clear_next)[(size_t)tile * a.clear_stride + k] = W(0);
   if (tile >= num_tiles) return;
+  // this pass's exclusive digit base (thread d < R holds digit d's) from the
+  // digit counts
+  uint32_t dig_base;
+  {
+    uint32_t tot0;
+    dig_base = block_exclusive_sum((uint32_t)tid < R ? a.dbase[tid] : 0u, s_misc + 8, &tot0);
+  }
 
   // Load (warp-striped: a warp's item j is 32 consecutive keys). Full tiles,
   // all but the last, need no bounds checks.
@@ -286,7 +293,7 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
       excl = digit_lookback<W>(lb, tile, R, (uint32_t)tid, a.status_word, kSpinLimit);
       Lb<W>::store(lb + (size_t)tile * R + tid, Lb<W>::make(Lb<W>::kPre, excl + agg));
     }
-    s_goff[tid] = a.dbase[tid] + excl - tstart;
+    s_goff[tid] = dig_base + excl - tstart;
   }
   __syncthreads();
   // Scatter: each digit's run is contiguous in the output.
@@ -325,17 +332,6 @@ __global__ void __launch_bounds__(kSortThreads, PAY2 ? 3 : 4) k_onesweep(const P
     if (PAY2) a.v1_out[g] = s_v1[padded(i)];
   }
   if (bad) atomicOr(a.status_word, kStatusCapacity);
-}
-
-// Exclusive digit bases of every pass from the digit counts, in place: block
-// p scans pass p's R counts.
-__global__ void k_digit_bases(uint32_t* hist, uint32_t radix) {
-  __shared__ uint32_t s_sums[32];
-  uint32_t* h = hist + (size_t)blockIdx.x * radix;
-  const uint32_t v = threadIdx.x < radix ? h[threadIdx.x] : 0u;
-  uint32_t tot;
-  const uint32_t ex = block_exclusive_sum(v, s_sums, &tot);
-  if (threadIdx.x < radix) h[threadIdx.x] = ex;
 }
 
 template <int RB, bool PAY2>
@@ -427,10 +423,6 @@ cudaError_t run_radix_sort(const SortArgs& a, int* out_src, cudaStream_t s) {
   const bool pay2 = a.vals2[0] != nullptr;
   const bool wide = a.wide_lookback;
   if (!wide && a.capacity > (1u << 30)) return cudaErrorInvalidValue;  // 30-bit counts
-  // counts -> exclusive bases (in place)
-  k_digit_bases<<<passes, 256, 0, s>>>(a.hist, R);
-  cudaError_t le = cudaGetLastError();
-  if (le != cudaSuccess) return le;
   for (uint32_t p = 0; p < passes; ++p) {
     PassArgs pa;
     pa.keys_in = a.keys[src];
