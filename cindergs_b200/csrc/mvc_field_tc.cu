@@ -5,7 +5,10 @@
 // last hidden layer and its tangents as the cached code (bf16 [4][128]).
 //
 // One CTA per SM, three warpgroups; each warpgroup owns a tile of 32 items
-// = 128 columns n = 4 p + s (item p, stream s = value, d/dx, d/dy, d/dz).
+// = 128 columns n = 8 (p / 2) + 2 s + p % 2 (item p, stream s = value, d/dx,
+// d/dy, d/dz): the 16-byte chunk of columns 8 c .. 8 c + 7 holds items 2 c
+// and 2 c + 1, and a stream of the two items sits in two adjacent columns,
+// so the epilogue works on item pairs with packed f32x2 instructions.
 // A hidden layer is one M = 128, N = 128 product per tile with the weights
 // as A (K-major, as stored) and the activations as B in MN-major order
 // (row k of the operand holds input k of every column), so the accumulator
@@ -171,6 +174,56 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
+// Two f32 lanes in one 64-bit register pair, for the packed f32x2 arithmetic
+// of sm_100 (one instruction for two IEEE-rounded products or sums).
+__device__ __forceinline__ uint64_t f2_make(uint32_t lo, uint32_t hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_splat(float x) {
+  return f2_make(__float_as_uint(x), __float_as_uint(x));
+}
+__device__ __forceinline__ void f2_split(uint64_t a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+// bf16 pair (lo in the low half) of the two lanes, each rounded to nearest
+__device__ __forceinline__ uint32_t f2_bf16(uint64_t a) {
+  float lo, hi;
+  f2_split(a, lo, hi);
+  return pack2(lo, hi);
+}
+// 2^x and 1/x on the special-function unit, per lane
+__device__ __forceinline__ uint64_t f2_ex2(uint64_t a) {
+  float lo, hi;
+  f2_split(a, lo, hi);
+  asm("ex2.approx.ftz.f32 %0, %0;" : "+f"(lo));
+  asm("ex2.approx.ftz.f32 %0, %0;" : "+f"(hi));
+  return f2_make(__float_as_uint(lo), __float_as_uint(hi));
+}
+__device__ __forceinline__ uint64_t f2_rcp(uint64_t a) {
+  float lo, hi;
+  f2_split(a, lo, hi);
+  asm("rcp.approx.ftz.f32 %0, %0;" : "+f"(lo));
+  asm("rcp.approx.ftz.f32 %0, %0;" : "+f"(hi));
+  return f2_make(__float_as_uint(lo), __float_as_uint(hi));
+}
+
 __device__ __forceinline__ float3 item_position(const FieldInfer& fi, uint32_t k_item) {
   const uint32_t gi = fi.gauss ? fi.gauss[fi.first + k_item] : fi.first + k_item;
   if (fi.points4) {
@@ -284,10 +337,18 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
       const float inv_s = fi.enc[3];
       const float xh[3] = {(x3.x - fi.enc[0]) * inv_s, (x3.y - fi.enc[1]) * inv_s,
                            (x3.z - fi.enc[2]) * inv_s};
-      // the 8-byte slot of column 4 p in row k
+      // row k, streams 0-3 (a, b, c, d) of item p: the even lane of a pair
+      // writes streams 0 and 1 of both items (the chunk's first 8 bytes), the
+      // odd lane streams 2 and 3, after one exchange of packed halves. Every
+      // call is made by the whole warp (k depends on the warp only).
       auto put4 = [&](uint32_t k, float a, float b, float c, float d) {
+        const bool odd = (p & 1u) != 0u;
+        const uint32_t keep = odd ? pack2(c, d) : pack2(a, b);
+        const uint32_t give = odd ? pack2(a, b) : pack2(c, d);
+        const uint32_t got = __shfl_xor_sync(0xffffffffu, give, 1);
+        const uint32_t lo = odd ? got : keep, hi = odd ? keep : got;  // item 2 c, item 2 c + 1
         *reinterpret_cast<uint2*>(Bt + mn_chunk(k, p >> 1) + (p & 1) * 8) =
-            make_uint2(pack2(a, b), pack2(c, d));
+            make_uint2(__byte_perm(lo, hi, 0x5410), __byte_perm(lo, hi, 0x7632));
       };
 #pragma unroll
       for (int kk = 0; kk < 6; ++kk) {
@@ -329,6 +390,11 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
       }
       if (!wait_mma()) break;
       const float bj = s_bias[l * kHid + j];
+      // SiLU a = x sigmoid(x) and its slope a' = sg (1 + x (1 - sg)), with
+      // sg = 1 / (1 + 2^(-x log2 e)) and x = pre-activation + bias
+      constexpr float kLog2e = 1.4426950408889634f;
+      const uint64_t b2 = f2_splat(bj), nl2 = f2_splat(-kLog2e), nbl2 = f2_splat(-bj * kLog2e);
+      const uint64_t one2 = f2_splat(1.0f), mone2 = f2_splat(-1.0f);
       const bool last = l == 3;
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {  // columns 64 h .. 64 h + 63 = items 16 h .. 16 h + 15
@@ -338,13 +404,16 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
         tmem_wait_ld();
         uint32_t o[32];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const float pre = __uint_as_float(v[4 * i]) + bj;
-          const float sg = __fdividef(1.0f, 1.0f + __expf(-pre));
-          const float sl = sg * (1.0f + pre * (1.0f - sg));
-          o[2 * i] = pack2(pre * sg, __uint_as_float(v[4 * i + 1]) * sl);
-          o[2 * i + 1] =
-              pack2(__uint_as_float(v[4 * i + 2]) * sl, __uint_as_float(v[4 * i + 3]) * sl);
+        for (int c = 0; c < 8; ++c) {  // items 16 h + 2 c and 16 h + 2 c + 1, lane-paired
+          const uint32_t* w = v + 8 * c;
+          const uint64_t acc = f2_make(w[0], w[1]);
+          const uint64_t pre = f2_add(acc, b2);
+          const uint64_t sg = f2_rcp(f2_add(f2_ex2(f2_fma(acc, nl2, nbl2)), one2));
+          const uint64_t sl = f2_mul(sg, f2_fma(pre, f2_fma(sg, mone2, one2), one2));
+          o[4 * c] = f2_bf16(f2_mul(pre, sg));
+          o[4 * c + 1] = f2_bf16(f2_mul(f2_make(w[2], w[3]), sl));
+          o[4 * c + 2] = f2_bf16(f2_mul(f2_make(w[4], w[5]), sl));
+          o[4 * c + 3] = f2_bf16(f2_mul(f2_make(w[6], w[7]), sl));
         }
         if (CODES && last) {
           // code of an item: [stream][unit] bf16
@@ -354,10 +423,10 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
             if (k_item < fi.count) {
               unsigned short* dst =
                   reinterpret_cast<unsigned short*>(fi.codes + (size_t)k_item * (4 * kHid)) + j;
-              dst[0] = (unsigned short)(o[2 * i] & 0xFFFFu);
-              dst[kHid] = (unsigned short)(o[2 * i] >> 16);
-              dst[2 * kHid] = (unsigned short)(o[2 * i + 1] & 0xFFFFu);
-              dst[3 * kHid] = (unsigned short)(o[2 * i + 1] >> 16);
+              const uint32_t* oc = o + 4 * (i >> 1);
+              const uint32_t sh = (uint32_t)(i & 1) * 16u;
+#pragma unroll
+              for (int s = 0; s < 4; ++s) dst[s * kHid] = (unsigned short)(oc[s] >> sh);
             }
           }
         } else {
@@ -387,7 +456,8 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
     if (!wait_mma()) break;
     uint32_t v[16];
     tmem_ld16(t_row, v);
-    const uint32_t k_item = t * kItems + (j >> 2), s_st = j & 3;
+    // lane j = column n: item 2 (n / 8) + n % 2, stream (n / 2) % 4
+    const uint32_t k_item = t * kItems + 2u * (j >> 3) + (j & 1u), s_st = (j >> 1) & 3u;
     if (k_item < fi.count) {
       float* out = reinterpret_cast<float*>(fi.xf) + 12 * (size_t)(fi.out_first + k_item);
       const float* pc = s_misc;
