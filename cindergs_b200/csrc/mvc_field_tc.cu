@@ -351,15 +351,23 @@ __global__ void __launch_bounds__(kTcWG * 128, 1) k_field_infer_tc(FieldInfer fi
             make_uint2(__byte_perm(lo, hi, 0x5410), __byte_perm(lo, hi, 0x7632));
       };
 #pragma unroll
-      for (int kk = 0; kk < 6; ++kk) {
-        const int i = 6 * q4 + kk, b = i / 3, d = i - 3 * b;
+      for (int d = 0; d < 3; ++d) {
+        // bands 2 q4 and 2 q4 + 1 of axis d: the second (twice the angle) from
+        // the first by the double-angle identities (a few ulp, far below the
+        // bf16 rounding of the operand)
+        const int b = 2 * q4;
         const float w = (float)(1 << b) * 1.57079632679489662f;
         float sn, cs;
-        sincosf(w * (d == 0 ? xh[0] : (d == 1 ? xh[1] : xh[2])), &sn, &cs);
-        const float ds = w * cs * inv_s, dc = -w * sn * inv_s;
-        const uint32_t ks = 3u + 6u * (uint32_t)b + 2u * (uint32_t)d;
-        put4(ks, sn, d == 0 ? ds : 0.0f, d == 1 ? ds : 0.0f, d == 2 ? ds : 0.0f);
-        put4(ks + 1, cs, d == 0 ? dc : 0.0f, d == 1 ? dc : 0.0f, d == 2 ? dc : 0.0f);
+        sincosf(w * xh[d], &sn, &cs);
+        const float sn2 = 2.0f * sn * cs, cs2 = (cs - sn) * (cs + sn);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const float we = e ? 2.0f * w : w, se = e ? sn2 : sn, ce = e ? cs2 : cs;
+          const float ds = we * ce * inv_s, dc = -we * se * inv_s;
+          const uint32_t ks = 3u + 6u * (uint32_t)(b + e) + 2u * (uint32_t)d;
+          put4(ks, se, d == 0 ? ds : 0.0f, d == 1 ? ds : 0.0f, d == 2 ? ds : 0.0f);
+          put4(ks + 1, ce, d == 0 ? dc : 0.0f, d == 1 ? dc : 0.0f, d == 2 ? dc : 0.0f);
+        }
       }
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk) {
