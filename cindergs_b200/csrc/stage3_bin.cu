@@ -537,14 +537,19 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_count(const BinArgs a) {
 //   write:  the stored masks are walked again and every hit is written at
 //           its place in depth order (key, splat index, 64-bit: depth word)
 //           and counted in per-warp histograms of the entry sort's digits.
-// Warps with more candidates than the masks hold test the rest again in the
-// write step. Entries at or beyond the capacity are not written and set the
-// capacity bit.
-constexpr int kDirMaskCap = 96;   // stored ballot masks per warp (3,072 candidates)
-constexpr int kDirTabCap = 448;   // term-table entries per warp
+// The scan and write of a tile are deferred by one tile: a warp publishes the
+// hit count of the tile it has just counted, then walks back and writes the
+// tile it counted before, whose predecessors have had a whole count step to
+// publish theirs. The state the write needs (owners, depth keys, splat
+// indices, masks) is therefore kept for two tiles per warp. A tile with more
+// candidates than the masks hold is scanned and written at once, testing the
+// rest of its candidates again. Entries at or beyond the capacity are not
+// written and set the capacity bit.
+constexpr int kDirMaskCap = 64;   // stored ballot masks per warp and tile (2,048 candidates)
+constexpr int kDirTabCap = 440;   // term-table entries per warp
 
 struct DirSplats {
-  uint4 own[kBinWarps][32];    // first candidate, ceil(2^32 / width) (0 if width 1), width, first tile id
+  // the tile being counted
   uint2 tb[kBinWarps][32];     // first column entry, first row entry in the term table
   uint2 xy[kBinWarps][32];     // box origin (tiles)
   float4 kq[kBinWarps][32];    // a, 2b, c, q_max + 1e-4
@@ -554,12 +559,14 @@ struct DirSplats {
   uint32_t base[kBinWarps][32];
   uint32_t cpre[kBinWarps][32];
   uint32_t rpre[kBinWarps][32];
-  uint32_t dq[kBinWarps][32];
-  uint32_t sid[kBinWarps][32];
-  uint32_t lor[kBinWarps][32];           // lane of the k-th splat with candidates
-  uint32_t sbits[kBinWarps][kDirMaskCap];  // start bit per splat's first candidate
-  uint32_t mask[kBinWarps][kDirMaskCap];   // hit ballots
-  uint32_t mrun[kBinWarps][kDirMaskCap];   // hits before each ballot
+  // what the write needs, for two tiles (the one counted and the one before)
+  uint4 own[2][kBinWarps][32];  // first candidate, ceil(2^32 / width) (0 if width 1), width, first tile id
+  uint32_t dq[2][kBinWarps][32];
+  uint32_t sid[2][kBinWarps][32];
+  uint32_t lor[2][kBinWarps][32];             // lane of the k-th splat with candidates
+  uint32_t sbits[2][kBinWarps][kDirMaskCap];  // start bit per splat's first candidate
+  uint32_t mask[2][kBinWarps][kDirMaskCap];   // hit ballots
+  uint32_t mrun[2][kBinWarps][kDirMaskCap];   // hits before each ballot
 };
 // tile-digit histograms: one per warp when a histogram has at most
 // kDirWarpBins bins (no contention between warps), else one per block
@@ -567,6 +574,8 @@ constexpr uint32_t kDirWarpBins = 256;
 constexpr size_t kDirSmem = sizeof(DirSplats) + sizeof(float4) * kBinWarps * kDirTabCap +
                             sizeof(uint32_t) * kBinWarps * kDirWarpBins;
 static_assert(kBinWarps * kDirWarpBins >= 1024, "a block histogram of 4 x 256 bins fits");
+// two blocks per SM: 228 KB of shared memory, 1 KB of it reserved per block
+static_assert(2 * (kDirSmem + 1024) <= 233472, "two binning blocks per SM");
 
 template <bool KEY64>
 __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) {
@@ -592,153 +601,34 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
   const uint32_t num_tiles = (a.max_n + 31u) / 32u;
   const uint32_t* wbase = sp.base[warp];
   float4* wtab = s_tab + warp * kDirTabCap;
-  uint32_t* wmask = sp.mask[warp];
-  uint32_t* wmrun = sp.mrun[warp];
   const uint32_t cap = a.entry_cap;
   bool overflow = false;
 
-  for (;;) {
-    uint32_t tile = 0;
-    if (lane == 0) tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
-    tile = __shfl_sync(0xffffffffu, tile, 0);
-    if (tile >= num_tiles) break;
-    const uint32_t s = tile * 32u + lane;  // slot in depth order
-    uint32_t sid = kInvalid, dq = 0;
-    if (s < active && s < a.max_n) {
-      sid = a.order_ids[s];
-      dq = a.order_keys[s];
-    }
-    const SplatBox b = load_box(a, sid, active);
-
-    // ---- setup
-    const uint32_t bw = b.valid ? (b.x1 - b.x0 + 1u) : 0u;
-    const uint32_t bh = b.valid ? (b.y1 - b.y0 + 1u) : 0u;
-    const uint32_t ncand = bw * bh;
-    uint32_t incl = ncand, cincl = bw, rincl = bh;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      const uint32_t yc = __shfl_up_sync(0xffffffffu, cincl, o);
-      const uint32_t yr = __shfl_up_sync(0xffffffffu, rincl, o);
-      if (lane >= o) {
-        incl += y;
-        cincl += yc;
-        rincl += yr;
-      }
-    }
-    const uint32_t base = incl - ncand;
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    const uint32_t wt = __shfl_sync(0xffffffffu, cincl, 31);
-    const uint32_t ht = __shfl_sync(0xffffffffu, rincl, 31);
-    const bool tab = wt + ht <= (uint32_t)kDirTabCap;            // warp-uniform
-    const bool big = total > (uint32_t)kDirMaskCap * 32u;        // warp-uniform
-    const uint32_t nonempty = __ballot_sync(0xffffffffu, ncand > 0u);
-    __syncwarp();  // the previous tile's readers are done with the warp's shared memory
-    {
-      const uint32_t w = b.valid ? bw : 1u;
-      const float ca_ = fmaxf(b.ca, 1e-12f), cc_ = fmaxf(b.cc, 1e-12f);
-      const float cb2 = __fmul_rn(2.0f, b.cb);
-      const float qlim =
-          __fadd_rn(b.valid ? clampf(__fmul_rn(2.0f, cgs_logf(__fmul_rn(255.0f, b.alpha))), 0.0f, 8.0f)
-                            : 0.0f,
-                    1e-4f);
-      sp.own[warp][lane] =
-          make_uint4(base, w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w), w,
-                     b.y0 * a.tiles_x + b.x0);
-      sp.tb[warp][lane] = make_uint2(cincl - bw, wt + rincl - bh);
-      sp.xy[warp][lane] = make_uint2(b.x0, b.y0);
-      sp.kq[warp][lane] = make_float4(b.ca, cb2, b.cc, qlim);
-      sp.geo[warp][lane] = make_float4(b.mu_x, b.mu_y, -b.cb, cb2);
-      sp.con[warp][lane] = make_float4(b.ca, b.cc, ca_, cc_);
-      sp.rcp[warp][lane] = make_double2(1.0 / (double)cc_, 1.0 / (double)ca_);
-      sp.base[warp][lane] = base;
-      sp.cpre[warp][lane] = cincl - bw;
-      sp.rpre[warp][lane] = rincl - bh;
-      sp.dq[warp][lane] = dq;
-      sp.sid[warp][lane] = sid;
-      if (ncand > 0u) sp.lor[warp][__popc(nonempty & lt)] = (uint32_t)lane;
-      if (!big) {
-#pragma unroll
-        for (int k = lane; k < kDirMaskCap; k += 32) sp.sbits[warp][k] = 0u;
-      }
-    }
-    __syncwarp();
-    if (!big && ncand > 0u) atomicOr(&sp.sbits[warp][base >> 5], 1u << (base & 31u));
-    // ---- tables: columns [0, wt), rows [wt, wt + ht)
+  // owner (lane) of candidate `item` in write buffer q; sb = start bits of its
+  // chunk, starts = splats starting before the chunk
+  auto owner = [&](int q, bool big, uint32_t item, uint32_t sb, uint32_t starts) -> int {
+    return big ? find_owner(wbase, item) : (int)sp.lor[q][warp][starts + __popc(sb & upto) - 1u];
+  };
+  // the test of candidate item of splat o (the tile being counted, buffer q)
+  auto test = [&](int q, bool tab, int o, uint32_t item) -> bool {
+    const uint4 ow = sp.own[q][warp][o];
+    const uint32_t ci = item - ow.x;
+    const uint32_t r = ow.y ? __umulhi(ci, ow.y) : ci;
+    const uint32_t c = ci - r * ow.z;
     if (tab) {
-      for (uint32_t i = lane; i < wt; i += 32) {
-        const int o = find_owner(sp.cpre[warp], i);
-        wtab[i] = col_terms(sp.xy[warp][o].x + (i - sp.cpre[warp][o]), lw, wm1, sp.geo[warp][o],
-                            sp.con[warp][o], sp.rcp[warp][o]);
-      }
-      for (uint32_t i = lane; i < ht; i += 32) {
-        const int o = find_owner(sp.rpre[warp], i);
-        wtab[wt + i] = row_terms(sp.xy[warp][o].y + (i - sp.rpre[warp][o]), lh, hm1,
-                                 sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o]);
-      }
+      const uint2 t = sp.tb[warp][o];
+      return tab_hit(wtab[t.x + c], wtab[t.y + r], sp.kq[warp][o]);
     }
-    __syncwarp();
-    // owner (lane) of candidate `item`; sb = start bits of its chunk, starts =
-    // splats starting before the chunk
-    auto owner = [&](uint32_t item, uint32_t sb, uint32_t starts) -> int {
-      return big ? find_owner(wbase, item) : (int)sp.lor[warp][starts + __popc(sb & upto) - 1u];
-    };
-    // the test of candidate item of splat o; r, c its row and column in the box
-    auto test = [&](int o, uint32_t item, uint32_t& r, uint32_t& c) -> bool {
-      const uint4 ow = sp.own[warp][o];
-      const uint32_t ci = item - ow.x;
-      r = ow.y ? __umulhi(ci, ow.y) : ci;
-      c = ci - r * ow.z;
-      if (tab) {
-        const uint2 t = sp.tb[warp][o];
-        return tab_hit(wtab[t.x + c], wtab[t.y + r], sp.kq[warp][o]);
-      }
-      const uint2 xy = sp.xy[warp][o];
-      return tile_hit(xy.x + c, xy.y + r, wm1, hm1, lw, lh, sp.geo[warp][o], sp.con[warp][o],
-                      sp.rcp[warp][o], sp.kq[warp][o].w);
-    };
-
-    // ---- count
-    uint32_t run = 0;     // hits before the current chunk (warp-uniform)
-    uint32_t own = 0;     // this lane's hits, accumulated only when `big`
-    uint32_t starts = 0;  // splats starting before the current chunk
-#pragma unroll 2
-    for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
-      const uint32_t item = chunk + lane;
-      const uint32_t sb = big ? 0u : sp.sbits[warp][c];
-      bool hit = false;
-      if (item < total) {
-        uint32_t r, cc;
-        hit = test(owner(item, sb, starts), item, r, cc);
-      }
-      const uint32_t hits = __ballot_sync(0xffffffffu, hit);
-      if (lane == 0 && c < (uint32_t)kDirMaskCap) {
-        wmask[c] = hits;
-        wmrun[c] = run;
-      }
-      if (big) {
-        const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
-        const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
-        own += __popc(hits & seg_mask(lo, hi));
-      }
-      run += __popc(hits);
-      starts += __popc(sb);
-    }
-    __syncwarp();
-    uint32_t count = own;
-    if (!big) {
-      // hits before this lane's first candidate, from the stored masks
-      uint32_t before = run;
-      if (base < total) {
-        const uint32_t c = base >> 5;
-        before = wmrun[c] + __popc(wmask[c] & ((1u << (base & 31u)) - 1u));
-      }
-      const uint32_t next = __shfl_down_sync(0xffffffffu, before, 1);
-      count = (lane == 31 ? run : next) - before;
-    }
-
-    // ---- scan
-    const uint32_t wexcl = chained_scan_warp<true>(a.lookback, tile, run, &a.fc->status);
+    const uint2 xy = sp.xy[warp][o];
+    return tile_hit(xy.x + c, xy.y + r, wm1, hm1, lw, lh, sp.geo[warp][o], sp.con[warp][o],
+                    sp.rcp[warp][o], sp.kq[warp][o].w);
+  };
+  // Scan and write of a counted tile whose masks are in buffer q (a tile with
+  // more candidates than the masks hold tests the rest again: only at once,
+  // while its test state is the current one).
+  auto scan_write = [&](int q, uint32_t tile, uint32_t total, bool big, bool tab, uint32_t run,
+                        uint32_t count, uint32_t s) {
+    const uint32_t wexcl = chained_resolve<true>(a.lookback, tile, run, &a.fc->status);
     {
       uint32_t cincl2 = count;
 #pragma unroll
@@ -749,40 +639,36 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
       if (s < a.max_n) a.offsets[s] = sat_add_u32(wexcl, cincl2 - count);
       if (tile == num_tiles - 1u && lane == 0) a.fc->entries = sat_add_u32(wexcl, run);
     }
-
-    // ---- write
-    uint32_t hrun = 0;
-    starts = 0;
+    const uint32_t* qmask = sp.mask[q][warp];
+    const uint32_t* qsbits = sp.sbits[q][warp];
+    uint32_t hrun = 0, starts = 0;
 #pragma unroll 2
     for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
       const uint32_t item = chunk + lane;
-      const uint32_t sb = big ? 0u : sp.sbits[warp][c];
+      const uint32_t sb = big ? 0u : qsbits[c];
       uint32_t hits;
       if (c < (uint32_t)kDirMaskCap) {
-        hits = wmask[c];
+        hits = qmask[c];
       } else {
         bool h = false;
-        if (item < total) {
-          uint32_t r, cc;
-          h = test(owner(item, sb, starts), item, r, cc);
-        }
+        if (item < total) h = test(q, tab, owner(q, big, item, sb, starts), item);
         hits = __ballot_sync(0xffffffffu, h);
       }
       const bool hit = (hits >> lane) & 1u;
       uint32_t word = 0;
       if (hit) {
-        const int o = owner(item, sb, starts);
-        const uint4 ow = sp.own[warp][o];
+        const int o = owner(q, big, item, sb, starts);
+        const uint4 ow = sp.own[q][warp][o];
         const uint32_t ci = item - ow.x;
         const uint32_t r = ow.y ? __umulhi(ci, ow.y) : ci;
         const uint32_t cc = ci - r * ow.z;
         const uint32_t tile_id = ow.w + r * a.tiles_x + cc;
-        const uint32_t d = sp.dq[warp][o];
+        const uint32_t d = sp.dq[q][warp][o];
         word = KEY64 ? tile_id : (a.depth_bits >= 32u ? d : ((tile_id << a.depth_bits) | d));
         const uint64_t pos = (uint64_t)wexcl + hrun + __popc(hits & lt);
         if (pos < cap) {
           a.keys[pos] = word;
-          a.ids[pos] = sp.sid[warp][o];
+          a.ids[pos] = sp.sid[q][warp][o];
           if (KEY64) a.depths[pos] = d;
         } else {
           overflow = true;
@@ -796,6 +682,151 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_direct(const BinArgs a) 
       }
       hrun += __popc(hits);
       starts += __popc(sb);
+    }
+  };
+
+  int cur = 0;        // write buffer of the tile being counted
+  bool pend = false;  // a counted tile waits for its scan and write (buffer cur ^ 1)
+  uint32_t p_tile = 0, p_total = 0, p_run = 0, p_count = 0, p_s = 0;
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(&a.fc->tile_ctr[1], 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    const bool have = tile < num_tiles;  // warp-uniform
+    uint32_t s = 0, total = 0, run = 0, count = 0;
+    bool big = false, tab = false;
+    if (have) {
+      s = tile * 32u + lane;  // slot in depth order
+      uint32_t sid = kInvalid, dq = 0;
+      if (s < active && s < a.max_n) {
+        sid = a.order_ids[s];
+        dq = a.order_keys[s];
+      }
+      const SplatBox b = load_box(a, sid, active);
+
+      // ---- setup
+      const uint32_t bw = b.valid ? (b.x1 - b.x0 + 1u) : 0u;
+      const uint32_t bh = b.valid ? (b.y1 - b.y0 + 1u) : 0u;
+      const uint32_t ncand = bw * bh;
+      uint32_t incl = ncand, cincl = bw, rincl = bh;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        const uint32_t yc = __shfl_up_sync(0xffffffffu, cincl, o);
+        const uint32_t yr = __shfl_up_sync(0xffffffffu, rincl, o);
+        if (lane >= o) {
+          incl += y;
+          cincl += yc;
+          rincl += yr;
+        }
+      }
+      const uint32_t base = incl - ncand;
+      total = __shfl_sync(0xffffffffu, incl, 31);
+      const uint32_t wt = __shfl_sync(0xffffffffu, cincl, 31);
+      const uint32_t ht = __shfl_sync(0xffffffffu, rincl, 31);
+      tab = wt + ht <= (uint32_t)kDirTabCap;       // warp-uniform
+      big = total > (uint32_t)kDirMaskCap * 32u;   // warp-uniform
+      const uint32_t nonempty = __ballot_sync(0xffffffffu, ncand > 0u);
+      __syncwarp();  // earlier readers are done with this buffer and the test state
+      {
+        const uint32_t w = b.valid ? bw : 1u;
+        const float ca_ = fmaxf(b.ca, 1e-12f), cc_ = fmaxf(b.cc, 1e-12f);
+        const float cb2 = __fmul_rn(2.0f, b.cb);
+        const float qlim =
+            __fadd_rn(b.valid ? clampf(__fmul_rn(2.0f, cgs_logf(__fmul_rn(255.0f, b.alpha))), 0.0f, 8.0f)
+                              : 0.0f,
+                      1e-4f);
+        sp.own[cur][warp][lane] =
+            make_uint4(base, w <= 1u ? 0u : (uint32_t)(((1ull << 32) + w - 1u) / w), w,
+                       b.y0 * a.tiles_x + b.x0);
+        sp.tb[warp][lane] = make_uint2(cincl - bw, wt + rincl - bh);
+        sp.xy[warp][lane] = make_uint2(b.x0, b.y0);
+        sp.kq[warp][lane] = make_float4(b.ca, cb2, b.cc, qlim);
+        sp.geo[warp][lane] = make_float4(b.mu_x, b.mu_y, -b.cb, cb2);
+        sp.con[warp][lane] = make_float4(b.ca, b.cc, ca_, cc_);
+        sp.rcp[warp][lane] = make_double2(1.0 / (double)cc_, 1.0 / (double)ca_);
+        sp.base[warp][lane] = base;
+        sp.cpre[warp][lane] = cincl - bw;
+        sp.rpre[warp][lane] = rincl - bh;
+        sp.dq[cur][warp][lane] = dq;
+        sp.sid[cur][warp][lane] = sid;
+        if (ncand > 0u) sp.lor[cur][warp][__popc(nonempty & lt)] = (uint32_t)lane;
+        if (!big) {
+#pragma unroll
+          for (int k = lane; k < kDirMaskCap; k += 32) sp.sbits[cur][warp][k] = 0u;
+        }
+      }
+      __syncwarp();
+      if (!big && ncand > 0u) atomicOr(&sp.sbits[cur][warp][base >> 5], 1u << (base & 31u));
+      // ---- tables: columns [0, wt), rows [wt, wt + ht)
+      if (tab) {
+        for (uint32_t i = lane; i < wt; i += 32) {
+          const int o = find_owner(sp.cpre[warp], i);
+          wtab[i] = col_terms(sp.xy[warp][o].x + (i - sp.cpre[warp][o]), lw, wm1, sp.geo[warp][o],
+                              sp.con[warp][o], sp.rcp[warp][o]);
+        }
+        for (uint32_t i = lane; i < ht; i += 32) {
+          const int o = find_owner(sp.rpre[warp], i);
+          wtab[wt + i] = row_terms(sp.xy[warp][o].y + (i - sp.rpre[warp][o]), lh, hm1,
+                                   sp.geo[warp][o], sp.con[warp][o], sp.rcp[warp][o]);
+        }
+      }
+      __syncwarp();
+      // ---- count
+      uint32_t* wmask = sp.mask[cur][warp];
+      uint32_t* wmrun = sp.mrun[cur][warp];
+      uint32_t own = 0;     // this lane's hits, accumulated only when `big`
+      uint32_t starts = 0;  // splats starting before the current chunk
+#pragma unroll 2
+      for (uint32_t chunk = 0, c = 0; chunk < total; chunk += 32, ++c) {
+        const uint32_t item = chunk + lane;
+        const uint32_t sb = big ? 0u : sp.sbits[cur][warp][c];
+        bool hit = false;
+        if (item < total) hit = test(cur, tab, owner(cur, big, item, sb, starts), item);
+        const uint32_t hits = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0 && c < (uint32_t)kDirMaskCap) {
+          wmask[c] = hits;
+          wmrun[c] = run;
+        }
+        if (big) {
+          const int lo = base > chunk ? (int)min(base - chunk, 32u) : 0;
+          const int hi = (base + ncand) > chunk ? (int)min(base + ncand - chunk, 32u) : 0;
+          own += __popc(hits & seg_mask(lo, hi));
+        }
+        run += __popc(hits);
+        starts += __popc(sb);
+      }
+      __syncwarp();
+      count = own;
+      if (!big) {
+        // hits before this lane's first candidate, from the stored masks
+        uint32_t before = run;
+        if (base < total) {
+          const uint32_t c = base >> 5;
+          before = wmrun[c] + __popc(wmask[c] & ((1u << (base & 31u)) - 1u));
+        }
+        const uint32_t next = __shfl_down_sync(0xffffffffu, before, 1);
+        count = (lane == 31 ? run : next) - before;
+      }
+      // publish this tile's hit count before any wait
+      chained_publish(a.lookback, tile, run);
+    }
+    // ---- scan and write of the tile counted before this one
+    if (pend) {
+      scan_write(cur ^ 1, p_tile, p_total, false, false, p_run, p_count, p_s);
+      pend = false;
+    }
+    if (!have) break;
+    if (big) {
+      scan_write(cur, tile, total, true, tab, run, count, s);
+    } else {
+      pend = true;
+      p_tile = tile;
+      p_total = total;
+      p_run = run;
+      p_count = count;
+      p_s = s;
+      cur ^= 1;
     }
   }
   if (overflow) atomicOr(&a.fc->status, kStatusCapacity);
