@@ -613,7 +613,7 @@ int enqueue_stage3(cgs_ctx* ctx, const FrameDesc& d, const ScratchLayout& L, int
   sa.smem_mask = 1u;
   ctx->kbegin(CGS_K_ENTRY_SORT);
   CGS_CUDA(run_radix_sort(sa, result_src, s), "radix sort");
-  if (sort_launches) *sort_launches = 1 + *passes;
+  if (sort_launches) *sort_launches = *passes;  // one onesweep launch per pass
   ctx->kend();
   ctx->kbegin(CGS_K_TILE_RANGES);
   if (pass_ranges)
