@@ -16,7 +16,11 @@
 //                    slot = n + (number of splitting Gaussians with a lower
 //                    index), from a block scan chained across blocks, instead
 //                    of the reference's atomic counter whose order varies
-//                    from run to run (deformation.rs:1191).
+//                    from run to run (deformation.rs:1191). Without the
+//                    split the Gaussian blocks are persistent (as many as
+//                    the SMs hold): each thread loads its next Gaussian's
+//                    60 B while deforming the current one, and the first
+//                    loads are issued before the wait for the tet blocks.
 //  k_bind            GPU barycentric binding (TetMesh::bind_point,
 //                    deformation/mod.rs:267-310).
 //
@@ -311,8 +315,213 @@ __device__ __forceinline__ void mip3d_cpu(float* cov, float& alpha, float var) {
   alpha = clampf(alpha * sqrtf(clampf(d0 / dr, 0.0f, 1.0f)), 0.0f, 1.0f);
 }
 
+// A Gaussian's Stage 1 inputs (60 B), loaded before the kernel waits for the
+// tet transforms so that the first blocks' DRAM reads overlap that wait.
+struct DeformIn {
+  uint32_t tet_raw;
+  float4 rp, rca, w;
+  float2 rcb;
+};
+
+__device__ __forceinline__ DeformIn deform_load(const DeformArgs& a, uint32_t i) {
+  DeformIn g;
+  g.tet_raw = a.bind_tet[i];
+  g.rp = a.rest_pos[i];
+  g.rca = a.rest_cova[i];
+  g.rcb = a.rest_covb[i];
+  g.w = a.bind_w[i];
+  return g;
+}
+
+// Deformed position, covariance and opacity of Gaussian i (and of its split
+// child: cx, cy, cz) from its loaded inputs.
 template <bool SPLIT>
-__global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
+__device__ __forceinline__ void deform_one(const DeformArgs& a, const DeformIn& g, bool& split,
+                                           float& cx, float& cy, float& cz, float4& out_pos,
+                                           float4& out_cova, float2& out_covb) {
+  const uint32_t tet_raw = g.tet_raw;
+  const float4 rp = g.rp, rca = g.rca;
+  const float2 rcb = g.rcb;
+  if (tet_raw == kMvcBound && a.mvc_xf) {
+    // Polygon-cage binding (deform_scene_cpu, mvc.rs:616-749): position and
+    // F from k_mvc_jacobian, rotation for SH, F S F^T, opacity unchanged.
+    const uint32_t slot = __float_as_uint(g.w.x);
+    const float4 q0 = a.mvc_xf[3 * (size_t)slot], q1 = a.mvc_xf[3 * (size_t)slot + 1],
+                 q2 = a.mvc_xf[3 * (size_t)slot + 2];
+    const GM3 Fm = {{q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
+    const GM3 R = polar_rotation(Fm);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a.mvc_R[9 * (size_t)slot + k] = R.c[k];
+    const GM3 S = {{rca.x, rca.y, rca.z, rca.y, rca.w, rcb.x, rca.z, rcb.x, rcb.y}};
+    const GM3 m = gm3_mul(gm3_mul(Fm, S), gm3_t(Fm));
+    float cv[6] = {m.c[0], m.c[1], m.c[2], m.c[4], m.c[5], m.c[8]};
+    float alpha = rp.w;
+    if (SPLIT && a.split_threshold > 0.0f) {
+      // jacobian_singular_values (polar.rs:89-109): sigma_1 of F
+      const GM3 C = gm3_mul(gm3_t(Fm), Fm);
+      const float packed[6] = {C.c[0], C.c[1], C.c[2], C.c[4], C.c[5], C.c[8]};
+      float ev[3];
+      GM3 basis;
+      sym_eigen3_f64(packed, ev, basis);
+      split = sqrtf(fmaxf(ev[0], 0.0f)) > a.split_threshold;
+    }
+    if (!split) {
+      if (a.mip > 0.0f) mip3d_cpu(cv, alpha, a.mip);
+      out_pos = make_float4(q0.x, q0.y, q0.z, alpha);
+    } else {
+      // split_gaussian_along_major_axis (math/covariance.rs:331-378)
+      float ev[3];
+      GM3 B;
+      sym_eigen3_f64(cv, ev, B);
+      const float min_var = 1e-4f * 1e-4f;
+      const GM3 D = {{fmaxf(ev[0] * 0.25f, min_var), 0, 0, 0, fmaxf(ev[1], min_var), 0, 0, 0,
+                      fmaxf(ev[2], min_var)}};
+      float ax[3] = {B.c[0], B.c[1], B.c[2]};
+      const float len2 = gdot(ax, ax);
+      if (len2 > 0.0f) {
+        const float inv = 1.0f / sqrtf(len2);
+        ax[0] *= inv; ax[1] *= inv; ax[2] *= inv;
+      }
+      const float om = 0.5f * sqrtf(fmaxf(ev[0], min_var));
+      const GM3 cm = gm3_mul(gm3_mul(B, D), gm3_t(B));
+      cv[0] = cm.c[0]; cv[1] = cm.c[1]; cv[2] = cm.c[2];
+      cv[3] = cm.c[4]; cv[4] = cm.c[5]; cv[5] = cm.c[8];
+      if (a.mip > 0.0f) mip3d_cpu(cv, alpha, a.mip);
+      const float ox = ax[0] * om, oy = ax[1] * om, oz = ax[2] * om;
+      out_pos = make_float4(q0.x + (-ox), q0.y + (-oy), q0.z + (-oz), alpha);
+      cx = q0.x + ox;
+      cy = q0.y + oy;
+      cz = q0.z + oz;
+    }
+    out_cova = make_float4(cv[0], cv[1], cv[2], cv[3]);
+    out_covb = make_float2(cv[4], cv[5]);
+  } else if (tet_raw >= a.num_tets) {
+    // Unbound: rest pose plus the Mip filter (deformation.rs:899-947).
+    float xx = rca.x, xy = rca.y, xz = rca.z, yy = rca.w, yz = rcb.x, zz = rcb.y;
+    float alpha = rp.w;
+    if (a.mip > 0.0f) mip3d(xx, xy, xz, yy, yz, zz, alpha, a.mip);
+    out_pos = make_float4(rp.x, rp.y, rp.z, alpha);
+    out_cova = make_float4(xx, xy, xz, yy);
+    out_covb = make_float2(yz, zz);
+  } else {
+    const float4 w = g.w;
+    const uint4 e = __ldg(&a.elems[tet_raw]);
+    const float* v0 = a.verts + 3 * (size_t)e.x;
+    const float* v1 = a.verts + 3 * (size_t)e.y;
+    const float* v2 = a.verts + 3 * (size_t)e.z;
+    const float* v3 = a.verts + 3 * (size_t)e.w;
+    const float px = w.x * __ldg(v0) + w.y * __ldg(v1) + w.z * __ldg(v2) + w.w * __ldg(v3);
+    const float py =
+        w.x * __ldg(v0 + 1) + w.y * __ldg(v1 + 1) + w.z * __ldg(v2 + 1) + w.w * __ldg(v3 + 1);
+    const float pz =
+        w.x * __ldg(v0 + 2) + w.y * __ldg(v1 + 2) + w.z * __ldg(v2 + 2) + w.w * __ldg(v3 + 2);
+    const float* J = a.tet_J + 9 * (size_t)tet_raw;
+    const float j_00 = __ldca(J + 0), j_10 = __ldca(J + 1), j_20 = __ldca(J + 2);
+    const float j_01 = __ldca(J + 3), j_11 = __ldca(J + 4), j_21 = __ldca(J + 5);
+    const float j_02 = __ldca(J + 6), j_12 = __ldca(J + 7), j_22 = __ldca(J + 8);
+    const float s_xx = rca.x, s_xy = rca.y, s_xz = rca.z, s_yy = rca.w, s_yz = rcb.x,
+                s_zz = rcb.y;
+    const float k_00 = j_00 * s_xx + j_01 * s_xy + j_02 * s_xz;
+    const float k_01 = j_00 * s_xy + j_01 * s_yy + j_02 * s_yz;
+    const float k_02 = j_00 * s_xz + j_01 * s_yz + j_02 * s_zz;
+    const float k_10 = j_10 * s_xx + j_11 * s_xy + j_12 * s_xz;
+    const float k_11 = j_10 * s_xy + j_11 * s_yy + j_12 * s_yz;
+    const float k_12 = j_10 * s_xz + j_11 * s_yz + j_12 * s_zz;
+    const float k_20 = j_20 * s_xx + j_21 * s_xy + j_22 * s_xz;
+    const float k_21 = j_20 * s_xy + j_21 * s_yy + j_22 * s_yz;
+    const float k_22 = j_20 * s_xz + j_21 * s_yz + j_22 * s_zz;
+    const float m00 = fmaxf(1e-4f, k_00 * j_00 + k_01 * j_01 + k_02 * j_02);
+    const float m01 = 0.5f * ((k_00 * j_10 + k_01 * j_11 + k_02 * j_12) +
+                              (k_10 * j_00 + k_11 * j_01 + k_12 * j_02));
+    const float m02 = 0.5f * ((k_00 * j_20 + k_01 * j_21 + k_02 * j_22) +
+                              (k_20 * j_00 + k_21 * j_01 + k_22 * j_02));
+    const float m11 = fmaxf(1e-4f, k_10 * j_10 + k_11 * j_11 + k_12 * j_12);
+    const float m12 = 0.5f * ((k_10 * j_20 + k_11 * j_21 + k_12 * j_22) +
+                              (k_20 * j_10 + k_21 * j_11 + k_22 * j_12));
+    const float m22 = fmaxf(1e-4f, k_20 * j_20 + k_21 * j_21 + k_22 * j_22);
+    const float det_j = j_00 * (j_11 * j_22 - j_12 * j_21) -
+                        j_01 * (j_10 * j_22 - j_12 * j_20) + j_02 * (j_10 * j_21 - j_11 * j_20);
+    const float s_det = clampf(det_j, 0.6f, 1.8f);
+    const float safe_base = clampf(1.0f - rp.w, 1e-4f, 0.999f);
+    const float alpha_prime = clampf(1.0f - cgs_powf(safe_base, 1.0f / s_det), 0.05f, 0.99f);
+    split = SPLIT && a.split_threshold > 0.0f && __ldca(&a.tet_stretch[tet_raw]) > a.split_threshold;
+    if (!split) {
+      float xx = m00, yy = m11, zz = m22, alpha = alpha_prime;
+      if (a.mip > 0.0f) mip3d(xx, m01, m02, yy, m12, zz, alpha, a.mip);
+      out_pos = make_float4(px, py, pz, alpha);
+      out_cova = make_float4(xx, m01, m02, yy);
+      out_covb = make_float2(m12, zz);
+    } else {
+      // Major eigenpair of M by Cardano + cross products (deformation.rs:1066-1143).
+      const float p1 = m01 * m01 + m02 * m02 + m12 * m12;
+      float lambda0 = fmaxf(m00, fmaxf(m11, m22));
+      float ux = 1.0f, uy = 0.0f, uz = 0.0f;
+      if (p1 <= 1e-10f) {
+        if (m11 >= m00 && m11 >= m22) {
+          ux = 0.0f; uy = 1.0f; uz = 0.0f;
+        } else if (m22 >= m00 && m22 >= m11) {
+          ux = 0.0f; uy = 0.0f; uz = 1.0f;
+        }
+      } else {
+        const float q = (m00 + m11 + m22) / 3.0f;
+        const float d0 = m00 - q, d1 = m11 - q, d2 = m22 - q;
+        const float p2 = d0 * d0 + d1 * d1 + d2 * d2 + 2.0f * p1;
+        const float p = sqrtf(fmaxf(p2 / 6.0f, 1e-12f));
+        const float inv_p = 1.0f / p;
+        const float b00 = d0 * inv_p, b11 = d1 * inv_p, b22 = d2 * inv_p;
+        const float b01 = m01 * inv_p, b02 = m02 * inv_p, b12 = m12 * inv_p;
+        const float det_b = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) +
+                            b02 * (b01 * b12 - b11 * b02);
+        const float r = clampf(0.5f * det_b, -1.0f, 1.0f);
+        const float phi = cgs_acosf(r) / 3.0f;
+        lambda0 = q + 2.0f * p * cgs_cosf(phi);
+        const float r0x = m00 - lambda0, r0y = m01, r0z = m02;
+        const float r1x = m01, r1y = m11 - lambda0, r1z = m12;
+        const float r2x = m02, r2y = m12, r2z = m22 - lambda0;
+        const float c01x = r0y * r1z - r0z * r1y, c01y = r0z * r1x - r0x * r1z,
+                    c01z = r0x * r1y - r0y * r1x;
+        const float n01 = c01x * c01x + c01y * c01y + c01z * c01z;
+        const float c12x = r1y * r2z - r1z * r2y, c12y = r1z * r2x - r1x * r2z,
+                    c12z = r1x * r2y - r1y * r2x;
+        const float n12 = c12x * c12x + c12y * c12y + c12z * c12z;
+        const float c02x = r0y * r2z - r0z * r2y, c02y = r0z * r2x - r0x * r2z,
+                    c02z = r0x * r2y - r0y * r2x;
+        const float n02 = c02x * c02x + c02y * c02y + c02z * c02z;
+        if (n01 >= n12 && n01 >= n02 && n01 > 1e-12f) {
+          const float inv = 1.0f / sqrtf(n01);
+          ux = c01x * inv; uy = c01y * inv; uz = c01z * inv;
+        } else if (n12 >= n02 && n12 > 1e-12f) {
+          const float inv = 1.0f / sqrtf(n12);
+          ux = c12x * inv; uy = c12y * inv; uz = c12z * inv;
+        } else if (n02 > 1e-12f) {
+          const float inv = 1.0f / sqrtf(n02);
+          ux = c02x * inv; uy = c02y * inv; uz = c02z * inv;
+        }
+      }
+      const float safe_l0 = fmaxf(lambda0, 1e-8f);
+      const float offset_mag = 0.5f * sqrtf(safe_l0);
+      const float dx = ux * offset_mag, dy = uy * offset_mag, dz = uz * offset_mag;
+      const float shrink = 0.75f * safe_l0;
+      float c00 = fmaxf(1e-8f, m00 - shrink * ux * ux);
+      const float c01 = m01 - shrink * ux * uy;
+      const float c02 = m02 - shrink * ux * uz;
+      float c11 = fmaxf(1e-8f, m11 - shrink * uy * uy);
+      const float c12 = m12 - shrink * uy * uz;
+      float c22 = fmaxf(1e-8f, m22 - shrink * uz * uz);
+      float child_alpha = alpha_prime;
+      if (a.mip > 0.0f) mip3d(c00, c01, c02, c11, c12, c22, child_alpha, a.mip);
+      out_pos = make_float4(px - dx, py - dy, pz - dz, child_alpha);
+      out_cova = make_float4(c00, c01, c02, c11);
+      out_covb = make_float2(c12, c22);
+      cx = px + dx;
+      cy = py + dy;
+      cz = pz + dz;
+    }
+  }
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(kDeformThreads, 4) k_deform(DeformArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_sums[32];
   __shared__ uint32_t s_base;
@@ -337,6 +546,11 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
   }
   tile -= tet_blocks;
   if (!SPLIT && tile == 0 && threadIdx.x == 0) *a.split_count = 0u;
+  const uint32_t num_tiles = (a.n + kDeformThreads - 1) / kDeformThreads;
+  if (tile >= num_tiles) return;
+  uint32_t i = tile * kDeformThreads + threadIdx.x;
+  DeformIn g{};
+  if (i < a.n) g = deform_load(a, i);
   if (tet_blocks) {
     // Wait (bounded) until every tet block has published; the tet data is
     // then read with ld.global.ca (L1-cached, ordered after the acquire; no
@@ -356,198 +570,43 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
     }
     __syncthreads();
   }
-  const uint32_t i = tile * kDeformThreads + threadIdx.x;
+  if (!SPLIT) {
+    // Persistent: the launch's Gaussian blocks take tiles tile, tile + stride,
+    // ... and load the next tile's inputs before deforming the current one.
+    const uint32_t stride = gridDim.x - tet_blocks;
+    for (;;) {
+      const uint32_t next = tile + stride;
+      const uint32_t ni = next * kDeformThreads + threadIdx.x;
+      DeformIn gn{};
+      if (next < num_tiles && ni < a.n) gn = deform_load(a, ni);
+      if (i < a.n) {
+        bool split = false;
+        float cx, cy, cz;
+        float4 out_pos, out_cova;
+        float2 out_covb;
+        deform_one<false>(a, g, split, cx, cy, cz, out_pos, out_cova, out_covb);
+        a.def_pos[i] = out_pos;
+        a.def_cova[i] = out_cova;
+        a.def_covb[i] = out_covb;
+      }
+      if (next >= num_tiles) break;
+      tile = next;
+      i = ni;
+      g = gn;
+    }
+    return;
+  }
   bool split = false;
-  uint32_t tet_raw = kInvalid;
   float cx = 0.0f, cy = 0.0f, cz = 0.0f;
   float4 out_pos = make_float4(0, 0, 0, 0), out_cova = make_float4(0, 0, 0, 0);
   float2 out_covb = make_float2(0, 0);
   if (i < a.n) {
-    tet_raw = a.bind_tet[i];
-    const float4 rp = a.rest_pos[i];
-    const float4 rca = a.rest_cova[i];
-    const float2 rcb = a.rest_covb[i];
-    if (tet_raw == kMvcBound && a.mvc_xf) {
-      // Polygon-cage binding (deform_scene_cpu, mvc.rs:616-749): position and
-      // F from k_mvc_jacobian, rotation for SH, F S F^T, opacity unchanged.
-      const uint32_t slot = __float_as_uint(a.bind_w[i].x);
-      const float4 q0 = a.mvc_xf[3 * (size_t)slot], q1 = a.mvc_xf[3 * (size_t)slot + 1],
-                   q2 = a.mvc_xf[3 * (size_t)slot + 2];
-      const GM3 Fm = {{q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
-      const GM3 R = polar_rotation(Fm);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) a.mvc_R[9 * (size_t)slot + k] = R.c[k];
-      const GM3 S = {{rca.x, rca.y, rca.z, rca.y, rca.w, rcb.x, rca.z, rcb.x, rcb.y}};
-      const GM3 m = gm3_mul(gm3_mul(Fm, S), gm3_t(Fm));
-      float cv[6] = {m.c[0], m.c[1], m.c[2], m.c[4], m.c[5], m.c[8]};
-      float alpha = rp.w;
-      if (SPLIT && a.split_threshold > 0.0f) {
-        // jacobian_singular_values (polar.rs:89-109): sigma_1 of F
-        const GM3 C = gm3_mul(gm3_t(Fm), Fm);
-        const float packed[6] = {C.c[0], C.c[1], C.c[2], C.c[4], C.c[5], C.c[8]};
-        float ev[3];
-        GM3 basis;
-        sym_eigen3_f64(packed, ev, basis);
-        split = sqrtf(fmaxf(ev[0], 0.0f)) > a.split_threshold;
-      }
-      if (!split) {
-        if (a.mip > 0.0f) mip3d_cpu(cv, alpha, a.mip);
-        out_pos = make_float4(q0.x, q0.y, q0.z, alpha);
-      } else {
-        // split_gaussian_along_major_axis (math/covariance.rs:331-378)
-        float ev[3];
-        GM3 B;
-        sym_eigen3_f64(cv, ev, B);
-        const float min_var = 1e-4f * 1e-4f;
-        const GM3 D = {{fmaxf(ev[0] * 0.25f, min_var), 0, 0, 0, fmaxf(ev[1], min_var), 0, 0, 0,
-                        fmaxf(ev[2], min_var)}};
-        float ax[3] = {B.c[0], B.c[1], B.c[2]};
-        const float len2 = gdot(ax, ax);
-        if (len2 > 0.0f) {
-          const float inv = 1.0f / sqrtf(len2);
-          ax[0] *= inv; ax[1] *= inv; ax[2] *= inv;
-        }
-        const float om = 0.5f * sqrtf(fmaxf(ev[0], min_var));
-        const GM3 cm = gm3_mul(gm3_mul(B, D), gm3_t(B));
-        cv[0] = cm.c[0]; cv[1] = cm.c[1]; cv[2] = cm.c[2];
-        cv[3] = cm.c[4]; cv[4] = cm.c[5]; cv[5] = cm.c[8];
-        if (a.mip > 0.0f) mip3d_cpu(cv, alpha, a.mip);
-        const float ox = ax[0] * om, oy = ax[1] * om, oz = ax[2] * om;
-        out_pos = make_float4(q0.x + (-ox), q0.y + (-oy), q0.z + (-oz), alpha);
-        cx = q0.x + ox;
-        cy = q0.y + oy;
-        cz = q0.z + oz;
-      }
-      out_cova = make_float4(cv[0], cv[1], cv[2], cv[3]);
-      out_covb = make_float2(cv[4], cv[5]);
-    } else if (tet_raw >= a.num_tets) {
-      // Unbound: rest pose plus the Mip filter (deformation.rs:899-947).
-      float xx = rca.x, xy = rca.y, xz = rca.z, yy = rca.w, yz = rcb.x, zz = rcb.y;
-      float alpha = rp.w;
-      if (a.mip > 0.0f) mip3d(xx, xy, xz, yy, yz, zz, alpha, a.mip);
-      out_pos = make_float4(rp.x, rp.y, rp.z, alpha);
-      out_cova = make_float4(xx, xy, xz, yy);
-      out_covb = make_float2(yz, zz);
-    } else {
-      const float4 w = a.bind_w[i];
-      const uint4 e = __ldg(&a.elems[tet_raw]);
-      const float* v0 = a.verts + 3 * (size_t)e.x;
-      const float* v1 = a.verts + 3 * (size_t)e.y;
-      const float* v2 = a.verts + 3 * (size_t)e.z;
-      const float* v3 = a.verts + 3 * (size_t)e.w;
-      const float px = w.x * __ldg(v0) + w.y * __ldg(v1) + w.z * __ldg(v2) + w.w * __ldg(v3);
-      const float py =
-          w.x * __ldg(v0 + 1) + w.y * __ldg(v1 + 1) + w.z * __ldg(v2 + 1) + w.w * __ldg(v3 + 1);
-      const float pz =
-          w.x * __ldg(v0 + 2) + w.y * __ldg(v1 + 2) + w.z * __ldg(v2 + 2) + w.w * __ldg(v3 + 2);
-      const float* J = a.tet_J + 9 * (size_t)tet_raw;
-      const float j_00 = __ldca(J + 0), j_10 = __ldca(J + 1), j_20 = __ldca(J + 2);
-      const float j_01 = __ldca(J + 3), j_11 = __ldca(J + 4), j_21 = __ldca(J + 5);
-      const float j_02 = __ldca(J + 6), j_12 = __ldca(J + 7), j_22 = __ldca(J + 8);
-      const float s_xx = rca.x, s_xy = rca.y, s_xz = rca.z, s_yy = rca.w, s_yz = rcb.x,
-                  s_zz = rcb.y;
-      const float k_00 = j_00 * s_xx + j_01 * s_xy + j_02 * s_xz;
-      const float k_01 = j_00 * s_xy + j_01 * s_yy + j_02 * s_yz;
-      const float k_02 = j_00 * s_xz + j_01 * s_yz + j_02 * s_zz;
-      const float k_10 = j_10 * s_xx + j_11 * s_xy + j_12 * s_xz;
-      const float k_11 = j_10 * s_xy + j_11 * s_yy + j_12 * s_yz;
-      const float k_12 = j_10 * s_xz + j_11 * s_yz + j_12 * s_zz;
-      const float k_20 = j_20 * s_xx + j_21 * s_xy + j_22 * s_xz;
-      const float k_21 = j_20 * s_xy + j_21 * s_yy + j_22 * s_yz;
-      const float k_22 = j_20 * s_xz + j_21 * s_yz + j_22 * s_zz;
-      const float m00 = fmaxf(1e-4f, k_00 * j_00 + k_01 * j_01 + k_02 * j_02);
-      const float m01 = 0.5f * ((k_00 * j_10 + k_01 * j_11 + k_02 * j_12) +
-                                (k_10 * j_00 + k_11 * j_01 + k_12 * j_02));
-      const float m02 = 0.5f * ((k_00 * j_20 + k_01 * j_21 + k_02 * j_22) +
-                                (k_20 * j_00 + k_21 * j_01 + k_22 * j_02));
-      const float m11 = fmaxf(1e-4f, k_10 * j_10 + k_11 * j_11 + k_12 * j_12);
-      const float m12 = 0.5f * ((k_10 * j_20 + k_11 * j_21 + k_12 * j_22) +
-                                (k_20 * j_10 + k_21 * j_11 + k_22 * j_12));
-      const float m22 = fmaxf(1e-4f, k_20 * j_20 + k_21 * j_21 + k_22 * j_22);
-      const float det_j = j_00 * (j_11 * j_22 - j_12 * j_21) -
-                          j_01 * (j_10 * j_22 - j_12 * j_20) + j_02 * (j_10 * j_21 - j_11 * j_20);
-      const float s_det = clampf(det_j, 0.6f, 1.8f);
-      const float safe_base = clampf(1.0f - rp.w, 1e-4f, 0.999f);
-      const float alpha_prime = clampf(1.0f - cgs_powf(safe_base, 1.0f / s_det), 0.05f, 0.99f);
-      split = SPLIT && a.split_threshold > 0.0f && __ldca(&a.tet_stretch[tet_raw]) > a.split_threshold;
-      if (!split) {
-        float xx = m00, yy = m11, zz = m22, alpha = alpha_prime;
-        if (a.mip > 0.0f) mip3d(xx, m01, m02, yy, m12, zz, alpha, a.mip);
-        out_pos = make_float4(px, py, pz, alpha);
-        out_cova = make_float4(xx, m01, m02, yy);
-        out_covb = make_float2(m12, zz);
-      } else {
-        // Major eigenpair of M by Cardano + cross products (deformation.rs:1066-1143).
-        const float p1 = m01 * m01 + m02 * m02 + m12 * m12;
-        float lambda0 = fmaxf(m00, fmaxf(m11, m22));
-        float ux = 1.0f, uy = 0.0f, uz = 0.0f;
-        if (p1 <= 1e-10f) {
-          if (m11 >= m00 && m11 >= m22) {
-            ux = 0.0f; uy = 1.0f; uz = 0.0f;
-          } else if (m22 >= m00 && m22 >= m11) {
-            ux = 0.0f; uy = 0.0f; uz = 1.0f;
-          }
-        } else {
-          const float q = (m00 + m11 + m22) / 3.0f;
-          const float d0 = m00 - q, d1 = m11 - q, d2 = m22 - q;
-          const float p2 = d0 * d0 + d1 * d1 + d2 * d2 + 2.0f * p1;
-          const float p = sqrtf(fmaxf(p2 / 6.0f, 1e-12f));
-          const float inv_p = 1.0f / p;
-          const float b00 = d0 * inv_p, b11 = d1 * inv_p, b22 = d2 * inv_p;
-          const float b01 = m01 * inv_p, b02 = m02 * inv_p, b12 = m12 * inv_p;
-          const float det_b = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) +
-                              b02 * (b01 * b12 - b11 * b02);
-          const float r = clampf(0.5f * det_b, -1.0f, 1.0f);
-          const float phi = cgs_acosf(r) / 3.0f;
-          lambda0 = q + 2.0f * p * cgs_cosf(phi);
-          const float r0x = m00 - lambda0, r0y = m01, r0z = m02;
-          const float r1x = m01, r1y = m11 - lambda0, r1z = m12;
-          const float r2x = m02, r2y = m12, r2z = m22 - lambda0;
-          const float c01x = r0y * r1z - r0z * r1y, c01y = r0z * r1x - r0x * r1z,
-                      c01z = r0x * r1y - r0y * r1x;
-          const float n01 = c01x * c01x + c01y * c01y + c01z * c01z;
-          const float c12x = r1y * r2z - r1z * r2y, c12y = r1z * r2x - r1x * r2z,
-                      c12z = r1x * r2y - r1y * r2x;
-          const float n12 = c12x * c12x + c12y * c12y + c12z * c12z;
-          const float c02x = r0y * r2z - r0z * r2y, c02y = r0z * r2x - r0x * r2z,
-                      c02z = r0x * r2y - r0y * r2x;
-          const float n02 = c02x * c02x + c02y * c02y + c02z * c02z;
-          if (n01 >= n12 && n01 >= n02 && n01 > 1e-12f) {
-            const float inv = 1.0f / sqrtf(n01);
-            ux = c01x * inv; uy = c01y * inv; uz = c01z * inv;
-          } else if (n12 >= n02 && n12 > 1e-12f) {
-            const float inv = 1.0f / sqrtf(n12);
-            ux = c12x * inv; uy = c12y * inv; uz = c12z * inv;
-          } else if (n02 > 1e-12f) {
-            const float inv = 1.0f / sqrtf(n02);
-            ux = c02x * inv; uy = c02y * inv; uz = c02z * inv;
-          }
-        }
-        const float safe_l0 = fmaxf(lambda0, 1e-8f);
-        const float offset_mag = 0.5f * sqrtf(safe_l0);
-        const float dx = ux * offset_mag, dy = uy * offset_mag, dz = uz * offset_mag;
-        const float shrink = 0.75f * safe_l0;
-        float c00 = fmaxf(1e-8f, m00 - shrink * ux * ux);
-        const float c01 = m01 - shrink * ux * uy;
-        const float c02 = m02 - shrink * ux * uz;
-        float c11 = fmaxf(1e-8f, m11 - shrink * uy * uy);
-        const float c12 = m12 - shrink * uy * uz;
-        float c22 = fmaxf(1e-8f, m22 - shrink * uz * uz);
-        float child_alpha = alpha_prime;
-        if (a.mip > 0.0f) mip3d(c00, c01, c02, c11, c12, c22, child_alpha, a.mip);
-        out_pos = make_float4(px - dx, py - dy, pz - dz, child_alpha);
-        out_cova = make_float4(c00, c01, c02, c11);
-        out_covb = make_float2(c12, c22);
-        cx = px + dx;
-        cy = py + dy;
-        cz = pz + dz;
-      }
-    }
+    deform_one<SPLIT>(a, g, split, cx, cy, cz, out_pos, out_cova, out_covb);
     a.def_pos[i] = out_pos;
     a.def_cova[i] = out_cova;
     a.def_covb[i] = out_covb;
   }
-  if (SPLIT) {
+  {
     uint32_t agg;
     const uint32_t excl = block_exclusive_sum(split ? 1u : 0u, s_warp_sums, &agg);
     if (threadIdx.x < 32) {
@@ -561,9 +620,8 @@ __global__ void __launch_bounds__(kDeformThreads) k_deform(DeformArgs a) {
       a.def_pos[c] = make_float4(cx, cy, cz, out_pos.w);
       a.def_cova[c] = out_cova;
       a.def_covb[c] = out_covb;
-      a.split_meta[base + excl] = make_uint2(i, tet_raw);
+      a.split_meta[base + excl] = make_uint2(i, g.tet_raw);
     }
-    const uint32_t num_tiles = (a.n + kDeformThreads - 1) / kDeformThreads;
     if (tile == num_tiles - 1 && threadIdx.x == 0) *a.split_count = base + agg;
   }
 }
@@ -665,11 +723,26 @@ cudaError_t launch_tet_transforms(const DeformArgs& a, cudaStream_t s) {
 cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s) {
   if (a.n == 0) return a.fuse_tets ? launch_tet_transforms(a, s) : cudaSuccess;
   const uint32_t tet_blocks = a.fuse_tets ? (a.num_tets + kDeformThreads - 1) / kDeformThreads : 0u;
-  const uint32_t blocks = (a.n + kDeformThreads - 1) / kDeformThreads + tet_blocks;
-  if (a.split_threshold > 0.0f)
-    k_deform<true><<<blocks, kDeformThreads, 0, s>>>(a);
-  else
-    k_deform<false><<<blocks, kDeformThreads, 0, s>>>(a);
+  const uint32_t num_tiles = (a.n + kDeformThreads - 1) / kDeformThreads;
+  if (a.split_threshold > 0.0f) {
+    // one tile per block: the children's chained scan runs over the tiles
+    k_deform<true><<<num_tiles + tet_blocks, kDeformThreads, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+  // Persistent Gaussian blocks: as many as the SMs hold beside the tet blocks.
+  static int resident = 0;
+  if (resident == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deform<false>, kDeformThreads, 0);
+    if (e != cudaSuccess) return e;
+    resident = std::max(1, sms * per_sm);
+  }
+  const uint32_t gauss_blocks =
+      std::max<uint32_t>(1u, std::min<uint32_t>(num_tiles, (uint32_t)std::max<int>(1, resident - (int)tet_blocks)));
+  k_deform<false><<<gauss_blocks + tet_blocks, kDeformThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
