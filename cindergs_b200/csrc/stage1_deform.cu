@@ -5,9 +5,9 @@
 //                    steps with chirality fix
 //                    (render/kernels/deformation.rs:684-865).
 //                    In frames the first blocks of the k_deform launch run
-//                    these transforms (tet_transform) and publish a count;
-//                    the Gaussian blocks wait for it (bounded), so Stage 1 is
-//                    one launch.
+//                    these transforms (tet_transform) and publish a count,
+//                    so Stage 1 is one launch; the Gaussian blocks of a
+//                    deform with strain split wait for it (bounded).
 //  k_deform<SPLIT>   per Gaussian: x' = sum w_k x_k, M = J S J^T (diag >= 1e-4,
 //                    symmetrised), det-J opacity, 3D Mip filter, strain split
 //                    along the major eigenvector
@@ -17,10 +17,12 @@
 //                    index), from a block scan chained across blocks, instead
 //                    of the reference's atomic counter whose order varies
 //                    from run to run (deformation.rs:1191). Without the
-//                    split the Gaussian blocks are persistent (as many as
-//                    the SMs hold): each thread loads its next Gaussian's
-//                    60 B while deforming the current one, and the first
-//                    loads are issued before the wait for the tet blocks.
+//                    split the Gaussians evaluate their tet's J from the
+//                    four vertices they load anyway (tet_jacobian, as the
+//                    tet blocks do) and never wait; their blocks are
+//                    persistent (as many as the SMs hold), and each thread
+//                    loads its next Gaussian's 60 B while deforming the
+//                    current one.
 //  k_bind            GPU barycentric binding (TetMesh::bind_point,
 //                    deformation/mod.rs:267-310).
 //
@@ -37,6 +39,29 @@ namespace {
 
 constexpr int kDeformThreads = 256;
 
+// J = D_s D_m^-1 of one tet from its four vertices (x[k] = vertex k's xyz)
+// and its D_m^-1 (column-major), into j (column-major). The tet blocks and the
+// Gaussians of a deform without strain split both evaluate it; with every
+// operation rounded separately (-fmad=false) the two agree bit for bit.
+__device__ __forceinline__ void tet_jacobian(const float (&x)[4][3], const float* __restrict__ a,
+                                             float (&j)[9]) {
+  const float x0x = x[0][0], x0y = x[0][1], x0z = x[0][2];
+  const float ds_00 = x[1][0] - x0x, ds_10 = x[1][1] - x0y, ds_20 = x[1][2] - x0z;
+  const float ds_01 = x[2][0] - x0x, ds_11 = x[2][1] - x0y, ds_21 = x[2][2] - x0z;
+  const float ds_02 = x[3][0] - x0x, ds_12 = x[3][1] - x0y, ds_22 = x[3][2] - x0z;
+  const float a_00 = a[0], a_10 = a[1], a_20 = a[2], a_01 = a[3], a_11 = a[4], a_21 = a[5];
+  const float a_02 = a[6], a_12 = a[7], a_22 = a[8];
+  j[0] = ds_00 * a_00 + ds_01 * a_10 + ds_02 * a_20;
+  j[1] = ds_10 * a_00 + ds_11 * a_10 + ds_12 * a_20;
+  j[2] = ds_20 * a_00 + ds_21 * a_10 + ds_22 * a_20;
+  j[3] = ds_00 * a_01 + ds_01 * a_11 + ds_02 * a_21;
+  j[4] = ds_10 * a_01 + ds_11 * a_11 + ds_12 * a_21;
+  j[5] = ds_20 * a_01 + ds_21 * a_11 + ds_22 * a_21;
+  j[6] = ds_00 * a_02 + ds_01 * a_12 + ds_02 * a_22;
+  j[7] = ds_10 * a_02 + ds_11 * a_12 + ds_12 * a_22;
+  j[8] = ds_20 * a_02 + ds_21 * a_12 + ds_22 * a_22;
+}
+
 // J, sigma_1 and R of tet t (compute_tet_transforms_kernel,
 // deformation.rs:684-865).
 __device__ __forceinline__ void tet_transform(uint32_t t, const float* __restrict__ verts,
@@ -45,26 +70,17 @@ __device__ __forceinline__ void tet_transform(uint32_t t, const float* __restric
                                               float* __restrict__ J_out, float* __restrict__ R_out,
                                               float* __restrict__ S_out) {
   const uint4 e = elems[t];
-  const float* x0 = verts + 3 * (size_t)e.x;
-  const float* x1 = verts + 3 * (size_t)e.y;
-  const float* x2 = verts + 3 * (size_t)e.z;
-  const float* x3 = verts + 3 * (size_t)e.w;
-  const float x0x = x0[0], x0y = x0[1], x0z = x0[2];
-  const float ds_00 = x1[0] - x0x, ds_10 = x1[1] - x0y, ds_20 = x1[2] - x0z;
-  const float ds_01 = x2[0] - x0x, ds_11 = x2[1] - x0y, ds_21 = x2[2] - x0z;
-  const float ds_02 = x3[0] - x0x, ds_12 = x3[1] - x0y, ds_22 = x3[2] - x0z;
-  const float* a = inv_dm + 9 * (size_t)t;
-  const float a_00 = a[0], a_10 = a[1], a_20 = a[2], a_01 = a[3], a_11 = a[4], a_21 = a[5];
-  const float a_02 = a[6], a_12 = a[7], a_22 = a[8];
-  const float j_00 = ds_00 * a_00 + ds_01 * a_10 + ds_02 * a_20;
-  const float j_10 = ds_10 * a_00 + ds_11 * a_10 + ds_12 * a_20;
-  const float j_20 = ds_20 * a_00 + ds_21 * a_10 + ds_22 * a_20;
-  const float j_01 = ds_00 * a_01 + ds_01 * a_11 + ds_02 * a_21;
-  const float j_11 = ds_10 * a_01 + ds_11 * a_11 + ds_12 * a_21;
-  const float j_21 = ds_20 * a_01 + ds_21 * a_11 + ds_22 * a_21;
-  const float j_02 = ds_00 * a_02 + ds_01 * a_12 + ds_02 * a_22;
-  const float j_12 = ds_10 * a_02 + ds_11 * a_12 + ds_12 * a_22;
-  const float j_22 = ds_20 * a_02 + ds_21 * a_12 + ds_22 * a_22;
+  const uint32_t vi[4] = {e.x, e.y, e.z, e.w};
+  float x[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[k][c] = verts[3 * (size_t)vi[k] + c];
+  float jm[9];
+  tet_jacobian(x, inv_dm + 9 * (size_t)t, jm);
+  const float j_00 = jm[0], j_10 = jm[1], j_20 = jm[2];
+  const float j_01 = jm[3], j_11 = jm[4], j_21 = jm[5];
+  const float j_02 = jm[6], j_12 = jm[7], j_22 = jm[8];
   float* J = J_out + 9 * (size_t)t;
   J[0] = j_00; J[1] = j_10; J[2] = j_20; J[3] = j_01; J[4] = j_11; J[5] = j_21;
   J[6] = j_02; J[7] = j_12; J[8] = j_22;
@@ -406,19 +422,29 @@ __device__ __forceinline__ void deform_one(const DeformArgs& a, const DeformIn& 
   } else {
     const float4 w = g.w;
     const uint4 e = __ldg(&a.elems[tet_raw]);
-    const float* v0 = a.verts + 3 * (size_t)e.x;
-    const float* v1 = a.verts + 3 * (size_t)e.y;
-    const float* v2 = a.verts + 3 * (size_t)e.z;
-    const float* v3 = a.verts + 3 * (size_t)e.w;
-    const float px = w.x * __ldg(v0) + w.y * __ldg(v1) + w.z * __ldg(v2) + w.w * __ldg(v3);
-    const float py =
-        w.x * __ldg(v0 + 1) + w.y * __ldg(v1 + 1) + w.z * __ldg(v2 + 1) + w.w * __ldg(v3 + 1);
-    const float pz =
-        w.x * __ldg(v0 + 2) + w.y * __ldg(v1 + 2) + w.z * __ldg(v2 + 2) + w.w * __ldg(v3 + 2);
-    const float* J = a.tet_J + 9 * (size_t)tet_raw;
-    const float j_00 = __ldca(J + 0), j_10 = __ldca(J + 1), j_20 = __ldca(J + 2);
-    const float j_01 = __ldca(J + 3), j_11 = __ldca(J + 4), j_21 = __ldca(J + 5);
-    const float j_02 = __ldca(J + 6), j_12 = __ldca(J + 7), j_22 = __ldca(J + 8);
+    const uint32_t vi[4] = {e.x, e.y, e.z, e.w};
+    float x[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) x[k][c] = __ldg(a.verts + 3 * (size_t)vi[k] + c);
+    const float px = w.x * x[0][0] + w.y * x[1][0] + w.z * x[2][0] + w.w * x[3][0];
+    const float py = w.x * x[0][1] + w.y * x[1][1] + w.z * x[2][1] + w.w * x[3][1];
+    const float pz = w.x * x[0][2] + w.y * x[1][2] + w.z * x[2][2] + w.w * x[3][2];
+    float jm[9];
+    if (SPLIT) {
+      // the tet blocks' J (this variant waited for them)
+      const float* J = a.tet_J + 9 * (size_t)tet_raw;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) jm[k] = __ldca(J + k);
+    } else {
+      // J of the Gaussian's tet evaluated here from the vertices just loaded,
+      // as the tet blocks evaluate it, so this variant never waits for them
+      tet_jacobian(x, a.inv_dm + 9 * (size_t)tet_raw, jm);
+    }
+    const float j_00 = jm[0], j_10 = jm[1], j_20 = jm[2];
+    const float j_01 = jm[3], j_11 = jm[4], j_21 = jm[5];
+    const float j_02 = jm[6], j_12 = jm[7], j_22 = jm[8];
     const float s_xx = rca.x, s_xy = rca.y, s_xz = rca.z, s_yy = rca.w, s_yz = rcb.x,
                 s_zz = rcb.y;
     const float k_00 = j_00 * s_xx + j_01 * s_xy + j_02 * s_xz;
@@ -551,8 +577,10 @@ __global__ void __launch_bounds__(kDeformThreads, 4) k_deform(DeformArgs a) {
   uint32_t i = tile * kDeformThreads + threadIdx.x;
   DeformIn g{};
   if (i < a.n) g = deform_load(a, i);
-  if (tet_blocks) {
-    // Wait (bounded) until every tet block has published; the tet data is
+  if (SPLIT && tet_blocks) {
+    // Wait (bounded) until every tet block has published (the split needs
+    // their sigma_1; without it the Gaussians evaluate their tets' J
+    // themselves and the tet blocks only serve the later stages); the tet data is
     // then read with ld.global.ca (L1-cached, ordered after the acquire; no
     // SM has cached those lines earlier in this launch, and L1 holds no lines
     // from earlier launches), never through the incoherent read-only path. A
