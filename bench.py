@@ -13,7 +13,8 @@ the frame's formulas on a sample, against the f32 frame), `mvc` (the
 polygon-cage leg below, with fewer frames) and `views` (the multi-view leg
 below); `--no-legs` leaves them out. `e2e` runs the same frames through the C
 ABI with the cage vertices uploaded and the RGBA8 frame read back every step,
-and reports the host time per step by part.
+three timed runs of K frames of which the median is reported (all three are
+listed), and reports the host time per step by part.
 
 Arms:
   python bench.py [--gpus N --steps K --warmup W]     this library (CUDA, sm_100a)
@@ -350,9 +351,6 @@ def run_ours(args):
     import ctypes
     from cindergs_b200 import _abi
     lib, ctx = st._lib, st.handle
-    e2e_frames = [frame + world * i for i in range(args.steps)]
-    cams_c = [st._camera(wl.camera(f)) for f in e2e_frames]
-    comps_c = [st._compositor(wl.compositor(wl.camera(f))) for f in e2e_frames]
     params_c = _abi.CgsFrameParams(float(wl.strain_split_threshold), float(wl.mip_filter_3d_var),
                                    1.0 / 255.0, 0.5, 0, 0, 0, int(args.radix_bits),
                                    int(args.entry_sort), int(args.tile_shape))
@@ -362,43 +360,62 @@ def run_ours(args):
     nverts = wl.cage.mesh.rest_vertices.shape[0]
     vert_host = np.empty((nverts, 3), np.float32)
     ticket = ctypes.c_uint64()
-    host_ms = {"spring_step": 0.0, "enqueue": 0.0, "readback_wait": 0.0}
-    barrier()
-    t0 = time.perf_counter()
-    e2e_start = torch.cuda.Event(enable_timing=True)
-    e2e_end = torch.cuda.Event(enable_timing=True)
-    e2e_start.record(stream)
-    prev_ticket = None
-    for step in range(args.steps):
-        ta = time.perf_counter()
-        wl.step()
-        vert_host[:] = wl.cage.vertices()
-        tb = time.perf_counter()
-        _abi.check(lib.cgs_cage_vertices_update(ctx, vert_host.ctypes.data_as(ctypes.c_void_p),
-                                                nverts), "cgs_cage_vertices_update", ctx)
-        _abi.check(lib.cgs_execute_frame(ctx, ctypes.byref(cams_c[step]),
-                                         ctypes.byref(comps_c[step]), ctypes.byref(params_c),
-                                         None), "cgs_execute_frame", ctx)
-        _abi.check(lib.cgs_readback_rgba8_async(ctx, out_ptr[step % 2], args.width, args.height,
-                                                ctypes.byref(ticket)),
-                   "cgs_readback_rgba8_async", ctx)
-        tc = time.perf_counter()
-        if prev_ticket is not None:  # the previous frame's pixels are on the host
+
+    def e2e_run(frame0):
+        """K frames through the C ABI; returns (ms over ranks, host ms by part, wall, device)."""
+        e2e_frames = [frame0 + world * i for i in range(args.steps)]
+        cams_c = [st._camera(wl.camera(f)) for f in e2e_frames]
+        comps_c = [st._compositor(wl.compositor(wl.camera(f))) for f in e2e_frames]
+        host_ms = {"spring_step": 0.0, "enqueue": 0.0, "readback_wait": 0.0}
+        barrier()
+        t0 = time.perf_counter()
+        e2e_start = torch.cuda.Event(enable_timing=True)
+        e2e_end = torch.cuda.Event(enable_timing=True)
+        e2e_start.record(stream)
+        prev_ticket = None
+        for step in range(args.steps):
+            ta = time.perf_counter()
+            wl.step()
+            vert_host[:] = wl.cage.vertices()
+            tb = time.perf_counter()
+            _abi.check(lib.cgs_cage_vertices_update(ctx, vert_host.ctypes.data_as(ctypes.c_void_p),
+                                                    nverts), "cgs_cage_vertices_update", ctx)
+            _abi.check(lib.cgs_execute_frame(ctx, ctypes.byref(cams_c[step]),
+                                             ctypes.byref(comps_c[step]), ctypes.byref(params_c),
+                                             None), "cgs_execute_frame", ctx)
+            _abi.check(lib.cgs_readback_rgba8_async(ctx, out_ptr[step % 2], args.width,
+                                                    args.height, ctypes.byref(ticket)),
+                       "cgs_readback_rgba8_async", ctx)
+            tc = time.perf_counter()
+            if prev_ticket is not None:  # the previous frame's pixels are on the host
+                _abi.check(lib.cgs_readback_wait(ctx, prev_ticket), "cgs_readback_wait", ctx)
+            prev_ticket = ticket.value
+            td = time.perf_counter()
+            host_ms["spring_step"] += (tb - ta) * 1000.0
+            host_ms["enqueue"] += (tc - tb) * 1000.0
+            host_ms["readback_wait"] += (td - tc) * 1000.0
+        if prev_ticket is not None:
             _abi.check(lib.cgs_readback_wait(ctx, prev_ticket), "cgs_readback_wait", ctx)
-        prev_ticket = ticket.value
-        td = time.perf_counter()
-        host_ms["spring_step"] += (tb - ta) * 1000.0
-        host_ms["enqueue"] += (tc - tb) * 1000.0
-        host_ms["readback_wait"] += (td - tc) * 1000.0
-    if prev_ticket is not None:
-        _abi.check(lib.cgs_readback_wait(ctx, prev_ticket), "cgs_readback_wait", ctx)
-    e2e_end.record(stream)
-    barrier()
+        e2e_end.record(stream)
+        barrier()
+        wall = (time.perf_counter() - t0) * 1000.0
+        dev = e2e_start.elapsed_time(e2e_end)
+        return max_over_ranks(max(dev, wall), device=f"cuda:{local}"), host_ms, wall, dev
+
+    # One untimed run first (the readback path's first use: its snapshot
+    # buffers, copy stream and page-locked staging), then three runs of K
+    # frames each, every copy inside each timed region; the median run is
+    # reported (the GPUs' host links are shared with other jobs, and one
+    # stalled copy should not set the figure), all three are listed.
+    e2e_run(frame)
     frame += world * args.steps
-    e2e_wall = (time.perf_counter() - t0) * 1000.0
-    e2e_dev = e2e_start.elapsed_time(e2e_end)
-    e2e_ms = max_over_ranks(max(e2e_dev, e2e_wall), device=f"cuda:{local}")
+    e2e_runs = []
+    for _ in range(3):
+        e2e_runs.append(e2e_run(frame))
+        frame += world * args.steps
+    e2e_ms, host_ms, e2e_wall, e2e_dev = sorted(e2e_runs, key=lambda r: r[0])[1]
     e2e_value = world * args.steps / (e2e_ms / 1000.0)
+    e2e_all = [world * args.steps / (r[0] / 1000.0) for r in e2e_runs]
     e2e_parts = {k: v / args.steps for k, v in host_ms.items()}
     e2e_parts["wall_ms_per_step"] = e2e_wall / args.steps
     e2e_parts["device_ms_per_step"] = e2e_dev / args.steps
@@ -492,6 +509,7 @@ def run_ours(args):
                     int(wl.cage.mesh.rest_vertices.nbytes) + 96 + 48 + 40,
                     "d2h_bytes_per_step": int(args.width * args.height * 4 + 36),
                     "host_ms_per_step": e2e_parts,
+                    "runs": e2e_all, "reported": "median of 3 timed runs of K frames",
                     "path": "C ABI: cage vertices up, frame, asynchronous RGBA8 readback"},
             "gpu_launches": gpu_launches,
             "clocks": clock.summary(),
